@@ -1,0 +1,130 @@
+/* thorx — B200-native HE-VI dynamical core and double-gray RT for THOR, C ABI.
+ *
+ * One context owns one simulation on one GPU: the grid geometry, the prognostic state and the
+ * scratch of the dynamical core, all resident in device memory in a column-index-fastest
+ * layout. Host buffers passed across this interface use the reference THOR layouts:
+ *   cell scalar    [col][lev]            (ESP::Rho_d, pressure_d, ...   src/headers/esp.h:226-371)
+ *   cell vector    [col][lev][xyz]       (ESP::Mh_d)
+ *   interface      [col][lev+1]          (ESP::Wh_d)
+ *   grid arrays    as built by Icogrid   (src/ESP/grid.cu:84-302)
+ * so that ESP can hand its own arrays over unchanged.
+ *
+ * Every function returns 0 on success and a negative THORX_E* code on error; the message of the
+ * last error of a context is available from thorx_last_error(). Nothing calls exit().
+ * One host thread per context. All work is ordered on the context's CUDA stream.
+ */
+#ifndef THORX_H
+#define THORX_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define THORX_OK 0
+#define THORX_E_ARG -1      /* bad argument (null pointer, bad size, unknown name)        */
+#define THORX_E_CUDA -2     /* a CUDA call failed (message has the CUDA error string)     */
+#define THORX_E_NAN -3      /* the NaN check after the physics step tripped               */
+#define THORX_E_UNSUPPORTED -4 /* option outside what this build implements               */
+#define THORX_E_STATE -5    /* call out of order (e.g. stepping before the state is set)  */
+
+typedef struct thorx_ctx thorx_ctx;
+
+/* Grid geometry, reference layouts (Icogrid members, src/headers/grid.h:66-117).
+ * The pointers are read during thorx_create only. */
+typedef struct {
+    int           point_num;  /* 2 + 10 * 4^glevel                                    */
+    int           nv;         /* vertical layers                                       */
+    int           nl_region;  /* rhombus side (16 for glevel 4..7)                     */
+    int           nr;         /* number of rhombi                                      */
+    int           glevel;
+    const int*    maps;        /* [nr][(nl_region+2)^2]                                 */
+    const int*    point_local; /* [point_num][6]                                        */
+    const double* Altitude;    /* [nv]                                                  */
+    const double* Altitudeh;   /* [nv+1]                                                */
+    const double* lonlat;      /* [point_num][2]                                        */
+    const double* areas;       /* [point_num][6][3]                                     */
+    const double* areasTr;     /* [point_num][6]                                        */
+    const double* areasT;      /* [point_num]                                           */
+    const double* nvecoa;      /* [point_num][6][3]                                     */
+    const double* nvecti;      /* [point_num][6][3]                                     */
+    const double* nvecte;      /* [point_num][6][3]                                     */
+    const double* div;         /* [point_num][7][3]                                     */
+    const double* grad;        /* [point_num][7][3]                                     */
+    const double* func_r;      /* [point_num][3]                                        */
+} thorx_grid;
+
+/* Precision forms of the dynamical core. */
+#define THORX_FP64 0  /* every operation in FP64                                                */
+#define THORX_MIXED 1 /* horizontal stencils and tendencies in FP32; Thomas solve, pressure and
+                         density update, hydrostatic/effective-gravity integration and global
+                         sums in FP64                                                          */
+
+/* Thermodynamic equation (reference .thr key thermo_equation). */
+#define THORX_ENTROPY 0
+#define THORX_ENERGY 1
+
+/* Benchmark forcing (reference .thr key core_benchmark). */
+#define THORX_NO_BENCHMARK 0
+#define THORX_HELD_SUAREZ 1
+
+/* Simulation switches: the SimulationSetup members the step reads
+ * (src/headers/simulation_setup.h) and the .thr keys they come from. */
+typedef struct {
+    double A;            /* radius [m]                        (radius)          */
+    double Omega;        /* rotation rate [1/s]               (rotation_rate)   */
+    double Gravit;       /* gravity [m/s^2]                   (gravitation)     */
+    double Rd;           /* gas constant [J/kg/K]             (Rd)              */
+    double Cp;           /* heat capacity [J/kg/K]            (Cp)              */
+    double P_Ref;        /* reference pressure [Pa]           (P_ref)           */
+    double Top_altitude; /* model top [m]                     (Top_altitude)    */
+    double timestep;     /* large step [s]                    (timestep)        */
+    double Diffc;        /* hyperdiffusion coefficient        (Diffc)           */
+    double DivDampc;     /* divergence damping coefficient    (DivDampc)        */
+    int    HyDiffOrder;  /* even, >= 4                        (HyDiffOrder)     */
+    int    DeepModel;    /*                                   (DeepModel)       */
+    int    NonHydro;     /*                                   (NonHydro)        */
+    int    GravHeightVar;/*                                   (GravHeightVar)   */
+    int    HyDiff;       /*                                   (HyDiff)          */
+    int    DivDampP;     /*                                   (DivDampP)        */
+    int    thermo_equation; /* THORX_ENTROPY | THORX_ENERGY   (thermo_equation) */
+    int    core_benchmark;  /* THORX_NO_BENCHMARK | THORX_HELD_SUAREZ           */
+    int    precision;       /* THORX_FP64 | THORX_MIXED                         */
+} thorx_params;
+
+/* Creates a context on the current CUDA device. `stream` is a cudaStream_t (NULL: the context
+ * creates its own non-blocking stream). Replaces the device allocation and geometry upload of
+ * ESP::ESP / ESP::alloc_data / initial_values (src/ESP/esp_initial.cu:68-484,1292-1393). */
+int thorx_create(const thorx_grid* grid, const thorx_params* params, void* stream,
+                 thorx_ctx** out);
+void thorx_destroy(thorx_ctx* ctx);
+const char* thorx_last_error(const thorx_ctx* ctx);
+
+/* Copies a named field between a host buffer in the reference layout and the device.
+ * Names are the reference ESP member names without the _d suffix: "Rho", "pressure", "Mh",
+ * "Wh", "W", "temperature", "Rd", "Cp", "profx_Qheat", and the slow-mode tendencies of the last
+ * RK stage "SlowMh", "SlowWh", "SlowRho", "Slowpressure". thorx_field_size gives the element
+ * count of a name (negative if unknown). */
+long thorx_field_size(const thorx_ctx* ctx, const char* name);
+int thorx_set_field(thorx_ctx* ctx, const char* name, const double* host);
+int thorx_get_field(thorx_ctx* ctx, const char* name, double* host);
+
+/* One physics step, ESP::ProfX (src/ESP/profx_driver.cu:70-474): W from Wh, T and potential
+ * temperature from p and rho, Held-Suarez forcing when core_benchmark says so, p = rho Rd T,
+ * and the NaN check (reported at the next synchronising call as THORX_E_NAN). */
+int thorx_profx(thorx_ctx* ctx);
+/* One dynamical-core large step, ESP::Thor (src/ESP/thor_driver.cu:70-1466). */
+int thorx_thor(thorx_ctx* ctx);
+/* `nsteps` x (ProfX, Thor), the inner part of the main loop of src/esp.cu:1382-1398. The first
+ * call captures one step as a CUDA graph; every step is a replay of it. */
+int thorx_step(thorx_ctx* ctx, int nsteps);
+/* Waits for the context's stream; returns THORX_E_NAN if a NaN check tripped since the last
+ * synchronisation. */
+int thorx_sync(thorx_ctx* ctx);
+/* Number of kernels one thorx_step(ctx, 1) launches. */
+int thorx_kernels_per_step(const thorx_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* THORX_H */

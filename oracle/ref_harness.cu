@@ -1,0 +1,563 @@
+// Reference harness: TEST INFRASTRUCTURE ONLY.
+//
+// Compiles the reference's own grid builder (src/ESP/grid.cu) and its own dynamical-core and
+// physics kernels (src/headers/dyn/*.h, src/headers/phy/profx_{auxiliary,held_suarez}.h) into
+// oracle/_ref/libthor_ref.so, and drives them with the launch sequence of
+//   ESP::Thor   src/ESP/thor_driver.cu:70-1466
+//   ESP::ProfX  src/ESP/profx_driver.cu:70-474   (Held-Suarez branch, no sponge, no modules)
+// on one GPU, all FP64, default stream, one launch after another. It is the "reference's own FP64
+// CUDA build" against which the CPU restatement (oracle/thor_oracle.cpp) and the product kernels
+// are checked, and it is the timing of the reference's CUDA kernels on the same B200.
+//
+// Only tests/ (and bench.py's reference-CUDA side leg) load this library. The product never does.
+//
+// Subset mirrored (the configurations this repository measures): entropy or energy equation,
+// HyDiff of any even order, DivDampP on/off, DeepModel, NonHydro, GravHeightVar, no Rayleigh
+// sponge, no diffusive sponge, no vertical hyperdiffusion, no ultrahot thermodynamics, no
+// convective adjustment, no increased damping, Held-Suarez forcing on/off.
+
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "vector_operations.h"
+
+#include "dyn/phy_modules_device.h"
+
+#include "dyn/thor_adv_cor.h"
+#include "dyn/thor_auxiliary.h"
+// The RK-array registry itself is defined by the reference's src/ESP/phy_modules_device.cu:47-48,
+// compiled alongside (relocatable device code). It stays empty in every configuration here.
+#include "dyn/thor_diff.h"
+#include "dyn/thor_div.h"
+#include "dyn/thor_fastmodes.h"
+#include "dyn/thor_slowmodes.h"
+#include "dyn/thor_vertical_int.h"
+#include "phy/profx_auxiliary.h"
+#include "phy/profx_held_suarez.h"
+
+#include "grid.h"
+#include "log_writer.h"
+
+FILE* log::pFILE = nullptr;
+
+#define REF_CHECK(call)                                                                           \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess) {                                                                  \
+            std::fprintf(stderr, "ref harness: %s at %s:%d\n", cudaGetErrorString(e_), __FILE__, \
+                         __LINE__);                                                               \
+            return -1;                                                                            \
+        }                                                                                         \
+    } while (0)
+
+// ---------------------------------------------------------------------------------------------
+// Grid
+// ---------------------------------------------------------------------------------------------
+struct RefGrid {
+    Icogrid* g = nullptr;
+    int      glevel;
+    int      nv;
+};
+
+extern "C" void* ref_grid_new(int    glevel,
+                              int    vlevel,
+                              double A,
+                              double top_altitude,
+                              int    sprd,
+                              double spring_beta) {
+    RefGrid* r   = new RefGrid;
+    int max_count = 0;
+    // output path without a cached aux_grid_constructs.h5: the grid is always built from scratch
+    r->g      = new Icogrid(sprd != 0, spring_beta, glevel, vlevel, 20, A, top_altitude, false,
+                       &max_count, false, 2.0, 1000.0, false, 0.7, 1.0, 6.0,
+                       std::string("/nonexistent-thorx-ref-cache"));
+    r->glevel = glevel;
+    r->nv     = vlevel;
+    return r;
+}
+
+extern "C" void ref_grid_dims(void* h, int* point_num, int* nv, int* nl_region, int* nr) {
+    RefGrid* r = (RefGrid*)h;
+    *point_num = r->g->point_num;
+    *nv        = r->g->nv;
+    *nl_region = r->g->nl_region;
+    *nr        = r->g->nr;
+}
+
+// Copies one named grid array into `out`. Returns the number of elements, or -1 for an unknown
+// name. Pass out == nullptr to query the size.
+extern "C" long ref_grid_get(void* h, const char* name, void* out) {
+    RefGrid* r  = (RefGrid*)h;
+    Icogrid* g  = r->g;
+    int      N  = g->point_num;
+    int      nl = g->nl_region;
+    struct Item {
+        const void* p;
+        long        n;
+        size_t      es;
+    };
+    std::map<std::string, Item> m = {
+        {"point_xyz", {g->point_xyz, 3L * N, 8}},
+        {"point_xyzq", {g->point_xyzq, 18L * N, 8}},
+        {"pent_ind", {g->pent_ind, 12, 4}},
+        {"maps", {g->maps, (long)(nl + 2) * (nl + 2) * g->nr, 4}},
+        {"point_local", {g->point_local, 6L * N, 4}},
+        {"Altitude", {g->Altitude, g->nv, 8}},
+        {"Altitudeh", {g->Altitudeh, g->nvi, 8}},
+        {"lonlat", {g->lonlat, 2L * N, 8}},
+        {"areas", {g->areas, 18L * N, 8}},
+        {"areasT", {g->areasT, N, 8}},
+        {"areasTr", {g->areasTr, 6L * N, 8}},
+        {"nvec", {g->nvec, 18L * N, 8}},
+        {"nvecoa", {g->nvecoa, 18L * N, 8}},
+        {"nvecti", {g->nvecti, 18L * N, 8}},
+        {"nvecte", {g->nvecte, 18L * N, 8}},
+        {"mvec", {g->mvec, 18L * N, 8}},
+        {"div", {g->div, 21L * N, 8}},
+        {"grad", {g->grad, 21L * N, 8}},
+        {"curlz", {g->curlz, 21L * N, 8}},
+        {"func_r", {g->func_r, 3L * N, 8}},
+    };
+    auto it = m.find(name);
+    if (it == m.end())
+        return -1;
+    if (out)
+        std::memcpy(out, it->second.p, it->second.n * it->second.es);
+    return it->second.n;
+}
+
+extern "C" void ref_grid_free(void* h) {
+    RefGrid* r = (RefGrid*)h;
+    r->g->free_memory();
+    delete r->g;
+    delete r;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Simulation state on the device, reference layout ([col][lev], [col][lev][xyz], [col][lev+1])
+// ---------------------------------------------------------------------------------------------
+struct ref_params {
+    double A, Omega, Gravit, Rd, Cp, P_Ref, timestep, Diffc, DivDampc;
+    int    HyDiffOrder;
+    int    DeepModel, NonHydro, GravHeightVar, HyDiff, DivDampP, energy_equation, held_suarez;
+    int    glevel;
+};
+
+struct RefSim {
+    ref_params                     p;
+    int                            N, nv, nvi, nl_region, nr;
+    std::map<std::string, double*> f;    // device fields
+    std::map<std::string, long>    size; // element counts
+    int*                           maps_d        = nullptr;
+    int*                           point_local_d = nullptr;
+    unsigned int*                  diag_flag_d   = nullptr;
+    diag_data*                     diag_data_d   = nullptr;
+    double*                        Altitude_h    = nullptr;
+};
+
+static int sim_alloc(RefSim* s, const char* name, long n) {
+    double* d = nullptr;
+    REF_CHECK(cudaMalloc(&d, n * sizeof(double)));
+    REF_CHECK(cudaMemset(d, 0, n * sizeof(double)));
+    s->f[name]    = d;
+    s->size[name] = n;
+    return 0;
+}
+
+extern "C" void* ref_sim_new(void* gh, const ref_params* p) {
+    RefGrid* rg = (RefGrid*)gh;
+    Icogrid* g  = rg->g;
+    RefSim*  s  = new RefSim;
+    s->p        = *p;
+    s->N        = g->point_num;
+    s->nv       = g->nv;
+    s->nvi      = g->nvi;
+    s->nl_region = g->nl_region;
+    s->nr       = g->nr;
+    long N = s->N, nv = s->nv, nvi = s->nvi;
+
+    const char* cell1[] = {"Rho", "Rhok", "Rhos", "pressure", "pressurek", "pressures",
+                           "temperature", "W", "Wk", "Ws", "h", "pt", "gtil", "SlowRho",
+                           "Slowpressure", "Sp", "Sd", "diffw", "diffrh", "diffpr", "diffwv",
+                           "diffrv", "diffprv", "epotential", "ekinetic", "Etotal", "Cp", "Rd",
+                           "profx_Qheat", "profx_dW"};
+    const char* cell3[] = {"Mh", "Mhk", "Mhs", "Adv", "v", "SlowMh", "DivM", "divg_Mh",
+                           "diffmh", "diffmv", "profx_dMh"};
+    const char* iface[] = {"Wh", "Whk", "Whs", "hh", "pth", "gtilh", "SlowWh", "epotentialh",
+                           "ekinetich", "profx_dWh"};
+    const char* cell6[] = {"diff", "diff_sponge", "diff2", "boundary_flux"};
+    for (auto n : cell1)
+        if (sim_alloc(s, n, N * nv))
+            return nullptr;
+    for (auto n : cell3)
+        if (sim_alloc(s, n, 3 * N * nv))
+            return nullptr;
+    for (auto n : iface)
+        if (sim_alloc(s, n, N * nvi))
+            return nullptr;
+    for (auto n : cell6)
+        if (sim_alloc(s, n, 6 * N * nv))
+            return nullptr;
+    for (auto n : {"Kdh4", "Kdhz", "Kdh2"})
+        if (sim_alloc(s, n, nv))
+            return nullptr;
+
+    // geometry (reference layout, copied as built by Icogrid)
+    struct G {
+        const char* n;
+        double*     h;
+        long        c;
+    } geo[] = {{"Altitude", g->Altitude, nv},  {"Altitudeh", g->Altitudeh, nvi},
+               {"lonlat", g->lonlat, 2 * N},   {"areas", g->areas, 18 * N},
+               {"areasT", g->areasT, N},       {"areasTr", g->areasTr, 6 * N},
+               {"nvecoa", g->nvecoa, 18 * N},  {"nvecti", g->nvecti, 18 * N},
+               {"nvecte", g->nvecte, 18 * N},  {"div", g->div, 21 * N},
+               {"grad", g->grad, 21 * N},      {"func_r", g->func_r, 3 * N}};
+    for (auto& x : geo) {
+        if (sim_alloc(s, x.n, x.c))
+            return nullptr;
+        if (cudaMemcpy(s->f[x.n], x.h, x.c * 8, cudaMemcpyHostToDevice) != cudaSuccess)
+            return nullptr;
+    }
+    long nmaps = (long)(s->nl_region + 2) * (s->nl_region + 2) * s->nr;
+    if (cudaMalloc(&s->maps_d, nmaps * sizeof(int)) != cudaSuccess)
+        return nullptr;
+    cudaMemcpy(s->maps_d, g->maps, nmaps * sizeof(int), cudaMemcpyHostToDevice);
+    if (cudaMalloc(&s->point_local_d, 6 * N * sizeof(int)) != cudaSuccess)
+        return nullptr;
+    cudaMemcpy(s->point_local_d, g->point_local, 6 * N * sizeof(int), cudaMemcpyHostToDevice);
+    cudaMalloc(&s->diag_flag_d, sizeof(unsigned int));
+    cudaMemset(s->diag_flag_d, 0, sizeof(unsigned int));
+    cudaMalloc(&s->diag_data_d, N * nvi * sizeof(diag_data));
+
+    s->Altitude_h = new double[nv];
+    std::memcpy(s->Altitude_h, g->Altitude, nv * 8);
+
+    // Hyperdiffusion and divergence-damping strengths (src/ESP/esp_initial.cu:1292-1335,
+    // no diffusive sponge).
+    std::vector<double> kdh4(nv), kdhz(nv);
+    for (int lev = 0; lev < nv; lev++) {
+        double dbar = sqrt(2 * M_PI / 5) * p->A / (pow(2, p->glevel));
+        kdh4[lev]   = (p->Diffc) * pow(dbar, 1.0 * p->HyDiffOrder) / p->timestep;
+        kdhz[lev]   = (p->DivDampc) * pow(dbar, 4.) / p->timestep;
+    }
+    cudaMemcpy(s->f["Kdh4"], kdh4.data(), nv * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(s->f["Kdhz"], kdhz.data(), nv * 8, cudaMemcpyHostToDevice);
+    int zero = 0;
+    cudaMemcpyToSymbol(num_dynamical_arrays, &zero, sizeof(int));
+    if (cudaDeviceSynchronize() != cudaSuccess)
+        return nullptr;
+    return s;
+}
+
+extern "C" long ref_sim_set(void* h, const char* name, const double* host) {
+    RefSim* s  = (RefSim*)h;
+    auto    it = s->f.find(name);
+    if (it == s->f.end())
+        return -1;
+    long n = s->size[name];
+    if (cudaMemcpy(it->second, host, n * 8, cudaMemcpyHostToDevice) != cudaSuccess)
+        return -2;
+    return n;
+}
+
+extern "C" long ref_sim_get(void* h, const char* name, double* host) {
+    RefSim* s  = (RefSim*)h;
+    auto    it = s->f.find(name);
+    if (it == s->f.end())
+        return -1;
+    long n = s->size[name];
+    if (host && cudaMemcpy(host, it->second, n * 8, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return -2;
+    return n;
+}
+
+// One ProfX call, Held-Suarez branch (src/ESP/profx_driver.cu:70-474).
+static int ref_profx(RefSim* s) {
+    auto&     F   = s->f;
+    const int NTH = 256;
+    int       N = s->N, nv = s->nv;
+    dim3      NB((N / NTH) + 1, nv, 1);
+    REF_CHECK(cudaMemset(F["profx_Qheat"], 0, sizeof(double) * N * nv));
+    Recompute_W<<<NB, NTH>>>(F["W"], F["Wh"], F["Altitude"], F["Altitudeh"], N);
+    REF_CHECK(cudaDeviceSynchronize());
+    Compute_temperature<<<NB, NTH>>>(F["temperature"], F["pt"], F["pressure"], F["Rho"],
+                                     s->p.P_Ref, F["Rd"], F["Cp"], N, true);
+    REF_CHECK(cudaDeviceSynchronize());
+    if (s->p.held_suarez) {
+        held_suarez<<<NB, NTH>>>(F["Mh"], F["pressure"], F["Rho"], F["temperature"], s->p.Gravit,
+                                 s->p.Cp, s->p.Rd, F["Altitude"], F["Altitudeh"], F["lonlat"],
+                                 s->p.timestep, N);
+        REF_CHECK(cudaDeviceSynchronize());
+    }
+    Compute_pressure<<<NB, NTH>>>(F["pressure"], F["temperature"], F["Rho"], F["Rd"], N);
+    REF_CHECK(cudaDeviceSynchronize());
+    return 0;
+}
+
+// One ESP::Thor call (src/ESP/thor_driver.cu:70-1466) for the subset described above.
+static int ref_thor(RefSim* s) {
+    auto&      F  = s->f;
+    ref_params P  = s->p;
+    const int  NTH = 256;
+    const int  num_th_vertical_eq = 32;
+    const int  LN                 = 16;
+    int        N = s->N, nv = s->nv, nvi = s->nvi, nl_region = s->nl_region, nr = s->nr;
+    dim3       NT(nl_region, nl_region, 1);
+    dim3       NB(nr, nv, 1);
+    dim3       NBD(nr, nv, 6);
+    dim3       NBDP(2, nv, 6);
+    dim3       NBP(2, nv, 1);
+    dim3       NBALL1((N / NTH) + 1, nv, 1);
+    int*       maps = s->maps_d;
+    int*       loc  = s->point_local_d;
+    bool       deep = P.DeepModel, nonh = P.NonHydro, ghv = P.GravHeightVar;
+    bool       eeq  = P.energy_equation;
+    double     A = P.A, dt = P.timestep;
+
+    REF_CHECK(cudaDeviceSynchronize());
+    cudaMemcpy(F["Mhk"], F["Mh"], N * nv * 3 * 8, cudaMemcpyDeviceToDevice);
+    cudaMemcpy(F["Whk"], F["Wh"], N * nvi * 8, cudaMemcpyDeviceToDevice);
+    cudaMemcpy(F["Wk"], F["W"], N * nv * 8, cudaMemcpyDeviceToDevice);
+    cudaMemcpy(F["Rhok"], F["Rho"], N * nv * 8, cudaMemcpyDeviceToDevice);
+    cudaMemcpy(F["pressurek"], F["pressure"], N * nv * 8, cudaMemcpyDeviceToDevice);
+    cudaMemset(F["Mhs"], 0, 8 * 3 * N * nv);
+    cudaMemset(F["Rhos"], 0, 8 * N * nv);
+    cudaMemset(F["Whs"], 0, 8 * N * nvi);
+    cudaMemset(F["Ws"], 0, 8 * N * nv);
+    cudaMemset(F["pressures"], 0, 8 * N * nv);
+
+    for (int rk = 0; rk < 3; rk++) {
+        int    ns_it = (rk == 0) ? 1 : (rk == 1 ? 3 : 6);
+        double times = (rk == 0) ? dt / 3.0 : dt / 6.0;
+
+        cudaMemset(F["Adv"], 0, 8 * 3 * N * nv);
+        REF_CHECK(cudaDeviceSynchronize());
+        Compute_Advec_Cori1<LN, LN><<<NB, NT>>>(
+            (double3*)F["Adv"], (double3*)F["v"], (double3*)F["Mhk"], (double3*)F["div"], F["Wk"],
+            F["Rhok"], F["Altitude"], A, (double3*)F["func_r"], maps, nl_region, deep);
+        Compute_Advec_Cori_Poles<6><<<2, 1>>>(F["Adv"], F["v"], F["Mhk"], F["div"], F["Wk"],
+                                              F["Rhok"], F["Altitude"], A, F["func_r"], loc, N, nv,
+                                              deep);
+        REF_CHECK(cudaDeviceSynchronize());
+        Compute_Advec_Cori2<<<(N / NTH) + 1, NTH>>>(F["Adv"], F["v"], F["Whk"], F["Rhok"],
+                                                    F["Altitude"], F["Altitudeh"], F["func_r"],
+                                                    P.Omega, A, nv, N, deep);
+        REF_CHECK(cudaDeviceSynchronize());
+        Compute_Temperature_H_Pt_Geff<<<(N / NTH) + 1, NTH>>>(
+            F["temperature"], F["pressurek"], F["Rhok"], F["Mhk"], F["h"], F["hh"], F["pt"],
+            F["pth"], F["gtil"], F["gtilh"], F["Whk"], F["Wk"], F["epotential"], F["epotentialh"],
+            F["ekinetic"], F["ekinetich"], F["Etotal"], P.P_Ref, P.Gravit, F["Cp"], F["Rd"],
+            F["Altitude"], F["Altitudeh"], A, N, nv, true, eeq, ghv);
+        REF_CHECK(cudaDeviceSynchronize());
+        cudaMemset(F["SlowMh"], 0, 8 * 3 * N * nv);
+        cudaMemset(F["SlowWh"], 0, 8 * N * nvi);
+        cudaMemset(F["SlowRho"], 0, 8 * N * nv);
+        cudaMemset(F["Slowpressure"], 0, 8 * N * nv);
+
+        if (P.HyDiff) {
+            cudaMemset(F["diff"], 0, 8 * 6 * N * nv);
+            REF_CHECK(cudaDeviceSynchronize());
+            int stepnum = 0;
+            for (int ihyp = 0; ihyp < P.HyDiffOrder / 2 - 1; ihyp++) {
+                Diffusion_Op<LN, LN><<<NBD, NT>>>(
+                    F["diffmh"], F["diffw"], F["diffrh"], F["diffpr"], F["diff"], F["diff_sponge"],
+                    F["Mhk"], F["Rhok"], F["temperature"], F["Wk"], F["areasTr"], F["areas"],
+                    F["nvecoa"], F["nvecti"], F["nvecte"], F["func_r"], F["Kdh4"], F["Altitude"], A,
+                    F["Rd"], F["Cp"], maps, nl_region, stepnum, false, deep, false, 2, F["Kdh2"],
+                    F["boundary_flux"], eeq, P.HyDiffOrder);
+                Diffusion_Op_Poles<5><<<NBDP, 1>>>(
+                    F["diffmh"], F["diffw"], F["diffrh"], F["diffpr"], F["diff"], F["diff_sponge"],
+                    F["Mhk"], F["Rhok"], F["temperature"], F["Wk"], F["func_r"], F["areasTr"],
+                    F["areas"], F["nvecoa"], F["nvecti"], F["nvecte"], F["Kdh4"], F["Altitude"],
+                    F["Altitudeh"], A, F["Rd"], F["Cp"], loc, N, stepnum, false, deep, false, 2,
+                    F["Kdh2"], F["boundary_flux"], eeq, P.HyDiffOrder);
+                REF_CHECK(cudaDeviceSynchronize());
+                stepnum += 1;
+            }
+            cudaMemset(F["diffrh"], 0, 8 * N * nv);
+            cudaMemset(F["boundary_flux"], 0, 8 * 6 * N * nv);
+            Diffusion_Op<LN, LN><<<NBD, NT>>>(
+                F["diffmh"], F["diffw"], F["diffrh"], F["diffpr"], F["diff"], F["diff_sponge"],
+                F["Mhk"], F["Rhok"], F["temperature"], F["Wk"], F["areasTr"], F["areas"],
+                F["nvecoa"], F["nvecti"], F["nvecte"], F["func_r"], F["Kdh4"], F["Altitude"], A,
+                F["Rd"], F["Cp"], maps, nl_region, stepnum, true, deep, false, 2, F["Kdh2"],
+                F["boundary_flux"], eeq, P.HyDiffOrder);
+            Diffusion_Op_Poles<5><<<NBDP, 1>>>(
+                F["diffmh"], F["diffw"], F["diffrh"], F["diffpr"], F["diff"], F["diff_sponge"],
+                F["Mhk"], F["Rhok"], F["temperature"], F["Wk"], F["func_r"], F["areasTr"],
+                F["areas"], F["nvecoa"], F["nvecti"], F["nvecte"], F["Kdh4"], F["Altitude"],
+                F["Altitudeh"], A, F["Rd"], F["Cp"], loc, N, stepnum, true, deep, false, 2,
+                F["Kdh2"], F["boundary_flux"], eeq, P.HyDiffOrder);
+            REF_CHECK(cudaDeviceSynchronize());
+            Correct_Horizontal<<<NBALL1, NTH>>>(F["diffmh"], F["diffmv"], F["func_r"], N);
+            REF_CHECK(cudaDeviceSynchronize());
+        }
+
+        cudaMemset(F["DivM"], 0, 8 * N * 3 * nv);
+        cudaMemset(F["divg_Mh"], 0, 8 * N * 3 * nv);
+        if (P.DivDampP) {
+            REF_CHECK(cudaDeviceSynchronize());
+            for (int pass = 0; pass < 2; pass++) {
+                DivM_Op<LN, LN><<<NB, NT>>>(F["DivM"], F["divg_Mh"], F["Mhk"], F["Whk"],
+                                            F["Kdhz"], F["areasTr"], F["areas"], F["nvecoa"],
+                                            F["nvecti"], F["nvecte"], F["func_r"], F["Altitudeh"],
+                                            F["Altitude"], A, maps, nl_region, pass, deep);
+                DivM_Op_Poles<5><<<NBP, 1>>>(F["DivM"], F["divg_Mh"], F["Mhk"], F["Whk"],
+                                             F["Kdhz"], F["areasTr"], F["areas"], F["nvecoa"],
+                                             F["nvecti"], F["nvecte"], F["func_r"], F["Altitudeh"],
+                                             F["Altitude"], A, loc, N, pass, deep);
+                REF_CHECK(cudaDeviceSynchronize());
+            }
+        }
+        REF_CHECK(cudaDeviceSynchronize());
+        Compute_Slow_Modes<LN, LN><<<NB, NT>>>(
+            F["SlowMh"], F["SlowWh"], F["SlowRho"], F["Slowpressure"], F["Mhk"], F["Whk"],
+            F["Rhok"], F["Adv"], F["DivM"], F["diffmh"], F["diffw"], F["diffrh"], F["diffpr"],
+            F["diffmv"], F["diffwv"], F["diffrv"], F["diffprv"], F["pressurek"], F["h"], F["hh"],
+            F["gtil"], F["grad"], F["div"], F["Altitude"], F["Altitudeh"], A, P.Gravit, F["Cp"],
+            F["Rd"], F["func_r"], maps, nl_region, deep, nonh, F["profx_dMh"], F["profx_dWh"],
+            F["profx_Qheat"], eeq, ghv);
+        REF_CHECK(cudaDeviceSynchronize());
+        Compute_Slow_Modes_Poles<6><<<2, 1>>>(
+            F["SlowMh"], F["SlowWh"], F["SlowRho"], F["Slowpressure"], F["Mhk"], F["Whk"],
+            F["Rhok"], F["Adv"], F["DivM"], F["diffmh"], F["diffw"], F["diffrh"], F["diffpr"],
+            F["diffmv"], F["diffwv"], F["diffrv"], F["diffprv"], F["pressurek"], F["h"], F["hh"],
+            F["gtil"], F["grad"], F["div"], F["Altitude"], F["Altitudeh"], A, P.Gravit, F["Cp"],
+            F["Rd"], F["func_r"], loc, nv, N, deep, nonh, F["profx_dMh"], F["profx_dWh"],
+            F["profx_Qheat"], eeq, ghv);
+        REF_CHECK(cudaDeviceSynchronize());
+
+        if (rk > 0) {
+            UpdateRK<<<(N / NTH) + 1, NTH>>>(F["Mhs"], F["Mhk"], F["Mh"], F["Whs"], F["Whk"],
+                                             F["Wh"], F["Ws"], F["Rhos"], F["Rhok"], F["Rho"],
+                                             F["pressures"], F["pressurek"], F["pressure"],
+                                             F["func_r"], F["Altitude"], F["Altitudeh"], N, nv);
+            REF_CHECK(cudaDeviceSynchronize());
+        }
+
+        for (int ns = 0; ns < ns_it; ns++) {
+            cudaMemset(F["DivM"], 0, 8 * N * 3 * nv);
+            cudaMemset(F["divg_Mh"], 0, 8 * N * 3 * nv);
+            if (P.DivDampP) {
+                REF_CHECK(cudaDeviceSynchronize());
+                for (int pass = 0; pass < 2; pass++) {
+                    DivM_Op<LN, LN><<<NB, NT>>>(F["DivM"], F["divg_Mh"], F["Mhs"], F["Whs"],
+                                                F["Kdhz"], F["areasTr"], F["areas"], F["nvecoa"],
+                                                F["nvecti"], F["nvecte"], F["func_r"],
+                                                F["Altitudeh"], F["Altitude"], A, maps, nl_region,
+                                                pass, deep);
+                    DivM_Op_Poles<5><<<NBP, 1>>>(F["DivM"], F["divg_Mh"], F["Mhs"], F["Whs"],
+                                                 F["Kdhz"], F["areasTr"], F["areas"], F["nvecoa"],
+                                                 F["nvecti"], F["nvecte"], F["func_r"],
+                                                 F["Altitudeh"], F["Altitude"], A, loc, N, pass,
+                                                 deep);
+                    REF_CHECK(cudaDeviceSynchronize());
+                }
+            }
+            REF_CHECK(cudaDeviceSynchronize());
+            Momentum_Eq<LN, LN><<<NB, NT>>>(F["Mhs"], F["pressures"], F["SlowMh"], F["grad"],
+                                            F["Altitude"], F["DivM"], A, F["func_r"], times, maps,
+                                            nl_region, deep);
+            Momentum_Eq_Poles<6><<<2, 1>>>(F["Mhs"], F["pressures"], F["SlowMh"], F["grad"],
+                                           F["Altitude"], F["DivM"], A, F["func_r"], times, loc,
+                                           nv, N, deep);
+            REF_CHECK(cudaDeviceSynchronize());
+            Prepare_Implicit_Vertical<LN, LN><<<NB, NT>>>(
+                F["Mhs"], F["h"], F["div"], F["Slowpressure"], F["SlowRho"], F["Sp"], F["Sd"],
+                F["Altitude"], F["Cp"], F["Rd"], A, maps, nl_region, deep);
+            REF_CHECK(cudaDeviceSynchronize());
+            Prepare_Implicit_Vertical_Poles<6><<<2, 1>>>(
+                F["Mhs"], F["h"], F["div"], F["Slowpressure"], F["SlowRho"], F["Sp"], F["Sd"],
+                F["Altitude"], F["Cp"], F["Rd"], A, loc, N, nv, deep);
+            REF_CHECK(cudaDeviceSynchronize());
+            Vertical_Eq<<<(N / num_th_vertical_eq) + 1, num_th_vertical_eq,
+                          2 * num_th_vertical_eq * nvi * sizeof(double)>>>(
+                F["Whs"], F["Ws"], F["pressures"], F["h"], F["hh"], F["Rhos"], F["gtil"],
+                F["gtilh"], F["Sp"], F["Sd"], F["SlowWh"], F["Cp"], F["Rd"], times, P.Gravit,
+                F["Altitude"], F["Altitudeh"], A, nonh, N, nv, nvi, deep, ghv, s->diag_flag_d,
+                s->diag_data_d);
+            REF_CHECK(cudaDeviceSynchronize());
+            REF_CHECK(cudaGetLastError());
+            Density_Pressure_Eqs<LN, LN><<<NB, NT>>>(
+                F["pressures"], F["pressurek"], F["Rhos"], F["Rhok"], F["Mhs"], F["Mhk"],
+                F["Whs"], F["Whk"], F["pt"], F["pth"], F["epotential"], F["epotentialh"],
+                F["ekinetic"], F["ekinetich"], F["Etotal"], F["h"], F["hh"], F["SlowRho"],
+                F["profx_Qheat"], F["diffpr"], F["diffprv"], F["div"], F["Altitude"],
+                F["Altitudeh"], F["Cp"], F["Rd"], A, P.P_Ref, P.Gravit, times, maps, nl_region,
+                deep, eeq, ghv, s->diag_flag_d, s->diag_data_d);
+            REF_CHECK(cudaDeviceSynchronize());
+            Density_Pressure_Eqs_Poles<6><<<2, 1>>>(
+                F["pressures"], F["pressurek"], F["Rhos"], F["Rhok"], F["Mhs"], F["Mhk"],
+                F["Whs"], F["Whk"], F["pt"], F["pth"], F["epotential"], F["epotentialh"],
+                F["ekinetic"], F["ekinetich"], F["Etotal"], F["h"], F["hh"], F["SlowRho"],
+                F["profx_Qheat"], F["diffpr"], F["diffprv"], F["div"], F["Altitude"],
+                F["Altitudeh"], F["Cp"], F["Rd"], A, P.P_Ref, P.Gravit, times, loc, N, nv, deep,
+                eeq, ghv, s->diag_flag_d, s->diag_data_d);
+            REF_CHECK(cudaDeviceSynchronize());
+        }
+        UpdateRK2<<<(N / NTH) + 1, NTH>>>(F["Mhs"], F["Mhk"], F["Whs"], F["Whk"], F["Wk"],
+                                          F["Rhos"], F["Rhok"], F["pressures"], F["pressurek"],
+                                          F["func_r"], F["Altitude"], F["Altitudeh"], N, nv);
+        REF_CHECK(cudaDeviceSynchronize());
+    }
+    REF_CHECK(cudaDeviceSynchronize());
+    cudaMemcpy(F["Mh"], F["Mhk"], N * nv * 3 * 8, cudaMemcpyDeviceToDevice);
+    cudaMemcpy(F["Wh"], F["Whk"], N * nvi * 8, cudaMemcpyDeviceToDevice);
+    cudaMemcpy(F["W"], F["Wk"], N * nv * 8, cudaMemcpyDeviceToDevice);
+    cudaMemcpy(F["Rho"], F["Rhok"], N * nv * 8, cudaMemcpyDeviceToDevice);
+    cudaMemcpy(F["pressure"], F["pressurek"], N * nv * 8, cudaMemcpyDeviceToDevice);
+    REF_CHECK(cudaDeviceSynchronize());
+    return 0;
+}
+
+// Runs `nsteps` large steps (ProfX then Thor, as the main loop of src/esp.cu:1382-1398).
+extern "C" int ref_sim_step(void* h, int nsteps, int do_profx, int do_thor) {
+    RefSim* s = (RefSim*)h;
+    for (int i = 0; i < nsteps; i++) {
+        if (do_profx && ref_profx(s))
+            return -1;
+        if (do_thor && ref_thor(s))
+            return -1;
+    }
+    return 0;
+}
+
+// Times `nsteps` large steps with CUDA events; returns milliseconds (negative on error).
+extern "C" double ref_sim_time(void* h, int nsteps) {
+    RefSim*     s = (RefSim*)h;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaDeviceSynchronize();
+    cudaEventRecord(a);
+    for (int i = 0; i < nsteps; i++) {
+        if (ref_profx(s) || ref_thor(s))
+            return -1.0;
+    }
+    cudaEventRecord(b);
+    cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return ms;
+}
+
+extern "C" void ref_sim_free(void* h) {
+    RefSim* s = (RefSim*)h;
+    for (auto& kv : s->f)
+        cudaFree(kv.second);
+    cudaFree(s->maps_d);
+    cudaFree(s->point_local_d);
+    cudaFree(s->diag_flag_d);
+    cudaFree(s->diag_data_d);
+    delete[] s->Altitude_h;
+    delete s;
+}

@@ -1,0 +1,1482 @@
+// CPU restatement of THOR's HE-VI dynamical core (ESP::Thor) and Held-Suarez ProfX step.
+//
+// TEST INFRASTRUCTURE ONLY: this is the oracle for the parity tests and the timed CPU baseline
+// (OpenMP over columns). It is never linked into, loaded by, or called from the product.
+//
+// Every routine restates one reference kernel, in the reference's memory layout
+//   scalar [col][lev], vector [col][lev][xyz], interface [col][lev+1],
+//   div/grad [col][7][xyz], areas/nvec* [col][6][xyz], areasTr [col][6],
+// with the same operand order and association as the reference source, so that with FMA
+// contraction off the CPU result differs from the reference's CUDA build only by the GPU's FMA
+// contraction and its pow/exp/log/sin/cos implementations (a few ulp per operation).
+//
+// The horizontal stencils see a cell's neighbours exactly as the reference kernels do:
+//  * interior cells through the rhombus maps tile (src/headers/kernel_halo_helpers.h:47-128):
+//    neighbours pt1..pt6 at tile offsets (x,y+1) (x+1,y+1) (x+1,y) (x,y-1) (x-1,y-1) (x-1,y);
+//    at a pentagon (tile corner with maps[0] == -1) pt5 is replaced by (x-1,y), and a tile
+//    entry of -1 contributes the value 0;
+//  * the two poles through point_local (5 neighbours), as the *_Poles kernels do.
+
+#include "thor_oracle.h"
+
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+using std::pow;
+using Vec = std::vector<double>;
+
+struct Oracle {
+    oracle_params P;
+    int           N, nv, nvi, nl, nr;
+    // geometry
+    std::vector<int> maps, point_local;
+    Vec              Altitude, Altitudeh, lonlat, areas, areasTr, nvecoa, nvecti, nvecte, div, grad,
+        func_r, Kdh4, Kdhz;
+    // neighbour tables: nb7[id*7 + j] j=0 self, j=1..6 = pt1..pt6 (-1 = tile hole -> value 0);
+    // nterms[id] = 7 (interior) or 6 (pole); ring[id*6 + j], nring[id] = 6 (hexagon) or 5.
+    std::vector<int>  nb7, nterms, ring, nring;
+    std::vector<char> pole, pent;
+    // state and intermediates
+    std::map<std::string, Vec> f;
+};
+
+inline double val(const Vec& a, int id, int nv, int lev) {
+    return id >= 0 ? a[(size_t)id * nv + lev] : 0.0;
+}
+inline double val3(const Vec& a, int id, int nv, int lev, int k) {
+    return id >= 0 ? a[((size_t)id * nv + lev) * 3 + k] : 0.0;
+}
+
+void build_neighbours(Oracle& o) {
+    int N = o.N, nl = o.nl, nhl = nl + 2, nhl2 = nhl * nhl;
+    o.nb7.assign((size_t)N * 7, -1);
+    o.nterms.assign(N, 7);
+    o.ring.assign((size_t)N * 6, -1);
+    o.nring.assign(N, 6);
+    o.pole.assign(N, 0);
+    o.pent.assign(N, 0);
+    for (int r = 0; r < o.nr; r++) {
+        const int* m = &o.maps[(size_t)r * nhl2];
+        for (int y = 0; y < nl; y++)
+            for (int x = 0; x < nl; x++) {
+                int  id = m[(y + 1) * nhl + x + 1];
+                bool pe = (x == 0 && y == 0 && m[0] == -1);
+                int  N0 = m[(y + 2) * nhl + x + 1], N1 = m[(y + 2) * nhl + x + 2],
+                    N2 = m[(y + 1) * nhl + x + 2], N3 = m[y * nhl + x + 1], N4 = m[y * nhl + x],
+                    N5 = m[(y + 1) * nhl + x];
+                int* nb = &o.nb7[(size_t)id * 7];
+                nb[0]   = id;
+                nb[1]   = N0;
+                nb[2]   = N1;
+                nb[3]   = N2;
+                nb[4]   = N3;
+                nb[5]   = pe ? N5 : N4;
+                nb[6]   = N5;
+                int* rg = &o.ring[(size_t)id * 6];
+                if (pe) {
+                    rg[0] = N0, rg[1] = N1, rg[2] = N2, rg[3] = N3, rg[4] = N5;
+                    o.nring[id] = 5;
+                }
+                else {
+                    rg[0] = N0, rg[1] = N1, rg[2] = N2, rg[3] = N3, rg[4] = N4, rg[5] = N5;
+                }
+                o.pent[id] = pe;
+            }
+    }
+    for (int id = N - 2; id < N; id++) {
+        int* nb = &o.nb7[(size_t)id * 7];
+        nb[0]   = id;
+        for (int i = 0; i < 5; i++) {
+            nb[i + 1]            = o.point_local[id * 6 + i];
+            o.ring[id * 6 + i]   = o.point_local[id * 6 + i];
+        }
+        nb[6]       = -1;
+        o.nterms[id] = 6;
+        o.nring[id]  = 5;
+        o.pole[id]   = 1;
+    }
+}
+
+Vec& F(Oracle& o, const char* n) { return o.f[n]; }
+
+// ---------------------------------------------------------------------------------------------
+// ProfX pieces (src/headers/phy/profx_auxiliary.h, src/headers/phy/profx_held_suarez.h)
+// ---------------------------------------------------------------------------------------------
+
+// Recompute_W, profx_auxiliary.h:109-130
+void recompute_w(Oracle& o) {
+    int   N = o.N, nv = o.nv, nvi = o.nvi;
+    Vec & W = F(o, "W"), &Wh = F(o, "Wh");
+#pragma omp parallel for schedule(static)
+    for (int id = 0; id < N; id++)
+        for (int lev = 0; lev < nv; lev++) {
+            double whl = Wh[id * nvi + lev], wht = Wh[id * nvi + lev + 1];
+            double xi = o.Altitude[lev], xim = o.Altitudeh[lev], xip = o.Altitudeh[lev + 1];
+            double intt = (xi - xip) / (xim - xip);
+            double intl = (xi - xim) / (xip - xim);
+            W[id * nv + lev] = whl * intt + wht * intl;
+        }
+}
+
+// Compute_temperature, profx_auxiliary.h:64-92 (calcT = true)
+void compute_temperature(Oracle& o) {
+    int   N = o.N, nv = o.nv;
+    Vec & T = F(o, "temperature"), &pt = F(o, "pt"), &p = F(o, "pressure"), &rho = F(o, "Rho"),
+        &Rd = F(o, "Rd"), &Cp = F(o, "Cp");
+    double P_Ref = o.P.P_Ref;
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < N * nv; i++) {
+        double Cv    = Cp[i] - Rd[i];
+        double CvoCp = Cv / Cp[i];
+        T[i]         = p[i] / (Rd[i] * rho[i]);
+        pt[i]        = (P_Ref / (Rd[i] * rho[i])) * pow(p[i] / P_Ref, CvoCp);
+    }
+}
+
+// held_suarez, profx_held_suarez.h:51-117
+void held_suarez(Oracle& o) {
+    int   N = o.N, nv = o.nv;
+    Vec & Mh = F(o, "Mh"), &p = F(o, "pressure"), &rho = F(o, "Rho"), &T = F(o, "temperature");
+    double Gravit = o.P.Gravit, Cp = o.P.Cp, Rd = o.P.Rd, dt = o.P.timestep;
+#pragma omp parallel for schedule(static)
+    for (int id = 0; id < N; id++)
+        for (int lev = 0; lev < nv; lev++) {
+            double sigmab = 0.7, ka = (1.0 / 40.0) * (1.0 / 86400.0), kf = 1.0 / 86400.0;
+            double ks = (1.0 / 4.0) * (1.0 / 86400.0), kappa = Rd / Cp, dTy = 60.0, dthetaz = 10.0;
+            double p0 = 100000.0, lat = o.lonlat[id * 2 + 1];
+            double psm1 = p[id * nv + 1] - rho[id * nv + 0] * Gravit
+                                               * (-o.Altitude[0] - o.Altitude[1]);
+            double ps     = 0.5 * (p[id * nv + 0] + psm1);
+            double pre    = p[id * nv + lev];
+            double sigma  = (pre / ps);
+            double sigma0 = (pre / p0);
+            double Teq    = std::fmax(200.0, (315.0 - dTy * pow(sin(lat), 2.0)
+                                           - dthetaz * log(sigma0) * pow(cos(lat), 2.0))
+                                              * pow(sigma0, kappa));
+            double kt = ka
+                        + (ks - ka) * std::fmax(0.0, (sigma - sigmab) / (1.0 - sigmab))
+                              * pow(cos(lat), 4.0);
+            double kv = kf * std::fmax(0.0, (sigma - sigmab) / (1.0 - sigmab));
+            for (int k = 0; k < 3; k++)
+                Mh[(id * nv + lev) * 3 + k] = Mh[(id * nv + lev) * 3 + k] / (1.0 + kv * dt);
+            T[id * nv + lev] -= kt * dt * (T[id * nv + lev] - Teq);
+        }
+}
+
+// Compute_pressure, profx_auxiliary.h:94-107
+void compute_pressure(Oracle& o) {
+    Vec & p = F(o, "pressure"), &T = F(o, "temperature"), &rho = F(o, "Rho"), &Rd = F(o, "Rd");
+    long  n = (long)o.N * o.nv;
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < n; i++)
+        p[i] = T[i] * Rd[i] * rho[i];
+}
+
+// ESP::ProfX, src/ESP/profx_driver.cu:70-474 (Held-Suarez branch, no sponge, no modules)
+void profx(Oracle& o) {
+    std::fill(F(o, "profx_Qheat").begin(), F(o, "profx_Qheat").end(), 0.0);
+    recompute_w(o);
+    compute_temperature(o);
+    if (o.P.held_suarez)
+        held_suarez(o);
+    compute_pressure(o);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Dynamical core (src/headers/dyn/*.h)
+// ---------------------------------------------------------------------------------------------
+
+// Compute_Advec_Cori1 (thor_adv_cor.h:51-235) and Compute_Advec_Cori_Poles (:240-362).
+void advec_cori1(Oracle& o) {
+    int   N = o.N, nv = o.nv;
+    Vec & Adv = F(o, "Adv"), &v = F(o, "v"), &Mh = F(o, "Mhk"), &W = F(o, "Wk"),
+        &Rho = F(o, "Rhok");
+    // velocities of every cell, v = M/rho + (w/rho) r
+    Vec vv((size_t)N * nv * 3);
+#pragma omp parallel for schedule(static)
+    for (int id = 0; id < N; id++)
+        for (int lev = 0; lev < nv; lev++) {
+            double rho = Rho[id * nv + lev], w = W[id * nv + lev];
+            for (int k = 0; k < 3; k++)
+                vv[(id * nv + lev) * 3 + k] =
+                    Mh[(id * nv + lev) * 3 + k] / rho + (w / rho) * o.func_r[id * 3 + k];
+        }
+#pragma omp parallel for schedule(static)
+    for (int id = 0; id < N; id++) {
+        const int* nb = &o.nb7[(size_t)id * 7];
+        int        nt = o.nterms[id];
+        for (int lev = 0; lev < nv; lev++) {
+            double rscale = o.P.DeepModel ? o.P.A / (o.Altitude[lev] + o.P.A) : 1.0;
+            double nflx[3] = {0.0, 0.0, 0.0};
+            for (int kk = 0; kk < 3; kk++)
+                for (int c = 0; c < 3; c++) {
+                    double s = 0.0;
+                    for (int j = 0; j < nt; j++) {
+                        double t = o.div[id * 21 + j * 3 + kk] * val3(vv, nb[j], nv, lev, c)
+                                   * val3(Mh, nb[j], nv, lev, kk);
+                        s = (j == 0) ? t : s + t;
+                    }
+                    nflx[c] += rscale * s;
+                }
+            for (int c = 0; c < 3; c++) {
+                Adv[(id * nv + lev) * 3 + c] = nflx[c];
+                v[(id * nv + lev) * 3 + c]   = vv[(id * nv + lev) * 3 + c];
+            }
+        }
+    }
+}
+
+// Compute_Advec_Cori2, thor_adv_cor.h:366-536
+void advec_cori2(Oracle& o) {
+    int    N = o.N, nv = o.nv, nvi = o.nvi;
+    Vec &  Adv = F(o, "Adv"), &v = F(o, "v"), &Wh = F(o, "Whk"), &Rho = F(o, "Rhok");
+    double A = o.P.A, Omega = o.P.Omega;
+    bool   deep = o.P.DeepModel;
+#pragma omp parallel for schedule(static)
+    for (int id = 0; id < N; id++) {
+        const double* fr = &o.func_r[id * 3];
+        for (int lev = 0; lev < nv; lev++) {
+            double altht = o.Altitudeh[lev + 1], althl = o.Altitudeh[lev], alt = o.Altitude[lev];
+            double dvwl[3] = {0, 0, 0}, dvwt[3] = {0, 0, 0};
+            double vc[3];
+            for (int k = 0; k < 3; k++)
+                vc[k] = v[(id * nv + lev) * 3 + k];
+            if (lev > 0) {
+                double xi = althl, xim = o.Altitude[lev - 1], xip = alt;
+                double intt = (xi - xip) / (xim - xip), intl = (xi - xim) / (xip - xim);
+                double whl = Wh[id * nvi + lev];
+                for (int k = 0; k < 3; k++)
+                    dvwl[k] = (v[(id * nv + lev - 1) * 3 + k] * intt + vc[k] * intl) * whl;
+            }
+            if (lev < nv - 1) {
+                double xi = altht, xim = alt, xip = o.Altitude[lev + 1];
+                double intt = (xi - xip) / (xim - xip), intl = (xi - xim) / (xip - xim);
+                double wht = Wh[id * nvi + lev + 1];
+                for (int k = 0; k < 3; k++)
+                    dvwt[k] = (vc[k] * intt + v[(id * nv + lev + 1) * 3 + k] * intl) * wht;
+            }
+            double r2p = 1.0, r2m = 1.0, r2l = 1.0;
+            if (deep) {
+                r2p = pow(altht + A, 2.0);
+                r2m = pow(alt + A, 2.0);
+                r2l = pow(althl + A, 2.0);
+            }
+            double dz  = 1.0 / ((althl - altht) * r2m);
+            double rho = Rho[id * nv + lev];
+            double C[3];
+            if (deep) {
+                C[0] = -2.0 * Omega * vc[1] * rho;
+                C[1] = 2.0 * Omega * vc[0] * rho;
+                C[2] = 0.0;
+            }
+            else {
+                C[0] = 2 * Omega * (vc[2] * fr[2] * fr[1] - vc[1] * pow(fr[2], 2)) * rho;
+                C[1] = -2 * Omega * (vc[2] * fr[2] * fr[0] - vc[0] * pow(fr[2], 2)) * rho;
+                C[2] = 2 * Omega * (vc[1] * fr[2] * fr[0] - vc[0] * fr[2] * fr[1]) * rho;
+            }
+            for (int k = 0; k < 3; k++) {
+                double dav = (dvwl[k] * r2l - dvwt[k] * r2p) * dz;
+                Adv[(id * nv + lev) * 3 + k] += dav + C[k];
+            }
+        }
+    }
+}
+
+// Compute_Temperature_H_Pt_Geff, thor_auxiliary.h:55-309 (calcT = true)
+void temperature_h_pt_geff(Oracle& o) {
+    int    N = o.N, nv = o.nv, nvi = o.nvi;
+    Vec &  T = F(o, "temperature"), &P = F(o, "pressurek"), &Rho = F(o, "Rhok"), &Mh = F(o, "Mhk"),
+        &h = F(o, "h"), &hh = F(o, "hh"), &pt = F(o, "pt"), &pth = F(o, "pth"), &gtil = F(o, "gtil"),
+        &gtilh = F(o, "gtilh"), &Wh = F(o, "Whk"), &W = F(o, "Wk"), &ep_d = F(o, "epotential"),
+        &eph_d = F(o, "epotentialh"), &ek_d = F(o, "ekinetic"), &ekh_d = F(o, "ekinetich"),
+        &Et = F(o, "Etotal"), &Cp = F(o, "Cp"), &Rd = F(o, "Rd");
+    const double* Alt  = o.Altitude.data();
+    const double* Alth = o.Altitudeh.data();
+    double        P_Ref = o.P.P_Ref, Gravit = o.P.Gravit, A = o.P.A;
+    bool          eeq = o.P.energy_equation, ghv = o.P.GravHeightVar;
+#pragma omp parallel for schedule(static)
+    for (int id = 0; id < N; id++) {
+        double temperature, rho = 0, rhoh, rhol = 0, rhop;
+        double pressure = 0, h_ = 0, hl = 0, pt_ = 0, ptl = 0, pl = 0, pp, dpdz, ep = 0, epl = 0,
+               ek = 0, ekl = 0;
+        double gtilh_ = 0, gtilht;
+        double dz, dp_dz, Cv, CvoCp;
+        double xi, xim, xip, intt, intl, extr;
+        double alt = 0, altl = 0, alth = 0, altht = 0;
+        for (int lev = 0; lev < nv + 1; lev++) {
+            if (lev < nv) {
+                Cv    = Cp[id * nv + lev] - Rd[id * nv + lev];
+                CvoCp = Cv / Cp[id * nv + lev];
+                if (lev > 0) {
+                    pl   = pressure;
+                    rhol = rho;
+                    hl   = h_;
+                    if (eeq) {
+                        epl = ep;
+                        ekl = ek;
+                    }
+                    else
+                        ptl = pt_;
+                    altl = alt;
+                }
+                pressure    = P[id * nv + lev];
+                rho         = Rho[id * nv + lev];
+                temperature = pressure / (rho * Rd[id * nv + lev]);
+                T[id * nv + lev] = temperature;
+                alt   = Alt[lev];
+                alth  = Alth[lev];
+                altht = Alth[lev + 1];
+                h_    = Cv * temperature + pressure / rho;
+                h[id * nv + lev] = h_;
+                if (eeq) {
+                    if (ghv)
+                        ep = Gravit * pow(A / (A + Alt[lev]), 2) * Alt[lev];
+                    else
+                        ep = Gravit * Alt[lev];
+                    ep_d[id * nv + lev] = ep;
+                    const double* m     = &Mh[(id * nv + lev) * 3];
+                    ek = 0.5 * (m[0] * m[0] + m[1] * m[1] + m[2] * m[2] + W[id * nv + lev] * W[id * nv + lev])
+                         / (Rho[id * nv + lev] * Rho[id * nv + lev]);
+                    ek_d[id * nv + lev] = ek;
+                    Et[id * nv + lev]   = Rho[id * nv + lev] * (ep + ek) + Cv / Rd[id * nv + lev] * pressure;
+                }
+                else {
+                    pt_ = (P_Ref / (Rd[id * nv + lev] * rho)) * pow(pressure / P_Ref, CvoCp);
+                    pt[id * nv + lev] = pt_;
+                }
+            }
+            if (lev == 0) {
+                extr              = (-alt - Alt[lev + 1]) / (Alt[lev + 1] - alt);
+                hh[id * nvi + 0]  = h_;
+                if (ghv)
+                    pl = P[id * nv + 1] - rho * Gravit * pow(A / (A + Alt[0]), 2) * (-alt - Alt[1]);
+                else
+                    pl = P[id * nv + 1] - rho * Gravit * (-alt - Alt[1]);
+                rhol = Rho[id * nv + 1] + (Rho[id * nv + 1] - rho) * extr;
+                rhoh = 0.5 * (rho + rhol);
+                dz   = 2.0 * Alt[0];
+                dpdz = (P[id * nv + 0] - pl) / dz;
+                gtilh[id * nvi + 0] = -(1.0 / rhoh) * dpdz;
+                gtilh_              = 0.0;
+            }
+            else if (lev == nv) {
+                extr = (2 * Alth[nv] - alt - Alt[nv - 2]) / (Alt[nv - 1] - Alt[nv - 2]);
+                Cv    = Cp[id * nv + lev - 1] - Rd[id * nv + lev - 1];
+                CvoCp = Cv / Cp[id * nv + lev - 1];
+                hh[id * nvi + nv] = h_;
+                if (ghv)
+                    pp = P[id * nv + nv - 2] - rho * Gravit * pow(A / (A + Alt[lev]), 2)
+                                                   * (2 * Alth[nv] - alt - Alt[nv - 2]);
+                else
+                    pp = P[id * nv + nv - 2] - rho * Gravit * (2 * Alth[nv] - alt - Alt[nv - 2]);
+                if (pp < 0)
+                    pp = 0;
+                rhop = Rho[id * nv + nv - 2] + (Rho[id * nv + nv - 1] - Rho[id * nv + nv - 2]) * extr;
+                rhoh = 0.5 * (rho + rhop);
+                if (eeq) {
+                    if (ghv) {
+                        eph_d[id * nvi + nv] = Gravit * pow(A / (A + Alth[nv]), 2) * Alth[nv];
+                        eph_d[id * nvi + 0]  = Gravit * pow(A / (A + Alth[0]), 2) * Alth[0];
+                    }
+                    else {
+                        eph_d[id * nvi + nv] = Gravit * Alth[nv];
+                        eph_d[id * nvi + 0]  = Gravit * Alth[0];
+                    }
+                    ekh_d[id * nvi + nv] = ek_d[id * nv + nv - 2]
+                                           + (ek_d[id * nv + nv - 1] - ek_d[id * nv + nv - 2]) * extr;
+                    ekh_d[id * nvi + 0] = ek_d[id * nv + 1]
+                                          + (ek_d[id * nv + 1] - ek_d[id * nv + 0])
+                                                * (Alth[0] - Alt[1]) / (Alt[1] - Alt[0]);
+                }
+                else {
+                    pth[id * nvi + nv] =
+                        pt[id * nv + nv - 2] + (pt[id * nv + nv - 1] - pt[id * nv + nv - 2]) * extr;
+                    pth[id * nvi + 0] = pt[id * nv + 1]
+                                        + (pt[id * nv + 1] - pt[id * nv + 0]) * (Alth[0] - Alt[1])
+                                              / (Alt[1] - Alt[0]);
+                }
+                dz = 2.0 * (Alth[nv] - Alt[nv - 1]);
+                if (ghv)
+                    pp = P[id * nv + nv - 2]
+                         - Rho[id * nv + nv - 1] * Gravit * pow(A / (A + Alt[nv - 1]), 2)
+                               * (2 * Alth[nv] - Alt[nv - 1] - Alt[nv - 2]);
+                else
+                    pp = P[id * nv + nv - 2]
+                         - Rho[id * nv + nv - 1] * Gravit * (2 * Alth[nv] - Alt[nv - 1] - Alt[nv - 2]);
+                dpdz               = (pp - P[id * nv + nv - 1]) / dz;
+                gtilh[id * nvi + nv] = -(1.0 / rhoh) * dpdz;
+                gtilht             = 0.0;
+                xi   = alt;
+                xim  = alth;
+                xip  = altht;
+                intt = (xi - xip) / (xim - xip);
+                intl = (xi - xim) / (xip - xim);
+                gtil[id * nv + nv - 1] = gtilh_ * intt + gtilht * intl;
+            }
+            else {
+                dz    = alt - altl;
+                dp_dz = (pressure - pl) / dz;
+                xi    = alth;
+                xim   = altl;
+                xip   = alt;
+                intt  = (xi - xip) / (xim - xip);
+                intl  = (xi - xim) / (xip - xim);
+                hh[id * nvi + lev] = hl * intt + h_ * intl;
+                if (eeq) {
+                    eph_d[id * nvi + lev] = epl * intt + ep * intl;
+                    ekh_d[id * nvi + lev] = ekl * intt + ek * intl;
+                }
+                else
+                    pth[id * nvi + lev] = ptl * intt + pt_ * intl;
+                rhoh   = rhol * intt + rho * intl;
+                gtilht = -(Wh[id * nvi + lev] / rhoh) * dp_dz;
+                xi     = alt;
+                xim    = alth;
+                xip    = altht;
+                intt   = (xi - xip) / (xim - xip);
+                intl   = (xi - xim) / (xip - xim);
+                gtil[id * nv + lev - 1] = gtilh_ * intt + gtilht * intl;
+                gtilh_                  = gtilht;
+                gtilh[id * nvi + lev]   = -(1.0 / rhoh) * dp_dz;
+            }
+        }
+    }
+}
+
+// One FV Laplacian of a cell-centred scalar `a` (values gathered per cell) around a cell's ring of
+// neighbours: Diffusion_Op (thor_diff.h:306-451) for interior cells, Diffusion_Op_Poles
+// (thor_diff.h:735-820) for the poles. The two are the same sequence of operations (the pole
+// kernel writes some sums with the operands swapped, which IEEE addition does not distinguish).
+double laplacian(const Oracle& o, int id, const double* a_ring, double a0, double rscale) {
+    int    n     = o.nring[id];
+    double lap   = 0.0;
+    double lap1 = 0, lap2 = 0, lap3 = 0, lapx1 = 0, lapx2 = 0, lapy1 = 0, lapy2 = 0, lapz1 = 0,
+           lapz2 = 0, AT1 = 0;
+    const double* ar = &o.areas[id * 18];
+    const double* at = &o.areasTr[id * 6];
+    const double* ti = &o.nvecti[id * 18];
+    const double* te = &o.nvecte[id * 18];
+    const double* oa = &o.nvecoa[id * 18];
+    for (int j = 0; j < n; j++) {
+        int    jp1 = (j + 1) % n, jp2 = (j + 2) % n;
+        double p1 = a_ring[j], p2 = a_ring[jp1], p3 = a_ring[jp2];
+        double vdiff = 0.5 * rscale;
+        double astar;
+        if (j == 0) {
+            AT1   = rscale / at[j];
+            astar = (ar[j * 3 + 0] * a0 + ar[j * 3 + 1] * p1 + ar[j * 3 + 2] * p2) / at[j];
+            lap1  = (0.5 * (p1 + a0) - astar);
+            lap2  = (0.5 * (p1 + p2) - astar);
+            lap3  = (0.5 * (a0 + p2) - astar);
+        }
+        double AT2 = rscale / at[jp1];
+        astar      = (ar[jp1 * 3 + 0] * a0 + ar[jp1 * 3 + 1] * p2 + ar[jp1 * 3 + 2] * p3) / at[jp1];
+        double lap4 = (0.5 * (a0 + p2) - astar);
+        double lap5 = (0.5 * (p2 + p3) - astar);
+        double lap6 = (0.5 * (a0 + p3) - astar);
+        if (j == 0) {
+            lapx1 = (-lap1 * ti[j * 3 + 0] + lap2 * te[j * 3 + 0] + lap3 * ti[jp1 * 3 + 0]) * AT1;
+            lapx2 = (-lap4 * ti[jp1 * 3 + 0] + lap5 * te[jp1 * 3 + 0] + lap6 * ti[jp2 * 3 + 0]) * AT2;
+            lapy1 = (-lap1 * ti[j * 3 + 1] + lap2 * te[j * 3 + 1] + lap3 * ti[jp1 * 3 + 1]) * AT1;
+            lapy2 = (-lap4 * ti[jp1 * 3 + 1] + lap5 * te[jp1 * 3 + 1] + lap6 * ti[jp2 * 3 + 1]) * AT2;
+            lapz1 = (-lap1 * ti[j * 3 + 2] + lap2 * te[j * 3 + 2] + lap3 * ti[jp1 * 3 + 2]) * AT1;
+            lapz2 = (-lap4 * ti[jp1 * 3 + 2] + lap5 * te[jp1 * 3 + 2] + lap6 * ti[jp2 * 3 + 2]) * AT2;
+        }
+        else {
+            lapx1 = lapx2;
+            lapx2 = (-lap4 * ti[jp1 * 3 + 0] + lap5 * te[jp1 * 3 + 0] + lap6 * ti[jp2 * 3 + 0]) * AT2;
+            lapy1 = lapy2;
+            lapy2 = (-lap4 * ti[jp1 * 3 + 1] + lap5 * te[jp1 * 3 + 1] + lap6 * ti[jp2 * 3 + 1]) * AT2;
+            lapz1 = lapz2;
+            lapz2 = (-lap4 * ti[jp1 * 3 + 2] + lap5 * te[jp1 * 3 + 2] + lap6 * ti[jp2 * 3 + 2]) * AT2;
+        }
+        lap += ((lapx1 + lapx2) * oa[j * 3 + 0] + (lapy1 + lapy2) * oa[j * 3 + 1]
+                + (lapz1 + lapz2) * oa[j * 3 + 2])
+               * vdiff;
+    }
+    return lap;
+}
+
+// Diffusion_Op (thor_diff.h:54-522) + Diffusion_Op_Poles (:524-880), without the diffusive
+// sponge, for one pass `stepnum` (laststep = final pass).
+void diffusion_pass(Oracle& o, int stepnum, bool laststep) {
+    int   N = o.N, nv = o.nv;
+    Vec & Mh = F(o, "Mhk"), &Rho = F(o, "Rhok"), &T = F(o, "temperature"), &W = F(o, "Wk"),
+        &Rd = F(o, "Rd"), &Cp = F(o, "Cp"), &diff = F(o, "diff"), &diffmh = F(o, "diffmh"),
+        &diffw = F(o, "diffw"), &diffrh = F(o, "diffrh"), &diffpr = F(o, "diffpr");
+    bool eeq = o.P.energy_equation;
+    // argument of the Laplacian per cell and variable
+    Vec a((size_t)N * nv * 6);
+#pragma omp parallel for schedule(static)
+    for (int id = 0; id < N; id++)
+        for (int lev = 0; lev < nv; lev++)
+            for (int var = 0; var < 6; var++) {
+                size_t i = (size_t)id * nv + lev;
+                double x;
+                if (stepnum == 0) {
+                    if (var == 0)
+                        x = Rho[i];
+                    else if (var <= 3)
+                        x = Mh[i * 3 + var - 1];
+                    else if (var == 4)
+                        x = W[i];
+                    else
+                        x = eeq ? (Cp[i] - Rd[i]) * T[i] : Rd[i] * T[i];
+                    if (var >= 1 && var <= 4)
+                        x = x / Rho[i];
+                }
+                else if (laststep)
+                    x = (var == 0) ? diff[i * 6 + var] : diff[i * 6 + var] * Rho[i];
+                else
+                    x = diff[i * 6 + var];
+                a[i * 6 + var] = x;
+            }
+    Vec out((size_t)N * nv * 6);
+#pragma omp parallel for schedule(static)
+    for (int id = 0; id < N; id++) {
+        const int* rg = &o.ring[(size_t)id * 6];
+        for (int lev = 0; lev < nv; lev++) {
+            double rscale = o.P.DeepModel ? o.P.A / (o.Altitude[lev] + o.P.A) : 1.0;
+            double sdiff  = -o.Kdh4[lev] * pow(-1.0, o.P.HyDiffOrder / 2);
+            for (int var = 0; var < 6; var++) {
+                double ring_v[6];
+                for (int j = 0; j < o.nring[id]; j++)
+                    ring_v[j] = rg[j] >= 0 ? a[((size_t)rg[j] * nv + lev) * 6 + var] : 0.0;
+                double a0  = a[((size_t)id * nv + lev) * 6 + var];
+                double lap = laplacian(o, id, ring_v, a0, rscale);
+                if (laststep)
+                    lap *= sdiff;
+                out[((size_t)id * nv + lev) * 6 + var] = lap;
+            }
+        }
+    }
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < (long)N * nv; i++)
+        for (int var = 0; var < 6; var++) {
+            double lap = out[i * 6 + var];
+            if (laststep) {
+                if (var == 0)
+                    diffrh[i] = lap;
+                else if (var <= 3)
+                    diffmh[i * 3 + var - 1] = lap;
+                else if (var == 4)
+                    diffw[i] = lap;
+                else
+                    diffpr[i] = lap;
+            }
+            else
+                diff[i * 6 + var] = lap;
+        }
+}
+
+// Correct_Horizontal, thor_diff.h:882-915
+void correct_horizontal(Oracle& o) {
+    int  N = o.N, nv = o.nv;
+    Vec &dmh = F(o, "diffmh"), &dmv = F(o, "diffmv");
+#pragma omp parallel for schedule(static)
+    for (int id = 0; id < N; id++)
+        for (int lev = 0; lev < nv; lev++) {
+            const double* fr = &o.func_r[id * 3];
+            double*       h  = &dmh[((size_t)id * nv + lev) * 3];
+            double*       v  = &dmv[((size_t)id * nv + lev) * 3];
+            double        dmhr = fr[0] * h[0] + fr[1] * h[1] + fr[2] * h[2];
+            h[0] += -fr[0] * dmhr;
+            h[1] += -fr[1] * dmhr;
+            h[2] += -fr[2] * dmhr;
+            double dmvr = fr[0] * v[0] + fr[1] * v[1] + fr[2] * v[2];
+            v[0] += -fr[0] * dmvr;
+            v[1] += -fr[1] * dmvr;
+            v[2] += -fr[2] * dmvr;
+        }
+}
+
+// DivM_Op (thor_div.h:49-315) and DivM_Op_Poles (:317-535), pass `laststep`, on (Mh, Wh).
+// The pole kernel's corner-mean of w uses the second sub-area twice (thor_div.h:443-454);
+// that is restated as it is.
+void divm_pass(Oracle& o, const Vec& Mh, const Vec& Wh, bool laststep) {
+    int  N = o.N, nv = o.nv, nvi = o.nvi;
+    Vec &DivM = F(o, "DivM"), &divg = F(o, "divg_Mh");
+#pragma omp parallel for schedule(static)
+    for (int id = 0; id < N; id++) {
+        const int*    rg = &o.ring[(size_t)id * 6];
+        int           n  = o.nring[id];
+        bool          pole = o.pole[id];
+        const double* ar = &o.areas[id * 18];
+        const double* at = &o.areasTr[id * 6];
+        const double* ti = &o.nvecti[id * 18];
+        const double* te = &o.nvecte[id * 18];
+        const double* oa = &o.nvecoa[id * 18];
+        for (int lev = 0; lev < nv; lev++) {
+            double rscale = o.P.DeepModel ? o.P.A / (o.Altitude[lev] + o.P.A) : 1.0;
+            double AT0    = 0.5 * rscale;
+            double lapx = 0.0, lapy = 0.0, lapz = 0.0;
+            double dz = 0;
+            if (!laststep)
+                dz = 1.0 / (o.Altitudeh[lev] - o.Altitudeh[lev + 1]);
+            const Vec& src = laststep ? divg : Mh;
+            double     a0[3], ar_[6][3], wl0 = 0, wt0 = 0, wl[6] = {0}, wt[6] = {0};
+            for (int k = 0; k < 3; k++)
+                a0[k] = src[((size_t)id * nv + lev) * 3 + k];
+            for (int j = 0; j < n; j++)
+                for (int k = 0; k < 3; k++)
+                    ar_[j][k] = rg[j] >= 0 ? src[((size_t)rg[j] * nv + lev) * 3 + k] : 0.0;
+            if (!laststep) {
+                wl0 = Wh[id * nvi + lev];
+                wt0 = Wh[id * nvi + lev + 1];
+                for (int j = 0; j < n; j++) {
+                    wl[j] = rg[j] >= 0 ? Wh[rg[j] * nvi + lev] : 0.0;
+                    wt[j] = rg[j] >= 0 ? Wh[rg[j] * nvi + lev + 1] : 0.0;
+                }
+            }
+            double a01x = 0, a01y = 0, a01z = 0, a12x = 0, a12y = 0, a12z = 0, AT1 = 0, lap1 = 0,
+                   lap2 = 0;
+            for (int j = 0; j < n; j++) {
+                int    jp1 = (j + 1) % n, jp2 = (j + 2) % n;
+                double dwdz = 0.0, dwdz2 = 0.0;
+                const double *p1 = ar_[j], *p2 = ar_[jp1], *p3 = ar_[jp2];
+                if (!laststep) {
+                    int    c2 = pole ? 1 : 2;
+                    double meanwl = (ar[j * 3 + 0] * wl0 + ar[j * 3 + 1] * wl[j] + ar[j * 3 + c2] * wl[jp1]) / at[j];
+                    double meanwt = (ar[j * 3 + 0] * wt0 + ar[j * 3 + 1] * wt[j] + ar[j * 3 + c2] * wt[jp1]) / at[j];
+                    double meanwl2 = (ar[jp1 * 3 + 0] * wl0 + ar[jp1 * 3 + 1] * wl[jp1]
+                                      + ar[jp1 * 3 + c2] * wl[jp2]) / at[jp1];
+                    double meanwt2 = (ar[jp1 * 3 + 0] * wt0 + ar[jp1 * 3 + 1] * wt[jp1]
+                                      + ar[jp1 * 3 + c2] * wt[jp2]) / at[jp1];
+                    dwdz  = (meanwl - meanwt) * dz;
+                    dwdz2 = (meanwl2 - meanwt2) * dz;
+                }
+                if (j == 0) {
+                    a01x = (a0[0] + p1[0]);
+                    a01y = (a0[1] + p1[1]);
+                    a01z = (a0[2] + p1[2]);
+                    a12x = (p1[0] + p2[0]);
+                    a12y = (p1[1] + p2[1]);
+                    a12z = (p1[2] + p2[2]);
+                    AT1  = 0.5 * rscale / at[j];
+                }
+                double AT2  = 0.5 * rscale / at[jp1];
+                double a02x = (a0[0] + p2[0]), a02y = (a0[1] + p2[1]), a02z = (a0[2] + p2[2]);
+                double a23x = (p2[0] + p3[0]), a23y = (p2[1] + p3[1]), a23z = (p2[2] + p3[2]);
+                double a03x = (a0[0] + p3[0]), a03y = (a0[1] + p3[1]), a03z = (a0[2] + p3[2]);
+                if (j == 0)
+                    lap1 = (-a01x * ti[j * 3 + 0] - a01y * ti[j * 3 + 1] - a01z * ti[j * 3 + 2]
+                            + a12x * te[j * 3 + 0] + a12y * te[j * 3 + 1] + a12z * te[j * 3 + 2]
+                            + a02x * ti[jp1 * 3 + 0] + a02y * ti[jp1 * 3 + 1]
+                            + a02z * ti[jp1 * 3 + 2])
+                           * AT1;
+                else
+                    lap1 = lap2;
+                lap2 = (-a02x * ti[jp1 * 3 + 0] - a02y * ti[jp1 * 3 + 1] - a02z * ti[jp1 * 3 + 2]
+                        + a23x * te[jp1 * 3 + 0] + a23y * te[jp1 * 3 + 1] + a23z * te[jp1 * 3 + 2]
+                        + a03x * ti[jp2 * 3 + 0] + a03y * ti[jp2 * 3 + 1] + a03z * ti[jp2 * 3 + 2])
+                       * AT2;
+                lapx += (lap1 + dwdz + lap2 + dwdz2) * oa[j * 3 + 0] * AT0;
+                lapy += (lap1 + dwdz + lap2 + dwdz2) * oa[j * 3 + 1] * AT0;
+                lapz += (lap1 + dwdz + lap2 + dwdz2) * oa[j * 3 + 2] * AT0;
+            }
+            double* out = laststep ? &DivM[((size_t)id * nv + lev) * 3] : &divg[((size_t)id * nv + lev) * 3];
+            if (laststep) {
+                double        sdiff = o.Kdhz[lev];
+                const double* fr    = &o.func_r[id * 3];
+                double        lapr  = fr[0] * lapx + fr[1] * lapy + fr[2] * lapz;
+                lapx                = lapx - fr[0] * lapr;
+                lapy                = lapy - fr[1] * lapr;
+                lapz                = lapz - fr[2] * lapr;
+                out[0]              = -lapx * sdiff;
+                out[1]              = -lapy * sdiff;
+                out[2]              = -lapz * sdiff;
+            }
+            else {
+                out[0] = lapx;
+                out[1] = lapy;
+                out[2] = lapz;
+            }
+        }
+    }
+}
+
+// Sum over the 7 (interior) or 6 (pole) stencil points of coef_j[k] * x_j, as the reference
+// writes it: ((c0 x0 + c1 x1) + c2 x2) + ...
+template<class G> inline double stencil_sum(const double* coef, int k, int nt, G get) {
+    double s = coef[0 * 3 + k] * get(0);
+    for (int j = 1; j < nt; j++)
+        s = s + coef[j * 3 + k] * get(j);
+    return s;
+}
+
+// The same sum for terms written coef_j[k] * x_j * y_j, i.e. (coef * x) * y.
+template<class GX, class GY>
+inline double stencil_sum2(const double* coef, int k, int nt, GX gx, GY gy) {
+    double s = coef[0 * 3 + k] * gx(0) * gy(0);
+    for (int j = 1; j < nt; j++)
+        s = s + coef[j * 3 + k] * gx(j) * gy(j);
+    return s;
+}
+
+// Compute_Slow_Modes (thor_slowmodes.h:48-382) and Compute_Slow_Modes_Poles (:384-683).
+void slow_modes(Oracle& o) {
+    int    N = o.N, nv = o.nv, nvi = o.nvi;
+    Vec &  SlowMh = F(o, "SlowMh"), &SlowWh = F(o, "SlowWh"), &SlowRho = F(o, "SlowRho"),
+        &Slowp = F(o, "Slowpressure"), &Mh = F(o, "Mhk"), &Wh = F(o, "Whk"), &Rho = F(o, "Rhok"),
+        &Adv = F(o, "Adv"), &DivM = F(o, "DivM"), &diffmh = F(o, "diffmh"),
+        &diffw = F(o, "diffw"), &diffrh = F(o, "diffrh"), &diffpr = F(o, "diffpr"),
+        &diffmv = F(o, "diffmv"), &diffwv = F(o, "diffwv"), &diffrv = F(o, "diffrv"),
+        &diffprv = F(o, "diffprv"), &p = F(o, "pressurek"), &h = F(o, "h"), &hh = F(o, "hh"),
+        &gtil = F(o, "gtil"), &Cp = F(o, "Cp"), &Rd = F(o, "Rd"), &dMh = F(o, "profx_dMh"),
+        &dWh = F(o, "profx_dWh"), &Qheat = F(o, "profx_Qheat");
+    double A = o.P.A, Gravit = o.P.Gravit;
+    bool   deep = o.P.DeepModel, nonh = o.P.NonHydro, eeq = o.P.energy_equation,
+         ghv = o.P.GravHeightVar;
+#pragma omp parallel for schedule(static)
+    for (int id = 0; id < N; id++) {
+        const int*    nb = &o.nb7[(size_t)id * 7];
+        int           nt = o.nterms[id];
+        bool          pole = o.pole[id];
+        const double* fr = &o.func_r[id * 3];
+        double        fx = fr[0], fy = fr[1], fz = fr[2];
+        for (int lev = 0; lev < nv; lev++) {
+            size_t i   = (size_t)id * nv + lev;
+            double Cv  = Cp[i] - Rd[i];
+            double advx = Adv[i * 3 + 0], advy = Adv[i * 3 + 1], advz = Adv[i * 3 + 2];
+            double rho = Rho[i], rhol = 0, altl = 0, pressurel = 0, advrl = 0;
+            if (lev != 0) {
+                advrl = Adv[(i - 1) * 3 + 0] * fx + Adv[(i - 1) * 3 + 1] * fy + Adv[(i - 1) * 3 + 2] * fz;
+                rhol      = Rho[i - 1];
+                altl      = o.Altitude[lev - 1];
+                pressurel = p[i - 1];
+            }
+            double advr = advx * fx + advy * fy + advz * fz;
+            advx += -advr * fx;
+            advy += -advr * fy;
+            advz += -advr * fz;
+            double altht = o.Altitudeh[lev + 1], althl = o.Altitudeh[lev], alt = o.Altitude[lev];
+            if (!nonh) {
+                advr = (pow(Mh[i * 3 + 0], 2) + pow(Mh[i * 3 + 1], 2) + pow(Mh[i * 3 + 2], 2))
+                       / (rho * (alt + A));
+                if (lev != 0)
+                    advrl = (pow(Mh[(i - 1) * 3 + 0], 2) + pow(Mh[(i - 1) * 3 + 1], 2)
+                             + pow(Mh[(i - 1) * 3 + 2], 2))
+                            / (rhol * (altl + A));
+            }
+            double dz = altht - althl;
+            double r2p, r2m, r2l, rscale, dr2dz;
+            if (deep) {
+                r2p    = pow(altht + A, 2.0);
+                r2m    = pow(alt + A, 2.0);
+                r2l    = pow(althl + A, 2.0);
+                rscale = A / (alt + A);
+                dr2dz  = (pow(altht + A, 3.0) - pow(althl + A, 3.0)) / 3;
+            }
+            else {
+                r2p = r2m = r2l = rscale = 1.0;
+                dr2dz                    = r2m * dz;
+            }
+            double nflxv[3], nflxr = 0.0, nflxp = 0.0;
+            const double* gr = &o.grad[id * 21];
+            const double* dv = &o.div[id * 21];
+            for (int k = 0; k < 3; k++) {
+                nflxv[k] = rscale * stencil_sum(gr, k, nt, [&](int j) { return val(p, nb[j], nv, lev); });
+                nflxr += rscale * stencil_sum(dv, k, nt, [&](int j) { return val3(Mh, nb[j], nv, lev, k); });
+                nflxp += rscale * stencil_sum2(dv, k, nt,
+                                               [&](int j) { return val3(Mh, nb[j], nv, lev, k); },
+                                               [&](int j) { return val(h, nb[j], nv, lev); });
+            }
+            double whl, wht, hhl, hht;
+            if (lev == 0) {
+                whl = 0.0;
+                wht = Wh[id * nvi + lev + 1];
+                hhl = 0.0;
+                hht = hh[id * nvi + lev + 1];
+            }
+            else {
+                whl = Wh[id * nvi + lev];
+                wht = Wh[id * nvi + lev + 1];
+                hhl = hh[id * nvi + lev];
+                hht = hh[id * nvi + lev + 1];
+            }
+            double dwdz  = pole ? (wht * r2p - whl * r2l) / (dz * r2m) : (wht * r2p - whl * r2l) / (dr2dz);
+            double dwhdz = (wht * r2p * hht - whl * r2l * hhl) / (dz * r2m);
+            double dpr   = nflxv[0] * fx + nflxv[1] * fy + nflxv[2] * fz;
+            double adv[3] = {advx, advy, advz};
+            for (int k = 0; k < 3; k++)
+                SlowMh[i * 3 + k] = -(nflxv[k] - dpr * fr[k]) - adv[k] + DivM[i * 3 + k]
+                                    + diffmh[i * 3 + k] + diffmv[i * 3 + k] + dMh[i * 3 + k];
+            if (lev == 0) {
+                SlowWh[id * nvi + 0]  = 0.0;
+                SlowWh[id * nvi + nv] = 0.0;
+            }
+            else {
+                double xi = althl, xim = altl, xip = alt;
+                double intt = (xi - xip) / (xim - xip), intl = (xi - xim) / (xip - xim);
+                double swr;
+                if (deep) {
+                    if (ghv)
+                        swr = (advrl + rhol * Gravit * pow(A / (A + altl), 2)) * intt
+                              + (advr + rho * Gravit * pow(A / (A + alt), 2)) * intl;
+                    else
+                        swr = (advrl + rhol * Gravit) * intt + (advr + rho * Gravit) * intl;
+                }
+                else {
+                    if (ghv)
+                        swr = (rhol * Gravit * pow(A / (A + altl), 2)) * intt
+                              + (rho * Gravit * pow(A / (A + alt), 2)) * intl;
+                    else
+                        swr = (rhol * Gravit) * intt + (rho * Gravit) * intl;
+                }
+                if (nonh)
+                    swr += (-diffw[i - 1] - diffwv[i - 1]) * intt + (-diffw[i] - diffwv[i]) * intl;
+                double dz2  = alt - altl;
+                double dpdz = (p[i] - pressurel) / dz2;
+                swr += dpdz;
+                swr -= dWh[id * nvi + lev];
+                SlowWh[id * nvi + lev] = -swr;
+            }
+            nflxr += dwdz;
+            SlowRho[i] = -nflxr + diffrh[i] + diffrv[i];
+            double r   = 1.0 / rho;
+            double vgp = (nflxv[0] - dpr * fx) * Mh[i * 3 + 0] * r + (nflxv[1] - dpr * fy) * Mh[i * 3 + 1] * r
+                         + (nflxv[2] - dpr * fz) * Mh[i * 3 + 2] * r;
+            Slowp[i] = (Rd[i] / Cv) * (-nflxp - gtil[i] - dwhdz + vgp + Qheat[i]);
+            if (eeq)
+                Slowp[i] += Rd[i] / Cv * (diffpr[i] + diffprv[i]);
+            else
+                Slowp[i] += diffpr[i] + diffprv[i];
+        }
+    }
+}
+
+// UpdateRK, thor_auxiliary.h:311-418 (no module arrays)
+void update_rk(Oracle& o) {
+    int  N = o.N, nv = o.nv, nvi = o.nvi;
+    Vec &M = F(o, "Mhs"), &Mk = F(o, "Mhk"), &Mi = F(o, "Mh"), &Wh = F(o, "Whs"), &Whk = F(o, "Whk"),
+        &Whi = F(o, "Wh"), &W = F(o, "Ws"), &R = F(o, "Rhos"), &Rk = F(o, "Rhok"), &Ri = F(o, "Rho"),
+        &P = F(o, "pressures"), &Pk = F(o, "pressurek"), &Pi = F(o, "pressure");
+#pragma omp parallel for schedule(static)
+    for (int id = 0; id < N; id++) {
+        double fx = o.func_r[id * 3 + 0], fy = o.func_r[id * 3 + 1], fz = o.func_r[id * 3 + 2];
+        for (int lev = 0; lev < nv; lev++) {
+            size_t i  = (size_t)id * nv + lev;
+            double Mx = Mi[i * 3 + 0] - Mk[i * 3 + 0], My = Mi[i * 3 + 1] - Mk[i * 3 + 1],
+                   Mz = Mi[i * 3 + 2] - Mk[i * 3 + 2];
+            double aux = Mx * fx + My * fy + Mz * fz;
+            M[i * 3 + 0] = Mx - aux * fx;
+            M[i * 3 + 1] = My - aux * fy;
+            M[i * 3 + 2] = Mz - aux * fz;
+            R[i]         = Ri[i] - Rk[i];
+            P[i]         = Pi[i] - Pk[i];
+        }
+        double altht = 0, althl, wht = 0, whl;
+        for (int lev = 0; lev < nv + 1; lev++) {
+            if (lev == 0) {
+                Wh[id * nvi + 0] = 0.0;
+                altht            = o.Altitudeh[lev];
+                wht              = 0.0;
+            }
+            else {
+                whl = wht;
+                if (lev == nv)
+                    wht = 0.0;
+                else
+                    wht = Whi[id * nvi + lev] - Whk[id * nvi + lev];
+                Wh[id * nvi + lev] = wht;
+                althl              = altht;
+                altht              = o.Altitudeh[lev];
+                double xi = o.Altitude[lev - 1], xim = althl, xip = altht;
+                double intt = (xi - xip) / (xim - xip), intl = (xi - xim) / (xip - xim);
+                W[id * nv + lev - 1] = whl * intt + wht * intl;
+            }
+        }
+    }
+}
+
+// UpdateRK2, thor_auxiliary.h:420-529 (no module arrays)
+void update_rk2(Oracle& o) {
+    int  N = o.N, nv = o.nv, nvi = o.nvi;
+    Vec &M = F(o, "Mhs"), &Mk = F(o, "Mhk"), &Wh = F(o, "Whs"), &Whk = F(o, "Whk"), &Wk = F(o, "Wk"),
+        &R = F(o, "Rhos"), &Rk = F(o, "Rhok"), &P = F(o, "pressures"), &Pk = F(o, "pressurek");
+#pragma omp parallel for schedule(static)
+    for (int id = 0; id < N; id++) {
+        double fx = o.func_r[id * 3 + 0], fy = o.func_r[id * 3 + 1], fz = o.func_r[id * 3 + 2];
+        for (int lev = 0; lev < nv; lev++) {
+            size_t i  = (size_t)id * nv + lev;
+            double Mx = M[i * 3 + 0] + Mk[i * 3 + 0], My = M[i * 3 + 1] + Mk[i * 3 + 1],
+                   Mz = M[i * 3 + 2] + Mk[i * 3 + 2];
+            double aux = Mx * fx + My * fy + Mz * fz;
+            Mk[i * 3 + 0] = Mx - aux * fx;
+            Mk[i * 3 + 1] = My - aux * fy;
+            Mk[i * 3 + 2] = Mz - aux * fz;
+            Rk[i] += R[i];
+            Pk[i] += P[i];
+        }
+        for (int lev = 0; lev < nv + 1; lev++) {
+            if (lev == 0 || lev == nv)
+                Whk[id * nvi + lev] = 0.0;
+            else
+                Whk[id * nvi + lev] += Wh[id * nvi + lev];
+        }
+        double althl = 0, altht = o.Altitudeh[1], whl = 0.0, wht = Whk[id * nvi + 1];
+        for (int lev = 0; lev < nv; lev++) {
+            double xi = o.Altitude[lev], xim = althl, xip = altht;
+            double intt = (xi - xip) / (xim - xip), intl = (xi - xim) / (xip - xim);
+            Wk[id * nv + lev] = whl * intt + wht * intl;
+            if (lev < nv - 1) {
+                althl = altht;
+                altht = o.Altitudeh[lev + 2];
+                whl   = wht;
+                wht   = Whk[id * nvi + lev + 2];
+            }
+        }
+    }
+}
+
+// Momentum_Eq (thor_fastmodes.h:54-167) and Momentum_Eq_Poles (:169-253)
+void momentum_eq(Oracle& o, double dt) {
+    int  N = o.N, nv = o.nv;
+    Vec &M = F(o, "Mhs"), &p = F(o, "pressures"), &SlowMh = F(o, "SlowMh"), &DivM = F(o, "DivM");
+#pragma omp parallel for schedule(static)
+    for (int id = 0; id < N; id++) {
+        const int*    nb = &o.nb7[(size_t)id * 7];
+        int           nt = o.nterms[id];
+        const double* fr = &o.func_r[id * 3];
+        const double* gr = &o.grad[id * 21];
+        for (int lev = 0; lev < nv; lev++) {
+            size_t i      = (size_t)id * nv + lev;
+            double rscale = o.P.DeepModel ? o.P.A / (o.Altitude[lev] + o.P.A) : 1.0;
+            double nflxv[3], Mv[3];
+            for (int k = 0; k < 3; k++)
+                nflxv[k] = rscale * stencil_sum(gr, k, nt, [&](int j) { return val(p, nb[j], nv, lev); });
+            for (int k = 0; k < 3; k++)
+                Mv[k] = (-nflxv[k] + SlowMh[i * 3 + k] + DivM[i * 3 + k]) * dt;
+            double vr = Mv[0] * fr[0] + Mv[1] * fr[1] + Mv[2] * fr[2];
+            for (int k = 0; k < 3; k++)
+                Mv[k] += -vr * fr[k];
+            for (int k = 0; k < 3; k++)
+                M[i * 3 + k] += Mv[k];
+        }
+    }
+}
+
+// Prepare_Implicit_Vertical (thor_vertical_int.h:566-688) and its poles kernel (:690-771)
+void prepare_implicit_vertical(Oracle& o) {
+    int  N = o.N, nv = o.nv;
+    Vec &M = F(o, "Mhs"), &h = F(o, "h"), &Slowp = F(o, "Slowpressure"), &SlowRho = F(o, "SlowRho"),
+        &Sp = F(o, "Sp"), &Sd = F(o, "Sd"), &Cp = F(o, "Cp"), &Rd = F(o, "Rd");
+#pragma omp parallel for schedule(static)
+    for (int id = 0; id < N; id++) {
+        const int*    nb = &o.nb7[(size_t)id * 7];
+        int           nt = o.nterms[id];
+        const double* dv = &o.div[id * 21];
+        for (int lev = 0; lev < nv; lev++) {
+            size_t i      = (size_t)id * nv + lev;
+            double RoC    = Rd[i] / (Cp[i] - Rd[i]);
+            double rscale = o.P.DeepModel ? o.P.A / (o.Altitude[lev] + o.P.A) : 1.0;
+            double nflxr = 0.0, nflxp = 0.0;
+            for (int k = 0; k < 3; k++) {
+                nflxr -= rscale * stencil_sum(dv, k, nt, [&](int j) { return val3(M, nb[j], nv, lev, k); });
+                nflxp -= (RoC)*rscale * stencil_sum2(dv, k, nt,
+                                                     [&](int j) { return val3(M, nb[j], nv, lev, k); },
+                                                     [&](int j) { return val(h, nb[j], nv, lev); });
+            }
+            Sp[i] = nflxp + Slowp[i];
+            Sd[i] = nflxr + SlowRho[i];
+        }
+    }
+}
+
+// Vertical_Eq, thor_vertical_int.h:52-563 (Thomas algorithm per column)
+void vertical_eq(Oracle& o, double deltat) {
+    int    N = o.N, nv = o.nv, nvi = o.nvi;
+    Vec &  Whs = F(o, "Whs"), &Ws = F(o, "Ws"), &ps = F(o, "pressures"), &hh = F(o, "hh"),
+        &Rhos = F(o, "Rhos"), &gtilh = F(o, "gtilh"), &Sp_ = F(o, "Sp"), &Sd_ = F(o, "Sd"),
+        &Srh = F(o, "SlowWh"), &Cp = F(o, "Cp"), &Rd = F(o, "Rd");
+    double A = o.P.A, Gravit = o.P.Gravit;
+    bool   deep = o.P.DeepModel, nonh = o.P.NonHydro, ghv = o.P.GravHeightVar;
+    const double* Alt  = o.Altitude.data();
+    const double* Alth = o.Altitudeh.data();
+#pragma omp parallel for schedule(static)
+    for (int id = 0; id < N; id++) {
+        std::vector<double> cc(nvi), dd(nvi);
+        double althl = 0, alth = 0, altht = 0, alt = 0, altl = 0;
+        double Sp = 0, Spl = 0, p = 0, pl = 0, r = 0, rl = 0, Sdl = 0, Sd = 0;
+        double hp = 0, h = 0, hm = 0, gp = 0, g = 0, gm = 0;
+        double GCoRl = 0, GCoRu = 0, CRddl = 0, CRddu = 0;
+        for (int lev = 1; lev < nv; lev++) {
+            if (lev == 1) {
+                altht = Alth[lev + 1];
+                althl = Alth[lev - 1];
+                alth  = Alth[lev];
+                alt   = Alt[lev];
+                altl  = Alt[lev - 1];
+                hp    = hh[id * nvi + lev + 1];
+                h     = hh[id * nvi + lev];
+                hm    = hh[id * nvi + lev - 1];
+                gp    = gtilh[id * nvi + lev + 1];
+                g     = gtilh[id * nvi + lev];
+                gm    = gtilh[id * nvi + lev - 1];
+                Sp    = Sp_[id * nv + lev];
+                Spl   = Sp_[id * nv + lev - 1];
+                p     = ps[id * nv + lev];
+                pl    = ps[id * nv + lev - 1];
+                rl    = Rhos[id * nv + lev - 1];
+                r     = Rhos[id * nv + lev];
+                Sdl   = Sd_[id * nv + lev - 1];
+                Sd    = Sd_[id * nv + lev];
+                CRddl = (Cp[id * nv + lev - 1] - Rd[id * nv + lev - 1]) / (Rd[id * nv + lev - 1] * deltat * deltat);
+                CRddu = (Cp[id * nv + lev] - Rd[id * nv + lev]) / (Rd[id * nv + lev] * deltat * deltat);
+                if (ghv) {
+                    GCoRl = Gravit * pow(A / (A + altl), 2) * (Cp[id * nv + lev - 1] - Rd[id * nv + lev - 1])
+                            / Rd[id * nv + lev - 1];
+                    GCoRu = Gravit * pow(A / (A + alt), 2) * (Cp[id * nv + lev] - Rd[id * nv + lev]) / Rd[id * nv + lev];
+                }
+                else {
+                    GCoRl = Gravit * (Cp[id * nv + lev - 1] - Rd[id * nv + lev - 1]) / Rd[id * nv + lev - 1];
+                    GCoRu = Gravit * (Cp[id * nv + lev] - Rd[id * nv + lev]) / Rd[id * nv + lev];
+                }
+            }
+            double aa, bb, C0, intl, inttm, intt;
+            double dzp  = 1.0 / (altht - alth);
+            double dzh  = 1.0 / (alt - altl);
+            double dzm  = 1.0 / (alth - althl);
+            double dzph = dzp * dzh;
+            double dzmh = dzm * dzh;
+            double xi, xim, xip;
+            if (deep) {
+                // the reference scales its h registers in place here; the scaled copies are
+                // what the coefficients use, and the next level reloads them from memory
+                double hp_ = hp * pow(altht + A, 2);
+                double h_  = h * pow(alth + A, 2);
+                double hm_ = hm * pow(althl + A, 2);
+                double or2  = 1 / pow(alth + A, 2);
+                double tor3 = 2 / pow(alth + A, 3);
+                xi    = alt;
+                xim   = alth;
+                xip   = altht;
+                intl  = (xi - xim) * dzp * dzh;
+                xi    = altl;
+                xim   = althl;
+                xip   = alth;
+                inttm = -(xi - xip) * dzm * dzh;
+                double CRdd = (CRddl * (alt - alth) + CRddu * (alth - altl)) / (alt - altl);
+                double GCoR = (GCoRl * (alt - alth) + GCoRu * (alth - altl)) / (alt - altl);
+                cc[lev]     = -dzph * or2 * hp_ - inttm * (gp + GCoR - tor3 * hp_);
+                if (nonh)
+                    bb = CRdd + (dzph + dzmh) * or2 * h_ + (intl - inttm) * (g + GCoR - tor3 * h_);
+                else
+                    bb = (dzph + dzmh) * or2 * h_ + (intl - inttm) * (g + GCoR - tor3 * h_);
+                aa = -dzmh * or2 * hm_ + intl * (gm + GCoR - tor3 * hm_);
+                double dSpdz = (Sp - Spl) * dzh;
+                double dPdz  = (p - pl) * dzh;
+                xi   = alth;
+                xim  = altl;
+                xip  = alt;
+                intt = (xi - xip) / (xim - xip);
+                intl = (xi - xim) / (xip - xim);
+                double rhohs = rl * intt + r * intl;
+                double Sdh   = Sdl * intt + Sd * intl;
+                double gg    = ghv ? Gravit * pow(A / (A + alt), 2) : Gravit;
+                if (!nonh) {
+                    if (ghv)
+                        C0 = (pow(deltat, 2.0) * dSpdz + pow(deltat, 2.0) * Gravit * pow(A / (A + alt), 2) * Sdh + gg * deltat * rhohs
+                              + deltat * dPdz - deltat * Srh[id * nvi + lev])
+                             * (CRdd);
+                    else
+                        C0 = (pow(deltat, 2.0) * dSpdz + pow(deltat, 2.0) * Gravit * Sdh
+                              + Gravit * deltat * rhohs + deltat * dPdz - deltat * Srh[id * nvi + lev])
+                             * (CRdd);
+                }
+                else {
+                    if (ghv)
+                        C0 = (-Whs[id * nvi + lev] + pow(deltat, 2.0) * dSpdz + pow(deltat, 2.0) * Gravit * pow(A / (A + alt), 2) * Sdh
+                              + gg * deltat * rhohs + deltat * dPdz - deltat * Srh[id * nvi + lev])
+                             * (CRdd);
+                    else
+                        C0 = (-Whs[id * nvi + lev] + pow(deltat, 2.0) * dSpdz + pow(deltat, 2.0) * Gravit * Sdh
+                              + Gravit * deltat * rhohs + deltat * dPdz - deltat * Srh[id * nvi + lev])
+                             * (CRdd);
+                }
+                // (the deep branch reloads hm, h, hp from memory for the next level)
+                if (lev < nv - 1) {
+                    hm = hh[id * nvi + lev];
+                    h  = hh[id * nvi + lev + 1];
+                    hp = hh[id * nvi + lev + 2];
+                }
+            }
+            else {
+                xi    = alt;
+                xim   = alth;
+                xip   = altht;
+                intl  = (xi - xim) * dzp * dzh;
+                xi    = altl;
+                xim   = althl;
+                xip   = alth;
+                inttm = -(xi - xip) * dzm * dzh;
+                double CRdd = (CRddl * (alt - alth) + CRddu * (alth - altl)) / (alt - altl);
+                double GCoR = (GCoRl * (alt - alth) + GCoRu * (alth - altl)) / (alt - altl);
+                cc[lev]     = -dzph * hp - inttm * (gp + GCoR);
+                if (nonh)
+                    bb = CRdd + (dzph + dzmh) * h + (intl - inttm) * (g + GCoR);
+                else
+                    bb = (dzph + dzmh) * h + (intl - inttm) * (g + GCoR);
+                aa = -dzmh * hm + intl * (gm + GCoR);
+                double dSpdz = (Sp - Spl) * dzh;
+                double dPdz  = (p - pl) * dzh;
+                xi   = alth;
+                xim  = altl;
+                xip  = alt;
+                intt = (xi - xip) / (xim - xip);
+                intl = (xi - xim) / (xip - xim);
+                double rhohs = rl * intt + r * intl;
+                double Sdh   = Sdl * intt + Sd * intl;
+                double gg    = ghv ? Gravit * pow(A / (A + alt), 2) : Gravit;
+                if (!nonh) {
+                    if (ghv)
+                        C0 = (pow(deltat, 2.0) * dSpdz + pow(deltat, 2.0) * Gravit * pow(A / (A + alt), 2) * Sdh + gg * deltat * rhohs
+                              + deltat * dPdz - deltat * Srh[id * nvi + lev])
+                             * (CRdd);
+                    else
+                        C0 = (pow(deltat, 2.0) * dSpdz + pow(deltat, 2.0) * Gravit * Sdh
+                              + Gravit * deltat * rhohs + deltat * dPdz - deltat * Srh[id * nvi + lev])
+                             * (CRdd);
+                }
+                else {
+                    if (ghv)
+                        C0 = (-Whs[id * nvi + lev] + pow(deltat, 2.0) * dSpdz + pow(deltat, 2.0) * Gravit * pow(A / (A + alt), 2) * Sdh
+                              + gg * deltat * rhohs + deltat * dPdz - deltat * Srh[id * nvi + lev])
+                             * (CRdd);
+                    else
+                        C0 = (-Whs[id * nvi + lev] + pow(deltat, 2.0) * dSpdz + pow(deltat, 2.0) * Gravit * Sdh
+                              + Gravit * deltat * rhohs + deltat * dPdz - deltat * Srh[id * nvi + lev])
+                             * (CRdd);
+                }
+                if (lev < nv - 1) {
+                    hm = h;
+                    h  = hp;
+                    hp = hh[id * nvi + lev + 2];
+                }
+            }
+            if (lev < nv - 1) { // fetch the next level
+                althl = alth;
+                alth  = altht;
+                altht = Alth[lev + 2];
+                altl  = alt;
+                alt   = Alt[lev + 1];
+                gm    = g;
+                g     = gp;
+                gp    = gtilh[id * nvi + lev + 2];
+                Spl   = Sp;
+                Sp    = Sp_[id * nv + lev + 1];
+                pl    = p;
+                p     = ps[id * nv + lev + 1];
+                rl    = r;
+                r     = Rhos[id * nv + lev + 1];
+                Sdl   = Sd;
+                Sd    = Sd_[id * nv + lev + 1];
+                CRddl = CRddu;
+                CRddu = (Cp[id * nv + lev + 1] - Rd[id * nv + lev + 1]) / (Rd[id * nv + lev + 1] * deltat * deltat);
+                GCoRl = GCoRu;
+                if (ghv)
+                    GCoRu = Gravit * pow(A / (A + alt), 2) * (Cp[id * nv + lev + 1] - Rd[id * nv + lev + 1])
+                            / Rd[id * nv + lev + 1];
+                else
+                    GCoRu = Gravit * (Cp[id * nv + lev + 1] - Rd[id * nv + lev + 1]) / Rd[id * nv + lev + 1];
+            }
+            dd[lev] = -C0;
+            if (lev == 1) {
+                cc[1] = cc[1] / bb;
+                dd[1] = dd[1] / bb;
+            }
+            else {
+                double t = 1.0 / (bb - cc[lev - 1] * aa);
+                cc[lev] *= t;
+                dd[lev] = (dd[lev] - dd[lev - 1] * aa) * t;
+            }
+        }
+        Whs[id * nvi + nv]     = 0.0;
+        Whs[id * nvi]          = 0.0;
+        Whs[id * nvi + nv - 1] = dd[nv - 1];
+        for (int lev = nvi - 2; lev > 0; lev--)
+            Whs[id * nvi + lev] = (-cc[lev] * Whs[id * nvi + lev + 1] + dd[lev]);
+        double althl2 = 0, altht2 = Alth[1], whl = 0.0, wht = Whs[id * nvi + 1];
+        for (int lev = 0; lev < nv; lev++) {
+            double xi = Alt[lev], xim = althl2, xip = altht2;
+            double intt = (xi - xip) / (xim - xip), intl = (xi - xim) / (xip - xim);
+            Ws[id * nv + lev] = whl * intt + wht * intl;
+            if (lev < nv - 1) {
+                althl2 = altht2;
+                altht2 = Alth[lev + 2];
+                whl    = wht;
+                wht    = Whs[id * nvi + lev + 2];
+            }
+        }
+    }
+}
+
+// Density_Pressure_Eqs (thor_fastmodes.h:255-574) and its poles kernel (:577-847)
+void density_pressure_eqs(Oracle& o, double dt) {
+    int    N = o.N, nv = o.nv, nvi = o.nvi;
+    Vec &  ps = F(o, "pressures"), &pk = F(o, "pressurek"), &Rhos = F(o, "Rhos"), &Rhok = F(o, "Rhok"),
+        &Mhs = F(o, "Mhs"), &Mhk = F(o, "Mhk"), &Whs = F(o, "Whs"), &Whk = F(o, "Whk"), &pt = F(o, "pt"),
+        &pth = F(o, "pth"), &ep = F(o, "epotential"), &eph = F(o, "epotentialh"), &ek = F(o, "ekinetic"),
+        &ekh = F(o, "ekinetich"), &Et = F(o, "Etotal"), &h = F(o, "h"), &hh = F(o, "hh"),
+        &SlowRho = F(o, "SlowRho"), &Q = F(o, "profx_Qheat"), &diffpr = F(o, "diffpr"),
+        &diffprv = F(o, "diffprv"), &Cp = F(o, "Cp"), &Rd = F(o, "Rd");
+    double A = o.P.A, P_Ref = o.P.P_Ref, Gravit = o.P.Gravit;
+    bool   deep = o.P.DeepModel, eeq = o.P.energy_equation, ghv = o.P.GravHeightVar;
+    // thermodynamic variable advected horizontally
+    auto ptv = [&](int id, int lev) -> double {
+        if (id < 0)
+            return 0.0;
+        size_t i = (size_t)id * nv + lev;
+        return eeq ? (h[i] + ep[i] + ek[i]) : pt[i];
+    };
+#pragma omp parallel for schedule(static)
+    for (int id = 0; id < N; id++) {
+        const int*    nb = &o.nb7[(size_t)id * 7];
+        int           nt = o.nterms[id];
+        bool          pole = o.pole[id];
+        const double* dv = &o.div[id * 21];
+        for (int lev = 0; lev < nv; lev++) {
+            size_t i     = (size_t)id * nv + lev;
+            double Cv    = Cp[i] - Rd[i];
+            double altht = o.Altitudeh[lev + 1], althl = o.Altitudeh[lev];
+            double dz    = altht - althl;
+            double r2p, r2m, r2l, rscale, dr2dz;
+            if (deep) {
+                double alt = o.Altitude[lev];
+                r2p        = pow(altht + A, 2.0);
+                r2m        = pow(alt + A, 2.0);
+                r2l        = pow(althl + A, 2.0);
+                rscale     = A / (alt + A);
+                dr2dz      = (pow(altht + A, 3.0) - pow(althl + A, 3.0)) / 3.0;
+            }
+            else {
+                r2p = r2m = r2l = rscale = 1.0;
+                dr2dz                    = r2m * dz;
+            }
+            double nflxr = 0.0, nflxpt = 0.0;
+            for (int k = 0; k < 3; k++) {
+                nflxr += rscale * stencil_sum(dv, k, nt, [&](int j) { return val3(Mhs, nb[j], nv, lev, k); });
+                nflxpt += rscale * stencil_sum2(dv, k, nt,
+                                                [&](int j) {
+                                                    int c = nb[j];
+                                                    return c >= 0 ? Mhs[((size_t)c * nv + lev) * 3 + k]
+                                                                        + Mhk[((size_t)c * nv + lev) * 3 + k]
+                                                                  : 0.0;
+                                                },
+                                                [&](int j) { return ptv(nb[j], lev); });
+            }
+            auto phv = [&](int l) -> double {
+                size_t j = (size_t)id * nvi + l;
+                return eeq ? (hh[j] + eph[j] + ekh[j]) : pth[j];
+            };
+            double whl, wht, whl2, wht2, phl, pht;
+            if (lev == 0) {
+                whl  = 0.0;
+                wht  = Whs[id * nvi + lev + 1];
+                whl2 = 0.0;
+                wht2 = Whs[id * nvi + lev + 1] + Whk[id * nvi + lev + 1];
+                phl  = 0.0;
+                pht  = phv(lev + 1);
+            }
+            else {
+                whl  = Whs[id * nvi + lev];
+                wht  = Whs[id * nvi + lev + 1];
+                whl2 = Whs[id * nvi + lev] + Whk[id * nvi + lev];
+                wht2 = Whs[id * nvi + lev + 1] + Whk[id * nvi + lev + 1];
+                phl  = phv(lev);
+                pht  = phv(lev + 1);
+            }
+            double dwdz   = pole ? (wht * r2p - whl * r2l) / (dz * r2m) : (wht * r2p - whl * r2l) / (dr2dz);
+            double dwptdz = (wht2 * pht * r2p - whl2 * phl * r2l) / (dz * r2m);
+            double aux    = -(nflxpt + dwptdz) * dt;
+            double r      = Rhok[i] + Rhos[i];
+            nflxr += dwdz;
+            Rhos[i] += (SlowRho[i] - nflxr) * dt;
+            if (eeq) {
+                aux += Et[i] + (diffpr[i] + diffprv[i]) * dt + Q[i] * dt;
+                Et[i]    = aux;
+                double w = (whl2 * (o.Altitudeh[lev + 1] - o.Altitude[lev]) + wht2 * (o.Altitude[lev] - o.Altitudeh[lev]))
+                           / (o.Altitudeh[lev + 1] - o.Altitudeh[lev]);
+                double v1x = Mhs[i * 3 + 0] + Mhk[i * 3 + 0], v1y = Mhs[i * 3 + 1] + Mhk[i * 3 + 1],
+                       v1z = Mhs[i * 3 + 2] + Mhk[i * 3 + 2];
+                double Epot_kin;
+                if (ghv)
+                    Epot_kin = (Rhos[i] + Rhok[i]) * Gravit * pow(A / (A + o.Altitude[lev]), 2) * o.Altitude[lev]
+                               + 0.5 * (pow(v1x, 2) + pow(v1y, 2) + pow(v1z, 2) + pow(w, 2)) / (Rhos[i] + Rhok[i]);
+                else
+                    Epot_kin = (Rhos[i] + Rhok[i]) * Gravit * o.Altitude[lev]
+                               + 0.5 * (pow(v1x, 2) + pow(v1y, 2) + pow(v1z, 2) + pow(w, 2)) / (Rhos[i] + Rhok[i]);
+                ps[i] = Rd[i] / Cv * (aux - Epot_kin) - pk[i];
+            }
+            else {
+                double ptc = (P_Ref / (Rd[i] * r)) * pow((ps[i] + pk[i]) / P_Ref, Cv / Cp[i]);
+                aux += ptc * r;
+                double pn = P_Ref * pow(Rd[i] * aux / P_Ref, Cp[i] / Cv);
+                ps[i]     = pn - pk[i] + (diffpr[i] + diffprv[i]) * dt + Rd[i] / Cv * Q[i] * dt;
+            }
+        }
+    }
+}
+
+// ESP::Thor, src/ESP/thor_driver.cu:70-1466
+void thor(Oracle& o) {
+    auto copy = [&](const char* d, const char* s) { F(o, d) = F(o, s); };
+    auto zero = [&](const char* n) { std::fill(F(o, n).begin(), F(o, n).end(), 0.0); };
+    copy("Mhk", "Mh");
+    copy("Whk", "Wh");
+    copy("Wk", "W");
+    copy("Rhok", "Rho");
+    copy("pressurek", "pressure");
+    for (auto n : {"Mhs", "Rhos", "Whs", "Ws", "pressures"})
+        zero(n);
+    double dt = o.P.timestep;
+    for (int rk = 0; rk < 3; rk++) {
+        int    ns_it = (rk == 0) ? 1 : (rk == 1 ? 3 : 6);
+        double times = (rk == 0) ? dt / 3.0 : dt / 6.0;
+        zero("Adv");
+        advec_cori1(o);
+        advec_cori2(o);
+        temperature_h_pt_geff(o);
+        for (auto n : {"SlowMh", "SlowWh", "SlowRho", "Slowpressure"})
+            zero(n);
+        if (o.P.HyDiff) {
+            zero("diff");
+            int stepnum = 0;
+            for (int ihyp = 0; ihyp < o.P.HyDiffOrder / 2 - 1; ihyp++) {
+                diffusion_pass(o, stepnum, false);
+                stepnum += 1;
+            }
+            zero("diffrh");
+            diffusion_pass(o, stepnum, true);
+            correct_horizontal(o);
+        }
+        zero("DivM");
+        zero("divg_Mh");
+        if (o.P.DivDampP) {
+            divm_pass(o, F(o, "Mhk"), F(o, "Whk"), false);
+            divm_pass(o, F(o, "Mhk"), F(o, "Whk"), true);
+        }
+        slow_modes(o);
+        if (rk > 0)
+            update_rk(o);
+        for (int ns = 0; ns < ns_it; ns++) {
+            zero("DivM");
+            zero("divg_Mh");
+            if (o.P.DivDampP) {
+                divm_pass(o, F(o, "Mhs"), F(o, "Whs"), false);
+                divm_pass(o, F(o, "Mhs"), F(o, "Whs"), true);
+            }
+            momentum_eq(o, times);
+            prepare_implicit_vertical(o);
+            vertical_eq(o, times);
+            density_pressure_eqs(o, times);
+        }
+        update_rk2(o);
+    }
+    copy("Mh", "Mhk");
+    copy("Wh", "Whk");
+    copy("W", "Wk");
+    copy("Rho", "Rhok");
+    copy("pressure", "pressurek");
+}
+
+} // namespace
+
+extern "C" void* oracle_new(const oracle_grid* g, const oracle_params* p) {
+    Oracle* o = new Oracle;
+    o->P      = *p;
+    o->N      = g->point_num;
+    o->nv     = g->nv;
+    o->nvi    = g->nv + 1;
+    o->nl     = g->nl_region;
+    o->nr     = g->nr;
+    int N = o->N, nv = o->nv, nvi = o->nvi;
+    o->maps.assign(g->maps, g->maps + (size_t)(o->nl + 2) * (o->nl + 2) * o->nr);
+    o->point_local.assign(g->point_local, g->point_local + (size_t)6 * N);
+    o->Altitude.assign(g->Altitude, g->Altitude + nv);
+    o->Altitudeh.assign(g->Altitudeh, g->Altitudeh + nvi);
+    o->lonlat.assign(g->lonlat, g->lonlat + 2 * (size_t)N);
+    o->areas.assign(g->areas, g->areas + 18 * (size_t)N);
+    o->areasTr.assign(g->areasTr, g->areasTr + 6 * (size_t)N);
+    o->nvecoa.assign(g->nvecoa, g->nvecoa + 18 * (size_t)N);
+    o->nvecti.assign(g->nvecti, g->nvecti + 18 * (size_t)N);
+    o->nvecte.assign(g->nvecte, g->nvecte + 18 * (size_t)N);
+    o->div.assign(g->div, g->div + 21 * (size_t)N);
+    o->grad.assign(g->grad, g->grad + 21 * (size_t)N);
+    o->func_r.assign(g->func_r, g->func_r + 3 * (size_t)N);
+    build_neighbours(*o);
+    // src/ESP/esp_initial.cu:1292-1335 without the diffusive sponge
+    o->Kdh4.resize(nv);
+    o->Kdhz.resize(nv);
+    for (int lev = 0; lev < nv; lev++) {
+        double dbar  = sqrt(2 * M_PI / 5) * p->A / (pow(2, p->glevel));
+        o->Kdh4[lev] = (p->Diffc) * pow(dbar, 1.0 * p->HyDiffOrder) / p->timestep;
+        o->Kdhz[lev] = (p->DivDampc) * pow(dbar, 4.) / p->timestep;
+    }
+    const char* cell1[] = {"Rho", "Rhok", "Rhos", "pressure", "pressurek", "pressures",
+                           "temperature", "W", "Wk", "Ws", "h", "pt", "gtil", "SlowRho",
+                           "Slowpressure", "Sp", "Sd", "diffw", "diffrh", "diffpr", "diffwv",
+                           "diffrv", "diffprv", "epotential", "ekinetic", "Etotal", "Cp", "Rd",
+                           "profx_Qheat", "profx_dW"};
+    const char* cell3[] = {"Mh", "Mhk", "Mhs", "Adv", "v", "SlowMh", "DivM", "divg_Mh",
+                           "diffmh", "diffmv", "profx_dMh"};
+    const char* iface[] = {"Wh", "Whk", "Whs", "hh", "pth", "gtilh", "SlowWh", "epotentialh",
+                           "ekinetich", "profx_dWh"};
+    for (auto n : cell1)
+        o->f[n].assign((size_t)N * nv, 0.0);
+    for (auto n : cell3)
+        o->f[n].assign((size_t)N * nv * 3, 0.0);
+    for (auto n : iface)
+        o->f[n].assign((size_t)N * nvi, 0.0);
+    o->f["diff"].assign((size_t)N * nv * 6, 0.0);
+    return o;
+}
+
+extern "C" long oracle_set(void* h, const char* name, const double* src) {
+    Oracle* o  = (Oracle*)h;
+    auto    it = o->f.find(name);
+    if (it == o->f.end())
+        return -1;
+    std::memcpy(it->second.data(), src, it->second.size() * sizeof(double));
+    return (long)it->second.size();
+}
+
+extern "C" long oracle_get(void* h, const char* name, double* dst) {
+    Oracle* o  = (Oracle*)h;
+    auto    it = o->f.find(name);
+    if (it == o->f.end())
+        return -1;
+    if (dst)
+        std::memcpy(dst, it->second.data(), it->second.size() * sizeof(double));
+    return (long)it->second.size();
+}
+
+extern "C" int oracle_step(void* h, int nsteps, int do_profx, int do_thor) {
+    Oracle* o = (Oracle*)h;
+    for (int s = 0; s < nsteps; s++) {
+        if (do_profx)
+            profx(*o);
+        if (do_thor)
+            thor(*o);
+    }
+    return 0;
+}
+
+extern "C" void oracle_set_threads(int n) {
+#ifdef _OPENMP
+    omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}
+
+extern "C" void oracle_free(void* h) { delete (Oracle*)h; }

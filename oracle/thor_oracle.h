@@ -1,0 +1,41 @@
+// CPU restatement of THOR's HE-VI dynamical-core step and Held-Suarez ProfX step.
+// TEST INFRASTRUCTURE ONLY: the oracle for parity tests and the timed CPU baseline. The product
+// (thor_b200/) never links, loads or calls it.
+#pragma once
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+// Physical and numerical switches, as in the reference's SimulationSetup
+// (src/headers/simulation_setup.h) and ESP members (src/headers/esp.h).
+typedef struct {
+    double A, Omega, Gravit, Rd, Cp, P_Ref, timestep, Diffc, DivDampc;
+    int    HyDiffOrder;
+    int    DeepModel, NonHydro, GravHeightVar, HyDiff, DivDampP, energy_equation, held_suarez;
+    int    glevel;
+} oracle_params;
+
+// Grid arrays in the reference layout (src/ESP/grid.cu): maps [nr][(nl+2)^2], point_local [N][6],
+// div/grad [N][7][3], areas/nvecoa/nvecti/nvecte [N][6][3], areasTr [N][6], func_r [N][3],
+// lonlat [N][2], Altitude [nv], Altitudeh [nv+1]. Copied at creation.
+typedef struct {
+    int           point_num, nv, nl_region, nr;
+    const int*    maps;
+    const int*    point_local;
+    const double *Altitude, *Altitudeh, *lonlat, *areas, *areasTr, *nvecoa, *nvecti, *nvecte,
+        *div, *grad, *func_r;
+} oracle_grid;
+
+void* oracle_new(const oracle_grid* g, const oracle_params* p);
+// Copy a named field in/out (reference layout). Returns element count, -1 if unknown.
+long oracle_set(void* h, const char* name, const double* src);
+long oracle_get(void* h, const char* name, double* dst);
+// nsteps x (ProfX if do_profx, then Thor if do_thor), as src/esp.cu:1382-1398.
+int  oracle_step(void* h, int nsteps, int do_profx, int do_thor);
+void oracle_set_threads(int n);
+void oracle_free(void* h);
+
+#ifdef __cplusplus
+}
+#endif

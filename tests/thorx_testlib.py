@@ -1,0 +1,313 @@
+"""Test helpers: ctypes access to the checkers and the seeded initial state.
+
+The checkers are test infrastructure, never the product:
+  * oracle/_build/liboracle.so  - the CPU restatement of the reference step (oracle/thor_oracle.cpp)
+  * oracle/_ref/libthor_ref.so  - the reference's own grid builder and FP64 CUDA kernels,
+                                  compiled from its sources by oracle/Makefile
+"""
+import ctypes
+import os
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_SO = os.path.join(ROOT, "oracle", "_build", "liboracle.so")
+REF_SO = os.path.join(ROOT, "oracle", "_ref", "libthor_ref.so")
+# the same reference sources built with FMA contraction off
+REF_NOFMA_SO = os.path.join(ROOT, "oracle", "_ref", "libthor_ref_nofma.so")
+
+# ------------------------------------------------------------------------------------------------
+# Configurations (Earth Held-Suarez; the reference's ifile/earth_hstest.thr constants)
+# ------------------------------------------------------------------------------------------------
+EARTH = dict(A=6.371e6, Omega=7.292e-5, Gravit=9.8, Rd=287.0, Cp=1005.0, P_Ref=1e5,
+             Top_altitude=36e3, Tmean=300.0, Diffc=0.0048, DivDampc=0.0048, HyDiffOrder=4,
+             DeepModel=1, NonHydro=1, GravHeightVar=0, HyDiff=1, DivDampP=1,
+             energy_equation=0, held_suarez=1)
+
+PARAM_FIELDS = [("A", ctypes.c_double), ("Omega", ctypes.c_double), ("Gravit", ctypes.c_double),
+                ("Rd", ctypes.c_double), ("Cp", ctypes.c_double), ("P_Ref", ctypes.c_double),
+                ("timestep", ctypes.c_double), ("Diffc", ctypes.c_double),
+                ("DivDampc", ctypes.c_double), ("HyDiffOrder", ctypes.c_int),
+                ("DeepModel", ctypes.c_int), ("NonHydro", ctypes.c_int),
+                ("GravHeightVar", ctypes.c_int), ("HyDiff", ctypes.c_int),
+                ("DivDampP", ctypes.c_int), ("energy_equation", ctypes.c_int),
+                ("held_suarez", ctypes.c_int), ("glevel", ctypes.c_int)]
+
+
+class Params(ctypes.Structure):
+    _fields_ = PARAM_FIELDS
+
+
+def make_params(glevel, timestep, **over):
+    c = dict(EARTH)
+    c.update(over)
+    p = Params()
+    for name, _ in PARAM_FIELDS:
+        if name == "timestep":
+            p.timestep = timestep
+        elif name == "glevel":
+            p.glevel = glevel
+        else:
+            setattr(p, name, c[name])
+    return p, c
+
+
+# ------------------------------------------------------------------------------------------------
+# Reference grid (reference src/ESP/grid.cu, host code, runs on the CPU)
+# ------------------------------------------------------------------------------------------------
+GRID_NAMES_F64 = ["point_xyz", "point_xyzq", "Altitude", "Altitudeh", "lonlat", "areas", "areasT",
+                  "areasTr", "nvec", "nvecoa", "nvecti", "nvecte", "mvec", "div", "grad", "curlz",
+                  "func_r"]
+GRID_NAMES_I32 = ["pent_ind", "maps", "point_local"]
+
+_ref = {}
+
+
+def ref_lib(nofma=False):
+    if nofma not in _ref:
+        lib = ctypes.CDLL(REF_NOFMA_SO if nofma else REF_SO)
+        lib.ref_grid_new.restype = ctypes.c_void_p
+        lib.ref_grid_new.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                     ctypes.c_int, ctypes.c_double]
+        lib.ref_grid_get.restype = ctypes.c_long
+        lib.ref_grid_get.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p]
+        lib.ref_grid_dims.argtypes = [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_int)] * 4
+        lib.ref_grid_free.argtypes = [ctypes.c_void_p]
+        lib.ref_sim_new.restype = ctypes.c_void_p
+        lib.ref_sim_new.argtypes = [ctypes.c_void_p, ctypes.POINTER(Params)]
+        lib.ref_sim_set.restype = ctypes.c_long
+        lib.ref_sim_set.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p]
+        lib.ref_sim_get.restype = ctypes.c_long
+        lib.ref_sim_get.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p]
+        lib.ref_sim_step.restype = ctypes.c_int
+        lib.ref_sim_step.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        lib.ref_sim_time.restype = ctypes.c_double
+        lib.ref_sim_time.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        lib.ref_sim_free.argtypes = [ctypes.c_void_p]
+        _ref[nofma] = lib
+    return _ref[nofma]
+
+
+class RefGrid:
+    """The reference's own Icogrid, built on the host, with its arrays copied out."""
+
+    def __init__(self, glevel, nv, A=EARTH["A"], top=EARTH["Top_altitude"], sprd=1, beta=1.15):
+        lib = ref_lib()
+        self.h = lib.ref_grid_new(glevel, nv, A, top, sprd, beta)
+        d = [ctypes.c_int() for _ in range(4)]
+        lib.ref_grid_dims(self.h, *[ctypes.byref(x) for x in d])
+        self.point_num, self.nv, self.nl_region, self.nr = [x.value for x in d]
+        self.glevel = glevel
+        self.arrays = {}
+        for name in GRID_NAMES_F64 + GRID_NAMES_I32:
+            n = lib.ref_grid_get(self.h, name.encode(), None)
+            a = np.zeros(n, dtype=np.float64 if name in GRID_NAMES_F64 else np.int32)
+            lib.ref_grid_get(self.h, name.encode(), a.ctypes.data)
+            self.arrays[name] = a
+
+    def __getitem__(self, k):
+        return self.arrays[k]
+
+    def close(self):
+        if self.h:
+            ref_lib().ref_grid_free(self.h)
+            self.h = None
+
+
+# ------------------------------------------------------------------------------------------------
+# Seeded initial state: isothermal hydrostatic column (reference src/ESP/esp_initial.cu:507-588)
+# plus uniform temperature noise from SplitMix64, p kept, rho = p / (Rd T).
+# ------------------------------------------------------------------------------------------------
+def splitmix64_uniform(n, seed):
+    """n uniform doubles in [0,1) from SplitMix64 (Steele, Lea & Flood 2014), top 53 bits."""
+    mask = (1 << 64) - 1
+    out = np.empty(n)
+    x = seed & mask
+    for i in range(n):
+        x = (x + 0x9E3779B97F4A7C15) & mask
+        z = x
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & mask
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & mask
+        z = z ^ (z >> 31)
+        out[i] = (z >> 11) * (1.0 / 9007199254740992.0)
+    return out
+
+
+def isothermal_column(Altitude, Altitudeh, c):
+    nv = len(Altitude)
+    p = np.zeros(nv)
+    rho = np.zeros(nv)
+    T = np.zeros(nv)
+    eps, it_max = 1e-15, 100
+    Rd, Tm, g = c["Rd"], c["Tmean"], c["Gravit"]
+    for lev in range(nv):
+        if lev == 0:
+            P_L, rho_L, T_L, dz = c["P_Ref"], c["P_Ref"] / (Rd * Tm), Tm, Altitude[0]
+            l_int = r_int = 0.5
+        else:
+            P_L, rho_L, T_L = p[lev - 1], rho[lev - 1], T[lev - 1]
+            dz = Altitude[lev] - Altitude[lev - 1]
+            l_int = (Altitude[lev] - Altitudeh[lev]) / dz
+            r_int = (Altitudeh[lev] - Altitude[lev - 1]) / dz
+        g_L = g
+        p[lev], rho[lev], T[lev] = P_L, rho_L, T_L
+        ptmp = p[lev] + 2 * eps * p[lev]
+        it = 0
+        while it < it_max and (ptmp - p[lev]) / p[lev] > eps:
+            ptmp = p[lev]
+            f = (p[lev] - P_L) / dz + (g * r_int + g_L * l_int) * (rho[lev] * r_int + rho_L * l_int)
+            df = 1.0 / dz + (g * r_int + g_L * l_int) * r_int / (Rd * T[lev])
+            p[lev] = p[lev] - f / df
+            rho[lev] = p[lev] / (Rd * T[lev])
+            it += 1
+    return p, rho, T
+
+
+def initial_state(grid_arrays, N, nv, c, seed=20260101, amp=0.1):
+    """Reference-layout initial state: dict of Rho, pressure, temperature, Mh, Wh, W, Rd, Cp."""
+    p0, rho0, T0 = isothermal_column(grid_arrays["Altitude"], grid_arrays["Altitudeh"], c)
+    noise = (2.0 * splitmix64_uniform(N * nv, seed) - 1.0) * amp
+    T = np.tile(T0, N) + noise
+    p = np.tile(p0, N)
+    rho = p / (c["Rd"] * T)
+    return dict(Rho=rho, pressure=p, temperature=T, Mh=np.zeros(3 * N * nv),
+                Wh=np.zeros(N * (nv + 1)), W=np.zeros(N * nv), Rd=np.full(N * nv, c["Rd"]),
+                Cp=np.full(N * nv, c["Cp"]))
+
+
+# ------------------------------------------------------------------------------------------------
+# The CPU restatement (oracle)
+# ------------------------------------------------------------------------------------------------
+class OracleGrid(ctypes.Structure):
+    _fields_ = [("point_num", ctypes.c_int), ("nv", ctypes.c_int), ("nl_region", ctypes.c_int),
+                ("nr", ctypes.c_int), ("maps", ctypes.c_void_p), ("point_local", ctypes.c_void_p),
+                ("Altitude", ctypes.c_void_p), ("Altitudeh", ctypes.c_void_p),
+                ("lonlat", ctypes.c_void_p), ("areas", ctypes.c_void_p),
+                ("areasTr", ctypes.c_void_p), ("nvecoa", ctypes.c_void_p),
+                ("nvecti", ctypes.c_void_p), ("nvecte", ctypes.c_void_p),
+                ("div", ctypes.c_void_p), ("grad", ctypes.c_void_p), ("func_r", ctypes.c_void_p)]
+
+
+_oracle = None
+
+
+def oracle_lib():
+    global _oracle
+    if _oracle is None:
+        lib = ctypes.CDLL(ORACLE_SO)
+        lib.oracle_new.restype = ctypes.c_void_p
+        lib.oracle_new.argtypes = [ctypes.POINTER(OracleGrid), ctypes.POINTER(Params)]
+        lib.oracle_set.restype = ctypes.c_long
+        lib.oracle_set.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p]
+        lib.oracle_get.restype = ctypes.c_long
+        lib.oracle_get.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p]
+        lib.oracle_step.restype = ctypes.c_int
+        lib.oracle_step.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        lib.oracle_set_threads.argtypes = [ctypes.c_int]
+        lib.oracle_free.argtypes = [ctypes.c_void_p]
+        _oracle = lib
+    return _oracle
+
+
+class Oracle:
+    def __init__(self, grid, params):
+        """grid: object with point_num, nv, nl_region, nr and reference-layout arrays."""
+        lib = oracle_lib()
+        self._keep = {k: np.ascontiguousarray(grid[k]) for k in
+                      ["maps", "point_local", "Altitude", "Altitudeh", "lonlat", "areas",
+                       "areasTr", "nvecoa", "nvecti", "nvecte", "div", "grad", "func_r"]}
+        g = OracleGrid(grid.point_num, grid.nv, grid.nl_region, grid.nr,
+                       *[self._keep[k].ctypes.data for k in
+                         ["maps", "point_local", "Altitude", "Altitudeh", "lonlat", "areas",
+                          "areasTr", "nvecoa", "nvecti", "nvecte", "div", "grad", "func_r"]])
+        self.h = lib.oracle_new(ctypes.byref(g), ctypes.byref(params))
+
+    def set(self, name, a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        n = oracle_lib().oracle_set(self.h, name.encode(), a.ctypes.data)
+        assert n == a.size, (name, n, a.size)
+
+    def get(self, name):
+        n = oracle_lib().oracle_get(self.h, name.encode(), None)
+        assert n >= 0, name
+        a = np.zeros(n)
+        oracle_lib().oracle_get(self.h, name.encode(), a.ctypes.data)
+        return a
+
+    def step(self, n=1, profx=True, thor=True):
+        assert oracle_lib().oracle_step(self.h, n, int(profx), int(thor)) == 0
+
+    def close(self):
+        if self.h:
+            oracle_lib().oracle_free(self.h)
+            self.h = None
+
+
+class RefSim:
+    """The reference's own FP64 CUDA kernels driven by oracle/ref_harness.cu (needs a GPU)."""
+
+    def __init__(self, refgrid, params, nofma=False):
+        self.lib = ref_lib(nofma)
+        self.h = self.lib.ref_sim_new(refgrid.h, ctypes.byref(params))
+        assert self.h, "ref_sim_new failed"
+
+    def set(self, name, a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        n = self.lib.ref_sim_set(self.h, name.encode(), a.ctypes.data)
+        assert n == a.size, (name, n, a.size)
+
+    def get(self, name):
+        n = self.lib.ref_sim_get(self.h, name.encode(), None)
+        assert n >= 0, name
+        a = np.zeros(n)
+        assert self.lib.ref_sim_get(self.h, name.encode(), a.ctypes.data) == n
+        return a
+
+    def step(self, n=1, profx=True, thor=True):
+        assert self.lib.ref_sim_step(self.h, n, int(profx), int(thor)) == 0
+
+    def time(self, n):
+        return self.lib.ref_sim_time(self.h, n)
+
+    def close(self):
+        if self.h:
+            self.lib.ref_sim_free(self.h)
+            self.h = None
+
+
+def rel_err(a, b):
+    """max|a-b| / max|b| (b the reference), 0 when both vanish."""
+    den = np.max(np.abs(b))
+    num = np.max(np.abs(a - b))
+    if den == 0.0:
+        return float(num)
+    return float(num / den)
+
+
+STATE_FIELDS = ["Rho", "pressure", "Mh", "Wh", "W"]
+
+
+# ------------------------------------------------------------------------------------------------
+# Product handles
+# ------------------------------------------------------------------------------------------------
+def thorx_params(c, timestep, precision=0):
+    """thorx_params dict from a configuration dict as returned by make_params."""
+    return dict(A=c["A"], Omega=c["Omega"], Gravit=c["Gravit"], Rd=c["Rd"], Cp=c["Cp"],
+                P_Ref=c["P_Ref"], Top_altitude=c["Top_altitude"], timestep=timestep,
+                Diffc=c["Diffc"], DivDampc=c["DivDampc"], HyDiffOrder=c["HyDiffOrder"],
+                DeepModel=c["DeepModel"], NonHydro=c["NonHydro"],
+                GravHeightVar=c["GravHeightVar"], HyDiff=c["HyDiff"], DivDampP=c["DivDampP"],
+                thermo_equation=c["energy_equation"], core_benchmark=c["held_suarez"],
+                precision=precision)
+
+
+def grid_dict(g):
+    d = dict(point_num=g.point_num, nv=g.nv, nl_region=g.nl_region, nr=g.nr)
+    d.update(g.arrays)
+    return d
+
+
+def field_tolerance(spread, floor=1e-12, factor=4.0):
+    """Tolerance of a field: 1e-12, or `factor` x the reference's own FMA / no-FMA spread where
+    cancellation makes the reference itself that uncertain."""
+    return max(floor, factor * spread)

@@ -1,0 +1,164 @@
+"""thor_b200: Python handle on the thorx C ABI (include/thorx.h, thor_b200/libthorx.so).
+
+The compute path is the CUDA library; this module only marshals host arrays in the reference
+THOR layouts across the C ABI. There is no CPU fallback: importing works without a GPU, but
+creating a context needs the library and a CUDA device and raises otherwise.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libthorx.so")
+
+FP64, MIXED = 0, 1
+ENTROPY, ENERGY = 0, 1
+NO_BENCHMARK, HELD_SUAREZ = 0, 1
+
+ERRORS = {-1: "THORX_E_ARG", -2: "THORX_E_CUDA", -3: "THORX_E_NAN", -4: "THORX_E_UNSUPPORTED",
+          -5: "THORX_E_STATE"}
+
+
+class ThorxError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s (%d): %s" % (ERRORS.get(code, "?"), code, msg))
+        self.code = code
+
+
+class GridC(ctypes.Structure):
+    _fields_ = [("point_num", ctypes.c_int), ("nv", ctypes.c_int), ("nl_region", ctypes.c_int),
+                ("nr", ctypes.c_int), ("glevel", ctypes.c_int)] + [
+        (n, ctypes.c_void_p) for n in
+        ["maps", "point_local", "Altitude", "Altitudeh", "lonlat", "areas", "areasTr", "areasT",
+         "nvecoa", "nvecti", "nvecte", "div", "grad", "func_r"]]
+
+
+class ParamsC(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in
+                ["A", "Omega", "Gravit", "Rd", "Cp", "P_Ref", "Top_altitude", "timestep", "Diffc",
+                 "DivDampc"]] + [
+        (n, ctypes.c_int) for n in
+        ["HyDiffOrder", "DeepModel", "NonHydro", "GravHeightVar", "HyDiff", "DivDampP",
+         "thermo_equation", "core_benchmark", "precision"]]
+
+
+_lib = None
+
+
+def lib():
+    """The loaded libthorx.so; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("thor_b200/libthorx.so is missing: run `python -m thor_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, cp, ci = ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int
+        L.thorx_create.argtypes = [ctypes.POINTER(GridC), ctypes.POINTER(ParamsC), vp,
+                                   ctypes.POINTER(vp)]
+        L.thorx_create.restype = ci
+        L.thorx_destroy.argtypes = [vp]
+        L.thorx_last_error.argtypes = [vp]
+        L.thorx_last_error.restype = cp
+        L.thorx_field_size.argtypes = [vp, cp]
+        L.thorx_field_size.restype = ctypes.c_long
+        for f in ("thorx_set_field", "thorx_get_field"):
+            getattr(L, f).argtypes = [vp, cp, vp]
+            getattr(L, f).restype = ci
+        for f in ("thorx_profx", "thorx_thor", "thorx_sync"):
+            getattr(L, f).argtypes = [vp]
+            getattr(L, f).restype = ci
+        L.thorx_step.argtypes = [vp, ci]
+        L.thorx_step.restype = ci
+        L.thorx_kernels_per_step.argtypes = [vp]
+        L.thorx_kernels_per_step.restype = ci
+        _lib = L
+    return _lib
+
+
+EXPORTED = ["thorx_create", "thorx_destroy", "thorx_last_error", "thorx_field_size",
+            "thorx_set_field", "thorx_get_field", "thorx_profx", "thorx_thor", "thorx_step",
+            "thorx_sync", "thorx_kernels_per_step"]
+
+GRID_KEYS = ["maps", "point_local", "Altitude", "Altitudeh", "lonlat", "areas", "areasTr",
+             "areasT", "nvecoa", "nvecti", "nvecte", "div", "grad", "func_r"]
+
+
+class Thorx:
+    """One simulation context (thorx_create .. thorx_destroy)."""
+
+    def __init__(self, grid, glevel, params, stream=None):
+        """grid: mapping with point_num, nv, nl_region, nr and the reference-layout arrays;
+        params: dict of thorx_params fields."""
+        L = lib()
+        keep = {}
+        g = GridC(int(grid["point_num"]), int(grid["nv"]), int(grid["nl_region"]),
+                  int(grid["nr"]), int(glevel))
+        for k in GRID_KEYS:
+            dt = np.int32 if k in ("maps", "point_local") else np.float64
+            a = np.ascontiguousarray(grid[k], dtype=dt)
+            keep[k] = a
+            setattr(g, k, a.ctypes.data)
+        p = ParamsC()
+        for name, _ in ParamsC._fields_:
+            setattr(p, name, params[name])
+        h = ctypes.c_void_p()
+        rc = L.thorx_create(ctypes.byref(g), ctypes.byref(p), stream, ctypes.byref(h))
+        self.h = h.value
+        if rc != 0:
+            msg = L.thorx_last_error(self.h).decode() if self.h else ""
+            if self.h:
+                L.thorx_destroy(self.h)
+                self.h = None
+            raise ThorxError(rc, msg)
+        self.N = int(grid["point_num"])
+        self.nv = int(grid["nv"])
+
+    def _check(self, rc):
+        if rc != 0:
+            raise ThorxError(rc, lib().thorx_last_error(self.h).decode())
+
+    def size(self, name):
+        return lib().thorx_field_size(self.h, name.encode())
+
+    def set(self, name, a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        n = self.size(name)
+        if n != a.size:
+            raise ValueError("%s: expected %d values, got %d" % (name, n, a.size))
+        self._check(lib().thorx_set_field(self.h, name.encode(), a.ctypes.data))
+
+    def get(self, name, out=None):
+        n = self.size(name)
+        if n < 0:
+            raise KeyError(name)
+        if out is None:
+            out = np.empty(n)
+        self._check(lib().thorx_get_field(self.h, name.encode(), out.ctypes.data))
+        return out
+
+    def profx(self):
+        self._check(lib().thorx_profx(self.h))
+
+    def thor(self):
+        self._check(lib().thorx_thor(self.h))
+
+    def step(self, n=1):
+        self._check(lib().thorx_step(self.h, n))
+
+    def sync(self):
+        self._check(lib().thorx_sync(self.h))
+
+    def kernels_per_step(self):
+        return lib().thorx_kernels_per_step(self.h)
+
+    def close(self):
+        if self.h:
+            lib().thorx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

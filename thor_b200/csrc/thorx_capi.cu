@@ -1,0 +1,552 @@
+// thorx C ABI: context creation, layout conversion, and the ProfX / Thor launch sequence.
+//
+// The large step reproduces the stage structure of ESP::Thor (src/ESP/thor_driver.cu:70-1466):
+// three RK stages with 1 / 3 / 6 forward-backward small steps of dt/3, dt/6, dt/6. Per stage:
+//   adv_temp                  Compute_Advec_Cori1/_Poles/2 + Compute_Temperature_H_Pt_Geff
+//   diffusion x (order/2)     Diffusion_Op/_Poles (+ Correct_Horizontal on the last pass)
+//   divm0                     DivM_Op/_Poles pass 0 on (Mhk, Whk)
+//   slow_modes                DivM pass 1 + Compute_Slow_Modes/_Poles (+ UpdateRK, stages 2,3)
+//   per small step:
+//     divm0                   DivM pass 0 on (Mhs, Whs)
+//     momentum                DivM pass 1 + Momentum_Eq/_Poles
+//     vertical                Prepare_Implicit_Vertical + Vertical_Eq + Density_Pressure_Eqs
+//   update_rk2                UpdateRK2
+// with no host synchronisation inside a step; thorx_step replays the whole step as a CUDA graph.
+
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/thorx.h"
+#include "thorx_internal.h"
+
+using namespace thorx;
+
+struct FieldDesc {
+    double** dev; // address of the device pointer in State
+    int      L;   // levels (nv or nv+1)
+    int      K;   // components (1 or 3)
+};
+
+struct thorx_ctx {
+    Geometry     g{};
+    Phys         P{};
+    State        s{};
+    cudaStream_t stream     = nullptr;
+    bool         own_stream = false;
+    int          glevel     = 0;
+    int          hydiff_order = 4;
+    // device allocations
+    std::vector<void*>               allocs;
+    std::map<std::string, FieldDesc> fields;
+    double*                          staging     = nullptr; // layout conversion buffer
+    size_t                           staging_len = 0;       // doubles
+    unsigned int*                    flags_host  = nullptr; // pinned
+    cudaGraphExec_t                  graph_exec  = nullptr;
+    cudaGraph_t                      graph       = nullptr;
+    std::string                      err;
+    bool                             state_set = false;
+};
+
+namespace {
+
+int fail(thorx_ctx* c, int code, const std::string& msg) {
+    if (c)
+        c->err = msg;
+    return code;
+}
+
+#define CK(call)                                                                                  \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess)                                                                    \
+            return fail(ctx, THORX_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));  \
+    } while (0)
+
+template<class T> int dev_alloc(thorx_ctx* ctx, T** p, size_t n) {
+    void* d = nullptr;
+    CK(cudaMalloc(&d, n * sizeof(T)));
+    CK(cudaMemset(d, 0, n * sizeof(T)));
+    ctx->allocs.push_back(d);
+    *p = (T*)d;
+    return 0;
+}
+
+// ref layout [N][L][K] <-> device layout [K][L][Np], through 32x32 shared-memory tiles of the
+// matrix view ref = [N rows][L*K columns].
+__global__ void ref_to_dev_kernel(const double* __restrict__ ref, double* __restrict__ dev, int N,
+                                  int Np, int L, int K) {
+    __shared__ double tile[32][33];
+    const int         Q  = L * K;
+    const int         c0 = blockIdx.x * 32, q0 = blockIdx.y * 32;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        int col = c0 + r, q = q0 + threadIdx.x;
+        tile[r][threadIdx.x] = (col < N && q < Q) ? ref[(size_t)col * Q + q] : 0.0;
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        int q = q0 + r, col = c0 + threadIdx.x;
+        if (q < Q && col < N) {
+            int l = q / K, k = q % K;
+            dev[((size_t)k * L + l) * Np + col] = tile[threadIdx.x][r];
+        }
+    }
+}
+
+__global__ void dev_to_ref_kernel(const double* __restrict__ dev, double* __restrict__ ref, int N,
+                                  int Np, int L, int K) {
+    __shared__ double tile[32][33];
+    const int         Q  = L * K;
+    const int         c0 = blockIdx.x * 32, q0 = blockIdx.y * 32;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        int q = q0 + r, col = c0 + threadIdx.x;
+        if (q < Q && col < N) {
+            int l = q / K, k = q % K;
+            tile[r][threadIdx.x] = dev[((size_t)k * L + l) * Np + col];
+        }
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        int col = c0 + r, q = q0 + threadIdx.x;
+        if (col < N && q < Q)
+            ref[(size_t)col * Q + q] = tile[threadIdx.x][r];
+    }
+}
+
+// Upload a reference-layout geometry array [N][J] to the device layout [J][Np].
+int upload_geo(thorx_ctx* ctx, const double* host, int J, const double** out) {
+    const int N = ctx->g.N, Np = ctx->g.Np;
+    std::vector<double> t((size_t)J * Np, 0.0);
+    for (int c = 0; c < N; c++)
+        for (int j = 0; j < J; j++)
+            t[(size_t)j * Np + c] = host[(size_t)c * J + j];
+    double* d;
+    if (dev_alloc(ctx, &d, t.size()))
+        return THORX_E_CUDA;
+    CK(cudaMemcpy(d, t.data(), t.size() * sizeof(double), cudaMemcpyHostToDevice));
+    *out = d;
+    return 0;
+}
+
+// Neighbour tables from the rhombus maps (halo tile of src/headers/kernel_halo_helpers.h:47-128)
+// and, for the two poles, point_local (the *_Poles kernels' neighbour lists).
+int build_neighbours(thorx_ctx* ctx, const thorx_grid* gr) {
+    const int N = gr->point_num, Np = ctx->g.Np, nl = gr->nl_region, nhl = nl + 2,
+              nhl2 = nhl * nhl;
+    std::vector<int>     nb((size_t)6 * Np, -1), ring((size_t)6 * Np, -1);
+    std::vector<uint8_t> flag(Np, 0);
+    std::vector<char>    seen(N, 0);
+    for (int r = 0; r < gr->nr; r++) {
+        const int* m = gr->maps + (size_t)r * nhl2;
+        for (int y = 0; y < nl; y++)
+            for (int x = 0; x < nl; x++) {
+                const int id = m[(y + 1) * nhl + x + 1];
+                if (id < 0 || id >= N - 2 || seen[id])
+                    return fail(ctx, THORX_E_ARG, "maps: bad or repeated interior index");
+                seen[id]      = 1;
+                const bool pe = (x == 0 && y == 0 && m[0] == -1);
+                const int  N0 = m[(y + 2) * nhl + x + 1], N1 = m[(y + 2) * nhl + x + 2],
+                          N2 = m[(y + 1) * nhl + x + 2], N3 = m[y * nhl + x + 1],
+                          N4 = m[y * nhl + x], N5 = m[(y + 1) * nhl + x];
+                const int p[6] = {N0, N1, N2, N3, pe ? N5 : N4, N5};
+                for (int j = 0; j < 6; j++) {
+                    if (p[j] >= N)
+                        return fail(ctx, THORX_E_ARG, "maps: neighbour index out of range");
+                    nb[(size_t)j * Np + id] = p[j];
+                }
+                const int rg[6] = {N0, N1, N2, N3, pe ? N5 : N4, pe ? -1 : N5};
+                for (int j = 0; j < 6; j++)
+                    ring[(size_t)j * Np + id] = rg[j];
+                flag[id] = pe ? kRing5 : 0;
+            }
+    }
+    for (int id = N - 2; id < N; id++) {
+        for (int i = 0; i < 5; i++) {
+            int v = gr->point_local[(size_t)id * 6 + i];
+            if (v < 0 || v >= N)
+                return fail(ctx, THORX_E_ARG, "point_local: bad pole neighbour");
+            nb[(size_t)i * Np + id]   = v;
+            ring[(size_t)i * Np + id] = v;
+        }
+        nb[(size_t)5 * Np + id] = -1;
+        flag[id]                = kPole | kRing5;
+        seen[id]                = 1;
+    }
+    for (int id = 0; id < N; id++)
+        if (!seen[id])
+            return fail(ctx, THORX_E_ARG, "maps do not cover every column");
+    int*     d_nb;
+    int*     d_ring;
+    uint8_t* d_flag;
+    if (dev_alloc(ctx, &d_nb, nb.size()) || dev_alloc(ctx, &d_ring, ring.size())
+        || dev_alloc(ctx, &d_flag, flag.size()))
+        return THORX_E_CUDA;
+    CK(cudaMemcpy(d_nb, nb.data(), nb.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_ring, ring.data(), ring.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_flag, flag.data(), flag.size(), cudaMemcpyHostToDevice));
+    ctx->g.nb    = d_nb;
+    ctx->g.ring  = d_ring;
+    ctx->g.cflag = d_flag;
+    return 0;
+}
+
+int check_flags(thorx_ctx* ctx) {
+    CK(cudaMemcpyAsync(ctx->flags_host, ctx->s.flags, sizeof(unsigned int),
+                       cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    unsigned int f = *ctx->flags_host;
+    if (f & kFlagNaN) {
+        CK(cudaMemsetAsync(ctx->s.flags, 0, sizeof(unsigned int), ctx->stream));
+        return fail(ctx, THORX_E_NAN, "NaN in temperature after the physics step");
+    }
+    return 0;
+}
+
+// ESP::ProfX
+int enqueue_profx(thorx_ctx* ctx) {
+    CK(cudaMemsetAsync(ctx->s.Qheat, 0, sizeof(double) * ctx->g.nv * ctx->g.Np, ctx->stream));
+    launch_profx(ctx->g, ctx->P, ctx->s, ctx->stream);
+    CK(cudaGetLastError());
+    return 0;
+}
+
+// ESP::Thor
+int enqueue_thor(thorx_ctx* ctx) {
+    const Geometry& g  = ctx->g;
+    const Phys&     P  = ctx->P;
+    State&          s  = ctx->s;
+    cudaStream_t    st = ctx->stream;
+    const size_t    cell = (size_t)g.nv * g.Np * sizeof(double), iface = (size_t)g.nvi * g.Np * sizeof(double);
+    CK(cudaMemcpyAsync(s.Mhk, s.Mh, 3 * cell, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(s.Whk, s.Wh, iface, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(s.Wk, s.W, cell, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(s.Rhok, s.Rho, cell, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(s.pk, s.p, cell, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemsetAsync(s.Mhs, 0, 3 * cell, st));
+    CK(cudaMemsetAsync(s.Rhos, 0, cell, st));
+    CK(cudaMemsetAsync(s.Whs, 0, iface, st));
+    CK(cudaMemsetAsync(s.ps, 0, cell, st));
+    for (int rk = 0; rk < 3; rk++) {
+        const int    ns_it = (rk == 0) ? 1 : (rk == 1 ? 3 : 6);
+        const double times = (rk == 0) ? P.timestep / 3.0 : P.timestep / 6.0;
+        launch_adv_temp(g, P, s, st);
+        if (P.HyDiff) {
+            int passes = P.HyDiffOrder / 2;
+            for (int i = 0; i < passes; i++)
+                launch_diffusion(g, P, s, i, i == passes - 1, st);
+        }
+        if (P.DivDampP)
+            launch_divm0(g, P, s, false, st);
+        launch_slow_modes(g, P, s, rk > 0, st);
+        for (int ns = 0; ns < ns_it; ns++) {
+            if (P.DivDampP)
+                launch_divm0(g, P, s, true, st);
+            launch_momentum(g, P, s, times, st);
+            launch_vertical(g, P, s, times, st);
+        }
+        launch_update_rk2(g, P, s, st);
+    }
+    CK(cudaMemcpyAsync(s.Mh, s.Mhk, 3 * cell, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(s.Wh, s.Whk, iface, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(s.W, s.Wk, cell, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(s.Rho, s.Rhok, cell, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(s.p, s.pk, cell, cudaMemcpyDeviceToDevice, st));
+    CK(cudaGetLastError());
+    return 0;
+}
+
+} // namespace
+
+extern "C" {
+
+int thorx_create(const thorx_grid* gr, const thorx_params* pr, void* stream, thorx_ctx** out) {
+    if (!out)
+        return THORX_E_ARG;
+    *out          = nullptr;
+    thorx_ctx* ctx = new thorx_ctx;
+    if (!gr || !pr || !gr->maps || !gr->point_local || !gr->Altitude || !gr->Altitudeh
+        || !gr->lonlat || !gr->areas || !gr->areasTr || !gr->nvecoa || !gr->nvecti || !gr->nvecte
+        || !gr->div || !gr->grad || !gr->func_r) {
+        *out = ctx;
+        return fail(ctx, THORX_E_ARG, "thorx_create: null grid or params pointer");
+    }
+    *out = ctx;
+    const int N = gr->point_num, nv = gr->nv;
+    if (N < 12 || nv < 3 || gr->nl_region < 2 || gr->nr < 1
+        || (long)gr->nr * gr->nl_region * gr->nl_region != N - 2)
+        return fail(ctx, THORX_E_ARG, "thorx_create: inconsistent grid sizes");
+    if (pr->HyDiffOrder < 2 || pr->HyDiffOrder % 2)
+        return fail(ctx, THORX_E_UNSUPPORTED, "HyDiffOrder must be even and >= 2");
+    if (pr->precision != THORX_FP64)
+        return fail(ctx, THORX_E_UNSUPPORTED, "precision: this build runs THORX_FP64 only");
+    if (pr->thermo_equation != THORX_ENTROPY && pr->thermo_equation != THORX_ENERGY)
+        return fail(ctx, THORX_E_ARG, "thermo_equation");
+    if (pr->core_benchmark != THORX_NO_BENCHMARK && pr->core_benchmark != THORX_HELD_SUAREZ)
+        return fail(ctx, THORX_E_UNSUPPORTED, "core_benchmark");
+    if (pr->timestep <= 0 || pr->A <= 0)
+        return fail(ctx, THORX_E_ARG, "timestep and radius must be positive");
+
+    if (stream) {
+        ctx->stream = (cudaStream_t)stream;
+    }
+    else {
+        CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+        ctx->own_stream = true;
+    }
+    ctx->glevel       = gr->glevel;
+    Geometry& g       = ctx->g;
+    g.N               = N;
+    g.Np              = (N + kColAlign - 1) / kColAlign * kColAlign;
+    g.nv              = nv;
+    g.nvi             = nv + 1;
+    const int Np      = g.Np;
+    Phys& P           = ctx->P;
+    P.A               = pr->A;
+    P.Omega           = pr->Omega;
+    P.Gravit          = pr->Gravit;
+    P.Rd              = pr->Rd;
+    P.Cp              = pr->Cp;
+    P.P_Ref           = pr->P_Ref;
+    P.timestep        = pr->timestep;
+    P.HyDiffOrder     = pr->HyDiffOrder;
+    P.DeepModel       = pr->DeepModel != 0;
+    P.NonHydro        = pr->NonHydro != 0;
+    P.GravHeightVar   = pr->GravHeightVar != 0;
+    P.HyDiff          = pr->HyDiff != 0;
+    P.DivDampP        = pr->DivDampP != 0;
+    P.energy          = pr->thermo_equation == THORX_ENERGY;
+    P.held_suarez     = pr->core_benchmark == THORX_HELD_SUAREZ;
+
+    int rc;
+    if ((rc = build_neighbours(ctx, gr)))
+        return rc;
+    if ((rc = upload_geo(ctx, gr->div, 21, &g.div)) || (rc = upload_geo(ctx, gr->grad, 21, &g.grad))
+        || (rc = upload_geo(ctx, gr->areas, 18, &g.areas))
+        || (rc = upload_geo(ctx, gr->areasTr, 6, &g.areasTr))
+        || (rc = upload_geo(ctx, gr->nvecoa, 18, &g.nvecoa))
+        || (rc = upload_geo(ctx, gr->nvecti, 18, &g.nvecti))
+        || (rc = upload_geo(ctx, gr->nvecte, 18, &g.nvecte))
+        || (rc = upload_geo(ctx, gr->func_r, 3, &g.func_r)))
+        return rc;
+    {
+        std::vector<double> lat(Np, 0.0);
+        for (int c = 0; c < N; c++)
+            lat[c] = gr->lonlat[2 * c + 1];
+        double* d;
+        if (dev_alloc(ctx, &d, Np))
+            return THORX_E_CUDA;
+        CK(cudaMemcpy(d, lat.data(), Np * sizeof(double), cudaMemcpyHostToDevice));
+        g.lat = d;
+    }
+    {
+        // hyperdiffusion and divergence damping strengths (src/ESP/esp_initial.cu:1292-1335,
+        // without the diffusive sponge)
+        std::vector<double> kdh4(nv), kdhz(nv);
+        for (int lev = 0; lev < nv; lev++) {
+            double dbar = sqrt(2 * M_PI / 5) * P.A / (pow(2, gr->glevel));
+            kdh4[lev]   = (pr->Diffc) * pow(dbar, 1.0 * pr->HyDiffOrder) / P.timestep;
+            kdhz[lev]   = (pr->DivDampc) * pow(dbar, 4.) / P.timestep;
+        }
+        double *a, *b, *alt, *alth;
+        if (dev_alloc(ctx, &a, nv) || dev_alloc(ctx, &b, nv) || dev_alloc(ctx, &alt, nv)
+            || dev_alloc(ctx, &alth, nv + 1))
+            return THORX_E_CUDA;
+        CK(cudaMemcpy(a, kdh4.data(), nv * 8, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(b, kdhz.data(), nv * 8, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(alt, gr->Altitude, nv * 8, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(alth, gr->Altitudeh, (nv + 1) * 8, cudaMemcpyHostToDevice));
+        g.Kdh4      = a;
+        g.Kdhz      = b;
+        g.Altitude  = alt;
+        g.Altitudeh = alth;
+    }
+
+    // state
+    State&       s     = ctx->s;
+    const size_t cell  = (size_t)nv * Np, iface = (size_t)(nv + 1) * Np;
+    struct A {
+        double** p;
+        size_t   n;
+    } al[] = {{&s.Mh, 3 * cell},    {&s.Mhk, 3 * cell},  {&s.Mhs, 3 * cell},   {&s.Rho, cell},
+              {&s.Rhok, cell},      {&s.Rhos, cell},     {&s.p, cell},         {&s.pk, cell},
+              {&s.ps, cell},        {&s.Wh, iface},      {&s.Whk, iface},      {&s.Whs, iface},
+              {&s.W, cell},         {&s.Wk, cell},       {&s.T, cell},         {&s.Rd, cell},
+              {&s.Cp, cell},        {&s.h, cell},        {&s.hh, iface},       {&s.pt, cell},
+              {&s.pth, iface},      {&s.gtil, cell},     {&s.gtilh, iface},    {&s.Adv, 3 * cell},
+              {&s.diff, 12 * cell}, {&s.diffmh, 3 * cell}, {&s.diffw, cell},   {&s.diffrh, cell},
+              {&s.diffpr, cell},    {&s.divg, 3 * cell}, {&s.SlowMh, 3 * cell}, {&s.SlowWh, iface},
+              {&s.SlowRho, cell},   {&s.Slowp, cell},    {&s.Qheat, cell},     {&s.dMh, 3 * cell},
+              {&s.dWh, iface}};
+    for (auto& x : al)
+        if (dev_alloc(ctx, x.p, x.n))
+            return THORX_E_CUDA;
+    if (P.energy) {
+        if (dev_alloc(ctx, &s.ep, cell) || dev_alloc(ctx, &s.eph, iface)
+            || dev_alloc(ctx, &s.ek, cell) || dev_alloc(ctx, &s.ekh, iface)
+            || dev_alloc(ctx, &s.Etotal, cell))
+            return THORX_E_CUDA;
+    }
+    if (dev_alloc(ctx, &s.flags, 1))
+        return THORX_E_CUDA;
+    CK(cudaMallocHost(&ctx->flags_host, sizeof(unsigned int)));
+    ctx->staging_len = (size_t)N * (nv + 1) * 3;
+    if (dev_alloc(ctx, &ctx->staging, ctx->staging_len))
+        return THORX_E_CUDA;
+
+    auto& F          = ctx->fields;
+    F["Rho"]         = {&s.Rho, nv, 1};
+    F["pressure"]    = {&s.p, nv, 1};
+    F["Mh"]          = {&s.Mh, nv, 3};
+    F["Wh"]          = {&s.Wh, nv + 1, 1};
+    F["W"]           = {&s.W, nv, 1};
+    F["temperature"] = {&s.T, nv, 1};
+    F["Rd"]          = {&s.Rd, nv, 1};
+    F["Cp"]          = {&s.Cp, nv, 1};
+    F["profx_Qheat"] = {&s.Qheat, nv, 1};
+    F["SlowMh"]      = {&s.SlowMh, nv, 3};
+    F["SlowWh"]      = {&s.SlowWh, nv + 1, 1};
+    F["SlowRho"]     = {&s.SlowRho, nv, 1};
+    F["Slowpressure"] = {&s.Slowp, nv, 1};
+    F["h"]           = {&s.h, nv, 1};
+    F["hh"]          = {&s.hh, nv + 1, 1};
+    F["pt"]          = {&s.pt, nv, 1};
+    F["pth"]         = {&s.pth, nv + 1, 1};
+    F["gtil"]        = {&s.gtil, nv, 1};
+    F["gtilh"]       = {&s.gtilh, nv + 1, 1};
+    F["Adv"]         = {&s.Adv, nv, 3};
+    F["diffmh"]      = {&s.diffmh, nv, 3};
+    F["diffw"]       = {&s.diffw, nv, 1};
+    F["diffrh"]      = {&s.diffrh, nv, 1};
+    F["diffpr"]      = {&s.diffpr, nv, 1};
+    CK(cudaDeviceSynchronize());
+    return 0;
+}
+
+void thorx_destroy(thorx_ctx* ctx) {
+    if (!ctx)
+        return;
+    if (ctx->graph_exec)
+        cudaGraphExecDestroy(ctx->graph_exec);
+    if (ctx->graph)
+        cudaGraphDestroy(ctx->graph);
+    if (ctx->stream)
+        cudaStreamSynchronize(ctx->stream);
+    for (void* p : ctx->allocs)
+        cudaFree(p);
+    if (ctx->flags_host)
+        cudaFreeHost(ctx->flags_host);
+    if (ctx->own_stream && ctx->stream)
+        cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char* thorx_last_error(const thorx_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+long thorx_field_size(const thorx_ctx* ctx, const char* name) {
+    if (!ctx || !name)
+        return THORX_E_ARG;
+    auto it = ctx->fields.find(name);
+    if (it == ctx->fields.end())
+        return THORX_E_ARG;
+    return (long)ctx->g.N * it->second.L * it->second.K;
+}
+
+int thorx_set_field(thorx_ctx* ctx, const char* name, const double* host) {
+    if (!ctx)
+        return THORX_E_ARG;
+    if (!name || !host)
+        return fail(ctx, THORX_E_ARG, "thorx_set_field: null argument");
+    auto it = ctx->fields.find(name);
+    if (it == ctx->fields.end())
+        return fail(ctx, THORX_E_ARG, std::string("thorx_set_field: unknown field ") + name);
+    const FieldDesc& f = it->second;
+    const size_t     n = (size_t)ctx->g.N * f.L * f.K;
+    CK(cudaMemcpyAsync(ctx->staging, host, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    dim3 grid((ctx->g.N + 31) / 32, (f.L * f.K + 31) / 32), block(32, 8);
+    ref_to_dev_kernel<<<grid, block, 0, ctx->stream>>>(ctx->staging, *f.dev, ctx->g.N, ctx->g.Np,
+                                                      f.L, f.K);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->state_set = true;
+    return 0;
+}
+
+int thorx_get_field(thorx_ctx* ctx, const char* name, double* host) {
+    if (!ctx)
+        return THORX_E_ARG;
+    if (!name || !host)
+        return fail(ctx, THORX_E_ARG, "thorx_get_field: null argument");
+    auto it = ctx->fields.find(name);
+    if (it == ctx->fields.end())
+        return fail(ctx, THORX_E_ARG, std::string("thorx_get_field: unknown field ") + name);
+    const FieldDesc& f = it->second;
+    const size_t     n = (size_t)ctx->g.N * f.L * f.K;
+    dim3 grid((ctx->g.N + 31) / 32, (f.L * f.K + 31) / 32), block(32, 8);
+    dev_to_ref_kernel<<<grid, block, 0, ctx->stream>>>(*f.dev, ctx->staging, ctx->g.N, ctx->g.Np,
+                                                      f.L, f.K);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(host, ctx->staging, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+int thorx_profx(thorx_ctx* ctx) {
+    if (!ctx)
+        return THORX_E_ARG;
+    int rc = enqueue_profx(ctx);
+    if (rc)
+        return rc;
+    return check_flags(ctx);
+}
+
+int thorx_thor(thorx_ctx* ctx) {
+    if (!ctx)
+        return THORX_E_ARG;
+    int rc = enqueue_thor(ctx);
+    if (rc)
+        return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+int thorx_step(thorx_ctx* ctx, int nsteps) {
+    if (!ctx || nsteps < 0)
+        return THORX_E_ARG;
+    if (!ctx->graph_exec) {
+        CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        int rc = enqueue_profx(ctx);
+        if (!rc)
+            rc = enqueue_thor(ctx);
+        cudaGraph_t graph = nullptr;
+        cudaError_t e     = cudaStreamEndCapture(ctx->stream, &graph);
+        if (rc)
+            return rc;
+        if (e != cudaSuccess)
+            return fail(ctx, THORX_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+        ctx->graph = graph;
+        CK(cudaGraphInstantiate(&ctx->graph_exec, graph, 0));
+    }
+    for (int i = 0; i < nsteps; i++)
+        CK(cudaGraphLaunch(ctx->graph_exec, ctx->stream));
+    return 0;
+}
+
+int thorx_sync(thorx_ctx* ctx) {
+    if (!ctx)
+        return THORX_E_ARG;
+    return check_flags(ctx);
+}
+
+int thorx_kernels_per_step(const thorx_ctx* ctx) {
+    if (!ctx)
+        return THORX_E_ARG;
+    const int passes = ctx->P.HyDiff ? ctx->P.HyDiffOrder / 2 : 0;
+    const int divm   = ctx->P.DivDampP ? 1 : 0;
+    // profx + 3 x (adv_temp + passes + divm0 + slow_modes + update_rk2) + 10 x (divm0 + 2)
+    return 1 + 3 * (1 + passes + divm + 1 + 1) + 10 * (divm + 2);
+}
+
+} // extern "C"

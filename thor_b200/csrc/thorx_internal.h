@@ -1,0 +1,99 @@
+// Internal definitions of the thorx dynamical core: device layout and kernel argument blocks.
+//
+// Device layout (column-index fastest, one plane per level):
+//   Np            point_num rounded up to a multiple of 32 (planes start on 256-byte boundaries)
+//   cell scalar   x[lev * Np + col]
+//   cell vector   x[(k * nv + lev) * Np + col], k = 0,1,2 (three planes per level)
+//   interface     x[lev * Np + col], lev = 0..nv
+//   div, grad     x[(j * 3 + k) * Np + col], j = 0..6 stencil point (self, pt1..pt6), k = xyz
+//   areas, nvec*  x[(j * 3 + k) * Np + col], j = 0..5 triangle / edge
+//   areasTr       x[j * Np + col]
+//   func_r        x[k * Np + col]
+// Columns keep the reference ordering (rhombus r, row j, column i -> r*nl^2 + j*nl + i; the two
+// poles last), so that a rhombus row of 16 columns is one 128-byte line of a plane.
+//
+// Neighbours are explicit per-column tables built from the rhombus maps
+// (reference src/headers/kernel_halo_helpers.h:47-128) and, for the poles, from point_local:
+//   nb[j * Np + col], j = 0..5  the stencil points pt1..pt6 of the reference kernels
+//                               (tile offsets (x,y+1) (x+1,y+1) (x+1,y) (x,y-1) (x-1,y-1)
+//                               (x-1,y); at a pentagon pt5 -> (x-1,y); -1 = a hole whose
+//                               value is 0, as the reference's zero-filled tile corner)
+//   ring[j * Np + col], j = 0..5 the neighbours in the order the Laplacian and the divergence
+//                               damping walk them (5 entries at pentagons and poles)
+//   cflag[col]                   bit 0: pole, bit 1: five-entry ring
+#pragma once
+
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+namespace thorx {
+
+constexpr int kColAlign = 32;
+
+enum : uint8_t { kPole = 1, kRing5 = 2 };
+
+struct Geometry {
+    int            N, Np, nv, nvi;
+    const int*     nb;
+    const int*     ring;
+    const uint8_t* cflag;
+    const double*  div;
+    const double*  grad;
+    const double*  areas;
+    const double*  areasTr;
+    const double*  nvecoa;
+    const double*  nvecti;
+    const double*  nvecte;
+    const double*  func_r;
+    const double*  lat;
+    const double*  Altitude;
+    const double*  Altitudeh;
+    const double*  Kdh4;
+    const double*  Kdhz;
+};
+
+struct Phys {
+    double A, Omega, Gravit, Rd, Cp, P_Ref, timestep;
+    int    HyDiffOrder;
+    bool   DeepModel, NonHydro, GravHeightVar, HyDiff, DivDampP, energy, held_suarez;
+};
+
+// Prognostic state (start of large step "x", RK stage "xk", small-step deviation "xs"),
+// diagnostics and tendencies. All device pointers in the layout above.
+struct State {
+    double *Mh, *Mhk, *Mhs;       // 3 planes per level
+    double *Rho, *Rhok, *Rhos;
+    double *p, *pk, *ps;
+    double *Wh, *Whk, *Whs;       // interfaces
+    double *W, *Wk;
+    double *T, *Rd, *Cp;
+    double *h, *hh, *pt, *pth, *gtil, *gtilh;
+    double *ep, *eph, *ek, *ekh, *Etotal; // energy equation only
+    double *Adv;                  // 3 planes
+    double *diff;                 // 6 planes (intermediate hyperdiffusion passes)
+    double *diffmh, *diffw, *diffrh, *diffpr;
+    double *divg;                 // 3 planes
+    double *SlowMh, *SlowWh, *SlowRho, *Slowp;
+    double *Qheat, *dMh, *dWh;    // physics-module coupling (profx_Qheat_d, profx_dMh_d, ...)
+    unsigned int* flags;          // device status word (bit 0: NaN in temperature)
+};
+
+enum : unsigned int { kFlagNaN = 1u };
+
+// Kernel launchers (thor_b200/csrc/dyn_fp64.cu).
+void launch_profx(const Geometry& g, const Phys& P, const State& s, cudaStream_t st);
+void launch_adv_temp(const Geometry& g, const Phys& P, const State& s, cudaStream_t st);
+void launch_diffusion(const Geometry& g, const Phys& P, const State& s, int stepnum, bool last,
+                      cudaStream_t st);
+void launch_divm0(const Geometry& g, const Phys& P, const State& s, bool small_step,
+                  cudaStream_t st);
+void launch_slow_modes(const Geometry& g, const Phys& P, const State& s, bool update_rk,
+                       cudaStream_t st);
+void launch_momentum(const Geometry& g, const Phys& P, const State& s, double dt,
+                     cudaStream_t st);
+void launch_vertical(const Geometry& g, const Phys& P, const State& s, double dt,
+                     cudaStream_t st);
+void launch_update_rk2(const Geometry& g, const Phys& P, const State& s, cudaStream_t st);
+
+} // namespace thorx
