@@ -123,6 +123,24 @@ int thorx_sync(thorx_ctx* ctx);
 /* Number of kernels one thorx_step(ctx, 1) launches. */
 int thorx_kernels_per_step(const thorx_ctx* ctx);
 
+/* ---- Icosahedral grid (replaces Icogrid::Icogrid, src/ESP/grid.cu:84-302) ----
+ * Builds THOR's grid on the host: same point order, neighbours, rhombus maps, spring-dynamics
+ * relaxation (beta = spring_beta, when spring_dynamics != 0), control volumes and operators,
+ * uniform vertical levels up to Top_altitude. glevel 4..7. */
+typedef struct thorx_icogrid thorx_icogrid;
+int thorx_grid_build(int glevel, int vlevel, double A, double Top_altitude, int spring_dynamics,
+                     double spring_beta, thorx_icogrid** out);
+int thorx_grid_info(const thorx_icogrid* g, int* point_num, int* nv, int* nl_region, int* nr,
+                    int* spring_iterations);
+/* Copies a named array (the Icogrid member names: "point_xyz", "point_xyzq", "maps",
+ * "point_local", "pent_ind", "Altitude", "Altitudeh", "lonlat", "areas", "areasT", "areasTr",
+ * "nvec", "nvecoa", "nvecti", "nvecte", "div", "grad", "func_r") into `out` (int32 for the
+ * first three integer arrays, double otherwise). Returns the element count; out may be NULL. */
+long thorx_grid_get(const thorx_icogrid* g, const char* name, void* out);
+/* Fills a thorx_grid with pointers into `g` (valid until thorx_grid_free), for thorx_create. */
+int thorx_grid_describe(const thorx_icogrid* g, thorx_grid* out);
+void thorx_grid_free(thorx_icogrid* g);
+
 #ifdef __cplusplus
 }
 #endif

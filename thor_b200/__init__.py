@@ -72,13 +72,59 @@ def lib():
         L.thorx_step.restype = ci
         L.thorx_kernels_per_step.argtypes = [vp]
         L.thorx_kernels_per_step.restype = ci
+        L.thorx_grid_build.argtypes = [ci, ci, ctypes.c_double, ctypes.c_double, ci,
+                                       ctypes.c_double, ctypes.POINTER(vp)]
+        L.thorx_grid_build.restype = ci
+        L.thorx_grid_info.argtypes = [vp] + [ctypes.POINTER(ci)] * 5
+        L.thorx_grid_info.restype = ci
+        L.thorx_grid_get.argtypes = [vp, cp, vp]
+        L.thorx_grid_get.restype = ctypes.c_long
+        L.thorx_grid_free.argtypes = [vp]
         _lib = L
     return _lib
 
 
 EXPORTED = ["thorx_create", "thorx_destroy", "thorx_last_error", "thorx_field_size",
             "thorx_set_field", "thorx_get_field", "thorx_profx", "thorx_thor", "thorx_step",
-            "thorx_sync", "thorx_kernels_per_step"]
+            "thorx_sync", "thorx_kernels_per_step", "thorx_grid_build", "thorx_grid_info",
+            "thorx_grid_get", "thorx_grid_describe", "thorx_grid_free"]
+
+GRID_F64 = ["point_xyz", "point_xyzq", "Altitude", "Altitudeh", "lonlat", "areas", "areasT",
+            "areasTr", "nvec", "nvecoa", "nvecti", "nvecte", "div", "grad", "func_r"]
+GRID_I32 = ["maps", "point_local", "pent_ind"]
+
+
+class Icogrid:
+    """THOR's icosahedral grid built by thorx_grid_build (host code, no GPU needed)."""
+
+    def __init__(self, glevel, nv, A=6.371e6, Top_altitude=36e3, spring=True, beta=1.15):
+        L = lib()
+        h = ctypes.c_void_p()
+        rc = L.thorx_grid_build(glevel, nv, A, Top_altitude, int(spring), beta, ctypes.byref(h))
+        if rc != 0:
+            raise ThorxError(rc, "thorx_grid_build(glevel=%d, nv=%d)" % (glevel, nv))
+        self.h = h.value
+        d = [ctypes.c_int() for _ in range(5)]
+        L.thorx_grid_info(self.h, *[ctypes.byref(x) for x in d])
+        self.point_num, self.nv, self.nl_region, self.nr, self.spring_iterations = [
+            x.value for x in d]
+        self.glevel = glevel
+        self.arrays = {}
+        for name in GRID_F64 + GRID_I32:
+            n = L.thorx_grid_get(self.h, name.encode(), None)
+            a = np.empty(n, dtype=np.int32 if name in GRID_I32 else np.float64)
+            L.thorx_grid_get(self.h, name.encode(), a.ctypes.data)
+            self.arrays[name] = a
+        L.thorx_grid_free(self.h)
+        self.h = None
+
+    def __getitem__(self, k):
+        return self.arrays[k]
+
+    def as_dict(self):
+        d = dict(point_num=self.point_num, nv=self.nv, nl_region=self.nl_region, nr=self.nr)
+        d.update(self.arrays)
+        return d
 
 GRID_KEYS = ["maps", "point_local", "Altitude", "Altitudeh", "lonlat", "areas", "areasTr",
              "areasT", "nvecoa", "nvecti", "nvecte", "div", "grad", "func_r"]

@@ -11,9 +11,13 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libthorx.so")
 
-SOURCES = ["thorx_capi.cu", "dyn_fp64.cu"]
+SOURCES = ["thorx_capi.cu", "dyn_fp64.cu", "icogrid.cpp"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
-              "-Xcompiler", "-fPIC", "-shared", "-I" + os.path.join(ROOT, "include")]
+              "-Xcompiler", "-fPIC,-fopenmp", "-shared", "-lgomp",
+              "-I" + os.path.join(ROOT, "include")]
+# the environment's default host compiler may lack the OpenMP runtime; the system g++ has it
+if os.path.exists("/usr/bin/g++"):
+    NVCC_FLAGS += ["-ccbin", "/usr/bin/g++"]
 
 
 def sources():
