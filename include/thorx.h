@@ -108,6 +108,13 @@ long thorx_field_size(const thorx_ctx* ctx, const char* name);
 int thorx_set_field(thorx_ctx* ctx, const char* name, const double* host);
 int thorx_get_field(thorx_ctx* ctx, const char* name, double* host);
 
+/* Initial state at rest (src/ESP/esp_initial.cu:507-588, isothermal branch): the isothermal
+ * hydrostatic column at Tmean from the Newton-Raphson solve of the reference, the same in every
+ * column, plus a seeded uniform temperature perturbation in [-noise_amp, noise_amp) K from
+ * SplitMix64(seed) on index col*nv + lev, at fixed pressure (rho = p / (Rd T)); Mh = W = Wh = 0,
+ * Rd and Cp uniform. noise_amp = 0 gives the reference's noise-free rest state. */
+int thorx_init_rest_state(thorx_ctx* ctx, double Tmean, unsigned long long seed, double noise_amp);
+
 /* One physics step, ESP::ProfX (src/ESP/profx_driver.cu:70-474): W from Wh, T and potential
  * temperature from p and rho, Held-Suarez forcing when core_benchmark says so, p = rho Rd T,
  * and the NaN check (reported at the next synchronising call as THORX_E_NAN). */
@@ -122,6 +129,16 @@ int thorx_step(thorx_ctx* ctx, int nsteps);
 int thorx_sync(thorx_ctx* ctx);
 /* Number of kernels one thorx_step(ctx, 1) launches. */
 int thorx_kernels_per_step(const thorx_ctx* ctx);
+
+/* Kernel classes of a step, for roofline accounting: name, algorithmic bytes of one launch
+ * (every element the kernel must read or write counted once, geometry included) and launches per
+ * step. thorx_profile_steps runs `nsteps` steps eagerly with a CUDA event pair on the context's
+ * stream around every launch and returns the summed milliseconds of each class in
+ * ms_per_class[0 .. thorx_kernel_classes()-1]. */
+int thorx_kernel_classes(const thorx_ctx* ctx);
+int thorx_kernel_info(const thorx_ctx* ctx, int k, const char** name, double* bytes_per_launch,
+                      int* launches_per_step);
+int thorx_profile_steps(thorx_ctx* ctx, int nsteps, double* ms_per_class);
 
 /* ---- Icosahedral grid (replaces Icogrid::Icogrid, src/ESP/grid.cu:84-302) ----
  * Builds THOR's grid on the host: same point order, neighbours, rhombus maps, spring-dynamics

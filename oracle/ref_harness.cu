@@ -170,16 +170,38 @@ static int sim_alloc(RefSim* s, const char* name, long n) {
     return 0;
 }
 
+// Grid arrays handed over directly (reference layouts), e.g. from a grid built elsewhere.
+struct ref_grid_view {
+    int           point_num, nv, nl_region, nr;
+    const int*    maps;
+    const int*    point_local;
+    const double *Altitude, *Altitudeh, *lonlat, *areas, *areasT, *areasTr, *nvecoa, *nvecti,
+        *nvecte, *div, *grad, *func_r;
+};
+
+static void* sim_new(const ref_grid_view* g, const ref_params* p);
+
 extern "C" void* ref_sim_new(void* gh, const ref_params* p) {
-    RefGrid* rg = (RefGrid*)gh;
-    Icogrid* g  = rg->g;
-    RefSim*  s  = new RefSim;
-    s->p        = *p;
-    s->N        = g->point_num;
-    s->nv       = g->nv;
-    s->nvi      = g->nvi;
+    Icogrid*      ig = ((RefGrid*)gh)->g;
+    ref_grid_view v{ig->point_num, ig->nv,         ig->nl_region, ig->nr,      ig->maps,
+                    ig->point_local, ig->Altitude, ig->Altitudeh, ig->lonlat,  ig->areas,
+                    ig->areasT,     ig->areasTr,   ig->nvecoa,    ig->nvecti,  ig->nvecte,
+                    ig->div,        ig->grad,      ig->func_r};
+    return sim_new(&v, p);
+}
+
+extern "C" void* ref_sim_new_view(const ref_grid_view* g, const ref_params* p) {
+    return sim_new(g, p);
+}
+
+static void* sim_new(const ref_grid_view* g, const ref_params* p) {
+    RefSim* s    = new RefSim;
+    s->p         = *p;
+    s->N         = g->point_num;
+    s->nv        = g->nv;
+    s->nvi       = g->nv + 1;
     s->nl_region = g->nl_region;
-    s->nr       = g->nr;
+    s->nr        = g->nr;
     long N = s->N, nv = s->nv, nvi = s->nvi;
 
     const char* cell1[] = {"Rho", "Rhok", "Rhos", "pressure", "pressurek", "pressures",
@@ -210,9 +232,9 @@ extern "C" void* ref_sim_new(void* gh, const ref_params* p) {
 
     // geometry (reference layout, copied as built by Icogrid)
     struct G {
-        const char* n;
-        double*     h;
-        long        c;
+        const char*   n;
+        const double* h;
+        long          c;
     } geo[] = {{"Altitude", g->Altitude, nv},  {"Altitudeh", g->Altitudeh, nvi},
                {"lonlat", g->lonlat, 2 * N},   {"areas", g->areas, 18 * N},
                {"areasT", g->areasT, N},       {"areasTr", g->areasTr, 6 * N},

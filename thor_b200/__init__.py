@@ -80,6 +80,16 @@ def lib():
         L.thorx_grid_get.argtypes = [vp, cp, vp]
         L.thorx_grid_get.restype = ctypes.c_long
         L.thorx_grid_free.argtypes = [vp]
+        L.thorx_init_rest_state.argtypes = [vp, ctypes.c_double, ctypes.c_ulonglong,
+                                            ctypes.c_double]
+        L.thorx_init_rest_state.restype = ci
+        L.thorx_kernel_classes.argtypes = [vp]
+        L.thorx_kernel_classes.restype = ci
+        L.thorx_kernel_info.argtypes = [vp, ci, ctypes.POINTER(cp), ctypes.POINTER(ctypes.c_double),
+                                        ctypes.POINTER(ci)]
+        L.thorx_kernel_info.restype = ci
+        L.thorx_profile_steps.argtypes = [vp, ci, ctypes.POINTER(ctypes.c_double)]
+        L.thorx_profile_steps.restype = ci
         _lib = L
     return _lib
 
@@ -87,7 +97,8 @@ def lib():
 EXPORTED = ["thorx_create", "thorx_destroy", "thorx_last_error", "thorx_field_size",
             "thorx_set_field", "thorx_get_field", "thorx_profx", "thorx_thor", "thorx_step",
             "thorx_sync", "thorx_kernels_per_step", "thorx_grid_build", "thorx_grid_info",
-            "thorx_grid_get", "thorx_grid_describe", "thorx_grid_free"]
+            "thorx_grid_get", "thorx_grid_describe", "thorx_grid_free", "thorx_init_rest_state",
+            "thorx_kernel_classes", "thorx_kernel_info", "thorx_profile_steps"]
 
 GRID_F64 = ["point_xyz", "point_xyzq", "Altitude", "Altitudeh", "lonlat", "areas", "areasT",
             "areasTr", "nvec", "nvecoa", "nvecti", "nvecte", "div", "grad", "func_r"]
@@ -183,6 +194,9 @@ class Thorx:
         self._check(lib().thorx_get_field(self.h, name.encode(), out.ctypes.data))
         return out
 
+    def init_rest_state(self, Tmean, seed=20260101, noise_amp=0.1):
+        self._check(lib().thorx_init_rest_state(self.h, Tmean, seed, noise_amp))
+
     def profx(self):
         self._check(lib().thorx_profx(self.h))
 
@@ -197,6 +211,24 @@ class Thorx:
 
     def kernels_per_step(self):
         return lib().thorx_kernels_per_step(self.h)
+
+    def kernel_table(self):
+        """[(name, algorithmic bytes per launch, launches per step)] for each kernel class."""
+        L = lib()
+        out = []
+        for k in range(L.thorx_kernel_classes(self.h)):
+            name, b, n = ctypes.c_char_p(), ctypes.c_double(), ctypes.c_int()
+            self._check(L.thorx_kernel_info(self.h, k, ctypes.byref(name), ctypes.byref(b),
+                                            ctypes.byref(n)))
+            out.append((name.value.decode(), b.value, n.value))
+        return out
+
+    def profile_steps(self, n):
+        """Summed ms per kernel class over n eager steps timed with CUDA events."""
+        k = lib().thorx_kernel_classes(self.h)
+        ms = (ctypes.c_double * k)()
+        self._check(lib().thorx_profile_steps(self.h, n, ms))
+        return list(ms)
 
     def close(self):
         if self.h:

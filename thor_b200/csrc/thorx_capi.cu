@@ -15,6 +15,8 @@
 
 #include <cstdio>
 #include <cstdlib>
+#include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <map>
 #include <string>
@@ -33,6 +35,7 @@ struct FieldDesc {
 
 struct thorx_ctx {
     Geometry     g{};
+    std::vector<double> Altitude_h, Altitudeh_h;
     Phys         P{};
     State        s{};
     cudaStream_t stream     = nullptr;
@@ -49,6 +52,11 @@ struct thorx_ctx {
     cudaGraph_t                      graph       = nullptr;
     std::string                      err;
     bool                             state_set = false;
+    // per-launch CUDA events of a profiled (eager) step, grouped by kernel class
+    bool                                                 profiling = false;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> prof;
+    std::vector<cudaEvent_t>                             event_pool;
+    size_t                                               event_next = 0;
 };
 
 namespace {
@@ -205,10 +213,101 @@ int check_flags(thorx_ctx* ctx) {
     return 0;
 }
 
+// Kernel classes of one step, for thorx_kernel_info / thorx_profile_steps.
+enum KClass { KProfx = 0, KAdvTemp, KDiffFirst, KDiffLast, KDivm0, KSlow, KMomentum, KVertical,
+              KUpdateRk2, KNumClasses };
+const char* const kClassName[KNumClasses] = {"profx", "adv_temp", "diffusion_first",
+                                             "diffusion_last", "divm0", "slow_modes", "momentum",
+                                             "vertical", "update_rk2"};
+
+cudaEvent_t next_event(thorx_ctx* ctx) {
+    if (ctx->event_next == ctx->event_pool.size()) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        ctx->event_pool.push_back(e);
+    }
+    return ctx->event_pool[ctx->event_next++];
+}
+
+// Brackets one launch with events when the context is profiling.
+struct KScope {
+    thorx_ctx*  ctx;
+    int         cls;
+    cudaEvent_t a = nullptr;
+    KScope(thorx_ctx* c, int k) : ctx(c), cls(k) {
+        if (ctx->profiling) {
+            a = next_event(ctx);
+            cudaEventRecord(a, ctx->stream);
+        }
+    }
+    ~KScope() {
+        if (ctx->profiling) {
+            cudaEvent_t b = next_event(ctx);
+            cudaEventRecord(b, ctx->stream);
+            ctx->prof.push_back({cls, {a, b}});
+        }
+    }
+};
+
+// Algorithmic bytes of one launch of a kernel class: every element the kernel must read or
+// write, counted once (neighbour re-reads are not counted), geometry included.
+double class_bytes(const thorx_ctx* ctx, int k) {
+    const double N = ctx->g.N, nv = ctx->g.nv, nvi = ctx->g.nvi;
+    const double S = 8.0 * N * nv, Si = 8.0 * N * nvi, G = 8.0 * N, I = 4.0 * N;
+    const Phys&  P = ctx->P;
+    const double ring_geo = 78 * G + 6 * I + N; // areas, areasTr, nvecoa/ti/te, ring, flag
+    switch (k) {
+    case KProfx: // Wh, p, Rd, Rho, Mh | W, T, p, Mh
+        return Si + 3 * S + (P.held_suarez ? 3 * S : 0) + G + 3 * S + (P.held_suarez ? 3 * S : 0);
+    case KAdvTemp: // Mhk, Rhok, Wk, Whk, pk, Rd, Cp | Adv, T, h, hh, pt, pth, gtil, gtilh
+        return 7 * S + Si + 21 * G + 3 * G + 6 * I + 7 * S + 3 * Si
+               + (P.energy ? 3 * S + 2 * Si - 2 * S - Si : 0);
+    case KDiffFirst: // Rhok, Mhk, Wk, T, Rd (Cp) | diff (6)
+        return (6 + (P.energy ? 1 : 0)) * S + ring_geo + 6 * S;
+    case KDiffLast: // diff (6), Rhok | diffrh, diffmh, diffw, diffpr
+        return 7 * S + ring_geo + 3 * G + 6 * S;
+    case KDivm0: // Mh, Wh | divg
+        return 3 * S + Si + ring_geo + 3 * S;
+    case KSlow: // divg, Cp, Rd, Adv, Rhok, pk, Mhk, h, Whk, hh, diffmh, dMh, diffw, dWh, diffrh,
+                // gtil, Qheat, diffpr (+ Mh, Rho, p, Wh) | SlowMh, SlowWh, SlowRho, Slowp (+ Mhs,
+                // Rhos, ps, Whs)
+        return (P.DivDampP ? 3 * S + ring_geo : 0) + 21 * S + 3 * Si + 45 * G + 6 * I
+               + 5 * S + Si;
+    case KMomentum: // divg, ps, SlowMh, Mhs | Mhs
+        return (P.DivDampP ? 3 * S + ring_geo : 0) + 7 * S + 24 * G + 6 * I + 3 * S;
+    case KVertical: // Mhs, h, Slowp, SlowRho, hh, gtilh, ps, Rhos, SlowWh, Whs, Cp, Rd, Mhk, pt,
+                    // pth, Rhok, pk, Whk, Qheat, diffpr | Whs, Rhos, ps
+        return 19 * S + 6 * Si + 21 * G + 6 * I + N + Si + 2 * S;
+    case KUpdateRk2: // Mhs, Mhk, Rhok, Rhos, pk, ps, Whk, Whs | Mhk, Rhok, pk, Whk, Wk
+        return 10 * S + 2 * Si + 3 * G + 6 * S + Si;
+    }
+    return 0;
+}
+
+int class_launches(const thorx_ctx* ctx, int k) {
+    const Phys& P      = ctx->P;
+    const int   passes = P.HyDiff ? P.HyDiffOrder / 2 : 0;
+    switch (k) {
+    case KProfx: return 1;
+    case KAdvTemp: return 3;
+    case KDiffFirst: return 3 * (passes - (passes > 0 ? 1 : 0));
+    case KDiffLast: return passes > 0 ? 3 : 0;
+    case KDivm0: return P.DivDampP ? 3 + 10 : 0;
+    case KSlow: return 3;
+    case KMomentum: return 10;
+    case KVertical: return 10;
+    case KUpdateRk2: return 3;
+    }
+    return 0;
+}
+
 // ESP::ProfX
 int enqueue_profx(thorx_ctx* ctx) {
     CK(cudaMemsetAsync(ctx->s.Qheat, 0, sizeof(double) * ctx->g.nv * ctx->g.Np, ctx->stream));
-    launch_profx(ctx->g, ctx->P, ctx->s, ctx->stream);
+    {
+        KScope k(ctx, KProfx);
+        launch_profx(ctx->g, ctx->P, ctx->s, ctx->stream);
+    }
     CK(cudaGetLastError());
     return 0;
 }
@@ -232,22 +331,43 @@ int enqueue_thor(thorx_ctx* ctx) {
     for (int rk = 0; rk < 3; rk++) {
         const int    ns_it = (rk == 0) ? 1 : (rk == 1 ? 3 : 6);
         const double times = (rk == 0) ? P.timestep / 3.0 : P.timestep / 6.0;
-        launch_adv_temp(g, P, s, st);
+        {
+            KScope k(ctx, KAdvTemp);
+            launch_adv_temp(g, P, s, st);
+        }
         if (P.HyDiff) {
             int passes = P.HyDiffOrder / 2;
-            for (int i = 0; i < passes; i++)
+            for (int i = 0; i < passes; i++) {
+                KScope k(ctx, i == passes - 1 ? KDiffLast : KDiffFirst);
                 launch_diffusion(g, P, s, i, i == passes - 1, st);
+            }
         }
-        if (P.DivDampP)
+        if (P.DivDampP) {
+            KScope k(ctx, KDivm0);
             launch_divm0(g, P, s, false, st);
-        launch_slow_modes(g, P, s, rk > 0, st);
-        for (int ns = 0; ns < ns_it; ns++) {
-            if (P.DivDampP)
-                launch_divm0(g, P, s, true, st);
-            launch_momentum(g, P, s, times, st);
-            launch_vertical(g, P, s, times, st);
         }
-        launch_update_rk2(g, P, s, st);
+        {
+            KScope k(ctx, KSlow);
+            launch_slow_modes(g, P, s, rk > 0, st);
+        }
+        for (int ns = 0; ns < ns_it; ns++) {
+            if (P.DivDampP) {
+                KScope k(ctx, KDivm0);
+                launch_divm0(g, P, s, true, st);
+            }
+            {
+                KScope k(ctx, KMomentum);
+                launch_momentum(g, P, s, times, st);
+            }
+            {
+                KScope k(ctx, KVertical);
+                launch_vertical(g, P, s, times, st);
+            }
+        }
+        {
+            KScope k(ctx, KUpdateRk2);
+            launch_update_rk2(g, P, s, st);
+        }
     }
     CK(cudaMemcpyAsync(s.Mh, s.Mhk, 3 * cell, cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync(s.Wh, s.Whk, iface, cudaMemcpyDeviceToDevice, st));
@@ -357,6 +477,8 @@ int thorx_create(const thorx_grid* gr, const thorx_params* pr, void* stream, tho
         CK(cudaMemcpy(a, kdh4.data(), nv * 8, cudaMemcpyHostToDevice));
         CK(cudaMemcpy(b, kdhz.data(), nv * 8, cudaMemcpyHostToDevice));
         CK(cudaMemcpy(alt, gr->Altitude, nv * 8, cudaMemcpyHostToDevice));
+        ctx->Altitude_h.assign(gr->Altitude, gr->Altitude + nv);
+        ctx->Altitudeh_h.assign(gr->Altitudeh, gr->Altitudeh + nv + 1);
         CK(cudaMemcpy(alth, gr->Altitudeh, (nv + 1) * 8, cudaMemcpyHostToDevice));
         g.Kdh4      = a;
         g.Kdhz      = b;
@@ -434,6 +556,8 @@ void thorx_destroy(thorx_ctx* ctx) {
         cudaGraphDestroy(ctx->graph);
     if (ctx->stream)
         cudaStreamSynchronize(ctx->stream);
+    for (cudaEvent_t e : ctx->event_pool)
+        cudaEventDestroy(e);
     for (void* p : ctx->allocs)
         cudaFree(p);
     if (ctx->flags_host)
@@ -493,6 +617,80 @@ int thorx_get_field(thorx_ctx* ctx, const char* name, double* host) {
     return 0;
 }
 
+int thorx_init_rest_state(thorx_ctx* ctx, double Tmean, unsigned long long seed,
+                          double noise_amp) {
+    if (!ctx)
+        return THORX_E_ARG;
+    if (!(Tmean > 0) || !(noise_amp >= 0) || noise_amp >= Tmean)
+        return fail(ctx, THORX_E_ARG, "thorx_init_rest_state: bad Tmean or noise amplitude");
+    const int  N = ctx->g.N, nv = ctx->g.nv;
+    const Phys& P = ctx->P;
+    const double* Alt  = ctx->Altitude_h.data();
+    const double* Alth = ctx->Altitudeh_h.data();
+    // isothermal hydrostatic column: Newton-Raphson on the discrete hydrostatic balance between
+    // consecutive levels (src/ESP/esp_initial.cu:518-587, GravHeightVar as configured)
+    std::vector<double> p0(nv), r0(nv), T0(nv);
+    const double        eps = 1e-15;
+    const int           it_max = 100;
+    for (int lev = 0; lev < nv; lev++) {
+        double P_L, rho_L, T_L, dz, g_L, l_int, r_int;
+        if (lev == 0) {
+            P_L   = P.P_Ref;
+            rho_L = P.P_Ref / (P.Rd * Tmean);
+            T_L   = Tmean;
+            dz    = Alt[0];
+            g_L   = P.GravHeightVar ? P.Gravit * pow(P.A / (P.A + Alt[0]), 2) : P.Gravit;
+            l_int = 0.5;
+            r_int = 0.5;
+        }
+        else {
+            P_L   = p0[lev - 1];
+            rho_L = r0[lev - 1];
+            T_L   = T0[lev - 1];
+            dz    = Alt[lev] - Alt[lev - 1];
+            g_L   = P.GravHeightVar ? P.Gravit * pow(P.A / (P.A + Alt[lev - 1]), 2) : P.Gravit;
+            l_int = (Alt[lev] - Alth[lev]) / dz;
+            r_int = (Alth[lev] - Alt[lev - 1]) / dz;
+        }
+        p0[lev]     = P_L;
+        r0[lev]     = rho_L;
+        T0[lev]     = T_L;
+        double ptmp = p0[lev] + 2 * eps * p0[lev];
+        double g    = P.GravHeightVar ? P.Gravit * pow(P.A / (P.A + Alt[lev]), 2) : P.Gravit;
+        for (int it = 0; it < it_max && (ptmp - p0[lev]) / p0[lev] > eps; it++) {
+            ptmp      = p0[lev];
+            double f  = (p0[lev] - P_L) / dz + (g * r_int + g_L * l_int) * (r0[lev] * r_int + rho_L * l_int);
+            double df = 1.0 / dz + (g * r_int + g_L * l_int) * r_int / (P.Rd * T0[lev]);
+            p0[lev]   = p0[lev] - f / df;
+            r0[lev]   = p0[lev] / (P.Rd * T0[lev]);
+        }
+    }
+    // per-column fields with the seeded perturbation (SplitMix64: Steele, Lea & Flood 2014)
+    const size_t        n = (size_t)N * nv;
+    std::vector<double> T(n), p(n), rho(n), Rd(n, P.Rd), Cp(n, P.Cp), zero3(3 * n, 0.0),
+        zeroi((size_t)N * (nv + 1), 0.0), zero(n, 0.0);
+    uint64_t x = seed;
+    for (size_t i = 0; i < n; i++) {
+        x += 0x9E3779B97F4A7C15ull;
+        uint64_t z = x;
+        z          = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z          = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z          = z ^ (z >> 31);
+        double u   = (double)(z >> 11) * (1.0 / 9007199254740992.0);
+        int    lev = (int)(i % nv);
+        T[i]       = T0[lev] + (2.0 * u - 1.0) * noise_amp;
+        p[i]       = p0[lev];
+        rho[i]     = p[i] / (P.Rd * T[i]);
+    }
+    int rc;
+    if ((rc = thorx_set_field(ctx, "temperature", T.data())) || (rc = thorx_set_field(ctx, "pressure", p.data()))
+        || (rc = thorx_set_field(ctx, "Rho", rho.data())) || (rc = thorx_set_field(ctx, "Rd", Rd.data()))
+        || (rc = thorx_set_field(ctx, "Cp", Cp.data())) || (rc = thorx_set_field(ctx, "Mh", zero3.data()))
+        || (rc = thorx_set_field(ctx, "Wh", zeroi.data())) || (rc = thorx_set_field(ctx, "W", zero.data())))
+        return rc;
+    return 0;
+}
+
 int thorx_profx(thorx_ctx* ctx) {
     if (!ctx)
         return THORX_E_ARG;
@@ -543,10 +741,51 @@ int thorx_sync(thorx_ctx* ctx) {
 int thorx_kernels_per_step(const thorx_ctx* ctx) {
     if (!ctx)
         return THORX_E_ARG;
-    const int passes = ctx->P.HyDiff ? ctx->P.HyDiffOrder / 2 : 0;
-    const int divm   = ctx->P.DivDampP ? 1 : 0;
-    // profx + 3 x (adv_temp + passes + divm0 + slow_modes + update_rk2) + 10 x (divm0 + 2)
-    return 1 + 3 * (1 + passes + divm + 1 + 1) + 10 * (divm + 2);
+    int n = 0;
+    for (int k = 0; k < KNumClasses; k++)
+        n += class_launches(ctx, k);
+    return n;
+}
+
+int thorx_kernel_classes(const thorx_ctx* ctx) { return ctx ? (int)KNumClasses : THORX_E_ARG; }
+
+int thorx_kernel_info(const thorx_ctx* ctx, int k, const char** name, double* bytes_per_launch,
+                      int* launches_per_step) {
+    if (!ctx || k < 0 || k >= KNumClasses)
+        return THORX_E_ARG;
+    if (name)
+        *name = kClassName[k];
+    if (bytes_per_launch)
+        *bytes_per_launch = class_bytes(ctx, k);
+    if (launches_per_step)
+        *launches_per_step = class_launches(ctx, k);
+    return 0;
+}
+
+int thorx_profile_steps(thorx_ctx* ctx, int nsteps, double* ms_per_class) {
+    if (!ctx || nsteps < 1 || !ms_per_class)
+        return THORX_E_ARG;
+    ctx->profiling  = true;
+    ctx->event_next = 0;
+    ctx->prof.clear();
+    int rc = 0;
+    for (int i = 0; i < nsteps && !rc; i++) {
+        rc = enqueue_profx(ctx);
+        if (!rc)
+            rc = enqueue_thor(ctx);
+    }
+    ctx->profiling = false;
+    if (rc)
+        return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (int k = 0; k < KNumClasses; k++)
+        ms_per_class[k] = 0.0;
+    for (auto& e : ctx->prof) {
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, e.second.first, e.second.second));
+        ms_per_class[e.first] += ms;
+    }
+    return 0;
 }
 
 } // extern "C"
