@@ -99,3 +99,18 @@ def test_sixth_order_hyperdiffusion_matches_oracle():
     lim = {"SlowWh": 1e-6, "Slowpressure": 1e-8, "SlowRho": 1e-9, "Wh": 1e-9, "W": 1e-9}
     bad = {f: e for f, e in errs.items() if not e <= lim.get(f, 1e-10)}
     assert not bad, errs
+
+
+@pytest.mark.gpu
+def test_product_grid_and_rest_state_match_the_test_setup():
+    """thorx_grid_build + thorx_init_rest_state give the same state as the reference grid + the
+    test helper (bit for bit), so bench.py's workload is the one the parity tests check."""
+    glevel, nv, dt = 4, 12, 1200.0
+    mine = thor_b200.Icogrid(glevel, nv)
+    p, c = make_params(glevel, dt)
+    x = thor_b200.Thorx(mine.as_dict(), glevel, thorx_params(c, dt))
+    x.init_rest_state(300.0, 20260101, 0.1)
+    ic = initial_state(mine.arrays, mine.point_num, nv, c)
+    for f in ["Rho", "pressure", "temperature", "Mh", "Wh", "W"]:
+        assert np.array_equal(x.get(f), ic[f]), f
+    x.close()

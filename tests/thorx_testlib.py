@@ -120,17 +120,13 @@ class RefGrid:
 # ------------------------------------------------------------------------------------------------
 def splitmix64_uniform(n, seed):
     """n uniform doubles in [0,1) from SplitMix64 (Steele, Lea & Flood 2014), top 53 bits."""
-    mask = (1 << 64) - 1
-    out = np.empty(n)
-    x = seed & mask
-    for i in range(n):
-        x = (x + 0x9E3779B97F4A7C15) & mask
-        z = x
-        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & mask
-        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & mask
-        z = z ^ (z >> 31)
-        out[i] = (z >> 11) * (1.0 / 9007199254740992.0)
-    return out
+    with np.errstate(over="ignore"):
+        x = np.uint64(seed) + (np.arange(1, n + 1, dtype=np.uint64)
+                               * np.uint64(0x9E3779B97F4A7C15))
+        z = (x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    return (z >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
 
 
 def isothermal_column(Altitude, Altitudeh, c):
