@@ -5,23 +5,27 @@
 // order and association, same math-library calls), so that the only differences from the
 // reference build are the FMA contractions the compiler chooses.
 //
-// Work decomposition:
-//   * column kernels (profx, adv_temp, vertical, update_rk2): one thread per column, looping over
-//     the levels, because they carry a vertical recurrence (extrapolations, Thomas solve);
-//   * stencil kernels (diffusion, divm0, slow_modes, momentum): one thread per column and a
-//     chunk of kLevChunk levels, so that the column's geometry (up to 78 doubles) is loaded once
-//     into registers and reused across the chunk.
+// Work decomposition: every kernel except ProfX runs on tiles of 32 consecutive columns (one per
+// lane, so that each plane access of a warp is one or two 128-byte lines) times all levels, the
+// levels spread over kLevGroups warps (lane x = column, warp y = levels y, y+8, ...). What a
+// column needs from the grid (stencil weights, ring geometry) is staged once per tile in shared
+// memory, [quantity][32 columns], and shared by the 8 level groups.
+// Where the reference carries values down a column loop (Compute_Temperature_H_Pt_Geff,
+// Vertical_Eq, UpdateRK2) each level recomputes what it needs from the neighbouring levels
+// instead, with the same operations, so that all levels run in parallel; only the Thomas
+// elimination itself stays sequential, in shared memory.
 // Neighbours come from the per-column tables described in thorx_internal.h; a hole (-1) reads 0.
+// Stencils are templated on the ring size (6, or 5 at pentagons and poles) so that every index
+// is static and the ring values stay in registers.
 
 #include "thorx_internal.h"
 
 namespace thorx {
 namespace {
 
-constexpr int kColBlock  = 128; // threads per block, column kernels
-constexpr int kStenBlock = 64;  // threads per block, stencil kernels
-constexpr int kLevChunk  = 4;   // levels per thread, stencil kernels
-constexpr int kVertBlock = 64;  // threads per block, vertical implicit kernel
+constexpr int kTile      = 32; // columns per tile (lanes)
+constexpr int kLevGroups = 8;  // warps per tile, each taking every 8th level
+constexpr int kColBlock  = 128;
 
 __device__ __forceinline__ double gz(const double* __restrict__ plane, int id) {
     return id >= 0 ? __ldg(plane + id) : 0.0;
@@ -31,10 +35,60 @@ __device__ __forceinline__ double rscale_of(const Phys& P, const Geometry& g, in
     return P.DeepModel ? P.A / (g.Altitude[lev] + P.A) : 1.0;
 }
 
+// Copies rows 0..Q-1 of a [q][Np] grid array for the tile's 32 columns into smem [q][32].
+__device__ __forceinline__ void stage(double* sm, const double* __restrict__ src, int Q, int Np,
+                                      int c0) {
+    for (int q = threadIdx.y; q < Q; q += blockDim.y)
+        sm[q * kTile + threadIdx.x] = __ldg(src + (size_t)q * Np + c0 + threadIdx.x);
+}
+
+// Column of lane x in a stencil kernel with a five-entry-ring tail CTA. The regular tiles cover
+// columns c0..c0+31 and skip the 10 pentagons and 2 poles; the last CTA of the grid takes exactly
+// those 12 columns (g.special), one per lane, with the n = 5 stencil code. Returns -1 for an
+// idle lane.
+__device__ __forceinline__ bool tail_cta() { return blockIdx.x == gridDim.x - 1; }
+__device__ __forceinline__ int lane_column(const Geometry& g) {
+    const int x = threadIdx.x;
+    if (tail_cta())
+        return x < g.nspecial ? g.special[x] : -1;
+    const int c = blockIdx.x * kTile + x;
+    return (c < g.N && !(g.cflag[c] & kRing5)) ? c : -1;
+}
+// Copies rows 0..Q-1 of a [q][Np] grid array for the lanes' columns into smem [q][32].
+__device__ __forceinline__ void stage_cols(double* sm, const double* __restrict__ src, int Q,
+                                           int Np, int col) {
+    for (int q = threadIdx.y; q < Q; q += blockDim.y)
+        sm[q * kTile + threadIdx.x] = col >= 0 ? __ldg(src + (size_t)q * Np + col) : 0.0;
+}
+
+// Shared-memory view of one column's ring geometry, [quantity][32].
+struct SGeo {
+    const double *ar, *at, *ti, *te, *oa;
+    int           x;
+    __device__ double AR(int q) const { return ar[q * kTile + x]; }
+    __device__ double AT(int q) const { return at[q * kTile + x]; }
+    __device__ double TI(int q) const { return ti[q * kTile + x]; }
+    __device__ double TE(int q) const { return te[q * kTile + x]; }
+    __device__ double OA(int q) const { return oa[q * kTile + x]; }
+};
+
+constexpr int kRingGeoRows = 78; // areas 18, areasTr 6, nvecti 18, nvecte 18, nvecoa 18
+
+__device__ __forceinline__ SGeo stage_ring_geo(double* sm, const Geometry& g, int col) {
+    stage_cols(sm, g.areas, 18, g.Np, col);
+    stage_cols(sm + 18 * kTile, g.areasTr, 6, g.Np, col);
+    stage_cols(sm + 24 * kTile, g.nvecti, 18, g.Np, col);
+    stage_cols(sm + 42 * kTile, g.nvecte, 18, g.Np, col);
+    stage_cols(sm + 60 * kTile, g.nvecoa, 18, g.Np, col);
+    return SGeo{sm, sm + 18 * kTile, sm + 24 * kTile, sm + 42 * kTile, sm + 60 * kTile,
+                (int)threadIdx.x};
+}
+
 // ---------------------------------------------------------------------------------------------
 // ProfX: Recompute_W (reference src/headers/phy/profx_auxiliary.h:109-130), Compute_temperature
 // (:64-92), held_suarez (src/headers/phy/profx_held_suarez.h:51-117), Compute_pressure (:94-107)
 // and the NaN check on temperature (:132-146, src/ESP/profx_driver.cu:389-396,451-458).
+// One thread per column (1% of a step).
 // ---------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(kColBlock) profx_kernel(Geometry g, Phys P, State s) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -51,8 +105,8 @@ __global__ void __launch_bounds__(kColBlock) profx_kernel(Geometry g, Phys P, St
         s.W[lev * Np + c] = whl * intt + wht * intl;
     }
     for (int lev = 0; lev < nv; lev++) {
-        int i   = lev * Np + c;
-        s.T[i]  = s.p[i] / (s.Rd[i] * s.Rho[i]);
+        int i  = lev * Np + c;
+        s.T[i] = s.p[i] / (s.Rd[i] * s.Rho[i]);
     }
     if (P.held_suarez) {
         const double sigmab = 0.7, ka = (1.0 / 40.0) * (1.0 / 86400.0), kf = 1.0 / 86400.0;
@@ -74,7 +128,7 @@ __global__ void __launch_bounds__(kColBlock) profx_kernel(Geometry g, Phys P, St
                               * pow(cos(lat), 4.0);
             double kv = kf * fmax(0.0, (sigma - sigmab) / (1.0 - sigmab));
             for (int k = 0; k < 3; k++) {
-                int j    = (k * nv + lev) * Np + c;
+                int j   = (k * nv + lev) * Np + c;
                 s.Mh[j] = s.Mh[j] / (1.0 + kv * P.timestep);
             }
             s.T[i] -= kt * P.timestep * (s.T[i] - Teq);
@@ -97,78 +151,128 @@ __global__ void __launch_bounds__(kColBlock) profx_kernel(Geometry g, Phys P, St
 //   (src/headers/dyn/thor_auxiliary.h:55-309, calcT = true).
 // The cartesian velocity v of the reference is recomputed where it is used instead of stored.
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(kColBlock) adv_temp_kernel(Geometry g, Phys P, State s) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+struct ColLevel { // thermodynamic quantities of one column at one level
+    double p, rho, Rd, Cp;
+};
+
+__device__ __forceinline__ ColLevel col_level(const State& s, int Np, int lev, int c) {
+    const int i = lev * Np + c;
+    return ColLevel{s.pk[i], s.Rhok[i], s.Rd[i], s.Cp[i]};
+}
+// enthalpy h = Cv T + p / rho (thor_auxiliary.h:111,130,140)
+__device__ __forceinline__ double enthalpy(const ColLevel& q) {
+    const double Cv = q.Cp - q.Rd;
+    const double T  = q.p / (q.rho * q.Rd);
+    return Cv * T + q.p / q.rho;
+}
+// potential temperature (thor_auxiliary.h:111-112,163)
+__device__ __forceinline__ double pot_temp(const ColLevel& q, double P_Ref) {
+    const double Cv    = q.Cp - q.Rd;
+    const double CvoCp = Cv / q.Cp;
+    return (P_Ref / (q.Rd * q.rho)) * pow(q.p / P_Ref, CvoCp);
+}
+
+__global__ void __launch_bounds__(kTile* kLevGroups) adv_temp_kernel(Geometry g, Phys P, State s) {
+    __shared__ double sdiv[21 * kTile];
+    const int         c0 = blockIdx.x * kTile, x = threadIdx.x, c = c0 + x;
+    const int         Np = g.Np, nv = g.nv;
+    stage(sdiv, g.div, 21, Np, c0);
+    __syncthreads();
     if (c >= g.N)
         return;
-    const int     Np = g.Np, nv = g.nv;
     const double* Alt  = g.Altitude;
     const double* Alth = g.Altitudeh;
-    const double  A = P.A, Omega = P.Omega;
+    const double  A = P.A, Omega = P.Omega, P_Ref = P.P_Ref, Gravit = P.Gravit;
+    const bool    eeq = P.energy, ghv = P.GravHeightVar;
 
     int nb[7];
     nb[0] = c;
     for (int j = 0; j < 6; j++)
         nb[j + 1] = g.nb[j * Np + c];
-    double dv[21];
-    for (int q = 0; q < 21; q++)
-        dv[q] = g.div[q * Np + c];
     double fr[7][3];
     for (int j = 0; j < 7; j++)
         for (int k = 0; k < 3; k++)
             fr[j][k] = gz(g.func_r + k * Np, nb[j]);
 
-    // own-column velocity at a level: v = M/rho + (w/rho) r
     auto vown = [&](int lev, double* v) {
         double rho = s.Rhok[lev * Np + c], w = s.Wk[lev * Np + c];
         for (int k = 0; k < 3; k++)
             v[k] = s.Mhk[(k * nv + lev) * Np + c] / rho + (w / rho) * fr[0][k];
     };
+    // kinetic energy per mass of the column at a level (thor_auxiliary.h:152-157)
+    auto ekin = [&](int lev) {
+        const int    i  = lev * Np + c;
+        const double m0 = s.Mhk[(0 * nv + lev) * Np + c], m1 = s.Mhk[(1 * nv + lev) * Np + c],
+                     m2 = s.Mhk[(2 * nv + lev) * Np + c], w = s.Wk[i], r = s.Rhok[i];
+        return 0.5 * (m0 * m0 + m1 * m1 + m2 * m2 + w * w) / (r * r);
+    };
+    auto epot = [&](int lev) {
+        return ghv ? Gravit * pow(A / (A + Alt[lev]), 2) * Alt[lev] : Gravit * Alt[lev];
+    };
+    // velocity-weighted effective gravity at interior interface i (thor_auxiliary.h:288-289)
+    auto gtil_w = [&](int i) -> double {
+        if (i <= 0 || i >= nv)
+            return 0.0;
+        const ColLevel lo = col_level(s, Np, i - 1, c), hi = col_level(s, Np, i, c);
+        const double   dz    = Alt[i] - Alt[i - 1];
+        const double   dp_dz = (hi.p - lo.p) / dz;
+        const double   xi = Alth[i], xim = Alt[i - 1], xip = Alt[i];
+        const double   intt = (xi - xip) / (xim - xip), intl = (xi - xim) / (xip - xim);
+        const double   rhoh = lo.rho * intt + hi.rho * intl;
+        return -(s.Whk[i * Np + c] / rhoh) * dp_dz;
+    };
 
-    double vprev[3] = {0, 0, 0}, vcur[3], vnext[3] = {0, 0, 0};
-    vown(0, vcur);
-    for (int lev = 0; lev < nv; lev++) {
+    for (int lev = threadIdx.y; lev < nv; lev += kLevGroups) {
+        const int    i      = lev * Np + c;
         const double rscale = rscale_of(P, g, lev);
-        // horizontal flux divergence of v (x) M over the 7-point stencil
+        // ---- horizontal flux divergence of v (x) M over the 7-point stencil ----
         double M[7][3], V[7][3];
+#pragma unroll
         for (int j = 0; j < 7; j++) {
-            int id = nb[j];
+            const int id = nb[j];
             if (id >= 0) {
-                double rho = s.Rhok[lev * Np + id], w = s.Wk[lev * Np + id];
+                const double rho = s.Rhok[lev * Np + id], w = s.Wk[lev * Np + id];
+#pragma unroll
                 for (int k = 0; k < 3; k++) {
                     M[j][k] = s.Mhk[(k * nv + lev) * Np + id];
                     V[j][k] = M[j][k] / rho + (w / rho) * fr[j][k];
                 }
             }
             else {
+#pragma unroll
                 for (int k = 0; k < 3; k++)
                     M[j][k] = V[j][k] = 0.0;
             }
         }
         double nflx[3] = {0.0, 0.0, 0.0};
+#pragma unroll
         for (int kk = 0; kk < 3; kk++)
+#pragma unroll
             for (int cc = 0; cc < 3; cc++) {
-                double sum = dv[kk] * V[0][cc] * M[0][kk];
+                double sum = sdiv[kk * kTile + x] * V[0][cc] * M[0][kk];
+#pragma unroll
                 for (int j = 1; j < 7; j++)
-                    sum = sum + dv[j * 3 + kk] * V[j][cc] * M[j][kk];
+                    sum = sum + sdiv[(j * 3 + kk) * kTile + x] * V[j][cc] * M[j][kk];
                 nflx[cc] += rscale * sum;
             }
-        // vertical flux of v w at the interfaces + Coriolis
-        if (lev < nv - 1)
-            vown(lev + 1, vnext);
-        const double altht = Alth[lev + 1], althl = Alth[lev], alt = Alt[lev];
-        double       dvwl[3] = {0, 0, 0}, dvwt[3] = {0, 0, 0};
+        // ---- vertical flux of v w at the interfaces + Coriolis ----
+        const double* vcur = V[0];
+        double        vprev[3] = {0, 0, 0}, vnext[3] = {0, 0, 0};
+        const double  altht = Alth[lev + 1], althl = Alth[lev], alt = Alt[lev];
+        double        dvwl[3] = {0, 0, 0}, dvwt[3] = {0, 0, 0};
         if (lev > 0) {
-            double xi = althl, xim = Alt[lev - 1], xip = alt;
-            double intt = (xi - xip) / (xim - xip), intl = (xi - xim) / (xip - xim);
-            double whl = s.Whk[lev * Np + c];
+            vown(lev - 1, vprev);
+            const double xi = althl, xim = Alt[lev - 1], xip = alt;
+            const double intt = (xi - xip) / (xim - xip), intl = (xi - xim) / (xip - xim);
+            const double whl = s.Whk[lev * Np + c];
             for (int k = 0; k < 3; k++)
                 dvwl[k] = (vprev[k] * intt + vcur[k] * intl) * whl;
         }
         if (lev < nv - 1) {
-            double xi = altht, xim = alt, xip = Alt[lev + 1];
-            double intt = (xi - xip) / (xim - xip), intl = (xi - xim) / (xip - xim);
-            double wht = s.Whk[(lev + 1) * Np + c];
+            vown(lev + 1, vnext);
+            const double xi = altht, xim = alt, xip = Alt[lev + 1];
+            const double intt = (xi - xip) / (xim - xip), intl = (xi - xim) / (xip - xim);
+            const double wht = s.Whk[(lev + 1) * Np + c];
             for (int k = 0; k < 3; k++)
                 dvwt[k] = (vcur[k] * intt + vnext[k] * intl) * wht;
         }
@@ -179,7 +283,7 @@ __global__ void __launch_bounds__(kColBlock) adv_temp_kernel(Geometry g, Phys P,
             r2l = pow(althl + A, 2.0);
         }
         const double dz  = 1.0 / ((althl - altht) * r2m);
-        const double rho = s.Rhok[lev * Np + c];
+        const double rho = s.Rhok[i];
         double       C[3];
         if (P.DeepModel) {
             C[0] = -2.0 * Omega * vcur[1] * rho;
@@ -193,95 +297,84 @@ __global__ void __launch_bounds__(kColBlock) adv_temp_kernel(Geometry g, Phys P,
             C[2] = 2 * Omega * (vcur[1] * f[2] * f[0] - vcur[0] * f[2] * f[1]) * rho;
         }
         for (int k = 0; k < 3; k++) {
-            double dav                          = (dvwl[k] * r2l - dvwt[k] * r2p) * dz;
+            const double dav               = (dvwl[k] * r2l - dvwt[k] * r2p) * dz;
             s.Adv[(k * nv + lev) * Np + c] = nflx[k] + (dav + C[k]);
         }
-        for (int k = 0; k < 3; k++) {
-            vprev[k] = vcur[k];
-            vcur[k]  = vnext[k];
-        }
-    }
 
-    // ---- Compute_Temperature_H_Pt_Geff: column recurrence over levels 0..nv ----
-    const bool   eeq = P.energy, ghv = P.GravHeightVar;
-    const double P_Ref = P.P_Ref, Gravit = P.Gravit;
-    double       rho = 0, rhoh, rhol = 0, rhop, pressure = 0, h_ = 0, hl = 0, pt_ = 0, ptl = 0,
-           pl = 0, pp, dpdz, ep = 0, epl = 0, ek = 0, ekl = 0, gtilh_ = 0, gtilht, dz, dp_dz, Cv,
-           CvoCp, xi, xim, xip, intt, intl, extr, alt = 0, altl = 0, alth = 0, altht = 0;
-    const double* Pk = s.pk;
-    const double* Rk = s.Rhok;
-    for (int lev = 0; lev < nv + 1; lev++) {
-        if (lev < nv) {
-            const int i = lev * Np + c;
-            Cv          = s.Cp[i] - s.Rd[i];
-            CvoCp       = Cv / s.Cp[i];
-            if (lev > 0) {
-                pl   = pressure;
-                rhol = rho;
-                hl   = h_;
-                if (eeq) {
-                    epl = ep;
-                    ekl = ek;
-                }
-                else
-                    ptl = pt_;
-                altl = alt;
-            }
-            pressure           = Pk[i];
-            rho                = Rk[i];
-            double temperature = pressure / (rho * s.Rd[i]);
-            s.T[i]             = temperature;
-            alt                = Alt[lev];
-            alth               = Alth[lev];
-            altht              = Alth[lev + 1];
-            h_                 = Cv * temperature + pressure / rho;
-            s.h[i]             = h_;
+        // ---- Compute_Temperature_H_Pt_Geff at this level (and its interface below) ----
+        const ColLevel q  = col_level(s, Np, lev, c);
+        const double   Cv = q.Cp - q.Rd;
+        const double   T  = q.p / (q.rho * q.Rd);
+        const double   h  = Cv * T + q.p / q.rho;
+        s.T[i]            = T;
+        s.h[i]            = h;
+        double ep = 0, ek = 0, pt = 0;
+        if (eeq) {
+            ep          = epot(lev);
+            ek          = ekin(lev);
+            s.ep[i]     = ep;
+            s.ek[i]     = ek;
+            s.Etotal[i] = q.rho * (ep + ek) + Cv / q.Rd * q.p;
+        }
+        else {
+            pt      = pot_temp(q, P_Ref);
+            s.pt[i] = pt;
+        }
+        if (lev > 0) { // interior interface `lev`
+            const ColLevel lo    = col_level(s, Np, lev - 1, c);
+            const double   dzl   = alt - Alt[lev - 1];
+            const double   dp_dz = (q.p - lo.p) / dzl;
+            const double   xi = althl, xim = Alt[lev - 1], xip = alt;
+            const double   intt = (xi - xip) / (xim - xip), intl = (xi - xim) / (xip - xim);
+            s.hh[i] = enthalpy(lo) * intt + h * intl;
             if (eeq) {
-                if (ghv)
-                    ep = Gravit * pow(A / (A + Alt[lev]), 2) * Alt[lev];
-                else
-                    ep = Gravit * Alt[lev];
-                s.ep[i] = ep;
-                double m0 = s.Mhk[(0 * nv + lev) * Np + c], m1 = s.Mhk[(1 * nv + lev) * Np + c],
-                       m2 = s.Mhk[(2 * nv + lev) * Np + c], w = s.Wk[i];
-                ek = 0.5 * (m0 * m0 + m1 * m1 + m2 * m2 + w * w) / (Rk[i] * Rk[i]);
-                s.ek[i]     = ek;
-                s.Etotal[i] = Rk[i] * (ep + ek) + Cv / s.Rd[i] * pressure;
+                s.eph[i] = epot(lev - 1) * intt + ep * intl;
+                s.ekh[i] = ekin(lev - 1) * intt + ek * intl;
             }
-            else {
-                pt_     = (P_Ref / (s.Rd[i] * rho)) * pow(pressure / P_Ref, CvoCp);
-                s.pt[i] = pt_;
-            }
-        }
-        if (lev == 0) {
-            extr     = (-alt - Alt[lev + 1]) / (Alt[lev + 1] - alt);
-            s.hh[c]  = h_;
-            if (ghv)
-                pl = Pk[Np + c] - rho * Gravit * pow(A / (A + Alt[0]), 2) * (-alt - Alt[1]);
             else
-                pl = Pk[Np + c] - rho * Gravit * (-alt - Alt[1]);
-            rhol       = Rk[Np + c] + (Rk[Np + c] - rho) * extr;
-            rhoh       = 0.5 * (rho + rhol);
-            dz         = 2.0 * Alt[0];
-            dpdz       = (Pk[c] - pl) / dz;
-            s.gtilh[c] = -(1.0 / rhoh) * dpdz;
-            gtilh_     = 0.0;
+                s.pth[i] = pot_temp(lo, P_Ref) * intt + pt * intl;
+            const double rhoh = lo.rho * intt + q.rho * intl;
+            s.gtilh[i]        = -(1.0 / rhoh) * dp_dz;
         }
-        else if (lev == nv) {
-            const int top = (nv - 1) * Np + c, top2 = (nv - 2) * Np + c;
-            extr  = (2 * Alth[nv] - alt - Alt[nv - 2]) / (Alt[nv - 1] - Alt[nv - 2]);
-            Cv    = s.Cp[top] - s.Rd[top];
-            CvoCp = Cv / s.Cp[top];
-            s.hh[nv * Np + c] = h_;
+        else { // bottom boundary, extrapolated (thor_auxiliary.h:167-187)
+            const ColLevel up   = col_level(s, Np, 1, c);
+            const double   extr = (-alt - Alt[1]) / (Alt[1] - alt);
+            s.hh[c]             = h;
+            double pl;
             if (ghv)
-                pp = Pk[top2] - rho * Gravit * pow(A / (A + Alt[lev]), 2)
-                                    * (2 * Alth[nv] - alt - Alt[nv - 2]);
+                pl = up.p - q.rho * Gravit * pow(A / (A + Alt[0]), 2) * (-alt - Alt[1]);
             else
-                pp = Pk[top2] - rho * Gravit * (2 * Alth[nv] - alt - Alt[nv - 2]);
+                pl = up.p - q.rho * Gravit * (-alt - Alt[1]);
+            const double rhol = up.rho + (up.rho - q.rho) * extr;
+            const double rhoh = 0.5 * (q.rho + rhol);
+            const double dzb  = 2.0 * Alt[0];
+            const double dpdz = (q.p - pl) / dzb;
+            s.gtilh[c]        = -(1.0 / rhoh) * dpdz;
+        }
+        // effective gravity at the layer centre (thor_auxiliary.h:293-300; :259-266 at the top,
+        // where the reference interpolates with the top layer's own geometry)
+        {
+            const int    L1   = (lev < nv - 1) ? lev + 1 : lev;
+            const double xi   = Alt[L1], xim = Alth[L1], xip = Alth[L1 + 1];
+            const double intt = (xi - xip) / (xim - xip), intl = (xi - xim) / (xip - xim);
+            const double gw0  = gtil_w(lev);
+            const double gw1  = (lev < nv - 1) ? gtil_w(lev + 1) : 0.0;
+            s.gtil[i]         = gw0 * intt + gw1 * intl;
+        }
+        if (lev == nv - 1) { // top boundary and the bottom extrapolations (thor_auxiliary.h:188-258)
+            const ColLevel lo2  = col_level(s, Np, nv - 2, c);
+            const ColLevel top  = q;
+            const double   extr = (2 * Alth[nv] - alt - Alt[nv - 2]) / (Alt[nv - 1] - Alt[nv - 2]);
+            s.hh[nv * Np + c]   = h;
+            double pp;
+            if (ghv)
+                pp = lo2.p - top.rho * Gravit * pow(A / (A + Alt[nv]), 2) * (2 * Alth[nv] - alt - Alt[nv - 2]);
+            else
+                pp = lo2.p - top.rho * Gravit * (2 * Alth[nv] - alt - Alt[nv - 2]);
             if (pp < 0)
                 pp = 0;
-            rhop = Rk[top2] + (Rk[top] - Rk[top2]) * extr;
-            rhoh = 0.5 * (rho + rhop);
+            const double rhop = lo2.rho + (top.rho - lo2.rho) * extr;
+            const double rhoh = 0.5 * (top.rho + rhop);
             if (eeq) {
                 if (ghv) {
                     s.eph[nv * Np + c] = Gravit * pow(A / (A + Alth[nv]), 2) * Alth[nv];
@@ -291,129 +384,73 @@ __global__ void __launch_bounds__(kColBlock) adv_temp_kernel(Geometry g, Phys P,
                     s.eph[nv * Np + c] = Gravit * Alth[nv];
                     s.eph[c]           = Gravit * Alth[0];
                 }
-                s.ekh[nv * Np + c] = s.ek[top2] + (s.ek[top] - s.ek[top2]) * extr;
-                s.ekh[c] = s.ek[Np + c] + (s.ek[Np + c] - s.ek[c]) * (Alth[0] - Alt[1]) / (Alt[1] - Alt[0]);
+                const double ek2 = ekin(nv - 2), ek0 = ekin(0), ek1 = ekin(1);
+                s.ekh[nv * Np + c] = ek2 + (ek - ek2) * extr;
+                s.ekh[c]           = ek1 + (ek1 - ek0) * (Alth[0] - Alt[1]) / (Alt[1] - Alt[0]);
             }
             else {
-                s.pth[nv * Np + c] = s.pt[top2] + (s.pt[top] - s.pt[top2]) * extr;
-                s.pth[c] = s.pt[Np + c] + (s.pt[Np + c] - s.pt[c]) * (Alth[0] - Alt[1]) / (Alt[1] - Alt[0]);
+                const double pt2 = pot_temp(lo2, P_Ref);
+                const double pt0 = pot_temp(col_level(s, Np, 0, c), P_Ref);
+                const double pt1 = pot_temp(col_level(s, Np, 1, c), P_Ref);
+                s.pth[nv * Np + c] = pt2 + (pt - pt2) * extr;
+                s.pth[c]           = pt1 + (pt1 - pt0) * (Alth[0] - Alt[1]) / (Alt[1] - Alt[0]);
             }
-            dz = 2.0 * (Alth[nv] - Alt[nv - 1]);
+            const double dzt = 2.0 * (Alth[nv] - Alt[nv - 1]);
+            double       pp2;
             if (ghv)
-                pp = Pk[top2] - Rk[top] * Gravit * pow(A / (A + Alt[nv - 1]), 2)
-                                    * (2 * Alth[nv] - Alt[nv - 1] - Alt[nv - 2]);
+                pp2 = lo2.p - top.rho * Gravit * pow(A / (A + Alt[nv - 1]), 2)
+                                  * (2 * Alth[nv] - Alt[nv - 1] - Alt[nv - 2]);
             else
-                pp = Pk[top2] - Rk[top] * Gravit * (2 * Alth[nv] - Alt[nv - 1] - Alt[nv - 2]);
-            dpdz                = (pp - Pk[top]) / dz;
+                pp2 = lo2.p - top.rho * Gravit * (2 * Alth[nv] - Alt[nv - 1] - Alt[nv - 2]);
+            const double dpdz    = (pp2 - top.p) / dzt;
             s.gtilh[nv * Np + c] = -(1.0 / rhoh) * dpdz;
-            gtilht              = 0.0;
-            xi                  = alt;
-            xim                 = alth;
-            xip                 = altht;
-            intt                = (xi - xip) / (xim - xip);
-            intl                = (xi - xim) / (xip - xim);
-            s.gtil[top]         = gtilh_ * intt + gtilht * intl;
-        }
-        else {
-            dz    = alt - altl;
-            dp_dz = (pressure - pl) / dz;
-            xi    = alth;
-            xim   = altl;
-            xip   = alt;
-            intt  = (xi - xip) / (xim - xip);
-            intl  = (xi - xim) / (xip - xim);
-            s.hh[lev * Np + c] = hl * intt + h_ * intl;
-            if (eeq) {
-                s.eph[lev * Np + c] = epl * intt + ep * intl;
-                s.ekh[lev * Np + c] = ekl * intt + ek * intl;
-            }
-            else
-                s.pth[lev * Np + c] = ptl * intt + pt_ * intl;
-            rhoh   = rhol * intt + rho * intl;
-            gtilht = -(s.Whk[lev * Np + c] / rhoh) * dp_dz;
-            xi     = alt;
-            xim    = alth;
-            xip    = altht;
-            intt   = (xi - xip) / (xim - xip);
-            intl   = (xi - xim) / (xip - xim);
-            s.gtil[(lev - 1) * Np + c] = gtilh_ * intt + gtilht * intl;
-            gtilh_                     = gtilht;
-            s.gtilh[lev * Np + c]      = -(1.0 / rhoh) * dp_dz;
         }
     }
 }
 
 // ---------------------------------------------------------------------------------------------
-// Geometry of the FV Laplacian / divergence damping of one column, held in registers.
+// FV Laplacian around a ring of n neighbours (Diffusion_Op, src/headers/dyn/thor_diff.h:306-451;
+// the pole kernel :735-820 is the same sequence with a five-entry ring).
 // ---------------------------------------------------------------------------------------------
-struct RingGeo {
-    double ar[18], at[6], ti[18], te[18], oa[18];
-    int    ring[6];
-    int    n;
-    bool   pole;
-};
-
-__device__ __forceinline__ void load_ring_geo(const Geometry& g, int c, RingGeo& r) {
-    const int Np = g.Np;
-    for (int q = 0; q < 18; q++) {
-        r.ar[q] = g.areas[q * Np + c];
-        r.ti[q] = g.nvecti[q * Np + c];
-        r.te[q] = g.nvecte[q * Np + c];
-        r.oa[q] = g.nvecoa[q * Np + c];
-    }
-    for (int j = 0; j < 6; j++) {
-        r.at[j]   = g.areasTr[j * Np + c];
-        r.ring[j] = g.ring[j * Np + c];
-    }
-    uint8_t f = g.cflag[c];
-    r.n       = (f & kRing5) ? 5 : 6;
-    r.pole    = (f & kPole) != 0;
-}
-
-// One FV Laplacian (Diffusion_Op, src/headers/dyn/thor_diff.h:306-451; the pole kernel :735-820
-// is the same sequence with a five-entry ring).
-__device__ __forceinline__ double laplacian(const RingGeo& r, const double* a, double a0,
+template<int n>
+__device__ __forceinline__ double laplacian(const SGeo& G, const double* a, double a0,
                                             double rscale) {
-    const int n   = r.n;
-    double    lap = 0.0;
-    double    lap1 = 0, lap2 = 0, lap3 = 0, lapx1 = 0, lapx2 = 0, lapy1 = 0, lapy2 = 0, lapz1 = 0,
+    double lap = 0.0;
+    double lap1 = 0, lap2 = 0, lap3 = 0, lapx1 = 0, lapx2 = 0, lapy1 = 0, lapy2 = 0, lapz1 = 0,
            lapz2 = 0, AT1 = 0;
 #pragma unroll
-    for (int j = 0; j < 6; j++) {
-        if (j >= n)
-            break;
-        const int    jp1 = (j + 1 == n) ? 0 : j + 1;
-        const int    jp2 = (jp1 + 1 == n) ? 0 : jp1 + 1;
+    for (int j = 0; j < n; j++) {
+        const int    jp1 = (j + 1) % n, jp2 = (j + 2) % n;
         const double p1 = a[j], p2 = a[jp1], p3 = a[jp2];
         const double vdiff = 0.5 * rscale;
         double       astar;
         if (j == 0) {
-            AT1   = rscale / r.at[j];
-            astar = (r.ar[j * 3 + 0] * a0 + r.ar[j * 3 + 1] * p1 + r.ar[j * 3 + 2] * p2) / r.at[j];
+            AT1   = rscale / G.AT(j);
+            astar = (G.AR(j * 3 + 0) * a0 + G.AR(j * 3 + 1) * p1 + G.AR(j * 3 + 2) * p2) / G.AT(j);
             lap1  = (0.5 * (p1 + a0) - astar);
             lap2  = (0.5 * (p1 + p2) - astar);
             lap3  = (0.5 * (a0 + p2) - astar);
         }
-        const double AT2 = rscale / r.at[jp1];
-        astar = (r.ar[jp1 * 3 + 0] * a0 + r.ar[jp1 * 3 + 1] * p2 + r.ar[jp1 * 3 + 2] * p3) / r.at[jp1];
+        const double AT2 = rscale / G.AT(jp1);
+        astar = (G.AR(jp1 * 3 + 0) * a0 + G.AR(jp1 * 3 + 1) * p2 + G.AR(jp1 * 3 + 2) * p3) / G.AT(jp1);
         const double lap4 = (0.5 * (a0 + p2) - astar);
         const double lap5 = (0.5 * (p2 + p3) - astar);
         const double lap6 = (0.5 * (a0 + p3) - astar);
         if (j == 0) {
-            lapx1 = (-lap1 * r.ti[j * 3 + 0] + lap2 * r.te[j * 3 + 0] + lap3 * r.ti[jp1 * 3 + 0]) * AT1;
-            lapy1 = (-lap1 * r.ti[j * 3 + 1] + lap2 * r.te[j * 3 + 1] + lap3 * r.ti[jp1 * 3 + 1]) * AT1;
-            lapz1 = (-lap1 * r.ti[j * 3 + 2] + lap2 * r.te[j * 3 + 2] + lap3 * r.ti[jp1 * 3 + 2]) * AT1;
+            lapx1 = (-lap1 * G.TI(j * 3 + 0) + lap2 * G.TE(j * 3 + 0) + lap3 * G.TI(jp1 * 3 + 0)) * AT1;
+            lapy1 = (-lap1 * G.TI(j * 3 + 1) + lap2 * G.TE(j * 3 + 1) + lap3 * G.TI(jp1 * 3 + 1)) * AT1;
+            lapz1 = (-lap1 * G.TI(j * 3 + 2) + lap2 * G.TE(j * 3 + 2) + lap3 * G.TI(jp1 * 3 + 2)) * AT1;
         }
         else {
             lapx1 = lapx2;
             lapy1 = lapy2;
             lapz1 = lapz2;
         }
-        lapx2 = (-lap4 * r.ti[jp1 * 3 + 0] + lap5 * r.te[jp1 * 3 + 0] + lap6 * r.ti[jp2 * 3 + 0]) * AT2;
-        lapy2 = (-lap4 * r.ti[jp1 * 3 + 1] + lap5 * r.te[jp1 * 3 + 1] + lap6 * r.ti[jp2 * 3 + 1]) * AT2;
-        lapz2 = (-lap4 * r.ti[jp1 * 3 + 2] + lap5 * r.te[jp1 * 3 + 2] + lap6 * r.ti[jp2 * 3 + 2]) * AT2;
-        lap += ((lapx1 + lapx2) * r.oa[j * 3 + 0] + (lapy1 + lapy2) * r.oa[j * 3 + 1]
-                + (lapz1 + lapz2) * r.oa[j * 3 + 2])
+        lapx2 = (-lap4 * G.TI(jp1 * 3 + 0) + lap5 * G.TE(jp1 * 3 + 0) + lap6 * G.TI(jp2 * 3 + 0)) * AT2;
+        lapy2 = (-lap4 * G.TI(jp1 * 3 + 1) + lap5 * G.TE(jp1 * 3 + 1) + lap6 * G.TI(jp2 * 3 + 1)) * AT2;
+        lapz2 = (-lap4 * G.TI(jp1 * 3 + 2) + lap5 * G.TE(jp1 * 3 + 2) + lap6 * G.TI(jp2 * 3 + 2)) * AT2;
+        lap += ((lapx1 + lapx2) * G.OA(j * 3 + 0) + (lapy1 + lapy2) * G.OA(j * 3 + 1)
+                + (lapz1 + lapz2) * G.OA(j * 3 + 2))
                * vdiff;
     }
     return lap;
@@ -428,111 +465,141 @@ __device__ __forceinline__ double laplacian(const RingGeo& r, const double* a, d
 //   final pass (last)     : argument = diff (rho-weighted for v, w, T), scaled by -Kdh4 (-1)^(o/2)
 //                            -> diffrh, diffmh(3), diffw, diffpr
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(kStenBlock)
-    diffusion_kernel(Geometry g, Phys P, State s, const double* __restrict__ diff_in,
-                     double* __restrict__ diff_out, int stepnum, bool last) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= g.N)
-        return;
-    const int Np = g.Np, nv = g.nv;
-    const int lev0 = blockIdx.y * kLevChunk;
-    const int lev1 = min(lev0 + kLevChunk, nv);
-    RingGeo   r;
-    load_ring_geo(g, c, r);
-    double fr[3];
-    for (int k = 0; k < 3; k++)
-        fr[k] = g.func_r[k * Np + c];
-    const bool eeq = P.energy;
-
-    for (int lev = lev0; lev < lev1; lev++) {
-        const double rscale = rscale_of(P, g, lev);
-        const double sdiff  = -g.Kdh4[lev] * pow(-1.0, P.HyDiffOrder / 2);
-        double       rho_r[6], rho0 = s.Rhok[lev * Np + c];
-        for (int j = 0; j < r.n; j++)
-            rho_r[j] = gz(s.Rhok + lev * Np, r.ring[j]);
-        double out[6];
-        for (int var = 0; var < 6; var++) {
-            // argument of the Laplacian at a column id (hole -> 0) with density rho
-            auto arg = [&](int id, double rho) -> double {
-                if (id < 0)
-                    return 0.0;
-                const int i = lev * Np + id;
-                double    x;
+template<int n>
+__device__ __forceinline__ void diffusion_point(const Geometry& g, const Phys& P, const State& s,
+                                                const SGeo& G, const double* fr, const int* ring,
+                                                const double* __restrict__ diff_in,
+                                                double* __restrict__ diff_out, int stepnum,
+                                                bool last, int c, int lev) {
+    const int    Np = g.Np, nv = g.nv;
+    const double rscale = rscale_of(P, g, lev);
+    const double sdiff  = -g.Kdh4[lev] * pow(-1.0, P.HyDiffOrder / 2);
+    const bool   eeq    = P.energy;
+    int          ids[n + 1];
+    double       rho[n + 1];
+    ids[0] = c;
+#pragma unroll
+    for (int j = 0; j < n; j++)
+        ids[j + 1] = ring[j];
+#pragma unroll
+    for (int j = 0; j <= n; j++)
+        rho[j] = gz(s.Rhok + lev * Np, ids[j]);
+    const int i = lev * Np + c;
+    double    m1 = 0, m2 = 0, m3 = 0; // momentum results, combined after the third
+#pragma unroll 1
+    for (int var = 0; var < 6; var++) {
+        double a[n + 1];
+#pragma unroll
+        for (int j = 0; j <= n; j++) {
+            const int id = ids[j];
+            double    v  = 0.0;
+            if (id >= 0) {
+                const int q = lev * Np + id;
                 if (stepnum == 0) {
                     if (var == 0)
-                        x = s.Rhok[i];
+                        v = s.Rhok[q];
                     else if (var <= 3)
-                        x = s.Mhk[((var - 1) * nv + lev) * Np + id];
+                        v = s.Mhk[((var - 1) * nv + lev) * Np + id];
                     else if (var == 4)
-                        x = s.Wk[i];
+                        v = s.Wk[q];
                     else
-                        x = eeq ? (s.Cp[i] - s.Rd[i]) * s.T[i] : s.Rd[i] * s.T[i];
+                        v = eeq ? (s.Cp[q] - s.Rd[q]) * s.T[q] : s.Rd[q] * s.T[q];
                     if (var >= 1 && var <= 4)
-                        x = x / rho;
+                        v = v / rho[j];
                 }
                 else if (last)
-                    x = (var == 0) ? diff_in[(var * nv + lev) * Np + id]
-                                   : diff_in[(var * nv + lev) * Np + id] * rho;
+                    v = (var == 0) ? diff_in[(var * nv + lev) * Np + id]
+                                   : diff_in[(var * nv + lev) * Np + id] * rho[j];
                 else
-                    x = diff_in[(var * nv + lev) * Np + id];
-                return x;
-            };
-            double a[6];
-            for (int j = 0; j < r.n; j++)
-                a[j] = arg(r.ring[j], rho_r[j]);
-            double lap = laplacian(r, a, arg(c, rho0), rscale);
-            if (last)
-                lap *= sdiff;
-            out[var] = lap;
+                    v = diff_in[(var * nv + lev) * Np + id];
+            }
+            a[j] = v;
         }
-        const int i = lev * Np + c;
-        if (last) {
-            s.diffrh[i] = out[0];
+        double lap = laplacian<n>(G, a + 1, a[0], rscale);
+        if (!last) {
+            diff_out[(var * nv + lev) * Np + c] = lap;
+            continue;
+        }
+        lap *= sdiff;
+        if (var == 0)
+            s.diffrh[i] = lap;
+        else if (var == 1)
+            m1 = lap;
+        else if (var == 2)
+            m2 = lap;
+        else if (var == 3) {
+            m3 = lap;
             // Correct_Horizontal: remove the radial component of the momentum diffusion
-            double dmhr = fr[0] * out[1] + fr[1] * out[2] + fr[2] * out[3];
-            for (int k = 0; k < 3; k++)
-                s.diffmh[(k * nv + lev) * Np + c] = out[1 + k] + -fr[k] * dmhr;
-            s.diffw[i]  = out[4];
-            s.diffpr[i] = out[5];
+            const double dmhr = fr[0] * m1 + fr[1] * m2 + fr[2] * m3;
+            s.diffmh[(0 * nv + lev) * Np + c] = m1 + -fr[0] * dmhr;
+            s.diffmh[(1 * nv + lev) * Np + c] = m2 + -fr[1] * dmhr;
+            s.diffmh[(2 * nv + lev) * Np + c] = m3 + -fr[2] * dmhr;
         }
-        else {
-            for (int var = 0; var < 6; var++)
-                diff_out[(var * nv + lev) * Np + c] = out[var];
-        }
+        else if (var == 4)
+            s.diffw[i] = lap;
+        else
+            s.diffpr[i] = lap;
     }
+}
+
+template<int n>
+__device__ __forceinline__ void diffusion_body(const Geometry& g, const Phys& P, const State& s,
+                                               const SGeo& G, const double* __restrict__ diff_in,
+                                               double* __restrict__ diff_out, int stepnum,
+                                               bool last, int c) {
+    const int Np = g.Np;
+    double    fr[3];
+    for (int k = 0; k < 3; k++)
+        fr[k] = g.func_r[k * Np + c];
+    int ring[6];
+    for (int j = 0; j < 6; j++)
+        ring[j] = g.ring[j * Np + c];
+    for (int lev = threadIdx.y; lev < g.nv; lev += kLevGroups)
+        diffusion_point<n>(g, P, s, G, fr, ring, diff_in, diff_out, stepnum, last, c, lev);
+}
+
+__global__ void __launch_bounds__(kTile* kLevGroups)
+    diffusion_kernel(Geometry g, Phys P, State s, const double* __restrict__ diff_in,
+                     double* __restrict__ diff_out, int stepnum, bool last) {
+    __shared__ double sgeo[kRingGeoRows * kTile];
+    const int         c = lane_column(g);
+    const SGeo        G = stage_ring_geo(sgeo, g, c);
+    __syncthreads();
+    if (c < 0)
+        return;
+    if (tail_cta())
+        diffusion_body<5>(g, P, s, G, diff_in, diff_out, stepnum, last, c);
+    else
+        diffusion_body<6>(g, P, s, G, diff_in, diff_out, stepnum, last, c);
 }
 
 // ---------------------------------------------------------------------------------------------
 // Divergence damping (DivM_Op / DivM_Op_Poles, src/headers/dyn/thor_div.h:49-535).
 // Pass 0: grad of the 3D divergence of (Mh, Wh) -> divg; pass 1 (divm_final): the tangential
 // part of grad(div) of divg scaled by -Kdhz. The poles' corner mean of w uses the second
-// sub-area in place of the third (thor_div.h:443-454), restated as it is.
+// sub-area in place of the third (thor_div.h:443-454), restated as it is (c2 = 1).
 // ---------------------------------------------------------------------------------------------
-__device__ __forceinline__ void divm_core(const RingGeo& r, const double* a0, const double (*ar)[3],
+template<int n>
+__device__ __forceinline__ void divm_core(const SGeo& G, const double* a0, const double (*ar)[3],
                                           bool with_w, double wl0, double wt0, const double* wl,
-                                          const double* wt, double dz, double rscale,
+                                          const double* wt, double dz, double rscale, int c2,
                                           double* lapo) {
-    const int n   = r.n;
-    double    AT0 = 0.5 * rscale;
-    double    lapx = 0.0, lapy = 0.0, lapz = 0.0;
-    double    a01x = 0, a01y = 0, a01z = 0, a12x = 0, a12y = 0, a12z = 0, AT1 = 0, lap1 = 0,
+    const double AT0 = 0.5 * rscale;
+    double       lapx = 0.0, lapy = 0.0, lapz = 0.0;
+    double       a01x = 0, a01y = 0, a01z = 0, a12x = 0, a12y = 0, a12z = 0, AT1 = 0, lap1 = 0,
            lap2 = 0;
-    const int c2 = r.pole ? 1 : 2;
 #pragma unroll
-    for (int j = 0; j < 6; j++) {
-        if (j >= n)
-            break;
-        const int     jp1 = (j + 1 == n) ? 0 : j + 1;
-        const int     jp2 = (jp1 + 1 == n) ? 0 : jp1 + 1;
+    for (int j = 0; j < n; j++) {
+        const int     jp1 = (j + 1) % n, jp2 = (j + 2) % n;
         const double *p1 = ar[j], *p2 = ar[jp1], *p3 = ar[jp2];
         double        dwdz = 0.0, dwdz2 = 0.0;
         if (with_w) {
-            double meanwl  = (r.ar[j * 3 + 0] * wl0 + r.ar[j * 3 + 1] * wl[j] + r.ar[j * 3 + c2] * wl[jp1]) / r.at[j];
-            double meanwt  = (r.ar[j * 3 + 0] * wt0 + r.ar[j * 3 + 1] * wt[j] + r.ar[j * 3 + c2] * wt[jp1]) / r.at[j];
-            double meanwl2 = (r.ar[jp1 * 3 + 0] * wl0 + r.ar[jp1 * 3 + 1] * wl[jp1] + r.ar[jp1 * 3 + c2] * wl[jp2]) / r.at[jp1];
-            double meanwt2 = (r.ar[jp1 * 3 + 0] * wt0 + r.ar[jp1 * 3 + 1] * wt[jp1] + r.ar[jp1 * 3 + c2] * wt[jp2]) / r.at[jp1];
-            dwdz           = (meanwl - meanwt) * dz;
-            dwdz2          = (meanwl2 - meanwt2) * dz;
+            const double meanwl = (G.AR(j * 3 + 0) * wl0 + G.AR(j * 3 + 1) * wl[j] + G.AR(j * 3 + c2) * wl[jp1]) / G.AT(j);
+            const double meanwt = (G.AR(j * 3 + 0) * wt0 + G.AR(j * 3 + 1) * wt[j] + G.AR(j * 3 + c2) * wt[jp1]) / G.AT(j);
+            const double meanwl2 = (G.AR(jp1 * 3 + 0) * wl0 + G.AR(jp1 * 3 + 1) * wl[jp1] + G.AR(jp1 * 3 + c2) * wl[jp2]) / G.AT(jp1);
+            const double meanwt2 = (G.AR(jp1 * 3 + 0) * wt0 + G.AR(jp1 * 3 + 1) * wt[jp1] + G.AR(jp1 * 3 + c2) * wt[jp2]) / G.AT(jp1);
+            dwdz  = (meanwl - meanwt) * dz;
+            dwdz2 = (meanwl2 - meanwt2) * dz;
         }
         if (j == 0) {
             a01x = (a0[0] + p1[0]);
@@ -541,84 +608,113 @@ __device__ __forceinline__ void divm_core(const RingGeo& r, const double* a0, co
             a12x = (p1[0] + p2[0]);
             a12y = (p1[1] + p2[1]);
             a12z = (p1[2] + p2[2]);
-            AT1  = 0.5 * rscale / r.at[j];
+            AT1  = 0.5 * rscale / G.AT(j);
         }
-        const double AT2  = 0.5 * rscale / r.at[jp1];
+        const double AT2  = 0.5 * rscale / G.AT(jp1);
         const double a02x = (a0[0] + p2[0]), a02y = (a0[1] + p2[1]), a02z = (a0[2] + p2[2]);
         const double a23x = (p2[0] + p3[0]), a23y = (p2[1] + p3[1]), a23z = (p2[2] + p3[2]);
         const double a03x = (a0[0] + p3[0]), a03y = (a0[1] + p3[1]), a03z = (a0[2] + p3[2]);
-        const double* ti = r.ti;
-        const double* te = r.te;
         if (j == 0)
-            lap1 = (-a01x * ti[j * 3 + 0] - a01y * ti[j * 3 + 1] - a01z * ti[j * 3 + 2]
-                    + a12x * te[j * 3 + 0] + a12y * te[j * 3 + 1] + a12z * te[j * 3 + 2]
-                    + a02x * ti[jp1 * 3 + 0] + a02y * ti[jp1 * 3 + 1] + a02z * ti[jp1 * 3 + 2])
+            lap1 = (-a01x * G.TI(j * 3 + 0) - a01y * G.TI(j * 3 + 1) - a01z * G.TI(j * 3 + 2)
+                    + a12x * G.TE(j * 3 + 0) + a12y * G.TE(j * 3 + 1) + a12z * G.TE(j * 3 + 2)
+                    + a02x * G.TI(jp1 * 3 + 0) + a02y * G.TI(jp1 * 3 + 1) + a02z * G.TI(jp1 * 3 + 2))
                    * AT1;
         else
             lap1 = lap2;
-        lap2 = (-a02x * ti[jp1 * 3 + 0] - a02y * ti[jp1 * 3 + 1] - a02z * ti[jp1 * 3 + 2]
-                + a23x * te[jp1 * 3 + 0] + a23y * te[jp1 * 3 + 1] + a23z * te[jp1 * 3 + 2]
-                + a03x * ti[jp2 * 3 + 0] + a03y * ti[jp2 * 3 + 1] + a03z * ti[jp2 * 3 + 2])
+        lap2 = (-a02x * G.TI(jp1 * 3 + 0) - a02y * G.TI(jp1 * 3 + 1) - a02z * G.TI(jp1 * 3 + 2)
+                + a23x * G.TE(jp1 * 3 + 0) + a23y * G.TE(jp1 * 3 + 1) + a23z * G.TE(jp1 * 3 + 2)
+                + a03x * G.TI(jp2 * 3 + 0) + a03y * G.TI(jp2 * 3 + 1) + a03z * G.TI(jp2 * 3 + 2))
                * AT2;
-        lapx += (lap1 + dwdz + lap2 + dwdz2) * r.oa[j * 3 + 0] * AT0;
-        lapy += (lap1 + dwdz + lap2 + dwdz2) * r.oa[j * 3 + 1] * AT0;
-        lapz += (lap1 + dwdz + lap2 + dwdz2) * r.oa[j * 3 + 2] * AT0;
+        lapx += (lap1 + dwdz + lap2 + dwdz2) * G.OA(j * 3 + 0) * AT0;
+        lapy += (lap1 + dwdz + lap2 + dwdz2) * G.OA(j * 3 + 1) * AT0;
+        lapz += (lap1 + dwdz + lap2 + dwdz2) * G.OA(j * 3 + 2) * AT0;
     }
     lapo[0] = lapx;
     lapo[1] = lapy;
     lapo[2] = lapz;
 }
 
+template<int n>
+__device__ __forceinline__ void divm0_point(const Geometry& g, const Phys& P, const SGeo& G,
+                                            const int* ring, int c2, const double* __restrict__ Mh,
+                                            const double* __restrict__ Wh,
+                                            double* __restrict__ divg, int c, int lev) {
+    const int    Np = g.Np, nv = g.nv;
+    const double rscale = rscale_of(P, g, lev);
+    const double dz     = 1.0 / (g.Altitudeh[lev] - g.Altitudeh[lev + 1]);
+    double       a0[3], ar[n][3], wl[n], wt[n];
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+        a0[k] = Mh[(k * nv + lev) * Np + c];
+#pragma unroll
+    for (int j = 0; j < n; j++) {
+#pragma unroll
+        for (int k = 0; k < 3; k++)
+            ar[j][k] = gz(Mh + (k * nv + lev) * Np, ring[j]);
+        wl[j] = gz(Wh + lev * Np, ring[j]);
+        wt[j] = gz(Wh + (lev + 1) * Np, ring[j]);
+    }
+    double out[3];
+    divm_core<n>(G, a0, ar, true, Wh[lev * Np + c], Wh[(lev + 1) * Np + c], wl, wt, dz, rscale, c2,
+                 out);
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+        divg[(k * nv + lev) * Np + c] = out[k];
+}
+
 // Pass 0 of the divergence damping on (Mh, Wh) -> divg.
-__global__ void __launch_bounds__(kStenBlock)
+template<int n>
+__device__ __forceinline__ void divm0_body(const Geometry& g, const Phys& P, const SGeo& G,
+                                           const double* __restrict__ Mh,
+                                           const double* __restrict__ Wh,
+                                           double* __restrict__ divg, int c) {
+    const int Np = g.Np;
+    int       ring[6];
+    for (int j = 0; j < 6; j++)
+        ring[j] = g.ring[j * Np + c];
+    const int c2 = (g.cflag[c] & kPole) ? 1 : 2;
+    for (int lev = threadIdx.y; lev < g.nv; lev += kLevGroups)
+        divm0_point<n>(g, P, G, ring, c2, Mh, Wh, divg, c, lev);
+}
+
+__global__ void __launch_bounds__(kTile* kLevGroups)
     divm0_kernel(Geometry g, Phys P, const double* __restrict__ Mh, const double* __restrict__ Wh,
                  double* __restrict__ divg) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= g.N)
+    __shared__ double sgeo[kRingGeoRows * kTile];
+    const int         c = lane_column(g);
+    const SGeo        G = stage_ring_geo(sgeo, g, c);
+    __syncthreads();
+    if (c < 0)
         return;
-    const int Np = g.Np, nv = g.nv;
-    const int lev0 = blockIdx.y * kLevChunk;
-    const int lev1 = min(lev0 + kLevChunk, nv);
-    RingGeo   r;
-    load_ring_geo(g, c, r);
-    for (int lev = lev0; lev < lev1; lev++) {
-        const double rscale = rscale_of(P, g, lev);
-        const double dz     = 1.0 / (g.Altitudeh[lev] - g.Altitudeh[lev + 1]);
-        double       a0[3], ar[6][3], wl[6], wt[6];
-        for (int k = 0; k < 3; k++)
-            a0[k] = Mh[(k * nv + lev) * Np + c];
-        for (int j = 0; j < r.n; j++) {
-            for (int k = 0; k < 3; k++)
-                ar[j][k] = gz(Mh + (k * nv + lev) * Np, r.ring[j]);
-            wl[j] = gz(Wh + lev * Np, r.ring[j]);
-            wt[j] = gz(Wh + (lev + 1) * Np, r.ring[j]);
-        }
-        double out[3];
-        divm_core(r, a0, ar, true, Wh[lev * Np + c], Wh[(lev + 1) * Np + c], wl, wt, dz, rscale,
-                  out);
-        for (int k = 0; k < 3; k++)
-            divg[(k * nv + lev) * Np + c] = out[k];
-    }
+    if (tail_cta())
+        divm0_body<5>(g, P, G, Mh, Wh, divg, c);
+    else
+        divm0_body<6>(g, P, G, Mh, Wh, divg, c);
 }
 
 // Pass 1 of the divergence damping at (column, level): DivM from divg.
-__device__ __forceinline__ void divm_final(const Geometry& g, const Phys& P, const RingGeo& r,
-                                           const double* __restrict__ divg, int c, int lev,
-                                           const double* fr, double* DivM) {
+template<int n>
+__device__ __forceinline__ void divm_final(const Geometry& g, const Phys& P, const SGeo& G,
+                                           const int* ring, const double* __restrict__ divg, int c,
+                                           int lev, const double* fr, double* DivM) {
     const int Np = g.Np, nv = g.nv;
-    double    a0[3], ar[6][3];
+    double    a0[3], ar[n][3];
+#pragma unroll
     for (int k = 0; k < 3; k++)
         a0[k] = divg[(k * nv + lev) * Np + c];
-    for (int j = 0; j < r.n; j++)
+#pragma unroll
+    for (int j = 0; j < n; j++)
+#pragma unroll
         for (int k = 0; k < 3; k++)
-            ar[j][k] = gz(divg + (k * nv + lev) * Np, r.ring[j]);
+            ar[j][k] = gz(divg + (k * nv + lev) * Np, ring[j]);
     double lap[3];
-    divm_core(r, a0, ar, false, 0, 0, nullptr, nullptr, 0, rscale_of(P, g, lev), lap);
+    divm_core<n>(G, a0, ar, false, 0, 0, nullptr, nullptr, 0, rscale_of(P, g, lev), 2, lap);
     const double sdiff = g.Kdhz[lev];
     const double lapr  = fr[0] * lap[0] + fr[1] * lap[1] + fr[2] * lap[2];
+#pragma unroll
     for (int k = 0; k < 3; k++) {
-        double l = lap[k] - fr[k] * lapr;
-        DivM[k]  = -l * sdiff;
+        const double l = lap[k] - fr[k] * lapr;
+        DivM[k]        = -l * sdiff;
     }
 }
 
@@ -628,37 +724,29 @@ __device__ __forceinline__ void divm_final(const Geometry& g, const Phys& P, con
 // (src/headers/dyn/thor_auxiliary.h:311-418, without module arrays and without the never-read
 // Ws). DivM is consumed where it is produced and not stored.
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(kStenBlock)
-    slow_modes_kernel(Geometry g, Phys P, State s, bool update_rk) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= g.N)
-        return;
-    const int Np = g.Np, nv = g.nv;
-    const int lev0 = blockIdx.y * kLevChunk;
-    const int lev1 = min(lev0 + kLevChunk, nv);
+template<int n>
+__device__ __forceinline__ void slow_modes_body(const Geometry& g, const Phys& P, const State& s,
+                                                const SGeo& G, const double* sdiv,
+                                                const double* sgrad, bool update_rk, int c) {
+    const int    x = threadIdx.x;
+    const int    Np = g.Np, nv = g.nv;
     const double A = P.A, Gravit = P.Gravit;
-    int          nb[7];
+    int          nb[7], ring[6];
     nb[0] = c;
-    for (int j = 0; j < 6; j++)
+    for (int j = 0; j < 6; j++) {
         nb[j + 1] = g.nb[j * Np + c];
-    double dv[21], gr[21], fr[3];
-    for (int q = 0; q < 21; q++) {
-        dv[q] = g.div[q * Np + c];
-        gr[q] = g.grad[q * Np + c];
+        ring[j]   = g.ring[j * Np + c];
     }
+    double fr[3];
     for (int k = 0; k < 3; k++)
         fr[k] = g.func_r[k * Np + c];
     const bool pole = (g.cflag[c] & kPole) != 0;
-    RingGeo    r;
-    if (P.DivDampP)
-        load_ring_geo(g, c, r);
 
-    for (int lev = lev0; lev < lev1; lev++) {
-        const int i = lev * Np + c;
+    for (int lev = threadIdx.y; lev < nv; lev += kLevGroups) {
+        const int i       = lev * Np + c;
         double    DivM[3] = {0.0, 0.0, 0.0};
         if (P.DivDampP)
-            divm_final(g, P, r, s.divg, c, lev, fr, DivM);
-
+            divm_final<n>(g, P, G, ring, s.divg, c, lev, fr, DivM);
         const double Cv = s.Cp[i] - s.Rd[i];
         double       adv[3];
         for (int k = 0; k < 3; k++)
@@ -701,19 +789,24 @@ __global__ void __launch_bounds__(kStenBlock)
         }
         // horizontal stencils at this level
         double pv[7], hv[7], Mv[7][3];
+#pragma unroll
         for (int j = 0; j < 7; j++) {
             pv[j] = gz(s.pk + lev * Np, nb[j]);
             hv[j] = gz(s.h + lev * Np, nb[j]);
+#pragma unroll
             for (int k = 0; k < 3; k++)
                 Mv[j][k] = gz(s.Mhk + (k * nv + lev) * Np, nb[j]);
         }
         double nflxv[3], nflxr = 0.0, nflxp = 0.0;
+#pragma unroll
         for (int k = 0; k < 3; k++) {
-            double sg = gr[k] * pv[0], sd = dv[k] * Mv[0][k], sp = dv[k] * Mv[0][k] * hv[0];
+            double sg = sgrad[k * kTile + x] * pv[0], sd = sdiv[k * kTile + x] * Mv[0][k],
+                   sp = sdiv[k * kTile + x] * Mv[0][k] * hv[0];
+#pragma unroll
             for (int j = 1; j < 7; j++) {
-                sg = sg + gr[j * 3 + k] * pv[j];
-                sd = sd + dv[j * 3 + k] * Mv[j][k];
-                sp = sp + dv[j * 3 + k] * Mv[j][k] * hv[j];
+                sg = sg + sgrad[(j * 3 + k) * kTile + x] * pv[j];
+                sd = sd + sdiv[(j * 3 + k) * kTile + x] * Mv[j][k];
+                sp = sp + sdiv[(j * 3 + k) * kTile + x] * Mv[j][k] * hv[j];
             }
             nflxv[k] = rscale * sg;
             nflxr += rscale * sd;
@@ -744,9 +837,9 @@ __global__ void __launch_bounds__(kStenBlock)
             s.SlowWh[nv * Np + c] = 0.0;
         }
         else {
-            double xi = althl, xim = altl, xip = alt;
-            double intt = (xi - xip) / (xim - xip), intl = (xi - xim) / (xip - xim);
-            double swr;
+            const double xi = althl, xim = altl, xip = alt;
+            const double intt = (xi - xip) / (xim - xip), intl = (xi - xim) / (xip - xim);
+            double       swr;
             if (P.DeepModel) {
                 if (P.GravHeightVar)
                     swr = (advrl + rhol * Gravit * pow(A / (A + altl), 2)) * intt
@@ -770,8 +863,8 @@ __global__ void __launch_bounds__(kStenBlock)
             s.SlowWh[lev * Np + c] = -swr;
         }
         nflxr += dwdz;
-        s.SlowRho[i]   = -nflxr + s.diffrh[i];
-        const double r_ = 1.0 / rho;
+        s.SlowRho[i]     = -nflxr + s.diffrh[i];
+        const double r_  = 1.0 / rho;
         const double vgp = (nflxv[0] - dpr * fr[0]) * M0[0] * r_ + (nflxv[1] - dpr * fr[1]) * M0[1] * r_
                            + (nflxv[2] - dpr * fr[2]) * M0[2] * r_;
         double sp = (s.Rd[i] / Cv) * (-nflxp - s.gtil[i] - dwhdz + vgp + s.Qheat[i]);
@@ -783,10 +876,10 @@ __global__ void __launch_bounds__(kStenBlock)
 
         if (update_rk) {
             // deviations from the start of the large step
-            double Mx = s.Mh[(0 * nv + lev) * Np + c] - M0[0];
-            double My = s.Mh[(1 * nv + lev) * Np + c] - M0[1];
-            double Mz = s.Mh[(2 * nv + lev) * Np + c] - M0[2];
-            double aux = Mx * fr[0] + My * fr[1] + Mz * fr[2];
+            const double Mx  = s.Mh[(0 * nv + lev) * Np + c] - M0[0];
+            const double My  = s.Mh[(1 * nv + lev) * Np + c] - M0[1];
+            const double Mz  = s.Mh[(2 * nv + lev) * Np + c] - M0[2];
+            const double aux = Mx * fr[0] + My * fr[1] + Mz * fr[2];
             s.Mhs[(0 * nv + lev) * Np + c] = Mx - aux * fr[0];
             s.Mhs[(1 * nv + lev) * Np + c] = My - aux * fr[1];
             s.Mhs[(2 * nv + lev) * Np + c] = Mz - aux * fr[2];
@@ -799,45 +892,63 @@ __global__ void __launch_bounds__(kStenBlock)
     }
 }
 
+__global__ void __launch_bounds__(kTile* kLevGroups)
+    slow_modes_kernel(Geometry g, Phys P, State s, bool update_rk) {
+    __shared__ double sgeo[kRingGeoRows * kTile];
+    __shared__ double sdiv[21 * kTile];
+    __shared__ double sgrad[21 * kTile];
+    const int         c = lane_column(g);
+    SGeo              G{};
+    if (P.DivDampP)
+        G = stage_ring_geo(sgeo, g, c);
+    stage_cols(sdiv, g.div, 21, g.Np, c);
+    stage_cols(sgrad, g.grad, 21, g.Np, c);
+    __syncthreads();
+    if (c < 0)
+        return;
+    if (tail_cta())
+        slow_modes_body<5>(g, P, s, G, sdiv, sgrad, update_rk, c);
+    else
+        slow_modes_body<6>(g, P, s, G, sdiv, sgrad, update_rk, c);
+}
+
 // ---------------------------------------------------------------------------------------------
 // Small step, horizontal momentum: divergence-damping pass 1 on the deviations (Mhs, Whs) +
 // Momentum_Eq / _Poles (src/headers/dyn/thor_fastmodes.h:54-253).
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(kStenBlock)
-    momentum_kernel(Geometry g, Phys P, State s, double dt) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= g.N)
-        return;
+template<int n>
+__device__ __forceinline__ void momentum_body(const Geometry& g, const Phys& P, const State& s,
+                                              const SGeo& G, const double* sgrad, double dt,
+                                              int c) {
+    const int x = threadIdx.x;
     const int Np = g.Np, nv = g.nv;
-    const int lev0 = blockIdx.y * kLevChunk;
-    const int lev1 = min(lev0 + kLevChunk, nv);
-    int       nb[7];
+    int       nb[7], ring[6];
     nb[0] = c;
-    for (int j = 0; j < 6; j++)
+    for (int j = 0; j < 6; j++) {
         nb[j + 1] = g.nb[j * Np + c];
-    double gr[21], fr[3];
-    for (int q = 0; q < 21; q++)
-        gr[q] = g.grad[q * Np + c];
+        ring[j]   = g.ring[j * Np + c];
+    }
+    double fr[3];
     for (int k = 0; k < 3; k++)
         fr[k] = g.func_r[k * Np + c];
-    RingGeo r;
-    if (P.DivDampP)
-        load_ring_geo(g, c, r);
-    for (int lev = lev0; lev < lev1; lev++) {
+    for (int lev = threadIdx.y; lev < nv; lev += kLevGroups) {
         double DivM[3] = {0.0, 0.0, 0.0};
         if (P.DivDampP)
-            divm_final(g, P, r, s.divg, c, lev, fr, DivM);
+            divm_final<n>(g, P, G, ring, s.divg, c, lev, fr, DivM);
         const double rscale = rscale_of(P, g, lev);
         double       pv[7];
+#pragma unroll
         for (int j = 0; j < 7; j++)
             pv[j] = gz(s.ps + lev * Np, nb[j]);
         double Mv[3];
+#pragma unroll
         for (int k = 0; k < 3; k++) {
-            double sg = gr[k] * pv[0];
+            double sg = sgrad[k * kTile + x] * pv[0];
+#pragma unroll
             for (int j = 1; j < 7; j++)
-                sg = sg + gr[j * 3 + k] * pv[j];
-            double nflxv = rscale * sg;
-            Mv[k]        = (-nflxv + s.SlowMh[(k * nv + lev) * Np + c] + DivM[k]) * dt;
+                sg = sg + sgrad[(j * 3 + k) * kTile + x] * pv[j];
+            const double nflxv = rscale * sg;
+            Mv[k]              = (-nflxv + s.SlowMh[(k * nv + lev) * Np + c] + DivM[k]) * dt;
         }
         const double vr = Mv[0] * fr[0] + Mv[1] * fr[1] + Mv[2] * fr[2];
         for (int k = 0; k < 3; k++) {
@@ -847,194 +958,242 @@ __global__ void __launch_bounds__(kStenBlock)
     }
 }
 
+__global__ void __launch_bounds__(kTile* kLevGroups)
+    momentum_kernel(Geometry g, Phys P, State s, double dt) {
+    __shared__ double sgeo[kRingGeoRows * kTile];
+    __shared__ double sgrad[21 * kTile];
+    const int         c = lane_column(g);
+    SGeo              G{};
+    if (P.DivDampP)
+        G = stage_ring_geo(sgeo, g, c);
+    stage_cols(sgrad, g.grad, 21, g.Np, c);
+    __syncthreads();
+    if (c < 0)
+        return;
+    if (tail_cta())
+        momentum_body<5>(g, P, s, G, sgrad, dt, c);
+    else
+        momentum_body<6>(g, P, s, G, sgrad, dt, c);
+}
+
 // ---------------------------------------------------------------------------------------------
-// Small step, vertically implicit part, one thread per column:
+// Small step, vertically implicit part:
 //   Prepare_Implicit_Vertical / _Poles (src/headers/dyn/thor_vertical_int.h:566-771),
 //   Vertical_Eq (:52-563, Thomas forward elimination and back substitution, FP64),
 //   Density_Pressure_Eqs / _Poles (src/headers/dyn/thor_fastmodes.h:255-847).
-// Sp and Sd are produced level by level inside the forward sweep that consumes them; the
-// Thomas coefficients live in shared memory, [interface][thread]; Whs is written once and the
-// density / pressure update reads it back from the same shared array.
+// Phase 1 (all levels in parallel): Sp, Sd at every level -> shared memory.
+// Phase 2 (all interfaces in parallel): the tridiagonal row (aa, bb, cc, -C0) of every interior
+//   interface, from the column's values at the two adjacent levels and Sp, Sd.
+// Phase 3 (one warp, lane = column): the Thomas elimination and back substitution, in shared
+//   memory, with the reference's operation sequence; Whs -> shared memory.
+// Phase 4 (all levels in parallel): Whs -> global and the density and pressure update.
+// Shared memory: div [21][32], Sp/Sd [2][nv][32], aa/bb/cc/dd [4][nv+1][32].
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(kVertBlock) vertical_kernel(Geometry g, Phys P, State s, double deltat) {
+__global__ void __launch_bounds__(kTile* kLevGroups)
+    vertical_kernel(Geometry g, Phys P, State s, double deltat) {
     extern __shared__ double smem[];
-    const int c  = blockIdx.x * blockDim.x + threadIdx.x;
     const int nv = g.nv, nvi = g.nvi, Np = g.Np;
-    double*   cc = smem;                      // [nvi][blockDim]
-    double*   dd = smem + nvi * blockDim.x;   // [nvi][blockDim]
-    const int t  = threadIdx.x;
-    const int B  = blockDim.x;
-    if (c >= g.N)
-        return;
+    double*   sdiv = smem;
+    double*   sSp  = sdiv + 21 * kTile;
+    double*   sSd  = sSp + nv * kTile;
+    double*   sa   = sSd + nv * kTile;
+    double*   sb   = sa + nvi * kTile;
+    double*   sc   = sb + nvi * kTile;
+    double*   sd   = sc + nvi * kTile;
+    const int c0 = blockIdx.x * kTile, x = threadIdx.x, c = c0 + x;
+    stage(sdiv, g.div, 21, Np, c0);
+    __syncthreads();
+    const bool    active = c < g.N;
     const double  A = P.A, Gravit = P.Gravit;
     const bool    deep = P.DeepModel, nonh = P.NonHydro, ghv = P.GravHeightVar;
     const double* Alt  = g.Altitude;
     const double* Alth = g.Altitudeh;
     int           nb[7];
-    nb[0] = c;
-    for (int j = 0; j < 6; j++)
-        nb[j + 1] = g.nb[j * Np + c];
-    double dv[21];
-    for (int q = 0; q < 21; q++)
-        dv[q] = g.div[q * Np + c];
-    const bool pole = (g.cflag[c] & kPole) != 0;
+    bool          pole = false;
+    if (active) {
+        nb[0] = c;
+        for (int j = 0; j < 6; j++)
+            nb[j + 1] = g.nb[j * Np + c];
+        pole = (g.cflag[c] & kPole) != 0;
+    }
 
-    // Sp, Sd at one level (Prepare_Implicit_Vertical)
-    auto prepare = [&](int lev, double& Sp, double& Sd) {
-        const int    i      = lev * Np + c;
-        const double RoC    = s.Rd[i] / (s.Cp[i] - s.Rd[i]);
-        const double rscale = rscale_of(P, g, lev);
-        double       hv[7], Mv[7][3];
-        for (int j = 0; j < 7; j++) {
-            hv[j] = gz(s.h + lev * Np, nb[j]);
-            for (int k = 0; k < 3; k++)
-                Mv[j][k] = gz(s.Mhs + (k * nv + lev) * Np, nb[j]);
-        }
-        double nflxr = 0.0, nflxp = 0.0;
-        for (int k = 0; k < 3; k++) {
-            double sd = dv[k] * Mv[0][k], sp = dv[k] * Mv[0][k] * hv[0];
-            for (int j = 1; j < 7; j++) {
-                sd = sd + dv[j * 3 + k] * Mv[j][k];
-                sp = sp + dv[j * 3 + k] * Mv[j][k] * hv[j];
+    // ---- phase 1: Sp, Sd (Prepare_Implicit_Vertical) ----
+    if (active)
+        for (int lev = threadIdx.y; lev < nv; lev += kLevGroups) {
+            const int    i      = lev * Np + c;
+            const double RoC    = s.Rd[i] / (s.Cp[i] - s.Rd[i]);
+            const double rscale = rscale_of(P, g, lev);
+            double       hv[7], Mv[7][3];
+#pragma unroll
+            for (int j = 0; j < 7; j++) {
+                hv[j] = gz(s.h + lev * Np, nb[j]);
+#pragma unroll
+                for (int k = 0; k < 3; k++)
+                    Mv[j][k] = gz(s.Mhs + (k * nv + lev) * Np, nb[j]);
             }
-            nflxr -= rscale * sd;
-            nflxp -= (RoC)*rscale * sp;
+            double nflxr = 0.0, nflxp = 0.0;
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                double sdv = sdiv[k * kTile + x] * Mv[0][k], spv = sdiv[k * kTile + x] * Mv[0][k] * hv[0];
+#pragma unroll
+                for (int j = 1; j < 7; j++) {
+                    sdv = sdv + sdiv[(j * 3 + k) * kTile + x] * Mv[j][k];
+                    spv = spv + sdiv[(j * 3 + k) * kTile + x] * Mv[j][k] * hv[j];
+                }
+                nflxr -= rscale * sdv;
+                nflxp -= (RoC)*rscale * spv;
+            }
+            sSp[lev * kTile + x] = nflxp + s.Slowp[i];
+            sSd[lev * kTile + x] = nflxr + s.SlowRho[i];
         }
-        Sp = nflxp + s.Slowp[i];
-        Sd = nflxr + s.SlowRho[i];
-    };
+    __syncthreads();
 
-    double Spl, Sdl, Sp, Sd;
-    prepare(0, Spl, Sdl);
-    for (int lev = 1; lev < nv; lev++) {
-        prepare(lev, Sp, Sd);
-        const double altht = Alth[lev + 1], althl = Alth[lev - 1], alth = Alth[lev];
-        const double alt = Alt[lev], altl = Alt[lev - 1];
-        double       hp = s.hh[(lev + 1) * Np + c], h = s.hh[lev * Np + c], hm = s.hh[(lev - 1) * Np + c];
-        const double gp = s.gtilh[(lev + 1) * Np + c], gg = s.gtilh[lev * Np + c], gm = s.gtilh[(lev - 1) * Np + c];
-        const int    iu = lev * Np + c, il = (lev - 1) * Np + c;
-        const double p = s.ps[iu], pl = s.ps[il], r = s.Rhos[iu], rl = s.Rhos[il];
-        const double CRddl = (s.Cp[il] - s.Rd[il]) / (s.Rd[il] * deltat * deltat);
-        const double CRddu = (s.Cp[iu] - s.Rd[iu]) / (s.Rd[iu] * deltat * deltat);
-        double       GCoRl, GCoRu;
-        if (ghv) {
-            GCoRl = Gravit * pow(A / (A + altl), 2) * (s.Cp[il] - s.Rd[il]) / s.Rd[il];
-            GCoRu = Gravit * pow(A / (A + alt), 2) * (s.Cp[iu] - s.Rd[iu]) / s.Rd[iu];
+    // ---- phase 2: tridiagonal rows at the interior interfaces ----
+    if (active)
+        for (int lev = 1 + threadIdx.y; lev < nv; lev += kLevGroups) {
+            const double altht = Alth[lev + 1], althl = Alth[lev - 1], alth = Alth[lev];
+            const double alt = Alt[lev], altl = Alt[lev - 1];
+            double       hp = s.hh[(lev + 1) * Np + c], h = s.hh[lev * Np + c], hm = s.hh[(lev - 1) * Np + c];
+            const double gp = s.gtilh[(lev + 1) * Np + c], gg = s.gtilh[lev * Np + c], gm = s.gtilh[(lev - 1) * Np + c];
+            const int    iu = lev * Np + c, il = (lev - 1) * Np + c;
+            const double p = s.ps[iu], pl = s.ps[il], r = s.Rhos[iu], rl = s.Rhos[il];
+            const double Sp = sSp[lev * kTile + x], Spl = sSp[(lev - 1) * kTile + x];
+            const double Sd = sSd[lev * kTile + x], Sdl = sSd[(lev - 1) * kTile + x];
+            const double CRddl = (s.Cp[il] - s.Rd[il]) / (s.Rd[il] * deltat * deltat);
+            const double CRddu = (s.Cp[iu] - s.Rd[iu]) / (s.Rd[iu] * deltat * deltat);
+            double       GCoRl, GCoRu;
+            if (ghv) {
+                GCoRl = Gravit * pow(A / (A + altl), 2) * (s.Cp[il] - s.Rd[il]) / s.Rd[il];
+                GCoRu = Gravit * pow(A / (A + alt), 2) * (s.Cp[iu] - s.Rd[iu]) / s.Rd[iu];
+            }
+            else {
+                GCoRl = Gravit * (s.Cp[il] - s.Rd[il]) / s.Rd[il];
+                GCoRu = Gravit * (s.Cp[iu] - s.Rd[iu]) / s.Rd[iu];
+            }
+            const double dzp  = 1.0 / (altht - alth);
+            const double dzh  = 1.0 / (alt - altl);
+            const double dzm  = 1.0 / (alth - althl);
+            const double dzph = dzp * dzh;
+            const double dzmh = dzm * dzh;
+            double       xi, xim, xip, intl, inttm, intt, aa, bb, ccv;
+            const double CRdd = (CRddl * (alt - alth) + CRddu * (alth - altl)) / (alt - altl);
+            const double GCoR = (GCoRl * (alt - alth) + GCoRu * (alth - altl)) / (alt - altl);
+            if (deep) {
+                hp                = hp * pow(altht + A, 2);
+                h                 = h * pow(alth + A, 2);
+                hm                = hm * pow(althl + A, 2);
+                const double or2  = 1 / pow(alth + A, 2);
+                const double tor3 = 2 / pow(alth + A, 3);
+                xi    = alt;
+                xim   = alth;
+                xip   = altht;
+                intl  = (xi - xim) * dzp * dzh;
+                xi    = altl;
+                xim   = althl;
+                xip   = alth;
+                inttm = -(xi - xip) * dzm * dzh;
+                ccv   = -dzph * or2 * hp - inttm * (gp + GCoR - tor3 * hp);
+                if (nonh)
+                    bb = CRdd + (dzph + dzmh) * or2 * h + (intl - inttm) * (gg + GCoR - tor3 * h);
+                else
+                    bb = (dzph + dzmh) * or2 * h + (intl - inttm) * (gg + GCoR - tor3 * h);
+                aa = -dzmh * or2 * hm + intl * (gm + GCoR - tor3 * hm);
+            }
+            else {
+                xi    = alt;
+                xim   = alth;
+                xip   = altht;
+                intl  = (xi - xim) * dzp * dzh;
+                xi    = altl;
+                xim   = althl;
+                xip   = alth;
+                inttm = -(xi - xip) * dzm * dzh;
+                ccv   = -dzph * hp - inttm * (gp + GCoR);
+                if (nonh)
+                    bb = CRdd + (dzph + dzmh) * h + (intl - inttm) * (gg + GCoR);
+                else
+                    bb = (dzph + dzmh) * h + (intl - inttm) * (gg + GCoR);
+                aa = -dzmh * hm + intl * (gm + GCoR);
+            }
+            const double dSpdz = (Sp - Spl) * dzh;
+            const double dPdz  = (p - pl) * dzh;
+            xi   = alth;
+            xim  = altl;
+            xip  = alt;
+            intt = (xi - xip) / (xim - xip);
+            intl = (xi - xim) / (xip - xim);
+            const double rhohs = rl * intt + r * intl;
+            const double Sdh   = Sdl * intt + Sd * intl;
+            const double Srh   = s.SlowWh[lev * Np + c];
+            double       C0;
+            if (!nonh) {
+                if (ghv)
+                    C0 = (pow(deltat, 2.0) * dSpdz + pow(deltat, 2.0) * Gravit * pow(A / (A + alt), 2) * Sdh
+                          + Gravit * pow(A / (A + alt), 2) * deltat * rhohs + deltat * dPdz - deltat * Srh)
+                         * (CRdd);
+                else
+                    C0 = (pow(deltat, 2.0) * dSpdz + pow(deltat, 2.0) * Gravit * Sdh + Gravit * deltat * rhohs
+                          + deltat * dPdz - deltat * Srh)
+                         * (CRdd);
+            }
+            else {
+                const double whs = s.Whs[lev * Np + c];
+                if (ghv)
+                    C0 = (-whs + pow(deltat, 2.0) * dSpdz + pow(deltat, 2.0) * Gravit * pow(A / (A + alt), 2) * Sdh
+                          + Gravit * pow(A / (A + alt), 2) * deltat * rhohs + deltat * dPdz - deltat * Srh)
+                         * (CRdd);
+                else
+                    C0 = (-whs + pow(deltat, 2.0) * dSpdz + pow(deltat, 2.0) * Gravit * Sdh
+                          + Gravit * deltat * rhohs + deltat * dPdz - deltat * Srh)
+                         * (CRdd);
+            }
+            sa[lev * kTile + x] = aa;
+            sb[lev * kTile + x] = bb;
+            sc[lev * kTile + x] = ccv;
+            sd[lev * kTile + x] = -C0;
         }
-        else {
-            GCoRl = Gravit * (s.Cp[il] - s.Rd[il]) / s.Rd[il];
-            GCoRu = Gravit * (s.Cp[iu] - s.Rd[iu]) / s.Rd[iu];
-        }
-        const double dzp  = 1.0 / (altht - alth);
-        const double dzh  = 1.0 / (alt - altl);
-        const double dzm  = 1.0 / (alth - althl);
-        const double dzph = dzp * dzh;
-        const double dzmh = dzm * dzh;
-        double       xi, xim, xip, intl, inttm, intt, aa, bb, ccv;
-        const double CRdd = (CRddl * (alt - alth) + CRddu * (alth - altl)) / (alt - altl);
-        const double GCoR = (GCoRl * (alt - alth) + GCoRu * (alth - altl)) / (alt - altl);
-        if (deep) {
-            hp                = hp * pow(altht + A, 2);
-            h                 = h * pow(alth + A, 2);
-            hm                = hm * pow(althl + A, 2);
-            const double or2  = 1 / pow(alth + A, 2);
-            const double tor3 = 2 / pow(alth + A, 3);
-            xi    = alt;
-            xim   = alth;
-            xip   = altht;
-            intl  = (xi - xim) * dzp * dzh;
-            xi    = altl;
-            xim   = althl;
-            xip   = alth;
-            inttm = -(xi - xip) * dzm * dzh;
-            ccv   = -dzph * or2 * hp - inttm * (gp + GCoR - tor3 * hp);
-            if (nonh)
-                bb = CRdd + (dzph + dzmh) * or2 * h + (intl - inttm) * (gg + GCoR - tor3 * h);
-            else
-                bb = (dzph + dzmh) * or2 * h + (intl - inttm) * (gg + GCoR - tor3 * h);
-            aa = -dzmh * or2 * hm + intl * (gm + GCoR - tor3 * hm);
-        }
-        else {
-            xi    = alt;
-            xim   = alth;
-            xip   = altht;
-            intl  = (xi - xim) * dzp * dzh;
-            xi    = altl;
-            xim   = althl;
-            xip   = alth;
-            inttm = -(xi - xip) * dzm * dzh;
-            ccv   = -dzph * hp - inttm * (gp + GCoR);
-            if (nonh)
-                bb = CRdd + (dzph + dzmh) * h + (intl - inttm) * (gg + GCoR);
-            else
-                bb = (dzph + dzmh) * h + (intl - inttm) * (gg + GCoR);
-            aa = -dzmh * hm + intl * (gm + GCoR);
-        }
-        const double dSpdz = (Sp - Spl) * dzh;
-        const double dPdz  = (p - pl) * dzh;
-        xi   = alth;
-        xim  = altl;
-        xip  = alt;
-        intt = (xi - xip) / (xim - xip);
-        intl = (xi - xim) / (xip - xim);
-        const double rhohs = rl * intt + r * intl;
-        const double Sdh   = Sdl * intt + Sd * intl;
-        const double Srh   = s.SlowWh[lev * Np + c];
-        double       C0;
-        if (!nonh) {
-            if (ghv)
-                C0 = (pow(deltat, 2.0) * dSpdz + pow(deltat, 2.0) * Gravit * pow(A / (A + alt), 2) * Sdh
-                      + Gravit * pow(A / (A + alt), 2) * deltat * rhohs + deltat * dPdz - deltat * Srh)
-                     * (CRdd);
-            else
-                C0 = (pow(deltat, 2.0) * dSpdz + pow(deltat, 2.0) * Gravit * Sdh + Gravit * deltat * rhohs
-                      + deltat * dPdz - deltat * Srh)
-                     * (CRdd);
-        }
-        else {
-            const double whs = s.Whs[lev * Np + c];
-            if (ghv)
-                C0 = (-whs + pow(deltat, 2.0) * dSpdz + pow(deltat, 2.0) * Gravit * pow(A / (A + alt), 2) * Sdh
-                      + Gravit * pow(A / (A + alt), 2) * deltat * rhohs + deltat * dPdz - deltat * Srh)
-                     * (CRdd);
-            else
-                C0 = (-whs + pow(deltat, 2.0) * dSpdz + pow(deltat, 2.0) * Gravit * Sdh
-                      + Gravit * deltat * rhohs + deltat * dPdz - deltat * Srh)
-                     * (CRdd);
-        }
-        double ddv = -C0;
-        if (lev == 1) {
-            ccv = ccv / bb;
-            ddv = ddv / bb;
-        }
-        else {
-            const double tt = 1.0 / (bb - cc[(lev - 1) * B + t] * aa);
-            ccv *= tt;
-            ddv = (ddv - dd[(lev - 1) * B + t] * aa) * tt;
-        }
-        cc[lev * B + t] = ccv;
-        dd[lev * B + t] = ddv;
-        Spl             = Sp;
-        Sdl             = Sd;
-    }
-    // back substitution; dd[] is overwritten with Whs
-    double wnext = 0.0;
-    dd[nv * B + t] = 0.0;
-    for (int lev = nv - 1; lev > 0; lev--) {
-        double w = (lev == nv - 1) ? dd[lev * B + t] : (-cc[lev * B + t] * wnext + dd[lev * B + t]);
-        dd[lev * B + t]     = w;
-        s.Whs[lev * Np + c] = w;
-        wnext               = w;
-    }
-    dd[t]                = 0.0;
-    s.Whs[c]             = 0.0;
-    s.Whs[nv * Np + c]   = 0.0;
+    __syncthreads();
 
-    // Density_Pressure_Eqs
-    const bool   eeq = P.energy;
+    // ---- phase 3: Thomas elimination and back substitution (one warp) ----
+    if (threadIdx.y == 0 && active) {
+        double cprev = 0, dprev = 0;
+        for (int lev = 1; lev < nv; lev++) {
+            const double aa = sa[lev * kTile + x], bb = sb[lev * kTile + x];
+            double       ccv = sc[lev * kTile + x], ddv = sd[lev * kTile + x];
+            if (lev == 1) {
+                ccv = ccv / bb;
+                ddv = ddv / bb;
+            }
+            else {
+                const double t = 1.0 / (bb - cprev * aa);
+                ccv *= t;
+                ddv = (ddv - dprev * aa) * t;
+            }
+            sc[lev * kTile + x] = ccv;
+            sd[lev * kTile + x] = ddv;
+            cprev               = ccv;
+            dprev               = ddv;
+        }
+        double w           = 0.0;
+        sd[nv * kTile + x] = 0.0;
+        for (int lev = nv - 1; lev > 0; lev--) {
+            w = (lev == nv - 1) ? sd[lev * kTile + x] : (-sc[lev * kTile + x] * w + sd[lev * kTile + x]);
+            sd[lev * kTile + x] = w; // sd now holds Whs
+        }
+        sd[x] = 0.0;
+    }
+    __syncthreads();
+    if (!active)
+        return;
+
+    // ---- phase 4: Whs out, Density_Pressure_Eqs ----
+    const bool   eeq   = P.energy;
     const double P_Ref = P.P_Ref;
-    for (int lev = 0; lev < nv; lev++) {
-        const int    i     = lev * Np + c;
+    for (int lev = threadIdx.y; lev < nv; lev += kLevGroups) {
+        const int i         = lev * Np + c;
+        s.Whs[lev * Np + c] = sd[lev * kTile + x];
+        if (lev == nv - 1)
+            s.Whs[nv * Np + c] = 0.0;
         const double Cv    = s.Cp[i] - s.Rd[i];
         const double altht = Alth[lev + 1], althl = Alth[lev];
         const double dz    = altht - althl;
@@ -1052,9 +1211,11 @@ __global__ void __launch_bounds__(kVertBlock) vertical_kernel(Geometry g, Phys P
             dr2dz                    = r2m * dz;
         }
         double vs[7][3], v1[7][3], ptv[7];
+#pragma unroll
         for (int j = 0; j < 7; j++) {
             const int id = nb[j];
             if (id >= 0) {
+#pragma unroll
                 for (int k = 0; k < 3; k++) {
                     vs[j][k] = s.Mhs[(k * nv + lev) * Np + id];
                     v1[j][k] = vs[j][k] + s.Mhk[(k * nv + lev) * Np + id];
@@ -1063,17 +1224,20 @@ __global__ void __launch_bounds__(kVertBlock) vertical_kernel(Geometry g, Phys P
                 ptv[j]      = eeq ? (s.h[q] + s.ep[q] + s.ek[q]) : s.pt[q];
             }
             else {
+#pragma unroll
                 for (int k = 0; k < 3; k++)
                     vs[j][k] = v1[j][k] = 0.0;
                 ptv[j] = 0.0;
             }
         }
         double nflxr = 0.0, nflxpt = 0.0;
+#pragma unroll
         for (int k = 0; k < 3; k++) {
-            double sr = dv[k] * vs[0][k], st = dv[k] * v1[0][k] * ptv[0];
+            double sr = sdiv[k * kTile + x] * vs[0][k], st = sdiv[k * kTile + x] * v1[0][k] * ptv[0];
+#pragma unroll
             for (int j = 1; j < 7; j++) {
-                sr = sr + dv[j * 3 + k] * vs[j][k];
-                st = st + dv[j * 3 + k] * v1[j][k] * ptv[j];
+                sr = sr + sdiv[(j * 3 + k) * kTile + x] * vs[j][k];
+                st = st + sdiv[(j * 3 + k) * kTile + x] * v1[j][k] * ptv[j];
             }
             nflxr += rscale * sr;
             nflxpt += rscale * st;
@@ -1085,17 +1249,17 @@ __global__ void __launch_bounds__(kVertBlock) vertical_kernel(Geometry g, Phys P
         double whl, wht, whl2, wht2, phl, pht;
         if (lev == 0) {
             whl  = 0.0;
-            wht  = dd[(lev + 1) * B + t];
+            wht  = sd[(lev + 1) * kTile + x];
             whl2 = 0.0;
-            wht2 = dd[(lev + 1) * B + t] + s.Whk[(lev + 1) * Np + c];
+            wht2 = sd[(lev + 1) * kTile + x] + s.Whk[(lev + 1) * Np + c];
             phl  = 0.0;
             pht  = phv(lev + 1);
         }
         else {
-            whl  = dd[lev * B + t];
-            wht  = dd[(lev + 1) * B + t];
-            whl2 = dd[lev * B + t] + s.Whk[lev * Np + c];
-            wht2 = dd[(lev + 1) * B + t] + s.Whk[(lev + 1) * Np + c];
+            whl  = sd[lev * kTile + x];
+            wht  = sd[(lev + 1) * kTile + x];
+            whl2 = sd[lev * kTile + x] + s.Whk[lev * Np + c];
+            wht2 = sd[(lev + 1) * kTile + x] + s.Whk[(lev + 1) * Np + c];
             phl  = phv(lev);
             pht  = phv(lev + 1);
         }
@@ -1103,9 +1267,10 @@ __global__ void __launch_bounds__(kVertBlock) vertical_kernel(Geometry g, Phys P
         const double dwptdz = (wht2 * pht * r2p - whl2 * phl * r2l) / (dz * r2m);
         double       aux    = -(nflxpt + dwptdz) * deltat;
         const double rk_    = s.Rhok[i];
-        const double r      = rk_ + s.Rhos[i];
+        const double rs     = s.Rhos[i];
+        const double r      = rk_ + rs;
         nflxr += dwdz;
-        const double rhos_new = s.Rhos[i] + (s.SlowRho[i] - nflxr) * deltat;
+        const double rhos_new = rs + (s.SlowRho[i] - nflxr) * deltat;
         s.Rhos[i]             = rhos_new;
         if (eeq) {
             aux += s.Etotal[i] + (s.diffpr[i]) * deltat + s.Qheat[i] * deltat;
@@ -1113,7 +1278,7 @@ __global__ void __launch_bounds__(kVertBlock) vertical_kernel(Geometry g, Phys P
             const double w = (whl2 * (Alth[lev + 1] - Alt[lev]) + wht2 * (Alt[lev] - Alth[lev]))
                              / (Alth[lev + 1] - Alth[lev]);
             double Epot_kin;
-            if (P.GravHeightVar)
+            if (ghv)
                 Epot_kin = (rhos_new + rk_) * Gravit * pow(A / (A + Alt[lev]), 2) * Alt[lev]
                            + 0.5 * (pow(v1[0][0], 2) + pow(v1[0][1], 2) + pow(v1[0][2], 2) + pow(w, 2))
                                  / (rhos_new + rk_);
@@ -1127,101 +1292,123 @@ __global__ void __launch_bounds__(kVertBlock) vertical_kernel(Geometry g, Phys P
             const double ptc = (P_Ref / (s.Rd[i] * r)) * pow((s.ps[i] + s.pk[i]) / P_Ref, Cv / s.Cp[i]);
             aux += ptc * r;
             const double pn = P_Ref * pow(s.Rd[i] * aux / P_Ref, s.Cp[i] / Cv);
-            s.ps[i] = pn - s.pk[i] + (s.diffpr[i]) * deltat + s.Rd[i] / Cv * s.Qheat[i] * deltat;
+            s.ps[i]         = pn - s.pk[i] + (s.diffpr[i]) * deltat + s.Rd[i] / Cv * s.Qheat[i] * deltat;
         }
     }
 }
 
 // ---------------------------------------------------------------------------------------------
 // End of an RK stage: UpdateRK2 (src/headers/dyn/thor_auxiliary.h:420-529, no module arrays).
+// Every level first reads the two interfaces it interpolates between; the writes follow a
+// barrier, so no level sees another's update.
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(kColBlock) update_rk2_kernel(Geometry g, Phys P, State s) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= g.N)
+constexpr int kMaxLevelsPerThread = 16; // nv <= kLevGroups * 16
+
+__global__ void __launch_bounds__(kTile* kLevGroups) update_rk2_kernel(Geometry g, Phys P, State s) {
+    const int  c  = blockIdx.x * kTile + threadIdx.x;
+    const int  Np = g.Np, nv = g.nv;
+    const bool active = c < g.N;
+    double     fr[3]  = {0, 0, 0};
+    if (active)
+        for (int k = 0; k < 3; k++)
+            fr[k] = g.func_r[k * Np + c];
+    double wk[kMaxLevelsPerThread], whk_new[kMaxLevelsPerThread];
+    auto   whk_after = [&](int i) -> double { // interface value after the update
+        return (i == 0 || i == nv) ? 0.0 : s.Whk[i * Np + c] + s.Whs[i * Np + c];
+    };
+    if (active) {
+        int cnt = 0;
+#pragma unroll
+        for (int t = 0; t < kMaxLevelsPerThread; t++) {
+            const int lev = threadIdx.y + t * kLevGroups;
+            if (lev < nv) {
+                const double althl = (lev == 0) ? 0.0 : g.Altitudeh[lev];
+                const double altht = g.Altitudeh[lev + 1];
+                const double xi = g.Altitude[lev], xim = althl, xip = altht;
+                const double intt = (xi - xip) / (xim - xip), intl = (xi - xim) / (xip - xim);
+                const double whl = (lev == 0) ? 0.0 : whk_after(lev);
+                wk[t]            = whl * intt + whk_after(lev + 1) * intl;
+                whk_new[t]       = whk_after(lev);
+                cnt++;
+            }
+        }
+    }
+    __syncthreads();
+    if (!active)
         return;
-    const int Np = g.Np, nv = g.nv;
-    double    fr[3];
-    for (int k = 0; k < 3; k++)
-        fr[k] = g.func_r[k * Np + c];
-    for (int lev = 0; lev < nv; lev++) {
-        double Mx = s.Mhs[(0 * nv + lev) * Np + c] + s.Mhk[(0 * nv + lev) * Np + c];
-        double My = s.Mhs[(1 * nv + lev) * Np + c] + s.Mhk[(1 * nv + lev) * Np + c];
-        double Mz = s.Mhs[(2 * nv + lev) * Np + c] + s.Mhk[(2 * nv + lev) * Np + c];
-        double aux = Mx * fr[0] + My * fr[1] + Mz * fr[2];
+#pragma unroll
+    for (int t = 0; t < kMaxLevelsPerThread; t++) {
+        const int lev = threadIdx.y + t * kLevGroups;
+        if (lev >= nv)
+            break;
+        const double Mx  = s.Mhs[(0 * nv + lev) * Np + c] + s.Mhk[(0 * nv + lev) * Np + c];
+        const double My  = s.Mhs[(1 * nv + lev) * Np + c] + s.Mhk[(1 * nv + lev) * Np + c];
+        const double Mz  = s.Mhs[(2 * nv + lev) * Np + c] + s.Mhk[(2 * nv + lev) * Np + c];
+        const double aux = Mx * fr[0] + My * fr[1] + Mz * fr[2];
         s.Mhk[(0 * nv + lev) * Np + c] = Mx - aux * fr[0];
         s.Mhk[(1 * nv + lev) * Np + c] = My - aux * fr[1];
         s.Mhk[(2 * nv + lev) * Np + c] = Mz - aux * fr[2];
         const int i = lev * Np + c;
         s.Rhok[i] += s.Rhos[i];
         s.pk[i] += s.ps[i];
-    }
-    for (int lev = 0; lev < nv + 1; lev++) {
-        if (lev == 0 || lev == nv)
-            s.Whk[lev * Np + c] = 0.0;
-        else
-            s.Whk[lev * Np + c] += s.Whs[lev * Np + c];
-    }
-    double althl = 0, altht = g.Altitudeh[1], whl = 0.0, wht = s.Whk[Np + c];
-    for (int lev = 0; lev < nv; lev++) {
-        double xi = g.Altitude[lev], xim = althl, xip = altht;
-        double intt = (xi - xip) / (xim - xip), intl = (xi - xim) / (xip - xim);
-        s.Wk[lev * Np + c] = whl * intt + wht * intl;
-        if (lev < nv - 1) {
-            althl = altht;
-            altht = g.Altitudeh[lev + 2];
-            whl   = wht;
-            wht   = s.Whk[(lev + 2) * Np + c];
-        }
+        s.Whk[lev * Np + c] = whk_new[t];
+        s.Wk[i]             = wk[t];
+        if (lev == nv - 1)
+            s.Whk[nv * Np + c] = 0.0;
     }
 }
 
-inline dim3 col_grid(const Geometry& g, int block) { return dim3((g.N + block - 1) / block); }
-inline dim3 sten_grid(const Geometry& g) {
-    return dim3((g.N + kStenBlock - 1) / kStenBlock, (g.nv + kLevChunk - 1) / kLevChunk);
-}
+inline dim3 tile_grid(const Geometry& g) { return dim3(g.Np / kTile); }
+inline dim3 tile_grid_tail(const Geometry& g) { return dim3(g.Np / kTile + 1); }
+inline dim3 tile_block() { return dim3(kTile, kLevGroups); }
 
 } // namespace
 
+int max_levels() { return kLevGroups * kMaxLevelsPerThread; }
+
 void launch_profx(const Geometry& g, const Phys& P, const State& s, cudaStream_t st) {
-    profx_kernel<<<col_grid(g, kColBlock), kColBlock, 0, st>>>(g, P, s);
+    profx_kernel<<<(g.N + kColBlock - 1) / kColBlock, kColBlock, 0, st>>>(g, P, s);
 }
 void launch_adv_temp(const Geometry& g, const Phys& P, const State& s, cudaStream_t st) {
-    adv_temp_kernel<<<col_grid(g, kColBlock), kColBlock, 0, st>>>(g, P, s);
+    adv_temp_kernel<<<tile_grid(g), tile_block(), 0, st>>>(g, P, s);
 }
 void launch_diffusion(const Geometry& g, const Phys& P, const State& s, int stepnum, bool last,
                       cudaStream_t st) {
     // passes alternate between the two halves of the diff buffer
-    const size_t plane6 = (size_t)6 * g.nv * g.Np;
-    const double* in    = s.diff + ((stepnum + 1) % 2) * plane6;
-    double*       out   = s.diff + (stepnum % 2) * plane6;
-    diffusion_kernel<<<sten_grid(g), kStenBlock, 0, st>>>(g, P, s, in, out, stepnum, last);
+    const size_t  plane6 = (size_t)6 * g.nv * g.Np;
+    const double* in     = s.diff + ((stepnum + 1) % 2) * plane6;
+    double*       out    = s.diff + (stepnum % 2) * plane6;
+    diffusion_kernel<<<tile_grid_tail(g), tile_block(), 0, st>>>(g, P, s, in, out, stepnum, last);
 }
 void launch_divm0(const Geometry& g, const Phys& P, const State& s, bool small_step,
                   cudaStream_t st) {
-    divm0_kernel<<<sten_grid(g), kStenBlock, 0, st>>>(g, P, small_step ? s.Mhs : s.Mhk,
-                                                      small_step ? s.Whs : s.Whk, s.divg);
+    divm0_kernel<<<tile_grid_tail(g), tile_block(), 0, st>>>(g, P, small_step ? s.Mhs : s.Mhk,
+                                                        small_step ? s.Whs : s.Whk, s.divg);
 }
 void launch_slow_modes(const Geometry& g, const Phys& P, const State& s, bool update_rk,
                        cudaStream_t st) {
-    slow_modes_kernel<<<sten_grid(g), kStenBlock, 0, st>>>(g, P, s, update_rk);
+    slow_modes_kernel<<<tile_grid_tail(g), tile_block(), 0, st>>>(g, P, s, update_rk);
 }
 void launch_momentum(const Geometry& g, const Phys& P, const State& s, double dt,
                      cudaStream_t st) {
-    momentum_kernel<<<sten_grid(g), kStenBlock, 0, st>>>(g, P, s, dt);
+    momentum_kernel<<<tile_grid_tail(g), tile_block(), 0, st>>>(g, P, s, dt);
+}
+size_t vertical_smem_bytes(const Geometry& g) {
+    return sizeof(double) * kTile * (21 + 2 * g.nv + 4 * g.nvi);
 }
 void launch_vertical(const Geometry& g, const Phys& P, const State& s, double dt,
                      cudaStream_t st) {
-    size_t smem = (size_t)2 * g.nvi * kVertBlock * sizeof(double);
+    const size_t  smem       = vertical_smem_bytes(g);
     static size_t configured = 0;
     if (smem > configured) {
         cudaFuncSetAttribute(vertical_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem);
         configured = smem;
     }
-    vertical_kernel<<<col_grid(g, kVertBlock), kVertBlock, smem, st>>>(g, P, s, dt);
+    vertical_kernel<<<tile_grid(g), tile_block(), smem, st>>>(g, P, s, dt);
 }
 void launch_update_rk2(const Geometry& g, const Phys& P, const State& s, cudaStream_t st) {
-    update_rk2_kernel<<<col_grid(g, kColBlock), kColBlock, 0, st>>>(g, P, s);
+    update_rk2_kernel<<<tile_grid(g), tile_block(), 0, st>>>(g, P, s);
 }
 
 } // namespace thorx

@@ -186,12 +186,22 @@ int build_neighbours(thorx_ctx* ctx, const thorx_grid* gr) {
     for (int id = 0; id < N; id++)
         if (!seen[id])
             return fail(ctx, THORX_E_ARG, "maps do not cover every column");
+    std::vector<int> special;
+    for (int id = 0; id < N; id++)
+        if (flag[id] & kRing5)
+            special.push_back(id);
+    if (special.size() > 32)
+        return fail(ctx, THORX_E_ARG, "more five-neighbour columns than one tile holds");
     int*     d_nb;
     int*     d_ring;
     uint8_t* d_flag;
+    int*     d_special;
     if (dev_alloc(ctx, &d_nb, nb.size()) || dev_alloc(ctx, &d_ring, ring.size())
-        || dev_alloc(ctx, &d_flag, flag.size()))
+        || dev_alloc(ctx, &d_flag, flag.size()) || dev_alloc(ctx, &d_special, 32))
         return THORX_E_CUDA;
+    CK(cudaMemcpy(d_special, special.data(), special.size() * sizeof(int), cudaMemcpyHostToDevice));
+    ctx->g.special  = d_special;
+    ctx->g.nspecial = (int)special.size();
     CK(cudaMemcpy(d_nb, nb.data(), nb.size() * sizeof(int), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(d_ring, ring.data(), ring.size() * sizeof(int), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(d_flag, flag.data(), flag.size(), cudaMemcpyHostToDevice));
@@ -398,6 +408,8 @@ int thorx_create(const thorx_grid* gr, const thorx_params* pr, void* stream, tho
     if (N < 12 || nv < 3 || gr->nl_region < 2 || gr->nr < 1
         || (long)gr->nr * gr->nl_region * gr->nl_region != N - 2)
         return fail(ctx, THORX_E_ARG, "thorx_create: inconsistent grid sizes");
+    if (nv > max_levels())
+        return fail(ctx, THORX_E_UNSUPPORTED, "nv above the supported maximum");
     if (pr->HyDiffOrder < 2 || pr->HyDiffOrder % 2)
         return fail(ctx, THORX_E_UNSUPPORTED, "HyDiffOrder must be even and >= 2");
     if (pr->precision != THORX_FP64)

@@ -38,6 +38,8 @@ struct Geometry {
     const int*     nb;
     const int*     ring;
     const uint8_t* cflag;
+    const int*     special;  // the columns with a five-entry ring (pentagons, poles)
+    int            nspecial; // 12
     const double*  div;
     const double*  grad;
     const double*  areas;
@@ -80,6 +82,11 @@ struct State {
 };
 
 enum : unsigned int { kFlagNaN = 1u };
+
+// Largest nv the kernels take (levels per thread are unrolled into registers).
+int max_levels();
+// Dynamic shared memory of the vertical implicit kernel.
+size_t vertical_smem_bytes(const Geometry& g);
 
 // Kernel launchers (thor_b200/csrc/dyn_fp64.cu).
 void launch_profx(const Geometry& g, const Phys& P, const State& s, cudaStream_t st);
