@@ -140,6 +140,25 @@ int thorx_kernel_info(const thorx_ctx* ctx, int k, const char** name, double* by
                       int* launches_per_step);
 int thorx_profile_steps(thorx_ctx* ctx, int nsteps, double* ms_per_class);
 
+/* ---- Global conserved quantities (replaces ESP::globdiag, src/ESP/profx_driver.cu:476-569,
+ * with the per-cell terms of CalcTotEnergy / CalcMass / CalcAngMom / CalcEntropy,
+ * src/ESP/profx_globdiag.cu:45-252; no surface term) ----
+ * out[0] total energy (J), out[1] mass (kg), out[2..4] angular momentum x, y, z (kg m^2 s^-1),
+ * out[5] entropy (J K^-1) of the current state. Each is a compensated sum whose order of
+ * addition is fixed: the same state gives the same bits on every call. Synchronises the
+ * context's stream. */
+int thorx_globdiag(thorx_ctx* ctx, double* out);
+
+/* Compensated sum of n doubles in device memory of the current device
+ * (replaces gpu_sum_on_device<1024>, src/headers/reduction_add.h:96-128). x must point into one
+ * device or managed allocation of the current device whose extent the driver reports
+ * (cudaMalloc, cudaMallocManaged, cudaMallocAsync) and which holds n doubles from x on; both
+ * are checked before any kernel runs (THORX_E_ARG otherwise). The sum runs on
+ * `stream` (NULL: the legacy default stream), which is synchronised before *out is written.
+ * Like the reference it allocates its partial sums with cudaMalloc for the call and frees them
+ * after. Context-free: on error, thorx_last_error(NULL) gives this thread's message. */
+int thorx_device_sum(const double* x, long long n, void* stream, double* out);
+
 /* ---- Icosahedral grid (replaces Icogrid::Icogrid, src/ESP/grid.cu:84-302) ----
  * Builds THOR's grid on the host: same point order, neighbours, rhombus maps, spring-dynamics
  * relaxation (beta = spring_beta, when spring_dynamics != 0), control volumes and operators,

@@ -39,7 +39,9 @@
 #include "dyn/thor_slowmodes.h"
 #include "dyn/thor_vertical_int.h"
 #include "phy/profx_auxiliary.h"
+#include "phy/profx_globdiag.h"
 #include "phy/profx_held_suarez.h"
+#include "reduction_add.h"
 
 #include "grid.h"
 #include "log_writer.h"
@@ -208,7 +210,8 @@ static void* sim_new(const ref_grid_view* g, const ref_params* p) {
                            "temperature", "W", "Wk", "Ws", "h", "pt", "gtil", "SlowRho",
                            "Slowpressure", "Sp", "Sd", "diffw", "diffrh", "diffpr", "diffwv",
                            "diffrv", "diffprv", "epotential", "ekinetic", "Etotal", "Cp", "Rd",
-                           "profx_Qheat", "profx_dW"};
+                           "profx_Qheat", "profx_dW", "Mass", "AngMomx", "AngMomy", "AngMomz",
+                           "Entropy"};
     const char* cell3[] = {"Mh", "Mhk", "Mhs", "Adv", "v", "SlowMh", "DivM", "divg_Mh",
                            "diffmh", "diffmv", "profx_dMh"};
     const char* iface[] = {"Wh", "Whk", "Whs", "hh", "pth", "gtilh", "SlowWh", "epotentialh",
@@ -549,6 +552,50 @@ extern "C" int ref_sim_step(void* h, int nsteps, int do_profx, int do_thor) {
             return -1;
     }
     return 0;
+}
+
+// Global conserved quantities of the current state: the kernel sequence of ESP::globdiag
+// (src/ESP/profx_driver.cu:476-560, no surface) with the reference's own per-cell kernels
+// (src/ESP/profx_globdiag.cu) and its own reduction gpu_sum_on_device<1024>
+// (src/headers/reduction_add.h:96-128). out = {energy, mass, AMx, AMy, AMz, entropy}.
+extern "C" int ref_sim_globdiag(void* h, double* out) {
+    RefSim*   s   = (RefSim*)h;
+    auto&     f   = s->f;
+    const int NTH = 256;
+    dim3      NB((s->N / NTH) + 1, s->nv, 1);
+    const ref_params& p = s->p;
+    CalcMass<<<NB, NTH>>>(f["Mass"], nullptr, f["Rho"], p.A, f["Altitudeh"], f["lonlat"],
+                          f["areasT"], s->N, p.DeepModel);
+    CalcTotEnergy<<<NB, NTH>>>(f["Etotal"], nullptr, f["Mh"], f["W"], f["Rho"], f["temperature"],
+                               p.Gravit, f["Cp"], f["Rd"], p.A, f["Altitude"], f["Altitudeh"],
+                               f["lonlat"], f["areasT"], f["func_r"], s->N, p.DeepModel);
+    CalcAngMom<<<NB, NTH>>>(f["AngMomx"], f["AngMomy"], f["AngMomz"], nullptr, nullptr, nullptr,
+                            f["Mh"], f["Rho"], p.A, p.Omega, f["Altitude"], f["Altitudeh"],
+                            f["lonlat"], f["areasT"], f["func_r"], s->N, p.DeepModel);
+    CalcEntropy<<<NB, NTH>>>(f["Entropy"], f["pressure"], f["temperature"], f["Cp"], f["Rd"], p.A,
+                             p.P_Ref, f["Altitude"], f["Altitudeh"], f["lonlat"], f["areasT"],
+                             f["func_r"], s->N, p.DeepModel);
+    REF_CHECK(cudaGetLastError());
+    const long n = (long)s->N * s->nv;
+    out[0]       = gpu_sum_on_device<1024>(f["Etotal"], n);
+    out[1]       = gpu_sum_on_device<1024>(f["Mass"], n);
+    out[2]       = gpu_sum_on_device<1024>(f["AngMomx"], n);
+    out[3]       = gpu_sum_on_device<1024>(f["AngMomy"], n);
+    out[4]       = gpu_sum_on_device<1024>(f["AngMomz"], n);
+    out[5]       = gpu_sum_on_device<1024>(f["Entropy"], n);
+    REF_CHECK(cudaDeviceSynchronize());
+    return 0;
+}
+
+// The reference's reduction on a host array copied to the device (gpu_sum_on_device<1024>).
+extern "C" double ref_device_sum(const double* host, long n) {
+    double* d = nullptr;
+    if (cudaMalloc(&d, (n > 0 ? n : 1) * sizeof(double)) != cudaSuccess)
+        return 0.0 / 0.0;
+    cudaMemcpy(d, host, n * sizeof(double), cudaMemcpyHostToDevice);
+    double r = gpu_sum_on_device<1024>(d, n);
+    cudaFree(d);
+    return r;
 }
 
 // Times `nsteps` large steps with CUDA events; returns milliseconds (negative on error).

@@ -40,7 +40,7 @@ struct Oracle {
     // geometry
     std::vector<int> maps, point_local;
     Vec              Altitude, Altitudeh, lonlat, areas, areasTr, nvecoa, nvecti, nvecte, div, grad,
-        func_r, Kdh4, Kdhz;
+        func_r, Kdh4, Kdhz, areasT;
     // neighbour tables: nb7[id*7 + j] j=0 self, j=1..6 = pt1..pt6 (-1 = tile hole -> value 0);
     // nterms[id] = 7 (interior) or 6 (pole); ring[id*6 + j], nring[id] = 6 (hexagon) or 5.
     std::vector<int>  nb7, nterms, ring, nring;
@@ -1413,6 +1413,8 @@ extern "C" void* oracle_new(const oracle_grid* g, const oracle_params* p) {
     o->div.assign(g->div, g->div + 21 * (size_t)N);
     o->grad.assign(g->grad, g->grad + 21 * (size_t)N);
     o->func_r.assign(g->func_r, g->func_r + 3 * (size_t)N);
+    if (g->areasT)
+        o->areasT.assign(g->areasT, g->areasT + (size_t)N);
     build_neighbours(*o);
     // src/ESP/esp_initial.cu:1292-1335 without the diffusive sponge
     o->Kdh4.resize(nv);
@@ -1469,6 +1471,100 @@ extern "C" int oracle_step(void* h, int nsteps, int do_profx, int do_thor) {
             thor(*o);
     }
     return 0;
+}
+
+namespace {
+
+// Neumaier's compensated summation (A. Neumaier, ZAMM 54, 1974): s + c carries the sum to about
+// one rounding of the exact result for any ordering of the terms.
+struct Neumaier {
+    double s = 0.0, c = 0.0;
+    void   add(double x) {
+        double t = s + x;
+        if (std::fabs(s) >= std::fabs(x))
+            c += (s - t) + x;
+        else
+            c += (x - t) + s;
+        s = t;
+    }
+    double value() const { return s + c; }
+};
+
+// Control volume of cell (id, lev) as CalcMass et al. compute it (src/ESP/profx_globdiag.cu:82-90).
+double control_volume(const Oracle& o, int id, int lev) {
+    double A = o.P.A, zup = o.Altitudeh[lev + 1] + A, zlow = o.Altitudeh[lev] + A;
+    if (o.P.DeepModel)
+        return o.areasT[id] / pow(A, 2) * (pow(zup, 3) - pow(zlow, 3)) / 3;
+    return o.areasT[id] * (zup - zlow);
+}
+
+} // namespace
+
+// Per-cell energy, mass, angular momentum and entropy in the reference's expressions
+// (CalcTotEnergy :45-112, CalcMass :182-212, CalcAngMom :119-180, CalcEntropy :214-252 of
+// src/ESP/profx_globdiag.cu), summed over all cells.
+extern "C" int oracle_globdiag(void* h, double* out, double* abs_out) {
+    Oracle& o = *(Oracle*)h;
+    if (o.areasT.empty())
+        return -1;
+    const int  nv = o.nv;
+    const Vec &Rho = o.f["Rho"], &Mh = o.f["Mh"], &W = o.f["W"], &T = o.f["temperature"],
+              &p = o.f["pressure"], &Cp = o.f["Cp"], &Rd = o.f["Rd"];
+    const double A = o.P.A, Omega = o.P.Omega, Gravit = o.P.Gravit, P_Ref = o.P.P_Ref;
+    Neumaier S[6], M[6];
+    for (int id = 0; id < o.N; id++) {
+        const double lon = o.lonlat[id * 2], lat = o.lonlat[id * 2 + 1];
+        for (int lev = 0; lev < nv; lev++) {
+            const size_t i   = (size_t)id * nv + lev;
+            const double Vol = control_volume(o, id, lev);
+            const double m0 = Mh[i * 3 + 0], m1 = Mh[i * 3 + 1], m2 = Mh[i * 3 + 2];
+            // energy
+            double Cv   = Cp[i] - Rd[i];
+            double wx   = W[i] * cos(lat) * cos(lon);
+            double wy   = W[i] * cos(lat) * sin(lon);
+            double wz   = W[i] * sin(lat);
+            double Ek   = 0.5 * ((m0 + wx) * (m0 + wx) + (m1 + wy) * (m1 + wy) + (m2 + wz) * (m2 + wz))
+                        / Rho[i];
+            double Eint = Cv * T[i] * Rho[i];
+            double Eg   = Rho[i] * Gravit * o.Altitude[lev];
+            double term[6];
+            term[0] = (Ek + Eint + Eg) * Vol;
+            // mass
+            term[1] = Rho[i] * Vol;
+            // angular momentum
+            double r  = (A + o.Altitude[lev]);
+            double rx = r * o.func_r[id * 3 + 0], ry = r * o.func_r[id * 3 + 1],
+                   rz = r * o.func_r[id * 3 + 2];
+            double AMx = ry * m2 - rz * m1 - Rho[i] * Omega * r * rz * cos(lat) * cos(lon);
+            double AMy = -rx * m2 + rz * m0 - Rho[i] * Omega * r * rz * cos(lat) * sin(lon);
+            double AMz = rx * m1 - ry * m0 + Rho[i] * Omega * r * r * cos(lat) * cos(lat);
+            term[2]    = AMx * Vol;
+            term[3]    = AMy * Vol;
+            term[4]    = AMz * Vol;
+            // entropy
+            double kappa = Rd[i] / Cp[i];
+            double potT  = T[i] * pow(P_Ref / p[i], kappa);
+            double Sdens = Cp[i] * log(potT);
+            term[5]      = Sdens * Vol;
+            for (int q = 0; q < 6; q++) {
+                S[q].add(term[q]);
+                M[q].add(std::fabs(term[q]));
+            }
+        }
+    }
+    for (int q = 0; q < 6; q++) {
+        out[q] = S[q].value();
+        if (abs_out)
+            abs_out[q] = M[q].value();
+    }
+    return 0;
+}
+
+extern "C" double oracle_sum(const double* x, long n) {
+    Neumaier s;
+    for (long i = 0; i < n; i++)
+        s.add(x[i]);
+    return s.value();
 }
 
 extern "C" void oracle_set_threads(int n) {

@@ -18,13 +18,14 @@ typedef struct {
 
 // Grid arrays in the reference layout (src/ESP/grid.cu): maps [nr][(nl+2)^2], point_local [N][6],
 // div/grad [N][7][3], areas/nvecoa/nvecti/nvecte [N][6][3], areasTr [N][6], func_r [N][3],
-// lonlat [N][2], Altitude [nv], Altitudeh [nv+1]. Copied at creation.
+// lonlat [N][2], Altitude [nv], Altitudeh [nv+1], areasT [N]. Copied at creation.
 typedef struct {
     int           point_num, nv, nl_region, nr;
     const int*    maps;
     const int*    point_local;
     const double *Altitude, *Altitudeh, *lonlat, *areas, *areasTr, *nvecoa, *nvecti, *nvecte,
         *div, *grad, *func_r;
+    const double* areasT; // may be null when oracle_globdiag is not used
 } oracle_grid;
 
 void* oracle_new(const oracle_grid* g, const oracle_params* p);
@@ -33,6 +34,12 @@ long oracle_set(void* h, const char* name, const double* src);
 long oracle_get(void* h, const char* name, double* dst);
 // nsteps x (ProfX if do_profx, then Thor if do_thor), as src/esp.cu:1382-1398.
 int  oracle_step(void* h, int nsteps, int do_profx, int do_thor);
+// Global conserved quantities of the current state (ESP::globdiag, src/ESP/profx_driver.cu:476-560):
+// out = {energy, mass, AMx, AMy, AMz, entropy}, each a compensated sum; if abs_out is not null it
+// receives the sums of the magnitudes of the per-cell terms (the scale of the rounding error).
+int    oracle_globdiag(void* h, double* out, double* abs_out);
+// Compensated (Neumaier) sum of x[0..n-1] in index order.
+double oracle_sum(const double* x, long n);
 void oracle_set_threads(int n);
 void oracle_free(void* h);
 

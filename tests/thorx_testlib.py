@@ -84,6 +84,10 @@ def ref_lib(nofma=False):
         lib.ref_sim_time.restype = ctypes.c_double
         lib.ref_sim_time.argtypes = [ctypes.c_void_p, ctypes.c_int]
         lib.ref_sim_free.argtypes = [ctypes.c_void_p]
+        lib.ref_sim_globdiag.restype = ctypes.c_int
+        lib.ref_sim_globdiag.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        lib.ref_device_sum.restype = ctypes.c_double
+        lib.ref_device_sum.argtypes = [ctypes.c_void_p, ctypes.c_long]
         _ref[nofma] = lib
     return _ref[nofma]
 
@@ -181,7 +185,8 @@ class OracleGrid(ctypes.Structure):
                 ("lonlat", ctypes.c_void_p), ("areas", ctypes.c_void_p),
                 ("areasTr", ctypes.c_void_p), ("nvecoa", ctypes.c_void_p),
                 ("nvecti", ctypes.c_void_p), ("nvecte", ctypes.c_void_p),
-                ("div", ctypes.c_void_p), ("grad", ctypes.c_void_p), ("func_r", ctypes.c_void_p)]
+                ("div", ctypes.c_void_p), ("grad", ctypes.c_void_p), ("func_r", ctypes.c_void_p),
+                ("areasT", ctypes.c_void_p)]
 
 
 _oracle = None
@@ -199,6 +204,10 @@ def oracle_lib():
         lib.oracle_get.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p]
         lib.oracle_step.restype = ctypes.c_int
         lib.oracle_step.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        lib.oracle_globdiag.restype = ctypes.c_int
+        lib.oracle_globdiag.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        lib.oracle_sum.restype = ctypes.c_double
+        lib.oracle_sum.argtypes = [ctypes.c_void_p, ctypes.c_long]
         lib.oracle_set_threads.argtypes = [ctypes.c_int]
         lib.oracle_free.argtypes = [ctypes.c_void_p]
         _oracle = lib
@@ -209,13 +218,11 @@ class Oracle:
     def __init__(self, grid, params):
         """grid: object with point_num, nv, nl_region, nr and reference-layout arrays."""
         lib = oracle_lib()
-        self._keep = {k: np.ascontiguousarray(grid[k]) for k in
-                      ["maps", "point_local", "Altitude", "Altitudeh", "lonlat", "areas",
-                       "areasTr", "nvecoa", "nvecti", "nvecte", "div", "grad", "func_r"]}
+        names = ["maps", "point_local", "Altitude", "Altitudeh", "lonlat", "areas", "areasTr",
+                 "nvecoa", "nvecti", "nvecte", "div", "grad", "func_r", "areasT"]
+        self._keep = {k: np.ascontiguousarray(grid[k]) for k in names}
         g = OracleGrid(grid.point_num, grid.nv, grid.nl_region, grid.nr,
-                       *[self._keep[k].ctypes.data for k in
-                         ["maps", "point_local", "Altitude", "Altitudeh", "lonlat", "areas",
-                          "areasTr", "nvecoa", "nvecti", "nvecte", "div", "grad", "func_r"]])
+                       *[self._keep[k].ctypes.data for k in names])
         self.h = lib.oracle_new(ctypes.byref(g), ctypes.byref(params))
 
     def set(self, name, a):
@@ -232,6 +239,12 @@ class Oracle:
 
     def step(self, n=1, profx=True, thor=True):
         assert oracle_lib().oracle_step(self.h, n, int(profx), int(thor)) == 0
+
+    def globdiag(self):
+        """(sums, sums of magnitudes) of energy, mass, AMx, AMy, AMz, entropy."""
+        out, mag = np.zeros(6), np.zeros(6)
+        assert oracle_lib().oracle_globdiag(self.h, out.ctypes.data, mag.ctypes.data) == 0
+        return out, mag
 
     def close(self):
         if self.h:
@@ -264,6 +277,11 @@ class RefSim:
 
     def time(self, n):
         return self.lib.ref_sim_time(self.h, n)
+
+    def globdiag(self):
+        out = np.zeros(6)
+        assert self.lib.ref_sim_globdiag(self.h, out.ctypes.data) == 0
+        return out
 
     def close(self):
         if self.h:

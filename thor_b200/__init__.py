@@ -16,6 +16,7 @@ FP64, MIXED = 0, 1
 ENTROPY, ENERGY = 0, 1
 NO_BENCHMARK, HELD_SUAREZ = 0, 1
 
+E_ARG, E_CUDA, E_NAN, E_UNSUPPORTED, E_STATE = -1, -2, -3, -4, -5
 ERRORS = {-1: "THORX_E_ARG", -2: "THORX_E_CUDA", -3: "THORX_E_NAN", -4: "THORX_E_UNSUPPORTED",
           -5: "THORX_E_STATE"}
 
@@ -90,6 +91,10 @@ def lib():
         L.thorx_kernel_info.restype = ci
         L.thorx_profile_steps.argtypes = [vp, ci, ctypes.POINTER(ctypes.c_double)]
         L.thorx_profile_steps.restype = ci
+        L.thorx_globdiag.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
+        L.thorx_globdiag.restype = ci
+        L.thorx_device_sum.argtypes = [vp, ctypes.c_longlong, vp, ctypes.POINTER(ctypes.c_double)]
+        L.thorx_device_sum.restype = ci
         _lib = L
     return _lib
 
@@ -98,7 +103,17 @@ EXPORTED = ["thorx_create", "thorx_destroy", "thorx_last_error", "thorx_field_si
             "thorx_set_field", "thorx_get_field", "thorx_profx", "thorx_thor", "thorx_step",
             "thorx_sync", "thorx_kernels_per_step", "thorx_grid_build", "thorx_grid_info",
             "thorx_grid_get", "thorx_grid_describe", "thorx_grid_free", "thorx_init_rest_state",
-            "thorx_kernel_classes", "thorx_kernel_info", "thorx_profile_steps"]
+            "thorx_kernel_classes", "thorx_kernel_info", "thorx_profile_steps", "thorx_globdiag",
+            "thorx_device_sum"]
+
+def device_sum(ptr, n, stream=0):
+    """Compensated sum of n doubles at device address `ptr` (thorx_device_sum)."""
+    out = ctypes.c_double()
+    rc = lib().thorx_device_sum(ctypes.c_void_p(ptr), n, ctypes.c_void_p(stream), ctypes.byref(out))
+    if rc:
+        raise ThorxError(rc, lib().thorx_last_error(None).decode())
+    return out.value
+
 
 GRID_F64 = ["point_xyz", "point_xyzq", "Altitude", "Altitudeh", "lonlat", "areas", "areasT",
             "areasTr", "nvec", "nvecoa", "nvecti", "nvecte", "div", "grad", "func_r"]
@@ -229,6 +244,12 @@ class Thorx:
         ms = (ctypes.c_double * k)()
         self._check(lib().thorx_profile_steps(self.h, n, ms))
         return list(ms)
+
+    def globdiag(self):
+        """Global energy, mass, angular momentum (x, y, z) and entropy of the current state."""
+        out = (ctypes.c_double * 6)()
+        self._check(lib().thorx_globdiag(self.h, out))
+        return list(out)
 
     def close(self):
         if self.h:

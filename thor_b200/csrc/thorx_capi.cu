@@ -22,6 +22,8 @@
 #include <string>
 #include <vector>
 
+#include <cuda.h>
+
 #include "../../include/thorx.h"
 #include "thorx_internal.h"
 
@@ -47,6 +49,8 @@ struct thorx_ctx {
     std::map<std::string, FieldDesc> fields;
     double*                          staging     = nullptr; // layout conversion buffer
     size_t                           staging_len = 0;       // doubles
+    double2*                         gd_part     = nullptr; // global-sum partials (6 quantities)
+    double*                          gd_out      = nullptr; // the six global sums
     unsigned int*                    flags_host  = nullptr; // pinned
     cudaGraphExec_t                  graph_exec  = nullptr;
     cudaGraph_t                      graph       = nullptr;
@@ -390,6 +394,71 @@ int enqueue_thor(thorx_ctx* ctx) {
 
 } // namespace
 
+namespace {
+
+// Message of the last failed call of this host thread that takes no context.
+thread_local std::string g_free_err;
+
+int free_fail(int code, const std::string& msg) {
+    g_free_err = msg;
+    return code;
+}
+
+// Largest n a device sum takes: its partial count must fit the final pass's int index.
+constexpr long long kDeviceSumMaxN = 2048LL * 0x7fffffffLL;
+
+// x must be memory of the current device (device or managed) that holds n doubles, inside one
+// allocation whose extent the driver reports (cuMemGetAddressRange); checked before any kernel
+// reads it, so that a host pointer or a short buffer is an error, not a fault.
+int check_device_range(const char* fn, const double* x, long long n) {
+    cudaPointerAttributes a{};
+    cudaError_t           e = cudaPointerGetAttributes(&a, x);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return free_fail(THORX_E_ARG, std::string(fn) + ": x is not a CUDA pointer");
+    }
+    int dev = -1;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess)
+        return free_fail(THORX_E_CUDA, std::string(fn) + ": cudaGetDevice: " + cudaGetErrorString(e));
+    if ((a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged) || a.device != dev)
+        return free_fail(THORX_E_ARG,
+                         std::string(fn) + ": x is not device memory of the current device");
+    using RangeFn = CUresult (*)(CUdeviceptr*, size_t*, CUdeviceptr);
+    static RangeFn range = [] {
+        void*                            f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuMemGetAddressRange", &f, cudaEnableDefault, &q) != cudaSuccess
+            || q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        cudaGetLastError();
+        return (RangeFn)f;
+    }();
+    CUdeviceptr base = 0;
+    size_t      size = 0;
+    if (!range || range(&base, &size, (CUdeviceptr)x) != CUDA_SUCCESS)
+        return free_fail(THORX_E_ARG,
+                         std::string(fn) + ": the driver reports no allocation extent for x");
+    const unsigned long long end = (unsigned long long)base + size;
+    if ((unsigned long long)(uintptr_t)x + (unsigned long long)n * sizeof(double) > end)
+        return free_fail(THORX_E_ARG, std::string(fn) + ": n = " + std::to_string(n)
+                                          + " runs past the end of x's allocation");
+    return 0;
+}
+
+int check_sum_args(const char* fn, const double* x, long long n, double* out) {
+    if (!out || n < 0 || (n > 0 && !x))
+        return free_fail(THORX_E_ARG, std::string(fn) + ": null pointer or negative n");
+    if (n > kDeviceSumMaxN)
+        return free_fail(THORX_E_ARG, std::string(fn) + ": n too large");
+    if (n == 0) {
+        *out = 0.0;
+        return 0;
+    }
+    return check_device_range(fn, x, n);
+}
+
+} // namespace
+
 extern "C" {
 
 int thorx_create(const thorx_grid* gr, const thorx_params* pr, void* stream, thorx_ctx** out) {
@@ -399,7 +468,7 @@ int thorx_create(const thorx_grid* gr, const thorx_params* pr, void* stream, tho
     thorx_ctx* ctx = new thorx_ctx;
     if (!gr || !pr || !gr->maps || !gr->point_local || !gr->Altitude || !gr->Altitudeh
         || !gr->lonlat || !gr->areas || !gr->areasTr || !gr->nvecoa || !gr->nvecti || !gr->nvecte
-        || !gr->div || !gr->grad || !gr->func_r) {
+        || !gr->div || !gr->grad || !gr->func_r || !gr->areasT) {
         *out = ctx;
         return fail(ctx, THORX_E_ARG, "thorx_create: null grid or params pointer");
     }
@@ -464,14 +533,21 @@ int thorx_create(const thorx_grid* gr, const thorx_params* pr, void* stream, tho
         || (rc = upload_geo(ctx, gr->func_r, 3, &g.func_r)))
         return rc;
     {
-        std::vector<double> lat(Np, 0.0);
-        for (int c = 0; c < N; c++)
-            lat[c] = gr->lonlat[2 * c + 1];
-        double* d;
-        if (dev_alloc(ctx, &d, Np))
+        std::vector<double> lat(Np, 0.0), lon(Np, 0.0), areasT(Np, 0.0);
+        for (int c = 0; c < N; c++) {
+            lon[c]    = gr->lonlat[2 * c];
+            lat[c]    = gr->lonlat[2 * c + 1];
+            areasT[c] = gr->areasT[c];
+        }
+        double *d, *d2, *d3;
+        if (dev_alloc(ctx, &d, Np) || dev_alloc(ctx, &d2, Np) || dev_alloc(ctx, &d3, Np))
             return THORX_E_CUDA;
         CK(cudaMemcpy(d, lat.data(), Np * sizeof(double), cudaMemcpyHostToDevice));
-        g.lat = d;
+        CK(cudaMemcpy(d2, lon.data(), Np * sizeof(double), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d3, areasT.data(), Np * sizeof(double), cudaMemcpyHostToDevice));
+        g.lat    = d;
+        g.lon    = d2;
+        g.areasT = d3;
     }
     {
         // hyperdiffusion and divergence damping strengths (src/ESP/esp_initial.cu:1292-1335,
@@ -529,6 +605,9 @@ int thorx_create(const thorx_grid* gr, const thorx_params* pr, void* stream, tho
     ctx->staging_len = (size_t)N * (nv + 1) * 3;
     if (dev_alloc(ctx, &ctx->staging, ctx->staging_len))
         return THORX_E_CUDA;
+    if (dev_alloc(ctx, &ctx->gd_part, (size_t)6 * globdiag_partials(g))
+        || dev_alloc(ctx, &ctx->gd_out, 6))
+        return THORX_E_CUDA;
 
     auto& F          = ctx->fields;
     F["Rho"]         = {&s.Rho, nv, 1};
@@ -579,7 +658,9 @@ void thorx_destroy(thorx_ctx* ctx) {
     delete ctx;
 }
 
-const char* thorx_last_error(const thorx_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+const char* thorx_last_error(const thorx_ctx* ctx) {
+    return ctx ? ctx->err.c_str() : g_free_err.c_str();
+}
 
 long thorx_field_size(const thorx_ctx* ctx, const char* name) {
     if (!ctx || !name)
@@ -797,6 +878,45 @@ int thorx_profile_steps(thorx_ctx* ctx, int nsteps, double* ms_per_class) {
         CK(cudaEventElapsedTime(&ms, e.second.first, e.second.second));
         ms_per_class[e.first] += ms;
     }
+    return 0;
+}
+
+int thorx_globdiag(thorx_ctx* ctx, double* out) {
+    if (!ctx)
+        return THORX_E_ARG;
+    if (!out)
+        return fail(ctx, THORX_E_ARG, "thorx_globdiag: null argument");
+    if (!ctx->state_set)
+        return fail(ctx, THORX_E_STATE, "thorx_globdiag: the state has not been set");
+    launch_globdiag(ctx->g, ctx->P, ctx->s, ctx->gd_part, ctx->gd_out, ctx->stream);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, ctx->gd_out, 6 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+int thorx_device_sum(const double* x, long long n, void* stream, double* out) {
+    int rc = check_sum_args("thorx_device_sum", x, n, out);
+    if (rc || n == 0)
+        return rc;
+    cudaStream_t    st = (cudaStream_t)stream;
+    const long long np = device_sum_partials(n);
+    double2*        part = nullptr;
+    cudaError_t     e    = cudaMalloc(&part, (size_t)(np + 1) * sizeof(double2));
+    if (e != cudaSuccess)
+        return free_fail(THORX_E_CUDA, std::string("thorx_device_sum: cudaMalloc: ") + cudaGetErrorString(e));
+    double* res = (double*)(part + np);
+    launch_device_sum(x, n, part, res, st);
+    e = cudaGetLastError();
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(out, res, sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(st);
+    cudaError_t ef = cudaFree(part);
+    if (e == cudaSuccess)
+        e = ef;
+    if (e != cudaSuccess)
+        return free_fail(THORX_E_CUDA, std::string("thorx_device_sum: ") + cudaGetErrorString(e));
     return 0;
 }
 

@@ -49,6 +49,8 @@ struct Geometry {
     const double*  nvecte;
     const double*  func_r;
     const double*  lat;
+    const double*  lon;
+    const double*  areasT;
     const double*  Altitude;
     const double*  Altitudeh;
     const double*  Kdh4;
@@ -102,5 +104,18 @@ void launch_momentum(const Geometry& g, const Phys& P, const State& s, double dt
 void launch_vertical(const Geometry& g, const Phys& P, const State& s, double dt,
                      cudaStream_t st);
 void launch_update_rk2(const Geometry& g, const Phys& P, const State& s, cudaStream_t st);
+
+// Global sums (thor_b200/csrc/globdiag.cu).
+// Partials the global-diagnostics reduction writes (double2 each, per quantity).
+int  globdiag_partials(const Geometry& g);
+// Energy, mass, AMx, AMy, AMz, entropy of the current state into out6 (device), using
+// 6 * globdiag_partials(g) double2 of scratch at part.
+void launch_globdiag(const Geometry& g, const Phys& P, const State& s, double2* part, double* out6,
+                     cudaStream_t st);
+// Partials a compensated sum of n doubles writes.
+long long device_sum_partials(long long n);
+// Compensated sum of x[0..n-1] (device) into *out (device), device_sum_partials(n) double2 of
+// scratch at part.
+void launch_device_sum(const double* x, long long n, double2* part, double* out, cudaStream_t st);
 
 } // namespace thorx
