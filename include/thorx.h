@@ -159,6 +159,29 @@ int thorx_globdiag(thorx_ctx* ctx, double* out);
  * after. Context-free: on error, thorx_last_error(NULL) gives this thread's message. */
 int thorx_device_sum(const double* x, long long n, void* stream, double* out);
 
+/* Allocation-free twin of thorx_device_sum. No counterpart in the reference.
+ *
+ * Same kernels, same order of addition, so the same bits as thorx_device_sum, but it allocates
+ * no memory at all: the partial sums go to a fixed 1 MiB array in the library's own device
+ * memory instead of a cudaMalloc per call. It is for callers that must not allocate:
+ *  - a time loop whose device memory is fully budgeted (the model's arrays plus a framework's
+ *    caching pool can leave no free megabyte, and a failed cudaMalloc mid-run loses the run);
+ *  - a loop that keeps other streams busy (output copies, physics on a second stream): cudaFree
+ *    synchronises the whole device and would stall that overlap at every diagnostic step.
+ * Limits and rules:
+ *  - n <= THORX_NOALLOC_SUM_MAX_N (134,217,728 doubles = 1 GiB of input); a larger n returns
+ *    THORX_E_ARG with a message saying so (use thorx_device_sum);
+ *  - there is one scratch per device per process: calls that overlap in time on the same device
+ *    (e.g. from two host threads at once) race on it and can return wrong sums; serialise them;
+ *  - the first call on each device sets the scratch up (it looks up the array's device address
+ *    with cudaGetSymbolAddress, with that device current); make that first call before any stream
+ *    capture begins;
+ *  - nothing in the scratch has to start at zero: every entry a call reads, that call has
+ *    written first.
+ * Argument checks, stream and error reporting as thorx_device_sum. */
+#define THORX_NOALLOC_SUM_MAX_N 134217728LL
+int thorx_device_sum_noalloc(const double* x, long long n, void* stream, double* out);
+
 /* ---- Icosahedral grid (replaces Icogrid::Icogrid, src/ESP/grid.cu:84-302) ----
  * Builds THOR's grid on the host: same point order, neighbours, rhombus maps, spring-dynamics
  * relaxation (beta = spring_beta, when spring_dynamics != 0), control volumes and operators,

@@ -95,6 +95,9 @@ def lib():
         L.thorx_globdiag.restype = ci
         L.thorx_device_sum.argtypes = [vp, ctypes.c_longlong, vp, ctypes.POINTER(ctypes.c_double)]
         L.thorx_device_sum.restype = ci
+        L.thorx_device_sum_noalloc.argtypes = [vp, ctypes.c_longlong, vp,
+                                               ctypes.POINTER(ctypes.c_double)]
+        L.thorx_device_sum_noalloc.restype = ci
         _lib = L
     return _lib
 
@@ -104,12 +107,26 @@ EXPORTED = ["thorx_create", "thorx_destroy", "thorx_last_error", "thorx_field_si
             "thorx_sync", "thorx_kernels_per_step", "thorx_grid_build", "thorx_grid_info",
             "thorx_grid_get", "thorx_grid_describe", "thorx_grid_free", "thorx_init_rest_state",
             "thorx_kernel_classes", "thorx_kernel_info", "thorx_profile_steps", "thorx_globdiag",
-            "thorx_device_sum"]
+            "thorx_device_sum", "thorx_device_sum_noalloc"]
 
 def device_sum(ptr, n, stream=0):
     """Compensated sum of n doubles at device address `ptr` (thorx_device_sum)."""
     out = ctypes.c_double()
     rc = lib().thorx_device_sum(ctypes.c_void_p(ptr), n, ctypes.c_void_p(stream), ctypes.byref(out))
+    if rc:
+        raise ThorxError(rc, lib().thorx_last_error(None).decode())
+    return out.value
+
+
+NOALLOC_SUM_MAX_N = 134217728
+
+
+def device_sum_noalloc(ptr, n, stream=0):
+    """thorx_device_sum_noalloc: the same sum with no allocation (fixed 1 MiB device scratch,
+    n <= NOALLOC_SUM_MAX_N, calls on one device must not overlap)."""
+    out = ctypes.c_double()
+    rc = lib().thorx_device_sum_noalloc(ctypes.c_void_p(ptr), n, ctypes.c_void_p(stream),
+                                        ctypes.byref(out))
     if rc:
         raise ThorxError(rc, lib().thorx_last_error(None).decode())
     return out.value

@@ -12,6 +12,8 @@
 // is the exact sum rounded once or twice, independent of the number of terms, and the order of
 // every addition is fixed by the launch shape alone: the same input gives the same bits on every
 // call.
+#include <mutex>
+
 #include "thorx_internal.h"
 
 namespace thorx {
@@ -178,6 +180,50 @@ void launch_device_sum(const double* x, long long n, double2* part, double* out,
     if (np > 0)
         sum_partials_kernel<<<(unsigned)np, kSumThreads, 0, st>>>(x, n, part);
     sum_final_kernel<<<1, kFinalThreads, 0, st>>>(part, (int)np, 0, out);
+}
+
+} // namespace thorx
+
+// ---------------------------------------------------------------------------------------------
+// Allocation-free device sum: the partials of a call live in this fixed array of the library's
+// own device memory instead of a cudaMalloc per call. 65536 partials of 2048 elements each cap
+// one call at 134,217,728 doubles; the entry after the partials holds the result. Nothing here
+// needs to start at zero: a call writes every partial it reads, and the result, before reading.
+// ---------------------------------------------------------------------------------------------
+namespace thorx {
+namespace {
+
+constexpr long long kNoAllocPartials = 65536;
+constexpr int       kMaxDevices      = 64;
+
+static __device__ __align__(256) double2 g_noalloc_scratch[kNoAllocPartials + 1];
+
+} // namespace
+
+long long noalloc_sum_max_n() { return kNoAllocPartials * kSumChunk; }
+
+// Device address of the scratch on the current device, looked up once per device (with that
+// device current) and remembered; later calls only read the table.
+cudaError_t noalloc_sum_scratch(double2** part, double** result) {
+    static std::mutex mu;
+    static double2*   addr[kMaxDevices] = {};
+    int               dev               = -1;
+    cudaError_t       e                 = cudaGetDevice(&dev);
+    if (e != cudaSuccess)
+        return e;
+    if (dev < 0 || dev >= kMaxDevices)
+        return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        void* p = nullptr;
+        e       = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess)
+            return e;
+        addr[dev] = (double2*)p;
+    }
+    *part   = addr[dev];
+    *result = (double*)(addr[dev] + kNoAllocPartials);
+    return cudaSuccess;
 }
 
 } // namespace thorx

@@ -920,4 +920,32 @@ int thorx_device_sum(const double* x, long long n, void* stream, double* out) {
     return 0;
 }
 
+int thorx_device_sum_noalloc(const double* x, long long n, void* stream, double* out) {
+    const char* fn = "thorx_device_sum_noalloc";
+    if (n > noalloc_sum_max_n())
+        return free_fail(THORX_E_ARG, std::string(fn) + ": n = " + std::to_string(n)
+                                          + " exceeds the fixed scratch limit of "
+                                          + std::to_string(noalloc_sum_max_n())
+                                          + " doubles; use thorx_device_sum");
+    int rc = check_sum_args(fn, x, n, out);
+    if (rc || n == 0)
+        return rc;
+    double2*    part   = nullptr;
+    double*     result = nullptr;
+    cudaError_t e      = noalloc_sum_scratch(&part, &result);
+    if (e != cudaSuccess)
+        return free_fail(THORX_E_CUDA, std::string(fn) + ": scratch set-up (cudaGetSymbolAddress): "
+                                           + cudaGetErrorString(e));
+    cudaStream_t st = (cudaStream_t)stream;
+    launch_device_sum(x, n, part, result, st);
+    e = cudaGetLastError();
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(out, result, sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess)
+        return free_fail(THORX_E_CUDA, std::string(fn) + ": " + cudaGetErrorString(e));
+    return 0;
+}
+
 } // extern "C"

@@ -117,5 +117,9 @@ long long device_sum_partials(long long n);
 // Compensated sum of x[0..n-1] (device) into *out (device), device_sum_partials(n) double2 of
 // scratch at part.
 void launch_device_sum(const double* x, long long n, double2* part, double* out, cudaStream_t st);
+// Largest n of the allocation-free sum, and its scratch on the current device (set up on the
+// first call per device): partials at *part, the result at *result.
+long long   noalloc_sum_max_n();
+cudaError_t noalloc_sum_scratch(double2** part, double** result);
 
 } // namespace thorx
