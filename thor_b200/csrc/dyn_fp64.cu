@@ -23,9 +23,41 @@
 namespace thorx {
 namespace {
 
-constexpr int kTile      = 32; // columns per tile (lanes)
-constexpr int kLevGroups = 8;  // warps per tile, each taking every 8th level
+#ifndef THORX_LEVGROUPS
+#define THORX_LEVGROUPS 8
+#endif
+constexpr int kTile      = 32;              // columns per tile (lanes)
+constexpr int kLevGroups = THORX_LEVGROUPS; // warps per tile, each taking every kLevGroups-th level
 constexpr int kColBlock  = 128;
+
+// Register budget of each tiled kernel (__maxnreg__), chosen by timing the g6/L48 step on a B200:
+// the kernels are latency-bound, and a cap of 80 registers lets 3 CTAs of 256 threads (24 warps)
+// share an SM where the uncapped code fits one or two; divm0 keeps 128 (2 CTAs), where tighter
+// caps spill more than the extra warps win back. Overridable with -DTHORX_REGS_<KERNEL>=n.
+#ifndef THORX_REGS_ADV
+#define THORX_REGS_ADV 80
+#endif
+#ifndef THORX_REGS_DIFF
+#define THORX_REGS_DIFF 80
+#endif
+#ifndef THORX_REGS_DIVM
+#define THORX_REGS_DIVM 128
+#endif
+#ifndef THORX_REGS_SLOW
+#define THORX_REGS_SLOW 80
+#endif
+#ifndef THORX_REGS_MOM
+#define THORX_REGS_MOM 80
+#endif
+#ifndef THORX_REGS_VERT
+#define THORX_REGS_VERT 80
+#endif
+#define THORX_KATTR_ADV __maxnreg__(THORX_REGS_ADV)
+#define THORX_KATTR_DIFF __maxnreg__(THORX_REGS_DIFF)
+#define THORX_KATTR_DIVM __maxnreg__(THORX_REGS_DIVM)
+#define THORX_KATTR_SLOW __maxnreg__(THORX_REGS_SLOW)
+#define THORX_KATTR_MOM __maxnreg__(THORX_REGS_MOM)
+#define THORX_KATTR_VERT __maxnreg__(THORX_REGS_VERT)
 
 __device__ __forceinline__ double gz(const double* __restrict__ plane, int id) {
     return id >= 0 ? __ldg(plane + id) : 0.0;
@@ -82,6 +114,49 @@ __device__ __forceinline__ SGeo stage_ring_geo(double* sm, const Geometry& g, in
     stage_cols(sm + 60 * kTile, g.nvecoa, 18, g.Np, col);
     return SGeo{sm, sm + 18 * kTile, sm + 24 * kTile, sm + 42 * kTile, sm + 60 * kTile,
                 (int)threadIdx.x};
+}
+
+// ---------------------------------------------------------------------------------------------
+// Per-level tables (LevelTable in thorx_internal.h), one thread per level/interface index. The
+// expressions are those the kernels evaluate per cell in the reference (same calls, same operand
+// order), so a table entry is the value each cell would have computed.
+// ---------------------------------------------------------------------------------------------
+__global__ void level_tables_kernel(Geometry g, Phys P, double* lt) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nv = g.nv, nvi = g.nvi;
+    if (i > nv)
+        return;
+    const double  A    = P.A;
+    const double* Alt  = g.Altitude;
+    const double* Alth = g.Altitudeh;
+    for (int t = 0; t < kLtCount; t++)
+        lt[t * nvi + i] = 0.0;
+    // interfaces (thor_vertical_int.h:188-420, thor_fastmodes.h:617-633, thor_adv_cor.h:330-336)
+    lt[kLtR2hD * nvi + i] = pow(Alth[i] + A, 2.0);
+    lt[kLtR2hI * nvi + i] = pow(Alth[i] + A, 2);
+    lt[kLtOr2 * nvi + i]  = 1 / pow(Alth[i] + A, 2);
+    lt[kLtTor3 * nvi + i] = 2 / pow(Alth[i] + A, 3);
+    if (i >= 1 && i <= nv - 1) {
+        const double dzp        = 1.0 / (Alth[i + 1] - Alth[i]);
+        const double dzh        = 1.0 / (Alt[i] - Alt[i - 1]);
+        const double dzm        = 1.0 / (Alth[i] - Alth[i - 1]);
+        lt[kLtDzp * nvi + i]    = dzp;
+        lt[kLtDzh * nvi + i]    = dzh;
+        lt[kLtDzm * nvi + i]    = dzm;
+        lt[kLtIntl * nvi + i]   = (Alt[i] - Alth[i]) * dzp * dzh;
+        lt[kLtInttm * nvi + i]  = -(Alt[i - 1] - Alth[i]) * dzm * dzh;
+        lt[kLtHIntt * nvi + i]  = (Alth[i] - Alt[i]) / (Alt[i - 1] - Alt[i]);
+        lt[kLtHIntl * nvi + i]  = (Alth[i] - Alt[i - 1]) / (Alt[i] - Alt[i - 1]);
+    }
+    // layer centres
+    if (i < nv) {
+        lt[kLtRscale * nvi + i] = P.DeepModel ? P.A / (Alt[i] + P.A) : 1.0;
+        lt[kLtR2cD * nvi + i]   = pow(Alt[i] + A, 2.0);
+        lt[kLtDr2dz * nvi + i]  = (pow(Alth[i + 1] + A, 3.0) - pow(Alth[i] + A, 3.0)) / 3.0;
+        lt[kLtGhv * nvi + i]    = pow(A / (A + Alt[i]), 2);
+        lt[kLtCIntt * nvi + i]  = (Alt[i] - Alth[i + 1]) / (Alth[i] - Alth[i + 1]);
+        lt[kLtCIntl * nvi + i]  = (Alt[i] - Alth[i]) / (Alth[i + 1] - Alth[i]);
+    }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -172,7 +247,7 @@ __device__ __forceinline__ double pot_temp(const ColLevel& q, double P_Ref) {
     return (P_Ref / (q.Rd * q.rho)) * pow(q.p / P_Ref, CvoCp);
 }
 
-__global__ void __launch_bounds__(kTile* kLevGroups) adv_temp_kernel(Geometry g, Phys P, State s) {
+__global__ void THORX_KATTR_ADV adv_temp_kernel(Geometry g, Phys P, State s) {
     __shared__ double sdiv[21 * kTile];
     const int         c0 = blockIdx.x * kTile, x = threadIdx.x, c = c0 + x;
     const int         Np = g.Np, nv = g.nv;
@@ -558,7 +633,7 @@ __device__ __forceinline__ void diffusion_body(const Geometry& g, const Phys& P,
         diffusion_point<n>(g, P, s, G, fr, ring, diff_in, diff_out, stepnum, last, c, lev);
 }
 
-__global__ void __launch_bounds__(kTile* kLevGroups)
+__global__ void THORX_KATTR_DIFF
     diffusion_kernel(Geometry g, Phys P, State s, const double* __restrict__ diff_in,
                      double* __restrict__ diff_out, int stepnum, bool last) {
     __shared__ double sgeo[kRingGeoRows * kTile];
@@ -677,7 +752,7 @@ __device__ __forceinline__ void divm0_body(const Geometry& g, const Phys& P, con
         divm0_point<n>(g, P, G, ring, c2, Mh, Wh, divg, c, lev);
 }
 
-__global__ void __launch_bounds__(kTile* kLevGroups)
+__global__ void THORX_KATTR_DIVM
     divm0_kernel(Geometry g, Phys P, const double* __restrict__ Mh, const double* __restrict__ Wh,
                  double* __restrict__ divg) {
     __shared__ double sgeo[kRingGeoRows * kTile];
@@ -892,7 +967,7 @@ __device__ __forceinline__ void slow_modes_body(const Geometry& g, const Phys& P
     }
 }
 
-__global__ void __launch_bounds__(kTile* kLevGroups)
+__global__ void THORX_KATTR_SLOW
     slow_modes_kernel(Geometry g, Phys P, State s, bool update_rk) {
     __shared__ double sgeo[kRingGeoRows * kTile];
     __shared__ double sdiv[21 * kTile];
@@ -958,7 +1033,7 @@ __device__ __forceinline__ void momentum_body(const Geometry& g, const Phys& P, 
     }
 }
 
-__global__ void __launch_bounds__(kTile* kLevGroups)
+__global__ void THORX_KATTR_MOM
     momentum_kernel(Geometry g, Phys P, State s, double dt) {
     __shared__ double sgeo[kRingGeoRows * kTile];
     __shared__ double sgrad[21 * kTile];
@@ -983,23 +1058,21 @@ __global__ void __launch_bounds__(kTile* kLevGroups)
 //   Density_Pressure_Eqs / _Poles (src/headers/dyn/thor_fastmodes.h:255-847).
 // Phase 1 (all levels in parallel): Sp, Sd at every level -> shared memory.
 // Phase 2 (all interfaces in parallel): the tridiagonal row (aa, bb, cc, -C0) of every interior
-//   interface, from the column's values at the two adjacent levels and Sp, Sd.
-// Phase 3 (one warp, lane = column): the Thomas elimination and back substitution, in shared
-//   memory, with the reference's operation sequence; Whs -> shared memory.
-// Phase 4 (all levels in parallel): Whs -> global and the density and pressure update.
-// Shared memory: div [21][32], Sp/Sd [2][nv][32], aa/bb/cc/dd [4][nv+1][32].
+//   interface, from the column's values at the two adjacent levels and Sp, Sd -> s.vrows.
+// Phase 3 (one warp, lane = column): the Thomas elimination and back substitution over the rows
+//   of its column, with the reference's operation sequence; Whs -> global.
+// Phase 4 (all levels in parallel): the density and pressure update.
+// The rows go through global memory (they stay in L1/L2: the same CTA writes and reads them
+// across a barrier) so that shared memory holds only div [21][32] and Sp/Sd [2][nv][32], and
+// several CTAs fit on an SM. Level-only factors come from the per-level tables.
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(kTile* kLevGroups)
+__global__ void THORX_KATTR_VERT
     vertical_kernel(Geometry g, Phys P, State s, double deltat) {
     extern __shared__ double smem[];
     const int nv = g.nv, nvi = g.nvi, Np = g.Np;
     double*   sdiv = smem;
     double*   sSp  = sdiv + 21 * kTile;
     double*   sSd  = sSp + nv * kTile;
-    double*   sa   = sSd + nv * kTile;
-    double*   sb   = sa + nvi * kTile;
-    double*   sc   = sb + nvi * kTile;
-    double*   sd   = sc + nvi * kTile;
     const int c0 = blockIdx.x * kTile, x = threadIdx.x, c = c0 + x;
     stage(sdiv, g.div, 21, Np, c0);
     __syncthreads();
@@ -1008,6 +1081,11 @@ __global__ void __launch_bounds__(kTile* kLevGroups)
     const bool    deep = P.DeepModel, nonh = P.NonHydro, ghv = P.GravHeightVar;
     const double* Alt  = g.Altitude;
     const double* Alth = g.Altitudeh;
+    const double* lt   = g.lt;
+    double*       ra   = s.vrows;                      // rows: a, b, c, d planes
+    double*       rb   = ra + (size_t)nvi * Np;
+    double*       rc   = rb + (size_t)nvi * Np;
+    double*       rd   = rc + (size_t)nvi * Np;
     int           nb[7];
     bool          pole = false;
     if (active) {
@@ -1022,26 +1100,30 @@ __global__ void __launch_bounds__(kTile* kLevGroups)
         for (int lev = threadIdx.y; lev < nv; lev += kLevGroups) {
             const int    i      = lev * Np + c;
             const double RoC    = s.Rd[i] / (s.Cp[i] - s.Rd[i]);
-            const double rscale = rscale_of(P, g, lev);
-            double       hv[7], Mv[7][3];
+            const double rscale = lt[kLtRscale * nvi + lev];
+            double       sdv[3], spv[3];
 #pragma unroll
             for (int j = 0; j < 7; j++) {
-                hv[j] = gz(s.h + lev * Np, nb[j]);
+                const double hv = gz(s.h + lev * Np, nb[j]);
 #pragma unroll
-                for (int k = 0; k < 3; k++)
-                    Mv[j][k] = gz(s.Mhs + (k * nv + lev) * Np, nb[j]);
+                for (int k = 0; k < 3; k++) {
+                    const double Mv = gz(s.Mhs + (k * nv + lev) * Np, nb[j]);
+                    const double d  = sdiv[(j * 3 + k) * kTile + x];
+                    if (j == 0) {
+                        sdv[k] = d * Mv;
+                        spv[k] = d * Mv * hv;
+                    }
+                    else {
+                        sdv[k] = sdv[k] + d * Mv;
+                        spv[k] = spv[k] + d * Mv * hv;
+                    }
+                }
             }
             double nflxr = 0.0, nflxp = 0.0;
 #pragma unroll
             for (int k = 0; k < 3; k++) {
-                double sdv = sdiv[k * kTile + x] * Mv[0][k], spv = sdiv[k * kTile + x] * Mv[0][k] * hv[0];
-#pragma unroll
-                for (int j = 1; j < 7; j++) {
-                    sdv = sdv + sdiv[(j * 3 + k) * kTile + x] * Mv[j][k];
-                    spv = spv + sdiv[(j * 3 + k) * kTile + x] * Mv[j][k] * hv[j];
-                }
-                nflxr -= rscale * sdv;
-                nflxp -= (RoC)*rscale * spv;
+                nflxr -= rscale * sdv[k];
+                nflxp -= (RoC)*rscale * spv[k];
             }
             sSp[lev * kTile + x] = nflxp + s.Slowp[i];
             sSd[lev * kTile + x] = nflxr + s.SlowRho[i];
@@ -1049,9 +1131,10 @@ __global__ void __launch_bounds__(kTile* kLevGroups)
     __syncthreads();
 
     // ---- phase 2: tridiagonal rows at the interior interfaces ----
-    if (active)
+    if (active) {
+        const double dt2 = pow(deltat, 2.0);
         for (int lev = 1 + threadIdx.y; lev < nv; lev += kLevGroups) {
-            const double altht = Alth[lev + 1], althl = Alth[lev - 1], alth = Alth[lev];
+            const double alth = Alth[lev];
             const double alt = Alt[lev], altl = Alt[lev - 1];
             double       hp = s.hh[(lev + 1) * Np + c], h = s.hh[lev * Np + c], hm = s.hh[(lev - 1) * Np + c];
             const double gp = s.gtilh[(lev + 1) * Np + c], gg = s.gtilh[lev * Np + c], gm = s.gtilh[(lev - 1) * Np + c];
@@ -1063,36 +1146,30 @@ __global__ void __launch_bounds__(kTile* kLevGroups)
             const double CRddu = (s.Cp[iu] - s.Rd[iu]) / (s.Rd[iu] * deltat * deltat);
             double       GCoRl, GCoRu;
             if (ghv) {
-                GCoRl = Gravit * pow(A / (A + altl), 2) * (s.Cp[il] - s.Rd[il]) / s.Rd[il];
-                GCoRu = Gravit * pow(A / (A + alt), 2) * (s.Cp[iu] - s.Rd[iu]) / s.Rd[iu];
+                GCoRl = Gravit * lt[kLtGhv * nvi + lev - 1] * (s.Cp[il] - s.Rd[il]) / s.Rd[il];
+                GCoRu = Gravit * lt[kLtGhv * nvi + lev] * (s.Cp[iu] - s.Rd[iu]) / s.Rd[iu];
             }
             else {
                 GCoRl = Gravit * (s.Cp[il] - s.Rd[il]) / s.Rd[il];
                 GCoRu = Gravit * (s.Cp[iu] - s.Rd[iu]) / s.Rd[iu];
             }
-            const double dzp  = 1.0 / (altht - alth);
-            const double dzh  = 1.0 / (alt - altl);
-            const double dzm  = 1.0 / (alth - althl);
-            const double dzph = dzp * dzh;
-            const double dzmh = dzm * dzh;
-            double       xi, xim, xip, intl, inttm, intt, aa, bb, ccv;
+            const double dzp   = lt[kLtDzp * nvi + lev];
+            const double dzh   = lt[kLtDzh * nvi + lev];
+            const double dzm   = lt[kLtDzm * nvi + lev];
+            const double dzph  = dzp * dzh;
+            const double dzmh  = dzm * dzh;
+            const double intl  = lt[kLtIntl * nvi + lev];
+            const double inttm = lt[kLtInttm * nvi + lev];
+            double       aa, bb, ccv;
             const double CRdd = (CRddl * (alt - alth) + CRddu * (alth - altl)) / (alt - altl);
             const double GCoR = (GCoRl * (alt - alth) + GCoRu * (alth - altl)) / (alt - altl);
             if (deep) {
-                hp                = hp * pow(altht + A, 2);
-                h                 = h * pow(alth + A, 2);
-                hm                = hm * pow(althl + A, 2);
-                const double or2  = 1 / pow(alth + A, 2);
-                const double tor3 = 2 / pow(alth + A, 3);
-                xi    = alt;
-                xim   = alth;
-                xip   = altht;
-                intl  = (xi - xim) * dzp * dzh;
-                xi    = altl;
-                xim   = althl;
-                xip   = alth;
-                inttm = -(xi - xip) * dzm * dzh;
-                ccv   = -dzph * or2 * hp - inttm * (gp + GCoR - tor3 * hp);
+                hp                = hp * lt[kLtR2hI * nvi + lev + 1];
+                h                 = h * lt[kLtR2hI * nvi + lev];
+                hm                = hm * lt[kLtR2hI * nvi + lev - 1];
+                const double or2  = lt[kLtOr2 * nvi + lev];
+                const double tor3 = lt[kLtTor3 * nvi + lev];
+                ccv               = -dzph * or2 * hp - inttm * (gp + GCoR - tor3 * hp);
                 if (nonh)
                     bb = CRdd + (dzph + dzmh) * or2 * h + (intl - inttm) * (gg + GCoR - tor3 * h);
                 else
@@ -1100,15 +1177,7 @@ __global__ void __launch_bounds__(kTile* kLevGroups)
                 aa = -dzmh * or2 * hm + intl * (gm + GCoR - tor3 * hm);
             }
             else {
-                xi    = alt;
-                xim   = alth;
-                xip   = altht;
-                intl  = (xi - xim) * dzp * dzh;
-                xi    = altl;
-                xim   = althl;
-                xip   = alth;
-                inttm = -(xi - xip) * dzm * dzh;
-                ccv   = -dzph * hp - inttm * (gp + GCoR);
+                ccv = -dzph * hp - inttm * (gp + GCoR);
                 if (nonh)
                     bb = CRdd + (dzph + dzmh) * h + (intl - inttm) * (gg + GCoR);
                 else
@@ -1117,49 +1186,52 @@ __global__ void __launch_bounds__(kTile* kLevGroups)
             }
             const double dSpdz = (Sp - Spl) * dzh;
             const double dPdz  = (p - pl) * dzh;
-            xi   = alth;
-            xim  = altl;
-            xip  = alt;
-            intt = (xi - xip) / (xim - xip);
-            intl = (xi - xim) / (xip - xim);
-            const double rhohs = rl * intt + r * intl;
-            const double Sdh   = Sdl * intt + Sd * intl;
+            const double intt2 = lt[kLtHIntt * nvi + lev];
+            const double intl2 = lt[kLtHIntl * nvi + lev];
+            const double rhohs = rl * intt2 + r * intl2;
+            const double Sdh   = Sdl * intt2 + Sd * intl2;
             const double Srh   = s.SlowWh[lev * Np + c];
+            const double whs   = nonh ? s.Whs[lev * Np + c] : 0.0;
             double       C0;
             if (!nonh) {
-                if (ghv)
-                    C0 = (pow(deltat, 2.0) * dSpdz + pow(deltat, 2.0) * Gravit * pow(A / (A + alt), 2) * Sdh
-                          + Gravit * pow(A / (A + alt), 2) * deltat * rhohs + deltat * dPdz - deltat * Srh)
-                         * (CRdd);
-                else
-                    C0 = (pow(deltat, 2.0) * dSpdz + pow(deltat, 2.0) * Gravit * Sdh + Gravit * deltat * rhohs
+                if (ghv) {
+                    const double gh = lt[kLtGhv * nvi + lev];
+                    C0 = (dt2 * dSpdz + dt2 * Gravit * gh * Sdh + Gravit * gh * deltat * rhohs
                           + deltat * dPdz - deltat * Srh)
+                         * (CRdd);
+                }
+                else
+                    C0 = (dt2 * dSpdz + dt2 * Gravit * Sdh + Gravit * deltat * rhohs + deltat * dPdz
+                          - deltat * Srh)
                          * (CRdd);
             }
             else {
-                const double whs = s.Whs[lev * Np + c];
-                if (ghv)
-                    C0 = (-whs + pow(deltat, 2.0) * dSpdz + pow(deltat, 2.0) * Gravit * pow(A / (A + alt), 2) * Sdh
-                          + Gravit * pow(A / (A + alt), 2) * deltat * rhohs + deltat * dPdz - deltat * Srh)
+                if (ghv) {
+                    const double gh = lt[kLtGhv * nvi + lev];
+                    C0 = (-whs + dt2 * dSpdz + dt2 * Gravit * gh * Sdh + Gravit * gh * deltat * rhohs
+                          + deltat * dPdz - deltat * Srh)
                          * (CRdd);
+                }
                 else
-                    C0 = (-whs + pow(deltat, 2.0) * dSpdz + pow(deltat, 2.0) * Gravit * Sdh
-                          + Gravit * deltat * rhohs + deltat * dPdz - deltat * Srh)
+                    C0 = (-whs + dt2 * dSpdz + dt2 * Gravit * Sdh + Gravit * deltat * rhohs
+                          + deltat * dPdz - deltat * Srh)
                          * (CRdd);
             }
-            sa[lev * kTile + x] = aa;
-            sb[lev * kTile + x] = bb;
-            sc[lev * kTile + x] = ccv;
-            sd[lev * kTile + x] = -C0;
+            ra[lev * Np + c] = aa;
+            rb[lev * Np + c] = bb;
+            rc[lev * Np + c] = ccv;
+            rd[lev * Np + c] = -C0;
         }
+    }
     __syncthreads();
 
     // ---- phase 3: Thomas elimination and back substitution (one warp) ----
     if (threadIdx.y == 0 && active) {
         double cprev = 0, dprev = 0;
         for (int lev = 1; lev < nv; lev++) {
-            const double aa = sa[lev * kTile + x], bb = sb[lev * kTile + x];
-            double       ccv = sc[lev * kTile + x], ddv = sd[lev * kTile + x];
+            const int    q  = lev * Np + c;
+            const double aa = ra[q], bb = rb[q];
+            double       ccv = rc[q], ddv = rd[q];
             if (lev == 1) {
                 ccv = ccv / bb;
                 ddv = ddv / bb;
@@ -1169,78 +1241,75 @@ __global__ void __launch_bounds__(kTile* kLevGroups)
                 ccv *= t;
                 ddv = (ddv - dprev * aa) * t;
             }
-            sc[lev * kTile + x] = ccv;
-            sd[lev * kTile + x] = ddv;
-            cprev               = ccv;
-            dprev               = ddv;
+            rc[q] = ccv;
+            rd[q] = ddv;
+            cprev = ccv;
+            dprev = ddv;
         }
         double w           = 0.0;
-        sd[nv * kTile + x] = 0.0;
+        s.Whs[nv * Np + c] = 0.0;
         for (int lev = nv - 1; lev > 0; lev--) {
-            w = (lev == nv - 1) ? sd[lev * kTile + x] : (-sc[lev * kTile + x] * w + sd[lev * kTile + x]);
-            sd[lev * kTile + x] = w; // sd now holds Whs
+            const int q = lev * Np + c;
+            w           = (lev == nv - 1) ? rd[q] : (-rc[q] * w + rd[q]);
+            s.Whs[q]    = w;
         }
-        sd[x] = 0.0;
+        s.Whs[c] = 0.0;
     }
     __syncthreads();
     if (!active)
         return;
 
-    // ---- phase 4: Whs out, Density_Pressure_Eqs ----
+    // ---- phase 4: Density_Pressure_Eqs ----
     const bool   eeq   = P.energy;
     const double P_Ref = P.P_Ref;
     for (int lev = threadIdx.y; lev < nv; lev += kLevGroups) {
-        const int i         = lev * Np + c;
-        s.Whs[lev * Np + c] = sd[lev * kTile + x];
-        if (lev == nv - 1)
-            s.Whs[nv * Np + c] = 0.0;
+        const int    i     = lev * Np + c;
         const double Cv    = s.Cp[i] - s.Rd[i];
-        const double altht = Alth[lev + 1], althl = Alth[lev];
-        const double dz    = altht - althl;
+        const double dz    = Alth[lev + 1] - Alth[lev];
         double       r2p, r2m, r2l, rscale, dr2dz;
         if (deep) {
-            const double alt = Alt[lev];
-            r2p              = pow(altht + A, 2.0);
-            r2m              = pow(alt + A, 2.0);
-            r2l              = pow(althl + A, 2.0);
-            rscale           = A / (alt + A);
-            dr2dz            = (pow(altht + A, 3.0) - pow(althl + A, 3.0)) / 3.0;
+            r2p    = lt[kLtR2hD * nvi + lev + 1];
+            r2m    = lt[kLtR2cD * nvi + lev];
+            r2l    = lt[kLtR2hD * nvi + lev];
+            rscale = lt[kLtRscale * nvi + lev];
+            dr2dz  = lt[kLtDr2dz * nvi + lev];
         }
         else {
             r2p = r2m = r2l = rscale = 1.0;
             dr2dz                    = r2m * dz;
         }
-        double vs[7][3], v1[7][3], ptv[7];
+        double sr[3], st[3];
 #pragma unroll
         for (int j = 0; j < 7; j++) {
             const int id = nb[j];
+            double    vs[3] = {0.0, 0.0, 0.0}, v1[3] = {0.0, 0.0, 0.0}, ptv = 0.0;
             if (id >= 0) {
 #pragma unroll
                 for (int k = 0; k < 3; k++) {
-                    vs[j][k] = s.Mhs[(k * nv + lev) * Np + id];
-                    v1[j][k] = vs[j][k] + s.Mhk[(k * nv + lev) * Np + id];
+                    vs[k] = s.Mhs[(k * nv + lev) * Np + id];
+                    v1[k] = vs[k] + s.Mhk[(k * nv + lev) * Np + id];
                 }
                 const int q = lev * Np + id;
-                ptv[j]      = eeq ? (s.h[q] + s.ep[q] + s.ek[q]) : s.pt[q];
+                ptv         = eeq ? (s.h[q] + s.ep[q] + s.ek[q]) : s.pt[q];
             }
-            else {
 #pragma unroll
-                for (int k = 0; k < 3; k++)
-                    vs[j][k] = v1[j][k] = 0.0;
-                ptv[j] = 0.0;
+            for (int k = 0; k < 3; k++) {
+                const double d = sdiv[(j * 3 + k) * kTile + x];
+                if (j == 0) {
+                    sr[k] = d * vs[k];
+                    st[k] = d * v1[k] * ptv;
+                }
+                else {
+                    sr[k] = sr[k] + d * vs[k];
+                    st[k] = st[k] + d * v1[k] * ptv;
+                }
             }
         }
         double nflxr = 0.0, nflxpt = 0.0;
 #pragma unroll
         for (int k = 0; k < 3; k++) {
-            double sr = sdiv[k * kTile + x] * vs[0][k], st = sdiv[k * kTile + x] * v1[0][k] * ptv[0];
-#pragma unroll
-            for (int j = 1; j < 7; j++) {
-                sr = sr + sdiv[(j * 3 + k) * kTile + x] * vs[j][k];
-                st = st + sdiv[(j * 3 + k) * kTile + x] * v1[j][k] * ptv[j];
-            }
-            nflxr += rscale * sr;
-            nflxpt += rscale * st;
+            nflxr += rscale * sr[k];
+            nflxpt += rscale * st[k];
         }
         auto phv = [&](int l) -> double {
             const int q = l * Np + c;
@@ -1249,17 +1318,17 @@ __global__ void __launch_bounds__(kTile* kLevGroups)
         double whl, wht, whl2, wht2, phl, pht;
         if (lev == 0) {
             whl  = 0.0;
-            wht  = sd[(lev + 1) * kTile + x];
+            wht  = s.Whs[(lev + 1) * Np + c];
             whl2 = 0.0;
-            wht2 = sd[(lev + 1) * kTile + x] + s.Whk[(lev + 1) * Np + c];
+            wht2 = wht + s.Whk[(lev + 1) * Np + c];
             phl  = 0.0;
             pht  = phv(lev + 1);
         }
         else {
-            whl  = sd[lev * kTile + x];
-            wht  = sd[(lev + 1) * kTile + x];
-            whl2 = sd[lev * kTile + x] + s.Whk[lev * Np + c];
-            wht2 = sd[(lev + 1) * kTile + x] + s.Whk[(lev + 1) * Np + c];
+            whl  = s.Whs[lev * Np + c];
+            wht  = s.Whs[(lev + 1) * Np + c];
+            whl2 = whl + s.Whk[lev * Np + c];
+            wht2 = wht + s.Whk[(lev + 1) * Np + c];
             phl  = phv(lev);
             pht  = phv(lev + 1);
         }
@@ -1275,16 +1344,19 @@ __global__ void __launch_bounds__(kTile* kLevGroups)
         if (eeq) {
             aux += s.Etotal[i] + (s.diffpr[i]) * deltat + s.Qheat[i] * deltat;
             s.Etotal[i] = aux;
-            const double w = (whl2 * (Alth[lev + 1] - Alt[lev]) + wht2 * (Alt[lev] - Alth[lev]))
+            const double m0 = s.Mhs[(0 * nv + lev) * Np + c] + s.Mhk[(0 * nv + lev) * Np + c];
+            const double m1 = s.Mhs[(1 * nv + lev) * Np + c] + s.Mhk[(1 * nv + lev) * Np + c];
+            const double m2 = s.Mhs[(2 * nv + lev) * Np + c] + s.Mhk[(2 * nv + lev) * Np + c];
+            const double w  = (whl2 * (Alth[lev + 1] - Alt[lev]) + wht2 * (Alt[lev] - Alth[lev]))
                              / (Alth[lev + 1] - Alth[lev]);
             double Epot_kin;
             if (ghv)
-                Epot_kin = (rhos_new + rk_) * Gravit * pow(A / (A + Alt[lev]), 2) * Alt[lev]
-                           + 0.5 * (pow(v1[0][0], 2) + pow(v1[0][1], 2) + pow(v1[0][2], 2) + pow(w, 2))
+                Epot_kin = (rhos_new + rk_) * Gravit * lt[kLtGhv * nvi + lev] * Alt[lev]
+                           + 0.5 * (pow(m0, 2) + pow(m1, 2) + pow(m2, 2) + pow(w, 2))
                                  / (rhos_new + rk_);
             else
                 Epot_kin = (rhos_new + rk_) * Gravit * Alt[lev]
-                           + 0.5 * (pow(v1[0][0], 2) + pow(v1[0][1], 2) + pow(v1[0][2], 2) + pow(w, 2))
+                           + 0.5 * (pow(m0, 2) + pow(m1, 2) + pow(m2, 2) + pow(w, 2))
                                  / (rhos_new + rk_);
             s.ps[i] = s.Rd[i] / Cv * (aux - Epot_kin) - s.pk[i];
         }
@@ -1302,9 +1374,10 @@ __global__ void __launch_bounds__(kTile* kLevGroups)
 // Every level first reads the two interfaces it interpolates between; the writes follow a
 // barrier, so no level sees another's update.
 // ---------------------------------------------------------------------------------------------
-constexpr int kMaxLevelsPerThread = 16; // nv <= kLevGroups * 16
+constexpr int kRk2Groups          = 8;
+constexpr int kMaxLevelsPerThread = 16; // nv <= kRk2Groups * 16
 
-__global__ void __launch_bounds__(kTile* kLevGroups) update_rk2_kernel(Geometry g, Phys P, State s) {
+__global__ void __launch_bounds__(kTile* kRk2Groups) update_rk2_kernel(Geometry g, Phys P, State s) {
     const int  c  = blockIdx.x * kTile + threadIdx.x;
     const int  Np = g.Np, nv = g.nv;
     const bool active = c < g.N;
@@ -1320,7 +1393,7 @@ __global__ void __launch_bounds__(kTile* kLevGroups) update_rk2_kernel(Geometry 
         int cnt = 0;
 #pragma unroll
         for (int t = 0; t < kMaxLevelsPerThread; t++) {
-            const int lev = threadIdx.y + t * kLevGroups;
+            const int lev = threadIdx.y + t * kRk2Groups;
             if (lev < nv) {
                 const double althl = (lev == 0) ? 0.0 : g.Altitudeh[lev];
                 const double altht = g.Altitudeh[lev + 1];
@@ -1338,7 +1411,7 @@ __global__ void __launch_bounds__(kTile* kLevGroups) update_rk2_kernel(Geometry 
         return;
 #pragma unroll
     for (int t = 0; t < kMaxLevelsPerThread; t++) {
-        const int lev = threadIdx.y + t * kLevGroups;
+        const int lev = threadIdx.y + t * kRk2Groups;
         if (lev >= nv)
             break;
         const double Mx  = s.Mhs[(0 * nv + lev) * Np + c] + s.Mhk[(0 * nv + lev) * Np + c];
@@ -1364,7 +1437,11 @@ inline dim3 tile_block() { return dim3(kTile, kLevGroups); }
 
 } // namespace
 
-int max_levels() { return kLevGroups * kMaxLevelsPerThread; }
+int max_levels() { return kRk2Groups * kMaxLevelsPerThread; }
+
+void launch_level_tables(const Geometry& g, const Phys& P, double* lt, cudaStream_t st) {
+    level_tables_kernel<<<(g.nvi + 127) / 128, 128, 0, st>>>(g, P, lt);
+}
 
 void launch_profx(const Geometry& g, const Phys& P, const State& s, cudaStream_t st) {
     profx_kernel<<<(g.N + kColBlock - 1) / kColBlock, kColBlock, 0, st>>>(g, P, s);
@@ -1393,9 +1470,7 @@ void launch_momentum(const Geometry& g, const Phys& P, const State& s, double dt
                      cudaStream_t st) {
     momentum_kernel<<<tile_grid_tail(g), tile_block(), 0, st>>>(g, P, s, dt);
 }
-size_t vertical_smem_bytes(const Geometry& g) {
-    return sizeof(double) * kTile * (21 + 2 * g.nv + 4 * g.nvi);
-}
+size_t vertical_smem_bytes(const Geometry& g) { return sizeof(double) * kTile * (21 + 2 * g.nv); }
 void launch_vertical(const Geometry& g, const Phys& P, const State& s, double dt,
                      cudaStream_t st) {
     const size_t  smem       = vertical_smem_bytes(g);
@@ -1408,7 +1483,7 @@ void launch_vertical(const Geometry& g, const Phys& P, const State& s, double dt
     vertical_kernel<<<tile_grid(g), tile_block(), smem, st>>>(g, P, s, dt);
 }
 void launch_update_rk2(const Geometry& g, const Phys& P, const State& s, cudaStream_t st) {
-    update_rk2_kernel<<<tile_grid(g), tile_block(), 0, st>>>(g, P, s);
+    update_rk2_kernel<<<tile_grid(g), dim3(kTile, kRk2Groups), 0, st>>>(g, P, s);
 }
 
 } // namespace thorx

@@ -568,10 +568,16 @@ int thorx_create(const thorx_grid* gr, const thorx_params* pr, void* stream, tho
         ctx->Altitude_h.assign(gr->Altitude, gr->Altitude + nv);
         ctx->Altitudeh_h.assign(gr->Altitudeh, gr->Altitudeh + nv + 1);
         CK(cudaMemcpy(alth, gr->Altitudeh, (nv + 1) * 8, cudaMemcpyHostToDevice));
+        double* lt;
+        if (dev_alloc(ctx, &lt, (size_t)kLtCount * (nv + 1)))
+            return THORX_E_CUDA;
+        g.lt = lt;
         g.Kdh4      = a;
         g.Kdhz      = b;
         g.Altitude  = alt;
         g.Altitudeh = alth;
+        launch_level_tables(g, P, lt, ctx->stream);
+        CK(cudaGetLastError());
     }
 
     // state
@@ -587,7 +593,8 @@ int thorx_create(const thorx_grid* gr, const thorx_params* pr, void* stream, tho
               {&s.Cp, cell},        {&s.h, cell},        {&s.hh, iface},       {&s.pt, cell},
               {&s.pth, iface},      {&s.gtil, cell},     {&s.gtilh, iface},    {&s.Adv, 3 * cell},
               {&s.diff, 12 * cell}, {&s.diffmh, 3 * cell}, {&s.diffw, cell},   {&s.diffrh, cell},
-              {&s.diffpr, cell},    {&s.divg, 3 * cell}, {&s.SlowMh, 3 * cell}, {&s.SlowWh, iface},
+              {&s.diffpr, cell},    {&s.divg, 3 * cell}, {&s.vrows, 4 * iface}, {&s.SlowMh, 3 * cell},
+              {&s.SlowWh, iface},
               {&s.SlowRho, cell},   {&s.Slowp, cell},    {&s.Qheat, cell},     {&s.dMh, 3 * cell},
               {&s.dWh, iface}};
     for (auto& x : al)

@@ -55,6 +55,32 @@ struct Geometry {
     const double*  Altitudeh;
     const double*  Kdh4;
     const double*  Kdhz;
+    const double*  lt; // per-level tables, lt[t * nvi + i] (LevelTable below)
+};
+
+// Per-level quantities that every column shares, tabulated once on the device at context
+// creation with the same expressions the kernels would evaluate per cell (so the values are
+// the same bits). "centre" entries are indexed by level 0..nv-1, "interface" entries by
+// interface 0..nv (only 1..nv-1 where marked interior).
+enum LevelTable : int {
+    kLtRscale, // centre: DeepModel ? A / (Alt + A) : 1
+    kLtR2cD,   // centre: pow(Alt + A, 2.0)
+    kLtDr2dz,  // centre: (pow(Alth[l+1] + A, 3.0) - pow(Alth[l] + A, 3.0)) / 3.0
+    kLtGhv,    // centre: pow(A / (A + Alt), 2)
+    kLtCIntt,  // centre from its interfaces: (Alt - Alth[l+1]) / (Alth[l] - Alth[l+1])
+    kLtCIntl,  // centre from its interfaces: (Alt - Alth[l]) / (Alth[l+1] - Alth[l])
+    kLtR2hD,   // interface: pow(Alth + A, 2.0)
+    kLtR2hI,   // interface: pow(Alth + A, 2)
+    kLtOr2,    // interface: 1 / pow(Alth + A, 2)
+    kLtTor3,   // interface: 2 / pow(Alth + A, 3)
+    kLtDzp,    // interior interface: 1 / (Alth[i+1] - Alth[i])
+    kLtDzh,    // interior interface: 1 / (Alt[i] - Alt[i-1])
+    kLtDzm,    // interior interface: 1 / (Alth[i] - Alth[i-1])
+    kLtIntl,   // interior interface: (Alt[i] - Alth[i]) * dzp * dzh
+    kLtInttm,  // interior interface: -(Alt[i-1] - Alth[i]) * dzm * dzh
+    kLtHIntt,  // interior interface from centres: (Alth[i] - Alt[i]) / (Alt[i-1] - Alt[i])
+    kLtHIntl,  // interior interface from centres: (Alth[i] - Alt[i-1]) / (Alt[i] - Alt[i-1])
+    kLtCount
 };
 
 struct Phys {
@@ -78,6 +104,7 @@ struct State {
     double *diff;                 // 6 planes (intermediate hyperdiffusion passes)
     double *diffmh, *diffw, *diffrh, *diffpr;
     double *divg;                 // 3 planes
+    double *vrows;                // 4 x (nv+1) planes: tridiagonal rows of the vertical solve
     double *SlowMh, *SlowWh, *SlowRho, *Slowp;
     double *Qheat, *dMh, *dWh;    // physics-module coupling (profx_Qheat_d, profx_dMh_d, ...)
     unsigned int* flags;          // device status word (bit 0: NaN in temperature)
@@ -89,6 +116,9 @@ enum : unsigned int { kFlagNaN = 1u };
 int max_levels();
 // Dynamic shared memory of the vertical implicit kernel.
 size_t vertical_smem_bytes(const Geometry& g);
+
+// Fills the per-level tables lt[kLtCount * (nv+1)] (thor_b200/csrc/dyn_fp64.cu).
+void launch_level_tables(const Geometry& g, const Phys& P, double* lt, cudaStream_t st);
 
 // Kernel launchers (thor_b200/csrc/dyn_fp64.cu).
 void launch_profx(const Geometry& g, const Phys& P, const State& s, cudaStream_t st);
