@@ -41,8 +41,21 @@ STATE = ["Rho", "pressure", "Mh", "Wh", "W"]
 FALLBACK_HBM_GBS = 6650.0
 
 
+CPU_SAMPLE_STEPS = 6  # oracle steps timed for cpu_baseline at g6/L48: ~10 s on 16 cores
+
+
+def workload_name():
+    return "Held-Suarez g%d/L%d dt=%g (%d columns x %d levels)" % (
+        GLEVEL, NV, DT, 2 + 10 * 4 ** GLEVEL, NV)
+
+
 def sim_days_per_hour(nsteps, seconds, dt=DT):
     return (nsteps * dt / 86400.0) / (seconds / 3600.0)
+
+
+def set_workload(glevel, nv):
+    global GLEVEL, NV
+    GLEVEL, NV = glevel, nv
 
 
 def params(form):
@@ -173,8 +186,8 @@ def cpu_baseline(grid, nsteps):
     o.close()
     return dict(value=sim_days_per_hour(nsteps, sec), unit="sim-days/wall-hour", cores=threads,
                 kind="port", seconds=sec,
-                sample="%d large steps of the g6/L48 Held-Suarez step (after 1 warm-up), "
-                       "oracle/thor_oracle.cpp, OpenMP over columns" % nsteps)
+                sample="%d large steps of the g%d/L%d Held-Suarez step (after 1 warm-up), "
+                       "oracle/thor_oracle.cpp, OpenMP over columns" % (nsteps, GLEVEL, NV))
 
 
 def initial_state_host(grid):
@@ -200,7 +213,7 @@ def run_reference(args):
             "ms_per_step": base["seconds"] * 1000.0 / max(1, min(args.steps, 3)),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded rest state)",
-            "config": {"workload": "Held-Suarez g6/L48 dt=600 (40962 columns x 48 levels)",
+            "config": {"workload": workload_name(),
                        "glevel": GLEVEL, "nv": NV, "dt": DT, "form": "fp64"},
             "cpu_baseline": {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": value, "unit": "sim-days/wall-hour", "h2d_bytes_per_step": 0,
@@ -315,26 +328,31 @@ def run_ours(args):
         x.get(f, host[f])
     ke = max(3, min(args.steps, 10))
     torch.cuda.synchronize(device)
-    t0 = time.perf_counter()
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
     for _ in range(ke):
         for f in STATE:
             x.set(f, host[f])
         x.step(1)
         for f in STATE:
             x.get(f, host[f])
+    e3.record(stream)
+    e3.synchronize()
     x.sync()
-    te = time.perf_counter() - t0
+    te = e2.elapsed_time(e3) / 1000.0
     te = max_over_ranks(te, world, device)
     io_bytes = sum(host[f].nbytes for f in STATE)
     e2e = {"value": world * sim_days_per_hour(ke, te), "unit": "sim-days/wall-hour",
            "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes, "steps": ke,
            "what": "thorx_set_field(state) + thorx_step(1) + thorx_get_field(state) per step, "
-                   "pinned host buffers in the reference layout"}
+                   "pinned host buffers in the reference layout, CUDA events on the context "
+                   "stream around all of it"}
     finite = all(np.isfinite(host[f]).all() for f in STATE)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        b = cpu_baseline(grid, 2)
+        b = cpu_baseline(grid, CPU_SAMPLE_STEPS)
         cpu = {k: b[k] for k in ("value", "unit", "cores", "kind", "sample")}
 
     line = {"metric": METRIC, "value": value, "unit": "sim-days/wall-hour", "n_gpus": world,
@@ -342,7 +360,7 @@ def run_ours(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if args.form == "fp64" else "f32+f64",
             "data": "synthetic (seeded isothermal rest state, Held-Suarez forcing)",
-            "config": {"workload": "Held-Suarez g6/L48 dt=600 (40962 columns x 48 levels)",
+            "config": {"workload": workload_name(),
                        "glevel": GLEVEL, "nv": NV, "dt": DT, "form": args.form,
                        "parallelism": "replicas%d" % world,
                        "l2": "state resident in HBM (%.2f GB per level-field x ~40 fields), "
@@ -374,7 +392,11 @@ def main():
     ap.add_argument("--form", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--glevel", type=int, default=GLEVEL,
+                    help="grid level (default 6; smaller cases are for profiling captures)")
+    ap.add_argument("--nv", type=int, default=NV, help="vertical levels (default 48)")
     args = ap.parse_args()
+    set_workload(args.glevel, args.nv)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
