@@ -140,6 +140,49 @@ int thorx_kernel_info(const thorx_ctx* ctx, int k, const char** name, double* by
                       int* launches_per_step);
 int thorx_profile_steps(thorx_ctx* ctx, int nsteps, double* ms_per_class);
 
+/* ---- Double-gray radiative transfer (radiative_transfer module with rt_type = DualbandGray,
+ * src/physics/modules/src/radiative_transfer.cu, kernel rtm_dual_band
+ * src/physics/modules/inc/profx_RT.h:316-587) and the insolation it uses (Insolation,
+ * src/ESP/insolation.cu). The .thr keys of the same names; lengths in m (the .thr file gives
+ * planet_star_dist in au and radius_star in solar radii), angles in degrees. ---- */
+typedef struct {
+    double Tstar;            /* stellar effective temperature [K]                      */
+    double planet_star_dist; /* semi-major axis [m]                                   */
+    double radius_star;      /* stellar radius [m]                                    */
+    double diff_ang;         /* 1 / diffusivity factor                                */
+    double Tint;             /* internal temperature [K]                              */
+    double albedo;           /* Bond albedo                                           */
+    double kappa_sw, kappa_lw, kappa_lw_pole; /* gray opacities [m^2/kg]              */
+    double n_sw, n_lw;       /* pressure-scaling exponents of the optical depths      */
+    double f_lw;             /* fraction of the LW optical depth that is uniform      */
+    double mean_motion;      /* orbital mean motion [rad/s] (sync_rot: Omega is used) */
+    double alpha_i;          /* initial right ascension of the star [deg]             */
+    double true_long_i;      /* initial true longitude of the planet [deg]            */
+    double ecc;              /* orbital eccentricity, 0 <= ecc < 1                    */
+    double obliquity;        /* [deg]                                                 */
+    double longp;            /* longitude of periastron [deg]                         */
+    int    latf_lw;          /* sin^2(lat) variation of kappa_lw toward kappa_lw_pole */
+    int    rt1Dmode;         /* cos(zenith) fixed at 0.5                              */
+    int    sync_rot;         /* synchronous rotation                                  */
+    int    surface;          /* must be 0: the surface layer is not implemented       */
+    int    spinup_start, spinup_stop, spindown_start, spindown_stop; /* steps, -1 = off */
+    int    first_step;       /* step number of the next physics step (1 at a fresh start) */
+} thorx_rt_params;
+
+/* Adds insolation + double-gray RT to every following ProfX, between the benchmark forcing and
+ * the pressure update, heating into profx_Qheat (replaces the module's initialise_memory /
+ * initial_conditions / phy_loop, radiative_transfer.cu:384-460,769-1105, and
+ * Insolation::initial_conditions / phy_loop, insolation.cu:292-490). Call once, after
+ * thorx_create; a step graph captured earlier is re-captured. Adds the fields "cos_zenith",
+ * "insol", "insol_ann", "ASR", "OLR" ([col]), "phtemp", "thtemp", "fsw_up", "fsw_dn",
+ * "flw_up", "flw_dn" ([col][lev+1]), "tau" ([col][lev][2]: SW, LW), "ttemp", "dtemp",
+ * "DG_Qheat" ([col][lev]). THORX_E_UNSUPPORTED for surface != 0 and for GravHeightVar (whose
+ * reference shortwave code reads past the end of Altitudeh). */
+int thorx_rt_enable(thorx_ctx* ctx, const thorx_rt_params* rt);
+/* Absorbed shortwave and outgoing longwave power of the last RT call, summed over the globe
+ * (the reference's ASR_tot / OLR_tot, radiative_transfer.cu:1083-1084), compensated sums. */
+int thorx_rt_totals(thorx_ctx* ctx, double* asr, double* olr);
+
 /* ---- Global conserved quantities (replaces ESP::globdiag, src/ESP/profx_driver.cu:476-569,
  * with the per-cell terms of CalcTotEnergy / CalcMass / CalcAngMom / CalcEntropy,
  * src/ESP/profx_globdiag.cu:45-252; no surface term) ----

@@ -41,6 +41,8 @@
 #include "phy/profx_auxiliary.h"
 #include "phy/profx_globdiag.h"
 #include "phy/profx_held_suarez.h"
+#include "physical_constants.h"
+#include "profx_RT.h"
 #include "reduction_add.h"
 
 #include "grid.h"
@@ -151,8 +153,25 @@ struct ref_params {
     int    glevel;
 };
 
+// Double-gray RT module and its insolation; same field order as oracle_rt_params.
+struct ref_rt_params {
+    double Tstar, planet_star_dist, radius_star, diff_ang, Tint, albedo;
+    double kappa_sw, kappa_lw, kappa_lw_pole, n_sw, n_lw, f_lw;
+    double mean_motion, alpha_i, true_long_i, ecc, obliquity, longp;
+    int    latf_lw, rt1Dmode, sync_rot, surface;
+    int    spinup_start, spinup_stop, spindown_start, spindown_stop;
+    int    first_step;
+};
+
 struct RefSim {
     ref_params                     p;
+    bool                           rt = false;
+    ref_rt_params                  R{};
+    double incflx = 0, mean_motion = 0, mean_anomaly_i = 0, true_long_i = 0, ecc = 0,
+           obliquity = 0, alpha_i = 0, longp = 0;
+    double r_orb = 1, sin_decl = 0, cos_decl = 1, alpha = 0; // Insolation member defaults
+    int    nstep = 1;
+    double ASR_tot = 0, OLR_tot = 0;
     int                            N, nv, nvi, nl_region, nr;
     std::map<std::string, double*> f;    // device fields
     std::map<std::string, long>    size; // element counts
@@ -304,6 +323,169 @@ extern "C" long ref_sim_get(void* h, const char* name, double* host) {
 }
 
 // One ProfX call, Held-Suarez branch (src/ESP/profx_driver.cu:70-474).
+
+// ---------------------------------------------------------------------------------------------
+// RT module. rtm_dual_band and annual_insol are the reference's own kernels
+// (src/physics/modules/inc/profx_RT.h); the argument list and the host logic around them follow
+// radiative_transfer::phy_loop (src/physics/modules/src/radiative_transfer.cu:769-1105) and
+// RTSetup (:1393-1437). The insolation step (src/ESP/insolation.cu) cannot be compiled here: its
+// header pulls the HDF5 storage header in through a quote include that the storage shim cannot
+// shadow. Its few lines of orbit and zenith arithmetic are therefore restated below (host orbit
+// update, one device kernel for the zenith angles).
+// ---------------------------------------------------------------------------------------------
+static double h_solve_kepler(double M, double ecc) { // insolation.cu:65-88
+    double E = M + (sin(M) < 0.0 ? -1.0 : 1.0) * 0.85 * ecc, d3 = 1.0;
+    for (int it = 0; it < 100 && d3 > 1e-15; it++) {
+        double fi = E - ecc * sin(E) - M, f1 = 1.0 - ecc * cos(E), f2 = ecc * sin(E), f3 = ecc * cos(E);
+        double d1 = -fi / f1;
+        double d2 = -fi / (f1 + 0.5 * d1 * f2);
+        d3        = -fi / (f1 + 0.5 * d2 * f2 + 1. / 6. * d2 * d2 * f3);
+        E         = E + d3;
+    }
+    return E;
+}
+static double h_ecc2true(double E, double ecc) { // insolation.cu:97-106
+    double f = 2.0 * atan(sqrt((1.0 + ecc) / (1.0 - ecc)) * tan(E / 2.0));
+    return f < 0.0 ? f + 2 * M_PI : f;
+}
+static double h_true2ecc(double f, double ecc) { // insolation.cu:108-125
+    while (f < 0.0)
+        f += 2 * M_PI;
+    while (f >= 2 * M_PI)
+        f -= 2 * M_PI;
+    double cosE = (cos(f) + ecc) / (1.0 + ecc * cos(f));
+    return f < M_PI ? acos(cosE) : 2 * M_PI - acos(cosE);
+}
+static void h_update_spin_orbit(RefSim* s, double time) { // insolation.cu:514-529
+    double M         = fmod((s->mean_motion * time + s->mean_anomaly_i), (2 * M_PI));
+    double E         = fmod(h_solve_kepler(M, s->ecc), (2 * M_PI));
+    s->r_orb         = 1.0 - s->ecc * cos(E);
+    double true_long = fmod((h_ecc2true(E, s->ecc) + s->longp), (2 * M_PI));
+    s->sin_decl      = sin(s->obliquity) * sin(true_long);
+    s->cos_decl      = sqrt(1.0 - s->sin_decl * s->sin_decl);
+    s->alpha         = -s->p.Omega * time + true_long - s->true_long_i + s->alpha_i;
+}
+__global__ void h_cos_zenith(double* cz, const double* lonlat, double alpha, double alpha_i,
+                             double sin_decl, double cos_decl, int sync_rot, double ecc,
+                             double obliquity, int N) { // insolation.cu:128-207
+    int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= N)
+        return;
+    double lon = lonlat[id * 2], lat = lonlat[id * 2 + 1], c;
+    bool   obl = !(obliquity < 1e-10);
+    if (sync_rot && ecc < 1e-10)
+        c = obl ? (sin(lat) * sin_decl + cos(lat) * cos_decl * cos(lon - alpha_i))
+                : cos(lat) * cos(lon - alpha_i);
+    else if (sync_rot && !obl)
+        c = cos(lat) * cos(lon - alpha);
+    else
+        c = (sin(lat) * sin_decl + cos(lat) * cos_decl * cos(lon - alpha));
+    cz[id] = c < 0.0 ? 0.0 : c;
+}
+
+extern "C" int ref_sim_rt(void* h, const ref_rt_params* rp) {
+    RefSim* s = (RefSim*)h;
+    if (rp->surface || s->p.GravHeightVar)
+        return -1;
+    s->R   = *rp;
+    s->rt  = true;
+    long N = s->N, nv = s->nv, nvi = s->nvi;
+    for (auto n : {"flw_up", "flw_dn", "fsw_up", "fsw_dn", "phtemp", "thtemp"})
+        if (sim_alloc(s, n, N * nvi))
+            return -2;
+    if (sim_alloc(s, "tau", N * nv * 2))
+        return -2;
+    for (auto n : {"ttemp", "dtemp", "DG_Qheat"})
+        if (sim_alloc(s, n, N * nv))
+            return -2;
+    for (auto n : {"insol", "insol_ann", "ASR", "OLR", "cos_zenith", "surf_flux", "Tsurface",
+                   "dTsurf_dt"})
+        if (sim_alloc(s, n, N))
+            return -2;
+    double resc_flx   = pow(rp->radius_star / rp->planet_star_dist, 2.0);
+    s->incflx         = resc_flx * SIGMA_SB_th * rp->Tstar * rp->Tstar * rp->Tstar * rp->Tstar;
+    s->mean_motion    = rp->sync_rot ? s->p.Omega : rp->mean_motion;
+    s->true_long_i    = rp->true_long_i * M_PI / 180.0;
+    s->longp          = rp->longp * M_PI / 180.0;
+    s->ecc            = rp->ecc;
+    double f_i        = fmod(s->true_long_i - s->longp, (2 * M_PI));
+    double E_i        = h_true2ecc(f_i, s->ecc);
+    s->mean_anomaly_i = fmod(E_i - s->ecc * sin(E_i), (2 * M_PI));
+    s->alpha_i        = rp->alpha_i * M_PI / 180.0;
+    s->obliquity      = rp->obliquity * M_PI / 180.0;
+    s->nstep          = rp->first_step;
+    return 0;
+}
+
+extern "C" void ref_sim_rt_totals(void* h, double* asr, double* olr) {
+    RefSim* s = (RefSim*)h;
+    *asr      = s->ASR_tot;
+    *olr      = s->OLR_tot;
+}
+
+// Insolation::phy_loop + radiative_transfer::phy_loop (DualbandGray), in ProfX order.
+static int ref_rt_step(RefSim* s) {
+    auto&        F = s->f;
+    const int    NTH = 256, N = s->N, nv = s->nv, nvi = s->nvi, nstep = s->nstep;
+    const double dt = s->p.timestep;
+    dim3         NBRT((N / NTH) + 1, 1, 1);
+    if (s->R.sync_rot) {
+        if (s->ecc > 1e-10)
+            h_update_spin_orbit(s, nstep * dt);
+    }
+    else
+        h_update_spin_orbit(s, nstep * dt);
+    h_cos_zenith<<<(N / NTH) + 1, NTH>>>(F["cos_zenith"], F["lonlat"], s->alpha, s->alpha_i,
+                                         s->sin_decl, s->cos_decl, s->R.sync_rot, s->ecc,
+                                         s->obliquity, N);
+    REF_CHECK(cudaDeviceSynchronize());
+    bool   run           = true;
+    double Qheat_scaling = 1.0;
+    const ref_rt_params& R = s->R;
+    if (R.spinup_start > -1 && R.spinup_stop > -1) {
+        if (nstep < R.spinup_start) {
+            run           = false;
+            Qheat_scaling = 0.0;
+        }
+        else if ((nstep >= R.spinup_start) && (nstep <= R.spinup_stop)) {
+            double x = (double)(nstep - R.spinup_start) / (double)(R.spinup_stop - R.spinup_start);
+            Qheat_scaling = (1 + sin(M_PI * x - M_PI / 2.0)) / 2.0;
+            run           = true;
+        }
+    }
+    if (R.spindown_start > -1 && R.spindown_stop > -1) {
+        if ((nstep >= R.spindown_start) && (nstep <= R.spindown_stop)) {
+            double x = (double)(nstep - R.spindown_start) / (double)(R.spindown_stop - R.spindown_start);
+            Qheat_scaling = 1.0 - (1 + sin(M_PI * x - M_PI / 2.0)) / 2.0;
+            run           = true;
+        }
+        else if (nstep >= R.spindown_stop) {
+            run           = false;
+            Qheat_scaling = 0.0;
+        }
+    }
+    if (run) {
+        rtm_dual_band<<<NBRT, NTH>>>(
+            F["pressure"], F["Rho"], F["temperature"], F["flw_up"], F["flw_dn"], F["fsw_up"],
+            F["fsw_dn"], F["tau"], s->p.Gravit, F["Cp"], F["lonlat"], F["Altitude"],
+            F["Altitudeh"], F["phtemp"], F["dtemp"], F["ttemp"], F["thtemp"], dt, R.Tstar,
+            R.planet_star_dist, R.radius_star, R.diff_ang, R.Tint, R.albedo, R.kappa_sw,
+            R.kappa_lw, R.latf_lw, R.kappa_lw_pole, R.n_sw, R.n_lw, R.f_lw, s->incflx, s->p.P_Ref,
+            N, nv, nvi, s->p.A, s->r_orb, F["cos_zenith"], F["insol"], false, 1e7, F["Tsurface"],
+            F["dTsurf_dt"], F["surf_flux"], F["areasT"], F["ASR"], F["OLR"], F["profx_Qheat"],
+            F["DG_Qheat"], F["Rd"], Qheat_scaling, false, R.rt1Dmode, s->p.DeepModel,
+            s->p.GravHeightVar);
+        REF_CHECK(cudaGetLastError());
+        s->ASR_tot = gpu_sum_on_device<1024>(F["ASR"], N);
+        s->OLR_tot = gpu_sum_on_device<1024>(F["OLR"], N);
+        if (nstep * dt < (2 * M_PI / s->mean_motion))
+            annual_insol<<<NBRT, NTH>>>(F["insol_ann"], F["insol"], nstep, N);
+    }
+    REF_CHECK(cudaDeviceSynchronize());
+    s->nstep++;
+    return 0;
+}
+
 static int ref_profx(RefSim* s) {
     auto&     F   = s->f;
     const int NTH = 256;
@@ -321,6 +503,8 @@ static int ref_profx(RefSim* s) {
                                  s->p.timestep, N);
         REF_CHECK(cudaDeviceSynchronize());
     }
+    if (s->rt && ref_rt_step(s))
+        return -1;
     Compute_pressure<<<NB, NTH>>>(F["pressure"], F["temperature"], F["Rho"], F["Rd"], N);
     REF_CHECK(cudaDeviceSynchronize());
     return 0;

@@ -47,6 +47,14 @@ struct Oracle {
     std::vector<char> pole, pent;
     // state and intermediates
     std::map<std::string, Vec> f;
+    // radiative transfer and insolation (when enabled)
+    bool             rt = false;
+    oracle_rt_params R{};
+    double           incflx = 0, mean_motion = 0, mean_anomaly_i = 0, true_long_i = 0, ecc = 0,
+           obliquity = 0, alpha_i = 0, longp = 0;
+    double r_orb = 1, sin_decl = 0, cos_decl = 1, alpha = 0; // Insolation member defaults
+    int    nstep = 1;
+    double ASR_tot = 0, OLR_tot = 0;
 };
 
 inline double val(const Vec& a, int id, int nv, int lev) {
@@ -182,12 +190,305 @@ void compute_pressure(Oracle& o) {
 }
 
 // ESP::ProfX, src/ESP/profx_driver.cu:70-474 (Held-Suarez branch, no sponge, no modules)
+// Neumaier's compensated summation (A. Neumaier, ZAMM 54, 1974): s + c carries the sum to about
+// one rounding of the exact result for any ordering of the terms.
+struct Neumaier {
+    double s = 0.0, c = 0.0;
+    void   add(double x) {
+        double t = s + x;
+        if (std::fabs(s) >= std::fabs(x))
+            c += (s - t) + x;
+        else
+            c += (x - t) + s;
+        s = t;
+    }
+    double value() const { return s + c; }
+};
+
+
+// ---------------------------------------------------------------------------------------------
+// Insolation (src/ESP/insolation.cu) and the double-gray radiative transfer
+// (rtm_dual_band, src/physics/modules/inc/profx_RT.h:39-587; phy_loop,
+// src/physics/modules/src/radiative_transfer.cu:769-1105)
+// ---------------------------------------------------------------------------------------------
+
+// Kepler's equation by the third-order iteration of insolation.cu:65-88 (which stops as soon as
+// the last correction is not above 1e-15, signed); bounded here at 100 iterations.
+double solve_kepler(double mean_anomaly, double ecc) {
+    double E  = mean_anomaly + (std::sin(mean_anomaly) < 0.0 ? -1.0 : 1.0) * 0.85 * ecc;
+    double d3 = 1.0;
+    for (int it = 0; it < 100 && d3 > 1e-15; it++) {
+        double fi = E - ecc * sin(E) - mean_anomaly, f1 = 1.0 - ecc * cos(E), f2 = ecc * sin(E),
+               f3 = ecc * cos(E);
+        double d1 = -fi / f1;
+        double d2 = -fi / (f1 + 0.5 * d1 * f2);
+        d3        = -fi / (f1 + 0.5 * d2 * f2 + 1. / 6. * d2 * d2 * f3);
+        E         = E + d3;
+    }
+    return E;
+}
+double ecc2true_anomaly(double E, double ecc) { // insolation.cu:97-106
+    double tanf2 = sqrt((1.0 + ecc) / (1.0 - ecc)) * tan(E / 2.0);
+    double f     = 2.0 * atan(tanf2);
+    if (f < 0.0)
+        f += 2 * M_PI;
+    return f;
+}
+double true2ecc_anomaly(double f, double ecc) { // insolation.cu:108-125
+    while (f < 0.0)
+        f += 2 * M_PI;
+    while (f >= 2 * M_PI)
+        f -= 2 * M_PI;
+    double cosE = (cos(f) + ecc) / (1.0 + ecc * cos(f));
+    return f < M_PI ? acos(cosE) : 2 * M_PI - acos(cosE);
+}
+void update_spin_orbit(Oracle& o, double time) { // insolation.cu:514-529
+    double M         = fmod((o.mean_motion * time + o.mean_anomaly_i), (2 * M_PI));
+    double E         = fmod(solve_kepler(M, o.ecc), (2 * M_PI));
+    o.r_orb          = 1.0 - o.ecc * cos(E);
+    double true_long = fmod((ecc2true_anomaly(E, o.ecc) + o.longp), (2 * M_PI));
+    o.sin_decl       = sin(o.obliquity) * sin(true_long);
+    o.cos_decl       = sqrt(1.0 - o.sin_decl * o.sin_decl);
+    o.alpha          = -o.P.Omega * time + true_long - o.true_long_i + o.alpha_i;
+}
+
+// calc_zenith + compute_cos_zenith_angles (insolation.cu:128-207)
+void cos_zenith(Oracle& o) {
+    Vec& cz = F(o, "cos_zenith");
+    for (int id = 0; id < o.N; id++) {
+        double lon = o.lonlat[id * 2], lat = o.lonlat[id * 2 + 1], c;
+        bool   obl = !(o.obliquity < 1e-10);
+        if (o.R.sync_rot && o.ecc < 1e-10)
+            c = obl ? (sin(lat) * o.sin_decl + cos(lat) * o.cos_decl * cos(lon - o.alpha_i))
+                    : cos(lat) * cos(lon - o.alpha_i);
+        else if (o.R.sync_rot && !obl)
+            c = cos(lat) * cos(lon - o.alpha);
+        else
+            c = (sin(lat) * o.sin_decl + cos(lat) * o.cos_decl * cos(lon - o.alpha));
+        cz[id] = c < 0.0 ? 0.0 : c;
+    }
+}
+
+int factorial_num(int n) {
+    int t = 1;
+    while (n != 0) {
+        t = t * n;
+        n = n - 1;
+    }
+    return t;
+}
+
+// linear-in-tau source function integral over a layer (profx_RT.h:133-160)
+double source_func_lin(double bb, double bl, double bt, double tau, double diff_ang) {
+    double e1 = 0.0, e2 = 0.0;
+    if (tau >= 1e-10) {
+        e1 = bb - bl + (bl - (diff_ang / (tau / 2.0)) * (bb - bl)) * (1.0 - exp(-(tau / 2.0) / diff_ang));
+        e2 = bl - bt + (bt - (diff_ang / (tau / 2.0)) * (bl - bt)) * (1.0 - exp(-(tau / 2.0) / diff_ang));
+    }
+    else {
+        for (int i = 0; i < 5; i++) {
+            int fac = factorial_num(i + 2);
+            e1      = e1 + (pow(-1.0, i + 2.0)) * ((bl + (i + 1) * bl) / fac) * pow((tau / 2.0) / diff_ang, i + 1.0);
+            e2      = e2 + (pow(-1.0, i + 2.0)) * ((bt + (i + 1) * bb) / fac) * pow((tau / 2.0) / diff_ang, i + 1.0);
+        }
+    }
+    return e1 + e2 * exp(-(tau / 2.0) / diff_ang);
+}
+
+void rtm_dual_band(Oracle& o, double Qheat_scaling) {
+    const int    N = o.N, nv = o.nv, nvi = o.nvi;
+    const double gravit = o.P.Gravit, A = o.P.A, ps0 = o.P.P_Ref, timestep = o.P.timestep;
+    const oracle_rt_params& R = o.R;
+    Vec &p = F(o, "pressure"), &Rho = F(o, "Rho"), &T = F(o, "temperature"), &Cp = F(o, "Cp"),
+        &Rd = F(o, "Rd"), &phtemp = F(o, "phtemp"), &thtemp = F(o, "thtemp"),
+        &ttemp = F(o, "ttemp"), &dtemp = F(o, "dtemp"), &tau = F(o, "tau"),
+        &fsw_up = F(o, "fsw_up"), &fsw_dn = F(o, "fsw_dn"), &flw_up = F(o, "flw_up"),
+        &flw_dn = F(o, "flw_dn"), &insol = F(o, "insol"), &ASR = F(o, "ASR"), &OLR = F(o, "OLR"),
+        &cz = F(o, "cos_zenith"), &Qheat = F(o, "profx_Qheat"), &DGQ = F(o, "DG_Qheat");
+    const Vec &Alt = o.Altitude, &Alth = o.Altitudeh;
+    const double bc = 5.677036E-8;
+#pragma omp parallel for schedule(static)
+    for (int id = 0; id < N; id++) {
+        for (int lev = 0; lev < nv; lev++)
+            dtemp[id * nv + lev] = 0.0;
+        // interface pressures and temperatures (profx_RT.h:419-466)
+        for (int lev = 0; lev <= nv; lev++) {
+            if (lev == 0) {
+                double psm;
+                if (o.P.GravHeightVar)
+                    psm = p[id * nv + 1] - Rho[id * nv + 0] * gravit * pow(A / (A + Alt[0]), 2) * (-Alt[0] - Alt[1]);
+                else
+                    psm = p[id * nv + 1] - Rho[id * nv + 0] * gravit * (-Alt[0] - Alt[1]);
+                double ps              = 0.5 * (p[id * nv + 0] + psm);
+                phtemp[id * nvi + 0]   = ps;
+                ttemp[id * nv + 0]     = T[id * nv + 0];
+                thtemp[id * nvi + 0]   = ttemp[id * nv + 0];
+            }
+            else if (lev == nv) {
+                double pp = p[id * nv + nv - 2]
+                            + (p[id * nv + nv - 1] - p[id * nv + nv - 2]) / (Alt[nv - 1] - Alt[nv - 2])
+                                  * (2 * Alth[nv] - Alt[nv - 1] - Alt[nv - 2]);
+                if (pp < 0)
+                    pp = 0;
+                double ptop            = 0.5 * (p[id * nv + nv - 1] + pp);
+                phtemp[id * nvi + nv]  = ptop;
+                thtemp[id * nvi + nv]  = T[id * nv + nv - 1];
+            }
+            else {
+                ttemp[id * nv + lev] = T[id * nv + lev];
+                double xi = Alth[lev], xim = Alt[lev - 1], xip = Alt[lev];
+                double a = (xi - xip) / (xim - xip), b = (xi - xim) / (xip - xim);
+                phtemp[id * nvi + lev] = p[id * nv + lev - 1] * a + p[id * nv + lev] * b;
+                thtemp[id * nvi + lev] = T[id * nv + lev - 1] * a + ttemp[id * nv + lev] * b;
+            }
+        }
+        double coszrs = R.rt1Dmode ? 0.5 : cz[id];
+        double kappa_lw_lat = R.latf_lw ? R.kappa_lw + (R.kappa_lw_pole - R.kappa_lw) * pow(sin(o.lonlat[id * 2 + 1]), 2)
+                                        : R.kappa_lw;
+        // computetau (profx_RT.h:278-314)
+        for (int lev = 0; lev < nv; lev++) {
+            tau[id * 2 * nv + lev * 2] = R.n_sw * R.kappa_sw * pow(p[id * nv + lev] / ps0, R.n_sw - 1)
+                                         * Rho[id * nv + lev] * (Alth[lev + 1] - Alth[lev]);
+            tau[id * 2 * nv + lev * 2 + 1] =
+                kappa_lw_lat * (1 + R.n_lw * (1 - R.f_lw) / R.f_lw * pow(p[id * nv + lev] / ps0, R.n_lw - 1))
+                * Rho[id * nv + lev] * (Alth[lev + 1] - Alth[lev]);
+        }
+        for (int lev = 0; lev <= nv; lev++)
+            fsw_up[id * nvi + lev] = 0.0;
+        for (int lev = 0; lev <= nv; lev++)
+            fsw_dn[id * nvi + lev] = 0.0;
+        if (coszrs > 0.0) { // radcsw (profx_RT.h:39-118), GravHeightVar excluded
+            double taut              = (R.kappa_sw / gravit) * (phtemp[id * (nv + 1) + nv]);
+            insol[id]                = o.incflx * pow(o.r_orb, -2) * coszrs;
+            double flux_top          = insol[id] * (1.0 - R.albedo);
+            fsw_dn[id * (nv + 1) + nv] = flux_top * exp(-(1.0 / coszrs) * taut);
+            for (int lev = nv; lev >= 1; lev--)
+                fsw_dn[id * (nv + 1) + lev - 1] =
+                    fsw_dn[id * (nv + 1) + lev] * exp(-(1.0 / coszrs) * tau[id * nv * 2 + (lev - 1) * 2]);
+            for (int lev = 0; lev <= nv; lev++)
+                fsw_up[id * (nv + 1) + lev] = 0.0;
+            for (int lev = 0; lev < nv; lev++) {
+                double rup = 1.0, rlow = 1.0;
+                dtemp[id * nv + lev] =
+                    -(pow(rlow, 2) * (fsw_up[id * (nv + 1) + lev] - fsw_dn[id * (nv + 1) + lev])
+                      - pow(rup, 2) * (fsw_up[id * (nv + 1) + lev + 1] - fsw_dn[id * (nv + 1) + lev + 1]))
+                    / ((Alth[lev] - Alth[lev + 1]));
+            }
+        }
+        else
+            insol[id] = 0;
+        double rscale = o.P.DeepModel ? (A + Alth[nv]) / A : 1.0;
+        ASR[id]       = fsw_dn[id * nvi + nv] * o.areasT[id] * pow(rscale, 2);
+        for (int lev = 0; lev <= nv; lev++)
+            flw_up[id * nvi + lev] = 0.0;
+        for (int lev = 0; lev <= nv; lev++)
+            flw_dn[id * nvi + lev] = 0.0;
+        // radclw (profx_RT.h:162-275), reflecting lower boundary (no surface)
+        flw_dn[id * (nv + 1) + nv] = 0.0;
+        for (int lev = nv - 1; lev >= 0; lev--) {
+            if (tau[id * nv * 2 + 2 * lev + 1] < 0.0)
+                tau[id * nv * 2 + 2 * lev + 1] = 0.0;
+            double tb = thtemp[id * (nv + 1) + lev], tl = ttemp[id * nv + lev],
+                   tt = thtemp[id * (nv + 1) + lev + 1];
+            double bb = bc * tb * tb * tb * tb, bl = bc * tl * tl * tl * tl, bt = bc * tt * tt * tt * tt;
+            double ed = source_func_lin(bb, bl, bt, tau[id * nv * 2 + 2 * lev + 1], R.diff_ang);
+            flw_dn[id * (nv + 1) + lev] =
+                ed + flw_dn[id * (nv + 1) + lev + 1] * exp(-(1. / R.diff_ang) * tau[id * nv * 2 + 2 * lev + 1]);
+        }
+        flw_up[id * (nv + 1) + 0] = bc * R.Tint * R.Tint * R.Tint * R.Tint;
+        flw_up[id * (nv + 1) + 0] += flw_dn[id * (nv + 1) + 0];
+        for (int lev = 1; lev <= nv; lev++) {
+            if (tau[id * nv * 2 + 2 * (lev - 1) + 1] < 0.0)
+                tau[id * nv * 2 + 2 * (lev - 1) + 1] = 0.0;
+            double tb = thtemp[id * (nv + 1) + lev - 1], tl = ttemp[id * nv + lev - 1],
+                   tt = thtemp[id * (nv + 1) + lev];
+            double bb = bc * tb * tb * tb * tb, bl = bc * tl * tl * tl * tl, bt = bc * tt * tt * tt * tt;
+            double eu = source_func_lin(bt, bl, bb, tau[id * nv * 2 + 2 * (lev - 1) + 1], R.diff_ang);
+            flw_up[id * (nv + 1) + lev] =
+                eu + flw_up[id * (nv + 1) + lev - 1] * exp(-(1. / R.diff_ang) * tau[id * nv * 2 + 2 * (lev - 1) + 1]);
+        }
+        for (int lev = 0; lev < nv; lev++) {
+            double rup = 1.0, rlow = 1.0;
+            dtemp[id * nv + lev] =
+                dtemp[id * nv + lev]
+                - (pow(rlow, 2) * (flw_up[id * (nv + 1) + lev] - flw_dn[id * (nv + 1) + lev])
+                   - pow(rup, 2) * (flw_up[id * (nv + 1) + lev + 1] - flw_dn[id * (nv + 1) + lev + 1]))
+                      / ((Alth[lev] - Alth[lev + 1]));
+        }
+        OLR[id] = flw_up[id * nvi + nv] * o.areasT[id] * pow(rscale, 2);
+        // cooling limiter and coupling to the dynamical core (profx_RT.h:560-584)
+        for (int lev = 0; lev < nv; lev++) {
+            const int i = id * nv + lev;
+            if (p[i] + Rd[i] / (Cp[i] - Rd[i]) * dtemp[i] * timestep < 0)
+                dtemp[i] = -p[i] / timestep;
+            DGQ[i] = dtemp[i];
+            Qheat[i] += Qheat_scaling * dtemp[i];
+        }
+    }
+}
+
+// Insolation::phy_loop then radiative_transfer::phy_loop for the DualbandGray type.
+void rt_step(Oracle& o) {
+    const int    nstep = o.nstep;
+    const double dt    = o.P.timestep;
+    if (o.R.sync_rot) {
+        if (o.ecc > 1e-10)
+            update_spin_orbit(o, nstep * dt);
+    }
+    else
+        update_spin_orbit(o, nstep * dt);
+    cos_zenith(o);
+    bool   run = true;
+    double Qs  = 1.0;
+    const oracle_rt_params& R = o.R;
+    if (R.spinup_start > -1 && R.spinup_stop > -1) {
+        if (nstep < R.spinup_start) {
+            run = false;
+            Qs  = 0.0;
+        }
+        else if (nstep >= R.spinup_start && nstep <= R.spinup_stop) {
+            double x = (double)(nstep - R.spinup_start) / (double)(R.spinup_stop - R.spinup_start);
+            Qs       = (1 + sin(M_PI * x - M_PI / 2.0)) / 2.0;
+            run      = true;
+        }
+    }
+    if (R.spindown_start > -1 && R.spindown_stop > -1) {
+        if (nstep >= R.spindown_start && nstep <= R.spindown_stop) {
+            double x = (double)(nstep - R.spindown_start) / (double)(R.spindown_stop - R.spindown_start);
+            Qs       = 1.0 - (1 + sin(M_PI * x - M_PI / 2.0)) / 2.0;
+            run      = true;
+        }
+        else if (nstep >= R.spindown_stop) {
+            run = false;
+            Qs  = 0.0;
+        }
+    }
+    if (run) {
+        rtm_dual_band(o, Qs);
+        Neumaier a, b;
+        for (int id = 0; id < o.N; id++) {
+            a.add(F(o, "ASR")[id]);
+            b.add(F(o, "OLR")[id]);
+        }
+        o.ASR_tot = a.value();
+        o.OLR_tot = b.value();
+        if (nstep * dt < (2 * M_PI / o.mean_motion)) { // annual_insol (profx_RT.h:30-37)
+            Vec &ann = F(o, "insol_ann"), &ins = F(o, "insol");
+            for (int id = 0; id < o.N; id++)
+                ann[id] = ann[id] * (nstep - 1) / nstep + ins[id] / nstep;
+        }
+    }
+    o.nstep++;
+}
+
 void profx(Oracle& o) {
     std::fill(F(o, "profx_Qheat").begin(), F(o, "profx_Qheat").end(), 0.0);
     recompute_w(o);
     compute_temperature(o);
     if (o.P.held_suarez)
         held_suarez(o);
+    if (o.rt)
+        rt_step(o);
     compute_pressure(o);
 }
 
@@ -1443,6 +1744,42 @@ extern "C" void* oracle_new(const oracle_grid* g, const oracle_params* p) {
     return o;
 }
 
+extern "C" int oracle_rt(void* h, const oracle_rt_params* rp) {
+    Oracle& o = *(Oracle*)h;
+    if (rp->surface || o.P.GravHeightVar || o.areasT.empty())
+        return -1;
+    o.R  = *rp;
+    o.rt = true;
+    const int N = o.N, nv = o.nv, nvi = o.nvi;
+    for (auto n : {"flw_up", "flw_dn", "fsw_up", "fsw_dn", "phtemp", "thtemp"})
+        o.f[n].assign((size_t)N * nvi, 0.0);
+    o.f["tau"].assign((size_t)N * nv * 2, 0.0);
+    for (auto n : {"ttemp", "dtemp", "DG_Qheat"})
+        o.f[n].assign((size_t)N * nv, 0.0);
+    for (auto n : {"insol", "insol_ann", "ASR", "OLR", "cos_zenith"})
+        o.f[n].assign((size_t)N, 0.0);
+    // RTSetup (radiative_transfer.cu:1431-1432) and Insolation::initial_conditions (insolation.cu:292-313)
+    double resc_flx = pow(rp->radius_star / rp->planet_star_dist, 2.0);
+    o.incflx        = resc_flx * 5.6703744191844314e-08 * rp->Tstar * rp->Tstar * rp->Tstar * rp->Tstar;
+    o.mean_motion   = rp->sync_rot ? o.P.Omega : rp->mean_motion;
+    o.true_long_i   = rp->true_long_i * M_PI / 180.0;
+    o.longp         = rp->longp * M_PI / 180.0;
+    o.ecc           = rp->ecc;
+    double f_i      = fmod(o.true_long_i - o.longp, (2 * M_PI));
+    double E_i      = true2ecc_anomaly(f_i, o.ecc);
+    o.mean_anomaly_i = fmod(E_i - o.ecc * sin(E_i), (2 * M_PI));
+    o.alpha_i        = rp->alpha_i * M_PI / 180.0;
+    o.obliquity      = rp->obliquity * M_PI / 180.0;
+    o.nstep          = rp->first_step;
+    return 0;
+}
+
+extern "C" void oracle_rt_totals(void* h, double* asr, double* olr) {
+    Oracle& o = *(Oracle*)h;
+    *asr      = o.ASR_tot;
+    *olr      = o.OLR_tot;
+}
+
 extern "C" long oracle_set(void* h, const char* name, const double* src) {
     Oracle* o  = (Oracle*)h;
     auto    it = o->f.find(name);
@@ -1474,21 +1811,6 @@ extern "C" int oracle_step(void* h, int nsteps, int do_profx, int do_thor) {
 }
 
 namespace {
-
-// Neumaier's compensated summation (A. Neumaier, ZAMM 54, 1974): s + c carries the sum to about
-// one rounding of the exact result for any ordering of the terms.
-struct Neumaier {
-    double s = 0.0, c = 0.0;
-    void   add(double x) {
-        double t = s + x;
-        if (std::fabs(s) >= std::fabs(x))
-            c += (s - t) + x;
-        else
-            c += (x - t) + s;
-        s = t;
-    }
-    double value() const { return s + c; }
-};
 
 // Control volume of cell (id, lev) as CalcMass et al. compute it (src/ESP/profx_globdiag.cu:82-90).
 double control_volume(const Oracle& o, int id, int lev) {

@@ -28,7 +28,25 @@ typedef struct {
     const double* areasT; // may be null when oracle_globdiag is not used
 } oracle_grid;
 
+// Double-gray radiative transfer module with the insolation it needs (radiative_transfer,
+// DualbandGray, src/physics/modules/src/radiative_transfer.cu; Insolation, src/ESP/insolation.cu).
+// Lengths in m, angles in degrees (as in the .thr file), spin-up/down in steps (-1 = off).
+typedef struct {
+    double Tstar, planet_star_dist, radius_star, diff_ang, Tint, albedo;
+    double kappa_sw, kappa_lw, kappa_lw_pole, n_sw, n_lw, f_lw;
+    double mean_motion, alpha_i, true_long_i, ecc, obliquity, longp;
+    int    latf_lw, rt1Dmode, sync_rot, surface;
+    int    spinup_start, spinup_stop, spindown_start, spindown_stop;
+    int    first_step;
+} oracle_rt_params;
+
 void* oracle_new(const oracle_grid* g, const oracle_params* p);
+// Enables the RT module in ProfX (between the benchmark forcing and Compute_pressure, as
+// src/ESP/profx_driver.cu:405-416). Returns 0, or -1 for an option the restatement lacks.
+int oracle_rt(void* h, const oracle_rt_params* rp);
+// Global absorbed shortwave and outgoing longwave of the last RT call (the reference's
+// ASR_tot / OLR_tot), compensated sums.
+void oracle_rt_totals(void* h, double* asr, double* olr);
 // Copy a named field in/out (reference layout). Returns element count, -1 if unknown.
 long oracle_set(void* h, const char* name, const double* src);
 long oracle_get(void* h, const char* name, double* dst);

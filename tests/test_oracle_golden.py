@@ -66,3 +66,43 @@ def test_golden_fixtures_are_nontrivial():
     assert np.abs(d["Mh"]).max() > 1e-3
     assert np.abs(d["Wh"]).max() > 1e-6
     assert np.abs(d["SlowMh"]).max() > 0
+
+
+def test_oracle_rt_matches_golden():
+    """Double-gray RT + insolation (one physics step), then a full step, against the reference's
+    own rtm_dual_band / Thor kernels (fixture from tests/golden/make_golden.py, RT case)."""
+    from thorx_testlib import RT_WASP43B, hot_jupiter_params
+    d = np.load(os.path.join(HERE, "golden", "rt_wasp43b_g4_l20_dt300.npz"))
+    assert d["rt"].item() == repr(sorted(RT_WASP43B.items()))
+    glevel, nv, dt, stride = int(d["glevel"]), int(d["nv"]), float(d["timestep"]), int(d["stride"])
+    p, c = hot_jupiter_params(glevel, dt)
+    g = RefGrid(glevel, nv, A=c["A"], top=c["Top_altitude"])
+    ic = initial_state(g.arrays, g.point_num, nv, c, amp=1.0)
+    o = Oracle(g, p)
+    for k, v in ic.items():
+        o.set(k, v)
+    o.rt(RT_WASP43B)
+    o.step(1, profx=True, thor=False)
+    N = g.point_num
+    bad = {}
+
+    def check(f, key):
+        mine = o.get(f).reshape(N, -1)[::stride]
+        ref, ref_nf = d[key], d["nofma_" + key]
+        spread = rel_err(ref_nf, ref)
+        e = max(rel_err(mine, ref), rel_err(mine, ref_nf))
+        if not e <= field_tolerance(spread):
+            bad[key] = dict(err=e, spread=spread)
+
+    for f in ["cos_zenith", "insol", "ASR", "OLR", "fsw_dn", "flw_up", "flw_dn", "tau", "dtemp",
+              "profx_Qheat"]:
+        check(f, f)
+    asr, olr = o.rt_totals()
+    for name, v in (("ASR_tot", asr), ("OLR_tot", olr)):
+        if not abs(v - float(d[name])) <= 1e-12 * abs(float(d[name])):
+            bad[name] = (v, float(d[name]))
+    o.step(1, profx=False, thor=True)
+    for f in STATE_FIELDS + ["temperature"]:
+        check(f, "step_" + f)
+    o.close(), g.close()
+    assert not bad, bad

@@ -1,0 +1,138 @@
+"""Double-gray radiative transfer + insolation: product and CPU restatement against the reference.
+
+The reference side is its own rtm_dual_band / annual_insol kernels and gpu_sum_on_device
+(oracle/ref_harness.cu, profx_RT.h compiled as shipped), driven with the host logic of
+radiative_transfer::phy_loop; the orbit/zenith arithmetic of insolation.cu is restated there
+(that file does not compile outside the full build). Configuration: the reference's WASP-43b
+example (ifile/wasp43b_ex.thr) at glevel 4, no sponge, no convective adjustment.
+
+Tolerance per field as in the dynamical-core tests: 1e-12 of max|field|, or 4x the spread between
+the reference's own FMA and no-FMA builds where that is larger.
+"""
+import numpy as np
+import pytest
+
+import thor_b200
+from thorx_testlib import (RT_WASP43B, STATE_FIELDS, Oracle, RefGrid, RefSim, field_tolerance,
+                           grid_dict, hot_jupiter_params, initial_state, rel_err, thorx_params)
+
+RT_FIELDS = ["cos_zenith", "insol", "ASR", "OLR", "fsw_dn", "flw_up", "flw_dn", "tau", "dtemp",
+             "DG_Qheat", "profx_Qheat", "phtemp", "thtemp", "insol_ann"]
+GLEVEL, NV, DT = 4, 20, 300.0
+
+
+def setup(rt=RT_WASP43B, glevel=GLEVEL, nv=NV, seed=20260101, amp=1.0):
+    p, c = hot_jupiter_params(glevel, DT)
+    g = RefGrid(glevel, nv, A=c["A"], top=c["Top_altitude"])
+    ic = initial_state(g.arrays, g.point_num, nv, c, seed=seed, amp=amp)
+    return g, p, c, ic
+
+
+def compare(got, ref, ref_nf, fields):
+    bad, res = {}, {}
+    for f in fields:
+        a, b, bn = got[f], ref[f], ref_nf[f]
+        err, spread = rel_err(a, b), rel_err(bn, b)
+        tol = field_tolerance(spread)
+        res[f] = (err, spread)
+        if not err <= tol:
+            bad[f] = (err, tol)
+    return bad, res
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("who", ["product", "oracle"])
+def test_rt_physics_step_matches_reference(who):
+    g, p, c, ic = setup()
+    s, sn = RefSim(g, p), RefSim(g, p, nofma=True)
+    if who == "product":
+        x = thor_b200.Thorx(grid_dict(g), GLEVEL, thorx_params(c, DT))
+    else:
+        x = Oracle(g, p)
+    for k, v in ic.items():
+        s.set(k, v), sn.set(k, v), x.set(k, v)
+    for h in (s, sn):
+        h.rt(RT_WASP43B)
+    if who == "product":
+        x.rt_enable(RT_WASP43B)
+        x.profx()
+        x.sync()
+    else:
+        x.rt(RT_WASP43B)
+        x.step(1, profx=True, thor=False)
+    s.step(1, profx=True, thor=False)
+    sn.step(1, profx=True, thor=False)
+    fields = RT_FIELDS + ["pressure", "temperature"]
+    got = {f: x.get(f) for f in fields}
+    ref = {f: s.get(f) for f in fields}
+    ref_nf = {f: sn.get(f) for f in fields}
+    mine_tot, ref_tot = x.rt_totals(), s.rt_totals()
+    x.close(), s.close(), sn.close(), g.close()
+    assert np.all(np.isfinite(got["profx_Qheat"])) and np.abs(ref["profx_Qheat"]).max() > 0
+    bad, res = compare(got, ref, ref_nf, fields)
+    assert not bad, {"failures": bad, "all": res}
+    for a, b in zip(mine_tot, ref_tot):
+        assert abs(a - b) <= 1e-12 * abs(b), (mine_tot, ref_tot)
+
+
+@pytest.mark.gpu
+def test_rt_full_steps_graph_replay_match_reference():
+    """Three large steps (ProfX with RT, then Thor) as one CUDA graph per step."""
+    g, p, c, ic = setup()
+    s, sn = RefSim(g, p), RefSim(g, p, nofma=True)
+    x = thor_b200.Thorx(grid_dict(g), GLEVEL, thorx_params(c, DT))
+    for k, v in ic.items():
+        s.set(k, v), sn.set(k, v), x.set(k, v)
+    for h in (s, sn):
+        h.rt(RT_WASP43B)
+    x.rt_enable(RT_WASP43B)
+    x.step(3)
+    x.sync()
+    s.step(3)
+    sn.step(3)
+    fields = STATE_FIELDS + ["temperature", "profx_Qheat", "insol_ann"]
+    got = {f: x.get(f) for f in fields}
+    ref = {f: s.get(f) for f in fields}
+    ref_nf = {f: sn.get(f) for f in fields}
+    x.close(), s.close(), sn.close(), g.close()
+    bad, res = {}, {}
+    for f in fields:
+        err, spread = rel_err(got[f], ref[f]), rel_err(ref_nf[f], ref[f])
+        tol = 1e-11 if f in ("Rho", "pressure", "temperature") else field_tolerance(spread, floor=1e-11)
+        res[f] = (err, spread)
+        if not err <= tol:
+            bad[f] = (err, tol)
+    assert not bad, {"failures": bad, "all": res}
+
+
+@pytest.mark.gpu
+def test_rt_eccentric_oblique_orbit_and_spinup():
+    """Not synchronised, eccentric, oblique: the orbit advances every step (on the device in the
+    product, on the host in the reference), and the heating spins up over steps 2..5."""
+    rt = dict(RT_WASP43B, sync_rot=0, mean_motion=2.0e-5, ecc=0.3, obliquity=23.0, longp=40.0,
+              true_long_i=10.0, alpha_i=5.0, spinup_start=2, spinup_stop=5, first_step=1)
+    g, p, c, ic = setup()
+    s, sn = RefSim(g, p), RefSim(g, p, nofma=True)
+    x = thor_b200.Thorx(grid_dict(g), GLEVEL, thorx_params(c, DT))
+    for k, v in ic.items():
+        s.set(k, v), sn.set(k, v), x.set(k, v)
+    for h in (s, sn):
+        h.rt(rt)
+    x.rt_enable(rt)
+    fields = ["cos_zenith", "insol", "profx_Qheat", "insol_ann"]
+    worst = {}
+    for step in range(1, 7):
+        x.profx()
+        x.sync()
+        s.step(1, profx=True, thor=False)
+        sn.step(1, profx=True, thor=False)
+        got = {f: x.get(f) for f in fields}
+        ref = {f: s.get(f) for f in fields}
+        ref_nf = {f: sn.get(f) for f in fields}
+        if step == 1:  # before the spin-up window: no heating at all
+            assert np.all(got["profx_Qheat"] == 0.0) and np.all(ref["profx_Qheat"] == 0.0)
+        bad, res = compare(got, ref, ref_nf, fields)
+        assert not bad, {"step": step, "failures": bad, "all": res}
+        for f, (e, _) in res.items():
+            worst[f] = max(worst.get(f, 0.0), e)
+    x.close(), s.close(), sn.close(), g.close()

@@ -52,6 +52,45 @@ def make_params(glevel, timestep, **over):
     return p, c
 
 
+# Hot Jupiter with double-gray RT: the reference's ifile/wasp43b_ex.thr constants (no sponge, no
+# convective adjustment), and its RT/insolation keys with lengths in m.
+AU, R_SUN = 149597870700.0, 695700000.0
+HOT_JUPITER = dict(A=72427000.0, Omega=9.09e-5, Gravit=47.0, Rd=3714.0, Cp=13000.0, P_Ref=1e7,
+                   Top_altitude=1.4e6, Tmean=1800.0, Diffc=0.015, DivDampc=0.015, HyDiffOrder=4,
+                   DeepModel=1, NonHydro=1, GravHeightVar=0, HyDiff=1, DivDampP=1,
+                   energy_equation=0, held_suarez=0)
+RT_WASP43B = dict(Tstar=4300.0, planet_star_dist=0.015 * AU, radius_star=0.667 * R_SUN,
+                  diff_ang=0.5, Tint=100.0, albedo=0.18, kappa_sw=0.00125, kappa_lw=0.0025,
+                  kappa_lw_pole=0.0025, n_sw=1.0, n_lw=2.0, f_lw=0.5, sync_rot=1)
+
+
+def hot_jupiter_params(glevel, timestep, **over):
+    c = dict(HOT_JUPITER)
+    c.update(over)
+    return make_params(glevel, timestep, **c)
+
+
+RT_F64 = ["Tstar", "planet_star_dist", "radius_star", "diff_ang", "Tint", "albedo", "kappa_sw",
+          "kappa_lw", "kappa_lw_pole", "n_sw", "n_lw", "f_lw", "mean_motion", "alpha_i",
+          "true_long_i", "ecc", "obliquity", "longp"]
+RT_INT = ["latf_lw", "rt1Dmode", "sync_rot", "surface", "spinup_start", "spinup_stop",
+          "spindown_start", "spindown_stop", "first_step"]
+RT_DEFAULTS = dict(latf_lw=0, rt1Dmode=0, sync_rot=1, surface=0, spinup_start=-1, spinup_stop=-1,
+                   spindown_start=-1, spindown_stop=-1, first_step=1, mean_motion=1.991e-7,
+                   alpha_i=0.0, true_long_i=0.0, ecc=0.0, obliquity=0.0, longp=0.0)
+
+
+class RtParams(ctypes.Structure):
+    """oracle_rt_params / ref_rt_params (the product's thorx_rt_params has the same layout)."""
+    _fields_ = [(n, ctypes.c_double) for n in RT_F64] + [(n, ctypes.c_int) for n in RT_INT]
+
+
+def rt_struct(d):
+    v = dict(RT_DEFAULTS)
+    v.update(d)
+    return RtParams(*[float(v[n]) for n in RT_F64], *[int(v[n]) for n in RT_INT])
+
+
 # ------------------------------------------------------------------------------------------------
 # Reference grid (reference src/ESP/grid.cu, host code, runs on the CPU)
 # ------------------------------------------------------------------------------------------------
@@ -86,6 +125,10 @@ def ref_lib(nofma=False):
         lib.ref_sim_free.argtypes = [ctypes.c_void_p]
         lib.ref_sim_globdiag.restype = ctypes.c_int
         lib.ref_sim_globdiag.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        lib.ref_sim_rt.restype = ctypes.c_int
+        lib.ref_sim_rt.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        lib.ref_sim_rt_totals.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                                          ctypes.POINTER(ctypes.c_double)]
         lib.ref_device_sum.restype = ctypes.c_double
         lib.ref_device_sum.argtypes = [ctypes.c_void_p, ctypes.c_long]
         _ref[nofma] = lib
@@ -206,6 +249,10 @@ def oracle_lib():
         lib.oracle_step.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         lib.oracle_globdiag.restype = ctypes.c_int
         lib.oracle_globdiag.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        lib.oracle_rt.restype = ctypes.c_int
+        lib.oracle_rt.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        lib.oracle_rt_totals.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                                         ctypes.POINTER(ctypes.c_double)]
         lib.oracle_sum.restype = ctypes.c_double
         lib.oracle_sum.argtypes = [ctypes.c_void_p, ctypes.c_long]
         lib.oracle_set_threads.argtypes = [ctypes.c_int]
@@ -239,6 +286,15 @@ class Oracle:
 
     def step(self, n=1, profx=True, thor=True):
         assert oracle_lib().oracle_step(self.h, n, int(profx), int(thor)) == 0
+
+    def rt(self, d):
+        self._rt = rt_struct(d)
+        assert oracle_lib().oracle_rt(self.h, ctypes.byref(self._rt)) == 0
+
+    def rt_totals(self):
+        a, o = ctypes.c_double(), ctypes.c_double()
+        oracle_lib().oracle_rt_totals(self.h, ctypes.byref(a), ctypes.byref(o))
+        return a.value, o.value
 
     def globdiag(self):
         """(sums, sums of magnitudes) of energy, mass, AMx, AMy, AMz, entropy."""
@@ -277,6 +333,15 @@ class RefSim:
 
     def time(self, n):
         return self.lib.ref_sim_time(self.h, n)
+
+    def rt(self, d):
+        self._rt = rt_struct(d)
+        assert self.lib.ref_sim_rt(self.h, ctypes.byref(self._rt)) == 0
+
+    def rt_totals(self):
+        a, o = ctypes.c_double(), ctypes.c_double()
+        self.lib.ref_sim_rt_totals(self.h, ctypes.byref(a), ctypes.byref(o))
+        return a.value, o.value
 
     def globdiag(self):
         out = np.zeros(6)

@@ -35,6 +35,28 @@ class GridC(ctypes.Structure):
          "nvecoa", "nvecti", "nvecte", "div", "grad", "func_r"]]
 
 
+RT_F64 = ["Tstar", "planet_star_dist", "radius_star", "diff_ang", "Tint", "albedo", "kappa_sw",
+          "kappa_lw", "kappa_lw_pole", "n_sw", "n_lw", "f_lw", "mean_motion", "alpha_i",
+          "true_long_i", "ecc", "obliquity", "longp"]
+RT_INT = ["latf_lw", "rt1Dmode", "sync_rot", "surface", "spinup_start", "spinup_stop",
+          "spindown_start", "spindown_stop", "first_step"]
+
+
+class RtParamsC(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in RT_F64] + [(n, ctypes.c_int) for n in RT_INT]
+
+
+def rt_params(d):
+    """thorx_rt_params from a dict (lengths in m, angles in degrees); missing switches off."""
+    defaults = dict(latf_lw=0, rt1Dmode=0, sync_rot=1, surface=0, spinup_start=-1,
+                    spinup_stop=-1, spindown_start=-1, spindown_stop=-1, first_step=1,
+                    mean_motion=1.991e-7, alpha_i=0.0, true_long_i=0.0, ecc=0.0, obliquity=0.0,
+                    longp=0.0)
+    v = dict(defaults)
+    v.update(d)
+    return RtParamsC(*[float(v[n]) for n in RT_F64], *[int(v[n]) for n in RT_INT])
+
+
 class ParamsC(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in
                 ["A", "Omega", "Gravit", "Rd", "Cp", "P_Ref", "Top_altitude", "timestep", "Diffc",
@@ -98,6 +120,11 @@ def lib():
         L.thorx_device_sum_noalloc.argtypes = [vp, ctypes.c_longlong, vp,
                                                ctypes.POINTER(ctypes.c_double)]
         L.thorx_device_sum_noalloc.restype = ci
+        L.thorx_rt_enable.argtypes = [vp, ctypes.POINTER(RtParamsC)]
+        L.thorx_rt_enable.restype = ci
+        L.thorx_rt_totals.argtypes = [vp, ctypes.POINTER(ctypes.c_double),
+                                      ctypes.POINTER(ctypes.c_double)]
+        L.thorx_rt_totals.restype = ci
         _lib = L
     return _lib
 
@@ -107,7 +134,8 @@ EXPORTED = ["thorx_create", "thorx_destroy", "thorx_last_error", "thorx_field_si
             "thorx_sync", "thorx_kernels_per_step", "thorx_grid_build", "thorx_grid_info",
             "thorx_grid_get", "thorx_grid_describe", "thorx_grid_free", "thorx_init_rest_state",
             "thorx_kernel_classes", "thorx_kernel_info", "thorx_profile_steps", "thorx_globdiag",
-            "thorx_device_sum", "thorx_device_sum_noalloc"]
+            "thorx_device_sum", "thorx_device_sum_noalloc", "thorx_rt_enable",
+            "thorx_rt_totals"]
 
 def device_sum(ptr, n, stream=0):
     """Compensated sum of n doubles at device address `ptr` (thorx_device_sum)."""
@@ -261,6 +289,17 @@ class Thorx:
         ms = (ctypes.c_double * k)()
         self._check(lib().thorx_profile_steps(self.h, n, ms))
         return list(ms)
+
+    def rt_enable(self, d):
+        """Double-gray RT + insolation in every following ProfX (dict as for rt_params)."""
+        self._rt = rt_params(d)
+        self._check(lib().thorx_rt_enable(self.h, ctypes.byref(self._rt)))
+
+    def rt_totals(self):
+        """(ASR, OLR) of the last RT call, globally summed."""
+        a, o = ctypes.c_double(), ctypes.c_double()
+        self._check(lib().thorx_rt_totals(self.h, ctypes.byref(a), ctypes.byref(o)))
+        return a.value, o.value
 
     def globdiag(self):
         """Global energy, mass, angular momentum (x, y, z) and entropy of the current state."""

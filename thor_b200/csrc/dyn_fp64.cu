@@ -165,7 +165,8 @@ __global__ void level_tables_kernel(Geometry g, Phys P, double* lt) {
 // and the NaN check on temperature (:132-146, src/ESP/profx_driver.cu:389-396,451-458).
 // One thread per column (1% of a step).
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(kColBlock) profx_kernel(Geometry g, Phys P, State s) {
+__global__ void __launch_bounds__(kColBlock) profx_kernel(Geometry g, Phys P, State s,
+                                                          bool finish) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= g.N)
         return;
@@ -209,9 +210,26 @@ __global__ void __launch_bounds__(kColBlock) profx_kernel(Geometry g, Phys P, St
             s.T[i] -= kt * P.timestep * (s.T[i] - Teq);
         }
     }
+    if (!finish) // physics modules run before the pressure update (profx_driver.cu:405-416)
+        return;
     bool bad = false;
     for (int lev = 0; lev < nv; lev++) {
         int i  = lev * Np + c;
+        s.p[i] = s.T[i] * s.Rd[i] * s.Rho[i];
+        bad |= isnan(s.T[i]);
+    }
+    if (bad)
+        atomicOr(s.flags, kFlagNaN);
+}
+
+// Compute_pressure (profx_auxiliary.h:94-107) and the NaN check, after the physics modules.
+__global__ void __launch_bounds__(kColBlock) profx_finish_kernel(Geometry g, State s) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= g.N)
+        return;
+    bool bad = false;
+    for (int lev = 0; lev < g.nv; lev++) {
+        int i  = lev * g.Np + c;
         s.p[i] = s.T[i] * s.Rd[i] * s.Rho[i];
         bad |= isnan(s.T[i]);
     }
@@ -1077,7 +1095,7 @@ __global__ void THORX_KATTR_VERT
     stage(sdiv, g.div, 21, Np, c0);
     __syncthreads();
     const bool    active = c < g.N;
-    const double  A = P.A, Gravit = P.Gravit;
+    const double  Gravit = P.Gravit;
     const bool    deep = P.DeepModel, nonh = P.NonHydro, ghv = P.GravHeightVar;
     const double* Alt  = g.Altitude;
     const double* Alth = g.Altitudeh;
@@ -1443,8 +1461,11 @@ void launch_level_tables(const Geometry& g, const Phys& P, double* lt, cudaStrea
     level_tables_kernel<<<(g.nvi + 127) / 128, 128, 0, st>>>(g, P, lt);
 }
 
-void launch_profx(const Geometry& g, const Phys& P, const State& s, cudaStream_t st) {
-    profx_kernel<<<(g.N + kColBlock - 1) / kColBlock, kColBlock, 0, st>>>(g, P, s);
+void launch_profx(const Geometry& g, const Phys& P, const State& s, bool finish, cudaStream_t st) {
+    profx_kernel<<<(g.N + kColBlock - 1) / kColBlock, kColBlock, 0, st>>>(g, P, s, finish);
+}
+void launch_profx_finish(const Geometry& g, const State& s, cudaStream_t st) {
+    profx_finish_kernel<<<(g.N + kColBlock - 1) / kColBlock, kColBlock, 0, st>>>(g, s);
 }
 void launch_adv_temp(const Geometry& g, const Phys& P, const State& s, cudaStream_t st) {
     adv_temp_kernel<<<tile_grid(g), tile_block(), 0, st>>>(g, P, s);

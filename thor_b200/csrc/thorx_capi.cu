@@ -49,6 +49,9 @@ struct thorx_ctx {
     std::map<std::string, FieldDesc> fields;
     double*                          staging     = nullptr; // layout conversion buffer
     size_t                           staging_len = 0;       // doubles
+    bool                             rt_enabled  = false;   // double-gray RT in ProfX
+    RtConst                          rt_c{};
+    RtFields                         rt_f{};
     double2*                         gd_part     = nullptr; // global-sum partials (6 quantities)
     double*                          gd_out      = nullptr; // the six global sums
     unsigned int*                    flags_host  = nullptr; // pinned
@@ -229,10 +232,10 @@ int check_flags(thorx_ctx* ctx) {
 
 // Kernel classes of one step, for thorx_kernel_info / thorx_profile_steps.
 enum KClass { KProfx = 0, KAdvTemp, KDiffFirst, KDiffLast, KDivm0, KSlow, KMomentum, KVertical,
-              KUpdateRk2, KNumClasses };
+              KUpdateRk2, KRt, KNumClasses };
 const char* const kClassName[KNumClasses] = {"profx", "adv_temp", "diffusion_first",
                                              "diffusion_last", "divm0", "slow_modes", "momentum",
-                                             "vertical", "update_rk2"};
+                                             "vertical", "update_rk2", "radiative_transfer"};
 
 cudaEvent_t next_event(thorx_ctx* ctx) {
     if (ctx->event_next == ctx->event_pool.size()) {
@@ -294,6 +297,9 @@ double class_bytes(const thorx_ctx* ctx, int k) {
         return 19 * S + 6 * Si + 21 * G + 6 * I + N + Si + 2 * S;
     case KUpdateRk2: // Mhs, Mhk, Rhok, Rhos, pk, ps, Whk, Whs | Mhk, Rhok, pk, Whk, Wk
         return 10 * S + 2 * Si + 3 * G + 6 * S + Si;
+    case KRt: // p, Rho, T, Rd, Cp, Qheat, lat, lon, areasT, insol_ann | phtemp, thtemp, fsw/flw
+              // up/down, tau (2), ttemp, dtemp, DG_Qheat, Qheat, insol, insol_ann, ASR, OLR, coszen
+        return ctx->rt_enabled ? 6 * S + 4 * G + 6 * Si + 6 * S + 6 * G : 0;
     }
     return 0;
 }
@@ -302,7 +308,8 @@ int class_launches(const thorx_ctx* ctx, int k) {
     const Phys& P      = ctx->P;
     const int   passes = P.HyDiff ? P.HyDiffOrder / 2 : 0;
     switch (k) {
-    case KProfx: return 1;
+    case KProfx: return ctx->rt_enabled ? 2 : 1; // ProfX, then its pressure update after RT
+    case KRt: return ctx->rt_enabled ? 1 : 0;     // one bracket: orbit kernel + column kernel
     case KAdvTemp: return 3;
     case KDiffFirst: return 3 * (passes - (passes > 0 ? 1 : 0));
     case KDiffLast: return passes > 0 ? 3 : 0;
@@ -318,9 +325,23 @@ int class_launches(const thorx_ctx* ctx, int k) {
 // ESP::ProfX
 int enqueue_profx(thorx_ctx* ctx) {
     CK(cudaMemsetAsync(ctx->s.Qheat, 0, sizeof(double) * ctx->g.nv * ctx->g.Np, ctx->stream));
-    {
+    if (!ctx->rt_enabled) {
         KScope k(ctx, KProfx);
-        launch_profx(ctx->g, ctx->P, ctx->s, ctx->stream);
+        launch_profx(ctx->g, ctx->P, ctx->s, true, ctx->stream);
+    }
+    else { // the physics modules run before Compute_pressure (profx_driver.cu:405-432)
+        {
+            KScope k(ctx, KProfx);
+            launch_profx(ctx->g, ctx->P, ctx->s, false, ctx->stream);
+        }
+        {
+            KScope k(ctx, KRt);
+            launch_rt(ctx->g, ctx->P, ctx->rt_c, ctx->rt_f, ctx->s, ctx->stream);
+        }
+        {
+            KScope k(ctx, KProfx);
+            launch_profx_finish(ctx->g, ctx->s, ctx->stream);
+        }
     }
     CK(cudaGetLastError());
     return 0;
@@ -844,7 +865,7 @@ int thorx_kernels_per_step(const thorx_ctx* ctx) {
     int n = 0;
     for (int k = 0; k < KNumClasses; k++)
         n += class_launches(ctx, k);
-    return n;
+    return n + (ctx->rt_enabled ? 1 : 0); // the RT bracket holds two kernels
 }
 
 int thorx_kernel_classes(const thorx_ctx* ctx) { return ctx ? (int)KNumClasses : THORX_E_ARG; }
@@ -885,6 +906,129 @@ int thorx_profile_steps(thorx_ctx* ctx, int nsteps, double* ms_per_class) {
         CK(cudaEventElapsedTime(&ms, e.second.first, e.second.second));
         ms_per_class[e.first] += ms;
     }
+    return 0;
+}
+
+int thorx_rt_enable(thorx_ctx* ctx, const thorx_rt_params* r) {
+    if (!ctx)
+        return THORX_E_ARG;
+    if (!r)
+        return fail(ctx, THORX_E_ARG, "thorx_rt_enable: null argument");
+    if (ctx->rt_enabled)
+        return fail(ctx, THORX_E_STATE, "thorx_rt_enable: RT is already enabled");
+    if (r->surface)
+        return fail(ctx, THORX_E_UNSUPPORTED, "thorx_rt_enable: surface = true is not implemented");
+    if (ctx->P.GravHeightVar)
+        return fail(ctx, THORX_E_UNSUPPORTED,
+                    "thorx_rt_enable: GravHeightVar with RT reads past Altitudeh in the reference "
+                    "(profx_RT.h:68); not supported");
+    if (!(r->planet_star_dist > 0) || !(r->radius_star > 0) || !(r->Tstar >= 0) || !(r->f_lw > 0)
+        || !(r->diff_ang > 0) || !(r->ecc >= 0 && r->ecc < 1) || r->first_step < 1
+        || (!r->sync_rot && !(r->mean_motion > 0)))
+        return fail(ctx, THORX_E_ARG, "thorx_rt_enable: parameter out of range");
+    const int N = ctx->g.N, nv = ctx->g.nv, nvi = nv + 1, Np = ctx->g.Np;
+    (void)N;
+    RtConst& c = ctx->rt_c;
+    // RTSetup (radiative_transfer.cu:1431-1432); Insolation::initial_conditions (insolation.cu:292-313)
+    const double resc_flx = pow(r->radius_star / r->planet_star_dist, 2.0);
+    c.incflx   = resc_flx * 5.6703744191844314e-08 * r->Tstar * r->Tstar * r->Tstar * r->Tstar;
+    c.diff_ang = r->diff_ang;
+    c.Tint     = r->Tint;
+    c.albedo   = r->albedo;
+    c.kappa_sw = r->kappa_sw;
+    c.kappa_lw = r->kappa_lw;
+    c.kappa_lw_pole = r->kappa_lw_pole;
+    c.n_sw     = r->n_sw;
+    c.n_lw     = r->n_lw;
+    c.f_lw     = r->f_lw;
+    c.mean_motion = r->sync_rot ? ctx->P.Omega : r->mean_motion;
+    c.true_long_i = r->true_long_i * M_PI / 180.0;
+    c.longp       = r->longp * M_PI / 180.0;
+    c.ecc         = r->ecc;
+    {
+        double f = fmod(c.true_long_i - c.longp, (2 * M_PI));
+        while (f < 0.0)
+            f += 2 * M_PI;
+        while (f >= 2 * M_PI)
+            f -= 2 * M_PI;
+        const double cosE = (cos(f) + c.ecc) / (1.0 + c.ecc * cos(f));
+        const double E_i  = f < M_PI ? acos(cosE) : 2 * M_PI - acos(cosE);
+        c.mean_anomaly_i  = fmod(E_i - c.ecc * sin(E_i), (2 * M_PI));
+    }
+    c.alpha_i        = r->alpha_i * M_PI / 180.0;
+    c.obliquity      = r->obliquity * M_PI / 180.0;
+    c.latf_lw        = r->latf_lw;
+    c.rt1Dmode       = r->rt1Dmode;
+    c.sync_rot       = r->sync_rot;
+    c.spinup_start   = r->spinup_start;
+    c.spinup_stop    = r->spinup_stop;
+    c.spindown_start = r->spindown_start;
+    c.spindown_stop  = r->spindown_stop;
+
+    RtFields& f = ctx->rt_f;
+    const size_t cell = (size_t)nv * Np, iface = (size_t)nvi * Np;
+    if (dev_alloc(ctx, &f.phtemp, iface) || dev_alloc(ctx, &f.thtemp, iface)
+        || dev_alloc(ctx, &f.fsw_up, iface) || dev_alloc(ctx, &f.fsw_dn, iface)
+        || dev_alloc(ctx, &f.flw_up, iface) || dev_alloc(ctx, &f.flw_dn, iface)
+        || dev_alloc(ctx, &f.tau, 2 * cell) || dev_alloc(ctx, &f.ttemp, cell)
+        || dev_alloc(ctx, &f.dtemp, cell) || dev_alloc(ctx, &f.qheat, cell)
+        || dev_alloc(ctx, &f.insol, (size_t)Np) || dev_alloc(ctx, &f.insol_ann, (size_t)Np)
+        || dev_alloc(ctx, &f.ASR, (size_t)Np) || dev_alloc(ctx, &f.OLR, (size_t)Np)
+        || dev_alloc(ctx, &f.cos_zenith, (size_t)Np) || dev_alloc(ctx, &f.step, 1))
+        return THORX_E_CUDA;
+    RtStep st{};
+    st.nstep         = r->first_step;
+    st.r_orb         = 1.0; // Insolation member defaults (insolation.h:112-118)
+    st.sin_decl      = 0.0;
+    st.cos_decl      = 1.0;
+    st.alpha         = 0.0;
+    st.Qheat_scaling = 1.0;
+    st.run           = 1;
+    CK(cudaMemcpy(f.step, &st, sizeof(st), cudaMemcpyHostToDevice));
+    auto& F         = ctx->fields;
+    F["phtemp"]     = {&f.phtemp, nvi, 1};
+    F["thtemp"]     = {&f.thtemp, nvi, 1};
+    F["fsw_up"]     = {&f.fsw_up, nvi, 1};
+    F["fsw_dn"]     = {&f.fsw_dn, nvi, 1};
+    F["flw_up"]     = {&f.flw_up, nvi, 1};
+    F["flw_dn"]     = {&f.flw_dn, nvi, 1};
+    F["tau"]        = {&f.tau, nv, 2};
+    F["ttemp"]      = {&f.ttemp, nv, 1};
+    F["dtemp"]      = {&f.dtemp, nv, 1};
+    F["DG_Qheat"]   = {&f.qheat, nv, 1};
+    F["insol"]      = {&f.insol, 1, 1};
+    F["insol_ann"]  = {&f.insol_ann, 1, 1};
+    F["ASR"]        = {&f.ASR, 1, 1};
+    F["OLR"]        = {&f.OLR, 1, 1};
+    F["cos_zenith"] = {&f.cos_zenith, 1, 1};
+    // a step graph captured before this call lacks the module: capture again on the next step
+    if (ctx->graph_exec) {
+        CK(cudaGraphExecDestroy(ctx->graph_exec));
+        ctx->graph_exec = nullptr;
+    }
+    if (ctx->graph) {
+        CK(cudaGraphDestroy(ctx->graph));
+        ctx->graph = nullptr;
+    }
+    ctx->rt_enabled = true;
+    return 0;
+}
+
+int thorx_rt_totals(thorx_ctx* ctx, double* asr, double* olr) {
+    if (!ctx)
+        return THORX_E_ARG;
+    if (!asr || !olr)
+        return fail(ctx, THORX_E_ARG, "thorx_rt_totals: null argument");
+    if (!ctx->rt_enabled)
+        return fail(ctx, THORX_E_STATE, "thorx_rt_totals: RT is not enabled");
+    launch_device_sum(ctx->rt_f.ASR, ctx->g.N, ctx->gd_part, ctx->gd_out, ctx->stream);
+    launch_device_sum(ctx->rt_f.OLR, ctx->g.N, ctx->gd_part, ctx->gd_out + 1, ctx->stream);
+    CK(cudaGetLastError());
+    double out[2];
+    CK(cudaMemcpyAsync(out, ctx->gd_out, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    *asr = out[0];
+    *olr = out[1];
     return 0;
 }
 

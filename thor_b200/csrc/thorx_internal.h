@@ -121,7 +121,10 @@ size_t vertical_smem_bytes(const Geometry& g);
 void launch_level_tables(const Geometry& g, const Phys& P, double* lt, cudaStream_t st);
 
 // Kernel launchers (thor_b200/csrc/dyn_fp64.cu).
-void launch_profx(const Geometry& g, const Phys& P, const State& s, cudaStream_t st);
+// ProfX up to the physics modules; with finish, also the pressure update and NaN check, which
+// launch_profx_finish does separately when modules run in between.
+void launch_profx(const Geometry& g, const Phys& P, const State& s, bool finish, cudaStream_t st);
+void launch_profx_finish(const Geometry& g, const State& s, cudaStream_t st);
 void launch_adv_temp(const Geometry& g, const Phys& P, const State& s, cudaStream_t st);
 void launch_diffusion(const Geometry& g, const Phys& P, const State& s, int stepnum, bool last,
                       cudaStream_t st);
@@ -134,6 +137,29 @@ void launch_momentum(const Geometry& g, const Phys& P, const State& s, double dt
 void launch_vertical(const Geometry& g, const Phys& P, const State& s, double dt,
                      cudaStream_t st);
 void launch_update_rk2(const Geometry& g, const Phys& P, const State& s, cudaStream_t st);
+
+// Double-gray radiative transfer with its insolation (thor_b200/csrc/rt.cu).
+struct RtConst { // set once by thorx_rt_enable; angles in radians, lengths in m
+    double incflx, diff_ang, Tint, albedo, kappa_sw, kappa_lw, kappa_lw_pole, n_sw, n_lw, f_lw;
+    double mean_motion, mean_anomaly_i, true_long_i, ecc, obliquity, alpha_i, longp;
+    int    latf_lw, rt1Dmode, sync_rot;
+    int    spinup_start, spinup_stop, spindown_start, spindown_stop;
+};
+struct RtStep { // per-step scalars, device-resident so that a captured step graph advances them
+    long long nstep;  // step number of the next physics step
+    long long cur;    // step number of the current one
+    double    r_orb, sin_decl, cos_decl, alpha; // Insolation state (member defaults 1, 0, 1, 0)
+    double    Qheat_scaling;
+    int       run;
+};
+struct RtFields { // column-fastest device arrays (interfaces nv+1 planes, tau 2 x nv planes)
+    double *phtemp, *thtemp, *ttemp, *dtemp, *qheat, *tau, *fsw_up, *fsw_dn, *flw_up, *flw_dn;
+    double *insol, *insol_ann, *ASR, *OLR, *cos_zenith;
+    RtStep* step;
+};
+// Insolation::phy_loop + radiative_transfer::phy_loop (DualbandGray) of one physics step.
+void launch_rt(const Geometry& g, const Phys& P, const RtConst& c, const RtFields& f,
+               const State& s, cudaStream_t st);
 
 // Global sums (thor_b200/csrc/globdiag.cu).
 // Partials the global-diagnostics reduction writes (double2 each, per quantity).
