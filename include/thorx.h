@@ -183,6 +183,68 @@ int thorx_rt_enable(thorx_ctx* ctx, const thorx_rt_params* rt);
  * (the reference's ASR_tot / OLR_tot, radiative_transfer.cu:1083-1084), compensated sums. */
 int thorx_rt_totals(thorx_ctx* ctx, double* asr, double* olr);
 
+/* ---- BF16 tensor-core GEMM (tcgen05, FP32 accumulate), the building block of the RT surrogate.
+ * No counterpart in the reference. D[M x N] = A[M x K] . B[N x K]^T with A, B bf16 (raw 16-bit
+ * patterns, row-major, K contiguous) and D float32, all host buffers. M a multiple of 128, N of
+ * 64, K of 64. Context-free; on error thorx_surrogate_last_error() has the message. */
+int thorx_bf16_gemm(const unsigned short* A, const unsigned short* B, int M, int N, int K, float* D);
+const char* thorx_surrogate_last_error(void);
+
+/* ---- Learned RT surrogate. No counterpart in the reference. ----
+ * A per-column MLP from (T per level, ln p per level, cos zenith) to the double-gray RT heating
+ * rates per level (W m^-3, what rtm_dual_band adds to profx_Qheat): 2 nv + 1 inputs, three hidden
+ * layers of `hidden` units with GELU, nv outputs; BF16 weights and activations, FP32
+ * accumulation on the tensor cores, FP32 master weights trained with Adam on the GPU. Inputs and
+ * outputs are standardised with the mean and standard deviation of the logged training data
+ * (fitted on the first thorx_surrogate_train call, or set with thorx_surrogate_normalisation).
+ * Modes, set between steps (a captured step graph is re-captured):
+ *   THORX_SUR_LOG  every physics step runs the plain RT and appends each column's inputs and
+ *                  heating rates to a ring of log_capacity columns (the training set);
+ *   THORX_SUR_USE  every physics step runs the surrogate on all columns and the plain RT only on
+ *                  the columns it re-checks this step (column % recheck_period == step %
+ *                  recheck_period) and on those that have fallen back: a re-checked column whose
+ *                  relative error max|Q_sur - Q_rt| / max|Q_rt| exceeds `tolerance` falls back
+ *                  to the plain RT until a later re-check passes; re-checked columns use the
+ *                  plain RT's heating. The cooling limiter and profx_Qheat coupling of the plain
+ *                  RT apply to the chosen heating. ASR/OLR are current only on the columns the
+ *                  plain RT ran on.
+ * Requires thorx_rt_enable first. */
+#define THORX_SUR_OFF 0
+#define THORX_SUR_LOG 1
+#define THORX_SUR_USE 2
+typedef struct {
+    int                hidden;         /* hidden width, a multiple of 256 (512)               */
+    int                train_batch;    /* largest training batch, a multiple of 128 (8192)     */
+    long long          log_capacity;   /* logged columns kept (ring), 0 = no logging           */
+    int                recheck_period; /* plain-RT re-check of 1/recheck_period columns (16)   */
+    double             tolerance;      /* relative heating error that triggers fallback (0.05) */
+    unsigned long long seed;           /* weight initialisation and batch sampling             */
+} thorx_surrogate_params;
+int thorx_surrogate_create(thorx_ctx* ctx, const thorx_surrogate_params* sp);
+int thorx_surrogate_set_mode(thorx_ctx* ctx, int mode);
+/* Columns logged so far (may exceed log_capacity: the ring keeps the latest). */
+long long thorx_surrogate_logged(thorx_ctx* ctx);
+/* `iterations` Adam steps (lr, batch rows drawn uniformly from the log); the mean squared error
+ * (standardised units) of the first and the last batch. */
+int thorx_surrogate_train(thorx_ctx* ctx, int iterations, int batch, double lr, double* loss_first,
+                          double* loss_last);
+/* Since the previous call: columns re-checked, re-checks that failed, the largest re-check error
+ * (in units of 1e-6), and column-steps heated by the plain RT. Resets the counters. */
+int thorx_surrogate_stats(thorx_ctx* ctx, unsigned int out[4]);
+/* Weights of layer 0..3 (padded shapes N x K from the call; W [N][K], b [N]), get or set. */
+int thorx_surrogate_layer(thorx_ctx* ctx, int layer, int* N, int* K, float* W, float* b, int set);
+/* Gradients of the last thorx_surrogate_gradients_host / training batch (padded shapes). */
+int thorx_surrogate_layer_grad(thorx_ctx* ctx, int layer, float* gW, float* gb);
+/* Standardisation: in_* [2 nv + 1], out_* [nv]; get or set (set marks the surrogate usable). */
+int thorx_surrogate_normalisation(thorx_ctx* ctx, float* in_mean, float* in_std, float* out_mean,
+                                  float* out_std, int set);
+/* Network output (standardised) for B standardised input rows x [B][2 nv + 1] -> y [B][nv]. */
+int thorx_surrogate_forward_host(thorx_ctx* ctx, const float* x, int B, float* y);
+/* Forward and backward pass of the MSE loss on (x [B][2 nv + 1], t [B][nv]) standardised rows,
+ * B a multiple of 128, without an optimiser step; gradients via thorx_surrogate_layer_grad. */
+int thorx_surrogate_gradients_host(thorx_ctx* ctx, const float* x, const float* t, int B,
+                                   double* loss);
+
 /* ---- Global conserved quantities (replaces ESP::globdiag, src/ESP/profx_driver.cu:476-569,
  * with the per-cell terms of CalcTotEnergy / CalcMass / CalcAngMom / CalcEntropy,
  * src/ESP/profx_globdiag.cu:45-252; no surface term) ----

@@ -20,6 +20,7 @@
 #include "thor_oracle.h"
 
 #include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <map>
 #include <string>
@@ -1887,6 +1888,116 @@ extern "C" double oracle_sum(const double* x, long n) {
     for (long i = 0; i < n; i++)
         s.add(x[i]);
     return s.value();
+}
+
+// ---- RT surrogate MLP (float64, bf16 rounding emulated) ---------------------------------------
+namespace {
+// round to the nearest bf16, ties to even (finite values)
+double to_bf16(double v) {
+    float    f = (float)v;
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    u = (u + 0x7FFFu + ((u >> 16) & 1u)) & 0xFFFF0000u;
+    std::memcpy(&f, &u, 4);
+    return f;
+}
+double gelu(double z) { return 0.5 * z * (1.0 + std::erf(z / std::sqrt(2.0))); }
+double gelu_grad(double z) {
+    return 0.5 * (1.0 + std::erf(z / std::sqrt(2.0)))
+           + z * std::exp(-0.5 * z * z) / std::sqrt(2.0 * M_PI);
+}
+} // namespace
+
+extern "C" int oracle_mlp(int nv, int H, const float* const* W, const float* const* b,
+                          const float* x, const float* t, int B, double* y, double* loss,
+                          double* const* gW, double* const* gb) {
+    const int n_in = 2 * nv + 1, Kin = ((n_in + 63) / 64) * 64, Nout = ((nv + 63) / 64) * 64;
+    const int N[4] = {H, H, H, Nout}, K[4] = {Kin, H, H, H};
+    std::vector<Vec> Wb(4);
+    for (int l = 0; l < 4; l++) {
+        Wb[l].resize((size_t)N[l] * K[l]);
+        for (size_t i = 0; i < Wb[l].size(); i++)
+            Wb[l][i] = to_bf16(W[l][i]);
+    }
+    // forward: act[0] = X0, act[l] = bf16(gelu(Z_l)) for l = 1..3, then Y
+    std::vector<Vec> act(4), Z(3);
+    act[0].assign((size_t)B * Kin, 0.0);
+    for (int r = 0; r < B; r++)
+        for (int j = 0; j < n_in; j++)
+            act[0][(size_t)r * Kin + j] = to_bf16(x[(size_t)r * n_in + j]);
+    Vec Y;
+    for (int l = 0; l < 4; l++) {
+        const Vec& in = act[l];
+        Vec        out((size_t)B * N[l]);
+#pragma omp parallel for schedule(static)
+        for (int r = 0; r < B; r++)
+            for (int n = 0; n < N[l]; n++) {
+                double acc = 0.0;
+                for (int k = 0; k < K[l]; k++)
+                    acc += in[(size_t)r * K[l] + k] * Wb[l][(size_t)n * K[l] + k];
+                out[(size_t)r * N[l] + n] = acc + (double)b[l][n];
+            }
+        if (l < 3) {
+            Z[l] = out;
+            act[l + 1].resize(out.size());
+            for (size_t i = 0; i < out.size(); i++)
+                act[l + 1][i] = to_bf16(gelu(out[i]));
+        }
+        else
+            Y = out;
+    }
+    if (y)
+        for (int r = 0; r < B; r++)
+            for (int j = 0; j < nv; j++)
+                y[(size_t)r * nv + j] = Y[(size_t)r * Nout + j];
+    if (!t)
+        return 0;
+    Vec    dYf((size_t)B * Nout, 0.0), dY((size_t)B * Nout, 0.0);
+    double L = 0.0;
+    for (int r = 0; r < B; r++)
+        for (int j = 0; j < nv; j++) {
+            const double d = Y[(size_t)r * Nout + j] - t[(size_t)r * nv + j];
+            L += d * d;
+            dYf[(size_t)r * Nout + j] = 2.0 * d / ((double)B * nv);
+            dY[(size_t)r * Nout + j]  = to_bf16(dYf[(size_t)r * Nout + j]);
+        }
+    if (loss)
+        *loss = L / ((double)B * nv);
+    if (!gW || !gb)
+        return 0;
+    // backward; G = gradient w.r.t. the layer's pre-activation as the GPU feeds it to the GEMMs
+    // (bf16); the output layer's bias gradient uses the unrounded output gradient
+    Vec G = dY;
+    for (int l = 3; l >= 0; l--) {
+        const Vec& in = act[l];
+        for (int n = 0; n < N[l]; n++) {
+            double sum = 0.0;
+            for (int r = 0; r < B; r++)
+                sum += (l == 3 ? dYf : G)[(size_t)r * N[l] + n];
+            gb[l][n] = sum;
+        }
+#pragma omp parallel for schedule(static)
+        for (int n = 0; n < N[l]; n++)
+            for (int k = 0; k < K[l]; k++) {
+                double sum = 0.0;
+                for (int r = 0; r < B; r++)
+                    sum += G[(size_t)r * N[l] + n] * in[(size_t)r * K[l] + k];
+                gW[l][(size_t)n * K[l] + k] = sum;
+            }
+        if (l == 0)
+            break;
+        Vec Gn((size_t)B * K[l]);
+#pragma omp parallel for schedule(static)
+        for (int r = 0; r < B; r++)
+            for (int k = 0; k < K[l]; k++) {
+                double sum = 0.0;
+                for (int n = 0; n < N[l]; n++)
+                    sum += G[(size_t)r * N[l] + n] * Wb[l][(size_t)n * K[l] + k];
+                Gn[(size_t)r * K[l] + k] = to_bf16(sum * gelu_grad(Z[l - 1][(size_t)r * K[l] + k]));
+            }
+        G.swap(Gn);
+    }
+    return 0;
 }
 
 extern "C" void oracle_set_threads(int n) {

@@ -58,6 +58,15 @@ int  oracle_step(void* h, int nsteps, int do_profx, int do_thor);
 int    oracle_globdiag(void* h, double* out, double* abs_out);
 // Compensated (Neumaier) sum of x[0..n-1] in index order.
 double oracle_sum(const double* x, long n);
+// The RT surrogate MLP (thor_b200/csrc/surrogate.cu) in float64 on the CPU, with the GPU's
+// bf16 rounding points: inputs, weights and hidden activations rounded to bf16, the output
+// gradient and the pre-activation gradients rounded to bf16 where the GPU feeds them to a GEMM.
+// Shapes padded as on the GPU: layer l has W[l] [N_l][K_l], b[l] [N_l] (N = H, H, H, Nout;
+// K = Kin, H, H, H). x [B][n_in], t [B][nv] standardised; outputs y [B][nv], loss (mean squared
+// error), gradients gW[l] (same shape as W[l]) and gb[l]. t, gW, gb may be null (forward only).
+int oracle_mlp(int nv, int H, const float* const* W, const float* const* b, const float* x,
+               const float* t, int B, double* y, double* loss, double* const* gW,
+               double* const* gb);
 void oracle_set_threads(int n);
 void oracle_free(void* h);
 

@@ -390,3 +390,33 @@ def field_tolerance(spread, floor=1e-12, factor=4.0):
     """Tolerance of a field: 1e-12, or `factor` x the reference's own FMA / no-FMA spread where
     cancellation makes the reference itself that uncertain."""
     return max(floor, factor * spread)
+
+
+# ------------------------------------------------------------------------------------------------
+# The surrogate MLP restated on the CPU (oracle_mlp)
+# ------------------------------------------------------------------------------------------------
+def oracle_mlp(nv, H, Ws, bs, x, t=None):
+    """float64 forward (and backward if t is given) of the surrogate network with the GPU's bf16
+    rounding points. Ws, bs: the four padded layers as float32 arrays. Returns y, loss, gW, gb."""
+    lib = oracle_lib()
+    lib.oracle_mlp.restype = ctypes.c_int
+    lib.oracle_mlp.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                               ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                               ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    Ws = [np.ascontiguousarray(w, dtype=np.float32) for w in Ws]
+    bs = [np.ascontiguousarray(b, dtype=np.float32) for b in bs]
+    Wp = (ctypes.c_void_p * 4)(*[w.ctypes.data for w in Ws])
+    bp = (ctypes.c_void_p * 4)(*[b.ctypes.data for b in bs])
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    B = x.shape[0]
+    y = np.zeros((B, nv))
+    loss = ctypes.c_double()
+    gW = [np.zeros(w.shape) for w in Ws]
+    gb = [np.zeros(b.shape) for b in bs]
+    gWp = (ctypes.c_void_p * 4)(*[g.ctypes.data for g in gW])
+    gbp = (ctypes.c_void_p * 4)(*[g.ctypes.data for g in gb])
+    tt = None if t is None else np.ascontiguousarray(t, dtype=np.float32)
+    assert lib.oracle_mlp(nv, H, Wp, bp, x.ctypes.data, None if tt is None else tt.ctypes.data, B,
+                          y.ctypes.data, ctypes.byref(loss), gWp if tt is not None else None,
+                          gbp if tt is not None else None) == 0
+    return y, loss.value, gW, gb

@@ -57,6 +57,15 @@ def rt_params(d):
     return RtParamsC(*[float(v[n]) for n in RT_F64], *[int(v[n]) for n in RT_INT])
 
 
+class SurrogateParamsC(ctypes.Structure):
+    _fields_ = [("hidden", ctypes.c_int), ("train_batch", ctypes.c_int),
+                ("log_capacity", ctypes.c_longlong), ("recheck_period", ctypes.c_int),
+                ("tolerance", ctypes.c_double), ("seed", ctypes.c_ulonglong)]
+
+
+SUR_OFF, SUR_LOG, SUR_USE = 0, 1, 2
+
+
 class ParamsC(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in
                 ["A", "Omega", "Gravit", "Rd", "Cp", "P_Ref", "Top_altitude", "timestep", "Diffc",
@@ -120,6 +129,28 @@ def lib():
         L.thorx_device_sum_noalloc.argtypes = [vp, ctypes.c_longlong, vp,
                                                ctypes.POINTER(ctypes.c_double)]
         L.thorx_device_sum_noalloc.restype = ci
+        L.thorx_bf16_gemm.argtypes = [vp, vp, ci, ci, ci, vp]
+        L.thorx_bf16_gemm.restype = ci
+        L.thorx_surrogate_last_error.restype = cp
+        L.thorx_surrogate_create.argtypes = [vp, ctypes.POINTER(SurrogateParamsC)]
+        L.thorx_surrogate_set_mode.argtypes = [vp, ci]
+        L.thorx_surrogate_logged.argtypes = [vp]
+        L.thorx_surrogate_logged.restype = ctypes.c_longlong
+        L.thorx_surrogate_train.argtypes = [vp, ci, ci, ctypes.c_double,
+                                            ctypes.POINTER(ctypes.c_double),
+                                            ctypes.POINTER(ctypes.c_double)]
+        L.thorx_surrogate_stats.argtypes = [vp, vp]
+        L.thorx_surrogate_layer.argtypes = [vp, ci, ctypes.POINTER(ci), ctypes.POINTER(ci), vp, vp,
+                                            ci]
+        L.thorx_surrogate_layer_grad.argtypes = [vp, ci, vp, vp]
+        L.thorx_surrogate_normalisation.argtypes = [vp, vp, vp, vp, vp, ci]
+        L.thorx_surrogate_forward_host.argtypes = [vp, vp, ci, vp]
+        L.thorx_surrogate_gradients_host.argtypes = [vp, vp, vp, ci, ctypes.POINTER(ctypes.c_double)]
+        for f in ["thorx_surrogate_create", "thorx_surrogate_set_mode", "thorx_surrogate_train",
+                  "thorx_surrogate_stats", "thorx_surrogate_layer", "thorx_surrogate_layer_grad",
+                  "thorx_surrogate_normalisation", "thorx_surrogate_forward_host",
+                  "thorx_surrogate_gradients_host"]:
+            getattr(L, f).restype = ci
         L.thorx_rt_enable.argtypes = [vp, ctypes.POINTER(RtParamsC)]
         L.thorx_rt_enable.restype = ci
         L.thorx_rt_totals.argtypes = [vp, ctypes.POINTER(ctypes.c_double),
@@ -135,7 +166,11 @@ EXPORTED = ["thorx_create", "thorx_destroy", "thorx_last_error", "thorx_field_si
             "thorx_grid_get", "thorx_grid_describe", "thorx_grid_free", "thorx_init_rest_state",
             "thorx_kernel_classes", "thorx_kernel_info", "thorx_profile_steps", "thorx_globdiag",
             "thorx_device_sum", "thorx_device_sum_noalloc", "thorx_rt_enable",
-            "thorx_rt_totals"]
+            "thorx_rt_totals", "thorx_bf16_gemm", "thorx_surrogate_last_error",
+            "thorx_surrogate_create", "thorx_surrogate_set_mode", "thorx_surrogate_logged",
+            "thorx_surrogate_train", "thorx_surrogate_stats", "thorx_surrogate_layer",
+            "thorx_surrogate_layer_grad", "thorx_surrogate_normalisation",
+            "thorx_surrogate_forward_host", "thorx_surrogate_gradients_host"]
 
 def device_sum(ptr, n, stream=0):
     """Compensated sum of n doubles at device address `ptr` (thorx_device_sum)."""
@@ -144,6 +179,31 @@ def device_sum(ptr, n, stream=0):
     if rc:
         raise ThorxError(rc, lib().thorx_last_error(None).decode())
     return out.value
+
+
+def bf16_bits(a):
+    """float array -> bf16 bit patterns (uint16), round to nearest even."""
+    u = np.ascontiguousarray(a, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) >> 16
+    return u.astype(np.uint16)
+
+
+def bf16_value(bits):
+    """bf16 bit patterns -> float32 values."""
+    return (np.asarray(bits, dtype=np.uint32) << 16).view(np.float32)
+
+
+def bf16_gemm(A_bits, B_bits):
+    """D = A . B^T on the tensor cores (thorx_bf16_gemm); A [M x K], B [N x K] bf16 bit patterns."""
+    A_bits = np.ascontiguousarray(A_bits, dtype=np.uint16)
+    B_bits = np.ascontiguousarray(B_bits, dtype=np.uint16)
+    M, K = A_bits.shape
+    N = B_bits.shape[0]
+    D = np.zeros((M, N), dtype=np.float32)
+    rc = lib().thorx_bf16_gemm(A_bits.ctypes.data, B_bits.ctypes.data, M, N, K, D.ctypes.data)
+    if rc:
+        raise ThorxError(rc, lib().thorx_surrogate_last_error().decode())
+    return D
 
 
 NOALLOC_SUM_MAX_N = 134217728
@@ -300,6 +360,81 @@ class Thorx:
         a, o = ctypes.c_double(), ctypes.c_double()
         self._check(lib().thorx_rt_totals(self.h, ctypes.byref(a), ctypes.byref(o)))
         return a.value, o.value
+
+    # ---- RT surrogate ----
+    def sur_create(self, hidden=512, train_batch=8192, log_capacity=0, recheck_period=16,
+                   tolerance=0.05, seed=1):
+        self._sp = SurrogateParamsC(hidden, train_batch, log_capacity, recheck_period, tolerance,
+                                    seed)
+        self._check(lib().thorx_surrogate_create(self.h, ctypes.byref(self._sp)))
+
+    def sur_mode(self, mode):
+        self._check(lib().thorx_surrogate_set_mode(self.h, mode))
+
+    def sur_logged(self):
+        n = lib().thorx_surrogate_logged(self.h)
+        if n < 0:
+            self._check(int(n))
+        return n
+
+    def sur_train(self, iterations, batch, lr=1e-3):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        self._check(lib().thorx_surrogate_train(self.h, iterations, batch, lr, ctypes.byref(a),
+                                                ctypes.byref(b)))
+        return a.value, b.value
+
+    def sur_stats(self):
+        out = (ctypes.c_uint * 4)()
+        self._check(lib().thorx_surrogate_stats(self.h, out))
+        return dict(rechecked=out[0], failed=out[1], max_err=out[2] * 1e-6, rt_columns=out[3])
+
+    def sur_layer(self, layer):
+        n, k = ctypes.c_int(), ctypes.c_int()
+        self._check(lib().thorx_surrogate_layer(self.h, layer, ctypes.byref(n), ctypes.byref(k),
+                                                None, None, 0))
+        W = np.zeros((n.value, k.value), dtype=np.float32)
+        b = np.zeros(n.value, dtype=np.float32)
+        self._check(lib().thorx_surrogate_layer(self.h, layer, None, None, W.ctypes.data,
+                                                b.ctypes.data, 0))
+        return W, b
+
+    def sur_set_layer(self, layer, W, b):
+        W = np.ascontiguousarray(W, dtype=np.float32)
+        b = np.ascontiguousarray(b, dtype=np.float32)
+        self._check(lib().thorx_surrogate_layer(self.h, layer, None, None, W.ctypes.data,
+                                                b.ctypes.data, 1))
+
+    def sur_grad(self, layer):
+        W, b = self.sur_layer(layer)
+        gW, gb = np.zeros_like(W), np.zeros_like(b)
+        self._check(lib().thorx_surrogate_layer_grad(self.h, layer, gW.ctypes.data,
+                                                     gb.ctypes.data))
+        return gW, gb
+
+    def sur_set_normalisation(self, in_mean, in_std, out_mean, out_std):
+        arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in (in_mean, in_std, out_mean,
+                                                                     out_std)]
+        self._check(lib().thorx_surrogate_normalisation(self.h, *[a.ctypes.data for a in arrs], 1))
+
+    def sur_normalisation(self, n_in, nv):
+        arrs = [np.zeros(n, dtype=np.float32) for n in (n_in, n_in, nv, nv)]
+        self._check(lib().thorx_surrogate_normalisation(self.h, *[a.ctypes.data for a in arrs], 0))
+        return arrs
+
+    def sur_forward(self, x, nv):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.zeros((x.shape[0], nv), dtype=np.float32)
+        self._check(lib().thorx_surrogate_forward_host(self.h, x.ctypes.data, x.shape[0],
+                                                       y.ctypes.data))
+        return y
+
+    def sur_gradients(self, x, t):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        loss = ctypes.c_double()
+        self._check(lib().thorx_surrogate_gradients_host(self.h, x.ctypes.data, t.ctypes.data,
+                                                         x.shape[0], ctypes.byref(loss)))
+        return loss.value
 
     def globdiag(self):
         """Global energy, mass, angular momentum (x, y, z) and entropy of the current state."""

@@ -11,7 +11,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libthorx.so")
 
-SOURCES = ["thorx_capi.cu", "dyn_fp64.cu", "rt.cu", "globdiag.cu", "icogrid.cpp"]
+SOURCES = ["thorx_capi.cu", "dyn_fp64.cu", "rt.cu", "globdiag.cu", "surrogate.cu", "icogrid.cpp"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC,-fopenmp", "-shared", "-lgomp",
               "-I" + os.path.join(ROOT, "include")]

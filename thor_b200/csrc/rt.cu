@@ -106,9 +106,11 @@ __device__ double source_func_lin(double bb, double bl, double bt, double tau, d
     return e1 + e2 * exp(-(tau / 2.0) / diff_ang);
 }
 
-// One thread per column: calc_zenith, then rtm_dual_band (profx_RT.h:316-587) with computetau,
-// radcsw (no surface, GravHeightVar excluded), radclw (reflecting lower boundary), the cooling
-// limiter and the coupling into profx_Qheat, and annual_insol.
+// One thread per column: calc_zenith, the top-of-atmosphere insolation and annual_insol, then
+// rtm_dual_band (profx_RT.h:316-587) with computetau, radcsw (no surface, GravHeightVar
+// excluded), radclw (reflecting lower boundary), the cooling limiter and the coupling into
+// profx_Qheat. The reference computes the insolation inside radcsw and the annual average after
+// the RT; both depend on the zenith angle only, so computing them first changes no value.
 __global__ void __launch_bounds__(128) rt_column_kernel(Geometry g, Phys P, RtConst c, RtFields f,
                                                        State s) {
     const int id = blockIdx.x * blockDim.x + threadIdx.x;
@@ -134,6 +136,15 @@ __global__ void __launch_bounds__(128) rt_column_kernel(Geometry g, Phys P, RtCo
         f.cos_zenith[id] = cz < 0.0 ? 0.0 : cz;
     }
     if (!st.run)
+        return;
+    const double coszrs = c.rt1Dmode ? 0.5 : f.cos_zenith[id];
+    // insolation at the top (radcsw, profx_RT.h:74; 0 on the night side) and its first-orbit
+    // average (annual_insol, profx_RT.h:30-37), for every column in either mode
+    f.insol[id]           = coszrs > 0.0 ? c.incflx * pow(st.r_orb, -2) * coszrs : 0.0;
+    const long long nstep = st.cur;
+    if (nstep * timestep < (2 * M_PI / c.mean_motion))
+        f.insol_ann[id] = f.insol_ann[id] * (nstep - 1) / nstep + f.insol[id] / nstep;
+    if (f.fallback && !(f.fallback[id] || id % f.period == (int)(nstep % f.period)))
         return;
     auto P_ = [&](int lev) { return s.p[lev * Np + id]; };
     auto R_ = [&](int lev) { return s.Rho[lev * Np + id]; };
@@ -170,7 +181,6 @@ __global__ void __launch_bounds__(128) rt_column_kernel(Geometry g, Phys P, RtCo
             H(f.thtemp, lev) = T_(lev - 1) * a + H(f.ttemp, lev) * b;
         }
     }
-    const double coszrs       = c.rt1Dmode ? 0.5 : f.cos_zenith[id];
     const double kappa_lw_lat = c.latf_lw ? c.kappa_lw + (c.kappa_lw_pole - c.kappa_lw) * pow(sin(lat), 2)
                                           : c.kappa_lw;
     // computetau (profx_RT.h:278-314)
@@ -184,8 +194,7 @@ __global__ void __launch_bounds__(128) rt_column_kernel(Geometry g, Phys P, RtCo
     for (int lev = 0; lev <= nv; lev++)
         H(f.fsw_dn, lev) = 0.0;
     if (coszrs > 0.0) { // radcsw (profx_RT.h:39-118)
-        const double tau = (c.kappa_sw / gravit) * (H(f.phtemp, nv));
-        f.insol[id]      = c.incflx * pow(st.r_orb, -2) * coszrs;
+        const double tau      = (c.kappa_sw / gravit) * (H(f.phtemp, nv));
         const double flux_top = f.insol[id] * (1.0 - c.albedo);
         H(f.fsw_dn, nv)       = flux_top * exp(-(1.0 / coszrs) * tau);
         for (int lev = nv; lev >= 1; lev--)
@@ -199,8 +208,6 @@ __global__ void __launch_bounds__(128) rt_column_kernel(Geometry g, Phys P, RtCo
                               / ((Alth[lev] - Alth[lev + 1]));
         }
     }
-    else
-        f.insol[id] = 0;
     const double rscale = P.DeepModel ? (A + Alth[nv]) / A : 1.0;
     f.ASR[id]           = H(f.fsw_dn, nv) * g.areasT[id] * pow(rscale, 2);
     for (int lev = 0; lev <= nv; lev++)
@@ -236,6 +243,8 @@ __global__ void __launch_bounds__(128) rt_column_kernel(Geometry g, Phys P, RtCo
                                 / ((Alth[lev] - Alth[lev + 1]));
     }
     f.OLR[id] = H(f.flw_up, nv) * g.areasT[id] * pow(rscale, 2);
+    if (f.fallback) // surrogate mode: the combine kernel limits and couples
+        return;
     // cooling limiter and coupling to the dynamical core (profx_RT.h:560-584)
     for (int lev = 0; lev < nv; lev++) {
         const int i = lev * Np + id;
@@ -246,10 +255,6 @@ __global__ void __launch_bounds__(128) rt_column_kernel(Geometry g, Phys P, RtCo
         f.qheat[i] = d;
         s.Qheat[i] += st.Qheat_scaling * d;
     }
-    // annual_insol (profx_RT.h:30-37; radiative_transfer.cu:1086-1100), first orbit only
-    const long long nstep = st.cur;
-    if (nstep * timestep < (2 * M_PI / c.mean_motion))
-        f.insol_ann[id] = f.insol_ann[id] * (nstep - 1) / nstep + f.insol[id] / nstep;
 }
 
 } // namespace

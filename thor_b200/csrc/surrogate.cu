@@ -1,0 +1,553 @@
+// RT surrogate: a per-column MLP that maps (T, log p per level, cos zenith) to the heating rates
+// of the double-gray RT, trained on the GPU from columns the plain RT produced, run inside the
+// physics step with the plain RT re-checking a rotating 1/period of the columns and taking over
+// wherever the surrogate's relative error exceeds a tolerance. No counterpart in the reference.
+//
+// Network: in = 2 nv + 1 features -> H -> H -> H -> nv, GELU after the hidden layers, BF16
+// weights and activations, FP32 accumulation (the tcgen05 GEMM of umma.cuh), FP32 master weights
+// with Adam. Every dimension is padded to the GEMM tile rules (batch to 128, in to a multiple of
+// 64, out to 64); padded weights, biases and their gradients are exactly zero and stay zero.
+// Features and targets are standardised per feature / per level with statistics of the logged
+// training data.
+//
+// Device layouts: batch-major, row = one column of the grid (or one training sample):
+//   X0 [B][Kin] bf16, Z_l [B][H] f32 (pre-activations), A_l [B][H] bf16, Y [B][Nout] f32.
+// Layer l: W [N][K] (f32 master, bf16 copy for the forward GEMM, bf16 transpose [K][N] for the
+// input-gradient GEMM), b [N].
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/thorx.h"
+#include "surrogate.h"
+#include "thorx_internal.h"
+#include "umma.cuh"
+
+namespace thorx {
+namespace {
+
+using bf16 = __nv_bfloat16;
+
+__device__ __forceinline__ uint64_t mix64(uint64_t z) { // SplitMix64 finaliser
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+__device__ __forceinline__ double uniform01(uint64_t seed, uint64_t i) {
+    return (double)(mix64(seed + 0x9E3779B97F4A7C15ull * (i + 1)) >> 11) * (1.0 / 9007199254740992.0);
+}
+
+// ---- parameters -----------------------------------------------------------------------------
+// W ~ U(-a, a), a = sqrt(6 / (fan_in + fan_out)) on the valid block, zero elsewhere; b = 0.
+__global__ void init_layer_kernel(float* W, float* b, int N, int K, int n_valid, int k_valid,
+                                  uint64_t seed) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < N * K) {
+        const int    n = i / K, k = i % K;
+        const double a = sqrt(6.0 / (double)(n_valid + k_valid));
+        W[i] = (n < n_valid && k < k_valid) ? (float)((2.0 * uniform01(seed, i) - 1.0) * a) : 0.0f;
+    }
+    if (i < N)
+        b[i] = 0.0f;
+}
+
+// bf16 copies of a layer: Wbf [N][K] and its transpose Wt [K][N].
+__global__ void cast_layer_kernel(const float* W, bf16* Wbf, bf16* Wt, int N, int K) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N * K)
+        return;
+    const int  n = i / K, k = i % K;
+    const bf16 v = __float2bfloat16_rn(W[i]);
+    Wbf[i]       = v;
+    Wt[(size_t)k * N + n] = v;
+}
+
+// Adam (Kingma & Ba 2015) on one tensor, bias-corrected with step t (c1 = 1 - b1^t, c2 = 1 - b2^t).
+__global__ void adam_kernel(float* w, float* m, float* v, const float* g, int n, float lr,
+                            float b1, float b2, float eps, float c1, float c2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.0f - b1) * gi;
+    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i]           = mi;
+    v[i]           = vi;
+    w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+// ---- batch assembly -------------------------------------------------------------------------
+// Standardised bf16 features of the grid columns at the physics step: T, log p per level, and
+// cos zenith; rows >= N and features >= n_in are zero.
+__global__ void features_state_kernel(SurNet net, Geometry g, State s, const double* cos_zenith,
+                                      bf16* X0, int Brows) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= Brows)
+        return;
+    const int nv = net.nv;
+    for (int j = 0; j < net.Kin; j++) {
+        float x = 0.0f;
+        if (r < g.N && j < net.n_in) {
+            double raw;
+            if (j < nv)
+                raw = s.T[(size_t)j * g.Np + r];
+            else if (j < 2 * nv)
+                raw = log(s.p[(size_t)(j - nv) * g.Np + r]);
+            else
+                raw = cos_zenith[r];
+            x = (float)((raw - net.in_mean[j]) / net.in_std[j]);
+        }
+        X0[(size_t)r * net.Kin + j] = __float2bfloat16_rn(x);
+    }
+}
+
+// Random training batch from the log: standardised bf16 features and f32 targets.
+__global__ void features_log_kernel(SurNet net, SurLog lg, long long nlogged, uint64_t seed,
+                                    bf16* X0, float* tgt, int B) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= B)
+        return;
+    const long long row = (long long)(uniform01(seed, r) * (double)nlogged) % nlogged;
+    const float*    x   = lg.X + (size_t)row * net.n_in;
+    const float*    y   = lg.Y + (size_t)row * net.nv;
+    for (int j = 0; j < net.Kin; j++) {
+        const float v = j < net.n_in ? (float)((x[j] - net.in_mean[j]) / net.in_std[j]) : 0.0f;
+        X0[(size_t)r * net.Kin + j] = __float2bfloat16_rn(v);
+    }
+    for (int j = 0; j < net.Nout; j++)
+        tgt[(size_t)r * net.Nout + j] =
+            j < net.nv ? (float)((y[j] - net.out_mean[j]) / net.out_std[j]) : 0.0f;
+}
+
+// Features and targets given on the host (tests), already standardised.
+__global__ void features_host_kernel(SurNet net, const float* x, const float* t, int B, bf16* X0,
+                                     float* tgt) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= B)
+        return;
+    for (int j = 0; j < net.Kin; j++)
+        X0[(size_t)r * net.Kin + j] =
+            __float2bfloat16_rn(j < net.n_in ? x[(size_t)r * net.n_in + j] : 0.0f);
+    if (t)
+        for (int j = 0; j < net.Nout; j++)
+            tgt[(size_t)r * net.Nout + j] = j < net.nv ? t[(size_t)r * net.nv + j] : 0.0f;
+}
+
+// MSE loss over the valid outputs of the first B rows: dY = 2 (Y - T) / (B nv) as f32 and bf16,
+// per-block partial losses into part[blockIdx.x] (summed in a fixed order on the host).
+__global__ void loss_grad_kernel(SurNet net, const float* Y, const float* tgt, int B, float* dYf,
+                                 bf16* dY, double* part) {
+    __shared__ double sh[256];
+    const int         i     = blockIdx.x * blockDim.x + threadIdx.x;
+    const int         total = B * net.Nout;
+    double            l     = 0.0;
+    if (i < total) {
+        const int   j  = i % net.Nout;
+        const float d  = (j < net.nv) ? Y[i] - tgt[i] : 0.0f;
+        const float gd = 2.0f * d / (float)(B * net.nv);
+        dYf[i]         = gd;
+        dY[i]          = __float2bfloat16_rn(gd);
+        l              = (double)d * d;
+    }
+    sh[threadIdx.x] = l;
+    __syncthreads();
+    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+        if (threadIdx.x < st)
+            sh[threadIdx.x] += sh[threadIdx.x + st];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        part[blockIdx.x] = sh[0];
+}
+
+// db[n] = sum over rows of G[r][n] (bias gradients), rows in a fixed order.
+template<class T> __global__ void colsum_kernel(const T* G, int B, int N, float* db) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N)
+        return;
+    float acc = 0.0f;
+    for (int r = 0; r < B; r++)
+        acc += (float)G[(size_t)r * N + n];
+    db[n] = acc;
+}
+
+// dst [C][ldd] = src [R][C]^T for bf16, 32 x 32 tiles through shared memory (R, C multiples of
+// 32); columns R..ldd-1 of the destination are left as they are.
+__global__ void transpose_bf16_kernel(const bf16* src, bf16* dst, int R, int C, int ldd) {
+    __shared__ bf16 t[32][33];
+    const int       r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+    for (int y = threadIdx.y; y < 32; y += blockDim.y)
+        t[y][threadIdx.x] = src[(size_t)(r0 + y) * C + c0 + threadIdx.x];
+    __syncthreads();
+    for (int y = threadIdx.y; y < 32; y += blockDim.y)
+        dst[(size_t)(c0 + y) * ldd + r0 + threadIdx.x] = t[threadIdx.x][y];
+}
+
+// ---- the physics step in surrogate mode -----------------------------------------------------
+// Per column: the surrogate's heating (de-standardised), or the plain RT's where the column was
+// re-checked this step or has fallen back; a re-checked column falls back (or returns to the
+// surrogate) according to its relative error max|Qs - Qrt| / max|Qrt|. Then the cooling limiter
+// and the coupling into profx_Qheat as the plain RT does (profx_RT.h:560-584).
+__global__ void combine_kernel(SurNet net, Geometry g, Phys P, State s, RtFields f, const float* Y,
+                               uint8_t* fallback, int period, double tol, unsigned int* stats) {
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= g.N)
+        return;
+    const RtStep st = *f.step;
+    if (!st.run)
+        return;
+    const int  nv = g.nv, Np = g.Np;
+    const bool recheck = id % period == (int)(st.cur % period);
+    const bool use_rt  = fallback[id] != 0 || recheck;
+    if (recheck) {
+        double num = 0.0, den = 0.0;
+        for (int lev = 0; lev < nv; lev++) {
+            const double qs =
+                (double)Y[(size_t)id * net.Nout + lev] * net.out_std[lev] + net.out_mean[lev];
+            const double qr = f.dtemp[(size_t)lev * Np + id];
+            num             = fmax(num, fabs(qs - qr));
+            den             = fmax(den, fabs(qr));
+        }
+        const double err = den > 0.0 ? num / den : (num > 0.0 ? 1.0e300 : 0.0);
+        fallback[id]     = err > tol ? 1 : 0;
+        atomicAdd(&stats[0], 1u); // columns re-checked
+        if (err > tol)
+            atomicAdd(&stats[1], 1u); // re-checks that failed
+        atomicMax(&stats[2], (unsigned)fmin(err * 1e6, 4.0e9)); // largest error, 1e-6 units
+    }
+    if (use_rt)
+        atomicAdd(&stats[3], 1u); // columns heated by the plain RT
+    for (int lev = 0; lev < nv; lev++) {
+        const int i = lev * Np + id;
+        double    d = use_rt ? f.dtemp[i]
+                             : (double)Y[(size_t)id * net.Nout + lev] * net.out_std[lev] + net.out_mean[lev];
+        if (s.p[i] + s.Rd[i] / (s.Cp[i] - s.Rd[i]) * d * P.timestep < 0)
+            d = -s.p[i] / P.timestep;
+        f.dtemp[i] = d;
+        f.qheat[i] = d;
+        s.Qheat[i] += st.Qheat_scaling * d;
+    }
+}
+
+// ---- logging of plain-RT columns for training -----------------------------------------------
+__global__ void log_reserve_kernel(SurLog lg, const RtStep* st, int N) {
+    if (!st->run) {
+        *lg.base = -1;
+        return;
+    }
+    *lg.base = *lg.count;
+    *lg.count += N;
+}
+
+__global__ void log_write_kernel(SurLog lg, SurNet net, Geometry g, State s, RtFields f) {
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= g.N)
+        return;
+    const long long base = *lg.base;
+    if (base < 0)
+        return;
+    const long long row = (base + id) % lg.cap;
+    float*          x   = lg.X + (size_t)row * net.n_in;
+    float*          y   = lg.Y + (size_t)row * net.nv;
+    for (int lev = 0; lev < net.nv; lev++) {
+        const size_t i  = (size_t)lev * g.Np + id;
+        x[lev]          = (float)s.T[i];
+        x[net.nv + lev] = (float)log(s.p[i]);
+        y[lev]          = (float)f.dtemp[i];
+    }
+    x[2 * net.nv] = (float)f.cos_zenith[id];
+}
+
+// Mean and standard deviation of column j of a [rows][ld] f32 table (one block per column).
+__global__ void stats_kernel(const float* X, long long rows, int ld, float* mean, float* stdv) {
+    __shared__ double s1[256], s2[256];
+    const int         j = blockIdx.x;
+    double            a = 0.0, b = 0.0;
+    for (long long r = threadIdx.x; r < rows; r += blockDim.x) {
+        const double v = X[(size_t)r * ld + j];
+        a += v;
+        b += v * v;
+    }
+    s1[threadIdx.x] = a;
+    s2[threadIdx.x] = b;
+    __syncthreads();
+    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+        if (threadIdx.x < st) {
+            s1[threadIdx.x] += s1[threadIdx.x + st];
+            s2[threadIdx.x] += s2[threadIdx.x + st];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double m  = s1[0] / (double)rows;
+        const double sd = sqrt(fmax(s2[0] / (double)rows - m * m, 0.0));
+        mean[j]         = (float)m;
+        stdv[j]         = (float)(sd > 0.0 ? sd : 1.0);
+    }
+}
+
+inline unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+} // namespace
+
+// ---- host side --------------------------------------------------------------------------------
+int Surrogate::init(int nv_, int hidden, long long log_capacity, int batch_rows, int ncols,
+                    uint64_t seed_) {
+    net.nv   = nv_;
+    net.n_in = 2 * nv_ + 1;
+    net.Kin  = ((net.n_in + 63) / 64) * 64;
+    net.H    = hidden;
+    net.Nout = ((nv_ + 63) / 64) * 64;
+    seed     = seed_;
+    Bcap     = ((batch_rows + 127) / 128) * 128;
+    const int Ns[4] = {net.H, net.H, net.H, net.Nout}, Ks[4] = {net.Kin, net.H, net.H, net.H};
+    const int nvalid[4] = {net.H, net.H, net.H, net.nv}, kvalid[4] = {net.n_in, net.H, net.H, net.H};
+    size_t    bytes = 0;
+    auto      alloc = [&](void** p, size_t n) -> bool {
+        if (cudaMalloc(p, n) != cudaSuccess)
+            return false;
+        allocs.push_back(*p);
+        bytes += n;
+        return cudaMemset(*p, 0, n) == cudaSuccess;
+    };
+    for (int l = 0; l < 4; l++) {
+        SurLayer& L = lay[l];
+        L.N         = Ns[l];
+        L.K         = Ks[l];
+        const size_t nw = (size_t)L.N * L.K;
+        // the weight-gradient GEMM's M is the layer's N, padded to 128 rows
+        const size_t ng = (size_t)std::max(L.N, 128) * L.K;
+        if (!alloc((void**)&L.W, nw * 4) || !alloc((void**)&L.b, L.N * 4)
+            || !alloc((void**)&L.mW, nw * 4) || !alloc((void**)&L.vW, nw * 4)
+            || !alloc((void**)&L.mb, L.N * 4) || !alloc((void**)&L.vb, L.N * 4)
+            || !alloc((void**)&L.gW, ng * 4) || !alloc((void**)&L.gb, L.N * 4)
+            || !alloc((void**)&L.Wbf, nw * 2) || !alloc((void**)&L.Wt, nw * 2))
+            return THORX_E_CUDA;
+        init_layer_kernel<<<nblk(nw, 256), 256>>>(L.W, L.b, L.N, L.K, nvalid[l], kvalid[l],
+                                                 seed + 7919ull * (l + 1));
+    }
+    if (!alloc((void**)&net.in_mean, net.Kin * 4) || !alloc((void**)&net.in_std, net.Kin * 4)
+        || !alloc((void**)&net.out_mean, net.Nout * 4) || !alloc((void**)&net.out_std, net.Nout * 4))
+        return THORX_E_CUDA;
+    {
+        std::vector<float> one(std::max(net.Kin, net.Nout), 1.0f);
+        cudaMemcpy(net.in_std, one.data(), net.Kin * 4, cudaMemcpyHostToDevice);
+        cudaMemcpy(net.out_std, one.data(), net.Nout * 4, cudaMemcpyHostToDevice);
+    }
+    const size_t B = Bcap;
+    if (!alloc((void**)&X0, B * net.Kin * 2) || !alloc((void**)&Y, B * net.Nout * 4)
+        || !alloc((void**)&tgt, B * net.Nout * 4) || !alloc((void**)&dYf, B * net.Nout * 4)
+        || !alloc((void**)&dY, B * net.Nout * 2) || !alloc((void**)&dZ[0], B * net.H * 2)
+        || !alloc((void**)&dZ[1], B * net.H * 2)
+        || !alloc((void**)&T1, (size_t)std::max(net.H, 128) * B * 2)
+        || !alloc((void**)&T2, (size_t)std::max(net.H, net.Kin) * B * 2)
+        || !alloc((void**)&lpart, nblk(B * net.Nout, 256) * 8) || !alloc((void**)&err, 4)
+        || !alloc((void**)&stats, 16))
+        return THORX_E_CUDA;
+    for (int l = 0; l < 3; l++)
+        if (!alloc((void**)&Z[l], B * net.H * 4) || !alloc((void**)&A[l], B * net.H * 2))
+            return THORX_E_CUDA;
+    log.cap = log_capacity;
+    if (log_capacity > 0)
+        if (!alloc((void**)&log.X, (size_t)log_capacity * net.n_in * 4)
+            || !alloc((void**)&log.Y, (size_t)log_capacity * net.nv * 4))
+            return THORX_E_CUDA;
+    if (!alloc((void**)&log.count, 8) || !alloc((void**)&log.base, 8)
+        || !alloc((void**)&fallback, (size_t)ncols))
+        return THORX_E_CUDA;
+    device_bytes = bytes;
+    cast_all(0);
+    return cudaDeviceSynchronize() == cudaSuccess ? 0 : THORX_E_CUDA;
+}
+
+void Surrogate::release() {
+    for (void* p : allocs)
+        cudaFree(p);
+    allocs.clear();
+}
+
+void Surrogate::cast_all(cudaStream_t st) {
+    for (int l = 0; l < 4; l++) {
+        SurLayer& L = lay[l];
+        cast_layer_kernel<<<nblk((long long)L.N * L.K, 256), 256, 0, st>>>(L.W, L.Wbf, L.Wt, L.N, L.K);
+    }
+}
+
+// Y = net(X0) for the first B rows (B a multiple of 128).
+void Surrogate::forward(int B, cudaStream_t st) {
+    for (int l = 0; l < 3; l++) {
+        const bf16*   in = l == 0 ? X0 : A[l - 1];
+        umma::EpiArgs e{nullptr, A[l], Z[l], nullptr, lay[l].b, net.H};
+        umma::gemm<256, umma::kEpiBiasGelu>(in, lay[l].Wbf, B, net.H, lay[l].K, e, err, st);
+    }
+    umma::EpiArgs e{Y, nullptr, nullptr, nullptr, lay[3].b, net.Nout};
+    umma::gemm<64, umma::kEpiBiasF32>(A[2], lay[3].Wbf, B, net.Nout, net.H, e, err, st);
+}
+
+// D[M x N] = A[M x K] . B[N x K]^T into f32, tile width chosen from N.
+void Surrogate::gemm_n(const bf16* Am, const bf16* Bm, int M, int N, int K, const umma::EpiArgs& e,
+                       cudaStream_t st) {
+    if (N % 256 == 0)
+        umma::gemm<256, umma::kEpiF32>(Am, Bm, M, N, K, e, err, st);
+    else if (N % 128 == 0)
+        umma::gemm<128, umma::kEpiF32>(Am, Bm, M, N, K, e, err, st);
+    else
+        umma::gemm<64, umma::kEpiF32>(Am, Bm, M, N, K, e, err, st);
+}
+void Surrogate::gemm_gelu_bwd(const bf16* Am, const bf16* Bm, int M, int N, int K,
+                              const umma::EpiArgs& e, cudaStream_t st) {
+    umma::gemm<256, umma::kEpiGeluBwdBf16>(Am, Bm, M, N, K, e, err, st);
+}
+
+// Gradients of the MSE loss for the first B rows (targets in tgt): fills gW, gb of every layer.
+void Surrogate::backward(int B, cudaStream_t st) {
+    const int H = net.H, Nout = net.Nout;
+    lpart_n     = nblk((long long)B * Nout, 256);
+    loss_grad_kernel<<<lpart_n, 256, 0, st>>>(net, Y, tgt, B, dYf, dY, lpart);
+    // output layer: gW4 = dY^T A3, gb4 = colsum dY, dZ3 = (dY W4) * gelu'(Z3)
+    colsum_kernel<float><<<nblk(Nout, 128), 128, 0, st>>>(dYf, B, Nout, lay[3].gb);
+    cudaMemsetAsync(T1, 0, (size_t)128 * B * 2, st); // dY^T padded to 128 rows
+    transpose_bf16_kernel<<<dim3(Nout / 32, B / 32), dim3(32, 8), 0, st>>>(dY, T1, B, Nout, B);
+    transpose_bf16_kernel<<<dim3(H / 32, B / 32), dim3(32, 8), 0, st>>>(A[2], T2, B, H, B);
+    {
+        umma::EpiArgs e{lay[3].gW, nullptr, nullptr, nullptr, nullptr, H};
+        gemm_n(T1, T2, 128, H, B, e, st);
+    }
+    {
+        umma::EpiArgs e{nullptr, dZ[0], nullptr, Z[2], nullptr, H};
+        gemm_gelu_bwd(dY, lay[3].Wt, B, H, Nout, e, st);
+    }
+    // hidden layers 3, 2, 1 (indices 2, 1, 0)
+    int cur = 0;
+    for (int l = 2; l >= 0; l--) {
+        const bf16* dz = dZ[cur];
+        colsum_kernel<bf16><<<nblk(H, 128), 128, 0, st>>>(dz, B, H, lay[l].gb);
+        transpose_bf16_kernel<<<dim3(H / 32, B / 32), dim3(32, 8), 0, st>>>(dz, T1, B, H, B);
+        const bf16* in  = l == 0 ? X0 : A[l - 1];
+        const int   Kin = lay[l].K;
+        transpose_bf16_kernel<<<dim3(Kin / 32, B / 32), dim3(32, 8), 0, st>>>(in, T2, B, Kin, B);
+        {
+            umma::EpiArgs e{lay[l].gW, nullptr, nullptr, nullptr, nullptr, Kin};
+            gemm_n(T1, T2, H, Kin, B, e, st);
+        }
+        if (l > 0) {
+            umma::EpiArgs e{nullptr, dZ[cur ^ 1], nullptr, Z[l - 1], nullptr, H};
+            gemm_gelu_bwd(dz, lay[l].Wt, B, H, H, e, st);
+            cur ^= 1;
+        }
+    }
+}
+
+void Surrogate::adam(float lr, cudaStream_t st) {
+    adam_t++;
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    const float c1 = 1.0f - powf(b1, (float)adam_t), c2 = 1.0f - powf(b2, (float)adam_t);
+    for (int l = 0; l < 4; l++) {
+        SurLayer& L  = lay[l];
+        const int nw = L.N * L.K;
+        adam_kernel<<<nblk(nw, 256), 256, 0, st>>>(L.W, L.mW, L.vW, L.gW, nw, lr, b1, b2, eps, c1, c2);
+        adam_kernel<<<nblk(L.N, 256), 256, 0, st>>>(L.b, L.mb, L.vb, L.gb, L.N, lr, b1, b2, eps, c1, c2);
+    }
+    cast_all(st);
+}
+
+void Surrogate::fit_normalisation(long long rows, cudaStream_t st) {
+    stats_kernel<<<net.n_in, 256, 0, st>>>(log.X, rows, net.n_in, net.in_mean, net.in_std);
+    stats_kernel<<<net.nv, 256, 0, st>>>(log.Y, rows, net.nv, net.out_mean, net.out_std);
+}
+
+void Surrogate::train_batch(long long nlogged, int B, float lr, cudaStream_t st) {
+    features_log_kernel<<<nblk(B, 128), 128, 0, st>>>(
+        net, log, nlogged, seed ^ (0xD1B54A32D192ED03ull * (uint64_t)(adam_t + 1)), X0, tgt, B);
+    forward(B, st);
+    backward(B, st);
+    adam(lr, st);
+}
+
+void Surrogate::load_host_batch(const float* dx, const float* dt, int B, cudaStream_t st) {
+    cudaMemsetAsync(X0, 0, (size_t)Bcap * net.Kin * 2, st);
+    cudaMemsetAsync(tgt, 0, (size_t)Bcap * net.Nout * 4, st);
+    features_host_kernel<<<nblk(B, 128), 128, 0, st>>>(net, dx, dt, B, X0, tgt);
+}
+
+void Surrogate::step_features(const Geometry& g, const State& s, const RtFields& f, cudaStream_t st) {
+    const int B = ((g.N + 127) / 128) * 128;
+    features_state_kernel<<<nblk(B, 128), 128, 0, st>>>(net, g, s, f.cos_zenith, X0, B);
+    forward(B, st);
+}
+
+void Surrogate::step_combine(const Geometry& g, const Phys& P, const State& s, const RtFields& f,
+                             cudaStream_t st) {
+    combine_kernel<<<nblk(g.N, 128), 128, 0, st>>>(net, g, P, s, f, Y, fallback, period, tol, stats);
+}
+
+void Surrogate::log_step(const Geometry& g, const State& s, const RtFields& f, cudaStream_t st) {
+    log_reserve_kernel<<<1, 1, 0, st>>>(log, f.step, g.N);
+    log_write_kernel<<<nblk(g.N, 128), 128, 0, st>>>(log, net, g, s, f);
+}
+
+} // namespace thorx
+
+// ---- context-free entry points -----------------------------------------------------------------
+namespace {
+thread_local std::string g_sur_err;
+int                      sur_fail(int code, const std::string& m) {
+    g_sur_err = m;
+    return code;
+}
+} // namespace
+
+extern "C" {
+
+const char* thorx_surrogate_last_error(void) { return g_sur_err.c_str(); }
+
+int thorx_bf16_gemm(const unsigned short* A, const unsigned short* B, int M, int N, int K, float* D) {
+    using namespace thorx;
+    if (!A || !B || !D || M <= 0 || N <= 0 || K <= 0)
+        return sur_fail(THORX_E_ARG, "thorx_bf16_gemm: null pointer or non-positive size");
+    if (M % umma::kM || K % umma::kKChunk || N % 64)
+        return sur_fail(THORX_E_ARG, "thorx_bf16_gemm: M must be a multiple of 128, N of 64, K of 64");
+    __nv_bfloat16 *dA = nullptr, *dB = nullptr;
+    float*         dD  = nullptr;
+    unsigned int*  err = nullptr;
+    cudaError_t    e   = cudaSuccess;
+    auto           ck  = [&](cudaError_t x) {
+        if (e == cudaSuccess)
+            e = x;
+    };
+    ck(cudaMalloc(&dA, (size_t)M * K * 2));
+    ck(cudaMalloc(&dB, (size_t)N * K * 2));
+    ck(cudaMalloc(&dD, (size_t)M * N * 4));
+    ck(cudaMalloc(&err, sizeof(unsigned int)));
+    if (e == cudaSuccess) {
+        ck(cudaMemcpy(dA, A, (size_t)M * K * 2, cudaMemcpyHostToDevice));
+        ck(cudaMemcpy(dB, B, (size_t)N * K * 2, cudaMemcpyHostToDevice));
+        ck(cudaMemset(err, 0, sizeof(unsigned int)));
+    }
+    if (e == cudaSuccess) {
+        umma::EpiArgs ea{dD, nullptr, nullptr, nullptr, nullptr, N};
+        if (N % 256 == 0)
+            umma::gemm<256, umma::kEpiF32>(dA, dB, M, N, K, ea, err, 0);
+        else if (N % 128 == 0)
+            umma::gemm<128, umma::kEpiF32>(dA, dB, M, N, K, ea, err, 0);
+        else
+            umma::gemm<64, umma::kEpiF32>(dA, dB, M, N, K, ea, err, 0);
+        ck(cudaGetLastError());
+        ck(cudaDeviceSynchronize());
+    }
+    unsigned int herr = 0;
+    if (e == cudaSuccess) {
+        ck(cudaMemcpy(D, dD, (size_t)M * N * 4, cudaMemcpyDeviceToHost));
+        ck(cudaMemcpy(&herr, err, sizeof(herr), cudaMemcpyDeviceToHost));
+    }
+    cudaFree(dA), cudaFree(dB), cudaFree(dD), cudaFree(err);
+    if (e != cudaSuccess)
+        return sur_fail(THORX_E_CUDA, std::string("thorx_bf16_gemm: ") + cudaGetErrorString(e));
+    if (herr)
+        return sur_fail(THORX_E_CUDA, "thorx_bf16_gemm: tensor-core wait timed out");
+    return 0;
+}
+
+} // extern "C"

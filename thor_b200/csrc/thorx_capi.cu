@@ -13,6 +13,7 @@
 //   update_rk2                UpdateRK2
 // with no host synchronisation inside a step; thorx_step replays the whole step as a CUDA graph.
 
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cmath>
@@ -25,6 +26,7 @@
 #include <cuda.h>
 
 #include "../../include/thorx.h"
+#include "surrogate.h"
 #include "thorx_internal.h"
 
 using namespace thorx;
@@ -50,6 +52,8 @@ struct thorx_ctx {
     double*                          staging     = nullptr; // layout conversion buffer
     size_t                           staging_len = 0;       // doubles
     bool                             rt_enabled  = false;   // double-gray RT in ProfX
+    Surrogate*                       sur         = nullptr; // RT surrogate (thorx_surrogate_create)
+    int                              sur_mode    = THORX_SUR_OFF;
     RtConst                          rt_c{};
     RtFields                         rt_f{};
     double2*                         gd_part     = nullptr; // global-sum partials (6 quantities)
@@ -232,10 +236,11 @@ int check_flags(thorx_ctx* ctx) {
 
 // Kernel classes of one step, for thorx_kernel_info / thorx_profile_steps.
 enum KClass { KProfx = 0, KAdvTemp, KDiffFirst, KDiffLast, KDivm0, KSlow, KMomentum, KVertical,
-              KUpdateRk2, KRt, KNumClasses };
+              KUpdateRk2, KRt, KSurrogate, KNumClasses };
 const char* const kClassName[KNumClasses] = {"profx", "adv_temp", "diffusion_first",
                                              "diffusion_last", "divm0", "slow_modes", "momentum",
-                                             "vertical", "update_rk2", "radiative_transfer"};
+                                             "vertical", "update_rk2", "radiative_transfer",
+                                             "rt_surrogate"};
 
 cudaEvent_t next_event(thorx_ctx* ctx) {
     if (ctx->event_next == ctx->event_pool.size()) {
@@ -300,6 +305,14 @@ double class_bytes(const thorx_ctx* ctx, int k) {
     case KRt: // p, Rho, T, Rd, Cp, Qheat, lat, lon, areasT, insol_ann | phtemp, thtemp, fsw/flw
               // up/down, tau (2), ttemp, dtemp, DG_Qheat, Qheat, insol, insol_ann, ASR, OLR, coszen
         return ctx->rt_enabled ? 6 * S + 4 * G + 6 * Si + 6 * S + 6 * G : 0;
+    case KSurrogate: // T, p, coszen | features; weights; dtemp (RT columns), Y | dtemp, DG_Qheat,
+                     // Qheat (bf16 activations between the layers stay in L2)
+        return (ctx->sur && ctx->sur_mode == THORX_SUR_USE)
+                   ? 2 * S + G + 2.0 * ctx->sur->net.Kin * N + 4.0 * ctx->sur->net.Nout * N
+                         + 2.0 * (ctx->sur->net.Kin + 2.0 * ctx->sur->net.H + ctx->sur->net.Nout)
+                               * ctx->sur->net.H
+                         + 5 * S
+                   : 0;
     }
     return 0;
 }
@@ -310,6 +323,7 @@ int class_launches(const thorx_ctx* ctx, int k) {
     switch (k) {
     case KProfx: return ctx->rt_enabled ? 2 : 1; // ProfX, then its pressure update after RT
     case KRt: return ctx->rt_enabled ? 1 : 0;     // one bracket: orbit kernel + column kernel
+    case KSurrogate: return (ctx->sur && ctx->sur_mode == THORX_SUR_USE) ? 1 : 0;
     case KAdvTemp: return 3;
     case KDiffFirst: return 3 * (passes - (passes > 0 ? 1 : 0));
     case KDiffLast: return passes > 0 ? 3 : 0;
@@ -334,9 +348,27 @@ int enqueue_profx(thorx_ctx* ctx) {
             KScope k(ctx, KProfx);
             launch_profx(ctx->g, ctx->P, ctx->s, false, ctx->stream);
         }
-        {
-            KScope k(ctx, KRt);
-            launch_rt(ctx->g, ctx->P, ctx->rt_c, ctx->rt_f, ctx->s, ctx->stream);
+        if (ctx->sur && ctx->sur_mode == THORX_SUR_USE) {
+            RtFields fm = ctx->rt_f; // plain RT only on re-checked and fallen-back columns
+            fm.fallback = ctx->sur->fallback;
+            fm.period   = ctx->sur->period;
+            {
+                KScope k(ctx, KRt);
+                launch_rt(ctx->g, ctx->P, ctx->rt_c, fm, ctx->s, ctx->stream);
+            }
+            {
+                KScope k(ctx, KSurrogate);
+                ctx->sur->step_features(ctx->g, ctx->s, fm, ctx->stream);
+                ctx->sur->step_combine(ctx->g, ctx->P, ctx->s, fm, ctx->stream);
+            }
+        }
+        else {
+            {
+                KScope k(ctx, KRt);
+                launch_rt(ctx->g, ctx->P, ctx->rt_c, ctx->rt_f, ctx->s, ctx->stream);
+            }
+            if (ctx->sur && ctx->sur_mode == THORX_SUR_LOG)
+                ctx->sur->log_step(ctx->g, ctx->s, ctx->rt_f, ctx->stream);
         }
         {
             KScope k(ctx, KProfx);
@@ -677,6 +709,10 @@ void thorx_destroy(thorx_ctx* ctx) {
         cudaStreamSynchronize(ctx->stream);
     for (cudaEvent_t e : ctx->event_pool)
         cudaEventDestroy(e);
+    if (ctx->sur) {
+        ctx->sur->release();
+        delete ctx->sur;
+    }
     for (void* p : ctx->allocs)
         cudaFree(p);
     if (ctx->flags_host)
@@ -865,7 +901,12 @@ int thorx_kernels_per_step(const thorx_ctx* ctx) {
     int n = 0;
     for (int k = 0; k < KNumClasses; k++)
         n += class_launches(ctx, k);
-    return n + (ctx->rt_enabled ? 1 : 0); // the RT bracket holds two kernels
+    n += ctx->rt_enabled ? 1 : 0; // the RT bracket holds two kernels
+    if (ctx->sur && ctx->sur_mode == THORX_SUR_USE)
+        n += 5; // features, four GEMMs and the combine in one bracket
+    if (ctx->sur && ctx->sur_mode == THORX_SUR_LOG)
+        n += 2; // log slot reservation and write
+    return n;
 }
 
 int thorx_kernel_classes(const thorx_ctx* ctx) { return ctx ? (int)KNumClasses : THORX_E_ARG; }
@@ -1030,6 +1071,280 @@ int thorx_rt_totals(thorx_ctx* ctx, double* asr, double* olr) {
     *asr = out[0];
     *olr = out[1];
     return 0;
+}
+
+// ---- RT surrogate ------------------------------------------------------------------------------
+namespace {
+int drop_graph(thorx_ctx* ctx) {
+    if (ctx->graph_exec) {
+        CK(cudaGraphExecDestroy(ctx->graph_exec));
+        ctx->graph_exec = nullptr;
+    }
+    if (ctx->graph) {
+        CK(cudaGraphDestroy(ctx->graph));
+        ctx->graph = nullptr;
+    }
+    return 0;
+}
+int sur_check(thorx_ctx* ctx, const char* fn) {
+    if (!ctx->sur)
+        return fail(ctx, THORX_E_STATE, std::string(fn) + ": no surrogate (thorx_surrogate_create)");
+    return 0;
+}
+int sur_err(thorx_ctx* ctx, const char* fn) {
+    unsigned int e = 0;
+    CK(cudaMemcpyAsync(&e, ctx->sur->err, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (e)
+        return fail(ctx, THORX_E_CUDA, std::string(fn) + ": tensor-core wait timed out");
+    return 0;
+}
+// Host rows -> a device copy the caller frees (test entry points only).
+int stage_host(thorx_ctx* ctx, const float* h, size_t n, float** d) {
+    CK(cudaMalloc(d, n * 4));
+    CK(cudaMemcpyAsync(*d, h, n * 4, cudaMemcpyHostToDevice, ctx->stream));
+    return 0;
+}
+} // namespace
+
+int thorx_surrogate_create(thorx_ctx* ctx, const thorx_surrogate_params* sp) {
+    if (!ctx)
+        return THORX_E_ARG;
+    if (!sp)
+        return fail(ctx, THORX_E_ARG, "thorx_surrogate_create: null argument");
+    if (ctx->sur)
+        return fail(ctx, THORX_E_STATE, "thorx_surrogate_create: already created");
+    if (sp->hidden < 256 || sp->hidden % 256 || sp->train_batch < 128 || sp->log_capacity < 0
+        || sp->recheck_period < 1 || !(sp->tolerance > 0))
+        return fail(ctx, THORX_E_ARG,
+                    "thorx_surrogate_create: hidden must be a positive multiple of 256, "
+                    "train_batch >= 128, log_capacity >= 0, recheck_period >= 1, tolerance > 0");
+    Surrogate* S   = new Surrogate;
+    S->period      = sp->recheck_period;
+    S->tol         = sp->tolerance;
+    const int rows = std::max(sp->train_batch, ctx->g.N);
+    const int rc   = S->init(ctx->g.nv, sp->hidden, sp->log_capacity, rows, ctx->g.N, sp->seed);
+    if (rc) {
+        S->release();
+        delete S;
+        return fail(ctx, THORX_E_CUDA, "thorx_surrogate_create: device allocation failed");
+    }
+    ctx->sur = S;
+    return 0;
+}
+
+int thorx_surrogate_set_mode(thorx_ctx* ctx, int mode) {
+    if (!ctx)
+        return THORX_E_ARG;
+    int rc;
+    if ((rc = sur_check(ctx, "thorx_surrogate_set_mode")))
+        return rc;
+    if (mode != THORX_SUR_OFF && mode != THORX_SUR_LOG && mode != THORX_SUR_USE)
+        return fail(ctx, THORX_E_ARG, "thorx_surrogate_set_mode: unknown mode");
+    if (mode != THORX_SUR_OFF && !ctx->rt_enabled)
+        return fail(ctx, THORX_E_STATE, "thorx_surrogate_set_mode: RT is not enabled");
+    if (mode == THORX_SUR_LOG && ctx->sur->log.cap == 0)
+        return fail(ctx, THORX_E_ARG, "thorx_surrogate_set_mode: log_capacity is 0");
+    if (mode == THORX_SUR_USE && !ctx->sur->norm_fitted)
+        return fail(ctx, THORX_E_STATE, "thorx_surrogate_set_mode: the surrogate is not trained");
+    if (mode == THORX_SUR_USE && mode != ctx->sur_mode)
+        CK(cudaMemsetAsync(ctx->sur->fallback, 0, ctx->g.N, ctx->stream));
+    if (mode != ctx->sur_mode && (rc = drop_graph(ctx)))
+        return rc;
+    ctx->sur_mode = mode;
+    return 0;
+}
+
+long long thorx_surrogate_logged(thorx_ctx* ctx) {
+    if (!ctx || !ctx->sur)
+        return THORX_E_ARG;
+    long long n = 0;
+    if (cudaMemcpyAsync(&n, ctx->sur->log.count, 8, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess
+        || cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+        return fail(ctx, THORX_E_CUDA, "thorx_surrogate_logged: copy failed");
+    return n;
+}
+
+int thorx_surrogate_train(thorx_ctx* ctx, int iterations, int batch, double lr, double* loss_first,
+                          double* loss_last) {
+    if (!ctx)
+        return THORX_E_ARG;
+    int rc;
+    if ((rc = sur_check(ctx, "thorx_surrogate_train")))
+        return rc;
+    Surrogate* S = ctx->sur;
+    if (iterations < 1 || batch < 128 || batch % 128 || batch > S->Bcap || !(lr > 0))
+        return fail(ctx, THORX_E_ARG, "thorx_surrogate_train: bad iterations, batch or lr");
+    const long long logged = thorx_surrogate_logged(ctx);
+    if (logged < batch)
+        return fail(ctx, THORX_E_STATE, "thorx_surrogate_train: fewer logged columns than a batch");
+    const long long nrows = std::min(logged, S->log.cap);
+    if (!S->norm_fitted) {
+        S->fit_normalisation(nrows, ctx->stream);
+        S->norm_fitted = true;
+    }
+    std::vector<double> part;
+    auto batch_loss = [&](double* out) -> int {
+        part.resize(S->lpart_n);
+        CK(cudaMemcpyAsync(part.data(), S->lpart, part.size() * 8, cudaMemcpyDeviceToHost,
+                           ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        double t = 0;
+        for (double v : part)
+            t += v;
+        *out = t / ((double)batch * S->net.nv);
+        return 0;
+    };
+    for (int it = 0; it < iterations; it++) {
+        S->train_batch(nrows, batch, (float)lr, ctx->stream);
+        CK(cudaGetLastError());
+        if (it == 0 && loss_first && (rc = batch_loss(loss_first)))
+            return rc;
+    }
+    if (loss_last && (rc = batch_loss(loss_last)))
+        return rc;
+    return sur_err(ctx, "thorx_surrogate_train");
+}
+
+int thorx_surrogate_stats(thorx_ctx* ctx, unsigned int* out) {
+    if (!ctx)
+        return THORX_E_ARG;
+    int rc;
+    if ((rc = sur_check(ctx, "thorx_surrogate_stats")))
+        return rc;
+    if (!out)
+        return fail(ctx, THORX_E_ARG, "thorx_surrogate_stats: null argument");
+    CK(cudaMemcpyAsync(out, ctx->sur->stats, 16, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemsetAsync(ctx->sur->stats, 0, 16, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+int thorx_surrogate_layer(thorx_ctx* ctx, int layer, int* N, int* K, float* W, float* b, int set) {
+    if (!ctx)
+        return THORX_E_ARG;
+    int rc;
+    if ((rc = sur_check(ctx, "thorx_surrogate_layer")))
+        return rc;
+    if (layer < 0 || layer > 3)
+        return fail(ctx, THORX_E_ARG, "thorx_surrogate_layer: layer out of range");
+    SurLayer& L = ctx->sur->lay[layer];
+    if (N)
+        *N = L.N;
+    if (K)
+        *K = L.K;
+    const size_t         nw   = (size_t)L.N * L.K;
+    const cudaMemcpyKind kind = set ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost;
+    if (W)
+        CK(cudaMemcpyAsync(set ? (void*)L.W : (void*)W, set ? (const void*)W : (const void*)L.W,
+                           nw * 4, kind, ctx->stream));
+    if (b)
+        CK(cudaMemcpyAsync(set ? (void*)L.b : (void*)b, set ? (const void*)b : (const void*)L.b,
+                           L.N * 4, kind, ctx->stream));
+    if (set)
+        ctx->sur->cast_all(ctx->stream);
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+int thorx_surrogate_layer_grad(thorx_ctx* ctx, int layer, float* gW, float* gb) {
+    if (!ctx)
+        return THORX_E_ARG;
+    int rc;
+    if ((rc = sur_check(ctx, "thorx_surrogate_layer_grad")))
+        return rc;
+    if (layer < 0 || layer > 3)
+        return fail(ctx, THORX_E_ARG, "thorx_surrogate_layer_grad: layer out of range");
+    SurLayer& L = ctx->sur->lay[layer];
+    if (gW)
+        CK(cudaMemcpyAsync(gW, L.gW, (size_t)L.N * L.K * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    if (gb)
+        CK(cudaMemcpyAsync(gb, L.gb, L.N * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+int thorx_surrogate_normalisation(thorx_ctx* ctx, float* in_mean, float* in_std, float* out_mean,
+                                  float* out_std, int set) {
+    if (!ctx)
+        return THORX_E_ARG;
+    int rc;
+    if ((rc = sur_check(ctx, "thorx_surrogate_normalisation")))
+        return rc;
+    if (!in_mean || !in_std || !out_mean || !out_std)
+        return fail(ctx, THORX_E_ARG, "thorx_surrogate_normalisation: null argument");
+    SurNet&              n    = ctx->sur->net;
+    const cudaMemcpyKind kind = set ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost;
+    struct Pair {
+        float* d;
+        float* h;
+        int    c;
+    } ps[] = {{n.in_mean, in_mean, n.n_in},
+              {n.in_std, in_std, n.n_in},
+              {n.out_mean, out_mean, n.nv},
+              {n.out_std, out_std, n.nv}};
+    for (auto& x : ps)
+        CK(cudaMemcpyAsync(set ? (void*)x.d : (void*)x.h, set ? (const void*)x.h : (const void*)x.d,
+                           (size_t)x.c * 4, kind, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (set)
+        ctx->sur->norm_fitted = true;
+    return 0;
+}
+
+int thorx_surrogate_forward_host(thorx_ctx* ctx, const float* x, int B, float* y) {
+    if (!ctx)
+        return THORX_E_ARG;
+    int rc;
+    if ((rc = sur_check(ctx, "thorx_surrogate_forward_host")))
+        return rc;
+    Surrogate* S = ctx->sur;
+    if (!x || !y || B < 1 || B > S->Bcap)
+        return fail(ctx, THORX_E_ARG, "thorx_surrogate_forward_host: bad arguments");
+    const int Bp = ((B + 127) / 128) * 128;
+    float*    dx = nullptr;
+    if ((rc = stage_host(ctx, x, (size_t)B * S->net.n_in, &dx)))
+        return rc;
+    S->load_host_batch(dx, nullptr, B, ctx->stream);
+    S->forward(Bp, ctx->stream);
+    std::vector<float> Y((size_t)Bp * S->net.Nout);
+    CK(cudaMemcpyAsync(Y.data(), S->Y, Y.size() * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    cudaFree(dx);
+    for (int r = 0; r < B; r++)
+        for (int j = 0; j < S->net.nv; j++)
+            y[(size_t)r * S->net.nv + j] = Y[(size_t)r * S->net.Nout + j];
+    return sur_err(ctx, "thorx_surrogate_forward_host");
+}
+
+int thorx_surrogate_gradients_host(thorx_ctx* ctx, const float* x, const float* t, int B,
+                                   double* loss) {
+    if (!ctx)
+        return THORX_E_ARG;
+    int rc;
+    if ((rc = sur_check(ctx, "thorx_surrogate_gradients_host")))
+        return rc;
+    Surrogate* S = ctx->sur;
+    if (!x || !t || B < 128 || B % 128 || B > S->Bcap)
+        return fail(ctx, THORX_E_ARG, "thorx_surrogate_gradients_host: B must be a multiple of 128");
+    float *dx = nullptr, *dt = nullptr;
+    if ((rc = stage_host(ctx, x, (size_t)B * S->net.n_in, &dx))
+        || (rc = stage_host(ctx, t, (size_t)B * S->net.nv, &dt)))
+        return rc;
+    S->load_host_batch(dx, dt, B, ctx->stream);
+    S->forward(B, ctx->stream);
+    S->backward(B, ctx->stream);
+    std::vector<double> part(S->lpart_n);
+    CK(cudaMemcpyAsync(part.data(), S->lpart, part.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    cudaFree(dx), cudaFree(dt);
+    if (loss) {
+        double sum = 0;
+        for (double v : part)
+            sum += v;
+        *loss = sum / ((double)B * S->net.nv);
+    }
+    return sur_err(ctx, "thorx_surrogate_gradients_host");
 }
 
 int thorx_globdiag(thorx_ctx* ctx, double* out) {

@@ -156,6 +156,12 @@ struct RtFields { // column-fastest device arrays (interfaces nv+1 planes, tau 2
     double *phtemp, *thtemp, *ttemp, *dtemp, *qheat, *tau, *fsw_up, *fsw_dn, *flw_up, *flw_dn;
     double *insol, *insol_ann, *ASR, *OLR, *cos_zenith;
     RtStep* step;
+    // Surrogate mode (fallback != nullptr): the RT runs only on the columns it re-checks this step
+    // (column % period == step % period) and on the columns that have fallen back to it
+    // (fallback[col] != 0), leaves dtemp unlimited and does not touch profx_Qheat: the surrogate's
+    // combine kernel chooses, limits and couples. nullptr: plain RT on every column.
+    const uint8_t* fallback;
+    int            period;
 };
 // Insolation::phy_loop + radiative_transfer::phy_loop (DualbandGray) of one physics step.
 void launch_rt(const Geometry& g, const Phys& P, const RtConst& c, const RtFields& f,
