@@ -192,7 +192,9 @@ const char* thorx_surrogate_last_error(void);
 
 /* ---- Learned RT surrogate. No counterpart in the reference. ----
  * A per-column MLP from (T per level, ln p per level, cos zenith) to the double-gray RT heating
- * rates per level (W m^-3, what rtm_dual_band adds to profx_Qheat): 2 nv + 1 inputs, three hidden
+ * rates per level as temperature tendencies dT/dt = Q / (rho c_v) in K/s (Q in W m^-3 is what
+ * rtm_dual_band adds to profx_Qheat; the surrogate's output is multiplied back by rho c_v before
+ * it is added), 2 nv + 1 inputs, three hidden
  * layers of `hidden` units with GELU, nv outputs; BF16 weights and activations, FP32
  * accumulation on the tensor cores, FP32 master weights trained with Adam on the GPU. Inputs and
  * outputs are standardised with the mean and standard deviation of the logged training data
@@ -203,7 +205,8 @@ const char* thorx_surrogate_last_error(void);
  *   THORX_SUR_USE  every physics step runs the surrogate on all columns and the plain RT only on
  *                  the columns it re-checks this step (column % recheck_period == step %
  *                  recheck_period) and on those that have fallen back: a re-checked column whose
- *                  relative error max|Q_sur - Q_rt| / max|Q_rt| exceeds `tolerance` falls back
+ *                  relative error max|q_sur - q_rt| / max|q_rt| (q in K/s, maxima over the
+ *                  column's levels) exceeds `tolerance` falls back
  *                  to the plain RT until a later re-check passes; re-checked columns use the
  *                  plain RT's heating. The cooling limiter and profx_Qheat coupling of the plain
  *                  RT apply to the chosen heating. ASR/OLR are current only on the columns the

@@ -84,3 +84,54 @@ def test_gradients_match_oracle():
             assert np.all(grads[l][0][:, 2 * NV + 1:] == 0.0)
         if l == 3:
             assert np.all(grads[l][0][NV:, :] == 0.0) and np.all(grads[l][1][NV:] == 0.0)
+
+
+@pytest.mark.gpu
+def test_training_on_logged_columns_and_in_step_use():
+    """Log the plain RT over 48 physics steps from a state S0, train on the GPU, then run the
+    first 16 of those steps again from S0 twice, with the plain RT and with the surrogate (the
+    states the surrogate sees are then of the kind it was trained on). Every column is
+    re-checked once per 16 steps, failed re-checks fall back to the plain RT, and the temperature
+    change over the 16 steps matches the plain RT's. The gain: the fraction of column-steps the
+    expensive RT still runs on."""
+    nlog, nuse = 48, 16
+    x, g = make_ctx(train_batch=2048, log_capacity=nlog * 2562, recheck_period=16,
+                    tolerance=0.05, seed=7)
+    N = g.point_num
+    fields = ["Rho", "pressure", "Mh", "Wh", "W", "temperature"]
+    x.step(4)  # leave the isothermal start
+    x.sync()
+    s0 = {f: x.get(f) for f in fields}
+    x.sur_mode(thor_b200.SUR_LOG)
+    x.step(nlog)
+    x.sync()
+    assert x.sur_logged() == nlog * N
+    first, last = x.sur_train(2000, 2048, lr=1e-3)
+
+    def run(mode):
+        for f, v in s0.items():
+            x.set(f, v)
+        x.sur_mode(mode)
+        x.sur_stats()
+        x.step(nuse)
+        x.sync()
+        return {f: x.get(f) for f in fields}, x.sur_stats()
+
+    plain, _ = run(thor_b200.SUR_OFF)
+    used, st = run(thor_b200.SUR_USE)
+    x.close(), g.close()
+    rt_fraction = st["rt_columns"] / (nuse * N)
+    dT_plain = plain["temperature"] - s0["temperature"]
+    dT_used = used["temperature"] - s0["temperature"]
+    change_err = np.max(np.abs(dT_used - dT_plain)) / np.max(np.abs(dT_plain))
+    print("surrogate: loss %.3g -> %.3g, stats %s, RT fraction %.3f, dT error %.3g"
+          % (first, last, st, rt_fraction, change_err))
+    assert last < 0.05 * first, (first, last)
+    assert st["rechecked"] == N, st  # each column exactly once in 16 steps
+    assert st["failed"] <= st["rechecked"]
+    for f in fields:
+        assert np.all(np.isfinite(used[f])), f
+    # surrogate columns are within the tolerance when re-checked; one that drifts out between
+    # two re-checks is caught at the next one
+    assert change_err < 0.2, change_err
+    assert rt_fraction < 0.5, (st, rt_fraction)

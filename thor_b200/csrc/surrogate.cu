@@ -1,7 +1,8 @@
 // RT surrogate: a per-column MLP that maps (T, log p per level, cos zenith) to the heating rates
-// of the double-gray RT, trained on the GPU from columns the plain RT produced, run inside the
-// physics step with the plain RT re-checking a rotating 1/period of the columns and taking over
-// wherever the surrogate's relative error exceeds a tolerance. No counterpart in the reference.
+// of the double-gray RT as temperature tendencies dT/dt = Q / (rho c_v) in K/s, trained on the
+// GPU from columns the plain RT produced, run inside the physics step with the plain RT
+// re-checking a rotating 1/period of the columns and taking over wherever the surrogate's
+// relative error exceeds a tolerance. No counterpart in the reference.
 //
 // Network: in = 2 nv + 1 features -> H -> H -> H -> nv, GELU after the hidden layers, BF16
 // weights and activations, FP32 accumulation (the tcgen05 GEMM of umma.cuh), FP32 master weights
@@ -201,12 +202,18 @@ __global__ void combine_kernel(SurNet net, Geometry g, Phys P, State s, RtFields
     const int  nv = g.nv, Np = g.Np;
     const bool recheck = id % period == (int)(st.cur % period);
     const bool use_rt  = fallback[id] != 0 || recheck;
+    // heating rates compared as temperature tendencies (K/s): the thin upper layers, whose
+    // W/m^3 are small, weigh as much as their temperature change does
+    auto rho_cv = [&](int lev) {
+        const size_t i = (size_t)lev * Np + id;
+        return s.Rho[i] * (s.Cp[i] - s.Rd[i]);
+    };
     if (recheck) {
         double num = 0.0, den = 0.0;
         for (int lev = 0; lev < nv; lev++) {
             const double qs =
                 (double)Y[(size_t)id * net.Nout + lev] * net.out_std[lev] + net.out_mean[lev];
-            const double qr = f.dtemp[(size_t)lev * Np + id];
+            const double qr = f.dtemp[(size_t)lev * Np + id] / rho_cv(lev);
             num             = fmax(num, fabs(qs - qr));
             den             = fmax(den, fabs(qr));
         }
@@ -222,7 +229,9 @@ __global__ void combine_kernel(SurNet net, Geometry g, Phys P, State s, RtFields
     for (int lev = 0; lev < nv; lev++) {
         const int i = lev * Np + id;
         double    d = use_rt ? f.dtemp[i]
-                             : (double)Y[(size_t)id * net.Nout + lev] * net.out_std[lev] + net.out_mean[lev];
+                             : ((double)Y[(size_t)id * net.Nout + lev] * net.out_std[lev]
+                                + net.out_mean[lev])
+                                   * rho_cv(lev);
         if (s.p[i] + s.Rd[i] / (s.Cp[i] - s.Rd[i]) * d * P.timestep < 0)
             d = -s.p[i] / P.timestep;
         f.dtemp[i] = d;
@@ -255,7 +264,7 @@ __global__ void log_write_kernel(SurLog lg, SurNet net, Geometry g, State s, RtF
         const size_t i  = (size_t)lev * g.Np + id;
         x[lev]          = (float)s.T[i];
         x[net.nv + lev] = (float)log(s.p[i]);
-        y[lev]          = (float)f.dtemp[i];
+        y[lev]          = (float)(f.dtemp[i] / (s.Rho[i] * (s.Cp[i] - s.Rd[i]))); // K/s
     }
     x[2 * net.nv] = (float)f.cos_zenith[id];
 }

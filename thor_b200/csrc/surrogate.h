@@ -15,7 +15,7 @@ struct SurNet { // shapes and standardisation, passed to kernels by value
     float *in_mean, *in_std, *out_mean, *out_std;
 };
 
-struct SurLog { // ring of logged plain-RT columns: X [cap][n_in] raw features, Y [cap][nv] W/m^3
+struct SurLog { // ring of logged plain-RT columns: X [cap][n_in] raw features, Y [cap][nv] K/s
     float*     X;
     float*     Y;
     long long  cap;
