@@ -505,45 +505,50 @@ __global__ void THORX_KATTR_ADV adv_temp_kernel(Geometry g, Phys P, State s) {
 // FV Laplacian around a ring of n neighbours (Diffusion_Op, src/headers/dyn/thor_diff.h:306-451;
 // the pole kernel :735-820 is the same sequence with a five-entry ring).
 // ---------------------------------------------------------------------------------------------
-template<int n>
-__device__ __forceinline__ double laplacian(const SGeo& G, const double* a, double a0,
-                                            double rscale) {
-    double lap = 0.0;
-    double lap1 = 0, lap2 = 0, lap3 = 0, lapx1 = 0, lapx2 = 0, lapy1 = 0, lapy2 = 0, lapz1 = 0,
-           lapz2 = 0, AT1 = 0;
+template<int n, class R>
+__device__ __forceinline__ R laplacian(const SGeo& G, const R* a, R a0, R rscale) {
+    auto AR = [&](int q) { return (R)G.AR(q); };
+    auto AT = [&](int q) { return (R)G.AT(q); };
+    auto TI = [&](int q) { return (R)G.TI(q); };
+    auto TE = [&](int q) { return (R)G.TE(q); };
+    auto OA = [&](int q) { return (R)G.OA(q); };
+    const R h = (R)0.5;
+    R       lap = 0;
+    R       lap1 = 0, lap2 = 0, lap3 = 0, lapx1 = 0, lapx2 = 0, lapy1 = 0, lapy2 = 0, lapz1 = 0,
+      lapz2 = 0, AT1 = 0;
 #pragma unroll
     for (int j = 0; j < n; j++) {
-        const int    jp1 = (j + 1) % n, jp2 = (j + 2) % n;
-        const double p1 = a[j], p2 = a[jp1], p3 = a[jp2];
-        const double vdiff = 0.5 * rscale;
-        double       astar;
+        const int jp1 = (j + 1) % n, jp2 = (j + 2) % n;
+        const R   p1 = a[j], p2 = a[jp1], p3 = a[jp2];
+        const R   vdiff = h * rscale;
+        R         astar;
         if (j == 0) {
-            AT1   = rscale / G.AT(j);
-            astar = (G.AR(j * 3 + 0) * a0 + G.AR(j * 3 + 1) * p1 + G.AR(j * 3 + 2) * p2) / G.AT(j);
-            lap1  = (0.5 * (p1 + a0) - astar);
-            lap2  = (0.5 * (p1 + p2) - astar);
-            lap3  = (0.5 * (a0 + p2) - astar);
+            AT1   = rscale / AT(j);
+            astar = (AR(j * 3 + 0) * a0 + AR(j * 3 + 1) * p1 + AR(j * 3 + 2) * p2) / AT(j);
+            lap1  = (h * (p1 + a0) - astar);
+            lap2  = (h * (p1 + p2) - astar);
+            lap3  = (h * (a0 + p2) - astar);
         }
-        const double AT2 = rscale / G.AT(jp1);
-        astar = (G.AR(jp1 * 3 + 0) * a0 + G.AR(jp1 * 3 + 1) * p2 + G.AR(jp1 * 3 + 2) * p3) / G.AT(jp1);
-        const double lap4 = (0.5 * (a0 + p2) - astar);
-        const double lap5 = (0.5 * (p2 + p3) - astar);
-        const double lap6 = (0.5 * (a0 + p3) - astar);
+        const R AT2 = rscale / AT(jp1);
+        astar = (AR(jp1 * 3 + 0) * a0 + AR(jp1 * 3 + 1) * p2 + AR(jp1 * 3 + 2) * p3) / AT(jp1);
+        const R lap4 = (h * (a0 + p2) - astar);
+        const R lap5 = (h * (p2 + p3) - astar);
+        const R lap6 = (h * (a0 + p3) - astar);
         if (j == 0) {
-            lapx1 = (-lap1 * G.TI(j * 3 + 0) + lap2 * G.TE(j * 3 + 0) + lap3 * G.TI(jp1 * 3 + 0)) * AT1;
-            lapy1 = (-lap1 * G.TI(j * 3 + 1) + lap2 * G.TE(j * 3 + 1) + lap3 * G.TI(jp1 * 3 + 1)) * AT1;
-            lapz1 = (-lap1 * G.TI(j * 3 + 2) + lap2 * G.TE(j * 3 + 2) + lap3 * G.TI(jp1 * 3 + 2)) * AT1;
+            lapx1 = (-lap1 * TI(j * 3 + 0) + lap2 * TE(j * 3 + 0) + lap3 * TI(jp1 * 3 + 0)) * AT1;
+            lapy1 = (-lap1 * TI(j * 3 + 1) + lap2 * TE(j * 3 + 1) + lap3 * TI(jp1 * 3 + 1)) * AT1;
+            lapz1 = (-lap1 * TI(j * 3 + 2) + lap2 * TE(j * 3 + 2) + lap3 * TI(jp1 * 3 + 2)) * AT1;
         }
         else {
             lapx1 = lapx2;
             lapy1 = lapy2;
             lapz1 = lapz2;
         }
-        lapx2 = (-lap4 * G.TI(jp1 * 3 + 0) + lap5 * G.TE(jp1 * 3 + 0) + lap6 * G.TI(jp2 * 3 + 0)) * AT2;
-        lapy2 = (-lap4 * G.TI(jp1 * 3 + 1) + lap5 * G.TE(jp1 * 3 + 1) + lap6 * G.TI(jp2 * 3 + 1)) * AT2;
-        lapz2 = (-lap4 * G.TI(jp1 * 3 + 2) + lap5 * G.TE(jp1 * 3 + 2) + lap6 * G.TI(jp2 * 3 + 2)) * AT2;
-        lap += ((lapx1 + lapx2) * G.OA(j * 3 + 0) + (lapy1 + lapy2) * G.OA(j * 3 + 1)
-                + (lapz1 + lapz2) * G.OA(j * 3 + 2))
+        lapx2 = (-lap4 * TI(jp1 * 3 + 0) + lap5 * TE(jp1 * 3 + 0) + lap6 * TI(jp2 * 3 + 0)) * AT2;
+        lapy2 = (-lap4 * TI(jp1 * 3 + 1) + lap5 * TE(jp1 * 3 + 1) + lap6 * TI(jp2 * 3 + 1)) * AT2;
+        lapz2 = (-lap4 * TI(jp1 * 3 + 2) + lap5 * TE(jp1 * 3 + 2) + lap6 * TI(jp2 * 3 + 2)) * AT2;
+        lap += ((lapx1 + lapx2) * OA(j * 3 + 0) + (lapy1 + lapy2) * OA(j * 3 + 1)
+                + (lapz1 + lapz2) * OA(j * 3 + 2))
                * vdiff;
     }
     return lap;
@@ -558,7 +563,7 @@ __device__ __forceinline__ double laplacian(const SGeo& G, const double* a, doub
 //   final pass (last)     : argument = diff (rho-weighted for v, w, T), scaled by -Kdh4 (-1)^(o/2)
 //                            -> diffrh, diffmh(3), diffw, diffpr
 // ---------------------------------------------------------------------------------------------
-template<int n>
+template<int n, class R>
 __device__ __forceinline__ void diffusion_point(const Geometry& g, const Phys& P, const State& s,
                                                 const SGeo& G, const double* fr, const int* ring,
                                                 const double* __restrict__ diff_in,
@@ -608,7 +613,16 @@ __device__ __forceinline__ void diffusion_point(const Geometry& g, const Phys& P
             }
             a[j] = v;
         }
-        double lap = laplacian<n>(G, a + 1, a[0], rscale);
+        double lap;
+        if (sizeof(R) < sizeof(double) && var >= 1 && var <= 4) { // v and w in the mixed form
+            R af[n + 1];
+#pragma unroll
+            for (int j = 0; j <= n; j++)
+                af[j] = (R)a[j];
+            lap = (double)laplacian<n, R>(G, af + 1, af[0], (R)rscale);
+        }
+        else
+            lap = laplacian<n, double>(G, a + 1, a[0], rscale);
         if (!last) {
             diff_out[(var * nv + lev) * Np + c] = lap;
             continue;
@@ -635,7 +649,7 @@ __device__ __forceinline__ void diffusion_point(const Geometry& g, const Phys& P
     }
 }
 
-template<int n>
+template<int n, class R>
 __device__ __forceinline__ void diffusion_body(const Geometry& g, const Phys& P, const State& s,
                                                const SGeo& G, const double* __restrict__ diff_in,
                                                double* __restrict__ diff_out, int stepnum,
@@ -648,9 +662,11 @@ __device__ __forceinline__ void diffusion_body(const Geometry& g, const Phys& P,
     for (int j = 0; j < 6; j++)
         ring[j] = g.ring[j * Np + c];
     for (int lev = threadIdx.y; lev < g.nv; lev += kLevGroups)
-        diffusion_point<n>(g, P, s, G, fr, ring, diff_in, diff_out, stepnum, last, c, lev);
+        diffusion_point<n, R>(g, P, s, G, fr, ring, diff_in, diff_out, stepnum, last, c, lev);
 }
 
+// R: compute type of the momentum and w Laplacians (double; float in the mixed form).
+template<class R>
 __global__ void THORX_KATTR_DIFF
     diffusion_kernel(Geometry g, Phys P, State s, const double* __restrict__ diff_in,
                      double* __restrict__ diff_out, int stepnum, bool last) {
@@ -661,9 +677,9 @@ __global__ void THORX_KATTR_DIFF
     if (c < 0)
         return;
     if (tail_cta())
-        diffusion_body<5>(g, P, s, G, diff_in, diff_out, stepnum, last, c);
+        diffusion_body<5, R>(g, P, s, G, diff_in, diff_out, stepnum, last, c);
     else
-        diffusion_body<6>(g, P, s, G, diff_in, diff_out, stepnum, last, c);
+        diffusion_body<6, R>(g, P, s, G, diff_in, diff_out, stepnum, last, c);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -672,25 +688,29 @@ __global__ void THORX_KATTR_DIFF
 // part of grad(div) of divg scaled by -Kdhz. The poles' corner mean of w uses the second
 // sub-area in place of the third (thor_div.h:443-454), restated as it is (c2 = 1).
 // ---------------------------------------------------------------------------------------------
-template<int n>
-__device__ __forceinline__ void divm_core(const SGeo& G, const double* a0, const double (*ar)[3],
-                                          bool with_w, double wl0, double wt0, const double* wl,
-                                          const double* wt, double dz, double rscale, int c2,
-                                          double* lapo) {
-    const double AT0 = 0.5 * rscale;
-    double       lapx = 0.0, lapy = 0.0, lapz = 0.0;
-    double       a01x = 0, a01y = 0, a01z = 0, a12x = 0, a12y = 0, a12z = 0, AT1 = 0, lap1 = 0,
-           lap2 = 0;
+template<int n, class R>
+__device__ __forceinline__ void divm_core(const SGeo& G, const R* a0, const R (*ar)[3], bool with_w,
+                                          R wl0, R wt0, const R* wl, const R* wt, R dz, R rscale,
+                                          int c2, R* lapo) {
+    auto    AR = [&](int q) { return (R)G.AR(q); };
+    auto    AT = [&](int q) { return (R)G.AT(q); };
+    auto    TI = [&](int q) { return (R)G.TI(q); };
+    auto    TE = [&](int q) { return (R)G.TE(q); };
+    auto    OA = [&](int q) { return (R)G.OA(q); };
+    const R h   = (R)0.5;
+    const R AT0 = h * rscale;
+    R       lapx = 0, lapy = 0, lapz = 0;
+    R       a01x = 0, a01y = 0, a01z = 0, a12x = 0, a12y = 0, a12z = 0, AT1 = 0, lap1 = 0, lap2 = 0;
 #pragma unroll
     for (int j = 0; j < n; j++) {
         const int     jp1 = (j + 1) % n, jp2 = (j + 2) % n;
-        const double *p1 = ar[j], *p2 = ar[jp1], *p3 = ar[jp2];
-        double        dwdz = 0.0, dwdz2 = 0.0;
+        const R *p1 = ar[j], *p2 = ar[jp1], *p3 = ar[jp2];
+        R        dwdz = 0, dwdz2 = 0;
         if (with_w) {
-            const double meanwl = (G.AR(j * 3 + 0) * wl0 + G.AR(j * 3 + 1) * wl[j] + G.AR(j * 3 + c2) * wl[jp1]) / G.AT(j);
-            const double meanwt = (G.AR(j * 3 + 0) * wt0 + G.AR(j * 3 + 1) * wt[j] + G.AR(j * 3 + c2) * wt[jp1]) / G.AT(j);
-            const double meanwl2 = (G.AR(jp1 * 3 + 0) * wl0 + G.AR(jp1 * 3 + 1) * wl[jp1] + G.AR(jp1 * 3 + c2) * wl[jp2]) / G.AT(jp1);
-            const double meanwt2 = (G.AR(jp1 * 3 + 0) * wt0 + G.AR(jp1 * 3 + 1) * wt[jp1] + G.AR(jp1 * 3 + c2) * wt[jp2]) / G.AT(jp1);
+            const R meanwl = (AR(j * 3 + 0) * wl0 + AR(j * 3 + 1) * wl[j] + AR(j * 3 + c2) * wl[jp1]) / AT(j);
+            const R meanwt = (AR(j * 3 + 0) * wt0 + AR(j * 3 + 1) * wt[j] + AR(j * 3 + c2) * wt[jp1]) / AT(j);
+            const R meanwl2 = (AR(jp1 * 3 + 0) * wl0 + AR(jp1 * 3 + 1) * wl[jp1] + AR(jp1 * 3 + c2) * wl[jp2]) / AT(jp1);
+            const R meanwt2 = (AR(jp1 * 3 + 0) * wt0 + AR(jp1 * 3 + 1) * wt[jp1] + AR(jp1 * 3 + c2) * wt[jp2]) / AT(jp1);
             dwdz  = (meanwl - meanwt) * dz;
             dwdz2 = (meanwl2 - meanwt2) * dz;
         }
@@ -701,33 +721,33 @@ __device__ __forceinline__ void divm_core(const SGeo& G, const double* a0, const
             a12x = (p1[0] + p2[0]);
             a12y = (p1[1] + p2[1]);
             a12z = (p1[2] + p2[2]);
-            AT1  = 0.5 * rscale / G.AT(j);
+            AT1  = h * rscale / AT(j);
         }
-        const double AT2  = 0.5 * rscale / G.AT(jp1);
-        const double a02x = (a0[0] + p2[0]), a02y = (a0[1] + p2[1]), a02z = (a0[2] + p2[2]);
-        const double a23x = (p2[0] + p3[0]), a23y = (p2[1] + p3[1]), a23z = (p2[2] + p3[2]);
-        const double a03x = (a0[0] + p3[0]), a03y = (a0[1] + p3[1]), a03z = (a0[2] + p3[2]);
+        const R AT2  = h * rscale / AT(jp1);
+        const R a02x = (a0[0] + p2[0]), a02y = (a0[1] + p2[1]), a02z = (a0[2] + p2[2]);
+        const R a23x = (p2[0] + p3[0]), a23y = (p2[1] + p3[1]), a23z = (p2[2] + p3[2]);
+        const R a03x = (a0[0] + p3[0]), a03y = (a0[1] + p3[1]), a03z = (a0[2] + p3[2]);
         if (j == 0)
-            lap1 = (-a01x * G.TI(j * 3 + 0) - a01y * G.TI(j * 3 + 1) - a01z * G.TI(j * 3 + 2)
-                    + a12x * G.TE(j * 3 + 0) + a12y * G.TE(j * 3 + 1) + a12z * G.TE(j * 3 + 2)
-                    + a02x * G.TI(jp1 * 3 + 0) + a02y * G.TI(jp1 * 3 + 1) + a02z * G.TI(jp1 * 3 + 2))
+            lap1 = (-a01x * TI(j * 3 + 0) - a01y * TI(j * 3 + 1) - a01z * TI(j * 3 + 2)
+                    + a12x * TE(j * 3 + 0) + a12y * TE(j * 3 + 1) + a12z * TE(j * 3 + 2)
+                    + a02x * TI(jp1 * 3 + 0) + a02y * TI(jp1 * 3 + 1) + a02z * TI(jp1 * 3 + 2))
                    * AT1;
         else
             lap1 = lap2;
-        lap2 = (-a02x * G.TI(jp1 * 3 + 0) - a02y * G.TI(jp1 * 3 + 1) - a02z * G.TI(jp1 * 3 + 2)
-                + a23x * G.TE(jp1 * 3 + 0) + a23y * G.TE(jp1 * 3 + 1) + a23z * G.TE(jp1 * 3 + 2)
-                + a03x * G.TI(jp2 * 3 + 0) + a03y * G.TI(jp2 * 3 + 1) + a03z * G.TI(jp2 * 3 + 2))
+        lap2 = (-a02x * TI(jp1 * 3 + 0) - a02y * TI(jp1 * 3 + 1) - a02z * TI(jp1 * 3 + 2)
+                + a23x * TE(jp1 * 3 + 0) + a23y * TE(jp1 * 3 + 1) + a23z * TE(jp1 * 3 + 2)
+                + a03x * TI(jp2 * 3 + 0) + a03y * TI(jp2 * 3 + 1) + a03z * TI(jp2 * 3 + 2))
                * AT2;
-        lapx += (lap1 + dwdz + lap2 + dwdz2) * G.OA(j * 3 + 0) * AT0;
-        lapy += (lap1 + dwdz + lap2 + dwdz2) * G.OA(j * 3 + 1) * AT0;
-        lapz += (lap1 + dwdz + lap2 + dwdz2) * G.OA(j * 3 + 2) * AT0;
+        lapx += (lap1 + dwdz + lap2 + dwdz2) * OA(j * 3 + 0) * AT0;
+        lapy += (lap1 + dwdz + lap2 + dwdz2) * OA(j * 3 + 1) * AT0;
+        lapz += (lap1 + dwdz + lap2 + dwdz2) * OA(j * 3 + 2) * AT0;
     }
     lapo[0] = lapx;
     lapo[1] = lapy;
     lapo[2] = lapz;
 }
 
-template<int n>
+template<int n, class R>
 __device__ __forceinline__ void divm0_point(const Geometry& g, const Phys& P, const SGeo& G,
                                             const int* ring, int c2, const double* __restrict__ Mh,
                                             const double* __restrict__ Wh,
@@ -735,28 +755,28 @@ __device__ __forceinline__ void divm0_point(const Geometry& g, const Phys& P, co
     const int    Np = g.Np, nv = g.nv;
     const double rscale = rscale_of(P, g, lev);
     const double dz     = 1.0 / (g.Altitudeh[lev] - g.Altitudeh[lev + 1]);
-    double       a0[3], ar[n][3], wl[n], wt[n];
+    R            a0[3], ar[n][3], wl[n], wt[n];
 #pragma unroll
     for (int k = 0; k < 3; k++)
-        a0[k] = Mh[(k * nv + lev) * Np + c];
+        a0[k] = (R)Mh[(k * nv + lev) * Np + c];
 #pragma unroll
     for (int j = 0; j < n; j++) {
 #pragma unroll
         for (int k = 0; k < 3; k++)
-            ar[j][k] = gz(Mh + (k * nv + lev) * Np, ring[j]);
-        wl[j] = gz(Wh + lev * Np, ring[j]);
-        wt[j] = gz(Wh + (lev + 1) * Np, ring[j]);
+            ar[j][k] = (R)gz(Mh + (k * nv + lev) * Np, ring[j]);
+        wl[j] = (R)gz(Wh + lev * Np, ring[j]);
+        wt[j] = (R)gz(Wh + (lev + 1) * Np, ring[j]);
     }
-    double out[3];
-    divm_core<n>(G, a0, ar, true, Wh[lev * Np + c], Wh[(lev + 1) * Np + c], wl, wt, dz, rscale, c2,
-                 out);
+    R out[3];
+    divm_core<n, R>(G, a0, ar, true, (R)Wh[lev * Np + c], (R)Wh[(lev + 1) * Np + c], wl, wt, (R)dz,
+                    (R)rscale, c2, out);
 #pragma unroll
     for (int k = 0; k < 3; k++)
-        divg[(k * nv + lev) * Np + c] = out[k];
+        divg[(k * nv + lev) * Np + c] = (double)out[k];
 }
 
 // Pass 0 of the divergence damping on (Mh, Wh) -> divg.
-template<int n>
+template<int n, class R>
 __device__ __forceinline__ void divm0_body(const Geometry& g, const Phys& P, const SGeo& G,
                                            const double* __restrict__ Mh,
                                            const double* __restrict__ Wh,
@@ -767,9 +787,10 @@ __device__ __forceinline__ void divm0_body(const Geometry& g, const Phys& P, con
         ring[j] = g.ring[j * Np + c];
     const int c2 = (g.cflag[c] & kPole) ? 1 : 2;
     for (int lev = threadIdx.y; lev < g.nv; lev += kLevGroups)
-        divm0_point<n>(g, P, G, ring, c2, Mh, Wh, divg, c, lev);
+        divm0_point<n, R>(g, P, G, ring, c2, Mh, Wh, divg, c, lev);
 }
 
+template<class R>
 __global__ void THORX_KATTR_DIVM
     divm0_kernel(Geometry g, Phys P, const double* __restrict__ Mh, const double* __restrict__ Wh,
                  double* __restrict__ divg) {
@@ -780,34 +801,35 @@ __global__ void THORX_KATTR_DIVM
     if (c < 0)
         return;
     if (tail_cta())
-        divm0_body<5>(g, P, G, Mh, Wh, divg, c);
+        divm0_body<5, R>(g, P, G, Mh, Wh, divg, c);
     else
-        divm0_body<6>(g, P, G, Mh, Wh, divg, c);
+        divm0_body<6, R>(g, P, G, Mh, Wh, divg, c);
 }
 
 // Pass 1 of the divergence damping at (column, level): DivM from divg.
-template<int n>
+template<int n, class R>
 __device__ __forceinline__ void divm_final(const Geometry& g, const Phys& P, const SGeo& G,
                                            const int* ring, const double* __restrict__ divg, int c,
-                                           int lev, const double* fr, double* DivM) {
+                                           int lev, const double* fr, R* DivM) {
     const int Np = g.Np, nv = g.nv;
-    double    a0[3], ar[n][3];
+    R         a0[3], ar[n][3];
 #pragma unroll
     for (int k = 0; k < 3; k++)
-        a0[k] = divg[(k * nv + lev) * Np + c];
+        a0[k] = (R)divg[(k * nv + lev) * Np + c];
 #pragma unroll
     for (int j = 0; j < n; j++)
 #pragma unroll
         for (int k = 0; k < 3; k++)
-            ar[j][k] = gz(divg + (k * nv + lev) * Np, ring[j]);
-    double lap[3];
-    divm_core<n>(G, a0, ar, false, 0, 0, nullptr, nullptr, 0, rscale_of(P, g, lev), 2, lap);
-    const double sdiff = g.Kdhz[lev];
-    const double lapr  = fr[0] * lap[0] + fr[1] * lap[1] + fr[2] * lap[2];
+            ar[j][k] = (R)gz(divg + (k * nv + lev) * Np, ring[j]);
+    R lap[3];
+    divm_core<n, R>(G, a0, ar, false, (R)0, (R)0, nullptr, nullptr, (R)0, (R)rscale_of(P, g, lev), 2,
+                    lap);
+    const R sdiff = (R)g.Kdhz[lev];
+    const R lapr  = (R)fr[0] * lap[0] + (R)fr[1] * lap[1] + (R)fr[2] * lap[2];
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-        const double l = lap[k] - fr[k] * lapr;
-        DivM[k]        = -l * sdiff;
+        const R l = lap[k] - (R)fr[k] * lapr;
+        DivM[k]   = -l * sdiff;
     }
 }
 
@@ -817,7 +839,7 @@ __device__ __forceinline__ void divm_final(const Geometry& g, const Phys& P, con
 // (src/headers/dyn/thor_auxiliary.h:311-418, without module arrays and without the never-read
 // Ws). DivM is consumed where it is produced and not stored.
 // ---------------------------------------------------------------------------------------------
-template<int n>
+template<int n, class R>
 __device__ __forceinline__ void slow_modes_body(const Geometry& g, const Phys& P, const State& s,
                                                 const SGeo& G, const double* sdiv,
                                                 const double* sgrad, bool update_rk, int c) {
@@ -837,9 +859,9 @@ __device__ __forceinline__ void slow_modes_body(const Geometry& g, const Phys& P
 
     for (int lev = threadIdx.y; lev < nv; lev += kLevGroups) {
         const int i       = lev * Np + c;
-        double    DivM[3] = {0.0, 0.0, 0.0};
+        R         DivM[3] = {0, 0, 0};
         if (P.DivDampP)
-            divm_final<n>(g, P, G, ring, s.divg, c, lev, fr, DivM);
+            divm_final<n, R>(g, P, G, ring, s.divg, c, lev, fr, DivM);
         const double Cv = s.Cp[i] - s.Rd[i];
         double       adv[3];
         for (int k = 0; k < 3; k++)
@@ -923,7 +945,7 @@ __device__ __forceinline__ void slow_modes_body(const Geometry& g, const Phys& P
         const double dpr   = nflxv[0] * fr[0] + nflxv[1] * fr[1] + nflxv[2] * fr[2];
         for (int k = 0; k < 3; k++) {
             const int j = (k * nv + lev) * Np + c;
-            s.SlowMh[j] = -(nflxv[k] - dpr * fr[k]) - adv[k] + DivM[k] + s.diffmh[j] + s.dMh[j];
+            s.SlowMh[j] = -(nflxv[k] - dpr * fr[k]) - adv[k] + (double)DivM[k] + s.diffmh[j] + s.dMh[j];
         }
         if (lev == 0) {
             s.SlowWh[c]           = 0.0;
@@ -985,6 +1007,7 @@ __device__ __forceinline__ void slow_modes_body(const Geometry& g, const Phys& P
     }
 }
 
+template<class R>
 __global__ void THORX_KATTR_SLOW
     slow_modes_kernel(Geometry g, Phys P, State s, bool update_rk) {
     __shared__ double sgeo[kRingGeoRows * kTile];
@@ -1000,16 +1023,16 @@ __global__ void THORX_KATTR_SLOW
     if (c < 0)
         return;
     if (tail_cta())
-        slow_modes_body<5>(g, P, s, G, sdiv, sgrad, update_rk, c);
+        slow_modes_body<5, R>(g, P, s, G, sdiv, sgrad, update_rk, c);
     else
-        slow_modes_body<6>(g, P, s, G, sdiv, sgrad, update_rk, c);
+        slow_modes_body<6, R>(g, P, s, G, sdiv, sgrad, update_rk, c);
 }
 
 // ---------------------------------------------------------------------------------------------
 // Small step, horizontal momentum: divergence-damping pass 1 on the deviations (Mhs, Whs) +
 // Momentum_Eq / _Poles (src/headers/dyn/thor_fastmodes.h:54-253).
 // ---------------------------------------------------------------------------------------------
-template<int n>
+template<int n, class R>
 __device__ __forceinline__ void momentum_body(const Geometry& g, const Phys& P, const State& s,
                                               const SGeo& G, const double* sgrad, double dt,
                                               int c) {
@@ -1025,9 +1048,9 @@ __device__ __forceinline__ void momentum_body(const Geometry& g, const Phys& P, 
     for (int k = 0; k < 3; k++)
         fr[k] = g.func_r[k * Np + c];
     for (int lev = threadIdx.y; lev < nv; lev += kLevGroups) {
-        double DivM[3] = {0.0, 0.0, 0.0};
+        R DivM[3] = {0, 0, 0};
         if (P.DivDampP)
-            divm_final<n>(g, P, G, ring, s.divg, c, lev, fr, DivM);
+            divm_final<n, R>(g, P, G, ring, s.divg, c, lev, fr, DivM);
         const double rscale = rscale_of(P, g, lev);
         double       pv[7];
 #pragma unroll
@@ -1041,7 +1064,7 @@ __device__ __forceinline__ void momentum_body(const Geometry& g, const Phys& P, 
             for (int j = 1; j < 7; j++)
                 sg = sg + sgrad[(j * 3 + k) * kTile + x] * pv[j];
             const double nflxv = rscale * sg;
-            Mv[k]              = (-nflxv + s.SlowMh[(k * nv + lev) * Np + c] + DivM[k]) * dt;
+            Mv[k]              = (-nflxv + s.SlowMh[(k * nv + lev) * Np + c] + (double)DivM[k]) * dt;
         }
         const double vr = Mv[0] * fr[0] + Mv[1] * fr[1] + Mv[2] * fr[2];
         for (int k = 0; k < 3; k++) {
@@ -1051,6 +1074,7 @@ __device__ __forceinline__ void momentum_body(const Geometry& g, const Phys& P, 
     }
 }
 
+template<class R>
 __global__ void THORX_KATTR_MOM
     momentum_kernel(Geometry g, Phys P, State s, double dt) {
     __shared__ double sgeo[kRingGeoRows * kTile];
@@ -1064,9 +1088,9 @@ __global__ void THORX_KATTR_MOM
     if (c < 0)
         return;
     if (tail_cta())
-        momentum_body<5>(g, P, s, G, sgrad, dt, c);
+        momentum_body<5, R>(g, P, s, G, sgrad, dt, c);
     else
-        momentum_body<6>(g, P, s, G, sgrad, dt, c);
+        momentum_body<6, R>(g, P, s, G, sgrad, dt, c);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1476,20 +1500,33 @@ void launch_diffusion(const Geometry& g, const Phys& P, const State& s, int step
     const size_t  plane6 = (size_t)6 * g.nv * g.Np;
     const double* in     = s.diff + ((stepnum + 1) % 2) * plane6;
     double*       out    = s.diff + (stepnum % 2) * plane6;
-    diffusion_kernel<<<tile_grid_tail(g), tile_block(), 0, st>>>(g, P, s, in, out, stepnum, last);
+    if (P.mixed)
+        diffusion_kernel<float><<<tile_grid_tail(g), tile_block(), 0, st>>>(g, P, s, in, out, stepnum, last);
+    else
+        diffusion_kernel<double><<<tile_grid_tail(g), tile_block(), 0, st>>>(g, P, s, in, out, stepnum, last);
 }
 void launch_divm0(const Geometry& g, const Phys& P, const State& s, bool small_step,
                   cudaStream_t st) {
-    divm0_kernel<<<tile_grid_tail(g), tile_block(), 0, st>>>(g, P, small_step ? s.Mhs : s.Mhk,
+    if (P.mixed)
+        divm0_kernel<float><<<tile_grid_tail(g), tile_block(), 0, st>>>(g, P, small_step ? s.Mhs : s.Mhk,
+                                                        small_step ? s.Whs : s.Whk, s.divg);
+    else
+        divm0_kernel<double><<<tile_grid_tail(g), tile_block(), 0, st>>>(g, P, small_step ? s.Mhs : s.Mhk,
                                                         small_step ? s.Whs : s.Whk, s.divg);
 }
 void launch_slow_modes(const Geometry& g, const Phys& P, const State& s, bool update_rk,
                        cudaStream_t st) {
-    slow_modes_kernel<<<tile_grid_tail(g), tile_block(), 0, st>>>(g, P, s, update_rk);
+    if (P.mixed)
+        slow_modes_kernel<float><<<tile_grid_tail(g), tile_block(), 0, st>>>(g, P, s, update_rk);
+    else
+        slow_modes_kernel<double><<<tile_grid_tail(g), tile_block(), 0, st>>>(g, P, s, update_rk);
 }
 void launch_momentum(const Geometry& g, const Phys& P, const State& s, double dt,
                      cudaStream_t st) {
-    momentum_kernel<<<tile_grid_tail(g), tile_block(), 0, st>>>(g, P, s, dt);
+    if (P.mixed)
+        momentum_kernel<float><<<tile_grid_tail(g), tile_block(), 0, st>>>(g, P, s, dt);
+    else
+        momentum_kernel<double><<<tile_grid_tail(g), tile_block(), 0, st>>>(g, P, s, dt);
 }
 size_t vertical_smem_bytes(const Geometry& g) { return sizeof(double) * kTile * (21 + 2 * g.nv); }
 void launch_vertical(const Geometry& g, const Phys& P, const State& s, double dt,

@@ -534,8 +534,8 @@ int thorx_create(const thorx_grid* gr, const thorx_params* pr, void* stream, tho
         return fail(ctx, THORX_E_UNSUPPORTED, "nv above the supported maximum");
     if (pr->HyDiffOrder < 2 || pr->HyDiffOrder % 2)
         return fail(ctx, THORX_E_UNSUPPORTED, "HyDiffOrder must be even and >= 2");
-    if (pr->precision != THORX_FP64)
-        return fail(ctx, THORX_E_UNSUPPORTED, "precision: this build runs THORX_FP64 only");
+    if (pr->precision != THORX_FP64 && pr->precision != THORX_MIXED)
+        return fail(ctx, THORX_E_ARG, "precision: THORX_FP64 or THORX_MIXED");
     if (pr->thermo_equation != THORX_ENTROPY && pr->thermo_equation != THORX_ENERGY)
         return fail(ctx, THORX_E_ARG, "thermo_equation");
     if (pr->core_benchmark != THORX_NO_BENCHMARK && pr->core_benchmark != THORX_HELD_SUAREZ)
@@ -573,6 +573,7 @@ int thorx_create(const thorx_grid* gr, const thorx_params* pr, void* stream, tho
     P.DivDampP        = pr->DivDampP != 0;
     P.energy          = pr->thermo_equation == THORX_ENERGY;
     P.held_suarez     = pr->core_benchmark == THORX_HELD_SUAREZ;
+    P.mixed           = pr->precision == THORX_MIXED;
 
     int rc;
     if ((rc = build_neighbours(ctx, gr)))

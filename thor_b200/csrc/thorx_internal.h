@@ -87,6 +87,7 @@ struct Phys {
     double A, Omega, Gravit, Rd, Cp, P_Ref, timestep;
     int    HyDiffOrder;
     bool   DeepModel, NonHydro, GravHeightVar, HyDiff, DivDampP, energy, held_suarez;
+    bool   mixed; // momentum-side horizontal stencils computed in FP32 (THORX_MIXED)
 };
 
 // Prognostic state (start of large step "x", RK stage "xk", small-step deviation "xs"),
