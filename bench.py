@@ -269,6 +269,93 @@ def reference_cuda(grid, args):
 METRIC = "sim-days/wall-hour at glevel6 L48, mixed+surrogate vs plain FP64; HBM GB/s"
 
 
+def time_steps(x, stream, precision, nsteps):
+    """ms per large step of a context in the given precision form (graph replays, CUDA events)."""
+    import torch
+    x.set_precision(precision)
+    x.step(3)
+    x.sync()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    x.step(nsteps)
+    e1.record(stream)
+    e1.synchronize()
+    x.sync()
+    return e0.elapsed_time(e1) / nsteps
+
+
+# Hot Jupiter with double-gray RT (the RT configuration): R = 1e8 m, g = 10, Rd = 3714,
+# Cp = 13000, surface 100 bar, top at 1e-3 bar, dt = 300 s, synchronous rotation with the
+# substellar point at longitude 0, gray opacities 4e-4 (SW) and 1e-3 (LW) m^2/kg, irradiation
+# temperature 2000 K (Tstar 4300 K, R* = 0.667 R_sun, a = R* (Tstar / T_irr)^2). Initial state:
+# isothermal at T_eq = T_irr / sqrt(2) (the Guillot-profile initialiser is not built) with seeded
+# +-1 K noise; the model top is the altitude of 1e-3 bar in that isothermal column.
+RT_GLEVEL, RT_NV, RT_DT = 5, 40, 300.0
+RT_TIRR, RT_TSTAR, RT_RSTAR = 2000.0, 4300.0, 0.667 * 695700000.0
+
+
+def rt_params_planet():
+    teq = RT_TIRR / 2 ** 0.5
+    top = 3714.0 * teq / 10.0 * np.log(1e7 / 1e2)
+    p = dict(A=1e8, Omega=9.09e-5, Gravit=10.0, Rd=3714.0, Cp=13000.0, P_Ref=1e7, Top_altitude=top,
+             timestep=RT_DT, Diffc=0.015, DivDampc=0.015, HyDiffOrder=4, DeepModel=1, NonHydro=1,
+             GravHeightVar=0, HyDiff=1, DivDampP=1, thermo_equation=0, core_benchmark=0,
+             precision=0)
+    rt = dict(Tstar=RT_TSTAR, radius_star=RT_RSTAR,
+              planet_star_dist=RT_RSTAR * (RT_TSTAR / RT_TIRR) ** 2, diff_ang=0.5, Tint=100.0,
+              albedo=0.0, kappa_sw=4e-4, kappa_lw=1e-3, kappa_lw_pole=1e-3, n_sw=1.0, n_lw=2.0,
+              f_lw=0.5, sync_rot=1, alpha_i=0.0)
+    return p, rt, teq
+
+
+def rt_surrogate_leg(torch, thor_b200, nlog=64, iters=1500, batch=8192, nsteps=20):
+    """Plain FP64 + RT against mixed + trained surrogate RT on the RT configuration (g5/L40):
+    time the plain form, log the plain RT, train the surrogate on the GPU, time the other form."""
+    try:
+        p, rt, teq = rt_params_planet()
+        grid = thor_b200.Icogrid(RT_GLEVEL, RT_NV, A=p["A"], Top_altitude=p["Top_altitude"])
+        stream = torch.cuda.Stream()
+        x = thor_b200.Thorx(grid.as_dict(), RT_GLEVEL, p, stream=stream.cuda_stream)
+        x.init_rest_state(teq, SEED, 1.0)
+        x.rt_enable(rt)
+        x.sur_create(hidden=512, train_batch=batch, log_capacity=nlog * grid.point_num,
+                     recheck_period=16, tolerance=0.05, seed=SEED)
+        ms_plain = time_steps(x, stream, thor_b200.FP64, nsteps)
+        kms_plain = dict(zip([t[0] for t in x.kernel_table()], x.profile_steps(1)))
+        x.sur_mode(thor_b200.SUR_LOG)
+        x.step(nlog)
+        x.sync()
+        t0 = time.perf_counter()
+        first, last = x.sur_train(iters, batch, lr=1e-3)
+        torch.cuda.synchronize()
+        train_s = time.perf_counter() - t0
+        x.sur_mode(thor_b200.SUR_USE)
+        x.sur_stats()
+        ms_sur = time_steps(x, stream, thor_b200.MIXED, nsteps)
+        st = x.sur_stats()
+        kms_sur = dict(zip([t[0] for t in x.kernel_table()], x.profile_steps(1)))
+        x.close()
+        N = grid.point_num
+        return {"workload": "hot Jupiter double-gray RT g%d/L%d dt=%g (%d columns), isothermal "
+                            "%.0f K start" % (RT_GLEVEL, RT_NV, RT_DT, N, teq),
+                "plain_fp64": {"ms_per_step": ms_plain,
+                               "value": sim_days_per_hour(1, ms_plain / 1000.0, dt=RT_DT)},
+                "mixed_surrogate": {"ms_per_step": ms_sur,
+                                    "value": sim_days_per_hour(1, ms_sur / 1000.0, dt=RT_DT)},
+                "ratio": ms_plain / ms_sur,
+                "rt_ms_per_step": {"plain": kms_plain.get("radiative_transfer", 0.0),
+                                   "surrogate_mode_rt": kms_sur.get("radiative_transfer", 0.0),
+                                   "surrogate_mode_net": kms_sur.get("rt_surrogate", 0.0)},
+                "training": {"columns_logged": nlog * N, "iterations": iters, "batch": batch,
+                             "lr": 1e-3, "loss_first": first, "loss_last": last,
+                             "seconds": train_s},
+                "recheck": {"steps": nsteps + 3, "rechecked": st["rechecked"],
+                            "failed": st["failed"], "max_rel_err": st["max_err"],
+                            "rt_column_fraction": st["rt_columns"] / ((nsteps + 3) * N)}}
+    except Exception as e:  # a side measurement never breaks the bench line
+        return {"unavailable": "%s" % e}
+
+
 def run_ours(args):
     import torch
     import thor_b200
@@ -375,6 +462,16 @@ def run_ours(args):
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
             "gpu_launches": x.kernels_per_step() * args.steps,
             "state_finite": bool(finite)}
+    if world == 1 and not args.no_extras:
+        # the mixed-precision form of the same context, same workload, after the measurements above
+        ms_mixed = time_steps(x, stream, thor_b200.MIXED, max(5, min(args.steps, 50)))
+        line["mixed_form"] = {"ms_per_step": ms_mixed,
+                              "value": sim_days_per_hour(1, ms_mixed / 1000.0),
+                              "ratio_vs_fp64": ms_step / ms_mixed,
+                              "what": "THORX_MIXED: FP32 momentum-side stencils, FP64 mass, "
+                                      "pressure, vertical solve and sums; same state, same graph "
+                                      "timing"}
+        line["rt_surrogate"] = rt_surrogate_leg(torch, thor_b200)
     x.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -392,6 +489,8 @@ def main():
     ap.add_argument("--form", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the mixed-form and RT/surrogate side measurements")
     ap.add_argument("--glevel", type=int, default=GLEVEL,
                     help="grid level (default 6; smaller cases are for profiling captures)")
     ap.add_argument("--nv", type=int, default=NV, help="vertical levels (default 48)")

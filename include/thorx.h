@@ -115,6 +115,10 @@ int thorx_get_field(thorx_ctx* ctx, const char* name, double* host);
  * Rd and Cp uniform. noise_amp = 0 gives the reference's noise-free rest state. */
 int thorx_init_rest_state(thorx_ctx* ctx, double Tmean, unsigned long long seed, double noise_amp);
 
+/* Switches the precision form (THORX_FP64 / THORX_MIXED) between steps; the state and everything
+ * else of the context carry over (both forms store FP64). A captured step graph is re-captured. */
+int thorx_set_precision(thorx_ctx* ctx, int precision);
+
 /* One physics step, ESP::ProfX (src/ESP/profx_driver.cu:70-474): W from Wh, T and potential
  * temperature from p and rho, Held-Suarez forcing when core_benchmark says so, p = rho Rd T,
  * and the NaN check (reported at the next synchronising call as THORX_E_NAN). */

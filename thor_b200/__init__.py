@@ -129,6 +129,8 @@ def lib():
         L.thorx_device_sum_noalloc.argtypes = [vp, ctypes.c_longlong, vp,
                                                ctypes.POINTER(ctypes.c_double)]
         L.thorx_device_sum_noalloc.restype = ci
+        L.thorx_set_precision.argtypes = [vp, ci]
+        L.thorx_set_precision.restype = ci
         L.thorx_bf16_gemm.argtypes = [vp, vp, ci, ci, ci, vp]
         L.thorx_bf16_gemm.restype = ci
         L.thorx_surrogate_last_error.restype = cp
@@ -166,7 +168,7 @@ EXPORTED = ["thorx_create", "thorx_destroy", "thorx_last_error", "thorx_field_si
             "thorx_grid_get", "thorx_grid_describe", "thorx_grid_free", "thorx_init_rest_state",
             "thorx_kernel_classes", "thorx_kernel_info", "thorx_profile_steps", "thorx_globdiag",
             "thorx_device_sum", "thorx_device_sum_noalloc", "thorx_rt_enable",
-            "thorx_rt_totals", "thorx_bf16_gemm", "thorx_surrogate_last_error",
+            "thorx_rt_totals", "thorx_set_precision", "thorx_bf16_gemm", "thorx_surrogate_last_error",
             "thorx_surrogate_create", "thorx_surrogate_set_mode", "thorx_surrogate_logged",
             "thorx_surrogate_train", "thorx_surrogate_stats", "thorx_surrogate_layer",
             "thorx_surrogate_layer_grad", "thorx_surrogate_normalisation",
@@ -360,6 +362,9 @@ class Thorx:
         a, o = ctypes.c_double(), ctypes.c_double()
         self._check(lib().thorx_rt_totals(self.h, ctypes.byref(a), ctypes.byref(o)))
         return a.value, o.value
+
+    def set_precision(self, precision):
+        self._check(lib().thorx_set_precision(self.h, precision))
 
     # ---- RT surrogate ----
     def sur_create(self, hidden=512, train_batch=8192, log_capacity=0, recheck_period=16,

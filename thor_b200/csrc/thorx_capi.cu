@@ -1074,6 +1074,26 @@ int thorx_rt_totals(thorx_ctx* ctx, double* asr, double* olr) {
     return 0;
 }
 
+int thorx_set_precision(thorx_ctx* ctx, int precision) {
+    if (!ctx)
+        return THORX_E_ARG;
+    if (precision != THORX_FP64 && precision != THORX_MIXED)
+        return fail(ctx, THORX_E_ARG, "thorx_set_precision: THORX_FP64 or THORX_MIXED");
+    const bool mixed = precision == THORX_MIXED;
+    if (mixed != ctx->P.mixed) {
+        if (ctx->graph_exec) {
+            CK(cudaGraphExecDestroy(ctx->graph_exec));
+            ctx->graph_exec = nullptr;
+        }
+        if (ctx->graph) {
+            CK(cudaGraphDestroy(ctx->graph));
+            ctx->graph = nullptr;
+        }
+        ctx->P.mixed = mixed;
+    }
+    return 0;
+}
+
 // ---- RT surrogate ------------------------------------------------------------------------------
 namespace {
 int drop_graph(thorx_ctx* ctx) {
