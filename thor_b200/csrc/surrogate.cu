@@ -163,15 +163,47 @@ __global__ void loss_grad_kernel(SurNet net, const float* Y, const float* tgt, i
         part[blockIdx.x] = sh[0];
 }
 
-// db[n] = sum over rows of G[r][n] (bias gradients), rows in a fixed order.
-template<class T> __global__ void colsum_kernel(const T* G, int B, int N, float* db) {
+// Column sums of G [B][N] (bias gradients) in two passes with a fixed order: block (32 columns
+// x 8 row lanes) of row chunk blockIdx.y writes part[blockIdx.y][n]; colsum_final adds the chunks.
+constexpr int kColsumChunks = 64;
+template<class T> __global__ void colsum_kernel(const T* G, int B, int N, float* part) {
+    __shared__ float sh[8][33];
+    const int        n = blockIdx.x * 32 + threadIdx.x;
+    const int        rows = (B + kColsumChunks - 1) / kColsumChunks;
+    const int        r0 = blockIdx.y * rows, r1 = min(B, r0 + rows);
+    float            acc = 0.0f;
+    if (n < N)
+        for (int r = r0 + threadIdx.y; r < r1; r += 8)
+            acc += (float)G[(size_t)r * N + n];
+    sh[threadIdx.y][threadIdx.x] = acc;
+    __syncthreads();
+    if (threadIdx.y == 0 && n < N) {
+        float t = 0.0f;
+        for (int y = 0; y < 8; y++)
+            t += sh[y][threadIdx.x];
+        part[(size_t)blockIdx.y * N + n] = t;
+    }
+}
+__global__ void colsum_final_kernel(const float* part, int N, float* db) {
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= N)
         return;
-    float acc = 0.0f;
-    for (int r = 0; r < B; r++)
-        acc += (float)G[(size_t)r * N + n];
-    db[n] = acc;
+    float t = 0.0f;
+    for (int z = 0; z < kColsumChunks; z++)
+        t += part[(size_t)z * N + n];
+    db[n] = t;
+}
+
+// out[i] = sum over z of part[z * stride + i] (split-K partial products), z in order.
+__global__ void splitk_reduce_kernel(const float* part, int splits, size_t stride, size_t n,
+                                     float* out) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    float t = 0.0f;
+    for (int z = 0; z < splits; z++)
+        t += part[(size_t)z * stride + i];
+    out[i] = t;
 }
 
 // dst [C][ldd] = src [R][C]^T for bf16, 32 x 32 tiles through shared memory (R, C multiples of
@@ -353,6 +385,9 @@ int Surrogate::init(int nv_, int hidden, long long log_capacity, int batch_rows,
         || !alloc((void**)&T1, (size_t)std::max(net.H, 128) * B * 2)
         || !alloc((void**)&T2, (size_t)std::max(net.H, net.Kin) * B * 2)
         || !alloc((void**)&lpart, nblk(B * net.Nout, 256) * 8) || !alloc((void**)&err, 4)
+        || !alloc((void**)&splitk, (size_t)kMaxSplits * std::max(net.H, 128)
+                                       * std::max(net.H, net.Kin) * 4)
+        || !alloc((void**)&colpart, (size_t)kColsumChunks * std::max(net.H, net.Nout) * 4)
         || !alloc((void**)&stats, 16))
         return THORX_E_CUDA;
     for (int l = 0; l < 3; l++)
@@ -405,6 +440,35 @@ void Surrogate::gemm_n(const bf16* Am, const bf16* Bm, int M, int N, int K, cons
     else
         umma::gemm<64, umma::kEpiF32>(Am, Bm, M, N, K, e, err, st);
 }
+// Weight gradient D[M x N] = A[M x K] . B[N x K]^T with K = the batch, split over CTAs in
+// partial products (so that the few 128 x N tiles of a layer fill the GPU) and reduced in order.
+void Surrogate::gemm_wgrad(const bf16* Am, const bf16* Bm, int M, int N, int K, float* out,
+                           cudaStream_t st) {
+    int splits = 1;
+    while (splits < kMaxSplits && K % (2 * splits * umma::kKChunk) == 0
+           && K / (2 * splits) >= 2 * umma::kKChunk)
+        splits *= 2;
+    const size_t  stride = (size_t)M * N;
+    umma::EpiArgs e{splitk, nullptr, nullptr, nullptr, nullptr, N, stride};
+    if (N % 256 == 0)
+        umma::gemm<256, umma::kEpiF32>(Am, Bm, M, N, K, e, err, st, splits);
+    else if (N % 128 == 0)
+        umma::gemm<128, umma::kEpiF32>(Am, Bm, M, N, K, e, err, st, splits);
+    else
+        umma::gemm<64, umma::kEpiF32>(Am, Bm, M, N, K, e, err, st, splits);
+    splitk_reduce_kernel<<<nblk((long long)stride, 256), 256, 0, st>>>(splitk, splits, stride,
+                                                                      stride, out);
+}
+
+void Surrogate::colsum(const float* G, int B, int N, float* db, cudaStream_t st) {
+    colsum_kernel<float><<<dim3(nblk(N, 32), kColsumChunks), dim3(32, 8), 0, st>>>(G, B, N, colpart);
+    colsum_final_kernel<<<nblk(N, 128), 128, 0, st>>>(colpart, N, db);
+}
+void Surrogate::colsum(const bf16* G, int B, int N, float* db, cudaStream_t st) {
+    colsum_kernel<bf16><<<dim3(nblk(N, 32), kColsumChunks), dim3(32, 8), 0, st>>>(G, B, N, colpart);
+    colsum_final_kernel<<<nblk(N, 128), 128, 0, st>>>(colpart, N, db);
+}
+
 void Surrogate::gemm_gelu_bwd(const bf16* Am, const bf16* Bm, int M, int N, int K,
                               const umma::EpiArgs& e, cudaStream_t st) {
     umma::gemm<256, umma::kEpiGeluBwdBf16>(Am, Bm, M, N, K, e, err, st);
@@ -416,13 +480,12 @@ void Surrogate::backward(int B, cudaStream_t st) {
     lpart_n     = nblk((long long)B * Nout, 256);
     loss_grad_kernel<<<lpart_n, 256, 0, st>>>(net, Y, tgt, B, dYf, dY, lpart);
     // output layer: gW4 = dY^T A3, gb4 = colsum dY, dZ3 = (dY W4) * gelu'(Z3)
-    colsum_kernel<float><<<nblk(Nout, 128), 128, 0, st>>>(dYf, B, Nout, lay[3].gb);
+    colsum(dYf, B, Nout, lay[3].gb, st);
     cudaMemsetAsync(T1, 0, (size_t)128 * B * 2, st); // dY^T padded to 128 rows
     transpose_bf16_kernel<<<dim3(Nout / 32, B / 32), dim3(32, 8), 0, st>>>(dY, T1, B, Nout, B);
     transpose_bf16_kernel<<<dim3(H / 32, B / 32), dim3(32, 8), 0, st>>>(A[2], T2, B, H, B);
     {
-        umma::EpiArgs e{lay[3].gW, nullptr, nullptr, nullptr, nullptr, H};
-        gemm_n(T1, T2, 128, H, B, e, st);
+        gemm_wgrad(T1, T2, 128, H, B, lay[3].gW, st);
     }
     {
         umma::EpiArgs e{nullptr, dZ[0], nullptr, Z[2], nullptr, H};
@@ -432,14 +495,13 @@ void Surrogate::backward(int B, cudaStream_t st) {
     int cur = 0;
     for (int l = 2; l >= 0; l--) {
         const bf16* dz = dZ[cur];
-        colsum_kernel<bf16><<<nblk(H, 128), 128, 0, st>>>(dz, B, H, lay[l].gb);
+        colsum(dz, B, H, lay[l].gb, st);
         transpose_bf16_kernel<<<dim3(H / 32, B / 32), dim3(32, 8), 0, st>>>(dz, T1, B, H, B);
         const bf16* in  = l == 0 ? X0 : A[l - 1];
         const int   Kin = lay[l].K;
         transpose_bf16_kernel<<<dim3(Kin / 32, B / 32), dim3(32, 8), 0, st>>>(in, T2, B, Kin, B);
         {
-            umma::EpiArgs e{lay[l].gW, nullptr, nullptr, nullptr, nullptr, Kin};
-            gemm_n(T1, T2, H, Kin, B, e, st);
+            gemm_wgrad(T1, T2, H, Kin, B, lay[l].gW, st);
         }
         if (l > 0) {
             umma::EpiArgs e{nullptr, dZ[cur ^ 1], nullptr, Z[l - 1], nullptr, H};

@@ -47,6 +47,9 @@ struct Surrogate {
     __nv_bfloat16*     dZ[2]{};
     float *            Y = nullptr, *tgt = nullptr, *dYf = nullptr;
     float*             Z[3]{};
+    float*             splitk   = nullptr; // split-K partial weight gradients
+    float*             colpart  = nullptr; // column-sum partials
+    static constexpr int kMaxSplits = 32;
     double*            lpart    = nullptr;
     int                lpart_n  = 0;
     unsigned int*      err      = nullptr;
@@ -68,6 +71,10 @@ struct Surrogate {
     void log_step(const Geometry& g, const State& s, const RtFields& f, cudaStream_t st);
     void gemm_n(const __nv_bfloat16* A, const __nv_bfloat16* B, int M, int N, int K,
                 const umma::EpiArgs& e, cudaStream_t st);
+    void gemm_wgrad(const __nv_bfloat16* A, const __nv_bfloat16* B, int M, int N, int K,
+                    float* out, cudaStream_t st);
+    void colsum(const float* G, int B, int N, float* db, cudaStream_t st);
+    void colsum(const __nv_bfloat16* G, int B, int N, float* db, cudaStream_t st);
     void gemm_gelu_bwd(const __nv_bfloat16* A, const __nv_bfloat16* B, int M, int N, int K,
                        const umma::EpiArgs& e, cudaStream_t st);
 };

@@ -3,15 +3,16 @@
 //   D[M x N] = A[M x K] . B[N x K]^T      A, B bf16, row-major (K contiguous, "K-major"),
 //                                         FP32 accumulation in tensor memory (TMEM)
 //
-// One CTA of 128 threads computes a 128 x BN tile of D. Per 64-wide K chunk, the four warps copy
-// the A and B tiles from global memory into shared memory in the canonical no-swizzle K-major
-// layout of the tensor core (8-row x 16-byte core matrices: element (r, k) at byte
-// (r/8)*1024 + (k/8)*128 + (r%8)*16 + (k%8)*2, i.e. leading-byte offset 128 between the core
-// matrices along K and stride-byte offset 1024 between 8-row groups), then one thread issues four
-// tcgen05.mma (K = 16 each) into the TMEM accumulator and commits them to an mbarrier that the
-// CTA waits on (bounded) before reusing the tiles. The epilogue reads the accumulator back with
-// tcgen05.ld (warp w owns TMEM lanes 32w..32w+31 = rows 32w.. of the tile) and applies a fused
-// element-wise operation before storing.
+// One CTA of 128 threads computes a 128 x BN tile of D. K is consumed in 64-wide chunks through
+// a ring of 3-4 shared-memory slots: the four warps copy the A and B tiles of a chunk from global
+// memory with 16-byte cp.async into the canonical no-swizzle K-major layout of the tensor core
+// (8-row x 16-byte core matrices: element (r, k) at byte (r/8)*1024 + (k/8)*128 + (r%8)*16 +
+// (k%8)*2, i.e. leading-byte offset 128 between the core matrices along K and stride-byte offset
+// 1024 between 8-row groups), one thread issues four tcgen05.mma (K = 16 each) into the TMEM
+// accumulator and commits them to the slot's mbarrier; a slot is refilled (S-1 chunks ahead)
+// once the bounded wait on that mbarrier shows its MMAs done, so copies overlap the MMAs. The
+// epilogue reads the accumulator back with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31 = rows
+// 32w.. of the tile) and applies a fused element-wise operation before storing.
 //
 // Descriptor formats (shared-memory matrix descriptor, instruction descriptor for kind::f16)
 // follow the PTX ISA for tcgen05; field positions as in CUTLASS's cute/arch/mma_sm100_desc.hpp.
@@ -46,7 +47,8 @@ struct EpiArgs {
     float*         out_z;
     const float*   z_in;
     const float*   bias;
-    int            ldo; // leading dimension of the outputs (elements)
+    int            ldo;     // leading dimension of the outputs (elements)
+    size_t         zstride; // split-K: elements between the partial outputs of consecutive splits
 };
 
 __device__ __forceinline__ float gelu(float z) {
@@ -158,62 +160,95 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
         v[i] = __uint_as_float(r[i]);
 }
 
-// Copies a rows x 64 bf16 block (row stride ld elements) into the canonical K-major layout.
-__device__ __forceinline__ void stage_kmajor(uint8_t* dst, const __nv_bfloat16* __restrict__ src,
-                                             int rows, int ld) {
+// Starts the copy of a rows x 64 bf16 block (row stride ld elements) into the canonical K-major
+// layout with 16-byte cp.async (no register staging); completion via cp.async.wait_group.
+__device__ __forceinline__ void stage_kmajor_async(uint8_t* dst, const __nv_bfloat16* __restrict__ src,
+                                                   int rows, int ld) {
     for (int v = threadIdx.x; v < rows * 8; v += kThreads) {
-        const int   r = v >> 3, kv = v & 7;
-        const uint4 x = *reinterpret_cast<const uint4*>(src + (size_t)r * ld + kv * 8);
-        *reinterpret_cast<uint4*>(dst + (r >> 3) * 1024 + kv * 128 + (r & 7) * 16) = x;
+        const int r = v >> 3, kv = v & 7;
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                         smem_u32(dst + (r >> 3) * 1024 + kv * 128 + (r & 7) * 16)),
+                     "l"(src + (size_t)r * ld + kv * 8)
+                     : "memory");
     }
 }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template<int N> __device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Stages of the shared-memory ring: the largest tile keeps 3 (144 KB, one CTA per SM), the
+// others 4 (two CTAs per SM).
+template<int BN> struct Stages {
+    static constexpr int value = BN >= 256 ? 3 : 4;
+};
 
 template<int BN, int EPI>
 __global__ void __launch_bounds__(kThreads)
     gemm_kernel(const __nv_bfloat16* __restrict__ A, const __nv_bfloat16* __restrict__ B, int K,
                 EpiArgs e, unsigned int* err) {
     static_assert(BN % 16 == 0 && BN >= 32 && BN <= 256, "tcgen05 M=128 needs N in 16..256");
+    constexpr int      S         = Stages<BN>::value;
+    constexpr int      kStage    = (kM + BN) * kKChunk * 2; // bytes per ring slot
     constexpr uint32_t kTmemCols = BN <= 32 ? 32 : (BN <= 64 ? 64 : (BN <= 128 ? 128 : 256));
     extern __shared__ __align__(1024) uint8_t smem[];
-    uint8_t*            sA = smem;                    // 128 x 64 bf16 = 16 KB
-    uint8_t*            sB = smem + kM * kKChunk * 2; // BN x 64 bf16
-    __shared__ uint64_t bar;
+    __shared__ uint64_t bar[S];
     __shared__ uint32_t tmem_base;
     const int           warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int           m0 = blockIdx.x * kM, n0 = blockIdx.y * BN;
+    const int           kz = K / gridDim.z;          // split-K: this CTA's share of K
+    const int           k0 = blockIdx.z * kz;
+    const int           nk = kz / kKChunk;
+    auto                sA = [&](int b) { return smem + b * kStage; };
+    auto                sB = [&](int b) { return smem + b * kStage + kM * kKChunk * 2; };
+    auto                load = [&](int kc) {
+        stage_kmajor_async(sA(kc % S), A + (size_t)m0 * K + k0 + kc * kKChunk, kM, K);
+        stage_kmajor_async(sB(kc % S), B + (size_t)n0 * K + k0 + kc * kKChunk, BN, K);
+    };
 
     if (warp == 0)
         tmem_alloc(&tmem_base, kTmemCols);
     if (threadIdx.x == 32)
-        mbar_init(&bar, 1);
+        for (int b = 0; b < S; b++)
+            mbar_init(&bar[b], 1);
+    for (int st = 0; st < S - 1; st++) { // prologue: the first S-1 chunks in flight
+        if (st < nk)
+            load(st);
+        cp_async_commit();
+    }
     fence_before_sync();
     __syncthreads();
     fence_after_sync();
     const uint32_t     tmem  = tmem_base;
     constexpr uint32_t idesc = instr_desc_bf16(kM, BN);
-    uint32_t           phase = 0;
     bool               ok    = true;
-    const int          nk    = K / kKChunk;
+    // chunk c's MMAs complete phase (c / S) of bar[c % S]; every completion is waited in order
+    auto mma_done = [&](int c) { return mbar_wait(&bar[c % S], (uint32_t)((c / S) & 1), 1u << 22); };
     for (int kc = 0; kc < nk && ok; kc++) {
-        stage_kmajor(sA, A + (size_t)m0 * K + kc * kKChunk, kM, K);
-        stage_kmajor(sB, B + (size_t)n0 * K + kc * kKChunk, BN, K);
+        cp_async_wait<S - 2>(); // this thread's part of chunk kc has landed
         fence_async_smem();
         __syncthreads();
         if (threadIdx.x == 0) {
             fence_after_sync();
+            const uint32_t a0 = smem_u32(sA(kc % S)), b0 = smem_u32(sB(kc % S));
 #pragma unroll
-            for (int kk = 0; kk < kKChunk / 16; kk++) {
-                const uint64_t ad = smem_desc(smem_u32(sA) + kk * 256, 128, 1024);
-                const uint64_t bd = smem_desc(smem_u32(sB) + kk * 256, 128, 1024);
-                mma_bf16(tmem, ad, bd, idesc, (kc | kk) != 0);
-            }
-            mma_commit(&bar);
+            for (int kk = 0; kk < kKChunk / 16; kk++)
+                mma_bf16(tmem, smem_desc(a0 + kk * 256, 128, 1024), smem_desc(b0 + kk * 256, 128, 1024),
+                         idesc, (kc | kk) != 0);
+            mma_commit(&bar[kc % S]);
         }
-        // every thread has seen the MMAs complete before the tiles are reused; a timed-out wait
-        // (bounded at ~2^22 polls) ends the loop in every thread alike
-        ok = __syncthreads_and(mbar_wait(&bar, phase, 1u << 22)) != 0;
-        phase ^= 1;
+        const int next = kc + S - 1; // refills the slot of chunk kc - 1 once its MMAs are done
+        if (next < nk) {
+            if (kc >= 1)
+                ok = __syncthreads_and(mma_done(kc - 1)) != 0;
+            if (ok)
+                load(next);
+        }
+        cp_async_commit();
     }
+    if (ok) // MMAs complete in order: the last chunk's completion covers them all
+        ok = __syncthreads_and(mma_done(nk - 1)) != 0;
+    cp_async_wait<0>();
     if (!ok) {
         if (threadIdx.x == 0)
             atomicOr(err, 1u);
@@ -224,23 +259,49 @@ __global__ void __launch_bounds__(kThreads)
         for (int c = 0; c < BN; c += 16) {
             float v[16];
             tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + c, v);
+            // this thread's 16 consecutive outputs of its row, written as 16-byte vectors
             const size_t o = (size_t)row * e.ldo + n0 + c;
+            if constexpr (EPI == kEpiBiasF32 || EPI == kEpiBiasGelu) {
 #pragma unroll
-            for (int i = 0; i < 16; i++) {
-                const int n = n0 + c + i;
-                if constexpr (EPI == kEpiF32)
-                    e.out_f32[o + i] = v[i];
-                else if constexpr (EPI == kEpiBiasF32)
-                    e.out_f32[o + i] = v[i] + e.bias[n];
-                else if constexpr (EPI == kEpiBiasGelu) {
-                    const float z     = v[i] + e.bias[n];
-                    e.out_z[o + i]    = z;
-                    e.out_bf16[o + i] = __float2bfloat16_rn(gelu(z));
+                for (int i = 0; i < 16; i++)
+                    v[i] += e.bias[n0 + c + i];
+            }
+            if constexpr (EPI == kEpiF32 || EPI == kEpiBiasF32) {
+                float4* d = reinterpret_cast<float4*>(e.out_f32 + blockIdx.z * e.zstride + o);
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+                    d[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+            }
+            else {
+                if constexpr (EPI == kEpiBiasGelu) {
+                    float4* dz = reinterpret_cast<float4*>(e.out_z + o);
+#pragma unroll
+                    for (int q = 0; q < 4; q++)
+                        dz[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+#pragma unroll
+                    for (int i = 0; i < 16; i++)
+                        v[i] = gelu(v[i]);
                 }
-                else if constexpr (EPI == kEpiGeluBwdBf16)
-                    e.out_bf16[o + i] = __float2bfloat16_rn(v[i] * gelu_grad(e.z_in[o + i]));
-                else
-                    e.out_bf16[o + i] = __float2bfloat16_rn(v[i]);
+                else if constexpr (EPI == kEpiGeluBwdBf16) {
+                    const float4* zi = reinterpret_cast<const float4*>(e.z_in + o);
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const float4 z = zi[q];
+                        v[4 * q] *= gelu_grad(z.x);
+                        v[4 * q + 1] *= gelu_grad(z.y);
+                        v[4 * q + 2] *= gelu_grad(z.z);
+                        v[4 * q + 3] *= gelu_grad(z.w);
+                    }
+                }
+                uint32_t pk[8];
+#pragma unroll
+                for (int q = 0; q < 8; q++) {
+                    __nv_bfloat162 h2 = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
+                    pk[q]             = *reinterpret_cast<uint32_t*>(&h2);
+                }
+                uint4* d = reinterpret_cast<uint4*>(e.out_bf16 + o);
+                d[0]     = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                d[1]     = make_uint4(pk[4], pk[5], pk[6], pk[7]);
             }
         }
     }
@@ -250,19 +311,23 @@ __global__ void __launch_bounds__(kThreads)
         tmem_dealloc(tmem, kTmemCols);
 }
 
-inline size_t gemm_smem_bytes(int BN) { return (size_t)(kM + BN) * kKChunk * 2; }
+inline size_t gemm_smem_bytes(int BN) {
+    return (size_t)(BN >= 256 ? 3 : 4) * (kM + BN) * kKChunk * 2;
+}
 
 // D = A . B^T for A [M x K], B [N x K] (bf16, K contiguous) with the given epilogue.
+// splits > 1 (kEpiF32 only): K is cut into `splits` equal parts, each written as a partial
+// product at out_f32 + z * zstride for the caller to reduce.
 template<int BN, int EPI>
 inline void gemm(const __nv_bfloat16* A, const __nv_bfloat16* B, int M, int N, int K,
-                 const EpiArgs& e, unsigned int* err, cudaStream_t st) {
+                 const EpiArgs& e, unsigned int* err, cudaStream_t st, int splits = 1) {
     static bool configured = false; // dynamic shared memory above the 48 KB default
     if (!configured) {
         cudaFuncSetAttribute(gemm_kernel<BN, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)gemm_smem_bytes(BN));
         configured = true;
     }
-    dim3 grid(M / kM, N / BN);
+    dim3 grid(M / kM, N / BN, splits);
     gemm_kernel<BN, EPI><<<grid, kThreads, gemm_smem_bytes(BN), st>>>(A, B, K, e, err);
 }
 
