@@ -308,7 +308,8 @@ def rt_params_planet():
     return p, rt, teq
 
 
-def rt_surrogate_leg(torch, thor_b200, nlog=64, iters=1500, batch=8192, nsteps=20):
+def rt_surrogate_leg(torch, thor_b200, nlog=64, iters=1500, batch=8192, nsteps=20,
+                     catch=True):
     """Plain FP64 + RT against mixed + trained surrogate RT on the RT configuration (g5/L40):
     time the plain form, log the plain RT, train the surrogate on the GPU, time the other form."""
     try:
@@ -353,6 +354,8 @@ def rt_surrogate_leg(torch, thor_b200, nlog=64, iters=1500, batch=8192, nsteps=2
                             "failed": st["failed"], "max_rel_err": st["max_err"],
                             "rt_column_fraction": st["rt_columns"] / ((nsteps + 3) * N)}}
     except Exception as e:  # a side measurement never breaks the bench line
+        if not catch:
+            raise
         return {"unavailable": "%s" % e}
 
 
@@ -494,12 +497,25 @@ def main():
     ap.add_argument("--glevel", type=int, default=GLEVEL,
                     help="grid level (default 6; smaller cases are for profiling captures)")
     ap.add_argument("--nv", type=int, default=NV, help="vertical levels (default 48)")
+    ap.add_argument("--surrogate-only", action="store_true",
+                    help="run only the RT surrogate leg (g5/L40) and print its JSON object; with "
+                         "--sur-log-steps / --sur-iters it is the small case for profiling captures")
+    ap.add_argument("--sur-log-steps", type=int, default=64,
+                    help="plain-RT steps logged for training (surrogate leg)")
+    ap.add_argument("--sur-iters", type=int, default=1500, help="Adam iterations (surrogate leg)")
     args = ap.parse_args()
     set_workload(args.glevel, args.nv)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
         return run_reference(args)
+    if args.surrogate_only:
+        import torch
+        import thor_b200
+        leg = rt_surrogate_leg(torch, thor_b200, nlog=args.sur_log_steps, iters=args.sur_iters,
+                               nsteps=args.steps, catch=False)
+        print(json.dumps(leg), flush=True)
+        return 0
     return run_ours(args)
 
 

@@ -194,6 +194,14 @@ int thorx_rt_totals(thorx_ctx* ctx, double* asr, double* olr);
 int thorx_bf16_gemm(const unsigned short* A, const unsigned short* B, int M, int N, int K, float* D);
 const char* thorx_surrogate_last_error(void);
 
+/* ---- Self-check of the division the stencil kernels use for the cell-area divisions: 1/b
+ * rounded once per column, then each a/b from it by fused multiply-adds (Markstein's theorem),
+ * which must equal the IEEE quotient bit for bit. n random (a, b) pairs per type, drawn on the
+ * device from seed (exponents over +-300 in double, +-60 in float; half of them with near-exact
+ * quotients), compared with a / b; mismatches[0] (double) and [1] (float) count the differing
+ * pairs. Context-free, current device, default stream. */
+int thorx_check_division(long long n, unsigned long long seed, long long mismatches[2]);
+
 /* ---- Learned RT surrogate. No counterpart in the reference. ----
  * A per-column MLP from (T per level, ln p per level, cos zenith) to the double-gray RT heating
  * rates per level as temperature tendencies dT/dt = Q / (rho c_v) in K/s (Q in W m^-3 is what

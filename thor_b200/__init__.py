@@ -134,6 +134,9 @@ def lib():
         L.thorx_bf16_gemm.argtypes = [vp, vp, ci, ci, ci, vp]
         L.thorx_bf16_gemm.restype = ci
         L.thorx_surrogate_last_error.restype = cp
+        L.thorx_check_division.argtypes = [ctypes.c_longlong, ctypes.c_ulonglong,
+                                           ctypes.POINTER(ctypes.c_longlong)]
+        L.thorx_check_division.restype = ci
         L.thorx_surrogate_create.argtypes = [vp, ctypes.POINTER(SurrogateParamsC)]
         L.thorx_surrogate_set_mode.argtypes = [vp, ci]
         L.thorx_surrogate_logged.argtypes = [vp]
@@ -172,7 +175,8 @@ EXPORTED = ["thorx_create", "thorx_destroy", "thorx_last_error", "thorx_field_si
             "thorx_surrogate_create", "thorx_surrogate_set_mode", "thorx_surrogate_logged",
             "thorx_surrogate_train", "thorx_surrogate_stats", "thorx_surrogate_layer",
             "thorx_surrogate_layer_grad", "thorx_surrogate_normalisation",
-            "thorx_surrogate_forward_host", "thorx_surrogate_gradients_host"]
+            "thorx_surrogate_forward_host", "thorx_surrogate_gradients_host",
+            "thorx_check_division"]
 
 def device_sum(ptr, n, stream=0):
     """Compensated sum of n doubles at device address `ptr` (thorx_device_sum)."""
@@ -206,6 +210,16 @@ def bf16_gemm(A_bits, B_bits):
     if rc:
         raise ThorxError(rc, lib().thorx_surrogate_last_error().decode())
     return D
+
+
+def check_division(n, seed=1):
+    """thorx_check_division: (double, float) counts of n random pairs whose reciprocal-based
+    quotient (the stencil kernels' area divisions) differs from the IEEE quotient."""
+    out = (ctypes.c_longlong * 2)()
+    rc = lib().thorx_check_division(n, seed, out)
+    if rc:
+        raise ThorxError(rc, lib().thorx_last_error(None).decode())
+    return out[0], out[1]
 
 
 NOALLOC_SUM_MAX_N = 134217728

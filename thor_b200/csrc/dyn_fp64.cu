@@ -93,18 +93,44 @@ __device__ __forceinline__ void stage_cols(double* sm, const double* __restrict_
         sm[q * kTile + threadIdx.x] = col >= 0 ? __ldg(src + (size_t)q * Np + col) : 0.0;
 }
 
+// a / b rounded to nearest, from y = 1/b rounded to nearest, with fused multiply-adds only.
+// Markstein's theorem (P. W. Markstein, IBM J. Res. Develop. 34(1):111-119, 1990; J.-M. Muller et
+// al., Handbook of Floating-Point Arithmetic, 2nd ed., 2018, sect. 4.7): if y = RN(1/b) and q is
+// within one ulp of a/b, the remainder a - b q is exact in one fma and RN(q + (a - b q) y) =
+// RN(a/b). q0 = RN(a y) is only within 1.5 ulp, so one correction step comes first. The result is
+// the IEEE quotient a / b bit for bit while a, b, the quotient and the remainders are normal
+// numbers (every field and grid quantity divided here); a zero numerator returns RN(a y), the
+// signed zero a / b has. Used where one divisor (a cell's sub-triangle area) serves many divisions,
+// so the one IEEE division of the reciprocal is paid once per column.
+__device__ __forceinline__ double div_rcp(double a, double b, double y) {
+    const double q0 = __dmul_rn(a, y);
+    const double q1 = __fma_rn(__fma_rn(-q0, b, a), y, q0);
+    const double q2 = __fma_rn(__fma_rn(-q1, b, a), y, q1);
+    return a == 0.0 ? q0 : q2;
+}
+__device__ __forceinline__ float div_rcp(float a, float b, float y) {
+    const float q0 = __fmul_rn(a, y);
+    const float q1 = __fmaf_rn(__fmaf_rn(-q0, b, a), y, q0);
+    const float q2 = __fmaf_rn(__fmaf_rn(-q1, b, a), y, q1);
+    return a == 0.0f ? q0 : q2;
+}
+
 // Shared-memory view of one column's ring geometry, [quantity][32].
 struct SGeo {
-    const double *ar, *at, *ti, *te, *oa;
+    const double *ar, *at, *ti, *te, *oa, *rat, *ratf;
     int           x;
     __device__ double AR(int q) const { return ar[q * kTile + x]; }
     __device__ double AT(int q) const { return at[q * kTile + x]; }
     __device__ double TI(int q) const { return ti[q * kTile + x]; }
     __device__ double TE(int q) const { return te[q * kTile + x]; }
     __device__ double OA(int q) const { return oa[q * kTile + x]; }
+    // 1 / areasTr rounded to nearest, in double and (for the FP32 stencils) in float
+    __device__ double RAT(int q) const { return rat[q * kTile + x]; }
+    __device__ float  RATF(int q) const { return (float)ratf[q * kTile + x]; }
 };
 
-constexpr int kRingGeoRows = 78; // areas 18, areasTr 6, nvecti 18, nvecte 18, nvecoa 18
+// areas 18, areasTr 6, nvecti 18, nvecte 18, nvecoa 18, 1/areasTr 6 (double), 6 (float)
+constexpr int kRingGeoRows = 90;
 
 __device__ __forceinline__ SGeo stage_ring_geo(double* sm, const Geometry& g, int col) {
     stage_cols(sm, g.areas, 18, g.Np, col);
@@ -112,9 +138,20 @@ __device__ __forceinline__ SGeo stage_ring_geo(double* sm, const Geometry& g, in
     stage_cols(sm + 24 * kTile, g.nvecti, 18, g.Np, col);
     stage_cols(sm + 42 * kTile, g.nvecte, 18, g.Np, col);
     stage_cols(sm + 60 * kTile, g.nvecoa, 18, g.Np, col);
+    for (int q = threadIdx.y; q < 6; q += blockDim.y) {
+        // a pentagon's sixth entry is 0 and never read; its reciprocal (inf) is not either
+        const double at = col >= 0 ? __ldg(g.areasTr + (size_t)q * g.Np + col) : 1.0;
+        sm[(78 + q) * kTile + threadIdx.x] = 1.0 / at;
+        sm[(84 + q) * kTile + threadIdx.x] = (double)(1.0f / (float)at);
+    }
     return SGeo{sm, sm + 18 * kTile, sm + 24 * kTile, sm + 42 * kTile, sm + 60 * kTile,
-                (int)threadIdx.x};
+                sm + 78 * kTile, sm + 84 * kTile, (int)threadIdx.x};
 }
+
+// The staged reciprocal of areasTr in the compute type R.
+template<class R> __device__ __forceinline__ R rat_of(const SGeo& G, int q);
+template<> __device__ __forceinline__ double rat_of<double>(const SGeo& G, int q) { return G.RAT(q); }
+template<> __device__ __forceinline__ float rat_of<float>(const SGeo& G, int q) { return G.RATF(q); }
 
 // ---------------------------------------------------------------------------------------------
 // Per-level tables (LevelTable in thorx_internal.h), one thread per level/interface index. The
@@ -512,6 +549,7 @@ __device__ __forceinline__ R laplacian(const SGeo& G, const R* a, R a0, R rscale
     auto TI = [&](int q) { return (R)G.TI(q); };
     auto TE = [&](int q) { return (R)G.TE(q); };
     auto OA = [&](int q) { return (R)G.OA(q); };
+    auto RAT = [&](int q) { return rat_of<R>(G, q); };
     const R h = (R)0.5;
     R       lap = 0;
     R       lap1 = 0, lap2 = 0, lap3 = 0, lapx1 = 0, lapx2 = 0, lapy1 = 0, lapy2 = 0, lapz1 = 0,
@@ -523,14 +561,14 @@ __device__ __forceinline__ R laplacian(const SGeo& G, const R* a, R a0, R rscale
         const R   vdiff = h * rscale;
         R         astar;
         if (j == 0) {
-            AT1   = rscale / AT(j);
-            astar = (AR(j * 3 + 0) * a0 + AR(j * 3 + 1) * p1 + AR(j * 3 + 2) * p2) / AT(j);
+            AT1   = div_rcp(rscale, AT(j), RAT(j));
+            astar = div_rcp(AR(j * 3 + 0) * a0 + AR(j * 3 + 1) * p1 + AR(j * 3 + 2) * p2, AT(j), RAT(j));
             lap1  = (h * (p1 + a0) - astar);
             lap2  = (h * (p1 + p2) - astar);
             lap3  = (h * (a0 + p2) - astar);
         }
-        const R AT2 = rscale / AT(jp1);
-        astar = (AR(jp1 * 3 + 0) * a0 + AR(jp1 * 3 + 1) * p2 + AR(jp1 * 3 + 2) * p3) / AT(jp1);
+        const R AT2 = div_rcp(rscale, AT(jp1), RAT(jp1));
+        astar = div_rcp(AR(jp1 * 3 + 0) * a0 + AR(jp1 * 3 + 1) * p2 + AR(jp1 * 3 + 2) * p3, AT(jp1), RAT(jp1));
         const R lap4 = (h * (a0 + p2) - astar);
         const R lap5 = (h * (p2 + p3) - astar);
         const R lap6 = (h * (a0 + p3) - astar);
@@ -697,6 +735,7 @@ __device__ __forceinline__ void divm_core(const SGeo& G, const R* a0, const R (*
     auto    TI = [&](int q) { return (R)G.TI(q); };
     auto    TE = [&](int q) { return (R)G.TE(q); };
     auto    OA = [&](int q) { return (R)G.OA(q); };
+    auto    RAT = [&](int q) { return rat_of<R>(G, q); };
     const R h   = (R)0.5;
     const R AT0 = h * rscale;
     R       lapx = 0, lapy = 0, lapz = 0;
@@ -707,10 +746,10 @@ __device__ __forceinline__ void divm_core(const SGeo& G, const R* a0, const R (*
         const R *p1 = ar[j], *p2 = ar[jp1], *p3 = ar[jp2];
         R        dwdz = 0, dwdz2 = 0;
         if (with_w) {
-            const R meanwl = (AR(j * 3 + 0) * wl0 + AR(j * 3 + 1) * wl[j] + AR(j * 3 + c2) * wl[jp1]) / AT(j);
-            const R meanwt = (AR(j * 3 + 0) * wt0 + AR(j * 3 + 1) * wt[j] + AR(j * 3 + c2) * wt[jp1]) / AT(j);
-            const R meanwl2 = (AR(jp1 * 3 + 0) * wl0 + AR(jp1 * 3 + 1) * wl[jp1] + AR(jp1 * 3 + c2) * wl[jp2]) / AT(jp1);
-            const R meanwt2 = (AR(jp1 * 3 + 0) * wt0 + AR(jp1 * 3 + 1) * wt[jp1] + AR(jp1 * 3 + c2) * wt[jp2]) / AT(jp1);
+            const R meanwl = div_rcp(AR(j * 3 + 0) * wl0 + AR(j * 3 + 1) * wl[j] + AR(j * 3 + c2) * wl[jp1], AT(j), RAT(j));
+            const R meanwt = div_rcp(AR(j * 3 + 0) * wt0 + AR(j * 3 + 1) * wt[j] + AR(j * 3 + c2) * wt[jp1], AT(j), RAT(j));
+            const R meanwl2 = div_rcp(AR(jp1 * 3 + 0) * wl0 + AR(jp1 * 3 + 1) * wl[jp1] + AR(jp1 * 3 + c2) * wl[jp2], AT(jp1), RAT(jp1));
+            const R meanwt2 = div_rcp(AR(jp1 * 3 + 0) * wt0 + AR(jp1 * 3 + 1) * wt[jp1] + AR(jp1 * 3 + c2) * wt[jp2], AT(jp1), RAT(jp1));
             dwdz  = (meanwl - meanwt) * dz;
             dwdz2 = (meanwl2 - meanwt2) * dz;
         }
@@ -721,9 +760,9 @@ __device__ __forceinline__ void divm_core(const SGeo& G, const R* a0, const R (*
             a12x = (p1[0] + p2[0]);
             a12y = (p1[1] + p2[1]);
             a12z = (p1[2] + p2[2]);
-            AT1  = h * rscale / AT(j);
+            AT1  = div_rcp(h * rscale, AT(j), RAT(j));
         }
-        const R AT2  = h * rscale / AT(jp1);
+        const R AT2  = div_rcp(h * rscale, AT(jp1), RAT(jp1));
         const R a02x = (a0[0] + p2[0]), a02y = (a0[1] + p2[1]), a02z = (a0[2] + p2[2]);
         const R a23x = (p2[0] + p3[0]), a23y = (p2[1] + p3[1]), a23z = (p2[2] + p3[2]);
         const R a03x = (a0[0] + p3[0]), a03y = (a0[1] + p3[1]), a03z = (a0[2] + p3[2]);
@@ -1477,6 +1516,62 @@ inline dim3 tile_grid(const Geometry& g) { return dim3(g.Np / kTile); }
 inline dim3 tile_grid_tail(const Geometry& g) { return dim3(g.Np / kTile + 1); }
 inline dim3 tile_block() { return dim3(kTile, kLevGroups); }
 
+// ---------------------------------------------------------------------------------------------
+// Self-check of div_rcp against the IEEE quotient: n random pairs per type from SplitMix64 on
+// (seed, index); exponents over +-300 (double) and +-60 (float); every second pair has a near-exact
+// quotient (a = b c rounded), where a wrong last bit would show first. cnt[0] / cnt[1] count the
+// double / float pairs whose bits differ.
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long splitmix(unsigned long long z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+__device__ __forceinline__ double rand_double(unsigned long long r, unsigned long long e, int emin,
+                                              int emax) {
+    const int          ex   = emin + (int)(e % (unsigned long long)(emax - emin + 1));
+    unsigned long long bits = ((unsigned long long)(ex + 1023) << 52) | (r & ((1ull << 52) - 1));
+    return __longlong_as_double((long long)(bits | ((r >> 63) << 63)));
+}
+__device__ __forceinline__ float rand_float(unsigned long long r, unsigned long long e, int emin,
+                                            int emax) {
+    const int    ex   = emin + (int)(e % (unsigned long long)(emax - emin + 1));
+    unsigned int bits = ((unsigned int)(ex + 127) << 23) | (unsigned int)(r & ((1u << 23) - 1));
+    return __int_as_float((int)(bits | (unsigned int)((r >> 63) << 31)));
+}
+__global__ void div_check_kernel(long long n, unsigned long long seed, unsigned long long* cnt) {
+    unsigned long long bad_d = 0, bad_f = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        unsigned long long k = seed ^ ((unsigned long long)i * 0xD1B54A32D192ED03ull);
+        const unsigned long long r0 = splitmix(k), r1 = splitmix(r0), r2 = splitmix(r1),
+                                 r3 = splitmix(r2);
+        double a, b;
+        float  af, bf;
+        if (i & 1) {
+            b  = rand_double(r0, r1 >> 40, -2, 2);
+            a  = b * rand_double(r2, r3 >> 40, -2, 2);
+            bf = rand_float(r1, r0 >> 40, -2, 2);
+            af = bf * rand_float(r3, r2 >> 40, -2, 2);
+        }
+        else {
+            a  = rand_double(r0, r1 >> 40, -300, 300);
+            b  = rand_double(r2, r3 >> 40, -300, 300);
+            af = rand_float(r1, r0 >> 40, -60, 60);
+            bf = rand_float(r3, r2 >> 40, -60, 60);
+        }
+        const double q = a / b, qr = div_rcp(a, b, 1.0 / b);
+        bad_d += __double_as_longlong(q) != __double_as_longlong(qr);
+        const float qf = af / bf, qfr = div_rcp(af, bf, 1.0f / bf);
+        bad_f += __float_as_int(qf) != __float_as_int(qfr);
+    }
+    if (bad_d)
+        atomicAdd(cnt, bad_d);
+    if (bad_f)
+        atomicAdd(cnt + 1, bad_f);
+}
+
 } // namespace
 
 int max_levels() { return kRk2Groups * kMaxLevelsPerThread; }
@@ -1542,6 +1637,10 @@ void launch_vertical(const Geometry& g, const Phys& P, const State& s, double dt
 }
 void launch_update_rk2(const Geometry& g, const Phys& P, const State& s, cudaStream_t st) {
     update_rk2_kernel<<<tile_grid(g), dim3(kTile, kRk2Groups), 0, st>>>(g, P, s);
+}
+void launch_div_check(long long n, unsigned long long seed, unsigned long long* cnt,
+                      cudaStream_t st) {
+    div_check_kernel<<<148 * 8, 256, 0, st>>>(n, seed, cnt);
 }
 
 } // namespace thorx

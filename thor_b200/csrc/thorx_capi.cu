@@ -1435,4 +1435,31 @@ int thorx_device_sum_noalloc(const double* x, long long n, void* stream, double*
     return 0;
 }
 
+int thorx_check_division(long long n, unsigned long long seed, long long mismatches[2]) {
+    const char* fn = "thorx_check_division";
+    if (n < 0 || !mismatches)
+        return free_fail(THORX_E_ARG, std::string(fn) + ": negative n or null output");
+    unsigned long long* cnt = nullptr;
+    unsigned long long  h[2] = {0, 0};
+    cudaError_t         e    = cudaMalloc(&cnt, 2 * sizeof(unsigned long long));
+    if (e == cudaSuccess)
+        e = cudaMemset(cnt, 0, 2 * sizeof(unsigned long long));
+    if (e == cudaSuccess && n > 0) {
+        launch_div_check(n, seed, cnt, 0);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpy(h, cnt, sizeof h, cudaMemcpyDeviceToHost);
+    if (cnt) {
+        cudaError_t ef = cudaFree(cnt);
+        if (e == cudaSuccess)
+            e = ef;
+    }
+    if (e != cudaSuccess)
+        return free_fail(THORX_E_CUDA, std::string(fn) + ": " + cudaGetErrorString(e));
+    mismatches[0] = (long long)h[0];
+    mismatches[1] = (long long)h[1];
+    return 0;
+}
+
 } // extern "C"

@@ -138,6 +138,9 @@ void launch_momentum(const Geometry& g, const Phys& P, const State& s, double dt
 void launch_vertical(const Geometry& g, const Phys& P, const State& s, double dt,
                      cudaStream_t st);
 void launch_update_rk2(const Geometry& g, const Phys& P, const State& s, cudaStream_t st);
+// cnt[0..1] += pairs whose reciprocal-based quotient differs from the IEEE one (double, float)
+void launch_div_check(long long n, unsigned long long seed, unsigned long long* cnt,
+                      cudaStream_t st);
 
 // Double-gray radiative transfer with its insolation (thor_b200/csrc/rt.cu).
 struct RtConst { // set once by thorx_rt_enable; angles in radians, lengths in m
