@@ -468,12 +468,18 @@ def run_ours(args):
     if world == 1 and not args.no_extras:
         # the mixed-precision form of the same context, same workload, after the measurements above
         ms_mixed = time_steps(x, stream, thor_b200.MIXED, max(5, min(args.steps, 50)))
+        kms_mixed = x.profile_steps(nprof)
+        x.sync()
         line["mixed_form"] = {"ms_per_step": ms_mixed,
                               "value": sim_days_per_hour(1, ms_mixed / 1000.0),
                               "ratio_vs_fp64": ms_step / ms_mixed,
-                              "what": "THORX_MIXED: FP32 momentum-side stencils, FP64 mass, "
-                                      "pressure, vertical solve and sums; same state, same graph "
-                                      "timing"}
+                              "kernels_ms_per_step": {t[0]: kms_mixed[i] / nprof
+                                                      for i, t in enumerate(table)
+                                                      if kms_mixed[i] > 0},
+                              "what": "THORX_MIXED: FP32 momentum-side stencils, hyperdiffusion "
+                                      "and divergence damping through per-column operator weights, "
+                                      "FP64 mass, pressure, vertical solve and sums; same state, "
+                                      "same graph timing"}
         line["rt_surrogate"] = rt_surrogate_leg(torch, thor_b200)
     x.close()
     if rank == 0:

@@ -127,10 +127,18 @@ struct SGeo {
     // 1 / areasTr rounded to nearest, in double and (for the FP32 stencils) in float
     __device__ double RAT(int q) const { return rat[q * kTile + x]; }
     __device__ float  RATF(int q) const { return (float)ratf[q * kTile + x]; }
+    // mixed form: the column's operator weights (Geometry::lapw, Geometry::dmw), [entry][32]
+    const double* lw;
+    const float * lwf, *dm;
 };
+
+// The mixed form (compute type float) applies the operators through per-column weights.
+template<class R> constexpr bool kOperatorWeights = sizeof(R) < sizeof(double);
 
 // areas 18, areasTr 6, nvecti 18, nvecte 18, nvecoa 18, 1/areasTr 6 (double), 6 (float)
 constexpr int kRingGeoRows = 90;
+static_assert(7 * 8 + 7 * 4 <= kRingGeoRows * 8 && 84 * 4 <= kRingGeoRows * 8,
+              "operator weights must fit the ring-geometry buffer");
 
 __device__ __forceinline__ SGeo stage_ring_geo(double* sm, const Geometry& g, int col) {
     stage_cols(sm, g.areas, 18, g.Np, col);
@@ -144,8 +152,42 @@ __device__ __forceinline__ SGeo stage_ring_geo(double* sm, const Geometry& g, in
         sm[(78 + q) * kTile + threadIdx.x] = 1.0 / at;
         sm[(84 + q) * kTile + threadIdx.x] = (double)(1.0f / (float)at);
     }
-    return SGeo{sm, sm + 18 * kTile, sm + 24 * kTile, sm + 42 * kTile, sm + 60 * kTile,
-                sm + 78 * kTile, sm + 84 * kTile, (int)threadIdx.x};
+    return SGeo{sm,       sm + 18 * kTile, sm + 24 * kTile, sm + 42 * kTile, sm + 60 * kTile,
+                sm + 78 * kTile, sm + 84 * kTile, (int)threadIdx.x, nullptr, nullptr, nullptr};
+}
+
+// Mixed form: the Laplacian weights of the lanes' columns in place of the ring geometry
+// (double [7][32], then float [7][32]; fits the ring-geometry buffer).
+__device__ __forceinline__ SGeo stage_lap_weights(double* sm, const Geometry& g, int col) {
+    float* smf = reinterpret_cast<float*>(sm + 7 * kTile);
+    for (int q = threadIdx.y; q < 7; q += blockDim.y) {
+        const double w = col >= 0 ? __ldg(g.lapw + (size_t)q * g.Np + col) : 0.0;
+        sm[q * kTile + threadIdx.x]  = w;
+        smf[q * kTile + threadIdx.x] = (float)w;
+    }
+    SGeo G{};
+    G.x   = threadIdx.x;
+    G.lw  = sm;
+    G.lwf = smf;
+    return G;
+}
+// Mixed form: the divergence-damping weights, float [84][32] (fits the ring-geometry buffer).
+__device__ __forceinline__ SGeo stage_divm_weights(double* sm, const Geometry& g, int col) {
+    float* smf = reinterpret_cast<float*>(sm);
+    for (int q = threadIdx.y; q < 84; q += blockDim.y)
+        smf[q * kTile + threadIdx.x] = col >= 0 ? __ldg(g.dmw + (size_t)q * g.Np + col) : 0.0f;
+    SGeo G{};
+    G.x  = threadIdx.x;
+    G.dm = smf;
+    return G;
+}
+// What a kernel with divergence damping stages: ring geometry (FP64 form) or weights (mixed).
+template<class R>
+__device__ __forceinline__ SGeo stage_divm_geo(double* sm, const Geometry& g, int col) {
+    if constexpr (kOperatorWeights<R>)
+        return stage_divm_weights(sm, g, col);
+    else
+        return stage_ring_geo(sm, g, col);
 }
 
 // The staged reciprocal of areasTr in the compute type R.
@@ -592,6 +634,26 @@ __device__ __forceinline__ R laplacian(const SGeo& G, const R* a, R a0, R rscale
     return lap;
 }
 
+// Laplacian from the weights: (w0 a0 + sum_k wk (ak - a0)) rscale^2, products and sums in R.
+template<int n, class R>
+__device__ __forceinline__ double laplacian_w(const SGeo& G, const double* a, double rscale) {
+    const int x = G.x;
+    if constexpr (sizeof(R) < sizeof(double)) {
+        float acc = G.lwf[x] * (float)a[0];
+#pragma unroll
+        for (int k = 1; k <= n; k++)
+            acc = fmaf(G.lwf[k * kTile + x], (float)(a[k] - a[0]), acc);
+        return (double)(acc * (float)(rscale * rscale));
+    }
+    else {
+        double acc = G.lw[x] * a[0];
+#pragma unroll
+        for (int k = 1; k <= n; k++)
+            acc = fma(G.lw[k * kTile + x], a[k] - a[0], acc);
+        return acc * (rscale * rscale);
+    }
+}
+
 // ---------------------------------------------------------------------------------------------
 // Hyperdiffusion pass: Diffusion_Op + Diffusion_Op_Poles (src/headers/dyn/thor_diff.h:54-880)
 // on the six variables rho, v(3), w, Rd T (or Cv T), without the diffusive sponge; the final pass
@@ -652,13 +714,9 @@ __device__ __forceinline__ void diffusion_point(const Geometry& g, const Phys& P
             a[j] = v;
         }
         double lap;
-        if (sizeof(R) < sizeof(double) && var >= 1 && var <= 4) { // v and w in the mixed form
-            R af[n + 1];
-#pragma unroll
-            for (int j = 0; j <= n; j++)
-                af[j] = (R)a[j];
-            lap = (double)laplacian<n, R>(G, af + 1, af[0], (R)rscale);
-        }
+        if constexpr (kOperatorWeights<R>) // mixed form: v and w in float, rho and T in double
+            lap = (var >= 1 && var <= 4) ? laplacian_w<n, float>(G, a, rscale)
+                                         : laplacian_w<n, double>(G, a, rscale);
         else
             lap = laplacian<n, double>(G, a + 1, a[0], rscale);
         if (!last) {
@@ -710,7 +768,11 @@ __global__ void THORX_KATTR_DIFF
                      double* __restrict__ diff_out, int stepnum, bool last) {
     __shared__ double sgeo[kRingGeoRows * kTile];
     const int         c = lane_column(g);
-    const SGeo        G = stage_ring_geo(sgeo, g, c);
+    SGeo              G;
+    if constexpr (kOperatorWeights<R>)
+        G = stage_lap_weights(sgeo, g, c);
+    else
+        G = stage_ring_geo(sgeo, g, c);
     __syncthreads();
     if (c < 0)
         return;
@@ -786,6 +848,129 @@ __device__ __forceinline__ void divm_core(const SGeo& G, const R* a0, const R (*
     lapo[2] = lapz;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Operator weights of the mixed form. Both stencil operators are linear in the point values, so
+// each is fixed per column by its response to unit inputs, computed here once per context with
+// the FP64 operator code above (laplacian, divm_core) at rscale = 1 (and dz = 1 for the w part of
+// the damping): the Laplacian scales with rscale^2 (rscale / areasTr and 0.5 rscale), the damping's
+// Mh part with rscale^2 and its w part with rscale dz. The centre entry is stored as the sum of
+// all the point weights and the ring entries as they are, so that at run time
+//   op(a) = (sum_k w_k) a_0 + sum_{k>=1} w_k (a_k - a_0),
+// the same linear operator; the differences a_k - a_0 are formed in FP64 before the FP32
+// multiply-adds, so the float arithmetic does not see the large common part of the values.
+// One thread per column; a column with a five-entry ring gets zero sixth weights.
+// ---------------------------------------------------------------------------------------------
+template<int n>
+__device__ void stencil_weights_of(const SGeo& G, int c2, int c, int Np, double* lapw, float* dmw) {
+    // Laplacian
+    double w[7] = {0, 0, 0, 0, 0, 0, 0}, wsum = 0.0;
+    for (int k = 0; k <= n; k++) {
+        double a[n + 1];
+        for (int j = 0; j <= n; j++)
+            a[j] = (j == k) ? 1.0 : 0.0;
+        w[k] = laplacian<n, double>(G, a + 1, a[0], 1.0);
+        wsum += w[k];
+    }
+    lapw[c] = wsum;
+    for (int k = 1; k < 7; k++)
+        lapw[(size_t)k * Np + c] = w[k];
+    // divergence damping, Mh part: response to a unit component comp at point k
+    double wm[3][7][3] = {};
+    for (int k = 0; k <= n; k++)
+        for (int comp = 0; comp < 3; comp++) {
+            double a0[3] = {0, 0, 0}, ar[n][3], out[3];
+            for (int j = 0; j < n; j++)
+                ar[j][0] = ar[j][1] = ar[j][2] = 0.0;
+            if (k == 0)
+                a0[comp] = 1.0;
+            else
+                ar[k - 1][comp] = 1.0;
+            divm_core<n, double>(G, a0, ar, false, 0.0, 0.0, nullptr, nullptr, 0.0, 1.0, c2, out);
+            for (int o = 0; o < 3; o++)
+                wm[o][k][comp] = out[o];
+        }
+    for (int o = 0; o < 3; o++)
+        for (int comp = 0; comp < 3; comp++) {
+            double sum = 0.0;
+            for (int k = 0; k <= n; k++)
+                sum += wm[o][k][comp];
+            dmw[(size_t)(o * 28 + comp) * Np + c] = (float)sum;
+            for (int k = 1; k < 7; k++)
+                dmw[(size_t)(o * 28 + k * 3 + comp) * Np + c] = (float)wm[o][k][comp];
+        }
+    // divergence damping, w part: response to a unit (Wh below - Wh above) at point k
+    for (int k = 0; k < 7; k++) {
+        double out[3] = {0, 0, 0};
+        if (k <= n) {
+            double a0[3] = {0, 0, 0}, ar[n][3], wl[n], wt[n];
+            for (int j = 0; j < n; j++) {
+                ar[j][0] = ar[j][1] = ar[j][2] = 0.0;
+                wl[j] = (j == k - 1) ? 1.0 : 0.0;
+                wt[j] = 0.0;
+            }
+            divm_core<n, double>(G, a0, ar, true, k == 0 ? 1.0 : 0.0, 0.0, wl, wt, 1.0, 1.0, c2,
+                                 out);
+        }
+        for (int o = 0; o < 3; o++)
+            dmw[(size_t)(o * 28 + 21 + k) * Np + c] = (float)out[o];
+    }
+}
+
+__global__ void __launch_bounds__(kTile) stencil_weights_kernel(Geometry g, double* lapw, float* dmw) {
+    __shared__ double sgeo[kRingGeoRows * kTile];
+    const int         c   = blockIdx.x * kTile + threadIdx.x;
+    const int         col = c < g.N ? c : -1;
+    const SGeo        G   = stage_ring_geo(sgeo, g, col);
+    __syncthreads();
+    if (col < 0)
+        return;
+    const int c2 = (g.cflag[c] & kPole) ? 1 : 2;
+    if (g.cflag[c] & kRing5)
+        stencil_weights_of<5>(G, c2, c, g.Np, lapw, dmw);
+    else
+        stencil_weights_of<6>(G, c2, c, g.Np, lapw, dmw);
+}
+
+// Divergence damping from the weights, in float: a0 [3] and ar [n][3] the Mh (or divg) vectors
+// at the centre and the ring; dw [n + 1] the (below - above) Wh differences when with_w.
+template<int n>
+__device__ __forceinline__ void divm_w(const SGeo& G, const double* a0, const double (*ar)[3],
+                                       bool with_w, const double* dw, double rscale, double dz,
+                                       float* out) {
+    const int x = G.x;
+    float     d[n][3], c0[3];
+#pragma unroll
+    for (int comp = 0; comp < 3; comp++) {
+        c0[comp] = (float)a0[comp];
+#pragma unroll
+        for (int j = 0; j < n; j++)
+            d[j][comp] = (float)(ar[j][comp] - a0[comp]);
+    }
+    const float sv = (float)(rscale * rscale), sw = (float)(rscale * dz);
+#pragma unroll
+    for (int o = 0; o < 3; o++) {
+        const float* W   = G.dm + o * 28 * kTile + x;
+        float        acc = 0.0f;
+#pragma unroll
+        for (int comp = 0; comp < 3; comp++)
+            acc = fmaf(W[comp * kTile], c0[comp], acc);
+#pragma unroll
+        for (int j = 0; j < n; j++)
+#pragma unroll
+            for (int comp = 0; comp < 3; comp++)
+                acc = fmaf(W[((j + 1) * 3 + comp) * kTile], d[j][comp], acc);
+        acc *= sv;
+        if (with_w) {
+            float accw = 0.0f;
+#pragma unroll
+            for (int k = 0; k <= n; k++)
+                accw = fmaf(W[(21 + k) * kTile], (float)dw[k], accw);
+            acc = fmaf(accw, sw, acc);
+        }
+        out[o] = acc;
+    }
+}
+
 template<int n, class R>
 __device__ __forceinline__ void divm0_point(const Geometry& g, const Phys& P, const SGeo& G,
                                             const int* ring, int c2, const double* __restrict__ Mh,
@@ -794,6 +979,26 @@ __device__ __forceinline__ void divm0_point(const Geometry& g, const Phys& P, co
     const int    Np = g.Np, nv = g.nv;
     const double rscale = rscale_of(P, g, lev);
     const double dz     = 1.0 / (g.Altitudeh[lev] - g.Altitudeh[lev + 1]);
+    if constexpr (kOperatorWeights<R>) {
+        double a0[3], ar[n][3], dw[n + 1];
+#pragma unroll
+        for (int k = 0; k < 3; k++)
+            a0[k] = Mh[(k * nv + lev) * Np + c];
+        dw[0] = Wh[lev * Np + c] - Wh[(lev + 1) * Np + c];
+#pragma unroll
+        for (int j = 0; j < n; j++) {
+#pragma unroll
+            for (int k = 0; k < 3; k++)
+                ar[j][k] = gz(Mh + (k * nv + lev) * Np, ring[j]);
+            dw[j + 1] = gz(Wh + lev * Np, ring[j]) - gz(Wh + (lev + 1) * Np, ring[j]);
+        }
+        float out[3];
+        divm_w<n>(G, a0, ar, true, dw, rscale, dz, out);
+#pragma unroll
+        for (int k = 0; k < 3; k++)
+            divg[(k * nv + lev) * Np + c] = (double)out[k];
+        return;
+    }
     R            a0[3], ar[n][3], wl[n], wt[n];
 #pragma unroll
     for (int k = 0; k < 3; k++)
@@ -835,7 +1040,7 @@ __global__ void THORX_KATTR_DIVM
                  double* __restrict__ divg) {
     __shared__ double sgeo[kRingGeoRows * kTile];
     const int         c = lane_column(g);
-    const SGeo        G = stage_ring_geo(sgeo, g, c);
+    const SGeo        G = stage_divm_geo<R>(sgeo, g, c);
     __syncthreads();
     if (c < 0)
         return;
@@ -851,18 +1056,32 @@ __device__ __forceinline__ void divm_final(const Geometry& g, const Phys& P, con
                                            const int* ring, const double* __restrict__ divg, int c,
                                            int lev, const double* fr, R* DivM) {
     const int Np = g.Np, nv = g.nv;
-    R         a0[3], ar[n][3];
-#pragma unroll
-    for (int k = 0; k < 3; k++)
-        a0[k] = (R)divg[(k * nv + lev) * Np + c];
-#pragma unroll
-    for (int j = 0; j < n; j++)
+    R         lap[3];
+    if constexpr (kOperatorWeights<R>) {
+        double a0[3], ar[n][3];
 #pragma unroll
         for (int k = 0; k < 3; k++)
-            ar[j][k] = (R)gz(divg + (k * nv + lev) * Np, ring[j]);
-    R lap[3];
-    divm_core<n, R>(G, a0, ar, false, (R)0, (R)0, nullptr, nullptr, (R)0, (R)rscale_of(P, g, lev), 2,
-                    lap);
+            a0[k] = divg[(k * nv + lev) * Np + c];
+#pragma unroll
+        for (int j = 0; j < n; j++)
+#pragma unroll
+            for (int k = 0; k < 3; k++)
+                ar[j][k] = gz(divg + (k * nv + lev) * Np, ring[j]);
+        divm_w<n>(G, a0, ar, false, nullptr, rscale_of(P, g, lev), 0.0, lap);
+    }
+    else {
+        R a0[3], ar[n][3];
+#pragma unroll
+        for (int k = 0; k < 3; k++)
+            a0[k] = (R)divg[(k * nv + lev) * Np + c];
+#pragma unroll
+        for (int j = 0; j < n; j++)
+#pragma unroll
+            for (int k = 0; k < 3; k++)
+                ar[j][k] = (R)gz(divg + (k * nv + lev) * Np, ring[j]);
+        divm_core<n, R>(G, a0, ar, false, (R)0, (R)0, nullptr, nullptr, (R)0,
+                        (R)rscale_of(P, g, lev), 2, lap);
+    }
     const R sdiff = (R)g.Kdhz[lev];
     const R lapr  = (R)fr[0] * lap[0] + (R)fr[1] * lap[1] + (R)fr[2] * lap[2];
 #pragma unroll
@@ -1055,7 +1274,7 @@ __global__ void THORX_KATTR_SLOW
     const int         c = lane_column(g);
     SGeo              G{};
     if (P.DivDampP)
-        G = stage_ring_geo(sgeo, g, c);
+        G = stage_divm_geo<R>(sgeo, g, c);
     stage_cols(sdiv, g.div, 21, g.Np, c);
     stage_cols(sgrad, g.grad, 21, g.Np, c);
     __syncthreads();
@@ -1121,7 +1340,7 @@ __global__ void THORX_KATTR_MOM
     const int         c = lane_column(g);
     SGeo              G{};
     if (P.DivDampP)
-        G = stage_ring_geo(sgeo, g, c);
+        G = stage_divm_geo<R>(sgeo, g, c);
     stage_cols(sgrad, g.grad, 21, g.Np, c);
     __syncthreads();
     if (c < 0)
@@ -1578,6 +1797,9 @@ int max_levels() { return kRk2Groups * kMaxLevelsPerThread; }
 
 void launch_level_tables(const Geometry& g, const Phys& P, double* lt, cudaStream_t st) {
     level_tables_kernel<<<(g.nvi + 127) / 128, 128, 0, st>>>(g, P, lt);
+}
+void launch_stencil_weights(const Geometry& g, double* lapw, float* dmw, cudaStream_t st) {
+    stencil_weights_kernel<<<(g.N + kTile - 1) / kTile, kTile, 0, st>>>(g, lapw, dmw);
 }
 
 void launch_profx(const Geometry& g, const Phys& P, const State& s, bool finish, cudaStream_t st) {

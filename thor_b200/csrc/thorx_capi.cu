@@ -633,6 +633,17 @@ int thorx_create(const thorx_grid* gr, const thorx_params* pr, void* stream, tho
         launch_level_tables(g, P, lt, ctx->stream);
         CK(cudaGetLastError());
     }
+    {
+        // operator weights of the mixed form, from the geometry just uploaded
+        double* lapw;
+        float*  dmw;
+        if (dev_alloc(ctx, &lapw, (size_t)7 * Np) || dev_alloc(ctx, &dmw, (size_t)84 * Np))
+            return THORX_E_CUDA;
+        g.lapw = lapw;
+        g.dmw  = dmw;
+        launch_stencil_weights(g, lapw, dmw, ctx->stream);
+        CK(cudaGetLastError());
+    }
 
     // state
     State&       s     = ctx->s;

@@ -56,6 +56,14 @@ struct Geometry {
     const double*  Kdh4;
     const double*  Kdhz;
     const double*  lt; // per-level tables, lt[t * nvi + i] (LevelTable below)
+    // Operator weights of the mixed form (stencil_weights_kernel), per column:
+    // lapw [7][Np]: hyperdiffusion Laplacian at rscale = 1; entry 0 = the sum of all seven
+    //   weights, entries 1..6 = the ring's, so lap = w0 a0 + sum_k wk (ak - a0).
+    // dmw [84][Np]: divergence damping, output o (x, y, z) at o * 28: the (Mh) vector part at
+    //   rscale = 1, entries 3 k + comp (k = 0 the centre, as the sum over all points, 1..6 the
+    //   ring), then 7 entries for (Wh below - Wh above) at points 0..6 at rscale = dz = 1.
+    const double*  lapw;
+    const float*   dmw;
 };
 
 // Per-level quantities that every column shares, tabulated once on the device at context
@@ -120,6 +128,7 @@ size_t vertical_smem_bytes(const Geometry& g);
 
 // Fills the per-level tables lt[kLtCount * (nv+1)] (thor_b200/csrc/dyn_fp64.cu).
 void launch_level_tables(const Geometry& g, const Phys& P, double* lt, cudaStream_t st);
+void launch_stencil_weights(const Geometry& g, double* lapw, float* dmw, cudaStream_t st);
 
 // Kernel launchers (thor_b200/csrc/dyn_fp64.cu).
 // ProfX up to the physics modules; with finish, also the pressure update and NaN check, which
