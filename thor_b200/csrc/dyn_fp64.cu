@@ -1,9 +1,12 @@
-// thorx dynamical-core kernels, all-FP64 form, for sm_100a.
+// thorx dynamical-core kernels for sm_100a: the all-FP64 form and the mixed form.
 //
-// Each kernel is a fusion of reference kernels (file:line in the comment above it). The
-// arithmetic of every fused piece follows the reference operation for operation (same operand
-// order and association, same math-library calls), so that the only differences from the
-// reference build are the FMA contractions the compiler chooses.
+// Each kernel is a fusion of reference kernels (file:line in the comment above it). In the FP64
+// form the arithmetic of every fused piece follows the reference operation for operation (same
+// operand order and association, same math-library calls; quotients by the cell areas come from
+// a staged reciprocal but are the IEEE quotients, div_rcp), so that the only differences from the
+// reference build are the FMA contractions the compiler chooses. The mixed form (template
+// compute type float) runs the momentum-side stencils in FP32 and applies the hyperdiffusion and
+// divergence-damping operators through per-column weights (stencil_weights_kernel).
 //
 // Work decomposition: every kernel except ProfX runs on tiles of 32 consecutive columns (one per
 // lane, so that each plane access of a warp is one or two 128-byte lines) times all levels, the
@@ -13,7 +16,7 @@
 // Where the reference carries values down a column loop (Compute_Temperature_H_Pt_Geff,
 // Vertical_Eq, UpdateRK2) each level recomputes what it needs from the neighbouring levels
 // instead, with the same operations, so that all levels run in parallel; only the Thomas
-// elimination itself stays sequential, in shared memory.
+// elimination itself stays sequential, one warp per tile, overlapped with the other warps' work.
 // Neighbours come from the per-column tables described in thorx_internal.h; a hole (-1) reads 0.
 // Stencils are templated on the ring size (6, or 5 at pentagons and poles) so that every index
 // is static and the ring values stay in registers.
@@ -30,18 +33,23 @@ constexpr int kTile      = 32;              // columns per tile (lanes)
 constexpr int kLevGroups = THORX_LEVGROUPS; // warps per tile, each taking every kLevGroups-th level
 constexpr int kColBlock  = 128;
 
-// Register budget of each tiled kernel (__maxnreg__), chosen by timing the g6/L48 step on a B200:
-// the kernels are latency-bound, and a cap of 80 registers lets 3 CTAs of 256 threads (24 warps)
-// share an SM where the uncapped code fits one or two; divm0 keeps 128 (2 CTAs), where tighter
-// caps spill more than the extra warps win back. Overridable with -DTHORX_REGS_<KERNEL>=n.
+// Register budget of each tiled kernel (__maxnreg__), chosen by timing the g6/L48 step on a B200
+// (caps of 64, 72, 80, 96, 112, 128 and 160 for every kernel in both forms): the kernels are
+// latency-bound, and a cap of 80 registers lets 3 CTAs of 256 threads (24 warps) share an SM where
+// the uncapped code fits one or two; adv_temp does best at 72; the FP64 divm0 keeps 128 (2 CTAs),
+// where tighter caps spill more than the extra warps win back, and the mixed form's divm0 (which
+// applies operator weights) 96. Overridable with -DTHORX_REGS_<KERNEL>=n.
 #ifndef THORX_REGS_ADV
-#define THORX_REGS_ADV 80
+#define THORX_REGS_ADV 72
 #endif
 #ifndef THORX_REGS_DIFF
 #define THORX_REGS_DIFF 80
 #endif
 #ifndef THORX_REGS_DIVM
 #define THORX_REGS_DIVM 128
+#endif
+#ifndef THORX_REGS_DIVM_MIXED
+#define THORX_REGS_DIVM_MIXED 96
 #endif
 #ifndef THORX_REGS_SLOW
 #define THORX_REGS_SLOW 80
@@ -54,7 +62,7 @@ constexpr int kColBlock  = 128;
 #endif
 #define THORX_KATTR_ADV __maxnreg__(THORX_REGS_ADV)
 #define THORX_KATTR_DIFF __maxnreg__(THORX_REGS_DIFF)
-#define THORX_KATTR_DIVM __maxnreg__(THORX_REGS_DIVM)
+#define THORX_KATTR_DIVM __maxnreg__(sizeof(R) < sizeof(double) ? THORX_REGS_DIVM_MIXED : THORX_REGS_DIVM)
 #define THORX_KATTR_SLOW __maxnreg__(THORX_REGS_SLOW)
 #define THORX_KATTR_MOM __maxnreg__(THORX_REGS_MOM)
 #define THORX_KATTR_VERT __maxnreg__(THORX_REGS_VERT)
@@ -117,16 +125,15 @@ __device__ __forceinline__ float div_rcp(float a, float b, float y) {
 
 // Shared-memory view of one column's ring geometry, [quantity][32].
 struct SGeo {
-    const double *ar, *at, *ti, *te, *oa, *rat, *ratf;
+    const double *ar, *at, *ti, *te, *oa, *rat;
     int           x;
     __device__ double AR(int q) const { return ar[q * kTile + x]; }
     __device__ double AT(int q) const { return at[q * kTile + x]; }
     __device__ double TI(int q) const { return ti[q * kTile + x]; }
     __device__ double TE(int q) const { return te[q * kTile + x]; }
     __device__ double OA(int q) const { return oa[q * kTile + x]; }
-    // 1 / areasTr rounded to nearest, in double and (for the FP32 stencils) in float
+    // 1 / areasTr rounded to nearest
     __device__ double RAT(int q) const { return rat[q * kTile + x]; }
-    __device__ float  RATF(int q) const { return (float)ratf[q * kTile + x]; }
     // mixed form: the column's operator weights (Geometry::lapw, Geometry::dmw), [entry][32]
     const double* lw;
     const float * lwf, *dm;
@@ -135,8 +142,8 @@ struct SGeo {
 // The mixed form (compute type float) applies the operators through per-column weights.
 template<class R> constexpr bool kOperatorWeights = sizeof(R) < sizeof(double);
 
-// areas 18, areasTr 6, nvecti 18, nvecte 18, nvecoa 18, 1/areasTr 6 (double), 6 (float)
-constexpr int kRingGeoRows = 90;
+// areas 18, areasTr 6, nvecti 18, nvecte 18, nvecoa 18, 1/areasTr 6
+constexpr int kRingGeoRows = 84;
 static_assert(7 * 8 + 7 * 4 <= kRingGeoRows * 8 && 84 * 4 <= kRingGeoRows * 8,
               "operator weights must fit the ring-geometry buffer");
 
@@ -150,10 +157,9 @@ __device__ __forceinline__ SGeo stage_ring_geo(double* sm, const Geometry& g, in
         // a pentagon's sixth entry is 0 and never read; its reciprocal (inf) is not either
         const double at = col >= 0 ? __ldg(g.areasTr + (size_t)q * g.Np + col) : 1.0;
         sm[(78 + q) * kTile + threadIdx.x] = 1.0 / at;
-        sm[(84 + q) * kTile + threadIdx.x] = (double)(1.0f / (float)at);
     }
     return SGeo{sm,       sm + 18 * kTile, sm + 24 * kTile, sm + 42 * kTile, sm + 60 * kTile,
-                sm + 78 * kTile, sm + 84 * kTile, (int)threadIdx.x, nullptr, nullptr, nullptr};
+                sm + 78 * kTile, (int)threadIdx.x, nullptr, nullptr, nullptr};
 }
 
 // Mixed form: the Laplacian weights of the lanes' columns in place of the ring geometry
@@ -190,10 +196,6 @@ __device__ __forceinline__ SGeo stage_divm_geo(double* sm, const Geometry& g, in
         return stage_ring_geo(sm, g, col);
 }
 
-// The staged reciprocal of areasTr in the compute type R.
-template<class R> __device__ __forceinline__ R rat_of(const SGeo& G, int q);
-template<> __device__ __forceinline__ double rat_of<double>(const SGeo& G, int q) { return G.RAT(q); }
-template<> __device__ __forceinline__ float rat_of<float>(const SGeo& G, int q) { return G.RATF(q); }
 
 // ---------------------------------------------------------------------------------------------
 // Per-level tables (LevelTable in thorx_internal.h), one thread per level/interface index. The
@@ -586,12 +588,13 @@ __global__ void THORX_KATTR_ADV adv_temp_kernel(Geometry g, Phys P, State s) {
 // ---------------------------------------------------------------------------------------------
 template<int n, class R>
 __device__ __forceinline__ R laplacian(const SGeo& G, const R* a, R a0, R rscale) {
+    static_assert(sizeof(R) == sizeof(double), "the FP32 stencils apply the operator weights");
     auto AR = [&](int q) { return (R)G.AR(q); };
     auto AT = [&](int q) { return (R)G.AT(q); };
     auto TI = [&](int q) { return (R)G.TI(q); };
     auto TE = [&](int q) { return (R)G.TE(q); };
     auto OA = [&](int q) { return (R)G.OA(q); };
-    auto RAT = [&](int q) { return rat_of<R>(G, q); };
+    auto RAT = [&](int q) { return G.RAT(q); };
     const R h = (R)0.5;
     R       lap = 0;
     R       lap1 = 0, lap2 = 0, lap3 = 0, lapx1 = 0, lapx2 = 0, lapy1 = 0, lapy2 = 0, lapz1 = 0,
@@ -792,12 +795,13 @@ template<int n, class R>
 __device__ __forceinline__ void divm_core(const SGeo& G, const R* a0, const R (*ar)[3], bool with_w,
                                           R wl0, R wt0, const R* wl, const R* wt, R dz, R rscale,
                                           int c2, R* lapo) {
+    static_assert(sizeof(R) == sizeof(double), "the FP32 stencils apply the operator weights");
     auto    AR = [&](int q) { return (R)G.AR(q); };
     auto    AT = [&](int q) { return (R)G.AT(q); };
     auto    TI = [&](int q) { return (R)G.TI(q); };
     auto    TE = [&](int q) { return (R)G.TE(q); };
     auto    OA = [&](int q) { return (R)G.OA(q); };
-    auto    RAT = [&](int q) { return rat_of<R>(G, q); };
+    auto    RAT = [&](int q) { return G.RAT(q); };
     const R h   = (R)0.5;
     const R AT0 = h * rscale;
     R       lapx = 0, lapy = 0, lapz = 0;
@@ -997,26 +1001,27 @@ __device__ __forceinline__ void divm0_point(const Geometry& g, const Phys& P, co
 #pragma unroll
         for (int k = 0; k < 3; k++)
             divg[(k * nv + lev) * Np + c] = (double)out[k];
-        return;
     }
-    R            a0[3], ar[n][3], wl[n], wt[n];
-#pragma unroll
-    for (int k = 0; k < 3; k++)
-        a0[k] = (R)Mh[(k * nv + lev) * Np + c];
-#pragma unroll
-    for (int j = 0; j < n; j++) {
+    else {
+        R            a0[3], ar[n][3], wl[n], wt[n];
 #pragma unroll
         for (int k = 0; k < 3; k++)
-            ar[j][k] = (R)gz(Mh + (k * nv + lev) * Np, ring[j]);
-        wl[j] = (R)gz(Wh + lev * Np, ring[j]);
-        wt[j] = (R)gz(Wh + (lev + 1) * Np, ring[j]);
-    }
-    R out[3];
-    divm_core<n, R>(G, a0, ar, true, (R)Wh[lev * Np + c], (R)Wh[(lev + 1) * Np + c], wl, wt, (R)dz,
-                    (R)rscale, c2, out);
+            a0[k] = (R)Mh[(k * nv + lev) * Np + c];
 #pragma unroll
-    for (int k = 0; k < 3; k++)
-        divg[(k * nv + lev) * Np + c] = (double)out[k];
+        for (int j = 0; j < n; j++) {
+#pragma unroll
+            for (int k = 0; k < 3; k++)
+                ar[j][k] = (R)gz(Mh + (k * nv + lev) * Np, ring[j]);
+            wl[j] = (R)gz(Wh + lev * Np, ring[j]);
+            wt[j] = (R)gz(Wh + (lev + 1) * Np, ring[j]);
+        }
+        R out[3];
+        divm_core<n, R>(G, a0, ar, true, (R)Wh[lev * Np + c], (R)Wh[(lev + 1) * Np + c], wl, wt, (R)dz,
+                        (R)rscale, c2, out);
+#pragma unroll
+        for (int k = 0; k < 3; k++)
+            divg[(k * nv + lev) * Np + c] = (double)out[k];
+    }
 }
 
 // Pass 0 of the divergence damping on (Mh, Wh) -> divg.
@@ -1525,92 +1530,106 @@ __global__ void THORX_KATTR_VERT
     }
     __syncthreads();
 
-    // ---- phase 3: Thomas elimination and back substitution (one warp) ----
-    if (threadIdx.y == 0 && active) {
-        double cprev = 0, dprev = 0;
-        for (int lev = 1; lev < nv; lev++) {
-            const int    q  = lev * Np + c;
-            const double aa = ra[q], bb = rb[q];
-            double       ccv = rc[q], ddv = rd[q];
-            if (lev == 1) {
-                ccv = ccv / bb;
-                ddv = ddv / bb;
+    // ---- phase 3: the Thomas elimination and back substitution (warp 0), while the other warps
+    // compute the horizontal flux divergences of Density_Pressure_Eqs, which do not depend on
+    // the solve, into the shared memory Sp and Sd no longer need ----
+    double*    sFr  = sSp; // rscale * div(Mhs) per level
+    double*    sFpt = sSd; // rscale * div((Mhs + Mhk) pt) (or the energy form's) per level
+    const bool eeq  = P.energy;
+    if (threadIdx.y == 0) {
+        if (active) {
+            double cprev = 0, dprev = 0;
+            for (int lev = 1; lev < nv; lev++) {
+                const int    q  = lev * Np + c;
+                const double aa = ra[q], bb = rb[q];
+                double       ccv = rc[q], ddv = rd[q];
+                if (lev == 1) {
+                    ccv = ccv / bb;
+                    ddv = ddv / bb;
+                }
+                else {
+                    const double t = 1.0 / (bb - cprev * aa);
+                    ccv *= t;
+                    ddv = (ddv - dprev * aa) * t;
+                }
+                rc[q] = ccv;
+                rd[q] = ddv;
+                cprev = ccv;
+                dprev = ddv;
             }
-            else {
-                const double t = 1.0 / (bb - cprev * aa);
-                ccv *= t;
-                ddv = (ddv - dprev * aa) * t;
+            double w           = 0.0;
+            s.Whs[nv * Np + c] = 0.0;
+            for (int lev = nv - 1; lev > 0; lev--) {
+                const int q = lev * Np + c;
+                w           = (lev == nv - 1) ? rd[q] : (-rc[q] * w + rd[q]);
+                s.Whs[q]    = w;
             }
-            rc[q] = ccv;
-            rd[q] = ddv;
-            cprev = ccv;
-            dprev = ddv;
+            s.Whs[c] = 0.0;
         }
-        double w           = 0.0;
-        s.Whs[nv * Np + c] = 0.0;
-        for (int lev = nv - 1; lev > 0; lev--) {
-            const int q = lev * Np + c;
-            w           = (lev == nv - 1) ? rd[q] : (-rc[q] * w + rd[q]);
-            s.Whs[q]    = w;
+    }
+    else if (active) {
+        for (int lev = threadIdx.y - 1; lev < nv; lev += kLevGroups - 1) {
+            const double rscale = deep ? lt[kLtRscale * nvi + lev] : 1.0;
+            double       sr[3], st[3];
+#pragma unroll
+            for (int j = 0; j < 7; j++) {
+                const int id = nb[j];
+                double    vs[3] = {0.0, 0.0, 0.0}, v1[3] = {0.0, 0.0, 0.0}, ptv = 0.0;
+                if (id >= 0) {
+#pragma unroll
+                    for (int k = 0; k < 3; k++) {
+                        vs[k] = s.Mhs[(k * nv + lev) * Np + id];
+                        v1[k] = vs[k] + s.Mhk[(k * nv + lev) * Np + id];
+                    }
+                    const int q = lev * Np + id;
+                    ptv         = eeq ? (s.h[q] + s.ep[q] + s.ek[q]) : s.pt[q];
+                }
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    const double d = sdiv[(j * 3 + k) * kTile + x];
+                    if (j == 0) {
+                        sr[k] = d * vs[k];
+                        st[k] = d * v1[k] * ptv;
+                    }
+                    else {
+                        sr[k] = sr[k] + d * vs[k];
+                        st[k] = st[k] + d * v1[k] * ptv;
+                    }
+                }
+            }
+            double nflxr = 0.0, nflxpt = 0.0;
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                nflxr += rscale * sr[k];
+                nflxpt += rscale * st[k];
+            }
+            sFr[lev * kTile + x]  = nflxr;
+            sFpt[lev * kTile + x] = nflxpt;
         }
-        s.Whs[c] = 0.0;
     }
     __syncthreads();
     if (!active)
         return;
 
-    // ---- phase 4: Density_Pressure_Eqs ----
-    const bool   eeq   = P.energy;
+    // ---- phase 4: Density_Pressure_Eqs, vertical terms and the update ----
     const double P_Ref = P.P_Ref;
     for (int lev = threadIdx.y; lev < nv; lev += kLevGroups) {
         const int    i     = lev * Np + c;
         const double Cv    = s.Cp[i] - s.Rd[i];
         const double dz    = Alth[lev + 1] - Alth[lev];
-        double       r2p, r2m, r2l, rscale, dr2dz;
+        double       r2p, r2m, r2l, dr2dz;
         if (deep) {
             r2p    = lt[kLtR2hD * nvi + lev + 1];
             r2m    = lt[kLtR2cD * nvi + lev];
             r2l    = lt[kLtR2hD * nvi + lev];
-            rscale = lt[kLtRscale * nvi + lev];
             dr2dz  = lt[kLtDr2dz * nvi + lev];
         }
         else {
-            r2p = r2m = r2l = rscale = 1.0;
-            dr2dz                    = r2m * dz;
+            r2p = r2m = r2l = 1.0;
+            dr2dz           = r2m * dz;
         }
-        double sr[3], st[3];
-#pragma unroll
-        for (int j = 0; j < 7; j++) {
-            const int id = nb[j];
-            double    vs[3] = {0.0, 0.0, 0.0}, v1[3] = {0.0, 0.0, 0.0}, ptv = 0.0;
-            if (id >= 0) {
-#pragma unroll
-                for (int k = 0; k < 3; k++) {
-                    vs[k] = s.Mhs[(k * nv + lev) * Np + id];
-                    v1[k] = vs[k] + s.Mhk[(k * nv + lev) * Np + id];
-                }
-                const int q = lev * Np + id;
-                ptv         = eeq ? (s.h[q] + s.ep[q] + s.ek[q]) : s.pt[q];
-            }
-#pragma unroll
-            for (int k = 0; k < 3; k++) {
-                const double d = sdiv[(j * 3 + k) * kTile + x];
-                if (j == 0) {
-                    sr[k] = d * vs[k];
-                    st[k] = d * v1[k] * ptv;
-                }
-                else {
-                    sr[k] = sr[k] + d * vs[k];
-                    st[k] = st[k] + d * v1[k] * ptv;
-                }
-            }
-        }
-        double nflxr = 0.0, nflxpt = 0.0;
-#pragma unroll
-        for (int k = 0; k < 3; k++) {
-            nflxr += rscale * sr[k];
-            nflxpt += rscale * st[k];
-        }
+        double       nflxr  = sFr[lev * kTile + x];
+        const double nflxpt = sFpt[lev * kTile + x];
         auto phv = [&](int l) -> double {
             const int q = l * Np + c;
             return eeq ? (s.hh[q] + s.eph[q] + s.ekh[q]) : s.pth[q];
