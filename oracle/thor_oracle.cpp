@@ -1704,7 +1704,11 @@ extern "C" void* oracle_new(const oracle_grid* g, const oracle_params* p) {
     int N = o->N, nv = o->nv, nvi = o->nvi;
     o->maps.assign(g->maps, g->maps + (size_t)(o->nl + 2) * (o->nl + 2) * o->nr);
     o->point_local.assign(g->point_local, g->point_local + (size_t)6 * N);
+    // one entry past the top layer, 0: Compute_Temperature_H_Pt_Geff reads Altitude[nv] at the
+    // top boundary with GravHeightVar (src/headers/dyn/thor_auxiliary.h:195-198, lev == nv), one
+    // past the reference's nv-entry array, where its fresh device allocation holds zero
     o->Altitude.assign(g->Altitude, g->Altitude + nv);
+    o->Altitude.push_back(0.0);
     o->Altitudeh.assign(g->Altitudeh, g->Altitudeh + nvi);
     o->lonlat.assign(g->lonlat, g->lonlat + 2 * (size_t)N);
     o->areas.assign(g->areas, g->areas + 18 * (size_t)N);

@@ -348,9 +348,17 @@ __device__ __forceinline__ double pot_temp(const ColLevel& q, double P_Ref) {
 
 __global__ void THORX_KATTR_ADV adv_temp_kernel(Geometry g, Phys P, State s) {
     __shared__ double sdiv[21 * kTile];
+    __shared__ double sfr[21 * kTile]; // func_r of the 7 stencil points, [point * 3 + k][32]
     const int         c0 = blockIdx.x * kTile, x = threadIdx.x, c = c0 + x;
     const int         Np = g.Np, nv = g.nv;
     stage(sdiv, g.div, 21, Np, c0);
+    for (int q = threadIdx.y; q < 21; q += blockDim.y) {
+        const int j = q / 3, k = q % 3;
+        int       id = -1;
+        if (c < g.N)
+            id = j == 0 ? c : g.nb[(j - 1) * Np + c];
+        sfr[q * kTile + x] = gz(g.func_r + k * Np, id);
+    }
     __syncthreads();
     if (c >= g.N)
         return;
@@ -359,19 +367,23 @@ __global__ void THORX_KATTR_ADV adv_temp_kernel(Geometry g, Phys P, State s) {
     const double  A = P.A, Omega = P.Omega, P_Ref = P.P_Ref, Gravit = P.Gravit;
     const bool    eeq = P.energy, ghv = P.GravHeightVar;
 
-    int nb[7];
+    const double* lt = g.lt;
+    const int     nvi = g.nvi;
+    int           nb[7];
     nb[0] = c;
     for (int j = 0; j < 6; j++)
         nb[j + 1] = g.nb[j * Np + c];
-    double fr[7][3];
-    for (int j = 0; j < 7; j++)
+    auto fr = [&](int j, int k) { return sfr[(j * 3 + k) * kTile + x]; };
+    // v = M / rho + (w / rho) r^, the quotients from one reciprocal of rho (div_rcp: IEEE quotients)
+    auto vel = [&](const double* M, double rho, double w, int j, double* v) {
+        const double yr = 1.0 / rho, wr = div_rcp(w, rho, yr);
         for (int k = 0; k < 3; k++)
-            fr[j][k] = gz(g.func_r + k * Np, nb[j]);
-
+            v[k] = div_rcp(M[k], rho, yr) + wr * fr(j, k);
+    };
     auto vown = [&](int lev, double* v) {
-        double rho = s.Rhok[lev * Np + c], w = s.Wk[lev * Np + c];
-        for (int k = 0; k < 3; k++)
-            v[k] = s.Mhk[(k * nv + lev) * Np + c] / rho + (w / rho) * fr[0][k];
+        const double M[3] = {s.Mhk[(0 * nv + lev) * Np + c], s.Mhk[(1 * nv + lev) * Np + c],
+                             s.Mhk[(2 * nv + lev) * Np + c]};
+        vel(M, s.Rhok[lev * Np + c], s.Wk[lev * Np + c], 0, v);
     };
     // kinetic energy per mass of the column at a level (thor_auxiliary.h:152-157)
     auto ekin = [&](int lev) {
@@ -381,7 +393,7 @@ __global__ void THORX_KATTR_ADV adv_temp_kernel(Geometry g, Phys P, State s) {
         return 0.5 * (m0 * m0 + m1 * m1 + m2 * m2 + w * w) / (r * r);
     };
     auto epot = [&](int lev) {
-        return ghv ? Gravit * pow(A / (A + Alt[lev]), 2) * Alt[lev] : Gravit * Alt[lev];
+        return ghv ? Gravit * lt[kLtGhv * nvi + lev] * Alt[lev] : Gravit * Alt[lev];
     };
     // velocity-weighted effective gravity at interior interface i (thor_auxiliary.h:288-289)
     auto gtil_w = [&](int i) -> double {
@@ -390,8 +402,7 @@ __global__ void THORX_KATTR_ADV adv_temp_kernel(Geometry g, Phys P, State s) {
         const ColLevel lo = col_level(s, Np, i - 1, c), hi = col_level(s, Np, i, c);
         const double   dz    = Alt[i] - Alt[i - 1];
         const double   dp_dz = (hi.p - lo.p) / dz;
-        const double   xi = Alth[i], xim = Alt[i - 1], xip = Alt[i];
-        const double   intt = (xi - xip) / (xim - xip), intl = (xi - xim) / (xip - xim);
+        const double   intt = lt[kLtHIntt * nvi + i], intl = lt[kLtHIntl * nvi + i];
         const double   rhoh = lo.rho * intt + hi.rho * intl;
         return -(s.Whk[i * Np + c] / rhoh) * dp_dz;
     };
@@ -399,62 +410,59 @@ __global__ void THORX_KATTR_ADV adv_temp_kernel(Geometry g, Phys P, State s) {
     for (int lev = threadIdx.y; lev < nv; lev += kLevGroups) {
         const int    i      = lev * Np + c;
         const double rscale = rscale_of(P, g, lev);
-        // ---- horizontal flux divergence of v (x) M over the 7-point stencil ----
-        double M[7][3], V[7][3];
+        // ---- horizontal flux divergence of v (x) M over the 7-point stencil: nine running sums
+        // sum[kk][cc] over the points j in order, one point's M and v at a time ----
+        double sum[3][3], vcur[3];
 #pragma unroll
         for (int j = 0; j < 7; j++) {
             const int id = nb[j];
+            double    M[3] = {0.0, 0.0, 0.0}, V[3] = {0.0, 0.0, 0.0};
             if (id >= 0) {
-                const double rho = s.Rhok[lev * Np + id], w = s.Wk[lev * Np + id];
-#pragma unroll
-                for (int k = 0; k < 3; k++) {
-                    M[j][k] = s.Mhk[(k * nv + lev) * Np + id];
-                    V[j][k] = M[j][k] / rho + (w / rho) * fr[j][k];
-                }
-            }
-            else {
 #pragma unroll
                 for (int k = 0; k < 3; k++)
-                    M[j][k] = V[j][k] = 0.0;
+                    M[k] = s.Mhk[(k * nv + lev) * Np + id];
+                vel(M, s.Rhok[lev * Np + id], s.Wk[lev * Np + id], j, V);
             }
+            if (j == 0)
+                for (int k = 0; k < 3; k++)
+                    vcur[k] = V[k];
+#pragma unroll
+            for (int kk = 0; kk < 3; kk++)
+#pragma unroll
+                for (int cc = 0; cc < 3; cc++) {
+                    const double t = sdiv[(j * 3 + kk) * kTile + x] * V[cc] * M[kk];
+                    sum[kk][cc]    = (j == 0) ? t : sum[kk][cc] + t;
+                }
         }
         double nflx[3] = {0.0, 0.0, 0.0};
 #pragma unroll
         for (int kk = 0; kk < 3; kk++)
 #pragma unroll
-            for (int cc = 0; cc < 3; cc++) {
-                double sum = sdiv[kk * kTile + x] * V[0][cc] * M[0][kk];
-#pragma unroll
-                for (int j = 1; j < 7; j++)
-                    sum = sum + sdiv[(j * 3 + kk) * kTile + x] * V[j][cc] * M[j][kk];
-                nflx[cc] += rscale * sum;
-            }
+            for (int cc = 0; cc < 3; cc++)
+                nflx[cc] += rscale * sum[kk][cc];
         // ---- vertical flux of v w at the interfaces + Coriolis ----
-        const double* vcur = V[0];
         double        vprev[3] = {0, 0, 0}, vnext[3] = {0, 0, 0};
         const double  altht = Alth[lev + 1], althl = Alth[lev], alt = Alt[lev];
         double        dvwl[3] = {0, 0, 0}, dvwt[3] = {0, 0, 0};
         if (lev > 0) {
             vown(lev - 1, vprev);
-            const double xi = althl, xim = Alt[lev - 1], xip = alt;
-            const double intt = (xi - xip) / (xim - xip), intl = (xi - xim) / (xip - xim);
+            const double intt = lt[kLtHIntt * nvi + lev], intl = lt[kLtHIntl * nvi + lev];
             const double whl = s.Whk[lev * Np + c];
             for (int k = 0; k < 3; k++)
                 dvwl[k] = (vprev[k] * intt + vcur[k] * intl) * whl;
         }
         if (lev < nv - 1) {
             vown(lev + 1, vnext);
-            const double xi = altht, xim = alt, xip = Alt[lev + 1];
-            const double intt = (xi - xip) / (xim - xip), intl = (xi - xim) / (xip - xim);
+            const double intt = lt[kLtHIntt * nvi + lev + 1], intl = lt[kLtHIntl * nvi + lev + 1];
             const double wht = s.Whk[(lev + 1) * Np + c];
             for (int k = 0; k < 3; k++)
                 dvwt[k] = (vcur[k] * intt + vnext[k] * intl) * wht;
         }
         double r2p = 1.0, r2m = 1.0, r2l = 1.0;
         if (P.DeepModel) {
-            r2p = pow(altht + A, 2.0);
-            r2m = pow(alt + A, 2.0);
-            r2l = pow(althl + A, 2.0);
+            r2p = lt[kLtR2hD * nvi + lev + 1];
+            r2m = lt[kLtR2cD * nvi + lev];
+            r2l = lt[kLtR2hD * nvi + lev];
         }
         const double dz  = 1.0 / ((althl - altht) * r2m);
         const double rho = s.Rhok[i];
@@ -465,7 +473,7 @@ __global__ void THORX_KATTR_ADV adv_temp_kernel(Geometry g, Phys P, State s) {
             C[2] = 0.0;
         }
         else {
-            const double* f = fr[0];
+            const double f[3] = {fr(0, 0), fr(0, 1), fr(0, 2)};
             C[0] = 2 * Omega * (vcur[2] * f[2] * f[1] - vcur[1] * pow(f[2], 2)) * rho;
             C[1] = -2 * Omega * (vcur[2] * f[2] * f[0] - vcur[0] * pow(f[2], 2)) * rho;
             C[2] = 2 * Omega * (vcur[1] * f[2] * f[0] - vcur[0] * f[2] * f[1]) * rho;
@@ -498,8 +506,7 @@ __global__ void THORX_KATTR_ADV adv_temp_kernel(Geometry g, Phys P, State s) {
             const ColLevel lo    = col_level(s, Np, lev - 1, c);
             const double   dzl   = alt - Alt[lev - 1];
             const double   dp_dz = (q.p - lo.p) / dzl;
-            const double   xi = althl, xim = Alt[lev - 1], xip = alt;
-            const double   intt = (xi - xip) / (xim - xip), intl = (xi - xim) / (xip - xim);
+            const double   intt = lt[kLtHIntt * nvi + lev], intl = lt[kLtHIntl * nvi + lev];
             s.hh[i] = enthalpy(lo) * intt + h * intl;
             if (eeq) {
                 s.eph[i] = epot(lev - 1) * intt + ep * intl;
@@ -529,8 +536,7 @@ __global__ void THORX_KATTR_ADV adv_temp_kernel(Geometry g, Phys P, State s) {
         // where the reference interpolates with the top layer's own geometry)
         {
             const int    L1   = (lev < nv - 1) ? lev + 1 : lev;
-            const double xi   = Alt[L1], xim = Alth[L1], xip = Alth[L1 + 1];
-            const double intt = (xi - xip) / (xim - xip), intl = (xi - xim) / (xip - xim);
+            const double intt = lt[kLtCIntt * nvi + L1], intl = lt[kLtCIntl * nvi + L1];
             const double gw0  = gtil_w(lev);
             const double gw1  = (lev < nv - 1) ? gtil_w(lev + 1) : 0.0;
             s.gtil[i]         = gw0 * intt + gw1 * intl;

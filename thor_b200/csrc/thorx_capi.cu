@@ -612,8 +612,12 @@ int thorx_create(const thorx_grid* gr, const thorx_params* pr, void* stream, tho
             kdh4[lev]   = (pr->Diffc) * pow(dbar, 1.0 * pr->HyDiffOrder) / P.timestep;
             kdhz[lev]   = (pr->DivDampc) * pow(dbar, 4.) / P.timestep;
         }
+        // Altitude gets one zero entry past the top layer: Compute_Temperature_H_Pt_Geff reads
+        // Altitude[nv] at the top boundary with GravHeightVar (src/headers/dyn/thor_auxiliary.h:
+        // 195-198, lev == nv), one past the reference's nv-entry array, where its fresh device
+        // allocation holds zero; here the read stays in bounds and sees that value
         double *a, *b, *alt, *alth;
-        if (dev_alloc(ctx, &a, nv) || dev_alloc(ctx, &b, nv) || dev_alloc(ctx, &alt, nv)
+        if (dev_alloc(ctx, &a, nv) || dev_alloc(ctx, &b, nv) || dev_alloc(ctx, &alt, nv + 1)
             || dev_alloc(ctx, &alth, nv + 1))
             return THORX_E_CUDA;
         CK(cudaMemcpy(a, kdh4.data(), nv * 8, cudaMemcpyHostToDevice));
