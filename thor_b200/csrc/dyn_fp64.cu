@@ -71,8 +71,9 @@ __device__ __forceinline__ double gz(const double* __restrict__ plane, int id) {
     return id >= 0 ? __ldg(plane + id) : 0.0;
 }
 
-__device__ __forceinline__ double rscale_of(const Phys& P, const Geometry& g, int lev) {
-    return P.DeepModel ? P.A / (g.Altitude[lev] + P.A) : 1.0;
+// DeepModel ? A / (Altitude + A) : 1, from the level table that holds that expression's value
+__device__ __forceinline__ double rscale_of(const Phys&, const Geometry& g, int lev) {
+    return g.lt[kLtRscale * g.nvi + lev];
 }
 
 // Copies rows 0..Q-1 of a [q][Np] grid array for the tile's 32 columns into smem [q][32].
@@ -677,10 +678,10 @@ __device__ __forceinline__ void diffusion_point(const Geometry& g, const Phys& P
                                                 const SGeo& G, const double* fr, const int* ring,
                                                 const double* __restrict__ diff_in,
                                                 double* __restrict__ diff_out, int stepnum,
-                                                bool last, int c, int lev) {
+                                                bool last, int c, int lev, double sign4) {
     const int    Np = g.Np, nv = g.nv;
     const double rscale = rscale_of(P, g, lev);
-    const double sdiff  = -g.Kdh4[lev] * pow(-1.0, P.HyDiffOrder / 2);
+    const double sdiff  = -g.Kdh4[lev] * sign4;
     const bool   eeq    = P.energy;
     int          ids[n + 1];
     double       rho[n + 1];
@@ -722,12 +723,7 @@ __device__ __forceinline__ void diffusion_point(const Geometry& g, const Phys& P
             }
             a[j] = v;
         }
-        double lap;
-        if constexpr (kOperatorWeights<R>) // mixed form: v and w in float, rho and T in double
-            lap = (var >= 1 && var <= 4) ? laplacian_w<n, float>(G, a, rscale)
-                                         : laplacian_w<n, double>(G, a, rscale);
-        else
-            lap = laplacian<n, double>(G, a + 1, a[0], rscale);
+        double lap = laplacian<n, double>(G, a + 1, a[0], rscale);
         if (!last) {
             diff_out[(var * nv + lev) * Np + c] = lap;
             continue;
@@ -754,6 +750,95 @@ __device__ __forceinline__ void diffusion_point(const Geometry& g, const Phys& P
     }
 }
 
+// Mixed form: the six Laplacians of one (column, level) in one pass over the stencil points. With
+// the operator weights each Laplacian is a running sum, so the values of all six variables at a
+// point are loaded together; each sum keeps laplacian_w's order (centre weight, then the ring in
+// order), v and w in float, rho and T in double.
+template<int n>
+__device__ __forceinline__ void diffusion_point_w(const Geometry& g, const Phys& P, const State& s,
+                                                  const SGeo& G, const double* fr, const int* ring,
+                                                  const double* __restrict__ diff_in,
+                                                  double* __restrict__ diff_out, int stepnum,
+                                                  bool last, int c, int lev, double sign4) {
+    const int    Np = g.Np, nv = g.nv, x = G.x;
+    const double rscale = rscale_of(P, g, lev);
+    const bool   eeq    = P.energy;
+    // the six variables at point id (0 at a hole), as the FP64 form forms them
+    auto point = [&](int id, double* v) {
+#pragma unroll
+        for (int var = 0; var < 6; var++)
+            v[var] = 0.0;
+        if (id < 0)
+            return;
+        const int q = lev * Np + id;
+        if (stepnum == 0) { // quotients by rho from one reciprocal (div_rcp: IEEE quotients)
+            const double rho = s.Rhok[q], yr = 1.0 / rho;
+            v[0]             = rho;
+#pragma unroll
+            for (int k = 0; k < 3; k++)
+                v[1 + k] = div_rcp(s.Mhk[(k * nv + lev) * Np + id], rho, yr);
+            v[4] = div_rcp(s.Wk[q], rho, yr);
+            v[5] = eeq ? (s.Cp[q] - s.Rd[q]) * s.T[q] : s.Rd[q] * s.T[q];
+        }
+        else {
+#pragma unroll
+            for (int var = 0; var < 6; var++)
+                v[var] = diff_in[(var * nv + lev) * Np + id];
+            if (last) {
+                const double rho = s.Rhok[q];
+#pragma unroll
+                for (int var = 1; var < 6; var++)
+                    v[var] = v[var] * rho;
+            }
+        }
+    };
+    double a0[6];
+    point(c, a0);
+    double accd0 = G.lw[x] * a0[0], accd5 = G.lw[x] * a0[5];
+    float  accf[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+        accf[k] = G.lwf[x] * (float)a0[1 + k];
+#pragma unroll 2
+    for (int j = 1; j <= n; j++) {
+        double v[6];
+        point(__ldg(g.ring + (j - 1) * Np + c), v);
+        const double w  = G.lw[j * kTile + x];
+        const float  wf = G.lwf[j * kTile + x];
+        accd0           = fma(w, v[0] - a0[0], accd0);
+        accd5           = fma(w, v[5] - a0[5], accd5);
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            accf[k] = fmaf(wf, (float)(v[1 + k] - a0[1 + k]), accf[k]);
+    }
+    const double sc = rscale * rscale;
+    double       lap[6];
+    lap[0] = accd0 * sc;
+    lap[5] = accd5 * sc;
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+        lap[1 + k] = (double)(accf[k] * (float)sc);
+    if (!last) {
+#pragma unroll
+        for (int var = 0; var < 6; var++)
+            diff_out[(var * nv + lev) * Np + c] = lap[var];
+        return;
+    }
+    const double sdiff = -g.Kdh4[lev] * sign4;
+    const int    i     = lev * Np + c;
+#pragma unroll
+    for (int var = 0; var < 6; var++)
+        lap[var] *= sdiff;
+    s.diffrh[i] = lap[0];
+    // Correct_Horizontal: remove the radial component of the momentum diffusion
+    const double dmhr = fr[0] * lap[1] + fr[1] * lap[2] + fr[2] * lap[3];
+    s.diffmh[(0 * nv + lev) * Np + c] = lap[1] + -fr[0] * dmhr;
+    s.diffmh[(1 * nv + lev) * Np + c] = lap[2] + -fr[1] * dmhr;
+    s.diffmh[(2 * nv + lev) * Np + c] = lap[3] + -fr[2] * dmhr;
+    s.diffw[i]                        = lap[4];
+    s.diffpr[i]                       = lap[5];
+}
+
 template<int n, class R>
 __device__ __forceinline__ void diffusion_body(const Geometry& g, const Phys& P, const State& s,
                                                const SGeo& G, const double* __restrict__ diff_in,
@@ -766,8 +851,12 @@ __device__ __forceinline__ void diffusion_body(const Geometry& g, const Phys& P,
     int ring[6];
     for (int j = 0; j < 6; j++)
         ring[j] = g.ring[j * Np + c];
+    const double sign4 = pow(-1.0, P.HyDiffOrder / 2); // (-1)^(order/2) of the last pass
     for (int lev = threadIdx.y; lev < g.nv; lev += kLevGroups)
-        diffusion_point<n, R>(g, P, s, G, fr, ring, diff_in, diff_out, stepnum, last, c, lev);
+        if constexpr (kOperatorWeights<R>)
+            diffusion_point_w<n>(g, P, s, G, fr, ring, diff_in, diff_out, stepnum, last, c, lev, sign4);
+        else
+            diffusion_point<n, R>(g, P, s, G, fr, ring, diff_in, diff_out, stepnum, last, c, lev, sign4);
 }
 
 // R: compute type of the momentum and w Laplacians (double; float in the mixed form).
@@ -1112,10 +1201,11 @@ template<int n, class R>
 __device__ __forceinline__ void slow_modes_body(const Geometry& g, const Phys& P, const State& s,
                                                 const SGeo& G, const double* sdiv,
                                                 const double* sgrad, bool update_rk, int c) {
-    const int    x = threadIdx.x;
-    const int    Np = g.Np, nv = g.nv;
-    const double A = P.A, Gravit = P.Gravit;
-    int          nb[7], ring[6];
+    const int     x = threadIdx.x;
+    const int     Np = g.Np, nv = g.nv, nvi = g.nvi;
+    const double  A = P.A, Gravit = P.Gravit;
+    const double* lt = g.lt;
+    int           nb[7], ring[6];
     nb[0] = c;
     for (int j = 0; j < 6; j++) {
         nb[j + 1] = g.nb[j * Np + c];
@@ -1160,41 +1250,47 @@ __device__ __forceinline__ void slow_modes_body(const Geometry& g, const Phys& P
         }
         const double dz = altht - althl;
         double       r2p, r2m, r2l, rscale, dr2dz;
-        if (P.DeepModel) {
-            r2p    = pow(altht + A, 2.0);
-            r2m    = pow(alt + A, 2.0);
-            r2l    = pow(althl + A, 2.0);
-            rscale = A / (alt + A);
-            dr2dz  = (pow(altht + A, 3.0) - pow(althl + A, 3.0)) / 3;
+        if (P.DeepModel) { // the level tables hold these expressions' values
+            r2p    = lt[kLtR2hD * nvi + lev + 1];
+            r2m    = lt[kLtR2cD * nvi + lev];
+            r2l    = lt[kLtR2hD * nvi + lev];
+            rscale = lt[kLtRscale * nvi + lev];
+            dr2dz  = lt[kLtDr2dz * nvi + lev];
         }
         else {
             r2p = r2m = r2l = rscale = 1.0;
             dr2dz                    = r2m * dz;
         }
-        // horizontal stencils at this level
-        double pv[7], hv[7], Mv[7][3];
+        // horizontal stencils at this level: running sums over the points in order, one point's
+        // p, h and M at a time
+        double sg[3], sd[3], sp3[3], pv0 = 0.0;
 #pragma unroll
         for (int j = 0; j < 7; j++) {
-            pv[j] = gz(s.pk + lev * Np, nb[j]);
-            hv[j] = gz(s.h + lev * Np, nb[j]);
+            const double pv = gz(s.pk + lev * Np, nb[j]), hv = gz(s.h + lev * Np, nb[j]);
+            if (j == 0)
+                pv0 = pv;
 #pragma unroll
-            for (int k = 0; k < 3; k++)
-                Mv[j][k] = gz(s.Mhk + (k * nv + lev) * Np, nb[j]);
+            for (int k = 0; k < 3; k++) {
+                const double Mv = gz(s.Mhk + (k * nv + lev) * Np, nb[j]);
+                const double dk = sdiv[(j * 3 + k) * kTile + x], gk = sgrad[(j * 3 + k) * kTile + x];
+                if (j == 0) {
+                    sg[k]  = gk * pv;
+                    sd[k]  = dk * Mv;
+                    sp3[k] = dk * Mv * hv;
+                }
+                else {
+                    sg[k]  = sg[k] + gk * pv;
+                    sd[k]  = sd[k] + dk * Mv;
+                    sp3[k] = sp3[k] + dk * Mv * hv;
+                }
+            }
         }
         double nflxv[3], nflxr = 0.0, nflxp = 0.0;
 #pragma unroll
         for (int k = 0; k < 3; k++) {
-            double sg = sgrad[k * kTile + x] * pv[0], sd = sdiv[k * kTile + x] * Mv[0][k],
-                   sp = sdiv[k * kTile + x] * Mv[0][k] * hv[0];
-#pragma unroll
-            for (int j = 1; j < 7; j++) {
-                sg = sg + sgrad[(j * 3 + k) * kTile + x] * pv[j];
-                sd = sd + sdiv[(j * 3 + k) * kTile + x] * Mv[j][k];
-                sp = sp + sdiv[(j * 3 + k) * kTile + x] * Mv[j][k] * hv[j];
-            }
-            nflxv[k] = rscale * sg;
-            nflxr += rscale * sd;
-            nflxp += rscale * sp;
+            nflxv[k] = rscale * sg[k];
+            nflxr += rscale * sd[k];
+            nflxp += rscale * sp3[k];
         }
         double whl, wht, hhl, hht;
         if (lev == 0) {
@@ -1221,27 +1317,26 @@ __device__ __forceinline__ void slow_modes_body(const Geometry& g, const Phys& P
             s.SlowWh[nv * Np + c] = 0.0;
         }
         else {
-            const double xi = althl, xim = altl, xip = alt;
-            const double intt = (xi - xip) / (xim - xip), intl = (xi - xim) / (xip - xim);
+            const double intt = lt[kLtHIntt * nvi + lev], intl = lt[kLtHIntl * nvi + lev];
             double       swr;
             if (P.DeepModel) {
                 if (P.GravHeightVar)
-                    swr = (advrl + rhol * Gravit * pow(A / (A + altl), 2)) * intt
-                          + (advr + rho * Gravit * pow(A / (A + alt), 2)) * intl;
+                    swr = (advrl + rhol * Gravit * lt[kLtGhv * nvi + lev - 1]) * intt
+                          + (advr + rho * Gravit * lt[kLtGhv * nvi + lev]) * intl;
                 else
                     swr = (advrl + rhol * Gravit) * intt + (advr + rho * Gravit) * intl;
             }
             else {
                 if (P.GravHeightVar)
-                    swr = (rhol * Gravit * pow(A / (A + altl), 2)) * intt
-                          + (rho * Gravit * pow(A / (A + alt), 2)) * intl;
+                    swr = (rhol * Gravit * lt[kLtGhv * nvi + lev - 1]) * intt
+                          + (rho * Gravit * lt[kLtGhv * nvi + lev]) * intl;
                 else
                     swr = (rhol * Gravit) * intt + (rho * Gravit) * intl;
             }
             if (P.NonHydro)
                 swr += (-s.diffw[i - Np]) * intt + (-s.diffw[i]) * intl;
             const double dz2  = alt - altl;
-            const double dpdz = (pv[0] - pressurel) / dz2;
+            const double dpdz = (pv0 - pressurel) / dz2;
             swr += dpdz;
             swr -= s.dWh[lev * Np + c];
             s.SlowWh[lev * Np + c] = -swr;
@@ -1370,12 +1465,15 @@ __global__ void THORX_KATTR_MOM
 // Phase 1 (all levels in parallel): Sp, Sd at every level -> shared memory.
 // Phase 2 (all interfaces in parallel): the tridiagonal row (aa, bb, cc, -C0) of every interior
 //   interface, from the column's values at the two adjacent levels and Sp, Sd -> s.vrows.
-// Phase 3 (one warp, lane = column): the Thomas elimination and back substitution over the rows
-//   of its column, with the reference's operation sequence; Whs -> global.
+// Phase 3 (warp 0, lane = column): the Thomas elimination and back substitution over the rows
+//   of its column, with the reference's operation sequence; Whs -> global. Meanwhile warps 1..7
+//   compute the horizontal flux divergences of phase 4 (they do not depend on the solve).
 // Phase 4 (all levels in parallel): the density and pressure update.
 // The rows go through global memory (they stay in L1/L2: the same CTA writes and reads them
-// across a barrier) so that shared memory holds only div [21][32] and Sp/Sd [2][nv][32], and
-// several CTAs fit on an SM. Level-only factors come from the per-level tables.
+// across a barrier); the eliminated coefficients c', d' go to shared memory, so that no global
+// store orders the sweep's row loads. Shared memory: div [21][32], Sp/Sd (then the flux
+// divergences) [2][nv][32] and c'/d' [2][nv][32], 55 KB at nv = 48, three CTAs per SM.
+// Level-only factors come from the per-level tables.
 // ---------------------------------------------------------------------------------------------
 __global__ void THORX_KATTR_VERT
     vertical_kernel(Geometry g, Phys P, State s, double deltat) {
@@ -1384,6 +1482,8 @@ __global__ void THORX_KATTR_VERT
     double*   sdiv = smem;
     double*   sSp  = sdiv + 21 * kTile;
     double*   sSd  = sSp + nv * kTile;
+    double*   sCp  = sSd + nv * kTile; // eliminated Thomas coefficients c', d' [nv][32]
+    double*   sDp  = sCp + nv * kTile;
     const int c0 = blockIdx.x * kTile, x = threadIdx.x, c = c0 + x;
     stage(sdiv, g.div, 21, Np, c0);
     __syncthreads();
@@ -1544,7 +1644,12 @@ __global__ void THORX_KATTR_VERT
     const bool eeq  = P.energy;
     if (threadIdx.y == 0) {
         if (active) {
-            double cprev = 0, dprev = 0;
+            // the eliminated coefficients go to shared memory: no store to global memory inside
+            // the sweep, so the row loads of later interfaces are free to be issued early
+            double* sc = sCp;
+            double* sd = sDp;
+            double  cprev = 0, dprev = 0;
+#pragma unroll 4
             for (int lev = 1; lev < nv; lev++) {
                 const int    q  = lev * Np + c;
                 const double aa = ra[q], bb = rb[q];
@@ -1558,17 +1663,17 @@ __global__ void THORX_KATTR_VERT
                     ccv *= t;
                     ddv = (ddv - dprev * aa) * t;
                 }
-                rc[q] = ccv;
-                rd[q] = ddv;
+                sc[lev * kTile + x] = ccv;
+                sd[lev * kTile + x] = ddv;
                 cprev = ccv;
                 dprev = ddv;
             }
             double w           = 0.0;
             s.Whs[nv * Np + c] = 0.0;
             for (int lev = nv - 1; lev > 0; lev--) {
-                const int q = lev * Np + c;
-                w           = (lev == nv - 1) ? rd[q] : (-rc[q] * w + rd[q]);
-                s.Whs[q]    = w;
+                const double cc = sc[lev * kTile + x], dd = sd[lev * kTile + x];
+                w               = (lev == nv - 1) ? dd : (-cc * w + dd);
+                s.Whs[lev * Np + c] = w;
             }
             s.Whs[c] = 0.0;
         }
@@ -1870,7 +1975,7 @@ void launch_momentum(const Geometry& g, const Phys& P, const State& s, double dt
     else
         momentum_kernel<double><<<tile_grid_tail(g), tile_block(), 0, st>>>(g, P, s, dt);
 }
-size_t vertical_smem_bytes(const Geometry& g) { return sizeof(double) * kTile * (21 + 2 * g.nv); }
+size_t vertical_smem_bytes(const Geometry& g) { return sizeof(double) * kTile * (21 + 4 * g.nv); }
 void launch_vertical(const Geometry& g, const Phys& P, const State& s, double dt,
                      cudaStream_t st) {
     const size_t  smem       = vertical_smem_bytes(g);
