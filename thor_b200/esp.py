@@ -1,0 +1,588 @@
+"""bin/esp for thorx: run THOR's large step from a .thr configuration file.
+
+    python -m thor_b200.esp [config.thr] [-g GPU] [-o DIR] [-N STEPS] [-i FILE | -c FILE | -b] [-w]
+
+Restates the program entry of the reference (src/esp.cu:164-1573): the same command-line
+arguments with the same meaning (src/esp.cu:183-198, overrides at :497-570), the same
+configuration syntax (key = value lines, comments, typed values; src/utils/config_file.cpp:60-130,
+src/headers/parser_helpers.h:77-365), the same keys and defaults for everything on the path
+(src/esp.cu:257-475, src/headers/define.h; the RT module's keys,
+src/physics/modules/src/radiative_transfer.cu:1107-1190; the insolation keys,
+src/ESP/insolation.cu:239-251), the same checks (src/esp.cu:574-700), the main loop's cadence of
+outputs, global diagnostics and log lines (src/esp.cu:1381-1480), batch and continue modes
+(src/esp.cu:848-940) and the three text logs (src/utils/log_writer.cpp).
+
+Differences, each stated where it applies:
+  * state files are NumPy .npz archives, not HDF5 (there is no HDF5 library here); the arrays keep
+    the reference's names and memory layout ([column][level][component]);
+  * keys for physics that this build does not implement (sponges, convective adjustment,
+    chemistry, boundary layer, ultra-hot thermodynamics, refined vertical grids, picket-fence or
+    two-stream RT, other initial profiles) are accepted at their default values and rejected
+    with an error naming the key otherwise;
+  * output_mean, out_interm_momentum and output_diffusion only add arrays to the output files in
+    the reference; here they are accepted and a warning says the arrays are not written;
+  * one extension key, `precision` = fp64 (default) | mixed, selects the compute form.
+The simulation itself runs on the GPU through the C ABI (include/thorx.h); nothing here computes.
+"""
+import argparse
+import os
+import re
+import signal
+import sys
+import time
+
+import numpy as np
+
+AU = 149597870700.0       # src/headers/physical_constants.h:9
+R_SUN = 695700000.0       # src/headers/physical_constants.h:15
+
+# ---------------------------------------------------------------------------------------------
+# Configuration syntax (src/headers/parser_helpers.h:77-130, 268-360)
+# ---------------------------------------------------------------------------------------------
+_PUNCT = re.escape("!\"#$%&'()*+,-./:;<=>?@[\\]^_`{|}~")
+_EMPTY = re.compile(r"^[ \t]*$")
+_COMMENT = re.compile(r"^[ \t]?#.*$")
+_KEY_VALUE = re.compile(r"^[ \t]*([A-Za-z0-9_]+)[ \t]*=[ \t]*((?:[A-Za-z0-9]|[" + _PUNCT
+                        + r"])+)[ \t]*(#.*)?$")
+_BOOL = re.compile(r"^(true|false)$")
+_INT = re.compile(r"^((-|\+)?[0-9]+)$")
+_DOUBLE = re.compile(r"^((-|\+)?[0-9]+(\.[0-9]+)?((E|e)(-|\+)?[0-9]+)?)$")
+
+
+def parse_value(kind, text):
+    """(ok, value) for one configuration value of type kind (bool, int, float, str)."""
+    if kind is bool:
+        m = _BOOL.match(text)
+        return (True, m.group(1) == "true") if m else (False, None)
+    if kind is int:
+        m = _INT.match(text)
+        return (True, int(m.group(1))) if m else (False, None)
+    if kind is float:
+        m = _DOUBLE.match(text)
+        return (True, float(m.group(1))) if m else (False, None)
+    return True, text
+
+
+# Keys: name -> (type, default, role). Roles: "path" (used), "output" (accepted, output only),
+# "fixed" (must keep one of the allowed values: physics outside this build), "ignored" (no effect
+# here, e.g. a parameter of a switched-off scheme). Defaults as the reference registers them: the
+# planet's from SimulationSetup (src/ESP/simulation_setup.cu:60-76, a hot Jupiter), the switches
+# from src/headers/define.h, and its own choice for MetStar, Tstar, radius_star and
+# planet_star_dist, which take the defaults of Tint, kappa_lw, kappa_sw and f_lw
+# (src/esp.cu:426-430).
+KEYS = {
+    "config_version": (int, -1, "ignored"),
+    "timestep": (int, 1800, "path"),
+    "num_steps": (int, 48000, "path"),
+    "simulation_ID": (str, "Earth", "path"),
+    "radius": (float, 72427000.0, "path"),
+    "rotation_rate": (float, 9.09e-5, "path"),
+    "gravitation": (float, 47.0, "path"),
+    "GravHeightVar": (bool, False, "path"),
+    "Rd": (float, 3714.0, "path"),
+    "Cp": (float, 13000.0, "path"),
+    "Tmean": (float, 1400.0, "path"),
+    "P_ref": (float, 10000000.0, "path"),
+    "Top_altitude": (float, 1235376.0, "path"),
+    "Diffc": (float, 0.009973, "path"),
+    "DivDampc": (float, 0.009973, "path"),
+    "Diffc_v": (float, 0.0, "ignored"),
+    "spring_dynamics": (bool, True, "path"),
+    "glevel": (int, 4, "path"),
+    "spring_beta": (float, 1.15, "path"),
+    "vlevel": (int, 32, "path"),
+    "HyDiff": (bool, True, "path"),
+    "HyDiffOrder": (int, 4, "path"),
+    "DivDampP": (bool, True, "path"),
+    "VertHyDiff": (bool, False, "fixed"),
+    "VertHyDiffOrder": (int, 6, "ignored"),
+    "increased_damping_for_n_steps": (int, 0, "fixed"),
+    "NonHydro": (bool, True, "path"),
+    "DeepModel": (bool, True, "path"),
+    "output_mean": (bool, True, "output"),
+    "out_interm_momentum": (bool, False, "output"),
+    "output_diffusion": (bool, False, "output"),
+    "RayleighSponge": (bool, False, "fixed"),
+    "RayleighSpongeT": (bool, False, "fixed"),
+    "DiffSponge": (bool, False, "fixed"),
+    "shrink_sponge": (bool, False, "fixed"),
+    "t_shrink": (int, 144000, "ignored"),
+    "raysp_calc_mode": (str, "imp", "ignored"),
+    "nlat_bins": (int, 20, "ignored"),
+    "Ruv_sponge": (float, 1e-4, "ignored"),
+    "Rw_sponge": (float, 1e-4, "ignored"),
+    "RT_sponge": (float, 1e-4, "ignored"),
+    "ns_ray_sponge": (float, 0.75, "ignored"),
+    "damp_uv_to_mean": (bool, True, "ignored"),
+    "damp_w_to_mean": (bool, True, "ignored"),
+    "Dv_sponge": (float, 0.01, "ignored"),
+    "ns_diff_sponge": (float, 0.75, "ignored"),
+    "order_diff_sponge": (int, 2, "ignored"),
+    "rest": (bool, True, "path"),
+    "initial": (str, "ifile/esp_initial.h5", "path"),
+    "core_benchmark": (str, "HeldSuarez", "path"),
+    "init_PT_profile": (str, "isothermal", "fixed"),
+    "conv_adj": (bool, False, "fixed"),
+    "conv_adj_iter": (int, 1, "ignored"),
+    "soft_adjustment": (bool, False, "ignored"),
+    "conv_adj_type": (str, "hourdin", "ignored"),
+    "GPU_ID_N": (int, 0, "path"),
+    "n_out": (int, 1000, "path"),
+    "results_path": (str, "results", "path"),
+    "gcm_off": (bool, False, "path"),
+    "globdiag": (bool, False, "path"),
+    "single_column": (bool, False, "fixed"),
+    "custom_global_n_out": (bool, False, "path"),
+    "global_n_out": (int, 1000, "path"),
+    "custom_log_n_out": (bool, False, "path"),
+    "log_n_out": (int, 1000, "path"),
+    "Tint": (float, 100.0, "path"),
+    "kappa_lw": (float, 0.002, "path"),
+    "kappa_sw": (float, 0.001, "path"),
+    "f_lw": (float, 0.5, "path"),
+    "bv_freq": (float, 0.01, "ignored"),
+    "MetStar": (float, 100.0, "ignored"),
+    "Tstar": (float, 0.002, "path"),
+    "radius_star": (float, 0.001, "path"),
+    "planet_star_dist": (float, 0.5, "path"),
+    "ultrahot_thermo": (str, "none", "fixed"),
+    "ultrahot_heating": (str, "none", "fixed"),
+    "thermo_equation": (str, "entropy", "path"),
+    "vert_refined": (bool, False, "fixed"),
+    "transition_altitude": (float, 1000.0, "ignored"),
+    "lowest_layer_thickness": (float, 2.0, "ignored"),
+    "vert_dense_around": (bool, False, "fixed"),
+    "frac_height_dense": (float, 0.7, "ignored"),
+    "a_dense": (float, 1.0, "ignored"),
+    "b_dense": (float, 6.0, "ignored"),
+    # physics modules (src/physics/managers/multi/src/phy_modules.cu:118-140)
+    "radiative_transfer": (bool, False, "path"),
+    "chemistry": (bool, False, "fixed"),
+    "chem_time_file": (str, "", "ignored"),
+    "chem_fEQ_file": (str, "", "ignored"),
+    "boundary_layer": (bool, False, "fixed"),
+    "bl_type": (str, "RayleighHS", "ignored"),
+    "two_streams_radiative_transfer": (bool, False, "fixed"),
+    # double-gray RT (radiative_transfer.cu:1146-1190, radiative_transfer.h:98-119)
+    "rt_type": (str, "DualbandGray", "fixed"),
+    "diff_ang": (float, 0.5, "path"),
+    "albedo": (float, 0.18, "path"),
+    "latf_lw": (bool, False, "path"),
+    "kappa_lw_pole": (float, 0.002, "path"),
+    "n_sw": (float, 1.0, "path"),
+    "n_lw": (float, 2.0, "path"),
+    "rt1Dmode": (bool, False, "path"),
+    "surface": (bool, False, "fixed"),
+    "Csurf": (float, 1e7, "ignored"),
+    "dgrt_spinup_start": (int, -1, "path"),
+    "dgrt_spinup_stop": (int, -1, "path"),
+    "dgrt_spindown_start": (int, -1, "path"),
+    "dgrt_spindown_stop": (int, -1, "path"),
+    # insolation (src/ESP/insolation.cu:239-251, src/headers/insolation.h:132-138)
+    "sync_rot": (bool, True, "path"),
+    "mean_motion": (float, 1.991e-7, "path"),
+    "alpha_i": (float, 0.0, "path"),
+    "true_long_i": (float, 0.0, "path"),
+    "ecc": (float, 0.0, "path"),
+    "obliquity": (float, 0.0, "path"),
+    "longp": (float, 0.0, "path"),
+    "insol_avg": (str, "NoInsolAvg", "fixed"),
+    # extension: compute form of this build
+    "precision": (str, "fp64", "path"),
+}
+# values a "fixed" key may take (its default unless listed)
+ALLOWED = {"init_PT_profile": ("isothermal",), "rt_type": ("DualbandGray",),
+           "ultrahot_thermo": ("none",), "ultrahot_heating": ("none",),
+           "insol_avg": ("NoInsolAvg",)}
+CHOICES = {"core_benchmark": ("HeldSuarez", "NoBenchmark"),
+           "thermo_equation": ("entropy", "energy"), "precision": ("fp64", "mixed")}
+
+
+class ConfigError(Exception):
+    pass
+
+
+def read_config(text, out=sys.stdout):
+    """Parse a .thr text into {key: value} with defaults, as the reference's config_file does:
+    unknown keys warn and are skipped, a malformed line or value fails the whole file."""
+    values = {k: v[1] for k, v in KEYS.items()}
+    given = set()
+    ok = True
+    for n, line in enumerate(text.splitlines(), 1):
+        if _EMPTY.match(line) or _COMMENT.match(line):
+            continue
+        m = _KEY_VALUE.match(line)
+        if not m:
+            out.write("ERROR in config file at line %d :\t [%s]\n" % (n, line))
+            ok = False
+            continue
+        key, value = m.group(1), m.group(2)
+        if key not in KEYS:
+            out.write("WARNING: config file key [%s] does not exist, skipping\n" % key)
+            continue
+        good, v = parse_value(KEYS[key][0], value)
+        if not good:
+            out.write("ERROR: parsing of value [%s] failed for key [%s] \n" % (value, key))
+            ok = False
+            continue
+        values[key] = v
+        given.add(key)
+    if not ok:
+        raise ConfigError("config file reading failed")
+    return values, given
+
+
+def check_config(c, out=sys.stdout):
+    """The reference's range checks (src/esp.cu:574-700) plus this build's scope; raises
+    ConfigError listing every problem."""
+    bad = []
+    def need(cond, msg):
+        if not cond:
+            bad.append(msg)
+    need(c["timestep"] > 0, "timestep must be > 0")
+    need(c["num_steps"] > 0, "nsmax must be > 0")
+    need(c["gravitation"] > 0, "gravitation must be > 0")
+    need(c["Rd"] > 0, "Rd must be > 0")
+    need(c["Tmean"] > 0, "T_mean must be > 0")
+    need(c["P_ref"] > 0, "P_Ref must be > 0")
+    need(c["Top_altitude"] > 0, "Top_altitude must be > 0")
+    need(3 <= c["glevel"] <= 8, "glevel must be in [3, 8]")
+    need(c["vlevel"] > 0, "vlevel must be > 0")
+    need(c["GPU_ID_N"] > -1, "GPU_ID_N must be > -1")
+    need(c["n_out"] > 0, "n_out must be > 0")
+    need(len(c["simulation_ID"]) < 160, "Bad value for config variable simulation_ID")
+    need(c["HyDiffOrder"] > 2 and c["HyDiffOrder"] % 2 == 0,
+         "Bad value for HyDiffOrder! Must be multiple of 2 greater than/equal to 4.")
+    need(c["VertHyDiffOrder"] > 2 and c["VertHyDiffOrder"] % 2 == 0,
+         "Bad value for VertHyDiffOrder! Must be multiple of 2 greater than/equal to 4.")
+    for k, allowed in CHOICES.items():
+        need(c[k] in allowed, "%s = %s: this build supports %s" % (k, c[k], " | ".join(allowed)))
+    for k, (kind, default, role) in KEYS.items():
+        if role == "fixed":
+            allowed = ALLOWED.get(k, (default,))
+            need(c[k] in allowed, "%s = %s: not implemented in this build (allowed: %s)"
+                 % (k, c[k], ", ".join(str(a) for a in allowed)))
+    if bad:
+        for b in bad:
+            out.write("Config error: %s\n" % b)
+        raise ConfigError("; ".join(bad))
+    for k in ("output_mean", "out_interm_momentum", "output_diffusion"):
+        if c[k]:
+            out.write("WARNING: %s = true: those arrays are not written by this build\n" % k)
+
+
+def thorx_params(c):
+    """The configuration as thorx_params (the Thorx constructor's dict)."""
+    return dict(A=c["radius"], Omega=c["rotation_rate"], Gravit=c["gravitation"], Rd=c["Rd"],
+                Cp=c["Cp"], P_Ref=c["P_ref"], Top_altitude=c["Top_altitude"],
+                timestep=float(c["timestep"]), Diffc=c["Diffc"], DivDampc=c["DivDampc"],
+                HyDiffOrder=c["HyDiffOrder"], DeepModel=int(c["DeepModel"]),
+                NonHydro=int(c["NonHydro"]), GravHeightVar=int(c["GravHeightVar"]),
+                HyDiff=int(c["HyDiff"]), DivDampP=int(c["DivDampP"]),
+                thermo_equation=1 if c["thermo_equation"] == "energy" else 0,
+                core_benchmark=1 if c["core_benchmark"] == "HeldSuarez" else 0,
+                precision=1 if c["precision"] == "mixed" else 0)
+
+
+def rt_config(c, first_step):
+    """The RT module's parameters in the C ABI's units (m, K, degrees): the configuration gives
+    the star radius in solar radii and the distance in au (src/ESP/esp_initial.cu:194-196)."""
+    return dict(Tstar=c["Tstar"], planet_star_dist=c["planet_star_dist"] * AU,
+                radius_star=c["radius_star"] * R_SUN, diff_ang=c["diff_ang"], Tint=c["Tint"],
+                albedo=c["albedo"], kappa_sw=c["kappa_sw"], kappa_lw=c["kappa_lw"],
+                kappa_lw_pole=c["kappa_lw_pole"], n_sw=c["n_sw"], n_lw=c["n_lw"], f_lw=c["f_lw"],
+                latf_lw=int(c["latf_lw"]), rt1Dmode=int(c["rt1Dmode"]),
+                sync_rot=int(c["sync_rot"]), surface=0, mean_motion=c["mean_motion"],
+                alpha_i=c["alpha_i"], true_long_i=c["true_long_i"], ecc=c["ecc"],
+                obliquity=c["obliquity"], longp=c["longp"],
+                spinup_start=c["dgrt_spinup_start"], spinup_stop=c["dgrt_spinup_stop"],
+                spindown_start=c["dgrt_spindown_start"], spindown_stop=c["dgrt_spindown_stop"],
+                first_step=first_step)
+
+
+# ---------------------------------------------------------------------------------------------
+# Files: state archives and the text logs (src/utils/log_writer.cpp)
+# ---------------------------------------------------------------------------------------------
+# what a restart needs: the prognostic fields and the per-cell gas constants (the step recomputes
+# the temperature from them)
+STATE = ["Rho", "pressure", "Mh", "Wh", "W", "Rd", "Cp"]
+ARCHIVE_NAMES = {"Rho": "Rho", "pressure": "Pressure", "Mh": "Mh", "Wh": "Wh", "W": "W",
+                 "Rd": "Rd", "Cp": "Cp"}
+
+
+def output_name(sim_id, idx):
+    return "esp_output_%s_%d.npz" % (sim_id, idx)
+
+
+def write_state(path, x, nstep, sim_time, extra=None):
+    arrays = {ARCHIVE_NAMES[f]: x.get(f) for f in STATE}
+    arrays["temperature"] = x.get("temperature")
+    arrays["nstep"] = np.array(nstep)
+    arrays["simulation_time"] = np.array(sim_time)
+    for k, v in (extra or {}).items():
+        arrays[k] = np.asarray(v)
+    tmp = path + ".tmp.npz"
+    np.savez(tmp, **arrays)
+    os.replace(tmp, path)
+
+
+def read_state(path):
+    """(fields present in the file, nstep, simulation time)."""
+    with np.load(path) as d:
+        state = {f: np.array(d[ARCHIVE_NAMES[f]]) for f in STATE if ARCHIVE_NAMES[f] in d}
+        return state, int(d["nstep"]), float(d["simulation_time"])
+
+
+class Logs:
+    """esp_write_log_<ID>.txt, esp_global_<ID>.txt, esp_diagnostics_<ID>.txt in the output
+    directory, with the reference's headers and columns."""
+
+    def __init__(self, out_dir, sim_id, append, globdiag):
+        self.out_dir, self.sim_id = out_dir, sim_id
+        mode = "a" if append else "w"
+        self.write_log = self._open("esp_write_log_%s.txt" % sim_id, mode,
+                                    "#step_number\tfile_number\tfilename")
+        self.glob = self._open("esp_global_%s.txt" % sim_id, mode,
+                               "#current_step\tsimulation_time\tGlobalE_h\tGlobalMass_h\t"
+                               "GlobalAMx_h\tGlobalAMy_h\tGlobalAMz_h\tGlobalEnt_h") \
+            if globdiag else None
+        self.diag = self._open("esp_diagnostics_%s.txt" % sim_id, mode,
+                               "#current_step\tsimulation_time\ttotal_bytes\tfree_bytes\t"
+                               "elapsed_time\ttime_left\tmean_delta_per_step\tend_time")
+
+    def _open(self, name, mode, header):
+        path = os.path.join(self.out_dir, name)
+        fresh = mode == "w" or not os.path.exists(path)
+        f = open(path, mode)
+        if fresh:
+            f.write(header + "\n")
+        return f
+
+    def output(self, step, idx, filename):
+        self.write_log.write("%d\t%d\t%s\n" % (step, idx, filename))
+        self.write_log.flush()
+
+    def globdiag(self, step, t, g):
+        self.glob.write("%d\t%s\t%s\n" % (step, _g16(t), "\t".join(_g16(v) for v in g)))
+        self.glob.flush()
+
+    def diagnostics(self, step, t, total, free, elapsed, left, mean_delta, end):
+        self.diag.write("%d\t%s\t%d\t%d\t%s\t%s\t%s\t%s\n"
+                        % (step, _g16(t), total, free, _g16(elapsed), _g16(left),
+                           _g16(mean_delta), end))
+        self.diag.flush()
+
+    def close(self):
+        for f in (self.write_log, self.glob, self.diag):
+            if f:
+                f.close()
+
+
+def _g16(v):
+    return "%.16g" % v
+
+
+def last_output(out_dir, sim_id):
+    """(file number, step, filename) of the last line of esp_write_log_<ID>.txt, or None
+    (log_writer::check_output_log, src/utils/log_writer.cpp:80-136)."""
+    path = os.path.join(out_dir, "esp_write_log_%s.txt" % sim_id)
+    if not os.path.exists(path):
+        return None
+    last = None
+    with open(path) as f:
+        for line in f:
+            parts = line.split()
+            if len(parts) == 3 and not line.startswith("#"):
+                last = (int(parts[1]), int(parts[0]), parts[2])
+    return last
+
+
+# ---------------------------------------------------------------------------------------------
+# The run
+# ---------------------------------------------------------------------------------------------
+_caught = []
+
+
+def _on_signal(signum, frame):  # the reference's sigterm/sigint handlers (src/esp.cu:99-110)
+    _caught.append(signum)
+
+
+def build_parser():
+    ap = argparse.ArgumentParser(prog="esp", description="run THOR GCM simulation (thorx)")
+    ap.add_argument("config", nargs="?", default="ifile/earth.thr", help="config filename")
+    ap.add_argument("-g", "--gpu_id", type=int, help="GPU_ID to run on")
+    ap.add_argument("-o", "--output_dir", help="results directory to store output")
+    ap.add_argument("-i", "--initial", help="start from this initial condition instead of rest")
+    ap.add_argument("-c", "--continue", dest="cont",
+                    help="continue simulation from this output file")
+    ap.add_argument("-N", "--numsteps", type=int, help="number of steps to run")
+    ap.add_argument("-w", "--overwrite", action="store_true",
+                    help="Force overwrite of output file if they exist")
+    ap.add_argument("-b", "--batch", action="store_true", help="Run as batch")
+    return ap
+
+
+def run(argv=None, out=sys.stdout):
+    """Run a simulation; returns the process exit status (0 ok)."""
+    args = build_parser().parse_args(argv)
+    try:
+        with open(args.config) as f:
+            text = f.read()
+    except OSError:
+        out.write(" Config file %s reading failed, aborting\n" % args.config)
+        return 255
+    try:
+        c, given = read_config(text, out)
+    except ConfigError:
+        out.write(" Config file %s reading failed, aborting\n" % args.config)
+        return 255
+    out.write(" Config file %s read\n" % args.config)
+    # command-line overrides (src/esp.cu:497-570)
+    if args.gpu_id is not None:
+        c["GPU_ID_N"] = args.gpu_id
+    if args.output_dir is not None:
+        c["results_path"] = args.output_dir
+    if args.numsteps is not None:
+        c["num_steps"] = args.numsteps
+    start_file = None
+    if args.initial is not None:
+        c["rest"] = False
+        start_file = args.initial
+    if args.cont is not None:
+        if args.batch:
+            out.write("--continue and --batch options set, options are exclusive, must set only one\n")
+            return 255
+        if args.initial is not None:
+            out.write("--continue and --initial options set, options are exclusive, must set only one\n")
+            return 255
+        c["rest"] = False
+        start_file = args.cont
+    if not c["rest"] and start_file is None:
+        start_file = c["initial"]
+    try:
+        check_config(c, out)
+    except ConfigError:
+        return 255
+    if start_file is not None and not os.path.exists(start_file):
+        out.write("Initial conditions file \"%s\" not found\n" % start_file)
+        return 255
+
+    out_dir, sim_id = c["results_path"], c["simulation_ID"]
+    os.makedirs(out_dir, exist_ok=True)
+    continuing = args.cont is not None
+    first_idx, step_idx, sim_time0 = 0, 1, 0.0
+    if args.batch:
+        last = last_output(out_dir, sim_id)
+        if last is not None:
+            start_file = os.path.join(out_dir, last[2])
+            continuing = True
+            out.write("continuing batch run from file %s\n" % start_file)
+        else:
+            out.write("No batch file found, initialise simulation.\n")
+    if not continuing and not args.overwrite and os.path.exists(
+            os.path.join(out_dir, output_name(sim_id, 0))):
+        out.write("output files already exist in %s; use -w to overwrite\n" % out_dir)
+        return 255
+
+    import thor_b200
+    # the device: GPU_ID_N (or -g) through CUDA_VISIBLE_DEVICES, before the first CUDA call
+    if "CUDA_VISIBLE_DEVICES" in os.environ:
+        if c["GPU_ID_N"] != 0:
+            out.write("WARNING: CUDA_VISIBLE_DEVICES is set; GPU_ID_N = %d ignored\n"
+                      % c["GPU_ID_N"])
+    else:
+        os.environ["CUDA_VISIBLE_DEVICES"] = str(c["GPU_ID_N"])
+    grid = thor_b200.Icogrid(c["glevel"], c["vlevel"], A=c["radius"],
+                             Top_altitude=c["Top_altitude"], spring=c["spring_dynamics"],
+                             beta=c["spring_beta"])
+    x = thor_b200.Thorx(grid.as_dict(), c["glevel"], thorx_params(c))
+    handlers = None
+    try:
+        if start_file is not None:
+            state, nstep0, sim_time0 = read_state(start_file)
+            missing = [f for f in ("Rho", "pressure", "Mh", "Wh", "W") if f not in state]
+            if missing:
+                out.write("start file %s lacks %s\n" % (start_file, ", ".join(missing)))
+                return 255
+            cells = x.size("Rho")
+            state.setdefault("Rd", np.full(cells, c["Rd"]))   # files without the gas constants
+            state.setdefault("Cp", np.full(cells, c["Cp"]))
+            for f, v in state.items():
+                x.set(f, v)
+            if continuing:
+                step_idx = nstep0 + 1
+                m = re.search(r"_(\d+)\.npz$", start_file)
+                first_idx = int(m.group(1)) + 1 if m else 1
+        else:
+            x.init_rest_state(c["Tmean"], 0, 0.0)
+        if c["radiative_transfer"]:
+            x.rt_enable(rt_config(c, step_idx))
+        nsmax = c["num_steps"]
+        logs = Logs(out_dir, sim_id, continuing, c["globdiag"])
+        grid_file = os.path.join(out_dir, "esp_output_grid_%s.npz" % sim_id)
+        np.savez(grid_file, **{k: v for k, v in grid.as_dict().items()
+                               if isinstance(v, np.ndarray)})
+        np.savez(os.path.join(out_dir, "esp_output_planet_%s.npz" % sim_id),
+                 **{k: np.array(v) for k, v in c.items()})
+        if not continuing:
+            name = output_name(sim_id, 0)
+            write_state(os.path.join(out_dir, name), x, 0, sim_time0)
+            logs.output(0, 0, name)
+            first_idx = 1
+        del _caught[:]
+        handlers = (signal.signal(signal.SIGTERM, _on_signal),
+                    signal.signal(signal.SIGINT, _on_signal))
+        dt = c["timestep"]
+        n_out = c["n_out"]
+        g_out = c["global_n_out"] if c["custom_global_n_out"] else n_out
+        l_out = c["log_n_out"] if c["custom_log_n_out"] else n_out
+        idx, nstep, t0 = first_idx, step_idx - 1, time.time()
+        out.write(" Starting the model integration.\n\n")
+        while nstep < nsmax:
+            # next step at which something is written: run up to it as one call (graph replays)
+            nxt = min(nsmax, *(((nstep // k) + 1) * k for k in (n_out, g_out, l_out)),
+                      nstep + 64)
+            k = nxt - nstep
+            if c["gcm_off"]:
+                for _ in range(k):
+                    x.profx()
+            else:
+                x.step(k)
+            x.sync()
+            nstep = nxt
+            sim_time = sim_time0 + (nstep - step_idx + 1) * dt
+            if c["globdiag"] and nstep % g_out == 0:
+                logs.globdiag(nstep, sim_time, x.globdiag())
+            if nstep % n_out == 0 or _caught:
+                name = output_name(sim_id, idx)
+                write_state(os.path.join(out_dir, name), x, nstep, sim_time)
+                logs.output(nstep, idx, name)
+                idx += 1
+            elapsed = time.time() - t0
+            done = nstep - step_idx + 1
+            mean = elapsed / done
+            left = mean * (nsmax - nstep)
+            end = time.strftime("%Y-%m-%d %H:%M:%S", time.localtime(time.time() + left))
+            if nstep % l_out == 0:
+                out.write("\n Time step number = %d/%d || Time = %f days. \n\t Elapsed %.0f s || "
+                          "Left: %.0f s || Completion: %s. \n"
+                          % (nstep, nsmax, sim_time / 86400.0, elapsed, left, end))
+                logs.diagnostics(nstep, sim_time, 0, 0, elapsed, left, mean, end)
+            if _caught:
+                out.write("\n Caught signal, stopping after step %d.\n" % nstep)
+                break
+        logs.close()
+    finally:
+        if handlers:
+            signal.signal(signal.SIGTERM, handlers[0])
+            signal.signal(signal.SIGINT, handlers[1])
+        x.close()
+    return 0
+
+
+def main():
+    sys.exit(run())
+
+
+if __name__ == "__main__":
+    main()
