@@ -26,6 +26,7 @@ extern "C" {
 #define THORX_E_NAN -3      /* the NaN check after the physics step tripped               */
 #define THORX_E_UNSUPPORTED -4 /* option outside what this build implements               */
 #define THORX_E_STATE -5    /* call out of order (e.g. stepping before the state is set)  */
+#define THORX_E_CONVERGENCE -6 /* a column's convective adjustment exceeded its pass bound    */
 
 typedef struct thorx_ctx thorx_ctx;
 
@@ -118,6 +119,14 @@ int thorx_init_rest_state(thorx_ctx* ctx, double Tmean, unsigned long long seed,
 /* Switches the precision form (THORX_FP64 / THORX_MIXED) between steps; the state and everything
  * else of the context carry over (both forms store FP64). A captured step graph is re-captured. */
 int thorx_set_precision(thorx_ctx* ctx, int precision);
+
+/* Dry convective adjustment in every following ProfX (sim.conv_adj with conv_adj_type = hourdin:
+ * dry_conv_adj, src/headers/phy/dry_conv_adj.h:50-311, called at src/ESP/profx_driver.cu:239-290):
+ * up to `iterations` rounds per step (the reference's conv_adj_iter; 0 switches it off);
+ * soft_adjustment != 0 turns the adjustment into heating in profx_Qheat (soft_adjustment).
+ * A column that exceeds the pass bound (the reference's loops have none) makes the next
+ * thorx_sync return THORX_E_CONVERGENCE. */
+int thorx_conv_adj_enable(thorx_ctx* ctx, int iterations, int soft_adjustment);
 
 /* One physics step, ESP::ProfX (src/ESP/profx_driver.cu:70-474): W from Wh, T and potential
  * temperature from p and rho, Held-Suarez forcing when core_benchmark says so, p = rho Rd T,

@@ -38,6 +38,7 @@
 #include "dyn/thor_fastmodes.h"
 #include "dyn/thor_slowmodes.h"
 #include "dyn/thor_vertical_int.h"
+#include "phy/dry_conv_adj.h"
 #include "phy/profx_auxiliary.h"
 #include "phy/profx_globdiag.h"
 #include "phy/profx_held_suarez.h"
@@ -165,6 +166,8 @@ struct ref_rt_params {
 
 struct RefSim {
     ref_params                     p;
+    int                            conv_adj_iter = 0; // dry_conv_adj when > 0
+    bool                           conv_soft     = false;
     bool                           rt = false;
     ref_rt_params                  R{};
     double incflx = 0, mean_motion = 0, mean_anomaly_i = 0, true_long_i = 0, ecc = 0,
@@ -417,6 +420,17 @@ extern "C" int ref_sim_rt(void* h, const ref_rt_params* rp) {
     return 0;
 }
 
+// The dry convective adjustment in ProfX (sim.conv_adj, conv_adj_type hourdin): the reference's
+// dry_conv_adj kernel as profx_driver.cu:239-290 launches it.
+extern "C" int ref_sim_conv_adj(void* h, int iterations, int soft) {
+    RefSim* s = (RefSim*)h;
+    if (!s->f.count("pressureh") && sim_alloc(s, "pressureh", (long)s->N * s->nvi))
+        return -2;
+    s->conv_adj_iter = iterations;
+    s->conv_soft     = soft != 0;
+    return 0;
+}
+
 extern "C" void ref_sim_rt_totals(void* h, double* asr, double* olr) {
     RefSim* s = (RefSim*)h;
     *asr      = s->ASR_tot;
@@ -497,6 +511,15 @@ static int ref_profx(RefSim* s) {
     Compute_temperature<<<NB, NTH>>>(F["temperature"], F["pt"], F["pressure"], F["Rho"],
                                      s->p.P_Ref, F["Rd"], F["Cp"], N, true);
     REF_CHECK(cudaDeviceSynchronize());
+    if (s->conv_adj_iter > 0) {
+        const int NBRT = (N / NTH) + 1;
+        dry_conv_adj<<<NBRT, NTH>>>(F["pressure"], F["pressureh"], F["temperature"],
+                                    F["profx_Qheat"], F["pt"], F["Rho"], F["Cp"], F["Rd"],
+                                    s->p.Gravit, F["Altitude"], F["Altitudeh"], s->p.timestep,
+                                    s->p.A, s->conv_adj_iter, s->conv_soft, N, nv,
+                                    s->p.GravHeightVar);
+        REF_CHECK(cudaDeviceSynchronize());
+    }
     if (s->p.held_suarez) {
         held_suarez<<<NB, NTH>>>(F["Mh"], F["pressure"], F["Rho"], F["temperature"], s->p.Gravit,
                                  s->p.Cp, s->p.Rd, F["Altitude"], F["Altitudeh"], F["lonlat"],

@@ -56,6 +56,10 @@ struct Oracle {
     double r_orb = 1, sin_decl = 0, cos_decl = 1, alpha = 0; // Insolation member defaults
     int    nstep = 1;
     double ASR_tot = 0, OLR_tot = 0;
+    // dry convective adjustment (when enabled)
+    int  conv_adj_iter = 0;
+    bool conv_soft     = false;
+    bool conv_fail     = false; // a column exceeded the pass bound
 };
 
 inline double val(const Vec& a, int id, int nv, int lev) {
@@ -482,10 +486,115 @@ void rt_step(Oracle& o) {
     o.nstep++;
 }
 
+// dry_conv_adj, src/headers/phy/dry_conv_adj.h:50-311 (conv_adj_type = hourdin): per column,
+// the same sequence and the same pass bounds as the product (the reference's loops have none).
+void dry_conv_adj(Oracle& o) {
+    int    N = o.N, nv = o.nv;
+    Vec &  T = F(o, "temperature"), &p = F(o, "pressure"), &pt = F(o, "pt"), &rho = F(o, "Rho"),
+        &Rd = F(o, "Rd"), &Cp = F(o, "Cp"), &Q = F(o, "profx_Qheat");
+    const Vec &Alt = o.Altitude, &Alth = o.Altitudeh;
+    const double g = o.P.Gravit, A = o.P.A, stable = 0.0;
+    bool         fail = false;
+#pragma omp parallel for schedule(dynamic, 64) reduction(|| : fail)
+    for (int id = 0; id < N; id++) {
+        auto   at     = [&](int lev) { return (size_t)id * nv + lev; };
+        int    iter   = 0;
+        bool   repeat = true, bad = false;
+        while (repeat && iter < o.conv_adj_iter && !bad) {
+            double psm;
+            if (o.P.GravHeightVar)
+                psm = p[at(1)] - rho[at(0)] * g * pow(A / (A + Alt[0]), 2) * (-Alt[0] - Alt[1]);
+            else
+                psm = p[at(1)] - rho[at(0)] * g * (-Alt[0] - Alt[1]);
+            double ps = 0.5 * (p[at(0)] + psm);
+            for (int lev = 0; lev < nv; lev++)
+                pt[at(lev)] = T[at(lev)] * pow(ps / p[at(lev)], Rd[at(lev)] / Cp[at(lev)]);
+            bool done_col = false;
+            int  passes   = 0;
+            while (!done_col && !bad) {
+                if (++passes > 2 * nv + 2) {
+                    bad = true;
+                    break;
+                }
+                int top = 0, bot = nv - 1;
+                for (int lev = 0; lev < nv - 1; lev++)
+                    if (pt[at(lev + 1)] - pt[at(lev)] < stable && bot > lev)
+                        bot = lev;
+                for (int lev = bot; lev < nv - 1; lev++) {
+                    if (pt[at(lev + 1)] - pt[at(lev)] > stable) {
+                        top = lev;
+                        break;
+                    }
+                    top = nv - 1;
+                }
+                if (bot < nv - 1) {
+                    bool   extend = true;
+                    int    ext    = 0;
+                    double thnew  = 0.0;
+                    while (extend) {
+                        if (++ext > nv + 2) {
+                            bad = true;
+                            break;
+                        }
+                        double h = 0.0, sum = 0.0;
+                        extend   = false;
+                        for (int lev = bot; lev <= top; lev++) {
+                            double pi = pow(p[at(lev)] / ps, Rd[at(lev)] / Cp[at(lev)]);
+                            double rho_g_dz = rho[at(lev)] * g * (Alth[lev + 1] - Alth[lev]);
+                            h   = h + pt[at(lev)] * pi * rho_g_dz;
+                            sum = sum + pi * rho_g_dz;
+                        }
+                        thnew = h / sum;
+                        if (bot > 0 && (thnew - pt[at(bot - 1)]) < stable) {
+                            bot    = bot - 1;
+                            extend = true;
+                        }
+                        if (top < nv - 1 && (pt[at(top + 1)] - thnew) < stable) {
+                            top    = top + 1;
+                            extend = true;
+                        }
+                    }
+                    if (bad)
+                        break;
+                    for (int lev = bot; lev <= top; lev++)
+                        pt[at(lev)] = thnew;
+                }
+                else
+                    done_col = true;
+            }
+            if (bad)
+                break;
+            repeat = false;
+            iter += 1;
+            for (int lev = 0; lev < nv; lev++) {
+                size_t i = at(lev);
+                if (o.conv_soft) {
+                    double Ttmp = pt[i] * pow(p[i] / ps, Rd[i] / Cp[i]);
+                    double Ptmp = Ttmp * Rd[i] * rho[i];
+                    pt[i]       = T[i] * pow(p[i] / ps, -Rd[i] / Cp[i]);
+                    Q[i] += (Cp[i] - Rd[i]) / Rd[i] * (Ptmp - p[i]) / o.P.timestep;
+                }
+                else {
+                    T[i]  = pt[i] * pow(p[i] / ps, Rd[i] / Cp[i]);
+                    p[i]  = T[i] * Rd[i] * rho[i];
+                    pt[i] = T[i] * pow(p[i] / ps, -Rd[i] / Cp[i]);
+                    if (lev > 0 && pt[i] - pt[at(lev - 1)] < stable)
+                        repeat = true;
+                }
+            }
+        }
+        fail = fail || bad;
+    }
+    if (fail)
+        o.conv_fail = true;
+}
+
 void profx(Oracle& o) {
     std::fill(F(o, "profx_Qheat").begin(), F(o, "profx_Qheat").end(), 0.0);
     recompute_w(o);
     compute_temperature(o);
+    if (o.conv_adj_iter > 0)
+        dry_conv_adj(o);
     if (o.P.held_suarez)
         held_suarez(o);
     if (o.rt)
@@ -1749,6 +1858,13 @@ extern "C" void* oracle_new(const oracle_grid* g, const oracle_params* p) {
     return o;
 }
 
+extern "C" int oracle_conv_adj(void* h, int iterations, int soft) {
+    Oracle* o        = (Oracle*)h;
+    o->conv_adj_iter = iterations;
+    o->conv_soft     = soft != 0;
+    return 0;
+}
+
 extern "C" int oracle_rt(void* h, const oracle_rt_params* rp) {
     Oracle& o = *(Oracle*)h;
     if (rp->surface || o.P.GravHeightVar || o.areasT.empty())
@@ -1809,6 +1925,10 @@ extern "C" int oracle_step(void* h, int nsteps, int do_profx, int do_thor) {
     for (int s = 0; s < nsteps; s++) {
         if (do_profx)
             profx(*o);
+        if (o->conv_fail) {
+            o->conv_fail = false;
+            return -3;
+        }
         if (do_thor)
             thor(*o);
     }

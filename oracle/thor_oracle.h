@@ -44,6 +44,10 @@ void* oracle_new(const oracle_grid* g, const oracle_params* p);
 // Enables the RT module in ProfX (between the benchmark forcing and Compute_pressure, as
 // src/ESP/profx_driver.cu:405-416). Returns 0, or -1 for an option the restatement lacks.
 int oracle_rt(void* h, const oracle_rt_params* rp);
+// Enables the dry convective adjustment in ProfX (after the temperature, before the forcing, as
+// src/ESP/profx_driver.cu:239-290): up to `iterations` rounds per step; soft != 0 for the soft form.
+// A column that exceeds the pass bound makes oracle_step return -3.
+int oracle_conv_adj(void* h, int iterations, int soft);
 // Global absorbed shortwave and outgoing longwave of the last RT call (the reference's
 // ASR_tot / OLR_tot), compensated sums.
 void oracle_rt_totals(void* h, double* asr, double* olr);

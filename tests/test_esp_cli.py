@@ -90,7 +90,7 @@ def test_bad_lines_fail_the_file(line):
 
 @pytest.mark.parametrize("line,what", [
     ("RayleighSponge = true", "RayleighSponge"),
-    ("conv_adj = true", "conv_adj"),
+    ("conv_adj_type = rayph", "conv_adj_type"),
     ("chemistry = true", "chemistry"),
     ("init_PT_profile = guillot", "init_PT_profile"),
     ("rt_type = PicketFence", "rt_type"),

@@ -127,6 +127,8 @@ def ref_lib(nofma=False):
         lib.ref_sim_globdiag.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         lib.ref_sim_rt.restype = ctypes.c_int
         lib.ref_sim_rt.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        lib.ref_sim_conv_adj.restype = ctypes.c_int
+        lib.ref_sim_conv_adj.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
         lib.ref_sim_rt_totals.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                           ctypes.POINTER(ctypes.c_double)]
         lib.ref_device_sum.restype = ctypes.c_double
@@ -206,6 +208,48 @@ def isothermal_column(Altitude, Altitudeh, c):
     return p, rho, T
 
 
+def hydrostatic_column(Altitude, Altitudeh, c, Tprof):
+    """Pressure and density of a column with temperature profile Tprof in the model's discrete
+    hydrostatic balance (the Newton iteration of isothermal_column, the temperature given)."""
+    nv = len(Altitude)
+    p, rho = np.zeros(nv), np.zeros(nv)
+    Rd, g = c["Rd"], c["Gravit"]
+    for lev in range(nv):
+        if lev == 0:
+            P_L, rho_L, dz = c["P_Ref"], c["P_Ref"] / (Rd * Tprof[0]), Altitude[0]
+            l_int = r_int = 0.5
+        else:
+            P_L, rho_L = p[lev - 1], rho[lev - 1]
+            dz = Altitude[lev] - Altitude[lev - 1]
+            l_int = (Altitude[lev] - Altitudeh[lev]) / dz
+            r_int = (Altitudeh[lev] - Altitude[lev - 1]) / dz
+        p[lev], rho[lev] = P_L, P_L / (Rd * Tprof[lev])
+        for _ in range(100):
+            f = (p[lev] - P_L) / dz + g * (rho[lev] * r_int + rho_L * l_int)
+            df = 1.0 / dz + g * r_int / (Rd * Tprof[lev])
+            step = f / df
+            p[lev] -= step
+            rho[lev] = p[lev] / (Rd * Tprof[lev])
+            if abs(step) <= 1e-15 * p[lev]:
+                break
+    return p, rho
+
+
+def unstable_state(grid_arrays, N, nv, c, seed=20260101, lapse=0.015, nlow=4, amp=2.0):
+    """A rest state whose lowest nlow levels are cooled superadiabatically (lapse in K/m, against
+    the dry adiabat g/Cp), in discrete hydrostatic balance, with +-amp K of seeded noise at fixed
+    pressure: many statically unstable stretches for the convective adjustment."""
+    alt = np.asarray(grid_arrays["Altitude"])
+    Tprof = c["Tmean"] - lapse * np.minimum(alt, alt[min(nlow, nv) - 1])
+    p0, _ = hydrostatic_column(alt, np.asarray(grid_arrays["Altitudeh"]), c, Tprof)
+    noise = (2.0 * splitmix64_uniform(N * nv, seed) - 1.0) * amp
+    T = np.tile(Tprof, N) + noise
+    p = np.tile(p0, N)
+    return dict(Rho=p / (c["Rd"] * T), pressure=p, temperature=T, Mh=np.zeros(3 * N * nv),
+                Wh=np.zeros(N * (nv + 1)), W=np.zeros(N * nv), Rd=np.full(N * nv, c["Rd"]),
+                Cp=np.full(N * nv, c["Cp"]))
+
+
 def initial_state(grid_arrays, N, nv, c, seed=20260101, amp=0.1):
     """Reference-layout initial state: dict of Rho, pressure, temperature, Mh, Wh, W, Rd, Cp."""
     p0, rho0, T0 = isothermal_column(grid_arrays["Altitude"], grid_arrays["Altitudeh"], c)
@@ -251,6 +295,8 @@ def oracle_lib():
         lib.oracle_globdiag.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         lib.oracle_rt.restype = ctypes.c_int
         lib.oracle_rt.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        lib.oracle_conv_adj.restype = ctypes.c_int
+        lib.oracle_conv_adj.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
         lib.oracle_rt_totals.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                          ctypes.POINTER(ctypes.c_double)]
         lib.oracle_sum.restype = ctypes.c_double
@@ -290,6 +336,9 @@ class Oracle:
     def rt(self, d):
         self._rt = rt_struct(d)
         assert oracle_lib().oracle_rt(self.h, ctypes.byref(self._rt)) == 0
+
+    def conv_adj(self, iterations=1, soft=False):
+        assert oracle_lib().oracle_conv_adj(self.h, iterations, int(soft)) == 0
 
     def rt_totals(self):
         a, o = ctypes.c_double(), ctypes.c_double()
@@ -337,6 +386,9 @@ class RefSim:
     def rt(self, d):
         self._rt = rt_struct(d)
         assert self.lib.ref_sim_rt(self.h, ctypes.byref(self._rt)) == 0
+
+    def conv_adj(self, iterations=1, soft=False):
+        assert self.lib.ref_sim_conv_adj(self.h, iterations, int(soft)) == 0
 
     def rt_totals(self):
         a, o = ctypes.c_double(), ctypes.c_double()

@@ -16,9 +16,9 @@ FP64, MIXED = 0, 1
 ENTROPY, ENERGY = 0, 1
 NO_BENCHMARK, HELD_SUAREZ = 0, 1
 
-E_ARG, E_CUDA, E_NAN, E_UNSUPPORTED, E_STATE = -1, -2, -3, -4, -5
+E_ARG, E_CUDA, E_NAN, E_UNSUPPORTED, E_STATE, E_CONVERGENCE = -1, -2, -3, -4, -5, -6
 ERRORS = {-1: "THORX_E_ARG", -2: "THORX_E_CUDA", -3: "THORX_E_NAN", -4: "THORX_E_UNSUPPORTED",
-          -5: "THORX_E_STATE"}
+          -5: "THORX_E_STATE", -6: "THORX_E_CONVERGENCE"}
 
 
 class ThorxError(RuntimeError):
@@ -131,6 +131,8 @@ def lib():
         L.thorx_device_sum_noalloc.restype = ci
         L.thorx_set_precision.argtypes = [vp, ci]
         L.thorx_set_precision.restype = ci
+        L.thorx_conv_adj_enable.argtypes = [vp, ci, ci]
+        L.thorx_conv_adj_enable.restype = ci
         L.thorx_bf16_gemm.argtypes = [vp, vp, ci, ci, ci, vp]
         L.thorx_bf16_gemm.restype = ci
         L.thorx_surrogate_last_error.restype = cp
@@ -176,7 +178,7 @@ EXPORTED = ["thorx_create", "thorx_destroy", "thorx_last_error", "thorx_field_si
             "thorx_surrogate_train", "thorx_surrogate_stats", "thorx_surrogate_layer",
             "thorx_surrogate_layer_grad", "thorx_surrogate_normalisation",
             "thorx_surrogate_forward_host", "thorx_surrogate_gradients_host",
-            "thorx_check_division"]
+            "thorx_check_division", "thorx_conv_adj_enable"]
 
 def device_sum(ptr, n, stream=0):
     """Compensated sum of n doubles at device address `ptr` (thorx_device_sum)."""
@@ -379,6 +381,10 @@ class Thorx:
 
     def set_precision(self, precision):
         self._check(lib().thorx_set_precision(self.h, precision))
+
+    def conv_adj(self, iterations=1, soft=False):
+        """Dry convective adjustment in every following ProfX (0 iterations: off)."""
+        self._check(lib().thorx_conv_adj_enable(self.h, iterations, int(soft)))
 
     # ---- RT surrogate ----
     def sur_create(self, hidden=512, train_batch=8192, log_capacity=0, recheck_period=16,

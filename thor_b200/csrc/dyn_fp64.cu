@@ -243,10 +243,120 @@ __global__ void level_tables_kernel(Geometry g, Phys P, double* lt) {
 
 // ---------------------------------------------------------------------------------------------
 // ProfX: Recompute_W (reference src/headers/phy/profx_auxiliary.h:109-130), Compute_temperature
-// (:64-92), held_suarez (src/headers/phy/profx_held_suarez.h:51-117), Compute_pressure (:94-107)
-// and the NaN check on temperature (:132-146, src/ESP/profx_driver.cu:389-396,451-458).
+// (:64-92), the dry convective adjustment when enabled (above), held_suarez
+// (src/headers/phy/profx_held_suarez.h:51-117), Compute_pressure (:94-107) and the NaN check on
+// temperature (:132-146, src/ESP/profx_driver.cu:389-396,451-458).
 // One thread per column (1% of a step).
 // ---------------------------------------------------------------------------------------------
+// ---------------------------------------------------------------------------------------------
+// Dry convective adjustment of one column, dry_conv_adj (src/headers/phy/dry_conv_adj.h:50-311),
+// the reference's operation sequence: potential temperature referred to the extrapolated surface
+// pressure; repeatedly the lowest unstable layer is found, the unstable stretch above it mixed to
+// the enthalpy-weighted mean (extended while the mean is unstable against the layer below or
+// above), then T and p recomputed; at most conv_adj_iter rounds. The interface pressures the
+// reference also stores are not used on this path and not written. The potential temperature
+// uses the pt plane as scratch (the dynamical core recomputes it before reading it). The
+// reference's loops end by construction; here each is also bounded (a mixing pass per layer, an
+// extension per layer), and a column that reaches a bound sets kFlagConvAdj and stops.
+// ---------------------------------------------------------------------------------------------
+__device__ void conv_adj_column(const Geometry& g, const Phys& P, const State& s, int c) {
+    const int     Np = g.Np, nv = g.nv;
+    const double* Alt  = g.Altitude;
+    const double* Alth = g.Altitudeh;
+    const double  stable = 0.0;
+    double*       pt  = s.pt;
+    double*       T   = s.T;
+    double*       p   = s.p;
+    const double* rho = s.Rho;
+    const double* Rd  = s.Rd;
+    const double* Cp  = s.Cp;
+    auto          at  = [&](int lev) { return lev * Np + c; };
+    int           iter   = 0;
+    bool          repeat = true;
+    while (repeat && iter < P.conv_adj_iter) {
+        double psm;
+        if (P.GravHeightVar)
+            psm = p[at(1)] - rho[at(0)] * P.Gravit * pow(P.A / (P.A + Alt[0]), 2) * (-Alt[0] - Alt[1]);
+        else
+            psm = p[at(1)] - rho[at(0)] * P.Gravit * (-Alt[0] - Alt[1]);
+        const double ps = 0.5 * (p[at(0)] + psm);
+        for (int lev = 0; lev < nv; lev++)
+            pt[at(lev)] = T[at(lev)] * pow(ps / p[at(lev)], Rd[at(lev)] / Cp[at(lev)]);
+        bool done_col = false;
+        int  passes   = 0;
+        while (!done_col) {
+            if (++passes > 2 * nv + 2) {
+                atomicOr(s.flags, kFlagConvAdj);
+                return;
+            }
+            int top = 0, bot = nv - 1;
+            for (int lev = 0; lev < nv - 1; lev++)
+                if (pt[at(lev + 1)] - pt[at(lev)] < stable && bot > lev)
+                    bot = lev;
+            for (int lev = bot; lev < nv - 1; lev++) {
+                if (pt[at(lev + 1)] - pt[at(lev)] > stable) {
+                    top = lev;
+                    break;
+                }
+                top = nv - 1;
+            }
+            if (bot < nv - 1) {
+                bool   extend = true;
+                int    ext    = 0;
+                double thnew  = 0.0;
+                while (extend) {
+                    if (++ext > nv + 2) {
+                        atomicOr(s.flags, kFlagConvAdj);
+                        return;
+                    }
+                    double h = 0.0, sum = 0.0;
+                    extend   = false;
+                    for (int lev = bot; lev <= top; lev++) {
+                        const double pi = pow(p[at(lev)] / ps, Rd[at(lev)] / Cp[at(lev)]);
+                        const double rho_g_dz = rho[at(lev)] * P.Gravit * (Alth[lev + 1] - Alth[lev]);
+                        h   = h + pt[at(lev)] * pi * rho_g_dz;
+                        sum = sum + pi * rho_g_dz;
+                    }
+                    thnew = h / sum;
+                    if (bot > 0 && (thnew - pt[at(bot - 1)]) < stable) {
+                        bot    = bot - 1;
+                        extend = true;
+                    }
+                    if (top < nv - 1 && (pt[at(top + 1)] - thnew) < stable) {
+                        top    = top + 1;
+                        extend = true;
+                    }
+                }
+                for (int lev = bot; lev <= top; lev++)
+                    pt[at(lev)] = thnew;
+            }
+            else
+                done_col = true;
+        }
+        repeat = false;
+        iter += 1;
+        if (P.conv_soft) {
+            for (int lev = 0; lev < nv; lev++) {
+                const int    i    = at(lev);
+                const double Ttmp = pt[i] * pow(p[i] / ps, Rd[i] / Cp[i]);
+                const double Ptmp = Ttmp * Rd[i] * rho[i];
+                pt[i]             = T[i] * pow(p[i] / ps, -Rd[i] / Cp[i]);
+                s.Qheat[i] += (Cp[i] - Rd[i]) / Rd[i] * (Ptmp - p[i]) / P.timestep;
+            }
+        }
+        else {
+            for (int lev = 0; lev < nv; lev++) {
+                const int i = at(lev);
+                T[i]        = pt[i] * pow(p[i] / ps, Rd[i] / Cp[i]);
+                p[i]        = T[i] * Rd[i] * rho[i];
+                pt[i]       = T[i] * pow(p[i] / ps, -Rd[i] / Cp[i]);
+                if (lev > 0 && pt[i] - pt[at(lev - 1)] < stable)
+                    repeat = true;
+            }
+        }
+    }
+}
+
 __global__ void __launch_bounds__(kColBlock) profx_kernel(Geometry g, Phys P, State s,
                                                           bool finish) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -266,6 +376,8 @@ __global__ void __launch_bounds__(kColBlock) profx_kernel(Geometry g, Phys P, St
         int i  = lev * Np + c;
         s.T[i] = s.p[i] / (s.Rd[i] * s.Rho[i]);
     }
+    if (P.conv_adj_iter > 0) // after the temperature, before the forcing (profx_driver.cu:239-290)
+        conv_adj_column(g, P, s, c);
     if (P.held_suarez) {
         const double sigmab = 0.7, ka = (1.0 / 40.0) * (1.0 / 86400.0), kf = 1.0 / 86400.0;
         const double ks = (1.0 / 4.0) * (1.0 / 86400.0), kappa = P.Rd / P.Cp, dTy = 60.0,

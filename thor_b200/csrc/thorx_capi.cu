@@ -227,10 +227,13 @@ int check_flags(thorx_ctx* ctx) {
                        cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     unsigned int f = *ctx->flags_host;
-    if (f & kFlagNaN) {
+    if (f)
         CK(cudaMemsetAsync(ctx->s.flags, 0, sizeof(unsigned int), ctx->stream));
+    if (f & kFlagNaN)
         return fail(ctx, THORX_E_NAN, "NaN in temperature after the physics step");
-    }
+    if (f & kFlagConvAdj)
+        return fail(ctx, THORX_E_CONVERGENCE,
+                    "convective adjustment: a column exceeded the pass bound");
     return 0;
 }
 
@@ -574,6 +577,8 @@ int thorx_create(const thorx_grid* gr, const thorx_params* pr, void* stream, tho
     P.energy          = pr->thermo_equation == THORX_ENERGY;
     P.held_suarez     = pr->core_benchmark == THORX_HELD_SUAREZ;
     P.mixed           = pr->precision == THORX_MIXED;
+    P.conv_adj_iter   = 0; // thorx_conv_adj_enable
+    P.conv_soft       = false;
 
     int rc;
     if ((rc = build_neighbours(ctx, gr)))
@@ -1105,6 +1110,24 @@ int thorx_set_precision(thorx_ctx* ctx, int precision) {
             ctx->graph = nullptr;
         }
         ctx->P.mixed = mixed;
+    }
+    return 0;
+}
+
+int thorx_conv_adj_enable(thorx_ctx* ctx, int iterations, int soft_adjustment) {
+    if (!ctx)
+        return THORX_E_ARG;
+    if (iterations < 0)
+        return fail(ctx, THORX_E_ARG, "thorx_conv_adj_enable: negative iteration count");
+    ctx->P.conv_adj_iter = iterations;
+    ctx->P.conv_soft     = soft_adjustment != 0;
+    if (ctx->graph_exec) { // the captured step holds the previous parameters
+        CK(cudaGraphExecDestroy(ctx->graph_exec));
+        ctx->graph_exec = nullptr;
+    }
+    if (ctx->graph) {
+        CK(cudaGraphDestroy(ctx->graph));
+        ctx->graph = nullptr;
     }
     return 0;
 }

@@ -96,6 +96,8 @@ struct Phys {
     int    HyDiffOrder;
     bool   DeepModel, NonHydro, GravHeightVar, HyDiff, DivDampP, energy, held_suarez;
     bool   mixed; // momentum-side horizontal stencils computed in FP32 (THORX_MIXED)
+    int    conv_adj_iter; // dry convective adjustment: iterations per step (0: off)
+    bool   conv_soft;     // its soft form (heating into profx_Qheat instead of T and p)
 };
 
 // Prognostic state (start of large step "x", RK stage "xk", small-step deviation "xs"),
@@ -116,10 +118,12 @@ struct State {
     double *vrows;                // 4 x (nv+1) planes: tridiagonal rows of the vertical solve
     double *SlowMh, *SlowWh, *SlowRho, *Slowp;
     double *Qheat, *dMh, *dWh;    // physics-module coupling (profx_Qheat_d, profx_dMh_d, ...)
-    unsigned int* flags;          // device status word (bit 0: NaN in temperature)
+    unsigned int* flags;          // device status word (kFlagNaN, kFlagConvAdj)
 };
 
-enum : unsigned int { kFlagNaN = 1u };
+// device-side error flags (State::flags), read by thorx_sync: a NaN in the temperature after
+// the physics step; a column whose convective adjustment exceeded its pass bound
+enum : unsigned int { kFlagNaN = 1u, kFlagConvAdj = 2u };
 
 // Largest nv the kernels take (levels per thread are unrolled into registers).
 int max_levels();

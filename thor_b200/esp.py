@@ -15,10 +15,10 @@ outputs, global diagnostics and log lines (src/esp.cu:1381-1480), batch and cont
 Differences, each stated where it applies:
   * state files are NumPy .npz archives, not HDF5 (there is no HDF5 library here); the arrays keep
     the reference's names and memory layout ([column][level][component]);
-  * keys for physics that this build does not implement (sponges, convective adjustment,
-    chemistry, boundary layer, ultra-hot thermodynamics, refined vertical grids, picket-fence or
-    two-stream RT, other initial profiles) are accepted at their default values and rejected
-    with an error naming the key otherwise;
+  * keys for physics that this build does not implement (sponges, the RayPH convective
+    adjustment, chemistry, boundary layer, ultra-hot thermodynamics, refined vertical grids,
+    picket-fence or two-stream RT, other initial profiles) are accepted at their default values
+    and rejected with an error naming the key otherwise;
   * output_mean, out_interm_momentum and output_diffusion only add arrays to the output files in
     the reference; here they are accepted and a warning says the arrays are not written;
   * one extension key, `precision` = fp64 (default) | mixed, selects the compute form.
@@ -122,10 +122,10 @@ KEYS = {
     "initial": (str, "ifile/esp_initial.h5", "path"),
     "core_benchmark": (str, "HeldSuarez", "path"),
     "init_PT_profile": (str, "isothermal", "fixed"),
-    "conv_adj": (bool, False, "fixed"),
-    "conv_adj_iter": (int, 1, "ignored"),
-    "soft_adjustment": (bool, False, "ignored"),
-    "conv_adj_type": (str, "hourdin", "ignored"),
+    "conv_adj": (bool, False, "path"),
+    "conv_adj_iter": (int, 1, "path"),
+    "soft_adjustment": (bool, False, "path"),
+    "conv_adj_type": (str, "hourdin", "fixed"),
     "GPU_ID_N": (int, 0, "path"),
     "n_out": (int, 1000, "path"),
     "results_path": (str, "results", "path"),
@@ -192,6 +192,7 @@ KEYS = {
 }
 # values a "fixed" key may take (its default unless listed)
 ALLOWED = {"init_PT_profile": ("isothermal",), "rt_type": ("DualbandGray",),
+           "conv_adj_type": ("hourdin", "Hourdin"),
            "ultrahot_thermo": ("none",), "ultrahot_heating": ("none",),
            "insol_avg": ("NoInsolAvg",)}
 CHOICES = {"core_benchmark": ("HeldSuarez", "NoBenchmark"),
@@ -517,6 +518,8 @@ def run(argv=None, out=sys.stdout):
             x.init_rest_state(c["Tmean"], 0, 0.0)
         if c["radiative_transfer"]:
             x.rt_enable(rt_config(c, step_idx))
+        if c["conv_adj"]:
+            x.conv_adj(c["conv_adj_iter"], c["soft_adjustment"])
         nsmax = c["num_steps"]
         logs = Logs(out_dir, sim_id, continuing, c["globdiag"])
         grid_file = os.path.join(out_dir, "esp_output_grid_%s.npz" % sim_id)
