@@ -64,9 +64,12 @@ typedef struct {
 #define THORX_ENTROPY 0
 #define THORX_ENERGY 1
 
-/* Benchmark forcing (reference .thr key core_benchmark). */
+/* Benchmark forcing (reference .thr key core_benchmark; the values of the reference's
+ * benchmark_types, src/headers/define.h:151-160). */
 #define THORX_NO_BENCHMARK 0
 #define THORX_HELD_SUAREZ 1
+#define THORX_TIDALLY_LOCKED_EARTH 2 /* tidalearth, src/headers/phy/profx_tidalearth.h:49-126   */
+#define THORX_SHALLOW_HOT_JUPITER 3  /* shallowHJ, src/headers/phy/profx_shallowHJ.h:50-128     */
 
 /* Simulation switches: the SimulationSetup members the step reads
  * (src/headers/simulation_setup.h) and the .thr keys they come from. */
@@ -88,7 +91,7 @@ typedef struct {
     int    HyDiff;       /*                                   (HyDiff)          */
     int    DivDampP;     /*                                   (DivDampP)        */
     int    thermo_equation; /* THORX_ENTROPY | THORX_ENERGY   (thermo_equation) */
-    int    core_benchmark;  /* THORX_NO_BENCHMARK | THORX_HELD_SUAREZ           */
+    int    core_benchmark;  /* THORX_NO_BENCHMARK .. THORX_SHALLOW_HOT_JUPITER   */
     int    precision;       /* THORX_FP64 | THORX_MIXED                         */
 } thorx_params;
 

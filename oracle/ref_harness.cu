@@ -42,6 +42,8 @@
 #include "phy/profx_auxiliary.h"
 #include "phy/profx_globdiag.h"
 #include "phy/profx_held_suarez.h"
+#include "phy/profx_shallowHJ.h"
+#include "phy/profx_tidalearth.h"
 #include "physical_constants.h"
 #include "profx_RT.h"
 #include "reduction_add.h"
@@ -520,10 +522,23 @@ static int ref_profx(RefSim* s) {
                                     s->p.GravHeightVar);
         REF_CHECK(cudaDeviceSynchronize());
     }
-    if (s->p.held_suarez) {
+    // benchmark forcing, profx_driver.cu:300-360 (held_suarez carries the benchmark_types value)
+    if (s->p.held_suarez == 1) {
         held_suarez<<<NB, NTH>>>(F["Mh"], F["pressure"], F["Rho"], F["temperature"], s->p.Gravit,
                                  s->p.Cp, s->p.Rd, F["Altitude"], F["Altitudeh"], F["lonlat"],
                                  s->p.timestep, N);
+        REF_CHECK(cudaDeviceSynchronize());
+    }
+    else if (s->p.held_suarez == 2) {
+        tidalearth<<<NB, NTH>>>(F["Mh"], F["pressure"], F["Rho"], F["temperature"], s->p.Gravit,
+                                s->p.Cp, s->p.Rd, F["Altitude"], F["Altitudeh"], F["lonlat"],
+                                s->p.timestep, N);
+        REF_CHECK(cudaDeviceSynchronize());
+    }
+    else if (s->p.held_suarez == 3) {
+        shallowHJ<<<NB, NTH>>>(F["Mh"], F["pressure"], F["Rho"], F["temperature"], s->p.Gravit,
+                               s->p.Cp, s->p.Rd, F["Altitude"], F["Altitudeh"], F["lonlat"],
+                               s->p.timestep, N);
         REF_CHECK(cudaDeviceSynchronize());
     }
     if (s->rt && ref_rt_step(s))

@@ -486,6 +486,69 @@ void rt_step(Oracle& o) {
     o.nstep++;
 }
 
+// tidalearth, src/headers/phy/profx_tidalearth.h:49-126 (core_benchmark = 2)
+void tidal_earth(Oracle& o) {
+    int   N = o.N, nv = o.nv;
+    Vec & Mh = F(o, "Mh"), &p = F(o, "pressure"), &rho = F(o, "Rho"), &T = F(o, "temperature");
+    double Gravit = o.P.Gravit, Cp = o.P.Cp, Rd = o.P.Rd, dt = o.P.timestep;
+#pragma omp parallel for schedule(static)
+    for (int id = 0; id < N; id++)
+        for (int lev = 0; lev < nv; lev++) {
+            double sigmab = 0.7, ka = (1.0 / 40.0) * (1.0 / 86400.0), kf = 1.0 / 86400.0;
+            double ks = (1.0 / 4.0) * (1.0 / 86400.0), kappa = Rd / Cp, dTy = 60.0, dthetaz = 10.0;
+            double p0 = 100000.0, lat = o.lonlat[id * 2 + 1], lon = o.lonlat[id * 2];
+            double psm1 = p[id * nv + 1] - rho[id * nv + 0] * Gravit
+                                               * (-o.Altitude[0] - o.Altitude[1]);
+            double ps     = 0.5 * (p[id * nv + 0] + psm1);
+            double pre    = p[id * nv + lev];
+            double sigma  = (pre / ps);
+            double sigma0 = (pre / p0);
+            double Teq    = std::fmax(200.0, (315.0 + dTy * cos(lon - M_PI) * cos(lat)
+                                           - dthetaz * log(sigma0) * pow(cos(lat), 2.0))
+                                              * pow(sigma0, kappa));
+            double kt = ka
+                        + (ks - ka) * std::fmax(0.0, (sigma - sigmab) / (1.0 - sigmab))
+                              * pow(cos(lat), 4.0);
+            double kv = kf * std::fmax(0.0, (sigma - sigmab) / (1.0 - sigmab));
+            for (int k = 0; k < 3; k++)
+                Mh[(id * nv + lev) * 3 + k] = Mh[(id * nv + lev) * 3 + k] / (1.0 + kv * dt);
+            T[id * nv + lev] -= kt * dt * (T[id * nv + lev] - Teq);
+        }
+}
+
+// shallowHJ, src/headers/phy/profx_shallowHJ.h:50-128 (core_benchmark = 3)
+void shallow_hot_jupiter(Oracle& o) {
+    int   N = o.N, nv = o.nv;
+    Vec & Mh = F(o, "Mh"), &p = F(o, "pressure"), &rho = F(o, "Rho"), &T = F(o, "temperature");
+    double Gravit = o.P.Gravit, dt = o.P.timestep;
+    const double dTy = 300.0, zstra = 2e6, sigma_stra = 0.12, Gamma_trop = 2e-4, T_surf = 1600,
+                 Delta_Tstra = 10;
+#pragma omp parallel for schedule(static)
+    for (int id = 0; id < N; id++)
+        for (int lev = 0; lev < nv; lev++) {
+            double lat = o.lonlat[id * 2 + 1], lon = o.lonlat[id * 2];
+            double psm1 = p[id * nv + 1] - rho[id * nv + 0] * Gravit
+                                               * (-o.Altitude[0] - o.Altitude[1]);
+            double ps    = 0.5 * (p[id * nv + 0] + psm1);
+            double sigma = (p[id * nv + lev] / ps);
+            double z     = o.Altitude[lev], beta_trop, T_vert;
+            if (z <= zstra) {
+                beta_trop = sin(0.5 * M_PI * (sigma - sigma_stra) / (1.0 - sigma_stra));
+                T_vert    = T_surf - Gamma_trop * (zstra + 0.5 * (z - zstra))
+                         + sqrt(pow(0.5 * Gamma_trop * (z - zstra), 2) + Delta_Tstra * Delta_Tstra);
+            }
+            else {
+                beta_trop = 0.0;
+                T_vert    = T_surf - Gamma_trop * zstra + Delta_Tstra;
+            }
+            double Teq = T_vert + beta_trop * dTy * cos(lon - M_PI) * cos(lat);
+            double kt = 1 / (1.5e5), kv = 0.0;
+            for (int k = 0; k < 3; k++)
+                Mh[(id * nv + lev) * 3 + k] = Mh[(id * nv + lev) * 3 + k] / (1.0 + kv * dt);
+            T[id * nv + lev] -= kt * dt * (T[id * nv + lev] - Teq);
+        }
+}
+
 // dry_conv_adj, src/headers/phy/dry_conv_adj.h:50-311 (conv_adj_type = hourdin): per column,
 // the same sequence and the same pass bounds as the product (the reference's loops have none).
 void dry_conv_adj(Oracle& o) {
@@ -595,8 +658,12 @@ void profx(Oracle& o) {
     compute_temperature(o);
     if (o.conv_adj_iter > 0)
         dry_conv_adj(o);
-    if (o.P.held_suarez)
+    if (o.P.held_suarez == 1)
         held_suarez(o);
+    else if (o.P.held_suarez == 2)
+        tidal_earth(o);
+    else if (o.P.held_suarez == 3)
+        shallow_hot_jupiter(o);
     if (o.rt)
         rt_step(o);
     compute_pressure(o);

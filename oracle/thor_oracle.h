@@ -12,6 +12,8 @@ extern "C" {
 typedef struct {
     double A, Omega, Gravit, Rd, Cp, P_Ref, timestep, Diffc, DivDampc;
     int    HyDiffOrder;
+    // held_suarez: the benchmark forcing, benchmark_types values (0 none, 1 Held-Suarez,
+    // 2 tidally locked Earth, 3 shallow hot Jupiter)
     int    DeepModel, NonHydro, GravHeightVar, HyDiff, DivDampP, energy_equation, held_suarez;
     int    glevel;
 } oracle_params;

@@ -16,8 +16,15 @@ from thorx_testlib import (RefGrid, RefSim, STATE_FIELDS, field_tolerance, grid_
 TEND = ["SlowMh", "SlowWh", "SlowRho", "Slowpressure"]
 TIGHT = {"Rho", "pressure", "temperature"}
 
+# the shallow hot Jupiter of the reference's ifile/shallowhj.thr (shallow model, 1e8 m, g = 8)
+SHALLOW_HJ = dict(A=1e8, Omega=2.1e-5, Gravit=8.0, Rd=3779.0, Cp=13226.5, Tmean=1600.0,
+                  P_Ref=1e5, Top_altitude=4875000.0, Diffc=0.019921, DivDampc=0.019921,
+                  DeepModel=0, held_suarez=3)
+
 CASES = [
     (4, 8, 1200.0, {}),
+    (4, 16, 600.0, dict(held_suarez=2, Omega=1.9964407939767282e-07)),  # tidally locked Earth
+    (4, 12, 600.0, SHALLOW_HJ),
     (4, 32, 1200.0, {}),
     (4, 16, 1200.0, dict(DeepModel=0, NonHydro=0, energy_equation=1)),
     (4, 16, 1200.0, dict(GravHeightVar=1, energy_equation=1)),
@@ -27,8 +34,8 @@ CASES = [
 
 
 def run_case(glevel, nv, dt, over, nsteps=1, use_graph=False):
-    g = RefGrid(glevel, nv)
     p, c = make_params(glevel, dt, **over)
+    g = RefGrid(glevel, nv, A=c["A"], top=c["Top_altitude"])
     ic = initial_state(g.arrays, g.point_num, g.nv, c)
     s, sn = RefSim(g, p), RefSim(g, p, nofma=True)
     x = thor_b200.Thorx(grid_dict(g), glevel, thorx_params(c, dt))

@@ -21,6 +21,7 @@
 // Stencils are templated on the ring size (6, or 5 at pentagons and poles) so that every index
 // is static and the ring values stay in registers.
 
+#include "thorx.h"
 #include "thorx_internal.h"
 
 namespace thorx {
@@ -243,9 +244,9 @@ __global__ void level_tables_kernel(Geometry g, Phys P, double* lt) {
 
 // ---------------------------------------------------------------------------------------------
 // ProfX: Recompute_W (reference src/headers/phy/profx_auxiliary.h:109-130), Compute_temperature
-// (:64-92), the dry convective adjustment when enabled (above), held_suarez
-// (src/headers/phy/profx_held_suarez.h:51-117), Compute_pressure (:94-107) and the NaN check on
-// temperature (:132-146, src/ESP/profx_driver.cu:389-396,451-458).
+// (:64-92), the dry convective adjustment when enabled (above), the benchmark forcing (held_suarez,
+// src/headers/phy/profx_held_suarez.h:51-117; tidalearth; shallowHJ), Compute_pressure (:94-107)
+// and the NaN check on temperature (:132-146, src/ESP/profx_driver.cu:389-396,451-458).
 // One thread per column (1% of a step).
 // ---------------------------------------------------------------------------------------------
 // ---------------------------------------------------------------------------------------------
@@ -397,6 +398,67 @@ __global__ void __launch_bounds__(kColBlock) profx_kernel(Geometry g, Phys P, St
                         + (ks - ka) * fmax(0.0, (sigma - sigmab) / (1.0 - sigmab))
                               * pow(cos(lat), 4.0);
             double kv = kf * fmax(0.0, (sigma - sigmab) / (1.0 - sigmab));
+            for (int k = 0; k < 3; k++) {
+                int j   = (k * nv + lev) * Np + c;
+                s.Mh[j] = s.Mh[j] / (1.0 + kv * P.timestep);
+            }
+            s.T[i] -= kt * P.timestep * (s.T[i] - Teq);
+        }
+    }
+    else if (P.benchmark == THORX_TIDALLY_LOCKED_EARTH) {
+        // tidalearth (src/headers/phy/profx_tidalearth.h:49-126): Held-Suarez with the
+        // equilibrium temperature of Heng, Menou & Phillips (2011), eq. 21, centred on the
+        // substellar point (longitude pi)
+        const double sigmab = 0.7, ka = (1.0 / 40.0) * (1.0 / 86400.0), kf = 1.0 / 86400.0;
+        const double ks = (1.0 / 4.0) * (1.0 / 86400.0), kappa = P.Rd / P.Cp, dTy = 60.0,
+                     dthetaz = 10.0, p0 = 100000.0;
+        const double lat  = g.lat[c], lon = g.lon[c];
+        const double psm1 = s.p[Np + c] - s.Rho[c] * P.Gravit * (-Alt[0] - Alt[1]);
+        const double ps   = 0.5 * (s.p[c] + psm1);
+        for (int lev = 0; lev < nv; lev++) {
+            int    i      = lev * Np + c;
+            double pre    = s.p[i];
+            double sigma  = (pre / ps);
+            double sigma0 = (pre / p0);
+            double Teq    = fmax(200.0, (315.0 + dTy * cos(lon - M_PI) * cos(lat)
+                                      - dthetaz * log(sigma0) * pow(cos(lat), 2.0))
+                                         * pow(sigma0, kappa));
+            double kt = ka
+                        + (ks - ka) * fmax(0.0, (sigma - sigmab) / (1.0 - sigmab))
+                              * pow(cos(lat), 4.0);
+            double kv = kf * fmax(0.0, (sigma - sigmab) / (1.0 - sigmab));
+            for (int k = 0; k < 3; k++) {
+                int j   = (k * nv + lev) * Np + c;
+                s.Mh[j] = s.Mh[j] / (1.0 + kv * P.timestep);
+            }
+            s.T[i] -= kt * P.timestep * (s.T[i] - Teq);
+        }
+    }
+    else if (P.benchmark == THORX_SHALLOW_HOT_JUPITER) {
+        // shallowHJ (src/headers/phy/profx_shallowHJ.h:50-128): Newtonian cooling towards the
+        // hot-Jupiter profile of Heng, Menou & Phillips (2011), eqs. 23-25; no friction
+        const double dTy = 300.0, zstra = 2e6, sigma_stra = 0.12, Gamma_trop = 2e-4,
+                     T_surf = 1600, Delta_Tstra = 10;
+        const double lat  = g.lat[c], lon = g.lon[c];
+        const double psm1 = s.p[Np + c] - s.Rho[c] * P.Gravit * (-Alt[0] - Alt[1]);
+        const double ps   = 0.5 * (s.p[c] + psm1);
+        for (int lev = 0; lev < nv; lev++) {
+            int    i     = lev * Np + c;
+            double sigma = (s.p[i] / ps);
+            double beta_trop, T_vert;
+            if (Alt[lev] <= zstra) {
+                beta_trop = sin(0.5 * M_PI * (sigma - sigma_stra) / (1.0 - sigma_stra));
+                T_vert    = T_surf - Gamma_trop * (zstra + 0.5 * (Alt[lev] - zstra))
+                         + sqrt(pow(0.5 * Gamma_trop * (Alt[lev] - zstra), 2)
+                                + Delta_Tstra * Delta_Tstra);
+            }
+            else {
+                beta_trop = 0.0;
+                T_vert    = T_surf - Gamma_trop * zstra + Delta_Tstra;
+            }
+            const double Teq = T_vert + beta_trop * dTy * cos(lon - M_PI) * cos(lat);
+            const double kt  = 1 / (1.5e5);
+            const double kv  = 0.0;
             for (int k = 0; k < 3; k++) {
                 int j   = (k * nv + lev) * Np + c;
                 s.Mh[j] = s.Mh[j] / (1.0 + kv * P.timestep);

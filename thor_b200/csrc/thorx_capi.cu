@@ -283,7 +283,7 @@ double class_bytes(const thorx_ctx* ctx, int k) {
     const double ring_geo = 78 * G + 6 * I + N; // areas, areasTr, nvecoa/ti/te, ring, flag
     switch (k) {
     case KProfx: // Wh, p, Rd, Rho, Mh | W, T, p, Mh
-        return Si + 3 * S + (P.held_suarez ? 3 * S : 0) + G + 3 * S + (P.held_suarez ? 3 * S : 0);
+        return Si + 3 * S + (P.benchmark ? 3 * S : 0) + G + 3 * S + (P.benchmark ? 3 * S : 0);
     case KAdvTemp: // Mhk, Rhok, Wk, Whk, pk, Rd, Cp | Adv, T, h, hh, pt, pth, gtil, gtilh
         return 7 * S + Si + 21 * G + 3 * G + 6 * I + 7 * S + 3 * Si
                + (P.energy ? 3 * S + 2 * Si - 2 * S - Si : 0);
@@ -541,7 +541,7 @@ int thorx_create(const thorx_grid* gr, const thorx_params* pr, void* stream, tho
         return fail(ctx, THORX_E_ARG, "precision: THORX_FP64 or THORX_MIXED");
     if (pr->thermo_equation != THORX_ENTROPY && pr->thermo_equation != THORX_ENERGY)
         return fail(ctx, THORX_E_ARG, "thermo_equation");
-    if (pr->core_benchmark != THORX_NO_BENCHMARK && pr->core_benchmark != THORX_HELD_SUAREZ)
+    if (pr->core_benchmark < THORX_NO_BENCHMARK || pr->core_benchmark > THORX_SHALLOW_HOT_JUPITER)
         return fail(ctx, THORX_E_UNSUPPORTED, "core_benchmark");
     if (pr->timestep <= 0 || pr->A <= 0)
         return fail(ctx, THORX_E_ARG, "timestep and radius must be positive");
@@ -576,6 +576,7 @@ int thorx_create(const thorx_grid* gr, const thorx_params* pr, void* stream, tho
     P.DivDampP        = pr->DivDampP != 0;
     P.energy          = pr->thermo_equation == THORX_ENERGY;
     P.held_suarez     = pr->core_benchmark == THORX_HELD_SUAREZ;
+    P.benchmark       = pr->core_benchmark;
     P.mixed           = pr->precision == THORX_MIXED;
     P.conv_adj_iter   = 0; // thorx_conv_adj_enable
     P.conv_soft       = false;

@@ -95,6 +95,7 @@ struct Phys {
     double A, Omega, Gravit, Rd, Cp, P_Ref, timestep;
     int    HyDiffOrder;
     bool   DeepModel, NonHydro, GravHeightVar, HyDiff, DivDampP, energy, held_suarez;
+    int    benchmark; // THORX_NO_BENCHMARK .. THORX_SHALLOW_HOT_JUPITER (forcing in ProfX)
     bool   mixed; // momentum-side horizontal stencils computed in FP32 (THORX_MIXED)
     int    conv_adj_iter; // dry convective adjustment: iterations per step (0: off)
     bool   conv_soft;     // its soft form (heating into profx_Qheat instead of T and p)

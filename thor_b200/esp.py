@@ -195,7 +195,8 @@ ALLOWED = {"init_PT_profile": ("isothermal",), "rt_type": ("DualbandGray",),
            "conv_adj_type": ("hourdin", "Hourdin"),
            "ultrahot_thermo": ("none",), "ultrahot_heating": ("none",),
            "insol_avg": ("NoInsolAvg",)}
-CHOICES = {"core_benchmark": ("HeldSuarez", "NoBenchmark"),
+CHOICES = {"core_benchmark": ("HeldSuarez", "NoBenchmark", "TidallyLockedEarth",
+                              "ShallowHotJupiter"),
            "thermo_equation": ("entropy", "energy"), "precision": ("fp64", "mixed")}
 
 
@@ -281,7 +282,8 @@ def thorx_params(c):
                 NonHydro=int(c["NonHydro"]), GravHeightVar=int(c["GravHeightVar"]),
                 HyDiff=int(c["HyDiff"]), DivDampP=int(c["DivDampP"]),
                 thermo_equation=1 if c["thermo_equation"] == "energy" else 0,
-                core_benchmark=1 if c["core_benchmark"] == "HeldSuarez" else 0,
+                core_benchmark={"NoBenchmark": 0, "HeldSuarez": 1, "TidallyLockedEarth": 2,
+                                "ShallowHotJupiter": 3}[c["core_benchmark"]],
                 precision=1 if c["precision"] == "mixed" else 0)
 
 
