@@ -2092,10 +2092,14 @@ double to_bf16(double v) {
     std::memcpy(&f, &u, 4);
     return f;
 }
-double gelu(double z) { return 0.5 * z * (1.0 + std::erf(z / std::sqrt(2.0))); }
+// GELU in its tanh form, as the GPU's epilogue computes it (thor_b200/csrc/umma.cuh)
+double gelu(double z) {
+    const double c = std::sqrt(2.0 / M_PI), a = 0.044715;
+    return 0.5 * z * (1.0 + std::tanh(c * (z + a * z * z * z)));
+}
 double gelu_grad(double z) {
-    return 0.5 * (1.0 + std::erf(z / std::sqrt(2.0)))
-           + z * std::exp(-0.5 * z * z) / std::sqrt(2.0 * M_PI);
+    const double c = std::sqrt(2.0 / M_PI), a = 0.044715, t = std::tanh(c * (z + a * z * z * z));
+    return 0.5 * (1.0 + t) + 0.5 * z * (1.0 - t * t) * c * (1.0 + 3.0 * a * z * z);
 }
 } // namespace
 
@@ -2184,7 +2188,8 @@ extern "C" int oracle_mlp(int nv, int H, const float* const* W, const float* con
                 double sum = 0.0;
                 for (int n = 0; n < N[l]; n++)
                     sum += G[(size_t)r * N[l] + n] * Wb[l][(size_t)n * K[l] + k];
-                Gn[(size_t)r * K[l] + k] = to_bf16(sum * gelu_grad(Z[l - 1][(size_t)r * K[l] + k]));
+                Gn[(size_t)r * K[l] + k] =
+                    to_bf16(sum * to_bf16(gelu_grad(Z[l - 1][(size_t)r * K[l] + k])));
             }
         G.swap(Gn);
     }

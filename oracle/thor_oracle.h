@@ -65,8 +65,9 @@ int    oracle_globdiag(void* h, double* out, double* abs_out);
 // Compensated (Neumaier) sum of x[0..n-1] in index order.
 double oracle_sum(const double* x, long n);
 // The RT surrogate MLP (thor_b200/csrc/surrogate.cu) in float64 on the CPU, with the GPU's
-// bf16 rounding points: inputs, weights and hidden activations rounded to bf16, the output
-// gradient and the pre-activation gradients rounded to bf16 where the GPU feeds them to a GEMM.
+// bf16 rounding points: inputs, weights and hidden activations rounded to bf16, the GELU
+// derivatives rounded to bf16 (as stored for the backward pass), the output gradient and the
+// pre-activation gradients rounded to bf16 where the GPU feeds them to a GEMM. GELU in its tanh form.
 // Shapes padded as on the GPU: layer l has W[l] [N_l][K_l], b[l] [N_l] (N = H, H, H, Nout;
 // K = Kin, H, H, H). x [B][n_in], t [B][nv] standardised; outputs y [B][nv], loss (mean squared
 // error), gradients gW[l] (same shape as W[l]) and gb[l]. t, gW, gb may be null (forward only).

@@ -82,13 +82,19 @@ __global__ void adam_kernel(float* w, float* m, float* v, const float* g, int n,
 // ---- batch assembly -------------------------------------------------------------------------
 // Standardised bf16 features of the grid columns at the physics step: T, log p per level, and
 // cos zenith; rows >= N and features >= n_in are zero.
-__global__ void features_state_kernel(SurNet net, Geometry g, State s, const double* cos_zenith,
-                                      bf16* X0, int Brows) {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= Brows)
-        return;
+// Standardised bf16 features of the columns in the step (rows >= N: zero), 32 columns per block:
+// the warps compute with lanes across columns (coalesced level planes) into a shared tile, then
+// write each column's row of Kin features contiguously.
+constexpr int kFeatCols = 32, kFeatWarps = 8;
+__global__ void __launch_bounds__(kFeatCols* kFeatWarps)
+    features_state_kernel(SurNet net, Geometry g, State s, const double* cos_zenith, bf16* X0,
+                          int Brows) {
+    extern __shared__ bf16 tile[]; // [32][Kin + 2]: an odd number of 4-byte words per row
+    const int pitch = net.Kin + 2;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int r0 = blockIdx.x * kFeatCols, r = r0 + lane;
     const int nv = net.nv;
-    for (int j = 0; j < net.Kin; j++) {
+    for (int j = w; j < net.Kin; j += kFeatWarps) {
         float x = 0.0f;
         if (r < g.N && j < net.n_in) {
             double raw;
@@ -100,7 +106,16 @@ __global__ void features_state_kernel(SurNet net, Geometry g, State s, const dou
                 raw = cos_zenith[r];
             x = (float)((raw - net.in_mean[j]) / net.in_std[j]);
         }
-        X0[(size_t)r * net.Kin + j] = __float2bfloat16_rn(x);
+        tile[lane * pitch + j] = __float2bfloat16_rn(x);
+    }
+    __syncthreads();
+    for (int rr = w; rr < kFeatCols; rr += kFeatWarps) {
+        if (r0 + rr >= Brows)
+            break;
+        bf16* dst = X0 + (size_t)(r0 + rr) * net.Kin;
+        for (int j = 2 * lane; j < net.Kin; j += 64)
+            *reinterpret_cast<__nv_bfloat162*>(dst + j) =
+                __halves2bfloat162(tile[rr * pitch + j], tile[rr * pitch + j + 1]);
     }
 }
 
@@ -223,47 +238,79 @@ __global__ void transpose_bf16_kernel(const bf16* src, bf16* dst, int R, int C, 
 // re-checked this step or has fallen back; a re-checked column falls back (or returns to the
 // surrogate) according to its relative error max|Qs - Qrt| / max|Qrt|. Then the cooling limiter
 // and the coupling into profx_Qheat as the plain RT does (profx_RT.h:560-584).
-__global__ void combine_kernel(SurNet net, Geometry g, Phys P, State s, RtFields f, const float* Y,
-                               uint8_t* fallback, int period, double tol, unsigned int* stats) {
-    const int id = blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= g.N)
-        return;
+// 32 columns per block (lane = column) x kCombGroups warps over the levels (warp y: levels y,
+// y + kCombGroups, ...); the re-check's column maxima are reduced over the warps in shared memory.
+constexpr int kCombGroups = 8;
+__global__ void __launch_bounds__(32 * kCombGroups)
+    combine_kernel(SurNet net, Geometry g, Phys P, State s, RtFields f, const float* Yt, int ldy,
+                   uint8_t* fallback, int period, double tol, unsigned int* stats) {
+    __shared__ double snum[kCombGroups][32], sden[kCombGroups][32];
+    __shared__ int    s_use[32];
+    const int    lane = threadIdx.x & 31, y = threadIdx.x >> 5;
+    const int    id = blockIdx.x * 32 + lane;
     const RtStep st = *f.step;
-    if (!st.run)
+    if (!st.run) // uniform: the RT does not run this step
         return;
+    const bool valid   = id < g.N;
     const int  nv = g.nv, Np = g.Np;
-    const bool recheck = id % period == (int)(st.cur % period);
-    const bool use_rt  = fallback[id] != 0 || recheck;
+    const bool recheck = valid && id % period == (int)(st.cur % period);
     // heating rates compared as temperature tendencies (K/s): the thin upper layers, whose
     // W/m^3 are small, weigh as much as their temperature change does
     auto rho_cv = [&](int lev) {
         const size_t i = (size_t)lev * Np + id;
         return s.Rho[i] * (s.Cp[i] - s.Rd[i]);
     };
-    if (recheck) {
-        double num = 0.0, den = 0.0;
-        for (int lev = 0; lev < nv; lev++) {
-            const double qs =
-                (double)Y[(size_t)id * net.Nout + lev] * net.out_std[lev] + net.out_mean[lev];
+    auto sur = [&](int lev) { // the network's heating rate at this level, K/s
+        return (double)Yt[(size_t)lev * ldy + id] * net.out_std[lev] + net.out_mean[lev];
+    };
+    double num = 0.0, den = 0.0;
+    if (recheck)
+        for (int lev = y; lev < nv; lev += kCombGroups) {
             const double qr = f.dtemp[(size_t)lev * Np + id] / rho_cv(lev);
-            num             = fmax(num, fabs(qs - qr));
+            num             = fmax(num, fabs(sur(lev) - qr));
             den             = fmax(den, fabs(qr));
         }
-        const double err = den > 0.0 ? num / den : (num > 0.0 ? 1.0e300 : 0.0);
-        fallback[id]     = err > tol ? 1 : 0;
-        atomicAdd(&stats[0], 1u); // columns re-checked
-        if (err > tol)
-            atomicAdd(&stats[1], 1u); // re-checks that failed
-        atomicMax(&stats[2], (unsigned)fmin(err * 1e6, 4.0e9)); // largest error, 1e-6 units
+    snum[y][lane] = num;
+    sden[y][lane] = den;
+    __syncthreads();
+    if (y == 0) {
+        unsigned int err_e6 = 0;
+        bool         failed = false;
+        if (recheck) {
+            for (int k = 1; k < kCombGroups; k++) {
+                num = fmax(num, snum[k][lane]);
+                den = fmax(den, sden[k][lane]);
+            }
+            const double err = den > 0.0 ? num / den : (num > 0.0 ? 1.0e300 : 0.0);
+            failed           = err > tol;
+            fallback[id]     = failed ? 1 : 0;
+            err_e6           = (unsigned)fmin(err * 1e6, 4.0e9);
+        }
+        const bool use_rt = valid && (fallback[id] != 0 || recheck);
+        s_use[lane]       = use_rt;
+        // statistics, one atomic per block: re-checked, failed, largest error (1e-6), plain RT
+        const unsigned n_re = __popc(__ballot_sync(0xffffffffu, recheck));
+        const unsigned n_fa = __popc(__ballot_sync(0xffffffffu, failed));
+        const unsigned n_rt = __popc(__ballot_sync(0xffffffffu, use_rt));
+        const unsigned mx   = __reduce_max_sync(0xffffffffu, err_e6);
+        if (lane == 0) {
+            if (n_re)
+                atomicAdd(&stats[0], n_re);
+            if (n_fa)
+                atomicAdd(&stats[1], n_fa);
+            if (n_re)
+                atomicMax(&stats[2], mx);
+            if (n_rt)
+                atomicAdd(&stats[3], n_rt);
+        }
     }
-    if (use_rt)
-        atomicAdd(&stats[3], 1u); // columns heated by the plain RT
-    for (int lev = 0; lev < nv; lev++) {
+    __syncthreads();
+    if (!valid)
+        return;
+    const bool use_rt = s_use[lane] != 0;
+    for (int lev = y; lev < nv; lev += kCombGroups) {
         const int i = lev * Np + id;
-        double    d = use_rt ? f.dtemp[i]
-                             : ((double)Y[(size_t)id * net.Nout + lev] * net.out_std[lev]
-                                + net.out_mean[lev])
-                                   * rho_cv(lev);
+        double    d = use_rt ? f.dtemp[i] : sur(lev) * rho_cv(lev);
         if (s.p[i] + s.Rd[i] / (s.Cp[i] - s.Rd[i]) * d * P.timestep < 0)
             d = -s.p[i] / P.timestep;
         f.dtemp[i] = d;
@@ -379,6 +426,7 @@ int Surrogate::init(int nv_, int hidden, long long log_capacity, int batch_rows,
     }
     const size_t B = Bcap;
     if (!alloc((void**)&X0, B * net.Kin * 2) || !alloc((void**)&Y, B * net.Nout * 4)
+        || !alloc((void**)&Yt, B * net.Nout * 4)
         || !alloc((void**)&tgt, B * net.Nout * 4) || !alloc((void**)&dYf, B * net.Nout * 4)
         || !alloc((void**)&dY, B * net.Nout * 2) || !alloc((void**)&dZ[0], B * net.H * 2)
         || !alloc((void**)&dZ[1], B * net.H * 2)
@@ -391,7 +439,7 @@ int Surrogate::init(int nv_, int hidden, long long log_capacity, int batch_rows,
         || !alloc((void**)&stats, 16))
         return THORX_E_CUDA;
     for (int l = 0; l < 3; l++)
-        if (!alloc((void**)&Z[l], B * net.H * 4) || !alloc((void**)&A[l], B * net.H * 2))
+        if (!alloc((void**)&Gd[l], B * net.H * 2) || !alloc((void**)&A[l], B * net.H * 2))
             return THORX_E_CUDA;
     log.cap = log_capacity;
     if (log_capacity > 0)
@@ -419,26 +467,34 @@ void Surrogate::cast_all(cudaStream_t st) {
     }
 }
 
-// Y = net(X0) for the first B rows (B a multiple of 128).
-void Surrogate::forward(int B, cudaStream_t st) {
+// Y = net(X0) for the first B rows (B a multiple of 128). keep_z (training, tests): the GELU
+// derivatives the backward pass needs (bf16) and Y row by row; otherwise (inference in the step)
+// neither, and the output transposed into Yt.
+void Surrogate::forward(int B, cudaStream_t st, bool keep_z) {
     for (int l = 0; l < 3; l++) {
         const bf16*   in = l == 0 ? X0 : A[l - 1];
-        umma::EpiArgs e{nullptr, A[l], Z[l], nullptr, lay[l].b, net.H};
-        umma::gemm<256, umma::kEpiBiasGelu>(in, lay[l].Wbf, B, net.H, lay[l].K, e, err, st);
+        umma::EpiArgs e{nullptr, A[l], keep_z ? Gd[l] : nullptr, nullptr, lay[l].b, net.H};
+        umma::gemm_tma<256, umma::kEpiBiasGelu>(in, lay[l].Wbf, B, net.H, lay[l].K, e, err, st);
     }
-    umma::EpiArgs e{Y, nullptr, nullptr, nullptr, lay[3].b, net.Nout};
-    umma::gemm<64, umma::kEpiBiasF32>(A[2], lay[3].Wbf, B, net.Nout, net.H, e, err, st);
+    if (keep_z) {
+        umma::EpiArgs e{Y, nullptr, nullptr, nullptr, lay[3].b, net.Nout};
+        umma::gemm_tma<64, umma::kEpiBiasF32>(A[2], lay[3].Wbf, B, net.Nout, net.H, e, err, st);
+    }
+    else { // inference: the output plane by plane (Yt [Nout][Bcap]) for the per-level combine
+        umma::EpiArgs e{Yt, nullptr, nullptr, nullptr, lay[3].b, Bcap};
+        umma::gemm_tma<64, umma::kEpiBiasF32T>(A[2], lay[3].Wbf, B, net.Nout, net.H, e, err, st);
+    }
 }
 
 // D[M x N] = A[M x K] . B[N x K]^T into f32, tile width chosen from N.
 void Surrogate::gemm_n(const bf16* Am, const bf16* Bm, int M, int N, int K, const umma::EpiArgs& e,
                        cudaStream_t st) {
     if (N % 256 == 0)
-        umma::gemm<256, umma::kEpiF32>(Am, Bm, M, N, K, e, err, st);
+        umma::gemm_tma<256, umma::kEpiF32>(Am, Bm, M, N, K, e, err, st);
     else if (N % 128 == 0)
-        umma::gemm<128, umma::kEpiF32>(Am, Bm, M, N, K, e, err, st);
+        umma::gemm_tma<128, umma::kEpiF32>(Am, Bm, M, N, K, e, err, st);
     else
-        umma::gemm<64, umma::kEpiF32>(Am, Bm, M, N, K, e, err, st);
+        umma::gemm_tma<64, umma::kEpiF32>(Am, Bm, M, N, K, e, err, st);
 }
 // Weight gradient D[M x N] = A[M x K] . B[N x K]^T with K = the batch, split over CTAs in
 // partial products (so that the few 128 x N tiles of a layer fill the GPU) and reduced in order.
@@ -451,11 +507,11 @@ void Surrogate::gemm_wgrad(const bf16* Am, const bf16* Bm, int M, int N, int K, 
     const size_t  stride = (size_t)M * N;
     umma::EpiArgs e{splitk, nullptr, nullptr, nullptr, nullptr, N, stride};
     if (N % 256 == 0)
-        umma::gemm<256, umma::kEpiF32>(Am, Bm, M, N, K, e, err, st, splits);
+        umma::gemm_tma<256, umma::kEpiF32>(Am, Bm, M, N, K, e, err, st, splits);
     else if (N % 128 == 0)
-        umma::gemm<128, umma::kEpiF32>(Am, Bm, M, N, K, e, err, st, splits);
+        umma::gemm_tma<128, umma::kEpiF32>(Am, Bm, M, N, K, e, err, st, splits);
     else
-        umma::gemm<64, umma::kEpiF32>(Am, Bm, M, N, K, e, err, st, splits);
+        umma::gemm_tma<64, umma::kEpiF32>(Am, Bm, M, N, K, e, err, st, splits);
     splitk_reduce_kernel<<<nblk((long long)stride, 256), 256, 0, st>>>(splitk, splits, stride,
                                                                       stride, out);
 }
@@ -471,7 +527,7 @@ void Surrogate::colsum(const bf16* G, int B, int N, float* db, cudaStream_t st) 
 
 void Surrogate::gemm_gelu_bwd(const bf16* Am, const bf16* Bm, int M, int N, int K,
                               const umma::EpiArgs& e, cudaStream_t st) {
-    umma::gemm<256, umma::kEpiGeluBwdBf16>(Am, Bm, M, N, K, e, err, st);
+    umma::gemm_tma<256, umma::kEpiGeluBwdBf16>(Am, Bm, M, N, K, e, err, st);
 }
 
 // Gradients of the MSE loss for the first B rows (targets in tgt): fills gW, gb of every layer.
@@ -479,7 +535,7 @@ void Surrogate::backward(int B, cudaStream_t st) {
     const int H = net.H, Nout = net.Nout;
     lpart_n     = nblk((long long)B * Nout, 256);
     loss_grad_kernel<<<lpart_n, 256, 0, st>>>(net, Y, tgt, B, dYf, dY, lpart);
-    // output layer: gW4 = dY^T A3, gb4 = colsum dY, dZ3 = (dY W4) * gelu'(Z3)
+    // output layer: gW4 = dY^T A3, gb4 = colsum dY, dZ3 = (dY W4) * gelu'(Z3) (stored in bf16)
     colsum(dYf, B, Nout, lay[3].gb, st);
     cudaMemsetAsync(T1, 0, (size_t)128 * B * 2, st); // dY^T padded to 128 rows
     transpose_bf16_kernel<<<dim3(Nout / 32, B / 32), dim3(32, 8), 0, st>>>(dY, T1, B, Nout, B);
@@ -488,7 +544,7 @@ void Surrogate::backward(int B, cudaStream_t st) {
         gemm_wgrad(T1, T2, 128, H, B, lay[3].gW, st);
     }
     {
-        umma::EpiArgs e{nullptr, dZ[0], nullptr, Z[2], nullptr, H};
+        umma::EpiArgs e{nullptr, dZ[0], nullptr, Gd[2], nullptr, H};
         gemm_gelu_bwd(dY, lay[3].Wt, B, H, Nout, e, st);
     }
     // hidden layers 3, 2, 1 (indices 2, 1, 0)
@@ -504,7 +560,7 @@ void Surrogate::backward(int B, cudaStream_t st) {
             gemm_wgrad(T1, T2, H, Kin, B, lay[l].gW, st);
         }
         if (l > 0) {
-            umma::EpiArgs e{nullptr, dZ[cur ^ 1], nullptr, Z[l - 1], nullptr, H};
+            umma::EpiArgs e{nullptr, dZ[cur ^ 1], nullptr, Gd[l - 1], nullptr, H};
             gemm_gelu_bwd(dz, lay[l].Wt, B, H, H, e, st);
             cur ^= 1;
         }
@@ -545,13 +601,16 @@ void Surrogate::load_host_batch(const float* dx, const float* dt, int B, cudaStr
 
 void Surrogate::step_features(const Geometry& g, const State& s, const RtFields& f, cudaStream_t st) {
     const int B = ((g.N + 127) / 128) * 128;
-    features_state_kernel<<<nblk(B, 128), 128, 0, st>>>(net, g, s, f.cos_zenith, X0, B);
-    forward(B, st);
+    features_state_kernel<<<B / kFeatCols, kFeatCols * kFeatWarps,
+                            (size_t)kFeatCols * (net.Kin + 2) * sizeof(bf16), st>>>(
+        net, g, s, f.cos_zenith, X0, B);
+    forward(B, st, false);
 }
 
 void Surrogate::step_combine(const Geometry& g, const Phys& P, const State& s, const RtFields& f,
                              cudaStream_t st) {
-    combine_kernel<<<nblk(g.N, 128), 128, 0, st>>>(net, g, P, s, f, Y, fallback, period, tol, stats);
+    combine_kernel<<<(g.N + 31) / 32, 32 * kCombGroups, 0, st>>>(net, g, P, s, f, Yt, Bcap, fallback,
+                                                                 period, tol, stats);
 }
 
 void Surrogate::log_step(const Geometry& g, const State& s, const RtFields& f, cudaStream_t st) {
@@ -600,11 +659,11 @@ int thorx_bf16_gemm(const unsigned short* A, const unsigned short* B, int M, int
     if (e == cudaSuccess) {
         umma::EpiArgs ea{dD, nullptr, nullptr, nullptr, nullptr, N};
         if (N % 256 == 0)
-            umma::gemm<256, umma::kEpiF32>(dA, dB, M, N, K, ea, err, 0);
+            umma::gemm_tma<256, umma::kEpiF32>(dA, dB, M, N, K, ea, err, 0);
         else if (N % 128 == 0)
-            umma::gemm<128, umma::kEpiF32>(dA, dB, M, N, K, ea, err, 0);
+            umma::gemm_tma<128, umma::kEpiF32>(dA, dB, M, N, K, ea, err, 0);
         else
-            umma::gemm<64, umma::kEpiF32>(dA, dB, M, N, K, ea, err, 0);
+            umma::gemm_tma<64, umma::kEpiF32>(dA, dB, M, N, K, ea, err, 0);
         ck(cudaGetLastError());
         ck(cudaDeviceSynchronize());
     }

@@ -46,7 +46,8 @@ struct Surrogate {
     __nv_bfloat16*     A[3]{};
     __nv_bfloat16*     dZ[2]{};
     float *            Y = nullptr, *tgt = nullptr, *dYf = nullptr;
-    float*             Z[3]{};
+    float*             Yt = nullptr; // inference output, transposed: [Nout][Bcap]
+    __nv_bfloat16*     Gd[3]{}; // gelu'(pre-activation) of the hidden layers (training)
     float*             splitk   = nullptr; // split-K partial weight gradients
     float*             colpart  = nullptr; // column-sum partials
     static constexpr int kMaxSplits = 32;
@@ -59,7 +60,7 @@ struct Surrogate {
     int  init(int nv, int hidden, long long log_capacity, int batch_rows, int ncols, uint64_t seed);
     void release();
     void cast_all(cudaStream_t st);
-    void forward(int B, cudaStream_t st);
+    void forward(int B, cudaStream_t st, bool keep_z = true);
     void backward(int B, cudaStream_t st);
     void adam(float lr, cudaStream_t st);
     void fit_normalisation(long long rows, cudaStream_t st);
