@@ -288,8 +288,9 @@ def time_steps(x, stream, precision, nsteps):
 # Cp = 13000, surface 100 bar, top at 1e-3 bar, dt = 300 s, synchronous rotation with the
 # substellar point at longitude 0, gray opacities 4e-4 (SW) and 1e-3 (LW) m^2/kg, irradiation
 # temperature 2000 K (Tstar 4300 K, R* = 0.667 R_sun, a = R* (Tstar / T_irr)^2). Initial state:
-# isothermal at T_eq = T_irr / sqrt(2) (the Guillot-profile initialiser is not built) with seeded
-# +-1 K noise; the model top is the altitude of 1e-3 bar in that isothermal column.
+# the Guillot profile (init_PT_profile = guillot) with T_eq = T_irr / sqrt(2), Tint = 100 K and the
+# RT's gray opacities, with seeded +-1 K noise; the model top is the altitude of 1e-3 bar in an
+# isothermal column at T_eq.
 RT_GLEVEL, RT_NV, RT_DT = 5, 40, 300.0
 RT_TIRR, RT_TSTAR, RT_RSTAR = 2000.0, 4300.0, 0.667 * 695700000.0
 
@@ -308,7 +309,7 @@ def rt_params_planet():
     return p, rt, teq
 
 
-def rt_surrogate_leg(torch, thor_b200, nlog=64, iters=1500, batch=8192, nsteps=20,
+def rt_surrogate_leg(torch, thor_b200, nlog=200, iters=5000, batch=8192, nsteps=20,
                      catch=True):
     """Plain FP64 + RT against mixed + trained surrogate RT on the RT configuration (g5/L40):
     time the plain form, log the plain RT, train the surrogate on the GPU, time the other form."""
@@ -317,7 +318,7 @@ def rt_surrogate_leg(torch, thor_b200, nlog=64, iters=1500, batch=8192, nsteps=2
         grid = thor_b200.Icogrid(RT_GLEVEL, RT_NV, A=p["A"], Top_altitude=p["Top_altitude"])
         stream = torch.cuda.Stream()
         x = thor_b200.Thorx(grid.as_dict(), RT_GLEVEL, p, stream=stream.cuda_stream)
-        x.init_rest_state(teq, SEED, 1.0)
+        x.init_guillot_state(teq, rt["Tint"], rt["f_lw"], rt["kappa_sw"], rt["kappa_lw"], SEED, 1.0)
         x.rt_enable(rt)
         x.sur_create(hidden=512, train_batch=batch, log_capacity=nlog * grid.point_num,
                      recheck_period=16, tolerance=0.05, seed=SEED)
@@ -327,7 +328,10 @@ def rt_surrogate_leg(torch, thor_b200, nlog=64, iters=1500, batch=8192, nsteps=2
         x.step(nlog)
         x.sync()
         t0 = time.perf_counter()
-        first, last = x.sur_train(iters, batch, lr=1e-3)
+        n_fine = iters // 5 # the last fifth of the iterations at a fifth of the learning rate
+        first, last = x.sur_train(iters - n_fine, batch, lr=1e-3)
+        if n_fine:
+            _, last = x.sur_train(n_fine, batch, lr=2e-4)
         torch.cuda.synchronize()
         train_s = time.perf_counter() - t0
         x.sur_mode(thor_b200.SUR_USE)
@@ -337,8 +341,8 @@ def rt_surrogate_leg(torch, thor_b200, nlog=64, iters=1500, batch=8192, nsteps=2
         kms_sur = dict(zip([t[0] for t in x.kernel_table()], x.profile_steps(1)))
         x.close()
         N = grid.point_num
-        return {"workload": "hot Jupiter double-gray RT g%d/L%d dt=%g (%d columns), isothermal "
-                            "%.0f K start" % (RT_GLEVEL, RT_NV, RT_DT, N, teq),
+        return {"workload": "hot Jupiter double-gray RT g%d/L%d dt=%g (%d columns), Guillot-profile "
+                            "start (Teq %.0f K)" % (RT_GLEVEL, RT_NV, RT_DT, N, teq),
                 "plain_fp64": {"ms_per_step": ms_plain,
                                "value": sim_days_per_hour(1, ms_plain / 1000.0, dt=RT_DT)},
                 "mixed_surrogate": {"ms_per_step": ms_sur,
@@ -348,8 +352,8 @@ def rt_surrogate_leg(torch, thor_b200, nlog=64, iters=1500, batch=8192, nsteps=2
                                    "surrogate_mode_rt": kms_sur.get("radiative_transfer", 0.0),
                                    "surrogate_mode_net": kms_sur.get("rt_surrogate", 0.0)},
                 "training": {"columns_logged": nlog * N, "iterations": iters, "batch": batch,
-                             "lr": 1e-3, "loss_first": first, "loss_last": last,
-                             "seconds": train_s},
+                             "lr": "1e-3, last fifth 2e-4", "loss_first": first,
+                             "loss_last": last, "seconds": train_s},
                 "recheck": {"steps": nsteps + 3, "rechecked": st["rechecked"],
                             "failed": st["failed"], "max_rel_err": st["max_err"],
                             "rt_column_fraction": st["rt_columns"] / ((nsteps + 3) * N)}}
@@ -506,9 +510,9 @@ def main():
     ap.add_argument("--surrogate-only", action="store_true",
                     help="run only the RT surrogate leg (g5/L40) and print its JSON object; with "
                          "--sur-log-steps / --sur-iters it is the small case for profiling captures")
-    ap.add_argument("--sur-log-steps", type=int, default=64,
+    ap.add_argument("--sur-log-steps", type=int, default=200,
                     help="plain-RT steps logged for training (surrogate leg)")
-    ap.add_argument("--sur-iters", type=int, default=1500, help="Adam iterations (surrogate leg)")
+    ap.add_argument("--sur-iters", type=int, default=5000, help="Adam iterations (surrogate leg)")
     args = ap.parse_args()
     set_workload(args.glevel, args.nv)
     if args.warmup < 3:

@@ -118,6 +118,14 @@ int thorx_get_field(thorx_ctx* ctx, const char* name, double* host);
  * SplitMix64(seed) on index col*nv + lev, at fixed pressure (rho = p / (Rd T)); Mh = W = Wh = 0,
  * Rd and Cp uniform. noise_amp = 0 gives the reference's noise-free rest state. */
 int thorx_init_rest_state(thorx_ctx* ctx, double Tmean, unsigned long long seed, double noise_amp);
+/* Rest state on the Guillot (2010) radiative-equilibrium profile (.thr init_PT_profile = guillot):
+ * the general rest-state branch of initial_values (src/ESP/esp_initial.cu:840-1000) with
+ * guillot_T (src/ESP/ultrahot_thermo.cu:121-161), Teq = Tmean, mu = 0.5 and the given internal
+ * temperature and gray opacities (the .thr keys Tint, f_lw, kappa_sw, kappa_lw), in discrete
+ * hydrostatic balance; then the seeded +-noise_amp K perturbation of thorx_init_rest_state. */
+int thorx_init_guillot_state(thorx_ctx* ctx, double Tmean, double Tint, double f_lw,
+                             double kappa_sw, double kappa_lw, unsigned long long seed,
+                             double noise_amp);
 
 /* Switches the precision form (THORX_FP64 / THORX_MIXED) between steps; the state and everything
  * else of the context carry over (both forms store FP64). A captured step graph is re-captured. */

@@ -92,7 +92,7 @@ def test_bad_lines_fail_the_file(line):
     ("RayleighSponge = true", "RayleighSponge"),
     ("conv_adj_type = rayph", "conv_adj_type"),
     ("chemistry = true", "chemistry"),
-    ("init_PT_profile = guillot", "init_PT_profile"),
+    ("init_PT_profile = parmentier", "init_PT_profile"),
     ("rt_type = PicketFence", "rt_type"),
     ("core_benchmark = JetSteady", "core_benchmark"),
     ("HyDiffOrder = 5", "HyDiffOrder"),

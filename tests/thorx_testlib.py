@@ -6,6 +6,7 @@ The checkers are test infrastructure, never the product:
                                   compiled from its sources by oracle/Makefile
 """
 import ctypes
+import math
 import os
 
 import numpy as np
@@ -206,6 +207,55 @@ def isothermal_column(Altitude, Altitudeh, c):
             rho[lev] = p[lev] / (Rd * T[lev])
             it += 1
     return p, rho, T
+
+
+def guillot_T(p, mu, Teq, P_Ref, g, Tint, f_lw, kappa_sw, kappa_lw):
+    """Guillot (2010) eq. 27 as the reference evaluates it (src/ESP/ultrahot_thermo.cu:121-161)."""
+    tau0 = kappa_lw * P_Ref / g
+    eps = 1.0 / f_lw
+    x0 = P_Ref / g
+    gamma0 = kappa_sw / kappa_lw
+    klw = kappa_lw * (1.0 + 2 * (eps - 1) * p / P_Ref)
+    x = p / g
+    tau = kappa_lw * x
+    tau_lw = tau0 * p / P_Ref + (eps - 1) * tau0 * (p / P_Ref) ** 2
+    gamma = kappa_sw / klw
+    e = math.exp(-gamma0 * tau / mu)
+    T4 = (0.75 * Tint ** 4 * (2. / 3 + tau_lw)
+          + 3 * mu * Teq ** 4 * (2. / 3 + gamma / (3 * mu) * e + mu / gamma0 * (1.0 - e)
+                                 + 2 * (eps - 1) * mu / (gamma0 * kappa_sw * x0)
+                                 * (mu - (mu + gamma0 * tau) * e)))
+    return T4 ** 0.25
+
+
+def guillot_column(Altitude, Altitudeh, c, Tint, f_lw, kappa_sw, kappa_lw):
+    """Rest column on the Guillot profile: the general branch of initial_values
+    (src/ESP/esp_initial.cu:840-1000), Teq = Tmean, mu = 0.5, constant gravity."""
+    nv = len(Altitude)
+    p, T = np.zeros(nv), np.zeros(nv)
+    g, Rd, PR, mu = c["Gravit"], c["Rd"], c["P_Ref"], 0.5
+    for lev in range(nv):
+        if lev == 0:
+            T[0] = guillot_T(PR, mu, c["Tmean"], PR, g, Tint, f_lw, kappa_sw, kappa_lw)
+            P_L, T_L, dz, l_int, r_int = PR, T[0], Altitude[0], 0.5, 0.5
+        else:
+            T[lev] = T[lev - 1]
+            P_L, T_L = p[lev - 1], T[lev - 1]
+            dz = Altitude[lev] - Altitude[lev - 1]
+            l_int = (Altitude[lev] - Altitudeh[lev]) / dz
+            r_int = (Altitudeh[lev] - Altitude[lev - 1]) / dz
+        p[lev], T[lev] = P_L, T_L
+        ptmp = p[lev] + 2 * 1e-15 * p[lev]
+        it = 0
+        while it < 100 and (ptmp - p[lev]) / p[lev] > 1e-15:
+            ptmp = p[lev]
+            f = (p[lev] - P_L) / dz + (g * r_int + g * l_int) / Rd * (p[lev] * r_int / T[lev]
+                                                                     + P_L * l_int / T_L)
+            df = 1.0 / dz + (g * r_int + g * l_int) * r_int / (Rd * T[lev])
+            p[lev] = p[lev] - f / df
+            T[lev] = guillot_T(p[lev], mu, c["Tmean"], PR, g, Tint, f_lw, kappa_sw, kappa_lw)
+            it += 1
+    return p, T, p / (T * Rd)
 
 
 def hydrostatic_column(Altitude, Altitudeh, c, Tprof):

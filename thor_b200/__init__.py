@@ -133,6 +133,9 @@ def lib():
         L.thorx_set_precision.restype = ci
         L.thorx_conv_adj_enable.argtypes = [vp, ci, ci]
         L.thorx_conv_adj_enable.restype = ci
+        L.thorx_init_guillot_state.argtypes = [vp] + [ctypes.c_double] * 5 + [ctypes.c_ulonglong,
+                                                                             ctypes.c_double]
+        L.thorx_init_guillot_state.restype = ci
         L.thorx_bf16_gemm.argtypes = [vp, vp, ci, ci, ci, vp]
         L.thorx_bf16_gemm.restype = ci
         L.thorx_surrogate_last_error.restype = cp
@@ -178,7 +181,7 @@ EXPORTED = ["thorx_create", "thorx_destroy", "thorx_last_error", "thorx_field_si
             "thorx_surrogate_train", "thorx_surrogate_stats", "thorx_surrogate_layer",
             "thorx_surrogate_layer_grad", "thorx_surrogate_normalisation",
             "thorx_surrogate_forward_host", "thorx_surrogate_gradients_host",
-            "thorx_check_division", "thorx_conv_adj_enable"]
+            "thorx_check_division", "thorx_conv_adj_enable", "thorx_init_guillot_state"]
 
 def device_sum(ptr, n, stream=0):
     """Compensated sum of n doubles at device address `ptr` (thorx_device_sum)."""
@@ -334,6 +337,11 @@ class Thorx:
 
     def init_rest_state(self, Tmean, seed=20260101, noise_amp=0.1):
         self._check(lib().thorx_init_rest_state(self.h, Tmean, seed, noise_amp))
+
+    def init_guillot_state(self, Tmean, Tint, f_lw, kappa_sw, kappa_lw, seed=20260101, noise_amp=0.0):
+        """Rest state on the Guillot (2010) profile (Teq = Tmean), as init_PT_profile = guillot."""
+        self._check(lib().thorx_init_guillot_state(self.h, Tmean, Tint, f_lw, kappa_sw, kappa_lw,
+                                                   seed, noise_amp))
 
     def profx(self):
         self._check(lib().thorx_profx(self.h))

@@ -870,6 +870,110 @@ int thorx_init_rest_state(thorx_ctx* ctx, double Tmean, unsigned long long seed,
     return 0;
 }
 
+namespace {
+// Temperature of Guillot's (2010) radiative-equilibrium profile, eq. 27, in the form of the
+// reference's guillot_T (src/ESP/ultrahot_thermo.cu:121-161): gray LW opacity increasing with
+// pressure (f_lw the well-mixed fraction), gray SW absorption, irradiation angle mu.
+double guillot_T(double pressure, double mu, double Teq, double P_Ref, double Gravit, double Tint,
+                 double f_lw, double kappa_sw, double kappa_lw) {
+    const double tau0   = kappa_lw * P_Ref / Gravit;
+    const double eps    = 1.0 / f_lw;
+    const double x0     = P_Ref / Gravit;
+    const double gamma0 = kappa_sw / kappa_lw;
+    const double klw    = kappa_lw * (1.0 + 2 * (eps - 1) * pressure / P_Ref);
+    const double x      = pressure / Gravit;
+    const double tau    = kappa_lw * x;
+    const double tau_lw = tau0 * pressure / P_Ref + (eps - 1) * tau0 * pow(pressure / P_Ref, 2);
+    const double gamma  = kappa_sw / klw;
+    const double T4 =
+        0.75 * pow(Tint, 4) * (2. / 3 + tau_lw)
+        + 3 * mu * pow(Teq, 4)
+              * (2. / 3 + gamma / (3 * mu) * exp(-gamma0 * tau / mu)
+                 + mu / gamma0 * (1.0 - exp(-gamma0 * tau / mu))
+                 + 2 * (eps - 1) * mu / (gamma0 * kappa_sw * x0)
+                       * (mu - (mu + gamma0 * tau) * exp(-gamma0 * tau / mu)));
+    return pow(T4, 0.25);
+}
+} // namespace
+
+int thorx_init_guillot_state(thorx_ctx* ctx, double Tmean, double Tint, double f_lw,
+                             double kappa_sw, double kappa_lw, unsigned long long seed,
+                             double noise_amp) {
+    if (!ctx)
+        return THORX_E_ARG;
+    if (!(Tmean > 0) || !(Tint >= 0) || !(f_lw > 0) || !(kappa_sw > 0) || !(kappa_lw > 0)
+        || !(noise_amp >= 0))
+        return fail(ctx, THORX_E_ARG, "thorx_init_guillot_state: bad profile parameter");
+    const int     N = ctx->g.N, nv = ctx->g.nv;
+    const Phys&   P = ctx->P;
+    const double* Alt  = ctx->Altitude_h.data();
+    const double* Alth = ctx->Altitudeh_h.data();
+    // one column, the general rest-state branch of initial_values (src/ESP/esp_initial.cu:840-1000):
+    // Newton-Raphson on the discrete hydrostatic balance with T re-evaluated from the profile at
+    // every iterate; Teq = Tmean, mu = 0.5, Rd and Cp constant
+    std::vector<double> p0(nv), T0(nv);
+    const double        eps = 1e-15, mu = 0.5;
+    const int           it_max = 100;
+    auto grav = [&](double alt) { return P.GravHeightVar ? P.Gravit * pow(P.A / (P.A + alt), 2) : P.Gravit; };
+    for (int lev = 0; lev < nv; lev++) {
+        double g_L, P_L, T_L, dz, l_int, r_int;
+        if (lev == 0) {
+            g_L   = grav(Alt[0]);
+            T0[0] = guillot_T(P.P_Ref, mu, Tmean, P.P_Ref, g_L, Tint, f_lw, kappa_sw, kappa_lw);
+            P_L   = P.P_Ref;
+            T_L   = T0[0];
+            dz    = Alt[0];
+            l_int = 0.5;
+            r_int = 0.5;
+        }
+        else {
+            g_L     = grav(Alt[lev - 1]);
+            T0[lev] = T0[lev - 1];
+            P_L     = p0[lev - 1];
+            T_L     = T0[lev - 1];
+            dz      = Alt[lev] - Alt[lev - 1];
+            l_int   = (Alt[lev] - Alth[lev]) / dz;
+            r_int   = (Alth[lev] - Alt[lev - 1]) / dz;
+        }
+        p0[lev]            = P_L;
+        T0[lev]            = T_L;
+        double       ptmp  = p0[lev] + 2 * eps * p0[lev];
+        const double g     = grav(Alt[lev]);
+        for (int it = 0; it < it_max && (ptmp - p0[lev]) / p0[lev] > eps; it++) {
+            ptmp            = p0[lev];
+            const double f  = (p0[lev] - P_L) / dz
+                             + (g * r_int + g_L * l_int) / P.Rd
+                                   * (p0[lev] * r_int / T0[lev] + P_L * l_int / T_L);
+            const double df = 1.0 / dz + (g * r_int + g_L * l_int) * r_int / (P.Rd * T0[lev]);
+            p0[lev]         = p0[lev] - f / df;
+            T0[lev] = guillot_T(p0[lev], mu, Tmean, P.P_Ref, g, Tint, f_lw, kappa_sw, kappa_lw);
+        }
+    }
+    const size_t        n = (size_t)N * nv;
+    std::vector<double> T(n), p(n), rho(n), Rd(n, P.Rd), Cp(n, P.Cp), zero3(3 * n, 0.0),
+        zeroi((size_t)N * (nv + 1), 0.0), zero(n, 0.0);
+    uint64_t x = seed; // the perturbation of thorx_init_rest_state
+    for (size_t i = 0; i < n; i++) {
+        x += 0x9E3779B97F4A7C15ull;
+        uint64_t z = x;
+        z          = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z          = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z          = z ^ (z >> 31);
+        double u   = (double)(z >> 11) * (1.0 / 9007199254740992.0);
+        int    lev = (int)(i % nv);
+        T[i]       = T0[lev] + (2.0 * u - 1.0) * noise_amp;
+        p[i]       = p0[lev];
+        rho[i]     = p[i] / (T[i] * P.Rd);
+    }
+    int rc;
+    if ((rc = thorx_set_field(ctx, "temperature", T.data())) || (rc = thorx_set_field(ctx, "pressure", p.data()))
+        || (rc = thorx_set_field(ctx, "Rho", rho.data())) || (rc = thorx_set_field(ctx, "Rd", Rd.data()))
+        || (rc = thorx_set_field(ctx, "Cp", Cp.data())) || (rc = thorx_set_field(ctx, "Mh", zero3.data()))
+        || (rc = thorx_set_field(ctx, "Wh", zeroi.data())) || (rc = thorx_set_field(ctx, "W", zero.data())))
+        return rc;
+    return 0;
+}
+
 int thorx_profx(thorx_ctx* ctx) {
     if (!ctx)
         return THORX_E_ARG;

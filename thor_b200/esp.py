@@ -17,7 +17,8 @@ Differences, each stated where it applies:
     the reference's names and memory layout ([column][level][component]);
   * keys for physics that this build does not implement (sponges, the RayPH convective
     adjustment, chemistry, boundary layer, ultra-hot thermodynamics, refined vertical grids,
-    picket-fence or two-stream RT, other initial profiles) are accepted at their default values
+    picket-fence or two-stream RT, the Parmentier and constant-N initial profiles) are accepted at
+    their default values
     and rejected with an error naming the key otherwise;
   * output_mean, out_interm_momentum and output_diffusion only add arrays to the output files in
     the reference; here they are accepted and a warning says the arrays are not written;
@@ -191,7 +192,7 @@ KEYS = {
     "precision": (str, "fp64", "path"),
 }
 # values a "fixed" key may take (its default unless listed)
-ALLOWED = {"init_PT_profile": ("isothermal",), "rt_type": ("DualbandGray",),
+ALLOWED = {"init_PT_profile": ("isothermal", "guillot"), "rt_type": ("DualbandGray",),
            "conv_adj_type": ("hourdin", "Hourdin"),
            "ultrahot_thermo": ("none",), "ultrahot_heating": ("none",),
            "insol_avg": ("NoInsolAvg",)}
@@ -516,6 +517,9 @@ def run(argv=None, out=sys.stdout):
                 step_idx = nstep0 + 1
                 m = re.search(r"_(\d+)\.npz$", start_file)
                 first_idx = int(m.group(1)) + 1 if m else 1
+        elif c["init_PT_profile"] == "guillot":
+            x.init_guillot_state(c["Tmean"], c["Tint"], c["f_lw"], c["kappa_sw"], c["kappa_lw"], 0,
+                                 0.0)
         else:
             x.init_rest_state(c["Tmean"], 0, 0.0)
         if c["radiative_transfer"]:
