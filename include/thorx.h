@@ -139,6 +139,33 @@ int thorx_set_precision(thorx_ctx* ctx, int precision);
  * thorx_sync return THORX_E_CONVERGENCE. */
 int thorx_conv_adj_enable(thorx_ctx* ctx, int iterations, int soft_adjustment);
 
+/* ---- Rayleigh sponge layer at the top of the model (RayleighSponge with raysp_calc_mode = imp:
+ * sponge_layer with its zonal means, src/ESP/profx_sponge.cu, run by ESP::ProfX at
+ * src/ESP/profx_driver.cu:96-194; latitude bins of Icogrid::zonal_mean_tab_f,
+ * src/ESP/grid.cu:3203-3260). The .thr keys of the same names. ---- */
+typedef struct {
+    int    nlat_bins;       /* latitude bins over which the zonal means are taken (>= 1)     */
+    double Ruv_sponge;      /* damping rate of the horizontal wind at the top [1/s]          */
+    double Rw_sponge;       /* damping rate of the vertical wind at the top [1/s]            */
+    double RT_sponge;       /* damping rate of the temperature (thermal sponge) [1/s]        */
+    double ns_ray_sponge;   /* bottom of the sponge as a fraction of the model top, [0, 1)   */
+    int    damp_uv_to_mean; /* damp u, v toward their zonal mean (else toward zero)          */
+    int    damp_w_to_mean;  /* damp w toward its zonal mean (else toward zero)               */
+    int    RayleighSpongeT; /* also damp the temperature toward its zonal mean               */
+    int    shrink_sponge;   /* weaken the sponge exponentially after t_shrink steps          */
+    int    t_shrink;        /* steps after which the sponge shrinks                          */
+    int    first_step;      /* step number of the next physics step (1 at a fresh start)     */
+} thorx_sponge_params;
+
+/* Adds the implicit Rayleigh sponge to every following ProfX, between Recompute_W and the
+ * temperature; NULL switches it off. A step graph captured earlier is re-captured.
+ * THORX_E_ARG for nlat_bins < 1 or ns_ray_sponge outside [0, 1). */
+int thorx_sponge_enable(thorx_ctx* ctx, const thorx_sponge_params* sp);
+/* The zonal means of the last sponge step: vbar [bin][lev][3] (u, v, w; the reference's vbar_h;
+ * zero where damp_*_to_mean is off) and Tbar [bin][lev] (zero without RayleighSpongeT); either
+ * may be NULL. THORX_E_STATE when the sponge is off. */
+int thorx_sponge_means(thorx_ctx* ctx, double* vbar, double* Tbar);
+
 /* One physics step, ESP::ProfX (src/ESP/profx_driver.cu:70-474): W from Wh, T and potential
  * temperature from p and rho, Held-Suarez forcing when core_benchmark says so, p = rho Rd T,
  * and the NaN check (reported at the next synchronising call as THORX_E_NAN). */

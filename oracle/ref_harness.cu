@@ -1,10 +1,10 @@
 // Reference harness: TEST INFRASTRUCTURE ONLY.
 //
 // Compiles the reference's own grid builder (src/ESP/grid.cu) and its own dynamical-core and
-// physics kernels (src/headers/dyn/*.h, src/headers/phy/profx_{auxiliary,held_suarez}.h) into
+// physics kernels (src/headers/dyn/*.h, src/headers/phy/profx_*.h, src/ESP/profx_sponge.cu) into
 // oracle/_ref/libthor_ref.so, and drives them with the launch sequence of
 //   ESP::Thor   src/ESP/thor_driver.cu:70-1466
-//   ESP::ProfX  src/ESP/profx_driver.cu:70-474   (Held-Suarez branch, no sponge, no modules)
+//   ESP::ProfX  src/ESP/profx_driver.cu:70-474   (the options listed below)
 // on one GPU, all FP64, default stream, one launch after another. It is the "reference's own FP64
 // CUDA build" against which the CPU restatement (oracle/thor_oracle.cpp) and the product kernels
 // are checked, and it is the timing of the reference's CUDA kernels on the same B200.
@@ -12,9 +12,11 @@
 // Only tests/ (and bench.py's reference-CUDA side leg) load this library. The product never does.
 //
 // Subset mirrored (the configurations this repository measures): entropy or energy equation,
-// HyDiff of any even order, DivDampP on/off, DeepModel, NonHydro, GravHeightVar, no Rayleigh
-// sponge, no diffusive sponge, no vertical hyperdiffusion, no ultrahot thermodynamics, no
-// convective adjustment, no increased damping, Held-Suarez forcing on/off.
+// HyDiff of any even order, DivDampP on/off, DeepModel, NonHydro, GravHeightVar, the Rayleigh
+// sponge in its implicit form (raysp_calc_mode = imp), no diffusive sponge, no vertical
+// hyperdiffusion, no ultrahot thermodynamics, dry convective adjustment on/off, no increased
+// damping, the benchmark forcings (Held-Suarez, tidally locked Earth, shallow hot Jupiter), the
+// double-gray RT module.
 
 #include <cstdio>
 #include <cstdlib>
@@ -43,6 +45,7 @@
 #include "phy/profx_globdiag.h"
 #include "phy/profx_held_suarez.h"
 #include "phy/profx_shallowHJ.h"
+#include "phy/profx_sponge.h"
 #include "phy/profx_tidalearth.h"
 #include "physical_constants.h"
 #include "profx_RT.h"
@@ -70,6 +73,8 @@ struct RefGrid {
     Icogrid* g = nullptr;
     int      glevel;
     int      nv;
+    int      nlat      = 0; // latitude bins of the zonal-mean table (0: built without)
+    int      max_count = 0;
 };
 
 extern "C" void* ref_grid_new(int    glevel,
@@ -86,6 +91,21 @@ extern "C" void* ref_grid_new(int    glevel,
                        std::string("/nonexistent-thorx-ref-cache"));
     r->glevel = glevel;
     r->nv     = vlevel;
+    return r;
+}
+
+// The same grid with the Rayleigh sponge's zonal-mean table (Icogrid with sponge = true and
+// nlat latitude bins, src/ESP/grid.cu:295-299).
+extern "C" void* ref_grid_new_sponge(int glevel, int vlevel, double A, double top_altitude,
+                                     int sprd, double spring_beta, int nlat) {
+    RefGrid* r    = new RefGrid;
+    r->max_count  = 0;
+    r->g          = new Icogrid(sprd != 0, spring_beta, glevel, vlevel, nlat, A, top_altitude, true,
+                       &r->max_count, false, 2.0, 1000.0, false, 0.7, 1.0, 6.0,
+                       std::string("/nonexistent-thorx-ref-cache"));
+    r->glevel = glevel;
+    r->nv     = vlevel;
+    r->nlat   = nlat;
     return r;
 }
 
@@ -131,6 +151,8 @@ extern "C" long ref_grid_get(void* h, const char* name, void* out) {
         {"curlz", {g->curlz, 21L * N, 8}},
         {"func_r", {g->func_r, 3L * N, 8}},
     };
+    if (r->nlat > 0) // [col][3]: latitude bin, members of the bin, slot in the bin
+        m["zonal_mean_tab"] = {g->zonal_mean_tab, 3L * N, 4};
     auto it = m.find(name);
     if (it == m.end())
         return -1;
@@ -166,8 +188,20 @@ struct ref_rt_params {
     int    first_step;
 };
 
+// Rayleigh sponge; same field order as oracle_sponge_params.
+struct ref_sponge_params {
+    int    nlat_bins;
+    double Ruv_sponge, Rw_sponge, RT_sponge, ns_ray_sponge;
+    int    damp_uv_to_mean, damp_w_to_mean, RayleighSpongeT, shrink_sponge, t_shrink, first_step;
+};
+
 struct RefSim {
     ref_params                     p;
+    bool                           sponge = false;
+    ref_sponge_params              S{};
+    int                            max_count = 0, sp_step = 1;
+    int*                           zonal_mean_tab_d = nullptr;
+    double *                       vbar_h = nullptr, *Tbar_h = nullptr;
     int                            conv_adj_iter = 0; // dry_conv_adj when > 0
     bool                           conv_soft     = false;
     bool                           rt = false;
@@ -433,6 +467,101 @@ extern "C" int ref_sim_conv_adj(void* h, int iterations, int soft) {
     return 0;
 }
 
+// The Rayleigh sponge in ProfX (sim.RayleighSponge with raysp_calc_mode = imp), launched as
+// profx_driver.cu:96-194 launches it, with the grid's zonal-mean table (gh from
+// ref_grid_new_sponge with the same nlat_bins).
+extern "C" int ref_sim_sponge(void* h, void* gh, const ref_sponge_params* sp) {
+    RefSim*  s = (RefSim*)h;
+    RefGrid* r = (RefGrid*)gh;
+    if (!r->g->zonal_mean_tab || r->nlat != sp->nlat_bins || r->g->point_num != s->N)
+        return -1;
+    s->S         = *sp;
+    s->sponge    = true;
+    s->max_count = r->max_count;
+    s->sp_step   = sp->first_step;
+    const long N = s->N, nv = s->nv, nlat = sp->nlat_bins, mc = r->max_count;
+    REF_CHECK(cudaMalloc(&s->zonal_mean_tab_d, 3 * N * sizeof(int)));
+    REF_CHECK(cudaMemcpy(s->zonal_mean_tab_d, r->g->zonal_mean_tab, 3 * N * sizeof(int),
+                         cudaMemcpyHostToDevice));
+    for (auto n : {"utmp", "vtmp", "wtmp", "Ttmp"})
+        if (sim_alloc(s, n, nlat * nv * mc))
+            return -2;
+    if (sim_alloc(s, "vbar", 3 * nlat * nv) || sim_alloc(s, "Tbar", nlat * nv))
+        return -2;
+    s->vbar_h = new double[3 * nlat * nv]();
+    s->Tbar_h = new double[nlat * nv]();
+    return 0;
+}
+
+extern "C" void ref_sim_sponge_means(void* h, double* vbar, double* Tbar) {
+    RefSim*    s = (RefSim*)h;
+    const long n = (long)s->S.nlat_bins * s->nv;
+    if (vbar)
+        std::memcpy(vbar, s->vbar_h, 3 * n * sizeof(double));
+    if (Tbar)
+        std::memcpy(Tbar, s->Tbar_h, n * sizeof(double));
+}
+
+static int ref_sponge_step(RefSim* s) {
+    auto&      F   = s->f;
+    const int  NTH = 256;
+    const int  N = s->N, nv = s->nv, nlat_bins = s->S.nlat_bins, max_count = s->max_count;
+    const bool uvm = s->S.damp_uv_to_mean != 0, wm = s->S.damp_w_to_mean != 0;
+    dim3       NB((N / NTH) + 1, nv, 1);
+    dim3       NBRT((N / NTH) + 1, 1, 1);
+    if (uvm) {
+        REF_CHECK(cudaMemset(F["utmp"], 0, sizeof(double) * nlat_bins * nv * max_count));
+        REF_CHECK(cudaMemset(F["vtmp"], 0, sizeof(double) * nlat_bins * nv * max_count));
+        zonal_uv<<<NB, NTH>>>(F["Mh"], F["Rho"], s->zonal_mean_tab_d, F["lonlat"], N, F["utmp"],
+                              F["vtmp"], max_count);
+        REF_CHECK(cudaDeviceSynchronize());
+    }
+    if (wm) {
+        REF_CHECK(cudaMemset(F["wtmp"], 0, sizeof(double) * nlat_bins * nv * max_count));
+        zonal_w<<<NB, NTH>>>(F["W"], F["Rho"], s->zonal_mean_tab_d, N, F["wtmp"], max_count);
+        REF_CHECK(cudaDeviceSynchronize());
+    }
+    if (uvm) {
+        gpu_sum_on_device_sponge<1024>(F["utmp"], max_count, s->vbar_h, nv, nlat_bins, 0);
+        gpu_sum_on_device_sponge<1024>(F["vtmp"], max_count, s->vbar_h, nv, nlat_bins, 1);
+    }
+    if (wm)
+        gpu_sum_on_device_sponge<1024>(F["wtmp"], max_count, s->vbar_h, nv, nlat_bins, 2);
+    if (uvm || wm) {
+        REF_CHECK(cudaMemset(F["vbar"], 0, sizeof(double) * 3 * nlat_bins * nv));
+        REF_CHECK(cudaMemcpy(F["vbar"], s->vbar_h, 3 * nlat_bins * nv * sizeof(double),
+                             cudaMemcpyHostToDevice));
+    }
+    if (s->S.RayleighSpongeT) {
+        zonal_temp<<<NB, NTH>>>(F["pressure"], F["Rho"], F["Tbar"], s->zonal_mean_tab_d,
+                                F["lonlat"], N, F["Ttmp"], F["Rd"], max_count);
+        REF_CHECK(cudaDeviceSynchronize());
+        for (int ilat = 0; ilat < nlat_bins; ilat++)
+            for (int lev = 0; lev < nv; lev++)
+                s->Tbar_h[ilat * nv + lev] = gpu_sum_on_device<1024>(
+                    &(F["Ttmp"][ilat * nv * max_count + lev * max_count]), max_count);
+        REF_CHECK(cudaMemcpy(F["Tbar"], s->Tbar_h, nlat_bins * nv * sizeof(double),
+                             cudaMemcpyHostToDevice));
+    }
+    const double timestep = s->p.timestep;
+    const int    current_step = s->sp_step++;
+    double       Rv_fac = 1;
+    if (s->S.shrink_sponge) {
+        if (current_step * timestep >= s->S.t_shrink * timestep) {
+            double shrink_scale = timestep * 1000;
+            Rv_fac = exp(-(current_step * timestep - s->S.t_shrink * timestep) / shrink_scale);
+        }
+    }
+    sponge_layer<<<NBRT, NTH>>>(F["Mh"], F["Rho"], F["W"], F["Wh"], F["pressure"], F["vbar"],
+                                F["Tbar"], s->zonal_mean_tab_d, F["lonlat"], F["Altitude"],
+                                F["Altitudeh"], s->S.Ruv_sponge, s->S.Rw_sponge, s->S.RT_sponge,
+                                Rv_fac, s->S.ns_ray_sponge, uvm, wm, true, timestep, F["Rd"],
+                                nlat_bins, N, nv, s->S.RayleighSpongeT != 0, F["profx_dMh"],
+                                F["profx_dWh"], F["profx_dW"], F["profx_Qheat"]);
+    REF_CHECK(cudaDeviceSynchronize());
+    return 0;
+}
+
 extern "C" void ref_sim_rt_totals(void* h, double* asr, double* olr) {
     RefSim* s = (RefSim*)h;
     *asr      = s->ASR_tot;
@@ -510,6 +639,8 @@ static int ref_profx(RefSim* s) {
     REF_CHECK(cudaMemset(F["profx_Qheat"], 0, sizeof(double) * N * nv));
     Recompute_W<<<NB, NTH>>>(F["W"], F["Wh"], F["Altitude"], F["Altitudeh"], N);
     REF_CHECK(cudaDeviceSynchronize());
+    if (s->sponge && ref_sponge_step(s))
+        return -1;
     Compute_temperature<<<NB, NTH>>>(F["temperature"], F["pt"], F["pressure"], F["Rho"],
                                      s->p.P_Ref, F["Rd"], F["Cp"], N, true);
     REF_CHECK(cudaDeviceSynchronize());
@@ -850,5 +981,8 @@ extern "C" void ref_sim_free(void* h) {
     cudaFree(s->diag_flag_d);
     cudaFree(s->diag_data_d);
     delete[] s->Altitude_h;
+    cudaFree(s->zonal_mean_tab_d);
+    delete[] s->vbar_h;
+    delete[] s->Tbar_h;
     delete s;
 }

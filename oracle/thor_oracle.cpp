@@ -60,6 +60,12 @@ struct Oracle {
     int  conv_adj_iter = 0;
     bool conv_soft     = false;
     bool conv_fail     = false; // a column exceeded the pass bound
+    // Rayleigh sponge (when enabled)
+    bool                 sponge = false;
+    oracle_sponge_params S{};
+    long long            sp_nstep = 1;
+    std::vector<int>     sp_bin, sp_start, sp_members; // bins, then members bin by bin
+    Vec                  vbar, Tbar;                     // [bin][lev][3], [bin][lev]
 };
 
 inline double val(const Vec& a, int id, int nv, int lev) {
@@ -652,9 +658,196 @@ void dry_conv_adj(Oracle& o) {
         o.conv_fail = true;
 }
 
+// Latitude bins, Icogrid::zonal_mean_tab_f (src/ESP/grid.cu:3203-3260): bin j holds
+// lat_array[j] <= lat < lat_array[j+1] (edges accumulated from -pi/2 in steps of pi/nlat);
+// lat >= lat_array[nlat] goes to the last bin. Members of a bin in increasing column index, the
+// order of the reference's slots.
+void sponge_bins(Oracle& o) {
+    const int nlat = o.S.nlat_bins, N = o.N;
+    Vec       lat_array(nlat + 1);
+    double    des_lat = M_PI / nlat;
+    lat_array[0]      = -M_PI / 2.0;
+    for (int j = 1; j < nlat + 1; j++)
+        lat_array[j] = lat_array[j - 1] + des_lat;
+    o.sp_bin.assign(N, 0);
+    o.sp_start.assign(nlat + 1, 0);
+    for (int i = 0; i < N; i++) {
+        double lat = o.lonlat[i * 2 + 1];
+        int    b   = 0;
+        for (int j = 0; j < nlat; j++)
+            if (lat >= lat_array[j] && lat < lat_array[j + 1]) {
+                b = j;
+                break;
+            }
+        if (lat >= lat_array[nlat])
+            b = nlat - 1;
+        o.sp_bin[i] = b;
+        o.sp_start[b + 1]++;
+    }
+    for (int j = 0; j < nlat; j++)
+        o.sp_start[j + 1] += o.sp_start[j];
+    o.sp_members.assign(N, 0);
+    std::vector<int> fill(nlat, 0);
+    for (int i = 0; i < N; i++)
+        o.sp_members[o.sp_start[o.sp_bin[i]] + fill[o.sp_bin[i]]++] = i;
+    o.vbar.assign((size_t)nlat * o.nv * 3, 0.0);
+    o.Tbar.assign((size_t)nlat * o.nv, 0.0);
+}
+
+// Horizontal wind (u, v) of a cell, as zonal_uv and sponge_layer compute it
+// (src/ESP/profx_sponge.cu:70-79, 292-300).
+inline void wind_uv(const Oracle& o, const Vec& Mh, int id, int lev, double rho, double& u,
+                    double& v) {
+    int    nv = o.nv;
+    double lon;
+    if (o.lonlat[id * 2] < 0)
+        lon = o.lonlat[id * 2] + 2.0 * M_PI;
+    else
+        lon = o.lonlat[id * 2];
+    double lat = o.lonlat[id * 2 + 1];
+    const double* m = &Mh[((size_t)id * nv + lev) * 3];
+    u = (m[0] * (-sin(lon)) + m[1] * (cos(lon)) + m[2] * 0) / rho;
+    v = (m[0] * (-sin(lat) * cos(lon)) + m[1] * (-sin(lat) * sin(lon)) + m[2] * (cos(lat))) / rho;
+}
+
+// The implicit Rayleigh sponge (sponge_layer with implicit = true, src/ESP/profx_sponge.cu:144-431)
+// after the zonal means of zonal_uv / zonal_w / zonal_temp (:50-130) and the step factor of
+// profx_driver.cu:154-160. The means are sums of x / count over a bin's members in member order
+// (the reference sums the same terms in a block tree: the results differ by rounding only).
+void sponge(Oracle& o) {
+    const int nlat = o.S.nlat_bins, nv = o.nv, nvi = o.nvi, N = o.N;
+    Vec &     Mh = F(o, "Mh"), &W = F(o, "W"), &Wh = F(o, "Wh"), &Rho = F(o, "Rho"),
+        &p = F(o, "pressure"), &Rd = F(o, "Rd");
+    const bool uvm = o.S.damp_uv_to_mean, wm = o.S.damp_w_to_mean, tsp = o.S.RayleighSpongeT;
+    if (uvm || wm || tsp) {
+#pragma omp parallel for schedule(static)
+        for (int bl = 0; bl < nlat * nv; bl++) {
+            const int    b = bl / nv, lev = bl % nv;
+            const double cnt = o.sp_start[b + 1] - o.sp_start[b];
+            double       su = 0, sv = 0, sw = 0, sT = 0;
+            for (int m = o.sp_start[b]; m < o.sp_start[b + 1]; m++) {
+                const int    id  = o.sp_members[m];
+                const double rho = Rho[id * nv + lev];
+                if (uvm) {
+                    double u, v;
+                    wind_uv(o, Mh, id, lev, rho, u, v);
+                    su += u / cnt;
+                    sv += v / cnt;
+                }
+                if (wm)
+                    sw += (W[id * nv + lev] / rho) / cnt;
+                if (tsp)
+                    sT += p[id * nv + lev] / Rd[id * nv + lev] / rho / cnt;
+            }
+            o.vbar[(b * nv + lev) * 3 + 0] = uvm ? su : 0.0;
+            o.vbar[(b * nv + lev) * 3 + 1] = uvm ? sv : 0.0;
+            o.vbar[(b * nv + lev) * 3 + 2] = wm ? sw : 0.0;
+            o.Tbar[b * nv + lev]           = tsp ? sT : 0.0;
+        }
+    }
+    const double dt = o.P.timestep;
+    double       Rv_fac = 1;
+    if (o.S.shrink_sponge) {
+        if (o.sp_nstep * dt >= o.S.t_shrink * dt) {
+            double shrink_scale = dt * 1000;
+            Rv_fac = exp(-(o.sp_nstep * dt - o.S.t_shrink * dt) / shrink_scale);
+        }
+    }
+    o.sp_nstep++;
+    const double ns = o.S.ns_ray_sponge, ztop = o.Altitudeh[nv];
+#pragma omp parallel for schedule(static)
+    for (int id = 0; id < N; id++) {
+        const int    intlat  = o.sp_bin[id];
+        const double des_lat = M_PI / nlat;
+        const double lat1    = -M_PI / 2 + 0.5 * des_lat + des_lat * (intlat - 1);
+        const double lat2    = -M_PI / 2 + 0.5 * des_lat + des_lat * (intlat);
+        const double lat3    = -M_PI / 2 + 0.5 * des_lat + des_lat * (intlat + 1);
+        const double lat     = o.lonlat[id * 2 + 1];
+        double       lon;
+        if (o.lonlat[id * 2] < 0)
+            lon = o.lonlat[id * 2] + 2.0 * M_PI;
+        else
+            lon = o.lonlat[id * 2];
+        // the mean of table tab (stride st, component k) at the column's latitude; a latitude
+        // outside both half-intervals of its bin takes the bin's own mean
+        auto mean = [&](const Vec& tab, int st, int k, int lev) {
+            if (lat <= -M_PI / 2 + 0.5 * des_lat)
+                return tab[(intlat * nv + lev) * st + k];
+            if (lat >= -M_PI / 2 + 0.5 * des_lat + des_lat * (nlat - 1))
+                return tab[(intlat * nv + lev) * st + k];
+            if (lat >= lat1 && lat < lat2) {
+                double intt = (lat - lat2) / (lat1 - lat2);
+                double intl = (lat - lat1) / (lat2 - lat1);
+                return tab[((intlat - 1) * nv + lev) * st + k] * intt
+                       + tab[(intlat * nv + lev) * st + k] * intl;
+            }
+            if (lat >= lat2 && lat < lat3) {
+                double intt = (lat - lat3) / (lat2 - lat3);
+                double intl = (lat - lat2) / (lat3 - lat2);
+                return tab[(intlat * nv + lev) * st + k] * intt
+                       + tab[((intlat + 1) * nv + lev) * st + k] * intl;
+            }
+            return tab[(intlat * nv + lev) * st + k];
+        };
+        for (int lev = 0; lev < nv; lev++) {
+            const double rho = Rho[id * nv + lev];
+            double       u, v;
+            wind_uv(o, Mh, id, lev, rho, u, v);
+            const double w = W[id * nv + lev] / rho;
+            const double n = o.Altitude[lev] / ztop;
+            double       kuv, kw;
+            if (n >= ns) {
+                kuv = Rv_fac * o.S.Ruv_sponge * pow(sin(0.5 * M_PI * (n - ns) * (1.0) / (1.0 - ns)), 2.0);
+                kw  = Rv_fac * o.S.Rw_sponge * pow(sin(0.5 * M_PI * (n - ns) * (1.0) / (1.0 - ns)), 2.0);
+            }
+            else {
+                kuv = 0.0;
+                kw  = 0.0;
+            }
+            double unew, vnew, wnew;
+            if (uvm) {
+                unew = (u / dt + kuv * mean(o.vbar, 3, 0, lev)) / (1.0 / dt + kuv);
+                vnew = (v / dt + kuv * mean(o.vbar, 3, 1, lev)) / (1.0 / dt + kuv);
+            }
+            else {
+                unew = (u / dt) / (1.0 / dt + kuv);
+                vnew = (v / dt) / (1.0 / dt + kuv);
+            }
+            if (wm)
+                wnew = (w / dt + kw * mean(o.vbar, 3, 2, lev)) / (1.0 / dt + kw);
+            else
+                wnew = (w / dt) / (1.0 / dt + kw);
+            double vx = unew * (-sin(lon)) + vnew * (-sin(lat) * cos(lon));
+            double vy = unew * (cos(lon)) + vnew * (-sin(lat) * sin(lon));
+            double vz = vnew * (cos(lat));
+            Mh[(id * nv + lev) * 3 + 0] = vx * rho;
+            Mh[(id * nv + lev) * 3 + 1] = vy * rho;
+            Mh[(id * nv + lev) * 3 + 2] = vz * rho;
+            W[id * nv + lev]            = wnew * rho;
+            if (tsp) {
+                double kvT = n >= ns ? Rv_fac * o.S.RT_sponge
+                                           * pow(sin(0.5 * M_PI * (n - ns) * (1.0) / (1.0 - ns)), 2.0)
+                                     : 0.0;
+                double temperature = p[id * nv + lev] / Rd[id * nv + lev] / Rho[id * nv + lev];
+                p[id * nv + lev]   = Rho[id * nv + lev] * Rd[id * nv + lev]
+                                   * (temperature / dt + kvT * mean(o.Tbar, 1, 0, lev))
+                                   / (1.0 / dt + kvT);
+            }
+        }
+        for (int lev = 1; lev < nv; lev++) {
+            double xi = o.Altitudeh[lev], xim = o.Altitude[lev - 1], xip = o.Altitude[lev];
+            double intt = (xi - xip) / (xim - xip);
+            double intl = (xi - xim) / (xip - xim);
+            Wh[id * nvi + lev] = W[id * nv + lev - 1] * intt + W[id * nv + lev] * intl;
+        }
+    }
+}
+
 void profx(Oracle& o) {
     std::fill(F(o, "profx_Qheat").begin(), F(o, "profx_Qheat").end(), 0.0);
     recompute_w(o);
+    if (o.sponge)
+        sponge(o);
     compute_temperature(o);
     if (o.conv_adj_iter > 0)
         dry_conv_adj(o);
@@ -1929,6 +2122,30 @@ extern "C" int oracle_conv_adj(void* h, int iterations, int soft) {
     Oracle* o        = (Oracle*)h;
     o->conv_adj_iter = iterations;
     o->conv_soft     = soft != 0;
+    return 0;
+}
+
+extern "C" int oracle_sponge(void* h, const oracle_sponge_params* sp) {
+    Oracle* o = (Oracle*)h;
+    if (!sp) {
+        o->sponge = false;
+        return 0;
+    }
+    o->S        = *sp;
+    o->sponge   = true;
+    o->sp_nstep = sp->first_step;
+    sponge_bins(*o);
+    return 0;
+}
+
+extern "C" int oracle_sponge_means(void* h, double* vbar, double* Tbar) {
+    Oracle* o = (Oracle*)h;
+    if (!o->sponge)
+        return -1;
+    if (vbar)
+        std::copy(o->vbar.begin(), o->vbar.end(), vbar);
+    if (Tbar)
+        std::copy(o->Tbar.begin(), o->Tbar.end(), Tbar);
     return 0;
 }
 

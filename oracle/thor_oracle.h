@@ -50,6 +50,18 @@ int oracle_rt(void* h, const oracle_rt_params* rp);
 // src/ESP/profx_driver.cu:239-290): up to `iterations` rounds per step; soft != 0 for the soft form.
 // A column that exceeds the pass bound makes oracle_step return -3.
 int oracle_conv_adj(void* h, int iterations, int soft);
+// Rayleigh sponge, implicit form (RayleighSponge with raysp_calc_mode = imp; sponge_layer with its
+// zonal means, src/ESP/profx_sponge.cu, run in ProfX after Recompute_W, src/ESP/profx_driver.cu:96-194).
+// Same fields as thorx_sponge_params.
+typedef struct {
+    int    nlat_bins;
+    double Ruv_sponge, Rw_sponge, RT_sponge, ns_ray_sponge;
+    int    damp_uv_to_mean, damp_w_to_mean, RayleighSpongeT, shrink_sponge, t_shrink, first_step;
+} oracle_sponge_params;
+// Enables the sponge (NULL: off). Returns 0.
+int oracle_sponge(void* h, const oracle_sponge_params* sp);
+// Zonal means of the last sponge step: vbar [bin][lev][3] (u, v, w), Tbar [bin][lev].
+int oracle_sponge_means(void* h, double* vbar, double* Tbar);
 // Global absorbed shortwave and outgoing longwave of the last RT call (the reference's
 // ASR_tot / OLR_tot), compensated sums.
 void oracle_rt_totals(void* h, double* asr, double* olr);

@@ -89,7 +89,10 @@ def test_bad_lines_fail_the_file(line):
 
 
 @pytest.mark.parametrize("line,what", [
-    ("RayleighSponge = true", "RayleighSponge"),
+    ("DiffSponge = true", "DiffSponge"),
+    ("RayleighSponge = true\nraysp_calc_mode = exp3", "raysp_calc_mode"),
+    ("RayleighSponge = true\nraysp_calc_mode = implicit", "raysp_calc_mode"),
+    ("RayleighSponge = true\nns_ray_sponge = 1.0", "ns_ray_sponge"),
     ("conv_adj_type = rayph", "conv_adj_type"),
     ("chemistry = true", "chemistry"),
     ("init_PT_profile = parmentier", "init_PT_profile"),
@@ -106,6 +109,19 @@ def test_unsupported_or_invalid_settings_are_rejected(line, what):
     with pytest.raises(esp.ConfigError):
         esp.check_config(c, out)
     assert what in out.getvalue()
+
+
+def test_sponge_keys():
+    c, _ = esp.read_config(HS_THR.replace("RayleighSponge = false", "RayleighSponge = true")
+                           + "nlat_bins = 12\nns_ray_sponge = 0.6\ndamp_w_to_mean = false\n",
+                           io.StringIO())
+    esp.check_config(c, io.StringIO())
+    d = esp.sponge_config(c, 9)
+    assert d["nlat_bins"] == 12 and d["ns_ray_sponge"] == 0.6 and d["first_step"] == 9
+    assert d["damp_w_to_mean"] == 0 and d["damp_uv_to_mean"] == 1 and d["Ruv_sponge"] == 1e-4
+    # the mode is not checked while the sponge is off (src/esp.cu:757-780)
+    c, _ = esp.read_config(HS_THR + "raysp_calc_mode = exp1\n", io.StringIO())
+    esp.check_config(c, io.StringIO())
 
 
 def test_defaults_and_unit_conversions():

@@ -92,6 +92,30 @@ def rt_struct(d):
     return RtParams(*[float(v[n]) for n in RT_F64], *[int(v[n]) for n in RT_INT])
 
 
+SPONGE_FIELDS = [("nlat_bins", ctypes.c_int), ("Ruv_sponge", ctypes.c_double),
+                 ("Rw_sponge", ctypes.c_double), ("RT_sponge", ctypes.c_double),
+                 ("ns_ray_sponge", ctypes.c_double), ("damp_uv_to_mean", ctypes.c_int),
+                 ("damp_w_to_mean", ctypes.c_int), ("RayleighSpongeT", ctypes.c_int),
+                 ("shrink_sponge", ctypes.c_int), ("t_shrink", ctypes.c_int),
+                 ("first_step", ctypes.c_int)]
+# the reference's defaults, src/headers/define.h:59-78
+SPONGE_DEFAULTS = dict(nlat_bins=20, Ruv_sponge=1e-4, Rw_sponge=1e-4, RT_sponge=1e-4,
+                       ns_ray_sponge=0.75, damp_uv_to_mean=1, damp_w_to_mean=1,
+                       RayleighSpongeT=0, shrink_sponge=0, t_shrink=144000, first_step=1)
+
+
+class SpongeParams(ctypes.Structure):
+    """oracle_sponge_params / ref_sponge_params (same layout as thorx_sponge_params)."""
+    _fields_ = SPONGE_FIELDS
+
+
+def sponge_struct(d):
+    v = dict(SPONGE_DEFAULTS)
+    v.update(d)
+    return SpongeParams(*[float(v[n]) if t is ctypes.c_double else int(v[n])
+                          for n, t in SPONGE_FIELDS])
+
+
 # ------------------------------------------------------------------------------------------------
 # Reference grid (reference src/ESP/grid.cu, host code, runs on the CPU)
 # ------------------------------------------------------------------------------------------------
@@ -109,6 +133,13 @@ def ref_lib(nofma=False):
         lib.ref_grid_new.restype = ctypes.c_void_p
         lib.ref_grid_new.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                      ctypes.c_int, ctypes.c_double]
+        lib.ref_grid_new_sponge.restype = ctypes.c_void_p
+        lib.ref_grid_new_sponge.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                            ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                            ctypes.c_int]
+        lib.ref_sim_sponge.restype = ctypes.c_int
+        lib.ref_sim_sponge.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        lib.ref_sim_sponge_means.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         lib.ref_grid_get.restype = ctypes.c_long
         lib.ref_grid_get.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p]
         lib.ref_grid_dims.argtypes = [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_int)] * 4
@@ -141,17 +172,23 @@ def ref_lib(nofma=False):
 class RefGrid:
     """The reference's own Icogrid, built on the host, with its arrays copied out."""
 
-    def __init__(self, glevel, nv, A=EARTH["A"], top=EARTH["Top_altitude"], sprd=1, beta=1.15):
+    def __init__(self, glevel, nv, A=EARTH["A"], top=EARTH["Top_altitude"], sprd=1, beta=1.15,
+                 nlat=None):
+        """nlat: also build the Rayleigh sponge's zonal-mean table with nlat latitude bins."""
         lib = ref_lib()
-        self.h = lib.ref_grid_new(glevel, nv, A, top, sprd, beta)
+        if nlat:
+            self.h = lib.ref_grid_new_sponge(glevel, nv, A, top, sprd, beta, nlat)
+        else:
+            self.h = lib.ref_grid_new(glevel, nv, A, top, sprd, beta)
         d = [ctypes.c_int() for _ in range(4)]
         lib.ref_grid_dims(self.h, *[ctypes.byref(x) for x in d])
         self.point_num, self.nv, self.nl_region, self.nr = [x.value for x in d]
         self.glevel = glevel
         self.arrays = {}
-        for name in GRID_NAMES_F64 + GRID_NAMES_I32:
+        for name in GRID_NAMES_F64 + GRID_NAMES_I32 + (["zonal_mean_tab"] if nlat else []):
             n = lib.ref_grid_get(self.h, name.encode(), None)
             a = np.zeros(n, dtype=np.float64 if name in GRID_NAMES_F64 else np.int32)
+            assert n >= 0, name
             lib.ref_grid_get(self.h, name.encode(), a.ctypes.data)
             self.arrays[name] = a
 
@@ -347,6 +384,10 @@ def oracle_lib():
         lib.oracle_rt.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         lib.oracle_conv_adj.restype = ctypes.c_int
         lib.oracle_conv_adj.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+        lib.oracle_sponge.restype = ctypes.c_int
+        lib.oracle_sponge.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        lib.oracle_sponge_means.restype = ctypes.c_int
+        lib.oracle_sponge_means.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         lib.oracle_rt_totals.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                          ctypes.POINTER(ctypes.c_double)]
         lib.oracle_sum.restype = ctypes.c_double
@@ -367,6 +408,7 @@ class Oracle:
         g = OracleGrid(grid.point_num, grid.nv, grid.nl_region, grid.nr,
                        *[self._keep[k].ctypes.data for k in names])
         self.h = lib.oracle_new(ctypes.byref(g), ctypes.byref(params))
+        self._nv = grid.nv
 
     def set(self, name, a):
         a = np.ascontiguousarray(a, dtype=np.float64)
@@ -389,6 +431,16 @@ class Oracle:
 
     def conv_adj(self, iterations=1, soft=False):
         assert oracle_lib().oracle_conv_adj(self.h, iterations, int(soft)) == 0
+
+    def sponge(self, d):
+        self._sp = sponge_struct(d)
+        assert oracle_lib().oracle_sponge(self.h, ctypes.byref(self._sp)) == 0
+
+    def sponge_means(self):
+        nlat, nv = self._sp.nlat_bins, self._nv
+        vbar, tbar = np.zeros((nlat, nv, 3)), np.zeros((nlat, nv))
+        assert oracle_lib().oracle_sponge_means(self.h, vbar.ctypes.data, tbar.ctypes.data) == 0
+        return vbar, tbar
 
     def rt_totals(self):
         a, o = ctypes.c_double(), ctypes.c_double()
@@ -414,6 +466,7 @@ class RefSim:
         self.lib = ref_lib(nofma)
         self.h = self.lib.ref_sim_new(refgrid.h, ctypes.byref(params))
         assert self.h, "ref_sim_new failed"
+        self._nv = refgrid.nv
 
     def set(self, name, a):
         a = np.ascontiguousarray(a, dtype=np.float64)
@@ -439,6 +492,17 @@ class RefSim:
 
     def conv_adj(self, iterations=1, soft=False):
         assert self.lib.ref_sim_conv_adj(self.h, iterations, int(soft)) == 0
+
+    def sponge(self, refgrid, d):
+        """refgrid: a RefGrid built with nlat = d's nlat_bins."""
+        self._sp = sponge_struct(d)
+        assert self.lib.ref_sim_sponge(self.h, refgrid.h, ctypes.byref(self._sp)) == 0
+
+    def sponge_means(self):
+        nlat, nv = self._sp.nlat_bins, self._nv
+        vbar, tbar = np.zeros((nlat, nv, 3)), np.zeros((nlat, nv))
+        self.lib.ref_sim_sponge_means(self.h, vbar.ctypes.data, tbar.ctypes.data)
+        return vbar, tbar
 
     def rt_totals(self):
         a, o = ctypes.c_double(), ctypes.c_double()

@@ -57,6 +57,29 @@ def rt_params(d):
     return RtParamsC(*[float(v[n]) for n in RT_F64], *[int(v[n]) for n in RT_INT])
 
 
+SPONGE_FIELDS = [("nlat_bins", ctypes.c_int), ("Ruv_sponge", ctypes.c_double),
+                 ("Rw_sponge", ctypes.c_double), ("RT_sponge", ctypes.c_double),
+                 ("ns_ray_sponge", ctypes.c_double), ("damp_uv_to_mean", ctypes.c_int),
+                 ("damp_w_to_mean", ctypes.c_int), ("RayleighSpongeT", ctypes.c_int),
+                 ("shrink_sponge", ctypes.c_int), ("t_shrink", ctypes.c_int),
+                 ("first_step", ctypes.c_int)]
+
+
+class SpongeParamsC(ctypes.Structure):
+    _fields_ = SPONGE_FIELDS
+
+
+def sponge_params(d):
+    """thorx_sponge_params from a dict; missing keys take the reference's defaults
+    (src/headers/define.h:59-78)."""
+    v = dict(nlat_bins=20, Ruv_sponge=1e-4, Rw_sponge=1e-4, RT_sponge=1e-4, ns_ray_sponge=0.75,
+             damp_uv_to_mean=1, damp_w_to_mean=1, RayleighSpongeT=0, shrink_sponge=0,
+             t_shrink=144000, first_step=1)
+    v.update(d)
+    return SpongeParamsC(*[float(v[n]) if t is ctypes.c_double else int(v[n])
+                           for n, t in SPONGE_FIELDS])
+
+
 class SurrogateParamsC(ctypes.Structure):
     _fields_ = [("hidden", ctypes.c_int), ("train_batch", ctypes.c_int),
                 ("log_capacity", ctypes.c_longlong), ("recheck_period", ctypes.c_int),
@@ -133,6 +156,10 @@ def lib():
         L.thorx_set_precision.restype = ci
         L.thorx_conv_adj_enable.argtypes = [vp, ci, ci]
         L.thorx_conv_adj_enable.restype = ci
+        L.thorx_sponge_enable.argtypes = [vp, ctypes.POINTER(SpongeParamsC)]
+        L.thorx_sponge_enable.restype = ci
+        L.thorx_sponge_means.argtypes = [vp, vp, vp]
+        L.thorx_sponge_means.restype = ci
         L.thorx_init_guillot_state.argtypes = [vp] + [ctypes.c_double] * 5 + [ctypes.c_ulonglong,
                                                                              ctypes.c_double]
         L.thorx_init_guillot_state.restype = ci
@@ -181,7 +208,8 @@ EXPORTED = ["thorx_create", "thorx_destroy", "thorx_last_error", "thorx_field_si
             "thorx_surrogate_train", "thorx_surrogate_stats", "thorx_surrogate_layer",
             "thorx_surrogate_layer_grad", "thorx_surrogate_normalisation",
             "thorx_surrogate_forward_host", "thorx_surrogate_gradients_host",
-            "thorx_check_division", "thorx_conv_adj_enable", "thorx_init_guillot_state"]
+            "thorx_check_division", "thorx_conv_adj_enable", "thorx_init_guillot_state",
+            "thorx_sponge_enable", "thorx_sponge_means"]
 
 def device_sum(ptr, n, stream=0):
     """Compensated sum of n doubles at device address `ptr` (thorx_device_sum)."""
@@ -393,6 +421,24 @@ class Thorx:
     def conv_adj(self, iterations=1, soft=False):
         """Dry convective adjustment in every following ProfX (0 iterations: off)."""
         self._check(lib().thorx_conv_adj_enable(self.h, iterations, int(soft)))
+
+    def sponge(self, d=None):
+        """Implicit Rayleigh sponge in every following ProfX (dict as for sponge_params; None:
+        off)."""
+        if d is None:
+            self._sponge = None
+            self._check(lib().thorx_sponge_enable(self.h, None))
+            return
+        self._sponge = sponge_params(d)
+        self._check(lib().thorx_sponge_enable(self.h, ctypes.byref(self._sponge)))
+
+    def sponge_means(self):
+        """(vbar [bin][lev][3], Tbar [bin][lev]) of the last sponge step."""
+        nlat, nv = self._sponge.nlat_bins, self.nv
+        vbar = np.zeros((nlat, nv, 3))
+        tbar = np.zeros((nlat, nv))
+        self._check(lib().thorx_sponge_means(self.h, vbar.ctypes.data, tbar.ctypes.data))
+        return vbar, tbar
 
     # ---- RT surrogate ----
     def sur_create(self, hidden=512, train_batch=8192, log_capacity=0, recheck_period=16,

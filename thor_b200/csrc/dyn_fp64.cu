@@ -358,7 +358,195 @@ __device__ void conv_adj_column(const Geometry& g, const Phys& P, const State& s
     }
 }
 
-__global__ void __launch_bounds__(kColBlock) profx_kernel(Geometry g, Phys P, State s,
+// ---------------------------------------------------------------------------------------------
+// Rayleigh sponge, implicit form (sponge_layer with implicit = true, src/ESP/profx_sponge.cu:144-431,
+// and the zonal means of zonal_uv / zonal_w / zonal_temp, :50-130, summed per bin and level by
+// gpu_sum_on_device_sponge, src/headers/reduction_add.h:242-288). Columns are binned by latitude
+// at set-up (Icogrid::zonal_mean_tab_f, src/ESP/grid.cu:3203-3260). The means kernel takes one
+// CTA per (bin, level) and sums the bin's members in a fixed order (thread-strided, then a fixed
+// tree), so the means are deterministic; W is recomputed from Wh there with Recompute_W's
+// arithmetic, as the reference's means read W after Recompute_W.
+// ---------------------------------------------------------------------------------------------
+constexpr int kSpongeThreads = 256;
+
+__global__ void sponge_trig_kernel(Geometry g, double* trig) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= g.N)
+        return;
+    const int Np  = g.Np;
+    double    lon = g.lon[c];
+    if (lon < 0)
+        lon = lon + 2.0 * M_PI;
+    trig[c]          = sin(lon);
+    trig[Np + c]     = cos(lon);
+    trig[2 * Np + c] = sin(g.lat[c]);
+    trig[3 * Np + c] = cos(g.lat[c]);
+}
+
+__global__ void __launch_bounds__(kSpongeThreads) sponge_means_kernel(Geometry g, Phys P,
+                                                                      Sponge sp, State s) {
+    const int b = blockIdx.x, lev = blockIdx.y;
+    if (b == 0 && lev == 0 && threadIdx.x == 0) { // step factor (profx_driver.cu:154-160)
+        const long long n  = sp.step->nstep;
+        const double    dt = P.timestep;
+        double          rv = 1;
+        if (sp.shrink && n * dt >= sp.t_shrink * dt) {
+            const double shrink_scale = dt * 1000;
+            rv = exp(-(n * dt - sp.t_shrink * dt) / shrink_scale);
+        }
+        sp.step->rv_fac = rv;
+        sp.step->nstep  = n + 1;
+    }
+    if (!(sp.uv_mean || sp.w_mean || sp.temp))
+        return;
+    const int     Np = g.Np, nv = g.nv;
+    const int     m0 = sp.start[b], m1 = sp.start[b + 1];
+    const double  cnt  = (double)(m1 - m0);
+    const double* Alt  = g.Altitude;
+    const double* Alth = g.Altitudeh;
+    const double  xi = Alt[lev], xim = Alth[lev], xip = Alth[lev + 1];
+    const double  intt = (xi - xip) / (xim - xip);
+    const double  intl = (xi - xim) / (xip - xim);
+    double        acc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int m = m0 + threadIdx.x; m < m1; m += kSpongeThreads) {
+        const int    c   = sp.members[m];
+        const int    i   = lev * Np + c;
+        const double rho = s.Rho[i];
+        if (sp.uv_mean) {
+            const double slon = sp.trig[c], clon = sp.trig[Np + c];
+            const double slat = sp.trig[2 * Np + c], clat = sp.trig[3 * Np + c];
+            const double mx = s.Mh[i], my = s.Mh[nv * Np + i], mz = s.Mh[2 * nv * Np + i];
+            const double u = (mx * (-slon) + my * (clon) + mz * 0) / rho;
+            const double v = (mx * (-slat * clon) + my * (-slat * slon) + mz * (clat)) / rho;
+            acc[0] += u / cnt;
+            acc[1] += v / cnt;
+        }
+        if (sp.w_mean) {
+            const double w = s.Wh[lev * Np + c] * intt + s.Wh[(lev + 1) * Np + c] * intl;
+            acc[2] += (w / rho) / cnt;
+        }
+        if (sp.temp)
+            acc[3] += s.p[i] / s.Rd[i] / rho / cnt;
+    }
+    __shared__ double red[kSpongeThreads / 32][4];
+    const int         lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        double x = acc[q];
+        for (int o = 16; o > 0; o >>= 1)
+            x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0)
+            red[warp][q] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+        const int q   = threadIdx.x;
+        double    sum = 0.0;
+        for (int w = 0; w < kSpongeThreads / 32; w++)
+            sum += red[w][q];
+        if (q < 3)
+            sp.vbar[(q * sp.nlat + b) * nv + lev] = sum;
+        else
+            sp.Tbar[b * nv + lev] = sum;
+    }
+}
+
+// The implicit sponge on one column: winds toward the zonal mean of the column's latitude
+// (interpolated between the two nearest bin centres; the polar halves of the outermost bins take
+// their bin's mean), with the rate Rv_fac R sin^2(pi/2 (z/ztop - ns) / (1 - ns)) above ns; then
+// Wh at the interior interfaces from the new W; with the thermal sponge, p from the relaxed T.
+__device__ void sponge_column(const Geometry& g, const Phys& P, const Sponge& sp, const State& s,
+                              int c) {
+    const int     Np = g.Np, nv = g.nv, nlat = sp.nlat;
+    const double* Alt  = g.Altitude;
+    const double* Alth = g.Altitudeh;
+    const double  ztop = Alth[nv];
+    const double  dt   = P.timestep;
+    const double  rv   = sp.step->rv_fac;
+    const double  slon = sp.trig[c], clon = sp.trig[Np + c];
+    const double  slat = sp.trig[2 * Np + c], clat = sp.trig[3 * Np + c];
+    const int     b       = sp.bin[c];
+    const double  des_lat = M_PI / nlat;
+    const double  lat1    = -M_PI / 2 + 0.5 * des_lat + des_lat * (b - 1);
+    const double  lat2    = -M_PI / 2 + 0.5 * des_lat + des_lat * (b);
+    const double  lat3    = -M_PI / 2 + 0.5 * des_lat + des_lat * (b + 1);
+    const double  lat     = g.lat[c];
+    // which means, and their weights: (ba, bb, wa, wb); interp = false takes bin b's mean. A
+    // latitude outside both half-intervals of its bin (only rounding at a bin edge can give one;
+    // the reference leaves the mean unset there) takes its bin's mean too.
+    bool   interp = false;
+    int    ba = b, bb = b;
+    double wa = 0.0, wb = 0.0;
+    if (lat <= -M_PI / 2 + 0.5 * des_lat) {
+    }
+    else if (lat >= -M_PI / 2 + 0.5 * des_lat + des_lat * (nlat - 1)) {
+    }
+    else if (lat >= lat1 && lat < lat2) {
+        interp = true;
+        ba = b - 1;
+        wa = (lat - lat2) / (lat1 - lat2);
+        wb = (lat - lat1) / (lat2 - lat1);
+    }
+    else if (lat >= lat2 && lat < lat3) {
+        interp = true;
+        bb = b + 1;
+        wa = (lat - lat3) / (lat2 - lat3);
+        wb = (lat - lat2) / (lat3 - lat2);
+    }
+    auto mean = [&](const double* tab, int lev) {
+        return interp ? tab[ba * nv + lev] * wa + tab[bb * nv + lev] * wb : tab[b * nv + lev];
+    };
+    const double* ubar = sp.vbar;
+    const double* vbar = sp.vbar + nlat * nv;
+    const double* wbar = sp.vbar + 2 * nlat * nv;
+    for (int lev = 0; lev < nv; lev++) {
+        const int    i   = lev * Np + c;
+        const double rho = s.Rho[i];
+        const double mx = s.Mh[i], my = s.Mh[nv * Np + i], mz = s.Mh[2 * nv * Np + i];
+        const double u = (mx * (-slon) + my * (clon) + mz * 0) / rho;
+        const double v = (mx * (-slat * clon) + my * (-slat * slon) + mz * (clat)) / rho;
+        const double w = s.W[i] / rho;
+        const double n = Alt[lev] / ztop;
+        double       kuv = 0.0, kw = 0.0, kvT = 0.0;
+        if (n >= sp.ns) {
+            const double sn = pow(sin(0.5 * M_PI * (n - sp.ns) * (1.0) / (1.0 - sp.ns)), 2.0);
+            kuv             = rv * sp.Ruv * sn;
+            kw              = rv * sp.Rw * sn;
+            kvT             = rv * sp.RT * sn;
+        }
+        double unew, vnew, wnew;
+        if (sp.uv_mean) {
+            unew = (u / dt + kuv * mean(ubar, lev)) / (1.0 / dt + kuv);
+            vnew = (v / dt + kuv * mean(vbar, lev)) / (1.0 / dt + kuv);
+        }
+        else {
+            unew = (u / dt) / (1.0 / dt + kuv);
+            vnew = (v / dt) / (1.0 / dt + kuv);
+        }
+        if (sp.w_mean)
+            wnew = (w / dt + kw * mean(wbar, lev)) / (1.0 / dt + kw);
+        else
+            wnew = (w / dt) / (1.0 / dt + kw);
+        const double vx = unew * (-slon) + vnew * (-slat * clon);
+        const double vy = unew * (clon) + vnew * (-slat * slon);
+        const double vz = vnew * (clat);
+        s.Mh[i]              = vx * rho;
+        s.Mh[nv * Np + i]     = vy * rho;
+        s.Mh[2 * nv * Np + i] = vz * rho;
+        s.W[i]               = wnew * rho;
+        if (sp.temp) {
+            const double temperature = s.p[i] / s.Rd[i] / rho;
+            s.p[i] = rho * s.Rd[i] * (temperature / dt + kvT * mean(sp.Tbar, lev)) / (1.0 / dt + kvT);
+        }
+    }
+    const int nvi = g.nvi;
+    for (int lev = 1; lev < nv; lev++) {
+        const double intt = g.lt[kLtHIntt * nvi + lev], intl = g.lt[kLtHIntl * nvi + lev];
+        s.Wh[lev * Np + c] = s.W[(lev - 1) * Np + c] * intt + s.W[lev * Np + c] * intl;
+    }
+}
+
+__global__ void __launch_bounds__(kColBlock) profx_kernel(Geometry g, Phys P, Sponge sp, State s,
                                                           bool finish) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= g.N)
@@ -373,6 +561,8 @@ __global__ void __launch_bounds__(kColBlock) profx_kernel(Geometry g, Phys P, St
         double intl = (xi - xim) / (xip - xim);
         s.W[lev * Np + c] = whl * intt + wht * intl;
     }
+    if (sp.nlat > 0) // after Recompute_W, before the temperature (profx_driver.cu:96-194)
+        sponge_column(g, P, sp, s, c);
     for (int lev = 0; lev < nv; lev++) {
         int i  = lev * Np + c;
         s.T[i] = s.p[i] / (s.Rd[i] * s.Rho[i]);
@@ -2106,8 +2296,16 @@ void launch_stencil_weights(const Geometry& g, double* lapw, float* dmw, cudaStr
     stencil_weights_kernel<<<(g.N + kTile - 1) / kTile, kTile, 0, st>>>(g, lapw, dmw);
 }
 
-void launch_profx(const Geometry& g, const Phys& P, const State& s, bool finish, cudaStream_t st) {
-    profx_kernel<<<(g.N + kColBlock - 1) / kColBlock, kColBlock, 0, st>>>(g, P, s, finish);
+void launch_sponge_trig(const Geometry& g, double* trig, cudaStream_t st) {
+    sponge_trig_kernel<<<(g.N + kColBlock - 1) / kColBlock, kColBlock, 0, st>>>(g, trig);
+}
+void launch_sponge_means(const Geometry& g, const Phys& P, const Sponge& sp, const State& s,
+                         cudaStream_t st) {
+    sponge_means_kernel<<<dim3(sp.nlat, g.nv), kSpongeThreads, 0, st>>>(g, P, sp, s);
+}
+void launch_profx(const Geometry& g, const Phys& P, const Sponge& sp, const State& s, bool finish,
+                  cudaStream_t st) {
+    profx_kernel<<<(g.N + kColBlock - 1) / kColBlock, kColBlock, 0, st>>>(g, P, sp, s, finish);
 }
 void launch_profx_finish(const Geometry& g, const State& s, cudaStream_t st) {
     profx_finish_kernel<<<(g.N + kColBlock - 1) / kColBlock, kColBlock, 0, st>>>(g, s);

@@ -52,6 +52,7 @@ struct thorx_ctx {
     double*                          staging     = nullptr; // layout conversion buffer
     size_t                           staging_len = 0;       // doubles
     bool                             rt_enabled  = false;   // double-gray RT in ProfX
+    Sponge                           sp{};                   // Rayleigh sponge (nlat 0: off)
     Surrogate*                       sur         = nullptr; // RT surrogate (thorx_surrogate_create)
     int                              sur_mode    = THORX_SUR_OFF;
     RtConst                          rt_c{};
@@ -239,11 +240,11 @@ int check_flags(thorx_ctx* ctx) {
 
 // Kernel classes of one step, for thorx_kernel_info / thorx_profile_steps.
 enum KClass { KProfx = 0, KAdvTemp, KDiffFirst, KDiffLast, KDivm0, KSlow, KMomentum, KVertical,
-              KUpdateRk2, KRt, KSurrogate, KNumClasses };
+              KUpdateRk2, KRt, KSurrogate, KSponge, KNumClasses };
 const char* const kClassName[KNumClasses] = {"profx", "adv_temp", "diffusion_first",
                                              "diffusion_last", "divm0", "slow_modes", "momentum",
                                              "vertical", "update_rk2", "radiative_transfer",
-                                             "rt_surrogate"};
+                                             "rt_surrogate", "sponge_means"};
 
 cudaEvent_t next_event(thorx_ctx* ctx) {
     if (ctx->event_next == ctx->event_pool.size()) {
@@ -282,8 +283,9 @@ double class_bytes(const thorx_ctx* ctx, int k) {
     const Phys&  P = ctx->P;
     const double ring_geo = 78 * G + 6 * I + N; // areas, areasTr, nvecoa/ti/te, ring, flag
     switch (k) {
-    case KProfx: // Wh, p, Rd, Rho, Mh | W, T, p, Mh
-        return Si + 3 * S + (P.benchmark ? 3 * S : 0) + G + 3 * S + (P.benchmark ? 3 * S : 0);
+    case KProfx: // Wh, p, Rd, Rho, Mh | W, T, p, Mh (+ with the sponge: Mh, sponge tables | Wh)
+        return Si + 3 * S + (P.benchmark || ctx->sp.nlat ? 3 * S : 0) + G + 3 * S
+               + (P.benchmark || ctx->sp.nlat ? 3 * S : 0) + (ctx->sp.nlat ? 5 * G + I + Si : 0);
     case KAdvTemp: // Mhk, Rhok, Wk, Whk, pk, Rd, Cp | Adv, T, h, hh, pt, pth, gtil, gtilh
         return 7 * S + Si + 21 * G + 3 * G + 6 * I + 7 * S + 3 * Si
                + (P.energy ? 3 * S + 2 * Si - 2 * S - Si : 0);
@@ -316,6 +318,8 @@ double class_bytes(const thorx_ctx* ctx, int k) {
                                * ctx->sur->net.H
                          + 5 * S
                    : 0;
+    case KSponge: // Mh, Rho, Wh (+ p, Rd with the thermal sponge), members, trig | means
+        return ctx->sp.nlat ? 4 * S + Si + (ctx->sp.temp ? 2 * S : 0) + I + 4 * G : 0;
     }
     return 0;
 }
@@ -327,6 +331,7 @@ int class_launches(const thorx_ctx* ctx, int k) {
     case KProfx: return ctx->rt_enabled ? 2 : 1; // ProfX, then its pressure update after RT
     case KRt: return ctx->rt_enabled ? 1 : 0;     // one bracket: orbit kernel + column kernel
     case KSurrogate: return (ctx->sur && ctx->sur_mode == THORX_SUR_USE) ? 1 : 0;
+    case KSponge: return ctx->sp.nlat ? 1 : 0;
     case KAdvTemp: return 3;
     case KDiffFirst: return 3 * (passes - (passes > 0 ? 1 : 0));
     case KDiffLast: return passes > 0 ? 3 : 0;
@@ -342,14 +347,18 @@ int class_launches(const thorx_ctx* ctx, int k) {
 // ESP::ProfX
 int enqueue_profx(thorx_ctx* ctx) {
     CK(cudaMemsetAsync(ctx->s.Qheat, 0, sizeof(double) * ctx->g.nv * ctx->g.Np, ctx->stream));
+    if (ctx->sp.nlat > 0) {
+        KScope k(ctx, KSponge);
+        launch_sponge_means(ctx->g, ctx->P, ctx->sp, ctx->s, ctx->stream);
+    }
     if (!ctx->rt_enabled) {
         KScope k(ctx, KProfx);
-        launch_profx(ctx->g, ctx->P, ctx->s, true, ctx->stream);
+        launch_profx(ctx->g, ctx->P, ctx->sp, ctx->s, true, ctx->stream);
     }
     else { // the physics modules run before Compute_pressure (profx_driver.cu:405-432)
         {
             KScope k(ctx, KProfx);
-            launch_profx(ctx->g, ctx->P, ctx->s, false, ctx->stream);
+            launch_profx(ctx->g, ctx->P, ctx->sp, ctx->s, false, ctx->stream);
         }
         if (ctx->sur && ctx->sur_mode == THORX_SUR_USE) {
             RtFields fm = ctx->rt_f; // plain RT only on re-checked and fallen-back columns
@@ -1234,6 +1243,113 @@ int thorx_conv_adj_enable(thorx_ctx* ctx, int iterations, int soft_adjustment) {
         CK(cudaGraphDestroy(ctx->graph));
         ctx->graph = nullptr;
     }
+    return 0;
+}
+
+int thorx_sponge_enable(thorx_ctx* ctx, const thorx_sponge_params* p) {
+    if (!ctx)
+        return THORX_E_ARG;
+    const Geometry& g = ctx->g;
+    if (p) {
+        if (p->nlat_bins < 1)
+            return fail(ctx, THORX_E_ARG, "thorx_sponge_enable: nlat_bins must be >= 1");
+        if (!(p->ns_ray_sponge >= 0.0 && p->ns_ray_sponge < 1.0))
+            return fail(ctx, THORX_E_ARG, "thorx_sponge_enable: ns_ray_sponge outside [0, 1)");
+        const int N = g.N, Np = g.Np, nv = g.nv, nlat = p->nlat_bins;
+        // latitude bins as Icogrid::zonal_mean_tab_f (src/ESP/grid.cu:3203-3260): bin j holds
+        // lat_array[j] <= lat < lat_array[j + 1], the edges accumulated from -pi/2 in steps of
+        // pi / nlat; lat >= lat_array[nlat] goes to the last bin. A latitude below -pi/2 (which
+        // the reference leaves without a slot) goes to bin 0.
+        std::vector<double> lat(Np), lat_array(nlat + 1);
+        CK(cudaMemcpy(lat.data(), g.lat, Np * sizeof(double), cudaMemcpyDeviceToHost));
+        const double des_lat = M_PI / nlat;
+        lat_array[0]         = -M_PI / 2.0;
+        for (int j = 1; j < nlat + 1; j++)
+            lat_array[j] = lat_array[j - 1] + des_lat;
+        std::vector<int> bin(Np, 0), start(nlat + 1, 0), members(N), fill(nlat, 0);
+        for (int c = 0; c < N; c++) {
+            int b = 0;
+            for (int j = 0; j < nlat; j++)
+                if (lat[c] >= lat_array[j] && lat[c] < lat_array[j + 1]) {
+                    b = j;
+                    break;
+                }
+            if (lat[c] >= lat_array[nlat])
+                b = nlat - 1;
+            bin[c] = b;
+            start[b + 1]++;
+        }
+        for (int j = 0; j < nlat; j++)
+            start[j + 1] += start[j];
+        for (int c = 0; c < N; c++)
+            members[start[bin[c]] + fill[bin[c]]++] = c;
+        Sponge sp{};
+        int *  dbin, *dstart, *dmem;
+        double *trig, *vbar, *Tbar;
+        if (dev_alloc(ctx, &dbin, (size_t)Np) || dev_alloc(ctx, &dstart, (size_t)nlat + 1)
+            || dev_alloc(ctx, &dmem, (size_t)N) || dev_alloc(ctx, &trig, (size_t)4 * Np)
+            || dev_alloc(ctx, &vbar, (size_t)3 * nlat * nv) || dev_alloc(ctx, &Tbar, (size_t)nlat * nv)
+            || dev_alloc(ctx, &sp.step, 1))
+            return THORX_E_CUDA;
+        CK(cudaMemcpy(dbin, bin.data(), Np * sizeof(int), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(dstart, start.data(), (nlat + 1) * sizeof(int), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(dmem, members.data(), N * sizeof(int), cudaMemcpyHostToDevice));
+        CK(cudaMemset(vbar, 0, (size_t)3 * nlat * nv * sizeof(double)));
+        CK(cudaMemset(Tbar, 0, (size_t)nlat * nv * sizeof(double)));
+        const SpongeStep st0{p->first_step, 1.0};
+        CK(cudaMemcpy(sp.step, &st0, sizeof(st0), cudaMemcpyHostToDevice));
+        launch_sponge_trig(g, trig, ctx->stream);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(ctx->stream));
+        sp.nlat     = nlat;
+        sp.Ruv      = p->Ruv_sponge;
+        sp.Rw       = p->Rw_sponge;
+        sp.RT       = p->RT_sponge;
+        sp.ns       = p->ns_ray_sponge;
+        sp.uv_mean  = p->damp_uv_to_mean != 0;
+        sp.w_mean   = p->damp_w_to_mean != 0;
+        sp.temp     = p->RayleighSpongeT != 0;
+        sp.shrink   = p->shrink_sponge != 0;
+        sp.t_shrink = p->t_shrink;
+        sp.bin      = dbin;
+        sp.start    = dstart;
+        sp.members  = dmem;
+        sp.trig     = trig;
+        sp.vbar     = vbar;
+        sp.Tbar     = Tbar;
+        ctx->sp     = sp;
+    }
+    else
+        ctx->sp.nlat = 0;
+    if (ctx->graph_exec) { // the captured step holds the previous set-up
+        CK(cudaGraphExecDestroy(ctx->graph_exec));
+        ctx->graph_exec = nullptr;
+    }
+    if (ctx->graph) {
+        CK(cudaGraphDestroy(ctx->graph));
+        ctx->graph = nullptr;
+    }
+    return 0;
+}
+
+int thorx_sponge_means(thorx_ctx* ctx, double* vbar, double* Tbar) {
+    if (!ctx)
+        return THORX_E_ARG;
+    const Sponge& sp = ctx->sp;
+    if (sp.nlat == 0)
+        return fail(ctx, THORX_E_STATE, "thorx_sponge_means: the sponge is off");
+    const int nlat = sp.nlat, nv = ctx->g.nv;
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (vbar) {
+        std::vector<double> t((size_t)3 * nlat * nv);
+        CK(cudaMemcpy(t.data(), sp.vbar, t.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        for (int k = 0; k < 3; k++)
+            for (int b = 0; b < nlat; b++)
+                for (int lev = 0; lev < nv; lev++)
+                    vbar[((size_t)b * nv + lev) * 3 + k] = t[((size_t)k * nlat + b) * nv + lev];
+    }
+    if (Tbar)
+        CK(cudaMemcpy(Tbar, sp.Tbar, (size_t)nlat * nv * sizeof(double), cudaMemcpyDeviceToHost));
     return 0;
 }
 

@@ -135,10 +135,41 @@ size_t vertical_smem_bytes(const Geometry& g);
 void launch_level_tables(const Geometry& g, const Phys& P, double* lt, cudaStream_t st);
 void launch_stencil_weights(const Geometry& g, double* lapw, float* dmw, cudaStream_t st);
 
+// Rayleigh sponge layer at the top of the model (RayleighSponge with raysp_calc_mode = imp,
+// reference src/ESP/profx_sponge.cu, called at src/ESP/profx_driver.cu:96-194): winds (and with
+// temp, the temperature) above the fractional height ns are relaxed implicitly toward the zonal
+// mean of their latitude bin (or toward zero). nlat == 0: off.
+struct SpongeStep { // device-resident so that a captured step graph advances it
+    long long nstep;  // step number of the next physics step
+    double    rv_fac; // strength factor of the current step (shrink_sponge)
+};
+struct Sponge {
+    int           nlat;            // latitude bins of the zonal means
+    double        Ruv, Rw, RT, ns; // damping rates [1/s]; bottom of the sponge (z / ztop)
+    bool          uv_mean, w_mean; // damp toward the zonal mean (else toward zero)
+    bool          temp;            // thermal sponge (RayleighSpongeT)
+    bool          shrink;          // shrink_sponge
+    long long     t_shrink;        // steps after which the sponge shrinks
+    const int*    bin;             // [Np] latitude bin of each column
+    const int*    start;           // [nlat + 1] first entry of each bin in members
+    const int*    members;         // [N] the columns of each bin, in increasing index
+    const double* trig;            // [4][Np] sin(lon), cos(lon) (lon in [0, 2 pi)), sin(lat), cos(lat)
+    double*       vbar;            // [3][nlat][nv] zonal means of u, v, w: (k * nlat + bin) * nv + lev
+    double*       Tbar;            // [nlat][nv] zonal mean temperature
+    SpongeStep*   step;
+};
+
 // Kernel launchers (thor_b200/csrc/dyn_fp64.cu).
+// The sponge's zonal means and step factor, before launch_profx (sp.nlat > 0 only); and the
+// per-column trigonometric table it uses, once at set-up.
+void launch_sponge_means(const Geometry& g, const Phys& P, const Sponge& sp, const State& s,
+                         cudaStream_t st);
+void launch_sponge_trig(const Geometry& g, double* trig, cudaStream_t st);
 // ProfX up to the physics modules; with finish, also the pressure update and NaN check, which
-// launch_profx_finish does separately when modules run in between.
-void launch_profx(const Geometry& g, const Phys& P, const State& s, bool finish, cudaStream_t st);
+// launch_profx_finish does separately when modules run in between. The sponge (sp.nlat > 0) runs
+// between Recompute_W and the temperature.
+void launch_profx(const Geometry& g, const Phys& P, const Sponge& sp, const State& s, bool finish,
+                  cudaStream_t st);
 void launch_profx_finish(const Geometry& g, const State& s, cudaStream_t st);
 void launch_adv_temp(const Geometry& g, const Phys& P, const State& s, cudaStream_t st);
 void launch_diffusion(const Geometry& g, const Phys& P, const State& s, int stepnum, bool last,

@@ -15,8 +15,8 @@ outputs, global diagnostics and log lines (src/esp.cu:1381-1480), batch and cont
 Differences, each stated where it applies:
   * state files are NumPy .npz archives, not HDF5 (there is no HDF5 library here); the arrays keep
     the reference's names and memory layout ([column][level][component]);
-  * keys for physics that this build does not implement (sponges, the RayPH convective
-    adjustment, chemistry, boundary layer, ultra-hot thermodynamics, refined vertical grids,
+  * keys for physics that this build does not implement (the diffusive sponge, the explicit
+    Rayleigh-sponge modes exp1 and exp3, the RayPH convective adjustment, chemistry, boundary layer, ultra-hot thermodynamics, refined vertical grids,
     picket-fence or two-stream RT, the Parmentier and constant-N initial profiles) are accepted at
     their default values
     and rejected with an error naming the key otherwise;
@@ -103,19 +103,19 @@ KEYS = {
     "output_mean": (bool, True, "output"),
     "out_interm_momentum": (bool, False, "output"),
     "output_diffusion": (bool, False, "output"),
-    "RayleighSponge": (bool, False, "fixed"),
-    "RayleighSpongeT": (bool, False, "fixed"),
+    "RayleighSponge": (bool, False, "path"),
+    "RayleighSpongeT": (bool, False, "path"),
     "DiffSponge": (bool, False, "fixed"),
-    "shrink_sponge": (bool, False, "fixed"),
-    "t_shrink": (int, 144000, "ignored"),
-    "raysp_calc_mode": (str, "imp", "ignored"),
-    "nlat_bins": (int, 20, "ignored"),
-    "Ruv_sponge": (float, 1e-4, "ignored"),
-    "Rw_sponge": (float, 1e-4, "ignored"),
-    "RT_sponge": (float, 1e-4, "ignored"),
-    "ns_ray_sponge": (float, 0.75, "ignored"),
-    "damp_uv_to_mean": (bool, True, "ignored"),
-    "damp_w_to_mean": (bool, True, "ignored"),
+    "shrink_sponge": (bool, False, "path"),
+    "t_shrink": (int, 144000, "path"),
+    "raysp_calc_mode": (str, "imp", "path"),
+    "nlat_bins": (int, 20, "path"),
+    "Ruv_sponge": (float, 1e-4, "path"),
+    "Rw_sponge": (float, 1e-4, "path"),
+    "RT_sponge": (float, 1e-4, "path"),
+    "ns_ray_sponge": (float, 0.75, "path"),
+    "damp_uv_to_mean": (bool, True, "path"),
+    "damp_w_to_mean": (bool, True, "path"),
     "Dv_sponge": (float, 0.01, "ignored"),
     "ns_diff_sponge": (float, 0.75, "ignored"),
     "order_diff_sponge": (int, 2, "ignored"),
@@ -260,6 +260,14 @@ def check_config(c, out=sys.stdout):
          "Bad value for VertHyDiffOrder! Must be multiple of 2 greater than/equal to 4.")
     for k, allowed in CHOICES.items():
         need(c[k] in allowed, "%s = %s: this build supports %s" % (k, c[k], " | ".join(allowed)))
+    if c["RayleighSponge"]:  # src/esp.cu:757-780: the mode is read only with the sponge on
+        need(c["raysp_calc_mode"] in ("imp", "exp1", "exp3"),
+             "raysp_calc_mode config item not recognised: [%s]" % c["raysp_calc_mode"])
+        need(c["raysp_calc_mode"] not in ("exp1", "exp3"),
+             "raysp_calc_mode = %s: not implemented in this build (allowed: imp)"
+             % c["raysp_calc_mode"])
+        need(c["nlat_bins"] >= 1, "nlat_bins must be >= 1")
+        need(0.0 <= c["ns_ray_sponge"] < 1.0, "ns_ray_sponge must be in [0, 1)")
     for k, (kind, default, role) in KEYS.items():
         if role == "fixed":
             allowed = ALLOWED.get(k, (default,))
@@ -272,6 +280,15 @@ def check_config(c, out=sys.stdout):
     for k in ("output_mean", "out_interm_momentum", "output_diffusion"):
         if c[k]:
             out.write("WARNING: %s = true: those arrays are not written by this build\n" % k)
+
+
+def sponge_config(c, first_step):
+    """The Rayleigh-sponge keys as thorx_sponge_params (the Thorx.sponge dict)."""
+    return dict(nlat_bins=c["nlat_bins"], Ruv_sponge=c["Ruv_sponge"], Rw_sponge=c["Rw_sponge"],
+                RT_sponge=c["RT_sponge"], ns_ray_sponge=c["ns_ray_sponge"],
+                damp_uv_to_mean=int(c["damp_uv_to_mean"]), damp_w_to_mean=int(c["damp_w_to_mean"]),
+                RayleighSpongeT=int(c["RayleighSpongeT"]), shrink_sponge=int(c["shrink_sponge"]),
+                t_shrink=c["t_shrink"], first_step=first_step)
 
 
 def thorx_params(c):
@@ -526,6 +543,8 @@ def run(argv=None, out=sys.stdout):
             x.rt_enable(rt_config(c, step_idx))
         if c["conv_adj"]:
             x.conv_adj(c["conv_adj_iter"], c["soft_adjustment"])
+        if c["RayleighSponge"]:
+            x.sponge(sponge_config(c, step_idx))
         nsmax = c["num_steps"]
         logs = Logs(out_dir, sim_id, continuing, c["globdiag"])
         grid_file = os.path.join(out_dir, "esp_output_grid_%s.npz" % sim_id)
