@@ -166,6 +166,45 @@ int thorx_sponge_enable(thorx_ctx* ctx, const thorx_sponge_params* sp);
  * may be NULL. THORX_E_STATE when the sponge is off. */
 int thorx_sponge_means(thorx_ctx* ctx, double* vbar, double* Tbar);
 
+/* ---- Physics modules: the reference's phy_modules_* interface (src/headers/phy_modules.h:57-98)
+ * as C callbacks, called where ESP calls the module manager: dyn_core_loop_init after Thor's
+ * initial copies (src/ESP/thor_driver.cu:116), dyn_core_loop_slow_modes after the hyperdiffusion of
+ * every RK stage (:641), dyn_core_loop_fast_modes between Vertical_Eq and Density_Pressure_Eqs of
+ * every small step (:1290), dyn_core_loop_end after Thor's final copies (:1465), phy_loop in ProfX
+ * after the benchmark forcing and the built-in RT, before Compute_pressure
+ * (src/ESP/profx_driver.cu:405-416). Every hook may be NULL. A hook enqueues its device work on
+ * `stream` (the context's stream) and returns 0, or a nonzero code that the enqueuing call
+ * returns. thorx_step captures one step as a CUDA graph, so there the hooks run once, at capture,
+ * and what they enqueued is replayed every step: their work must be stream-ordered device work
+ * (kernels, device-to-device copies and sets) that keeps any per-step state on the device.
+ * thorx_profx and thorx_thor call the hooks every time. rk (0..2) and ns (small step) locate the
+ * call; times is the reference's `times` (the RK stage's small time step). ---- */
+typedef struct {
+    void* user;
+    int (*dyn_core_loop_init)(void* user, thorx_ctx* ctx, void* stream);
+    int (*dyn_core_loop_slow_modes)(void* user, thorx_ctx* ctx, void* stream, int rk, double times);
+    int (*dyn_core_loop_fast_modes)(void* user, thorx_ctx* ctx, void* stream, int rk, int ns,
+                                    double times);
+    int (*dyn_core_loop_end)(void* user, thorx_ctx* ctx, void* stream);
+    int (*phy_loop)(void* user, thorx_ctx* ctx, void* stream, double time_step);
+} thorx_module;
+/* Adds a module (at most 8; hooks run in the order modules were added). A step graph captured
+ * earlier is re-captured. */
+int thorx_module_add(thorx_ctx* ctx, const thorx_module* m);
+/* device_RK_array_manager::register_array (src/ESP/phy_modules_device.cu:53-67): the RK stages
+ * reset array = arrayi - arrayk at the start of stages 2 and 3 (UpdateRK) and accumulate
+ * arrayk += array at the end of every stage (UpdateRK2), elementwise over
+ * dimensions * nv * plane doubles (plane from thorx_device_field). At most 10 arrays. */
+int thorx_rk_register_array(thorx_ctx* ctx, double* array, double* arrayk, double* arrayi,
+                            int dimensions);
+/* The context's device array of a field, for module kernels: *dev, its levels (nv or nv+1), its
+ * components (1 or 3) and the plane stride (doubles): element (lev, col, comp) is at
+ * dev[(comp * levels + lev) * plane + col]. Names: the thorx_get_field names and the dycore's
+ * stage and deviation arrays "Rhok", "Rhos", "Mhk", "Mhs", "Whk", "Whs", "Wk", "pressurek",
+ * "pressures", and "profx_dMh", "profx_dWh" (module tendencies of the slow modes). */
+int thorx_device_field(thorx_ctx* ctx, const char* name, double** dev, int* levels,
+                       int* components, long* plane);
+
 /* One physics step, ESP::ProfX (src/ESP/profx_driver.cu:70-474): W from Wh, T and potential
  * temperature from p and rho, Held-Suarez forcing when core_benchmark says so, p = rho Rd T,
  * and the NaN check (reported at the next synchronising call as THORX_E_NAN). */

@@ -197,6 +197,9 @@ struct ref_sponge_params {
 
 struct RefSim {
     ref_params                     p;
+    // the probe module (ref_sim_probe): a tracer through the reference's RK array registry
+    bool                           probe = false;
+    device_RK_array_manager        rkm;
     bool                           sponge = false;
     ref_sponge_params              S{};
     int                            max_count = 0, sp_step = 1;
@@ -562,6 +565,55 @@ static int ref_sponge_step(RefSim* s) {
     return 0;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Probe module: a physics module of this harness (not of the reference), called at the points
+// where ESP calls the module manager (src/ESP/thor_driver.cu:116,641,1290,1465;
+// src/ESP/profx_driver.cu:405-416). It carries a two-component tracer through the reference's own
+// RK array registry (device_RK_array_manager, consumed by UpdateRK/UpdateRK2) with a tendency of 1
+// per second, snapshots Rhos and Whs at the fast-mode hook of the last small step, and adds 0.5 K
+// to the temperature in phy_loop. The product's test module does the same through its C ABI.
+// ---------------------------------------------------------------------------------------------
+__global__ void probe_add(double* x, long n, double v) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        x[i] += v;
+}
+
+extern "C" int ref_sim_probe(void* h) {
+    RefSim*    s = (RefSim*)h;
+    const long N = s->N, nv = s->nv;
+    for (auto n : {"tracer", "tracerk", "tracers"})
+        if (sim_alloc(s, n, 2 * N * nv))
+            return -2;
+    if (sim_alloc(s, "snap_Rhos", N * nv) || sim_alloc(s, "snap_Whs", N * s->nvi))
+        return -2;
+    if (!s->rkm.register_array(s->f["tracers"], s->f["tracerk"], s->f["tracer"], 2))
+        return -1;
+    s->probe = true;
+    return 0;
+}
+
+static void probe_phy_loop(RefSim* s) {
+    probe_add<<<256, 256>>>(s->f["temperature"], (long)s->N * s->nv, 0.5);
+}
+static void probe_init(RefSim* s) {
+    const long n = 2L * s->N * s->nv;
+    cudaMemcpy(s->f["tracerk"], s->f["tracer"], n * 8, cudaMemcpyDeviceToDevice);
+    cudaMemset(s->f["tracers"], 0, n * 8);
+}
+static void probe_fast(RefSim* s, int rk, int ns, int ns_it, double times) {
+    probe_add<<<256, 256>>>(s->f["tracers"], 2L * s->N * s->nv, times);
+    if (rk == 2 && ns == ns_it - 1) {
+        cudaMemcpy(s->f["snap_Rhos"], s->f["Rhos"], (size_t)s->N * s->nv * 8,
+                   cudaMemcpyDeviceToDevice);
+        cudaMemcpy(s->f["snap_Whs"], s->f["Whs"], (size_t)s->N * s->nvi * 8,
+                   cudaMemcpyDeviceToDevice);
+    }
+    cudaDeviceSynchronize();
+}
+static void probe_end(RefSim* s) {
+    cudaMemcpy(s->f["tracer"], s->f["tracerk"], 2L * s->N * s->nv * 8, cudaMemcpyDeviceToDevice);
+}
+
 extern "C" void ref_sim_rt_totals(void* h, double* asr, double* olr) {
     RefSim* s = (RefSim*)h;
     *asr      = s->ASR_tot;
@@ -674,6 +726,10 @@ static int ref_profx(RefSim* s) {
     }
     if (s->rt && ref_rt_step(s))
         return -1;
+    if (s->probe) {
+        probe_phy_loop(s);
+        REF_CHECK(cudaDeviceSynchronize());
+    }
     Compute_pressure<<<NB, NTH>>>(F["pressure"], F["temperature"], F["Rho"], F["Rd"], N);
     REF_CHECK(cudaDeviceSynchronize());
     return 0;
@@ -700,6 +756,13 @@ static int ref_thor(RefSim* s) {
     double     A = P.A, dt = P.timestep;
 
     REF_CHECK(cudaDeviceSynchronize());
+    // the RK array registry is one set of constants per library: load this simulation's
+    if (s->probe)
+        s->rkm.allocate_device_array();
+    else {
+        int zero = 0;
+        cudaMemcpyToSymbol(num_dynamical_arrays, &zero, sizeof(int));
+    }
     cudaMemcpy(F["Mhk"], F["Mh"], N * nv * 3 * 8, cudaMemcpyDeviceToDevice);
     cudaMemcpy(F["Whk"], F["Wh"], N * nvi * 8, cudaMemcpyDeviceToDevice);
     cudaMemcpy(F["Wk"], F["W"], N * nv * 8, cudaMemcpyDeviceToDevice);
@@ -710,6 +773,8 @@ static int ref_thor(RefSim* s) {
     cudaMemset(F["Whs"], 0, 8 * N * nvi);
     cudaMemset(F["Ws"], 0, 8 * N * nv);
     cudaMemset(F["pressures"], 0, 8 * N * nv);
+    if (s->probe)
+        probe_init(s);
 
     for (int rk = 0; rk < 3; rk++) {
         int    ns_it = (rk == 0) ? 1 : (rk == 1 ? 3 : 6);
@@ -863,6 +928,8 @@ static int ref_thor(RefSim* s) {
                 s->diag_data_d);
             REF_CHECK(cudaDeviceSynchronize());
             REF_CHECK(cudaGetLastError());
+            if (s->probe)
+                probe_fast(s, rk, ns, ns_it, times);
             Density_Pressure_Eqs<LN, LN><<<NB, NT>>>(
                 F["pressures"], F["pressurek"], F["Rhos"], F["Rhok"], F["Mhs"], F["Mhk"],
                 F["Whs"], F["Whk"], F["pt"], F["pth"], F["epotential"], F["epotentialh"],
@@ -891,6 +958,8 @@ static int ref_thor(RefSim* s) {
     cudaMemcpy(F["W"], F["Wk"], N * nv * 8, cudaMemcpyDeviceToDevice);
     cudaMemcpy(F["Rho"], F["Rhok"], N * nv * 8, cudaMemcpyDeviceToDevice);
     cudaMemcpy(F["pressure"], F["pressurek"], N * nv * 8, cudaMemcpyDeviceToDevice);
+    if (s->probe)
+        probe_end(s);
     REF_CHECK(cudaDeviceSynchronize());
     return 0;
 }
@@ -982,6 +1051,10 @@ extern "C" void ref_sim_free(void* h) {
     cudaFree(s->diag_data_d);
     delete[] s->Altitude_h;
     cudaFree(s->zonal_mean_tab_d);
+    if (s->probe) { // leave the registry empty for the next simulation of this library
+        int zero = 0;
+        cudaMemcpyToSymbol(num_dynamical_arrays, &zero, sizeof(int));
+    }
     delete[] s->vbar_h;
     delete[] s->Tbar_h;
     delete s;

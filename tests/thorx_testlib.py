@@ -140,6 +140,8 @@ def ref_lib(nofma=False):
         lib.ref_sim_sponge.restype = ctypes.c_int
         lib.ref_sim_sponge.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         lib.ref_sim_sponge_means.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        lib.ref_sim_probe.restype = ctypes.c_int
+        lib.ref_sim_probe.argtypes = [ctypes.c_void_p]
         lib.ref_grid_get.restype = ctypes.c_long
         lib.ref_grid_get.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p]
         lib.ref_grid_dims.argtypes = [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_int)] * 4
@@ -492,6 +494,11 @@ class RefSim:
 
     def conv_adj(self, iterations=1, soft=False):
         assert self.lib.ref_sim_conv_adj(self.h, iterations, int(soft)) == 0
+
+    def probe(self):
+        """The harness's probe module (oracle/ref_harness.cu): a tracer through the reference's
+        RK array registry, snapshots at the fast-mode hook, +0.5 K in phy_loop."""
+        assert self.lib.ref_sim_probe(self.h) == 0
 
     def sponge(self, refgrid, d):
         """refgrid: a RefGrid built with nlat = d's nlat_bins."""

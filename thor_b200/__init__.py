@@ -160,6 +160,10 @@ def lib():
         L.thorx_sponge_enable.restype = ci
         L.thorx_sponge_means.argtypes = [vp, vp, vp]
         L.thorx_sponge_means.restype = ci
+        L.thorx_device_field.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(vp),
+                                         ctypes.POINTER(ci), ctypes.POINTER(ci),
+                                         ctypes.POINTER(ctypes.c_long)]
+        L.thorx_device_field.restype = ci
         L.thorx_init_guillot_state.argtypes = [vp] + [ctypes.c_double] * 5 + [ctypes.c_ulonglong,
                                                                              ctypes.c_double]
         L.thorx_init_guillot_state.restype = ci
@@ -209,7 +213,8 @@ EXPORTED = ["thorx_create", "thorx_destroy", "thorx_last_error", "thorx_field_si
             "thorx_surrogate_layer_grad", "thorx_surrogate_normalisation",
             "thorx_surrogate_forward_host", "thorx_surrogate_gradients_host",
             "thorx_check_division", "thorx_conv_adj_enable", "thorx_init_guillot_state",
-            "thorx_sponge_enable", "thorx_sponge_means"]
+            "thorx_sponge_enable", "thorx_sponge_means", "thorx_module_add",
+            "thorx_rk_register_array", "thorx_device_field"]
 
 def device_sum(ptr, n, stream=0):
     """Compensated sum of n doubles at device address `ptr` (thorx_device_sum)."""
@@ -431,6 +436,14 @@ class Thorx:
             return
         self._sponge = sponge_params(d)
         self._check(lib().thorx_sponge_enable(self.h, ctypes.byref(self._sponge)))
+
+    def device_field(self, name):
+        """(device address, levels, components, plane stride) of a context array, for module
+        kernels (thorx_device_field)."""
+        d, lv, k, pl = ctypes.c_void_p(), ctypes.c_int(), ctypes.c_int(), ctypes.c_long()
+        self._check(lib().thorx_device_field(self.h, name.encode(), ctypes.byref(d),
+                                             ctypes.byref(lv), ctypes.byref(k), ctypes.byref(pl)))
+        return d.value, lv.value, k.value, pl.value
 
     def sponge_means(self):
         """(vbar [bin][lev][3], Tbar [bin][lev]) of the last sponge step."""

@@ -1839,6 +1839,12 @@ __global__ void THORX_KATTR_MOM
 // divergences) [2][nv][32] and c'/d' [2][nv][32], 55 KB at nv = 48, three CTAs per SM.
 // Level-only factors come from the per-level tables.
 // ---------------------------------------------------------------------------------------------
+// kPart: 0 = the whole fused sequence; 1 = Prepare_Implicit_Vertical and Vertical_Eq only (Whs
+// written); 2 = Density_Pressure_Eqs only (horizontal flux divergences on every warp, then the
+// update, reading the Whs a part-1 launch wrote). Parts 1 and 2 bracket a physics module's
+// fast-mode hook, which the reference calls between Vertical_Eq and Density_Pressure_Eqs
+// (src/ESP/thor_driver.cu:1222-1304); they compute what the fused kernel computes, value for value.
+template<int kPart>
 __global__ void THORX_KATTR_VERT
     vertical_kernel(Geometry g, Phys P, State s, double deltat) {
     extern __shared__ double smem[];
@@ -1871,7 +1877,7 @@ __global__ void THORX_KATTR_VERT
     }
 
     // ---- phase 1: Sp, Sd (Prepare_Implicit_Vertical) ----
-    if (active)
+    if (kPart != 2 && active)
         for (int lev = threadIdx.y; lev < nv; lev += kLevGroups) {
             const int    i      = lev * Np + c;
             const double RoC    = s.Rd[i] / (s.Cp[i] - s.Rd[i]);
@@ -1903,10 +1909,11 @@ __global__ void THORX_KATTR_VERT
             sSp[lev * kTile + x] = nflxp + s.Slowp[i];
             sSd[lev * kTile + x] = nflxr + s.SlowRho[i];
         }
-    __syncthreads();
+    if (kPart != 2)
+        __syncthreads();
 
     // ---- phase 2: tridiagonal rows at the interior interfaces ----
-    if (active) {
+    if (kPart != 2 && active) {
         const double dt2 = pow(deltat, 2.0);
         for (int lev = 1 + threadIdx.y; lev < nv; lev += kLevGroups) {
             const double alth = Alth[lev];
@@ -1998,7 +2005,8 @@ __global__ void THORX_KATTR_VERT
             rd[lev * Np + c] = -C0;
         }
     }
-    __syncthreads();
+    if (kPart != 2)
+        __syncthreads();
 
     // ---- phase 3: the Thomas elimination and back substitution (warp 0), while the other warps
     // compute the horizontal flux divergences of Density_Pressure_Eqs, which do not depend on
@@ -2006,7 +2014,7 @@ __global__ void THORX_KATTR_VERT
     double*    sFr  = sSp; // rscale * div(Mhs) per level
     double*    sFpt = sSd; // rscale * div((Mhs + Mhk) pt) (or the energy form's) per level
     const bool eeq  = P.energy;
-    if (threadIdx.y == 0) {
+    if (kPart != 2 && threadIdx.y == 0) {
         if (active) {
             // the eliminated coefficients go to shared memory: no store to global memory inside
             // the sweep, so the row loads of later interfaces are free to be issued early
@@ -2042,8 +2050,11 @@ __global__ void THORX_KATTR_VERT
             s.Whs[c] = 0.0;
         }
     }
-    else if (active) {
-        for (int lev = threadIdx.y - 1; lev < nv; lev += kLevGroups - 1) {
+    else if (kPart != 1 && active) {
+        // the fused kernel's warp 0 is solving meanwhile; part 2 has every warp here
+        const int first = kPart == 2 ? (int)threadIdx.y : (int)threadIdx.y - 1;
+        const int step  = kPart == 2 ? kLevGroups : kLevGroups - 1;
+        for (int lev = first; lev < nv; lev += step) {
             const double rscale = deep ? lt[kLtRscale * nvi + lev] : 1.0;
             double       sr[3], st[3];
 #pragma unroll
@@ -2083,7 +2094,7 @@ __global__ void THORX_KATTR_VERT
         }
     }
     __syncthreads();
-    if (!active)
+    if (kPart == 1 || !active)
         return;
 
     // ---- phase 4: Density_Pressure_Eqs, vertical terms and the update ----
@@ -2348,16 +2359,48 @@ void launch_momentum(const Geometry& g, const Phys& P, const State& s, double dt
         momentum_kernel<double><<<tile_grid_tail(g), tile_block(), 0, st>>>(g, P, s, dt);
 }
 size_t vertical_smem_bytes(const Geometry& g) { return sizeof(double) * kTile * (21 + 4 * g.nv); }
-void launch_vertical(const Geometry& g, const Phys& P, const State& s, double dt,
-                     cudaStream_t st) {
+template<int kPart>
+void launch_vertical_part(const Geometry& g, const Phys& P, const State& s, double dt,
+                          cudaStream_t st) {
     const size_t  smem       = vertical_smem_bytes(g);
     static size_t configured = 0;
     if (smem > configured) {
-        cudaFuncSetAttribute(vertical_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(vertical_kernel<kPart>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem);
         configured = smem;
     }
-    vertical_kernel<<<tile_grid(g), tile_block(), smem, st>>>(g, P, s, dt);
+    vertical_kernel<kPart><<<tile_grid(g), tile_block(), smem, st>>>(g, P, s, dt);
+}
+void launch_vertical(const Geometry& g, const Phys& P, const State& s, double dt, int part,
+                     cudaStream_t st) {
+    if (part == 1)
+        launch_vertical_part<1>(g, P, s, dt, st);
+    else if (part == 2)
+        launch_vertical_part<2>(g, P, s, dt, st);
+    else
+        launch_vertical_part<0>(g, P, s, dt, st);
+}
+
+// Registered module arrays (device_RK_array_manager, src/ESP/phy_modules_device.cu:47-77): the
+// deviation reset of UpdateRK, array = arrayi - arrayk (src/headers/dyn/thor_auxiliary.h:376-387),
+// and the accumulation of UpdateRK2, arrayk += array (:483-494), elementwise.
+__global__ void rk_arrays_kernel(RkArrays t, int mode) {
+    const int       a = blockIdx.y;
+    const long long n = t.count[a];
+    double*         x = t.array[a];
+    double*         k = t.arrayk[a];
+    const double*   i = t.arrayi[a];
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+         e += (long long)gridDim.x * blockDim.x) {
+        if (mode == 0)
+            x[e] = i[e] - k[e];
+        else
+            k[e] += x[e];
+    }
+}
+void launch_rk_arrays(const RkArrays& t, int mode, cudaStream_t st) {
+    if (t.n > 0)
+        rk_arrays_kernel<<<dim3(148 * 4, t.n), 256, 0, st>>>(t, mode);
 }
 void launch_update_rk2(const Geometry& g, const Phys& P, const State& s, cudaStream_t st) {
     update_rk2_kernel<<<tile_grid(g), dim3(kTile, kRk2Groups), 0, st>>>(g, P, s);

@@ -53,6 +53,8 @@ struct thorx_ctx {
     size_t                           staging_len = 0;       // doubles
     bool                             rt_enabled  = false;   // double-gray RT in ProfX
     Sponge                           sp{};                   // Rayleigh sponge (nlat 0: off)
+    std::vector<thorx_module>        modules;                // physics modules, in call order
+    RkArrays                         rk_arrays{};            // their RK-updated arrays
     Surrogate*                       sur         = nullptr; // RT surrogate (thorx_surrogate_create)
     int                              sur_mode    = THORX_SUR_OFF;
     RtConst                          rt_c{};
@@ -275,6 +277,30 @@ struct KScope {
     }
 };
 
+// Calls one hook of every module that has it; a nonzero return ends the enqueuing call.
+#define THORX_HOOK(name, ...)                                                                      \
+    do {                                                                                          \
+        for (const thorx_module& m_ : ctx->modules)                                               \
+            if (m_.name) {                                                                        \
+                const int rc_ = m_.name(m_.user, ctx, (void*)ctx->stream, ##__VA_ARGS__);         \
+                if (rc_)                                                                          \
+                    return fail(ctx, rc_, "module hook " #name " returned " + std::to_string(rc_)); \
+            }                                                                                     \
+    } while (0)
+
+bool has_fast_hook(const thorx_ctx* ctx) {
+    for (const thorx_module& m : ctx->modules)
+        if (m.dyn_core_loop_fast_modes)
+            return true;
+    return false;
+}
+bool has_phy_loop(const thorx_ctx* ctx) {
+    for (const thorx_module& m : ctx->modules)
+        if (m.phy_loop)
+            return true;
+    return false;
+}
+
 // Algorithmic bytes of one launch of a kernel class: every element the kernel must read or
 // write, counted once (neighbour re-reads are not counted), geometry included.
 double class_bytes(const thorx_ctx* ctx, int k) {
@@ -328,7 +354,8 @@ int class_launches(const thorx_ctx* ctx, int k) {
     const Phys& P      = ctx->P;
     const int   passes = P.HyDiff ? P.HyDiffOrder / 2 : 0;
     switch (k) {
-    case KProfx: return ctx->rt_enabled ? 2 : 1; // ProfX, then its pressure update after RT
+    case KProfx: // ProfX, then its pressure update after RT or the modules' phy_loop
+        return ctx->rt_enabled || has_phy_loop(ctx) ? 2 : 1;
     case KRt: return ctx->rt_enabled ? 1 : 0;     // one bracket: orbit kernel + column kernel
     case KSurrogate: return (ctx->sur && ctx->sur_mode == THORX_SUR_USE) ? 1 : 0;
     case KSponge: return ctx->sp.nlat ? 1 : 0;
@@ -338,7 +365,7 @@ int class_launches(const thorx_ctx* ctx, int k) {
     case KDivm0: return P.DivDampP ? 3 + 10 : 0;
     case KSlow: return 3;
     case KMomentum: return 10;
-    case KVertical: return 10;
+    case KVertical: return has_fast_hook(ctx) ? 20 : 10; // split around the fast-mode hook
     case KUpdateRk2: return 3;
     }
     return 0;
@@ -351,7 +378,7 @@ int enqueue_profx(thorx_ctx* ctx) {
         KScope k(ctx, KSponge);
         launch_sponge_means(ctx->g, ctx->P, ctx->sp, ctx->s, ctx->stream);
     }
-    if (!ctx->rt_enabled) {
+    if (!ctx->rt_enabled && !has_phy_loop(ctx)) {
         KScope k(ctx, KProfx);
         launch_profx(ctx->g, ctx->P, ctx->sp, ctx->s, true, ctx->stream);
     }
@@ -360,7 +387,9 @@ int enqueue_profx(thorx_ctx* ctx) {
             KScope k(ctx, KProfx);
             launch_profx(ctx->g, ctx->P, ctx->sp, ctx->s, false, ctx->stream);
         }
-        if (ctx->sur && ctx->sur_mode == THORX_SUR_USE) {
+        if (!ctx->rt_enabled) {
+        }
+        else if (ctx->sur && ctx->sur_mode == THORX_SUR_USE) {
             RtFields fm = ctx->rt_f; // plain RT only on re-checked and fallen-back columns
             fm.fallback = ctx->sur->fallback;
             fm.period   = ctx->sur->period;
@@ -382,6 +411,7 @@ int enqueue_profx(thorx_ctx* ctx) {
             if (ctx->sur && ctx->sur_mode == THORX_SUR_LOG)
                 ctx->sur->log_step(ctx->g, ctx->s, ctx->rt_f, ctx->stream);
         }
+        THORX_HOOK(phy_loop, ctx->P.timestep);
         {
             KScope k(ctx, KProfx);
             launch_profx_finish(ctx->g, ctx->s, ctx->stream);
@@ -407,6 +437,8 @@ int enqueue_thor(thorx_ctx* ctx) {
     CK(cudaMemsetAsync(s.Rhos, 0, cell, st));
     CK(cudaMemsetAsync(s.Whs, 0, iface, st));
     CK(cudaMemsetAsync(s.ps, 0, cell, st));
+    THORX_HOOK(dyn_core_loop_init);
+    const bool split = has_fast_hook(ctx);
     for (int rk = 0; rk < 3; rk++) {
         const int    ns_it = (rk == 0) ? 1 : (rk == 1 ? 3 : 6);
         const double times = (rk == 0) ? P.timestep / 3.0 : P.timestep / 6.0;
@@ -421,6 +453,7 @@ int enqueue_thor(thorx_ctx* ctx) {
                 launch_diffusion(g, P, s, i, i == passes - 1, st);
             }
         }
+        THORX_HOOK(dyn_core_loop_slow_modes, rk, times);
         if (P.DivDampP) {
             KScope k(ctx, KDivm0);
             launch_divm0(g, P, s, false, st);
@@ -429,6 +462,8 @@ int enqueue_thor(thorx_ctx* ctx) {
             KScope k(ctx, KSlow);
             launch_slow_modes(g, P, s, rk > 0, st);
         }
+        if (rk > 0)
+            launch_rk_arrays(ctx->rk_arrays, 0, st);
         for (int ns = 0; ns < ns_it; ns++) {
             if (P.DivDampP) {
                 KScope k(ctx, KDivm0);
@@ -438,21 +473,34 @@ int enqueue_thor(thorx_ctx* ctx) {
                 KScope k(ctx, KMomentum);
                 launch_momentum(g, P, s, times, st);
             }
-            {
+            if (!split) {
                 KScope k(ctx, KVertical);
-                launch_vertical(g, P, s, times, st);
+                launch_vertical(g, P, s, times, 0, st);
+            }
+            else { // the modules' fast-mode hooks between Vertical_Eq and Density_Pressure_Eqs
+                {
+                    KScope k(ctx, KVertical);
+                    launch_vertical(g, P, s, times, 1, st);
+                }
+                THORX_HOOK(dyn_core_loop_fast_modes, rk, ns, times);
+                {
+                    KScope k(ctx, KVertical);
+                    launch_vertical(g, P, s, times, 2, st);
+                }
             }
         }
         {
             KScope k(ctx, KUpdateRk2);
             launch_update_rk2(g, P, s, st);
         }
+        launch_rk_arrays(ctx->rk_arrays, 1, st);
     }
     CK(cudaMemcpyAsync(s.Mh, s.Mhk, 3 * cell, cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync(s.Wh, s.Whk, iface, cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync(s.W, s.Wk, cell, cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync(s.Rho, s.Rhok, cell, cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync(s.p, s.pk, cell, cudaMemcpyDeviceToDevice, st));
+    THORX_HOOK(dyn_core_loop_end);
     CK(cudaGetLastError());
     return 0;
 }
@@ -1012,8 +1060,11 @@ int thorx_step(thorx_ctx* ctx, int nsteps) {
             rc = enqueue_thor(ctx);
         cudaGraph_t graph = nullptr;
         cudaError_t e     = cudaStreamEndCapture(ctx->stream, &graph);
-        if (rc)
+        if (rc) {
+            if (graph)
+                cudaGraphDestroy(graph);
             return rc;
+        }
         if (e != cudaSuccess)
             return fail(ctx, THORX_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
         ctx->graph = graph;
@@ -1037,6 +1088,8 @@ int thorx_kernels_per_step(const thorx_ctx* ctx) {
     for (int k = 0; k < KNumClasses; k++)
         n += class_launches(ctx, k);
     n += ctx->rt_enabled ? 1 : 0; // the RT bracket holds two kernels
+    if (ctx->rk_arrays.n > 0)
+        n += 5; // UpdateRK's reset in stages 2 and 3, UpdateRK2's accumulation in all three
     if (ctx->sur && ctx->sur_mode == THORX_SUR_USE)
         n += 5; // features, four GEMMs and the combine in one bracket
     if (ctx->sur && ctx->sur_mode == THORX_SUR_LOG)
@@ -1718,6 +1771,69 @@ int thorx_check_division(long long n, unsigned long long seed, long long mismatc
         return free_fail(THORX_E_CUDA, std::string(fn) + ": " + cudaGetErrorString(e));
     mismatches[0] = (long long)h[0];
     mismatches[1] = (long long)h[1];
+    return 0;
+}
+
+int thorx_module_add(thorx_ctx* ctx, const thorx_module* m) {
+    if (!ctx)
+        return THORX_E_ARG;
+    if (!m)
+        return fail(ctx, THORX_E_ARG, "thorx_module_add: null module");
+    if (ctx->modules.size() >= 8)
+        return fail(ctx, THORX_E_ARG, "thorx_module_add: at most 8 modules");
+    ctx->modules.push_back(*m);
+    return drop_graph(ctx);
+}
+
+int thorx_rk_register_array(thorx_ctx* ctx, double* array, double* arrayk, double* arrayi,
+                            int dimensions) {
+    if (!ctx)
+        return THORX_E_ARG;
+    RkArrays& t = ctx->rk_arrays;
+    if (!array || !arrayk || !arrayi || dimensions < 1)
+        return fail(ctx, THORX_E_ARG, "thorx_rk_register_array: null array or dimensions < 1");
+    if (t.n >= kMaxRkArrays)
+        return fail(ctx, THORX_E_ARG, "thorx_rk_register_array: at most 10 arrays");
+    t.array[t.n]  = array;
+    t.arrayk[t.n] = arrayk;
+    t.arrayi[t.n] = arrayi;
+    t.count[t.n]  = (long long)dimensions * ctx->g.nv * ctx->g.Np;
+    t.n++;
+    return drop_graph(ctx);
+}
+
+int thorx_device_field(thorx_ctx* ctx, const char* name, double** dev, int* levels,
+                       int* components, long* plane) {
+    if (!ctx)
+        return THORX_E_ARG;
+    if (!name || !dev)
+        return fail(ctx, THORX_E_ARG, "thorx_device_field: null argument");
+    State&    s  = ctx->s;
+    const int nv = ctx->g.nv;
+    const std::map<std::string, FieldDesc> stage = {
+        {"Rhok", {&s.Rhok, nv, 1}},       {"Rhos", {&s.Rhos, nv, 1}},
+        {"Mhk", {&s.Mhk, nv, 3}},         {"Mhs", {&s.Mhs, nv, 3}},
+        {"Whk", {&s.Whk, nv + 1, 1}},     {"Whs", {&s.Whs, nv + 1, 1}},
+        {"Wk", {&s.Wk, nv, 1}},           {"pressurek", {&s.pk, nv, 1}},
+        {"pressures", {&s.ps, nv, 1}},    {"profx_dMh", {&s.dMh, nv, 3}},
+        {"profx_dWh", {&s.dWh, nv + 1, 1}}};
+    const FieldDesc* f  = nullptr;
+    auto             it = ctx->fields.find(name);
+    if (it != ctx->fields.end())
+        f = &it->second;
+    else {
+        auto jt = stage.find(name);
+        if (jt == stage.end())
+            return fail(ctx, THORX_E_ARG, std::string("thorx_device_field: unknown field ") + name);
+        f = &jt->second;
+    }
+    *dev = *f->dev;
+    if (levels)
+        *levels = f->L;
+    if (components)
+        *components = f->K;
+    if (plane)
+        *plane = ctx->g.Np;
     return 0;
 }
 

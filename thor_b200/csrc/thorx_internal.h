@@ -180,8 +180,22 @@ void launch_slow_modes(const Geometry& g, const Phys& P, const State& s, bool up
                        cudaStream_t st);
 void launch_momentum(const Geometry& g, const Phys& P, const State& s, double dt,
                      cudaStream_t st);
-void launch_vertical(const Geometry& g, const Phys& P, const State& s, double dt,
+// part 0: Prepare_Implicit_Vertical + Vertical_Eq + Density_Pressure_Eqs in one launch; 1 and 2:
+// the same split before and after Density_Pressure_Eqs (for a module's fast-mode hook).
+void launch_vertical(const Geometry& g, const Phys& P, const State& s, double dt, int part,
                      cudaStream_t st);
+// Physics-module arrays that the RK stages update (device_RK_array_manager): at most
+// kMaxRkArrays, each `count` doubles.
+constexpr int kMaxRkArrays = 10;
+struct RkArrays {
+    int       n;
+    double*   array[kMaxRkArrays];
+    double*   arrayk[kMaxRkArrays];
+    double*   arrayi[kMaxRkArrays];
+    long long count[kMaxRkArrays];
+};
+// mode 0: UpdateRK's deviation reset (array = arrayi - arrayk); 1: UpdateRK2 (arrayk += array).
+void launch_rk_arrays(const RkArrays& t, int mode, cudaStream_t st);
 void launch_update_rk2(const Geometry& g, const Phys& P, const State& s, cudaStream_t st);
 // cnt[0..1] += pairs whose reciprocal-based quotient differs from the IEEE one (double, float)
 void launch_div_check(long long n, unsigned long long seed, unsigned long long* cnt,
