@@ -157,43 +157,56 @@ def test_exclusive_arguments(tmp_path):
 
 def test_batch_log_lookup(tmp_path):
     (tmp_path / "esp_write_log_X.txt").write_text(
-        "#step_number\tfile_number\tfilename\n0\t0\tesp_output_X_0.npz\n20\t1\tesp_output_X_1.npz\n")
-    assert esp.last_output(str(tmp_path), "X") == (1, 20, "esp_output_X_1.npz")
+        "#step_number\tfile_number\tfilename\n0\t0\tesp_output_X_0.h5\n20\t1\tesp_output_X_1.h5\n")
+    assert esp.last_output(str(tmp_path), "X") == (1, 20, "esp_output_X_1.h5")
     assert esp.last_output(str(tmp_path), "Y") is None
 
 
 @pytest.mark.gpu
 def test_run_outputs_logs_and_bitwise_continuation(tmp_path):
+    from thor_b200 import h5
     cfg = tmp_path / "hs.thr"
     cfg.write_text(HS_THR)
     a, b = tmp_path / "a", tmp_path / "b"
     out = io.StringIO()
     assert esp.run([str(cfg), "-o", str(a)], out) == 0, out.getvalue()
     names = sorted(os.listdir(a))
-    for n in ("esp_output_TestHS_0.npz", "esp_output_TestHS_1.npz", "esp_output_TestHS_2.npz",
+    for n in ("esp_output_TestHS_0.h5", "esp_output_TestHS_1.h5", "esp_output_TestHS_2.h5",
               "esp_write_log_TestHS.txt", "esp_global_TestHS.txt", "esp_diagnostics_TestHS.txt",
-              "esp_output_grid_TestHS.npz", "esp_output_planet_TestHS.npz"):
+              "esp_output_grid_TestHS.h5", "esp_output_planet_TestHS.h5"):
         assert n in names, names
     log = (a / "esp_write_log_TestHS.txt").read_text().splitlines()
     assert log[0] == "#step_number\tfile_number\tfilename"
-    assert log[1:] == ["0\t0\tesp_output_TestHS_0.npz", "2\t1\tesp_output_TestHS_1.npz",
-                       "4\t2\tesp_output_TestHS_2.npz"]
+    assert log[1:] == ["0\t0\tesp_output_TestHS_0.h5", "2\t1\tesp_output_TestHS_1.h5",
+                       "4\t2\tesp_output_TestHS_2.h5"]
     glob = [l.split("\t") for l in (a / "esp_global_TestHS.txt").read_text().splitlines()[1:]]
     assert [int(r[0]) for r in glob] == [2, 4] and float(glob[1][1]) == 4 * 1200.0
     m0, m1 = float(glob[0][3]), float(glob[1][3])
     assert abs(m1 - m0) <= 1e-12 * m0  # global mass, compensated sums
-    final = np.load(a / "esp_output_TestHS_2.npz")
-    assert int(final["nstep"]) == 4 and np.all(np.isfinite(final["Rho"]))
-    assert final["Mh"].shape == final["Rho"].shape + (3,) or final["Mh"].size == 3 * final["Rho"].size
+    final = h5.read(str(a / "esp_output_TestHS_2.h5"))
+    assert int(final["nstep"][0][0]) == 4 and np.all(np.isfinite(final["Rho"][0]))
+    assert final["Mh"][0].size == 3 * final["Rho"][0].size
+    assert final["Rho"][1] == {"Variable": "Density", "units": "kg/m^3"}
+    assert float(final["GlobalMass"][0][0]) == m1  # the file's global sums are the log's
+    planet = h5.read(str(a / "esp_output_planet_TestHS.h5"))
+    assert int(planet["glevel"][0][0]) == 4 and float(planet["A"][0][0]) == 6371000.0
     # run 2 steps, then continue from that output for the remaining 2
     out = io.StringIO()
     assert esp.run([str(cfg), "-o", str(b), "-N", "2"], out) == 0, out.getvalue()
     out = io.StringIO()
-    assert esp.run([str(cfg), "-o", str(b), "-c", str(b / "esp_output_TestHS_1.npz")], out) == 0
-    cont = np.load(b / "esp_output_TestHS_2.npz")
-    for f in ("Rho", "Pressure", "Mh", "Wh", "W"):
-        assert np.array_equal(cont[f], final[f]), f
+    assert esp.run([str(cfg), "-o", str(b), "-c", str(b / "esp_output_TestHS_1.h5")], out) == 0
+    cont = h5.read(str(b / "esp_output_TestHS_2.h5"))
+    for f in ("Rho", "Pressure", "Mh", "Wh"):
+        assert np.array_equal(cont[f][0], final[f][0]), f
     # batch mode finds the last output and has nothing left to do
     out = io.StringIO()
     assert esp.run([str(cfg), "-o", str(b), "-b"], out) == 0
     assert "continuing batch run from file" in out.getvalue()
+    # a planet file that does not match the configuration stops a restart
+    bad = HS_THR.replace("glevel = 4", "glevel = 5")
+    cfg2 = tmp_path / "hs5.thr"
+    cfg2.write_text(bad)
+    out = io.StringIO()
+    assert esp.run([str(cfg2), "-o", str(tmp_path / "c"), "-i",
+                    str(b / "esp_output_TestHS_1.h5")], out) == 255
+    assert "mismatch for /glevel" in out.getvalue()

@@ -251,5 +251,8 @@ def test_runner_with_the_sponge(tmp_path):
                    + "damp_uv_to_mean = true\ndamp_w_to_mean = true\nraysp_calc_mode = imp\n")
     out = io.StringIO()
     assert esp.run([str(cfg), "-o", str(tmp_path / "o")], out) == 0, out.getvalue()
-    final = np.load(tmp_path / "o" / "esp_output_TestHS_2.npz")
-    assert int(final["nstep"]) == 4 and np.all(np.isfinite(final["Mh"]))
+    from thor_b200 import h5
+    final = h5.read(str(tmp_path / "o" / "esp_output_TestHS_2.h5"))
+    assert int(final["nstep"][0][0]) == 4 and np.all(np.isfinite(final["Mh"][0]))
+    planet = h5.read(str(tmp_path / "o" / "esp_output_planet_TestHS.h5"))
+    assert planet["RayleighSponge"][0][0] == 1.0 and planet["nlat_bins"][0][0] == 20

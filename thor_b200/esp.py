@@ -13,8 +13,12 @@ outputs, global diagnostics and log lines (src/esp.cu:1381-1480), batch and cont
 (src/esp.cu:848-940) and the three text logs (src/utils/log_writer.cpp).
 
 Differences, each stated where it applies:
-  * state files are NumPy .npz archives, not HDF5 (there is no HDF5 library here); the arrays keep
-    the reference's names and memory layout ([column][level][component]);
+  * output files are HDF5 with the reference's file names, dataset names, units and descriptions
+    and memory layout ([column][level][component]) (src/ESP/esp_output.cu:136-487), written and read
+    by thor_b200/h5.py (there is no HDF5 library here); the grid file lacks the curl operator (not
+    built here), the output files lack the per-cell global-diagnostic arrays (their global sums are
+    written) and the RT's Qheat scaling; restart files may also be the .npz archives of earlier
+    versions of this runner;
   * keys for physics that this build does not implement (the diffusive sponge, the explicit
     Rayleigh-sponge modes exp1 and exp3, the RayPH convective adjustment, chemistry, boundary layer, ultra-hot thermodynamics, refined vertical grids,
     picket-fence or two-stream RT, the Parmentier and constant-N initial profiles) are accepted at
@@ -322,36 +326,228 @@ def rt_config(c, first_step):
 
 
 # ---------------------------------------------------------------------------------------------
-# Files: state archives and the text logs (src/utils/log_writer.cpp)
+# Files: HDF5 outputs (src/ESP/esp_output.cu) and the text logs (src/utils/log_writer.cpp)
 # ---------------------------------------------------------------------------------------------
-# what a restart needs: the prognostic fields and the per-cell gas constants (the step recomputes
-# the temperature from them)
-STATE = ["Rho", "pressure", "Mh", "Wh", "W", "Rd", "Cp"]
+# what a restart reads (src/ESP/esp_initial.cu:1215-1260): the prognostic fields and the per-cell
+# gas constants; dataset names of the output files
+STATE = ["Rho", "pressure", "Mh", "Wh", "Rd", "Cp"]
 ARCHIVE_NAMES = {"Rho": "Rho", "pressure": "Pressure", "Mh": "Mh", "Wh": "Wh", "W": "W",
                  "Rd": "Rd", "Cp": "Cp"}
 
 
 def output_name(sim_id, idx):
-    return "esp_output_%s_%d.npz" % (sim_id, idx)
+    return "esp_output_%s_%d.h5" % (sim_id, idx)
 
 
-def write_state(path, x, nstep, sim_time, extra=None):
-    arrays = {ARCHIVE_NAMES[f]: x.get(f) for f in STATE}
-    arrays["temperature"] = x.get("temperature")
-    arrays["nstep"] = np.array(nstep)
-    arrays["simulation_time"] = np.array(sim_time)
-    for k, v in (extra or {}).items():
-        arrays[k] = np.asarray(v)
-    tmp = path + ".tmp.npz"
-    np.savez(tmp, **arrays)
-    os.replace(tmp, path)
+def _atomic_h5(path):
+    from thor_b200 import h5
+    return h5.H5Writer(path + ".tmp")
+
+
+def write_state(path, x, nstep, sim_time, c, glob=None, rt=None):
+    """ESP::output's state file (src/ESP/esp_output.cu:306-470) and the RT module's and the
+    insolation's store() (radiative_transfer.cu:1286-1336, insolation.cu:484-493)."""
+    w = _atomic_h5(path)
+    w.value("/nstep", int(nstep), "-", "Step number")
+    w.value("/simulation_time", float(sim_time), "s", "Simulation time")
+    w.table("/Rho", x.get("Rho"), "kg/m^3", "Density")
+    w.table("/Pressure", x.get("pressure"), "Pa", "Pressure")
+    w.table("/Mh", x.get("Mh"), "kg m^-2 s^-1", "Horizontal Momentum")
+    w.table("/Wh", x.get("Wh"), "kg m^-2 s^-1", "Vertical Momentum")
+    if glob is not None:
+        E, M, AMx, AMy, AMz, Ent = glob
+        w.value("/GlobalE", E, "kg m^2/s^2", "Global Total Energy")
+        w.value("/GlobalEnt", Ent, "kg m^2/s^2 K^-1", "Global Entropy")
+        w.value("/GlobalMass", M, "kg", "Global Mass")
+        w.value("/GlobalAMx", AMx, "kg m^2/s", "Global AngMomX")
+        w.value("/GlobalAMy", AMy, "kg m^2/s", "Global AngMomY")
+        w.value("/GlobalAMz", AMz, "kg m^2/s", "Global AngMomZ")
+    w.table("/Qheat", x.get("profx_Qheat"), "W m^-3", "Physics module Qheat")
+    w.table("/Rd", x.get("Rd"), "J/K/kg", "Local gas constant")
+    w.table("/Cp", x.get("Cp"), "J/K/kg", "Local heat capacity")
+    if rt is not None:
+        asr, olr = rt
+        w.table("/insol", x.get("insol"), "W m^-2", "insolation (instantaneous)")
+        w.table("/insol_annual", x.get("insol_ann"), "W m^-2",
+                "insolation (annual/orbit averaged)")
+        w.table("/flw_up", x.get("flw_up"), "W m^-2", "upward flux (LW)")
+        w.table("/fsw_up", x.get("fsw_up"), "W m^-2", "upward flux (SW)")
+        w.table("/flw_dn", x.get("flw_dn"), "W m^-2", "downward flux (LW)")
+        w.table("/fsw_dn", x.get("fsw_dn"), "W m^-2", "downward flux (SW)")
+        w.table("/tau", x.get("tau"), " ", "optical depth across each layer (not total optical depth)")
+        w.table("/DGQheat", x.get("DG_Qheat"), " ", "Double Gray Qheat")
+        w.value("/ASR", asr, "W", "Absorbed Shortwave Radiation (global total)")
+        w.value("/OLR", olr, "W", "Outgoing Longwave Radiation (global total)")
+        w.table("/cos_zenith_angles", x.get("cos_zenith"), "-", "cos_zenith_angles per column")
+    w.close()
+    os.replace(path + ".tmp", path)
+
+
+def write_grid(path, grid):
+    """ESP::output's grid file (src/ESP/esp_output.cu:144-183), without the curl operator."""
+    d = grid.as_dict()
+    w = _atomic_h5(path)
+    w.table("/Altitude", d["Altitude"], "m", "Altitude")
+    w.table("/Altitudeh", d["Altitudeh"], "m", "Altitude at the interfaces")
+    w.table("/areasT", d["areasT"], "m^2", "Main cells areas")
+    w.table("/lonlat", d["lonlat"], "-", "Longitudes and latitudes")
+    w.value("/point_num", float(d["point_num"]), "-", "Number of grid points in one level")
+    w.value("/nv", float(d["nv"]), "-", "Number of vertical layers")
+    w.table("/pntloc", d["point_local"].astype(np.int32), "-", "Neighbours indexes")
+    w.table("/grad", d["grad"], "m^-1", "Horizontal gradient operator")
+    w.table("/div", d["div"], "m^-1", "Horizontal divergence operator")
+    w.close()
+    os.replace(path + ".tmp", path)
+
+
+def write_planet(path, c):
+    """ESP::output's planet file (src/ESP/esp_output.cu:186-304) with the module manager's, the
+    RT module's and the insolation's store_init (phy_modules.cu:219-237,
+    radiative_transfer.cu:1366-1388, insolation.cu:459-479)."""
+    b = lambda k: 1.0 if c[k] else 0.0
+    w = _atomic_h5(path)
+    w.value("/glevel", int(c["glevel"]), "-", "Horizontal subdivision level")
+    w.value("/vlevel", int(c["vlevel"]), "-", "Vertical subdivision level")
+    w.value("/spring_dynamics", b("spring_dynamics"), "-", "Spring dynamics")
+    w.value("/spring_beta", float(c["spring_beta"]), "-", "Spring Beta")
+    w.value("/A", float(c["radius"]), "m", "Planet radius")
+    w.value("/Rd", float(c["Rd"]), "J/(Kg K)", "Gas constant")
+    w.value("/Omega", float(c["rotation_rate"]), "1/s", "Rotation rate")
+    w.value("/Gravit", float(c["gravitation"]), "m/s^2", "Surface gravity")
+    w.value("/P_Ref", float(c["P_ref"]), "Pa", "Reference pressure")
+    w.value("/Top_altitude", float(c["Top_altitude"]), "m", "Top of the model's domain")
+    w.value("/Cp", float(c["Cp"]), "J/(Kg K)", "Specific heat capacity")
+    w.value("/RayleighSponge", b("RayleighSponge"), "-", "Using Rayleigh SpongeLayer?")
+    w.value("/RayleighSpongeT", b("RayleighSpongeT"), "-", "Using thermal SpongeLayer?")
+    w.value("/DiffSponge", b("DiffSponge"), "-", "Using Diffusive SpongeLayer?")
+    w.value("/DeepModel", b("DeepModel"), "-", "Using Deep Model")
+    w.value("/NonHydro", b("NonHydro"), "-", "Using Non Hydrostatic parameter")
+    w.value("/output_mean", b("output_mean"), "-", "outputting mean quantities")
+    w.value("/output_diffusion", b("output_diffusion"), "-", "outputting diffusion terms")
+    w.value("/out_interm_momentum", b("out_interm_momentum"), "-",
+            "outputting intermediate momentum values")
+    w.value("/DivDampP", b("DivDampP"), "-", "Using Divergence-damping")
+    w.value("/HyDiff", b("HyDiff"), "-", "Using Hyper diffusion")
+    w.value("/Diffc", float(c["Diffc"]), "-", "Hyperdiffusion strength")
+    w.value("/Diffc_v", float(c["Diffc_v"]), "-", "Vertical hyperdiffusion strength")
+    w.value("/Tmean", float(c["Tmean"]), "K", "Mean atmospheric temperature")
+    w.value("/conv_adj", b("conv_adj"), "-", "Using convection adjustment")
+    w.value("/gcm_off", b("gcm_off"), "-", "GCM off")
+    w.value("/single_column", b("single_column"), "-", "single column mode")
+    w.value("/rest", b("rest"), "-", "Starting from rest")
+    w.value("/core_benchmark", int(thorx_params(c)["core_benchmark"]), "-",
+            "Using benchmark forcing")
+    if c["RayleighSponge"]:
+        w.value("/nlat_bins", int(c["nlat_bins"]), "-",
+                "number of lat rings for Rayleigh sponge layer")
+        w.value("/ns_ray_sponge", float(c["ns_ray_sponge"]), "-", "Bottom of rayleigh sponge layer")
+        w.value("/Ruv_sponge", float(c["Ruv_sponge"]), "1/s",
+                "Strength of Rayleigh sponge layer (uv components)")
+        w.value("/Rw_sponge", float(c["Rw_sponge"]), "1/s",
+                "Strength of Rayleigh sponge layer (w component)")
+    w.value("/Tint", float(c["Tint"]), "K", "Temperature of interior heat flux")
+    w.value("/f_lw", float(c["f_lw"]), "-", "fraction of taulw in well-mixed absorber")
+    w.value("/kappa_lw", float(c["kappa_lw"]), "-", "longwave opacity")
+    w.value("/kappa_sw", float(c["kappa_sw"]), "-", "shortwave opacity")
+    w.value("/phy_module", 0.0, "-", "multi")
+    w.value("/surface", 0.0, "-", "include solid/liquid surface")
+    w.value("/Csurf", float(c["Csurf"]), "J/K/m^2", "heat capacity of surface by area")
+    # the module manager (multi) and its modules
+    w.value("/radiative_transfer", b("radiative_transfer"), "-", "Using radiative transfer")
+    w.value("/Tstar", float(c["Tstar"]), "K", "Temperature of host star")
+    w.value("/planet_star_dist", float(c["planet_star_dist"]), "au",
+            "distance b/w host star and planet")
+    w.value("/radius_star", float(c["radius_star"]), "R_sun", "radius of host star")
+    w.value("/diff_ang", float(c["diff_ang"]), "-", "diffusivity factor")
+    w.value("/albedo", float(c["albedo"]), "-", "bond albedo of planet")
+    w.value("/latf_lw", b("latf_lw"), "-", "use lat dependent opacity")
+    w.value("/kappa_lw_pole", float(c["kappa_lw_pole"]), "-", "gray opacity of longwave at poles")
+    w.value("/n_lw", float(c["n_lw"]), "-", "power law exponent for unmixed absorber in LW")
+    w.value("/n_sw", float(c["n_sw"]), "-", "power law exponent for mixed/unmixed absorber in SW")
+    w.value("/rt_type", 0, "-", "Type of radiative transfer physics")
+    w.value("/chemistry", 0.0, "-", "Using relaxation chemistry")
+    w.value("/boundary_layer", 0.0, "-", "Using boundary layer")
+    if c["radiative_transfer"]:
+        w.value("/sync_rot", b("sync_rot"), "-", "enforce synchronous rotation")
+        w.value("/mean_motion", float(c["mean_motion"]), "rad/s", "orbital mean motion")
+        w.value("/alpha_i", float(c["alpha_i"]), "deg", "initial RA of host star")
+        w.value("/true_long_i", float(c["true_long_i"]), "deg",
+                "initial orbital position of planet")
+        w.value("/ecc", float(c["ecc"]), "-", "orbital eccentricity")
+        w.value("/obliquity", float(c["obliquity"]), "deg", "tilt of spin axis")
+        w.value("/longp", float(c["longp"]), "deg", "longitude of periastron")
+    w.close()
+    os.replace(path + ".tmp", path)
+
+
+def output_numbering(path):
+    """(basename, number) of a file named esp_output_<basename>_<number>.h5, else None
+    (match_output_file_numbering_scheme, src/utils/directories.cpp:270-311)."""
+    if not path.endswith(".h5"):
+        return None
+    parts = os.path.basename(path)[:-3].split("_")
+    if len(parts) < 4 or parts[0] != "esp" or parts[1] != "output":
+        return None
+    try:
+        number = int(parts[-1])
+    except ValueError:
+        return None
+    return ("_".join(parts[2:-1]), number) if number > -1 else None
+
+
+def planet_file(initial, continuing):
+    """The planet file that goes with an initial-conditions file (find_continue_file,
+    src/utils/directories.cpp:313-362): esp_output_planet_<basename>.h5 beside an output-named
+    file, <stem>_planet.h5 beside any other. None when continuing from a file without the output
+    naming."""
+    d = os.path.dirname(initial) or "."
+    m = output_numbering(initial)
+    if m is not None:
+        return os.path.join(d, "esp_output_planet_%s.h5" % m[0])
+    if continuing:
+        return None
+    stem = os.path.splitext(os.path.basename(initial))[0]
+    return os.path.join(d, stem + "_planet.h5")
+
+
+def check_planet(path, c, out):
+    """The restart check of src/ESP/esp_initial.cu:1147-1205: A, Top_altitude, glevel, vlevel and
+    surface of the planet file must equal the configuration's. Returns True when they do."""
+    from thor_b200 import h5
+    try:
+        d = h5.read(path)
+    except (OSError, h5.H5FormatError) as e:
+        out.write("planet_file %s not readable: %s\n" % (path, e))
+        return False
+    ok = True
+    for key, want in (("A", float(c["radius"])), ("Top_altitude", float(c["Top_altitude"])),
+                      ("glevel", int(c["glevel"])), ("vlevel", int(c["vlevel"])),
+                      ("surface", 0.0)):
+        if key not in d:
+            out.write("Error reading key /%s from reload config.\n" % key)
+            ok = False
+            continue
+        have = d[key][0].reshape(-1)[0]
+        if have != want:
+            out.write("mismatch for /%s value between config value: %s and initial condition "
+                      "value %s.\n" % (key, want, have))
+            ok = False
+    if not ok:
+        out.write("Could not reload full configuration.\n")
+    return ok
 
 
 def read_state(path):
-    """(fields present in the file, nstep, simulation time)."""
-    with np.load(path) as d:
-        state = {f: np.array(d[ARCHIVE_NAMES[f]]) for f in STATE if ARCHIVE_NAMES[f] in d}
-        return state, int(d["nstep"]), float(d["simulation_time"])
+    """(fields present in the file, nstep, simulation time) of an output file (HDF5) or of an
+    .npz archive of earlier versions of this runner."""
+    if path.endswith(".npz"):
+        with np.load(path) as d:
+            state = {f: np.array(d[ARCHIVE_NAMES[f]]) for f in STATE if ARCHIVE_NAMES[f] in d}
+            return state, int(d["nstep"]), float(d["simulation_time"])
+    from thor_b200 import h5
+    d = h5.read(path)
+    state = {f: d[ARCHIVE_NAMES[f]][0] for f in STATE if ARCHIVE_NAMES[f] in d}
+    return state, int(d["nstep"][0][0]), float(d["simulation_time"][0][0])
 
 
 class Logs:
@@ -504,6 +700,17 @@ def run(argv=None, out=sys.stdout):
             os.path.join(out_dir, output_name(sim_id, 0))):
         out.write("output files already exist in %s; use -w to overwrite\n" % out_dir)
         return 255
+    if start_file is not None and start_file.endswith(".h5"):
+        pf = planet_file(start_file, continuing)
+        if pf is None:
+            out.write("Loading initial conditions: Could not recognise file numbering scheme for "
+                      "input %s\n" % start_file)
+            return 255
+        if not os.path.exists(pf):
+            out.write("planet_file %s not found.\n" % pf)
+            return 255
+        if not check_planet(pf, c, out):
+            return 255
 
     import thor_b200
     # the device: GPU_ID_N (or -g) through CUDA_VISIBLE_DEVICES, before the first CUDA call
@@ -521,7 +728,7 @@ def run(argv=None, out=sys.stdout):
     try:
         if start_file is not None:
             state, nstep0, sim_time0 = read_state(start_file)
-            missing = [f for f in ("Rho", "pressure", "Mh", "Wh", "W") if f not in state]
+            missing = [f for f in ("Rho", "pressure", "Mh", "Wh") if f not in state]
             if missing:
                 out.write("start file %s lacks %s\n" % (start_file, ", ".join(missing)))
                 return 255
@@ -532,7 +739,7 @@ def run(argv=None, out=sys.stdout):
                 x.set(f, v)
             if continuing:
                 step_idx = nstep0 + 1
-                m = re.search(r"_(\d+)\.npz$", start_file)
+                m = re.search(r"_(\d+)\.(h5|npz)$", start_file)
                 first_idx = int(m.group(1)) + 1 if m else 1
         elif c["init_PT_profile"] == "guillot":
             x.init_guillot_state(c["Tmean"], c["Tint"], c["f_lw"], c["kappa_sw"], c["kappa_lw"], 0,
@@ -547,14 +754,13 @@ def run(argv=None, out=sys.stdout):
             x.sponge(sponge_config(c, step_idx))
         nsmax = c["num_steps"]
         logs = Logs(out_dir, sim_id, continuing, c["globdiag"])
-        grid_file = os.path.join(out_dir, "esp_output_grid_%s.npz" % sim_id)
-        np.savez(grid_file, **{k: v for k, v in grid.as_dict().items()
-                               if isinstance(v, np.ndarray)})
-        np.savez(os.path.join(out_dir, "esp_output_planet_%s.npz" % sim_id),
-                 **{k: np.array(v) for k, v in c.items()})
+        write_grid(os.path.join(out_dir, "esp_output_grid_%s.h5" % sim_id), grid)
+        write_planet(os.path.join(out_dir, "esp_output_planet_%s.h5" % sim_id), c)
+        rt_tot = (lambda: x.rt_totals()) if c["radiative_transfer"] else (lambda: None)
         if not continuing:
             name = output_name(sim_id, 0)
-            write_state(os.path.join(out_dir, name), x, 0, sim_time0)
+            write_state(os.path.join(out_dir, name), x, 0, sim_time0, c,
+                        x.globdiag() if c["globdiag"] else None, rt_tot())
             logs.output(0, 0, name)
             first_idx = 1
         del _caught[:]
@@ -579,11 +785,12 @@ def run(argv=None, out=sys.stdout):
             x.sync()
             nstep = nxt
             sim_time = sim_time0 + (nstep - step_idx + 1) * dt
+            glob = x.globdiag() if c["globdiag"] else None
             if c["globdiag"] and nstep % g_out == 0:
-                logs.globdiag(nstep, sim_time, x.globdiag())
+                logs.globdiag(nstep, sim_time, glob)
             if nstep % n_out == 0 or _caught:
                 name = output_name(sim_id, idx)
-                write_state(os.path.join(out_dir, name), x, nstep, sim_time)
+                write_state(os.path.join(out_dir, name), x, nstep, sim_time, c, glob, rt_tot())
                 logs.output(nstep, idx, name)
                 idx += 1
             elapsed = time.time() - t0
