@@ -205,6 +205,13 @@ int thorx_rk_register_array(thorx_ctx* ctx, double* array, double* arrayk, doubl
 int thorx_device_field(thorx_ctx* ctx, const char* name, double** dev, int* levels,
                        int* components, long* plane);
 
+/* Sixth-order (or any even order >= 4) vertical hyperdiffusion in every following step (VertHyDiff
+ * with Diffc_v and VertHyDiffOrder: vertical_diff, src/headers/dyn/thor_diff.h:1198-1426, called
+ * in the hyperdiffusion block of ESP::Thor, src/ESP/thor_driver.cu:590-612; strengths
+ * Kdv6 = Diffc_v dz^order / dt, src/ESP/esp_initial.cu:1327-1335). Like the reference it acts only
+ * with HyDiff on. order 0 switches it off. A step graph captured earlier is re-captured. */
+int thorx_vert_hydiff_enable(thorx_ctx* ctx, double Diffc_v, int order);
+
 /* One physics step, ESP::ProfX (src/ESP/profx_driver.cu:70-474): W from Wh, T and potential
  * temperature from p and rho, Held-Suarez forcing when core_benchmark says so, p = rho Rd T,
  * and the NaN check (reported at the next synchronising call as THORX_E_NAN). */

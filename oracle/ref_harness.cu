@@ -201,6 +201,7 @@ struct RefSim {
     bool                           probe = false;
     device_RK_array_manager        rkm;
     bool                           sponge = false;
+    int                            vhd_order = 0; // vertical hyperdiffusion (VertHyDiff)
     ref_sponge_params              S{};
     int                            max_count = 0, sp_step = 1;
     int*                           zonal_mean_tab_d = nullptr;
@@ -473,6 +474,27 @@ extern "C" int ref_sim_conv_adj(void* h, int iterations, int soft) {
 // The Rayleigh sponge in ProfX (sim.RayleighSponge with raysp_calc_mode = imp), launched as
 // profx_driver.cu:96-194 launches it, with the grid's zonal-mean table (gh from
 // ref_grid_new_sponge with the same nlat_bins).
+// Vertical hyperdiffusion (sim.VertHyDiff): Kdv6 as src/ESP/esp_initial.cu:1327-1335, and the
+// reference's scratch diff2 of 6 (nv + 2) planes per column that vertical_diff needs.
+extern "C" int ref_sim_vert_hydiff(void* h, double Diffc_v, int order) {
+    RefSim*    s = (RefSim*)h;
+    const long N = s->N, nv = s->nv;
+    if (!s->f.count("Kdv6") && sim_alloc(s, "Kdv6", nv))
+        return -2;
+    if (!s->f.count("diff2v") && sim_alloc(s, "diff2v", 6 * N * (nv + 2)))
+        return -2;
+    std::vector<double> k(nv);
+    std::vector<double> alth(nv + 1);
+    REF_CHECK(cudaMemcpy(alth.data(), s->f["Altitudeh"], (nv + 1) * 8, cudaMemcpyDeviceToHost));
+    for (int lev = 0; lev < nv; lev++) {
+        double dz = alth[lev + 1] - alth[lev];
+        k[lev]    = Diffc_v * pow(dz, 1.0 * order) / s->p.timestep;
+    }
+    REF_CHECK(cudaMemcpy(s->f["Kdv6"], k.data(), nv * 8, cudaMemcpyHostToDevice));
+    s->vhd_order = order;
+    return 0;
+}
+
 extern "C" int ref_sim_sponge(void* h, void* gh, const ref_sponge_params* sp) {
     RefSim*  s = (RefSim*)h;
     RefGrid* r = (RefGrid*)gh;
@@ -839,6 +861,16 @@ static int ref_thor(RefSim* s) {
                 F["Altitudeh"], A, F["Rd"], F["Cp"], loc, N, stepnum, true, deep, false, 2,
                 F["Kdh2"], F["boundary_flux"], eeq, P.HyDiffOrder);
             REF_CHECK(cudaDeviceSynchronize());
+            if (s->vhd_order > 0) { // thor_driver.cu:590-612
+                cudaMemset(F["diff"], 0, sizeof(double) * 6 * N * nv);
+                cudaMemset(F["diff2v"], 0, sizeof(double) * 6 * N * (nv + 2));
+                dim3 NBALL0((N / NTH) + 1, 1, 6);
+                vertical_diff<<<NBALL0, NTH>>>(F["diffmv"], F["diffwv"], F["diffrv"], F["diffprv"],
+                                               F["diff"], F["diff2v"], F["Mhk"], F["Rhok"],
+                                               F["temperature"], F["Wk"], F["Kdv6"], F["Altitude"],
+                                               F["Altitudeh"], A, P.Rd, s->vhd_order, deep, N, nv);
+                REF_CHECK(cudaDeviceSynchronize());
+            }
             Correct_Horizontal<<<NBALL1, NTH>>>(F["diffmh"], F["diffmv"], F["func_r"], N);
             REF_CHECK(cudaDeviceSynchronize());
         }

@@ -60,6 +60,9 @@ struct Oracle {
     int  conv_adj_iter = 0;
     bool conv_soft     = false;
     bool conv_fail     = false; // a column exceeded the pass bound
+    // vertical hyperdiffusion (when enabled): order and strengths Kdv6[nv]
+    int vhd_order = 0;
+    Vec Kdv6;
     // Rayleigh sponge (when enabled)
     bool                 sponge = false;
     oracle_sponge_params S{};
@@ -1250,6 +1253,90 @@ void diffusion_pass(Oracle& o, int stepnum, bool laststep) {
 }
 
 // Correct_Horizontal, thor_diff.h:882-915
+// vertical_diff, src/headers/dyn/thor_diff.h:1198-1426, on the stage fields thor_driver.cu:594-612
+// passes (Mhk, Rhok, temperature, Wk): per column and variable, order/2 - 1 second-derivative
+// passes over the column extended by one ghost level at each end (copies of the end levels), the
+// last scaled by sign Kdv6 rho (no rho for the density itself), then a final pass (times Rd for
+// the temperature). diffrv stays zero (include_rho = false).
+void vertical_diff(Oracle& o) {
+    const int    N = o.N, nv = o.nv, order = o.vhd_order;
+    const double sign = pow(-1.0, order / 2 + 1), A = o.P.A, Rd = o.P.Rd;
+    Vec &Mh = F(o, "Mhk"), &Rho = F(o, "Rhok"), &T = F(o, "temperature"), &W = F(o, "Wk");
+    Vec &dmv = F(o, "diffmv"), &dwv = F(o, "diffwv"), &drv = F(o, "diffrv"),
+        &dpv = F(o, "diffprv");
+#pragma omp parallel for schedule(static)
+    for (int id = 0; id < N; id++) {
+        std::vector<double> b2(nv + 2), d(nv);
+        auto pass = [&](bool rd) {
+            for (int lev = 0; lev < nv; lev++) {
+                double dzi = 1.0 / (o.Altitudeh[lev + 1] - o.Altitudeh[lev]);
+                double ri, rup, rlow, dzup, dzlow;
+                if (o.P.DeepModel) {
+                    ri   = A + o.Altitude[lev];
+                    rup  = A + o.Altitudeh[lev + 1];
+                    rlow = A + o.Altitudeh[lev];
+                }
+                else {
+                    ri = rup = rlow = 1.0;
+                }
+                if (lev == 0) {
+                    dzup  = 1.0 / (o.Altitude[1] - o.Altitude[0]);
+                    dzlow = 1.0 / (2.0 * o.Altitude[0]);
+                }
+                else if (lev == nv - 1) {
+                    dzup  = 1.0 / (2 * (o.Altitudeh[lev + 1] - o.Altitude[lev]));
+                    dzlow = 1.0 / (o.Altitude[lev] - o.Altitude[lev - 1]);
+                }
+                else {
+                    dzup  = 1.0 / (o.Altitude[lev + 1] - o.Altitude[lev]);
+                    dzlow = 1.0 / (o.Altitude[lev] - o.Altitude[lev - 1]);
+                }
+                double t = pow(rup, 2) * (b2[lev + 2] - b2[lev + 1]) * dzup
+                           - pow(rlow, 2) * (b2[lev + 1] - b2[lev]) * dzlow;
+                d[lev] = rd ? t * dzi * Rd / pow(ri, 2) : t * dzi / pow(ri, 2);
+            }
+        };
+        for (int var = 0; var < 6; var++) {
+            for (int lev = 0; lev < nv + 2; lev++) {
+                int    l = lev == 0 ? 0 : (lev == nv + 1 ? nv - 1 : lev - 1);
+                double r = Rho[id * nv + l];
+                double v;
+                if (var == 0)
+                    v = r;
+                else if (var <= 3)
+                    v = Mh[(id * nv + l) * 3 + var - 1] / r;
+                else if (var == 4)
+                    v = W[id * nv + l] / r;
+                else
+                    v = T[id * nv + l];
+                b2[lev] = v;
+            }
+            int max_l = order / 2 - 1;
+            for (int l = 0; l < max_l; l++) {
+                pass(false);
+                bool last = l == max_l - 1;
+                for (int lev = 0; lev < nv; lev++)
+                    b2[lev + 1] = !last ? d[lev]
+                                        : (var == 0 ? sign * o.Kdv6[lev] * d[lev]
+                                                    : sign * Rho[id * nv + lev] * o.Kdv6[lev] * d[lev]);
+                b2[0]      = b2[1];
+                b2[nv + 1] = b2[nv];
+            }
+            pass(var == 5);
+            for (int lev = 0; lev < nv; lev++) {
+                if (var == 0)
+                    drv[id * nv + lev] = 0.0;
+                else if (var <= 3)
+                    dmv[(id * nv + lev) * 3 + var - 1] = d[lev];
+                else if (var == 4)
+                    dwv[id * nv + lev] = d[lev];
+                else
+                    dpv[id * nv + lev] = d[lev];
+            }
+        }
+    }
+}
+
 void correct_horizontal(Oracle& o) {
     int  N = o.N, nv = o.nv;
     Vec &dmh = F(o, "diffmh"), &dmv = F(o, "diffmv");
@@ -2028,6 +2115,8 @@ void thor(Oracle& o) {
             }
             zero("diffrh");
             diffusion_pass(o, stepnum, true);
+            if (o.vhd_order > 0)
+                vertical_diff(o);
             correct_horizontal(o);
         }
         zero("DivM");
@@ -2122,6 +2211,18 @@ extern "C" int oracle_conv_adj(void* h, int iterations, int soft) {
     Oracle* o        = (Oracle*)h;
     o->conv_adj_iter = iterations;
     o->conv_soft     = soft != 0;
+    return 0;
+}
+
+extern "C" int oracle_vert_hydiff(void* h, double Diffc_v, int order) {
+    Oracle* o    = (Oracle*)h;
+    o->vhd_order = order;
+    o->Kdv6.assign(o->nv, 0.0);
+    // Kdv6 = Diffc_v dz^order / dt (src/ESP/esp_initial.cu:1327-1335)
+    for (int lev = 0; lev < o->nv; lev++) {
+        double dz    = o->Altitudeh[lev + 1] - o->Altitudeh[lev];
+        o->Kdv6[lev] = Diffc_v * pow(dz, 1.0 * order) / o->P.timestep;
+    }
     return 0;
 }
 

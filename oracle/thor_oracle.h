@@ -62,6 +62,9 @@ typedef struct {
 int oracle_sponge(void* h, const oracle_sponge_params* sp);
 // Zonal means of the last sponge step: vbar [bin][lev][3] (u, v, w), Tbar [bin][lev].
 int oracle_sponge_means(void* h, double* vbar, double* Tbar);
+// Enables the vertical hyperdiffusion of the dynamical core (VertHyDiff, vertical_diff,
+// src/headers/dyn/thor_diff.h:1198-1426) with strength Diffc_v and the given even order (0: off).
+int oracle_vert_hydiff(void* h, double Diffc_v, int order);
 // Global absorbed shortwave and outgoing longwave of the last RT call (the reference's
 // ASR_tot / OLR_tot), compensated sums.
 void oracle_rt_totals(void* h, double* asr, double* olr);

@@ -142,6 +142,8 @@ def ref_lib(nofma=False):
         lib.ref_sim_sponge_means.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         lib.ref_sim_probe.restype = ctypes.c_int
         lib.ref_sim_probe.argtypes = [ctypes.c_void_p]
+        lib.ref_sim_vert_hydiff.restype = ctypes.c_int
+        lib.ref_sim_vert_hydiff.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
         lib.ref_grid_get.restype = ctypes.c_long
         lib.ref_grid_get.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p]
         lib.ref_grid_dims.argtypes = [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_int)] * 4
@@ -386,6 +388,8 @@ def oracle_lib():
         lib.oracle_rt.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         lib.oracle_conv_adj.restype = ctypes.c_int
         lib.oracle_conv_adj.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+        lib.oracle_vert_hydiff.restype = ctypes.c_int
+        lib.oracle_vert_hydiff.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
         lib.oracle_sponge.restype = ctypes.c_int
         lib.oracle_sponge.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         lib.oracle_sponge_means.restype = ctypes.c_int
@@ -437,6 +441,9 @@ class Oracle:
     def sponge(self, d):
         self._sp = sponge_struct(d)
         assert oracle_lib().oracle_sponge(self.h, ctypes.byref(self._sp)) == 0
+
+    def vert_hydiff(self, Diffc_v, order=6):
+        assert oracle_lib().oracle_vert_hydiff(self.h, Diffc_v, order) == 0
 
     def sponge_means(self):
         nlat, nv = self._sp.nlat_bins, self._nv
@@ -494,6 +501,9 @@ class RefSim:
 
     def conv_adj(self, iterations=1, soft=False):
         assert self.lib.ref_sim_conv_adj(self.h, iterations, int(soft)) == 0
+
+    def vert_hydiff(self, Diffc_v, order=6):
+        assert self.lib.ref_sim_vert_hydiff(self.h, Diffc_v, order) == 0
 
     def probe(self):
         """The harness's probe module (oracle/ref_harness.cu): a tracer through the reference's

@@ -164,6 +164,8 @@ def lib():
                                          ctypes.POINTER(ci), ctypes.POINTER(ci),
                                          ctypes.POINTER(ctypes.c_long)]
         L.thorx_device_field.restype = ci
+        L.thorx_vert_hydiff_enable.argtypes = [vp, ctypes.c_double, ci]
+        L.thorx_vert_hydiff_enable.restype = ci
         L.thorx_init_guillot_state.argtypes = [vp] + [ctypes.c_double] * 5 + [ctypes.c_ulonglong,
                                                                              ctypes.c_double]
         L.thorx_init_guillot_state.restype = ci
@@ -214,7 +216,7 @@ EXPORTED = ["thorx_create", "thorx_destroy", "thorx_last_error", "thorx_field_si
             "thorx_surrogate_forward_host", "thorx_surrogate_gradients_host",
             "thorx_check_division", "thorx_conv_adj_enable", "thorx_init_guillot_state",
             "thorx_sponge_enable", "thorx_sponge_means", "thorx_module_add",
-            "thorx_rk_register_array", "thorx_device_field"]
+            "thorx_rk_register_array", "thorx_device_field", "thorx_vert_hydiff_enable"]
 
 def device_sum(ptr, n, stream=0):
     """Compensated sum of n doubles at device address `ptr` (thorx_device_sum)."""
@@ -436,6 +438,10 @@ class Thorx:
             return
         self._sponge = sponge_params(d)
         self._check(lib().thorx_sponge_enable(self.h, ctypes.byref(self._sponge)))
+
+    def vert_hydiff(self, Diffc_v, order=6):
+        """Vertical hyperdiffusion (VertHyDiff) in every following step; order 0: off."""
+        self._check(lib().thorx_vert_hydiff_enable(self.h, Diffc_v, order))
 
     def device_field(self, name):
         """(device address, levels, components, plane stride) of a context array, for module

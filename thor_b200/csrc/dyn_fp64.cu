@@ -1839,6 +1839,120 @@ __global__ void THORX_KATTR_MOM
 // divergences) [2][nv][32] and c'/d' [2][nv][32], 55 KB at nv = 48, three CTAs per SM.
 // Level-only factors come from the per-level tables.
 // ---------------------------------------------------------------------------------------------
+// ---------------------------------------------------------------------------------------------
+// Vertical hyperdiffusion (VertHyDiff: vertical_diff, src/headers/dyn/thor_diff.h:1198-1426, and
+// its radial correction in Correct_Horizontal, :882-915). One thread per column: the variables
+// u, v, w (momentum over density) and T in turn; each goes through order/2 - 1 applications of the
+// reference's second-derivative stencil (values at the ghost levels 0 and nv+1 copied from the
+// end levels), the last one scaled by sign Kdv6 rho, and a final application (times Rd for T).
+// The column sits in shared memory (two planes of nv+2 values per column). The density part of
+// the reference is discarded there (include_rho = false) and is not computed. The results, the
+// momentum part with its radial component removed, are added into diffmh, diffw and diffpr,
+// where the reference keeps them in diffmv, diffwv and diffprv and every consumer adds the pairs.
+// ---------------------------------------------------------------------------------------------
+constexpr int kVdCols = 32;
+
+__global__ void __launch_bounds__(kVdCols) vertical_diff_kernel(Geometry g, Phys P, State s) {
+    extern __shared__ double vsm[];
+    const int nv = g.nv, Np = g.Np, x = threadIdx.x;
+    const int c  = blockIdx.x * kVdCols + x;
+    double*   b2 = vsm;                       // [nv + 2][kVdCols]
+    double*   d  = vsm + (nv + 2) * kVdCols;  // [nv][kVdCols]
+    if (c >= g.N)
+        return;
+    const double* Alt   = g.Altitude;
+    const double* Alth  = g.Altitudeh;
+    const int     order = P.vhd_order;
+    const double  sign  = pow(-1.0, order / 2 + 1);
+    const double  A     = P.A;
+    const int     max_l = order / 2 - 1;
+    const double* fr    = nullptr;
+    // one application of the stencil to b2 into d; scale_rd for the temperature's last one
+    auto stencil = [&](bool scale_rd) {
+        for (int lev = 0; lev < nv; lev++) {
+            const double dzi = 1.0 / (Alth[lev + 1] - Alth[lev]);
+            double       ri, rup, rlow, dzup, dzlow;
+            if (P.DeepModel) {
+                ri   = A + Alt[lev];
+                rup  = A + Alth[lev + 1];
+                rlow = A + Alth[lev];
+            }
+            else {
+                ri = rup = rlow = 1.0;
+            }
+            if (lev == 0) {
+                dzup  = 1.0 / (Alt[1] - Alt[0]);
+                dzlow = 1.0 / (2.0 * Alt[0]);
+            }
+            else if (lev == nv - 1) {
+                dzup  = 1.0 / (2 * (Alth[lev + 1] - Alt[lev]));
+                dzlow = 1.0 / (Alt[lev] - Alt[lev - 1]);
+            }
+            else {
+                dzup  = 1.0 / (Alt[lev + 1] - Alt[lev]);
+                dzlow = 1.0 / (Alt[lev] - Alt[lev - 1]);
+            }
+            const double up  = b2[(lev + 2) * kVdCols + x], mid = b2[(lev + 1) * kVdCols + x];
+            const double low = b2[lev * kVdCols + x];
+            const double t   = pow(rup, 2) * (up - mid) * dzup - pow(rlow, 2) * (mid - low) * dzlow;
+            d[lev * kVdCols + x] = scale_rd ? t * dzi * P.Rd / pow(ri, 2) : t * dzi / pow(ri, 2);
+        }
+    };
+    double* out[3] = {nullptr, nullptr, nullptr};
+    for (int var = 1; var <= 5; var++) {
+        for (int lev = 0; lev < nv + 2; lev++) {
+            const int    l = lev == 0 ? 0 : (lev == nv + 1 ? nv - 1 : lev - 1);
+            const int    i = l * Np + c;
+            const double r = s.Rhok[i];
+            double       v;
+            if (var <= 3)
+                v = s.Mhk[((var - 1) * nv + l) * Np + c] / r;
+            else if (var == 4)
+                v = s.Wk[i] / r;
+            else
+                v = s.T[i];
+            b2[lev * kVdCols + x] = v;
+        }
+        for (int l = 0; l < max_l; l++) {
+            stencil(false);
+            const bool last = l == max_l - 1;
+            for (int lev = 0; lev < nv; lev++) {
+                const double dv = d[lev * kVdCols + x];
+                b2[(lev + 1) * kVdCols + x] = last ? sign * s.Rhok[lev * Np + c] * g.Kdv6[lev] * dv : dv;
+            }
+            b2[x]                   = b2[kVdCols + x];
+            b2[(nv + 1) * kVdCols + x] = b2[nv * kVdCols + x];
+        }
+        stencil(var == 5);
+        if (var <= 3) { // the momentum components: kept (planes 0..2 of diff) until all three exist
+            out[var - 1] = s.diff + (size_t)(var - 1) * nv * Np;
+            for (int lev = 0; lev < nv; lev++)
+                out[var - 1][lev * Np + c] = d[lev * kVdCols + x];
+            if (var == 3) {
+                fr = g.func_r;
+                const double f0 = fr[c], f1 = fr[Np + c], f2 = fr[2 * Np + c];
+                for (int lev = 0; lev < nv; lev++) {
+                    const int i   = lev * Np + c;
+                    double    v0 = out[0][i], v1 = out[1][i], v2 = out[2][i];
+                    const double dmvr = f0 * v0 + f1 * v1 + f2 * v2;
+                    v0 += -f0 * dmvr;
+                    v1 += -f1 * dmvr;
+                    v2 += -f2 * dmvr;
+                    s.diffmh[(0 * nv + lev) * Np + c] += v0;
+                    s.diffmh[(1 * nv + lev) * Np + c] += v1;
+                    s.diffmh[(2 * nv + lev) * Np + c] += v2;
+                }
+            }
+        }
+        else if (var == 4)
+            for (int lev = 0; lev < nv; lev++)
+                s.diffw[lev * Np + c] += d[lev * kVdCols + x];
+        else
+            for (int lev = 0; lev < nv; lev++)
+                s.diffpr[lev * Np + c] += d[lev * kVdCols + x];
+    }
+}
+
 // kPart: 0 = the whole fused sequence; 1 = Prepare_Implicit_Vertical and Vertical_Eq only (Whs
 // written); 2 = Density_Pressure_Eqs only (horizontal flux divergences on every warp, then the
 // update, reading the Whs a part-1 launch wrote). Parts 1 and 2 bracket a physics module's
@@ -2401,6 +2515,16 @@ __global__ void rk_arrays_kernel(RkArrays t, int mode) {
 void launch_rk_arrays(const RkArrays& t, int mode, cudaStream_t st) {
     if (t.n > 0)
         rk_arrays_kernel<<<dim3(148 * 4, t.n), 256, 0, st>>>(t, mode);
+}
+void launch_vertical_diff(const Geometry& g, const Phys& P, const State& s, cudaStream_t st) {
+    const size_t  smem       = sizeof(double) * kVdCols * (2 * g.nv + 2);
+    static size_t configured = 0;
+    if (smem > configured) {
+        cudaFuncSetAttribute(vertical_diff_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+        configured = smem;
+    }
+    vertical_diff_kernel<<<(g.N + kVdCols - 1) / kVdCols, kVdCols, smem, st>>>(g, P, s);
 }
 void launch_update_rk2(const Geometry& g, const Phys& P, const State& s, cudaStream_t st) {
     update_rk2_kernel<<<tile_grid(g), dim3(kTile, kRk2Groups), 0, st>>>(g, P, s);

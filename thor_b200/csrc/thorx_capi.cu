@@ -242,11 +242,12 @@ int check_flags(thorx_ctx* ctx) {
 
 // Kernel classes of one step, for thorx_kernel_info / thorx_profile_steps.
 enum KClass { KProfx = 0, KAdvTemp, KDiffFirst, KDiffLast, KDivm0, KSlow, KMomentum, KVertical,
-              KUpdateRk2, KRt, KSurrogate, KSponge, KNumClasses };
+              KUpdateRk2, KRt, KSurrogate, KSponge, KVertDiff, KNumClasses };
 const char* const kClassName[KNumClasses] = {"profx", "adv_temp", "diffusion_first",
                                              "diffusion_last", "divm0", "slow_modes", "momentum",
                                              "vertical", "update_rk2", "radiative_transfer",
-                                             "rt_surrogate", "sponge_means"};
+                                             "rt_surrogate", "sponge_means",
+                                             "vertical_hyperdiffusion"};
 
 cudaEvent_t next_event(thorx_ctx* ctx) {
     if (ctx->event_next == ctx->event_pool.size()) {
@@ -346,6 +347,9 @@ double class_bytes(const thorx_ctx* ctx, int k) {
                    : 0;
     case KSponge: // Mh, Rho, Wh (+ p, Rd with the thermal sponge), members, trig | means
         return ctx->sp.nlat ? 4 * S + Si + (ctx->sp.temp ? 2 * S : 0) + I + 4 * G : 0;
+    case KVertDiff: // Mhk, Rhok, Wk, T, func_r, diffmh, diffw, diffpr | diff (3), diffmh, diffw,
+                    // diffpr
+        return P.vhd_order ? 11 * S + 3 * G + 3 * S + 5 * S : 0;
     }
     return 0;
 }
@@ -359,6 +363,7 @@ int class_launches(const thorx_ctx* ctx, int k) {
     case KRt: return ctx->rt_enabled ? 1 : 0;     // one bracket: orbit kernel + column kernel
     case KSurrogate: return (ctx->sur && ctx->sur_mode == THORX_SUR_USE) ? 1 : 0;
     case KSponge: return ctx->sp.nlat ? 1 : 0;
+    case KVertDiff: return (P.HyDiff && P.vhd_order) ? 3 : 0;
     case KAdvTemp: return 3;
     case KDiffFirst: return 3 * (passes - (passes > 0 ? 1 : 0));
     case KDiffLast: return passes > 0 ? 3 : 0;
@@ -451,6 +456,10 @@ int enqueue_thor(thorx_ctx* ctx) {
             for (int i = 0; i < passes; i++) {
                 KScope k(ctx, i == passes - 1 ? KDiffLast : KDiffFirst);
                 launch_diffusion(g, P, s, i, i == passes - 1, st);
+            }
+            if (P.vhd_order) { // thor_driver.cu:590-612, inside the hyperdiffusion block
+                KScope k(ctx, KVertDiff);
+                launch_vertical_diff(g, P, s, st);
             }
         }
         THORX_HOOK(dyn_core_loop_slow_modes, rk, times);
@@ -636,6 +645,7 @@ int thorx_create(const thorx_grid* gr, const thorx_params* pr, void* stream, tho
     P.benchmark       = pr->core_benchmark;
     P.mixed           = pr->precision == THORX_MIXED;
     P.conv_adj_iter   = 0; // thorx_conv_adj_enable
+    P.vhd_order       = 0; // thorx_vert_hydiff_enable
     P.conv_soft       = false;
 
     int rc;
@@ -1835,6 +1845,33 @@ int thorx_device_field(thorx_ctx* ctx, const char* name, double** dev, int* leve
     if (plane)
         *plane = ctx->g.Np;
     return 0;
+}
+
+int thorx_vert_hydiff_enable(thorx_ctx* ctx, double Diffc_v, int order) {
+    if (!ctx)
+        return THORX_E_ARG;
+    if (order != 0 && (order < 4 || order % 2))
+        return fail(ctx, THORX_E_ARG, "thorx_vert_hydiff_enable: order must be even and >= 4");
+    const int nv = ctx->g.nv;
+    if (order && nv < 2)
+        return fail(ctx, THORX_E_ARG, "thorx_vert_hydiff_enable: needs at least two levels");
+    if (order) {
+        // Kdv6 = Diffc_v dz^order / dt per level (src/ESP/esp_initial.cu:1327-1335)
+        std::vector<double> k(nv);
+        for (int lev = 0; lev < nv; lev++) {
+            const double dz = ctx->Altitudeh_h[lev + 1] - ctx->Altitudeh_h[lev];
+            k[lev]          = Diffc_v * pow(dz, 1.0 * order) / ctx->P.timestep;
+        }
+        double* d;
+        if (!ctx->g.Kdv6) {
+            if (dev_alloc(ctx, &d, nv))
+                return THORX_E_CUDA;
+            ctx->g.Kdv6 = d;
+        }
+        CK(cudaMemcpy((void*)ctx->g.Kdv6, k.data(), nv * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    ctx->P.vhd_order = order;
+    return drop_graph(ctx);
 }
 
 } // extern "C"

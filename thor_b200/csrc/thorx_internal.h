@@ -55,6 +55,7 @@ struct Geometry {
     const double*  Altitudeh;
     const double*  Kdh4;
     const double*  Kdhz;
+    const double*  Kdv6;     // vertical hyperdiffusion strength per level (null: off)
     const double*  lt; // per-level tables, lt[t * nvi + i] (LevelTable below)
     // Operator weights of the mixed form (stencil_weights_kernel), per column:
     // lapw [7][Np]: hyperdiffusion Laplacian at rscale = 1; entry 0 = the sum of all seven
@@ -98,6 +99,7 @@ struct Phys {
     int    benchmark; // THORX_NO_BENCHMARK .. THORX_SHALLOW_HOT_JUPITER (forcing in ProfX)
     bool   mixed; // momentum-side horizontal stencils computed in FP32 (THORX_MIXED)
     int    conv_adj_iter; // dry convective adjustment: iterations per step (0: off)
+    int    vhd_order;     // vertical hyperdiffusion order (VertHyDiffOrder; 0: off)
     bool   conv_soft;     // its soft form (heating into profx_Qheat instead of T and p)
 };
 
@@ -172,6 +174,8 @@ void launch_profx(const Geometry& g, const Phys& P, const Sponge& sp, const Stat
                   cudaStream_t st);
 void launch_profx_finish(const Geometry& g, const State& s, cudaStream_t st);
 void launch_adv_temp(const Geometry& g, const Phys& P, const State& s, cudaStream_t st);
+// Vertical hyperdiffusion of one RK stage, added into diffmh, diffw and diffpr (P.vhd_order > 0).
+void launch_vertical_diff(const Geometry& g, const Phys& P, const State& s, cudaStream_t st);
 void launch_diffusion(const Geometry& g, const Phys& P, const State& s, int stepnum, bool last,
                       cudaStream_t st);
 void launch_divm0(const Geometry& g, const Phys& P, const State& s, bool small_step,

@@ -91,7 +91,7 @@ KEYS = {
     "Top_altitude": (float, 1235376.0, "path"),
     "Diffc": (float, 0.009973, "path"),
     "DivDampc": (float, 0.009973, "path"),
-    "Diffc_v": (float, 0.0, "ignored"),
+    "Diffc_v": (float, 0.0, "path"),
     "spring_dynamics": (bool, True, "path"),
     "glevel": (int, 4, "path"),
     "spring_beta": (float, 1.15, "path"),
@@ -99,8 +99,8 @@ KEYS = {
     "HyDiff": (bool, True, "path"),
     "HyDiffOrder": (int, 4, "path"),
     "DivDampP": (bool, True, "path"),
-    "VertHyDiff": (bool, False, "fixed"),
-    "VertHyDiffOrder": (int, 6, "ignored"),
+    "VertHyDiff": (bool, False, "path"),
+    "VertHyDiffOrder": (int, 6, "path"),
     "increased_damping_for_n_steps": (int, 0, "fixed"),
     "NonHydro": (bool, True, "path"),
     "DeepModel": (bool, True, "path"),
@@ -752,6 +752,8 @@ def run(argv=None, out=sys.stdout):
             x.conv_adj(c["conv_adj_iter"], c["soft_adjustment"])
         if c["RayleighSponge"]:
             x.sponge(sponge_config(c, step_idx))
+        if c["VertHyDiff"]:
+            x.vert_hydiff(c["Diffc_v"], c["VertHyDiffOrder"])
         nsmax = c["num_steps"]
         logs = Logs(out_dir, sim_id, continuing, c["globdiag"])
         write_grid(os.path.join(out_dir, "esp_output_grid_%s.h5" % sim_id), grid)
