@@ -139,10 +139,11 @@ int thorx_set_precision(thorx_ctx* ctx, int precision);
  * thorx_sync return THORX_E_CONVERGENCE. */
 int thorx_conv_adj_enable(thorx_ctx* ctx, int iterations, int soft_adjustment);
 
-/* ---- Rayleigh sponge layer at the top of the model (RayleighSponge with raysp_calc_mode = imp:
- * sponge_layer with its zonal means, src/ESP/profx_sponge.cu, run by ESP::ProfX at
- * src/ESP/profx_driver.cu:96-194; latitude bins of Icogrid::zonal_mean_tab_f,
- * src/ESP/grid.cu:3203-3260). The .thr keys of the same names. ---- */
+/* ---- Rayleigh sponge layer at the top of the model (RayleighSponge: sponge_layer with its zonal
+ * means, src/ESP/profx_sponge.cu, run by ESP::ProfX at src/ESP/profx_driver.cu:96-194 in the
+ * implicit mode and by ESP::Thor at src/ESP/thor_driver.cu:749-866 in the explicit ones; latitude
+ * bins of Icogrid::zonal_mean_tab_f, src/ESP/grid.cu:3203-3260). The .thr keys of the same
+ * names. ---- */
 typedef struct {
     int    nlat_bins;       /* latitude bins over which the zonal means are taken (>= 1)     */
     double Ruv_sponge;      /* damping rate of the horizontal wind at the top [1/s]          */
@@ -155,11 +156,15 @@ typedef struct {
     int    shrink_sponge;   /* weaken the sponge exponentially after t_shrink steps          */
     int    t_shrink;        /* steps after which the sponge shrinks                          */
     int    first_step;      /* step number of the next physics step (1 at a fresh start)     */
+    int    raysp_calc_mode; /* 0 imp: implicit, in ProfX; 1 exp1 / 2 exp3: explicit tendencies
+                               in every RK stage of Thor, zonal means from the first stage (exp1)
+                               or every stage (exp3) (src/ESP/thor_driver.cu:749-866)           */
 } thorx_sponge_params;
 
-/* Adds the implicit Rayleigh sponge to every following ProfX, between Recompute_W and the
- * temperature; NULL switches it off. A step graph captured earlier is re-captured.
- * THORX_E_ARG for nlat_bins < 1 or ns_ray_sponge outside [0, 1). */
+/* Adds the Rayleigh sponge to every following step: the implicit one in ProfX between Recompute_W
+ * and the temperature, the explicit ones before the slow modes of every RK stage; NULL switches it
+ * off. A step graph captured earlier is re-captured. THORX_E_ARG for nlat_bins < 1, ns_ray_sponge
+ * outside [0, 1) or an unknown raysp_calc_mode. */
 int thorx_sponge_enable(thorx_ctx* ctx, const thorx_sponge_params* sp);
 /* The zonal means of the last sponge step: vbar [bin][lev][3] (u, v, w; the reference's vbar_h;
  * zero where damp_*_to_mean is off) and Tbar [bin][lev] (zero without RayleighSpongeT); either

@@ -193,6 +193,7 @@ struct ref_sponge_params {
     int    nlat_bins;
     double Ruv_sponge, Rw_sponge, RT_sponge, ns_ray_sponge;
     int    damp_uv_to_mean, damp_w_to_mean, RayleighSpongeT, shrink_sponge, t_shrink, first_step;
+    int    raysp_calc_mode; // 0 IMP, 1 EXP1, 2 EXP3 (define.h:169)
 };
 
 struct RefSim {
@@ -527,6 +528,73 @@ extern "C" void ref_sim_sponge_means(void* h, double* vbar, double* Tbar) {
         std::memcpy(Tbar, s->Tbar_h, n * sizeof(double));
 }
 
+// The explicit sponge of one RK stage (raysp_calc_mode exp1 / exp3), thor_driver.cu:749-866.
+static int ref_sponge_explicit(RefSim* s, int rk) {
+    auto&      F   = s->f;
+    const int  NTH = 256;
+    const int  N = s->N, nv = s->nv, nvi = s->nvi, nlat_bins = s->S.nlat_bins;
+    const int  max_count = s->max_count;
+    const bool uvm = s->S.damp_uv_to_mean != 0, wm = s->S.damp_w_to_mean != 0;
+    dim3       NB((N / NTH) + 1, nv, 1);
+    dim3       NBRT((N / NTH) + 1, 1, 1);
+    REF_CHECK(cudaMemset(F["profx_dMh"], 0, sizeof(double) * 3 * N * nv));
+    REF_CHECK(cudaMemset(F["profx_dWh"], 0, sizeof(double) * N * nvi));
+    REF_CHECK(cudaMemset(F["profx_dW"], 0, sizeof(double) * N * nv));
+    if (rk == 0 || s->S.raysp_calc_mode == 2) {
+        if (uvm) {
+            REF_CHECK(cudaMemset(F["utmp"], 0, sizeof(double) * nlat_bins * nv * max_count));
+            REF_CHECK(cudaMemset(F["vtmp"], 0, sizeof(double) * nlat_bins * nv * max_count));
+            zonal_uv<<<NB, NTH>>>(F["Mhk"], F["Rhok"], s->zonal_mean_tab_d, F["lonlat"], N,
+                                  F["utmp"], F["vtmp"], max_count);
+            REF_CHECK(cudaDeviceSynchronize());
+        }
+        if (wm) {
+            REF_CHECK(cudaMemset(F["wtmp"], 0, sizeof(double) * nlat_bins * nv * max_count));
+            zonal_w<<<NB, NTH>>>(F["Wk"], F["Rhok"], s->zonal_mean_tab_d, N, F["wtmp"], max_count);
+            REF_CHECK(cudaDeviceSynchronize());
+        }
+        if (uvm) {
+            gpu_sum_on_device_sponge<1024>(F["utmp"], max_count, s->vbar_h, nv, nlat_bins, 0);
+            gpu_sum_on_device_sponge<1024>(F["vtmp"], max_count, s->vbar_h, nv, nlat_bins, 1);
+        }
+        if (wm)
+            gpu_sum_on_device_sponge<1024>(F["wtmp"], max_count, s->vbar_h, nv, nlat_bins, 2);
+        if (uvm || wm) {
+            REF_CHECK(cudaMemset(F["vbar"], 0, sizeof(double) * 3 * nlat_bins * nv));
+            REF_CHECK(cudaMemcpy(F["vbar"], s->vbar_h, 3 * nlat_bins * nv * sizeof(double),
+                                 cudaMemcpyHostToDevice));
+        }
+        if (s->S.RayleighSpongeT) {
+            zonal_temp<<<NB, NTH>>>(F["pressurek"], F["Rhok"], F["Tbar"], s->zonal_mean_tab_d,
+                                    F["lonlat"], N, F["Ttmp"], F["Rd"], max_count);
+            REF_CHECK(cudaDeviceSynchronize());
+            for (int ilat = 0; ilat < nlat_bins; ilat++)
+                for (int lev = 0; lev < nv; lev++)
+                    s->Tbar_h[ilat * nv + lev] = gpu_sum_on_device<1024>(
+                        &(F["Ttmp"][ilat * nv * max_count + lev * max_count]), max_count);
+            REF_CHECK(cudaMemcpy(F["Tbar"], s->Tbar_h, nlat_bins * nv * sizeof(double),
+                                 cudaMemcpyHostToDevice));
+        }
+    }
+    const double timestep = s->p.timestep;
+    const int    current_step = s->sp_step;
+    double       Rv_fac = 1;
+    if (s->S.shrink_sponge) {
+        if (current_step * timestep >= s->S.t_shrink * timestep) {
+            double shrink_scale = timestep * 1000;
+            Rv_fac = exp(-(current_step * timestep - s->S.t_shrink * timestep) / shrink_scale);
+        }
+    }
+    sponge_layer<<<NBRT, NTH>>>(F["Mhk"], F["Rhok"], F["Wk"], F["Whk"], F["pressurek"], F["vbar"],
+                                F["Tbar"], s->zonal_mean_tab_d, F["lonlat"], F["Altitude"],
+                                F["Altitudeh"], s->S.Ruv_sponge, s->S.Rw_sponge, s->S.RT_sponge,
+                                Rv_fac, s->S.ns_ray_sponge, uvm, wm, false, timestep, F["Rd"],
+                                nlat_bins, N, nv, s->S.RayleighSpongeT != 0, F["profx_dMh"],
+                                F["profx_dWh"], F["profx_dW"], F["profx_Qheat"]);
+    REF_CHECK(cudaDeviceSynchronize());
+    return 0;
+}
+
 static int ref_sponge_step(RefSim* s) {
     auto&      F   = s->f;
     const int  NTH = 256;
@@ -713,7 +781,7 @@ static int ref_profx(RefSim* s) {
     REF_CHECK(cudaMemset(F["profx_Qheat"], 0, sizeof(double) * N * nv));
     Recompute_W<<<NB, NTH>>>(F["W"], F["Wh"], F["Altitude"], F["Altitudeh"], N);
     REF_CHECK(cudaDeviceSynchronize());
-    if (s->sponge && ref_sponge_step(s))
+    if (s->sponge && s->S.raysp_calc_mode == 0 && ref_sponge_step(s))
         return -1;
     Compute_temperature<<<NB, NTH>>>(F["temperature"], F["pt"], F["pressure"], F["Rho"],
                                      s->p.P_Ref, F["Rd"], F["Cp"], N, true);
@@ -892,6 +960,8 @@ static int ref_thor(RefSim* s) {
             }
         }
         REF_CHECK(cudaDeviceSynchronize());
+        if (s->sponge && s->S.raysp_calc_mode != 0 && ref_sponge_explicit(s, rk))
+            return -1;
         Compute_Slow_Modes<LN, LN><<<NB, NT>>>(
             F["SlowMh"], F["SlowWh"], F["SlowRho"], F["Slowpressure"], F["Mhk"], F["Whk"],
             F["Rhok"], F["Adv"], F["DivM"], F["diffmh"], F["diffw"], F["diffrh"], F["diffpr"],
@@ -992,6 +1062,8 @@ static int ref_thor(RefSim* s) {
     cudaMemcpy(F["pressure"], F["pressurek"], N * nv * 8, cudaMemcpyDeviceToDevice);
     if (s->probe)
         probe_end(s);
+    if (s->sponge && s->S.raysp_calc_mode != 0)
+        s->sp_step++; // the explicit sponge's step number moves on with the large step
     REF_CHECK(cudaDeviceSynchronize());
     return 0;
 }

@@ -67,6 +67,7 @@ struct Oracle {
     bool                 sponge = false;
     oracle_sponge_params S{};
     long long            sp_nstep = 1;
+    double               sp_rv    = 1; // the explicit sponge's step factor of the current step
     std::vector<int>     sp_bin, sp_start, sp_members; // bins, then members bin by bin
     Vec                  vbar, Tbar;                     // [bin][lev][3], [bin][lev]
 };
@@ -717,10 +718,9 @@ inline void wind_uv(const Oracle& o, const Vec& Mh, int id, int lev, double rho,
 // after the zonal means of zonal_uv / zonal_w / zonal_temp (:50-130) and the step factor of
 // profx_driver.cu:154-160. The means are sums of x / count over a bin's members in member order
 // (the reference sums the same terms in a block tree: the results differ by rounding only).
-void sponge(Oracle& o) {
-    const int nlat = o.S.nlat_bins, nv = o.nv, nvi = o.nvi, N = o.N;
-    Vec &     Mh = F(o, "Mh"), &W = F(o, "W"), &Wh = F(o, "Wh"), &Rho = F(o, "Rho"),
-        &p = F(o, "pressure"), &Rd = F(o, "Rd");
+void sponge_means(Oracle& o, const Vec& Mh, const Vec& W, const Vec& Rho, const Vec& p) {
+    const int  nlat = o.S.nlat_bins, nv = o.nv;
+    const Vec& Rd   = F(o, "Rd");
     const bool uvm = o.S.damp_uv_to_mean, wm = o.S.damp_w_to_mean, tsp = o.S.RayleighSpongeT;
     if (uvm || wm || tsp) {
 #pragma omp parallel for schedule(static)
@@ -748,6 +748,37 @@ void sponge(Oracle& o) {
             o.Tbar[b * nv + lev]           = tsp ? sT : 0.0;
         }
     }
+}
+
+// The mean of table tab (stride st, component k) at a column's latitude (sponge_layer,
+// src/ESP/profx_sponge.cu:196-286); a latitude outside both half-intervals of its bin takes the
+// bin's own mean.
+double sponge_mean(const Oracle& o, int id, const Vec& tab, int st, int k, int lev) {
+    const int    nlat = o.S.nlat_bins, nv = o.nv, intlat = o.sp_bin[id];
+    const double des_lat = M_PI / nlat;
+    const double lat1    = -M_PI / 2 + 0.5 * des_lat + des_lat * (intlat - 1);
+    const double lat2    = -M_PI / 2 + 0.5 * des_lat + des_lat * (intlat);
+    const double lat3    = -M_PI / 2 + 0.5 * des_lat + des_lat * (intlat + 1);
+    const double lat     = o.lonlat[id * 2 + 1];
+    if (lat <= -M_PI / 2 + 0.5 * des_lat)
+        return tab[(intlat * nv + lev) * st + k];
+    if (lat >= -M_PI / 2 + 0.5 * des_lat + des_lat * (nlat - 1))
+        return tab[(intlat * nv + lev) * st + k];
+    if (lat >= lat1 && lat < lat2) {
+        double intt = (lat - lat2) / (lat1 - lat2);
+        double intl = (lat - lat1) / (lat2 - lat1);
+        return tab[((intlat - 1) * nv + lev) * st + k] * intt + tab[(intlat * nv + lev) * st + k] * intl;
+    }
+    if (lat >= lat2 && lat < lat3) {
+        double intt = (lat - lat3) / (lat2 - lat3);
+        double intl = (lat - lat2) / (lat3 - lat2);
+        return tab[(intlat * nv + lev) * st + k] * intt + tab[((intlat + 1) * nv + lev) * st + k] * intl;
+    }
+    return tab[(intlat * nv + lev) * st + k];
+}
+
+// The step factor of profx_driver.cu:154-160 / thor_driver.cu:822-828 for the step starting now.
+double sponge_rv(Oracle& o) {
     const double dt = o.P.timestep;
     double       Rv_fac = 1;
     if (o.S.shrink_sponge) {
@@ -757,7 +788,93 @@ void sponge(Oracle& o) {
         }
     }
     o.sp_nstep++;
+    return Rv_fac;
+}
+
+// The explicit sponge of one RK stage (raysp_calc_mode exp1 / exp3, thor_driver.cu:749-866;
+// sponge_layer with implicit = false): tendencies into profx_dMh and profx_dWh (zeroed first),
+// heating added to profx_Qheat.
+void sponge_explicit(Oracle& o, int rk) {
+    const int nv = o.nv, nvi = o.nvi, N = o.N;
+    Vec &Mh = F(o, "Mhk"), &W = F(o, "Wk"), &Rho = F(o, "Rhok"), &p = F(o, "pressurek"),
+        &Rd = F(o, "Rd"), &dMh = F(o, "profx_dMh"), &dWh = F(o, "profx_dWh"), &Q = F(o, "profx_Qheat");
+    std::fill(dMh.begin(), dMh.end(), 0.0);
+    std::fill(dWh.begin(), dWh.end(), 0.0);
+    if (rk == 0 || o.S.raysp_calc_mode == 2)
+        sponge_means(o, Mh, W, Rho, p);
+    if (rk == 0)
+        o.sp_rv = sponge_rv(o);
+    const double Rv_fac = o.sp_rv;
+    const bool   uvm = o.S.damp_uv_to_mean, wm = o.S.damp_w_to_mean, tsp = o.S.RayleighSpongeT;
     const double ns = o.S.ns_ray_sponge, ztop = o.Altitudeh[nv];
+#pragma omp parallel for schedule(static)
+    for (int id = 0; id < N; id++) {
+        double lon;
+        if (o.lonlat[id * 2] < 0)
+            lon = o.lonlat[id * 2] + 2.0 * M_PI;
+        else
+            lon = o.lonlat[id * 2];
+        const double lat = o.lonlat[id * 2 + 1];
+        std::vector<double> dW(nv);
+        for (int lev = 0; lev < nv; lev++) {
+            const double rho = Rho[id * nv + lev];
+            double       u, v;
+            wind_uv(o, Mh, id, lev, rho, u, v);
+            const double w = W[id * nv + lev] / rho;
+            const double n = o.Altitude[lev] / ztop;
+            double       kuv = 0.0, kw = 0.0;
+            if (n >= ns) {
+                kuv = Rv_fac * o.S.Ruv_sponge * pow(sin(0.5 * M_PI * (n - ns) * (1.0) / (1.0 - ns)), 2.0);
+                kw  = Rv_fac * o.S.Rw_sponge * pow(sin(0.5 * M_PI * (n - ns) * (1.0) / (1.0 - ns)), 2.0);
+            }
+            double du, dv, dw;
+            if (uvm) {
+                du = -kuv * (u - sponge_mean(o, id, o.vbar, 3, 0, lev));
+                dv = -kuv * (v - sponge_mean(o, id, o.vbar, 3, 1, lev));
+            }
+            else {
+                du = -kuv * u;
+                dv = -kuv * v;
+            }
+            double vx = du * (-sin(lon)) + dv * (-sin(lat) * cos(lon));
+            double vy = du * (cos(lon)) + dv * (-sin(lat) * sin(lon));
+            double vz = dv * (cos(lat));
+            dMh[(id * nv + lev) * 3 + 0] += vx * rho;
+            dMh[(id * nv + lev) * 3 + 1] += vy * rho;
+            dMh[(id * nv + lev) * 3 + 2] += vz * rho;
+            if (wm)
+                dw = -kw * (w - sponge_mean(o, id, o.vbar, 3, 2, lev));
+            else
+                dw = -kw * (w);
+            dW[lev] = 0.0 + dw * rho;
+            if (tsp) {
+                double kvT = n >= ns ? Rv_fac * o.S.RT_sponge
+                                           * pow(sin(0.5 * M_PI * (n - ns) * (1.0) / (1.0 - ns)), 2.0)
+                                     : 0.0;
+                double temperature = p[id * nv + lev] / Rd[id * nv + lev] / Rho[id * nv + lev];
+                double dT          = -kvT * (temperature - sponge_mean(o, id, o.Tbar, 1, 0, lev));
+                Q[id * nv + lev] += Rd[id * nv + lev] * Rho[id * nv + lev] * dT;
+            }
+        }
+        for (int lev = 1; lev < nv; lev++) {
+            double xi = o.Altitudeh[lev], xim = o.Altitude[lev - 1], xip = o.Altitude[lev];
+            double intt = (xi - xip) / (xim - xip);
+            double intl = (xi - xim) / (xip - xim);
+            dWh[id * nvi + lev] = dW[lev - 1] * intt + dW[lev] * intl;
+        }
+    }
+}
+
+void sponge(Oracle& o) {
+    const int nlat = o.S.nlat_bins, nv = o.nv, nvi = o.nvi, N = o.N;
+    Vec &     Mh = F(o, "Mh"), &W = F(o, "W"), &Wh = F(o, "Wh"), &Rho = F(o, "Rho"),
+        &p = F(o, "pressure"), &Rd = F(o, "Rd");
+    const bool uvm = o.S.damp_uv_to_mean, wm = o.S.damp_w_to_mean, tsp = o.S.RayleighSpongeT;
+    sponge_means(o, Mh, W, Rho, p);
+    const double dt = o.P.timestep;
+    const double Rv_fac = sponge_rv(o);
+    const double ns = o.S.ns_ray_sponge, ztop = o.Altitudeh[nv];
+    (void)nlat;
 #pragma omp parallel for schedule(static)
     for (int id = 0; id < N; id++) {
         const int    intlat  = o.sp_bin[id];
@@ -849,7 +966,7 @@ void sponge(Oracle& o) {
 void profx(Oracle& o) {
     std::fill(F(o, "profx_Qheat").begin(), F(o, "profx_Qheat").end(), 0.0);
     recompute_w(o);
-    if (o.sponge)
+    if (o.sponge && o.S.raysp_calc_mode == 0)
         sponge(o);
     compute_temperature(o);
     if (o.conv_adj_iter > 0)
@@ -2125,6 +2242,8 @@ void thor(Oracle& o) {
             divm_pass(o, F(o, "Mhk"), F(o, "Whk"), false);
             divm_pass(o, F(o, "Mhk"), F(o, "Whk"), true);
         }
+        if (o.sponge && o.S.raysp_calc_mode != 0)
+            sponge_explicit(o, rk);
         slow_modes(o);
         if (rk > 0)
             update_rk(o);

@@ -57,6 +57,7 @@ typedef struct {
     int    nlat_bins;
     double Ruv_sponge, Rw_sponge, RT_sponge, ns_ray_sponge;
     int    damp_uv_to_mean, damp_w_to_mean, RayleighSpongeT, shrink_sponge, t_shrink, first_step;
+    int    raysp_calc_mode; // 0 imp (ProfX), 1 exp1, 2 exp3 (explicit, in the dynamical core)
 } oracle_sponge_params;
 // Enables the sponge (NULL: off). Returns 0.
 int oracle_sponge(void* h, const oracle_sponge_params* sp);

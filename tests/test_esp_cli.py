@@ -90,7 +90,6 @@ def test_bad_lines_fail_the_file(line):
 
 @pytest.mark.parametrize("line,what", [
     ("DiffSponge = true", "DiffSponge"),
-    ("RayleighSponge = true\nraysp_calc_mode = exp3", "raysp_calc_mode"),
     ("RayleighSponge = true\nraysp_calc_mode = implicit", "raysp_calc_mode"),
     ("RayleighSponge = true\nns_ray_sponge = 1.0", "ns_ray_sponge"),
     ("conv_adj_type = rayph", "conv_adj_type"),

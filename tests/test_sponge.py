@@ -167,6 +167,13 @@ CASES = {
     # the sponge at exp(-2) of its strength and weakening from step to step
     "shrinking": dict(nlat_bins=NLAT, shrink_sponge=1, t_shrink=1000, first_step=3000,
                       RayleighSpongeT=1, Ruv_sponge=1e-2, Rw_sponge=1e-2, RT_sponge=1e-2),
+    # the explicit modes: tendencies in every RK stage of the dynamical core, means from the
+    # first stage (exp1) or every stage (exp3)
+    "exp1": dict(nlat_bins=NLAT, raysp_calc_mode=1, ns_ray_sponge=0.5, Ruv_sponge=1e-3,
+                 Rw_sponge=1e-3),
+    "exp3_thermal_shrinking": dict(nlat_bins=NLAT, raysp_calc_mode=2, RayleighSpongeT=1,
+                                   shrink_sponge=1, t_shrink=1000, first_step=3000,
+                                   Ruv_sponge=1e-2, Rw_sponge=1e-2, RT_sponge=1e-2),
 }
 
 
@@ -175,7 +182,7 @@ CASES = {
 @pytest.mark.parametrize("case,nsteps,thor", [
     ("defaults", 1, False), ("to_zero", 1, False), ("thermal", 1, False),
     ("bins7_w_only", 1, False), ("shrinking", 2, False), ("defaults", 3, True),
-    ("thermal", 3, True)])
+    ("thermal", 3, True), ("exp1", 2, True), ("exp3_thermal_shrinking", 2, True)])
 def test_sponge_matches_reference(who, case, nsteps, thor):
     d = CASES[case]
     ref = run("reference", d, nsteps, thor)

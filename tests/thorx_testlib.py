@@ -97,11 +97,12 @@ SPONGE_FIELDS = [("nlat_bins", ctypes.c_int), ("Ruv_sponge", ctypes.c_double),
                  ("ns_ray_sponge", ctypes.c_double), ("damp_uv_to_mean", ctypes.c_int),
                  ("damp_w_to_mean", ctypes.c_int), ("RayleighSpongeT", ctypes.c_int),
                  ("shrink_sponge", ctypes.c_int), ("t_shrink", ctypes.c_int),
-                 ("first_step", ctypes.c_int)]
+                 ("first_step", ctypes.c_int), ("raysp_calc_mode", ctypes.c_int)]
 # the reference's defaults, src/headers/define.h:59-78
 SPONGE_DEFAULTS = dict(nlat_bins=20, Ruv_sponge=1e-4, Rw_sponge=1e-4, RT_sponge=1e-4,
                        ns_ray_sponge=0.75, damp_uv_to_mean=1, damp_w_to_mean=1,
-                       RayleighSpongeT=0, shrink_sponge=0, t_shrink=144000, first_step=1)
+                       RayleighSpongeT=0, shrink_sponge=0, t_shrink=144000, first_step=1,
+                       raysp_calc_mode=0)
 
 
 class SpongeParams(ctypes.Structure):

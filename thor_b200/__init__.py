@@ -62,7 +62,7 @@ SPONGE_FIELDS = [("nlat_bins", ctypes.c_int), ("Ruv_sponge", ctypes.c_double),
                  ("ns_ray_sponge", ctypes.c_double), ("damp_uv_to_mean", ctypes.c_int),
                  ("damp_w_to_mean", ctypes.c_int), ("RayleighSpongeT", ctypes.c_int),
                  ("shrink_sponge", ctypes.c_int), ("t_shrink", ctypes.c_int),
-                 ("first_step", ctypes.c_int)]
+                 ("first_step", ctypes.c_int), ("raysp_calc_mode", ctypes.c_int)]
 
 
 class SpongeParamsC(ctypes.Structure):
@@ -74,7 +74,7 @@ def sponge_params(d):
     (src/headers/define.h:59-78)."""
     v = dict(nlat_bins=20, Ruv_sponge=1e-4, Rw_sponge=1e-4, RT_sponge=1e-4, ns_ray_sponge=0.75,
              damp_uv_to_mean=1, damp_w_to_mean=1, RayleighSpongeT=0, shrink_sponge=0,
-             t_shrink=144000, first_step=1)
+             t_shrink=144000, first_step=1, raysp_calc_mode=0)
     v.update(d)
     return SpongeParamsC(*[float(v[n]) if t is ctypes.c_double else int(v[n])
                            for n, t in SPONGE_FIELDS])

@@ -384,9 +384,9 @@ __global__ void sponge_trig_kernel(Geometry g, double* trig) {
 }
 
 __global__ void __launch_bounds__(kSpongeThreads) sponge_means_kernel(Geometry g, Phys P,
-                                                                      Sponge sp, State s) {
+                                                                      Sponge sp, SpongeIn in) {
     const int b = blockIdx.x, lev = blockIdx.y;
-    if (b == 0 && lev == 0 && threadIdx.x == 0) { // step factor (profx_driver.cu:154-160)
+    if (in.advance && b == 0 && lev == 0 && threadIdx.x == 0) { // step factor (profx_driver.cu:154-160)
         const long long n  = sp.step->nstep;
         const double    dt = P.timestep;
         double          rv = 1;
@@ -411,22 +411,23 @@ __global__ void __launch_bounds__(kSpongeThreads) sponge_means_kernel(Geometry g
     for (int m = m0 + threadIdx.x; m < m1; m += kSpongeThreads) {
         const int    c   = sp.members[m];
         const int    i   = lev * Np + c;
-        const double rho = s.Rho[i];
+        const double rho = in.Rho[i];
         if (sp.uv_mean) {
             const double slon = sp.trig[c], clon = sp.trig[Np + c];
             const double slat = sp.trig[2 * Np + c], clat = sp.trig[3 * Np + c];
-            const double mx = s.Mh[i], my = s.Mh[nv * Np + i], mz = s.Mh[2 * nv * Np + i];
+            const double mx = in.M[i], my = in.M[nv * Np + i], mz = in.M[2 * nv * Np + i];
             const double u = (mx * (-slon) + my * (clon) + mz * 0) / rho;
             const double v = (mx * (-slat * clon) + my * (-slat * slon) + mz * (clat)) / rho;
             acc[0] += u / cnt;
             acc[1] += v / cnt;
         }
         if (sp.w_mean) {
-            const double w = s.Wh[lev * Np + c] * intt + s.Wh[(lev + 1) * Np + c] * intl;
+            const double w = in.W ? in.W[i]
+                                  : in.Wh[lev * Np + c] * intt + in.Wh[(lev + 1) * Np + c] * intl;
             acc[2] += (w / rho) / cnt;
         }
         if (sp.temp)
-            acc[3] += s.p[i] / s.Rd[i] / rho / cnt;
+            acc[3] += in.p[i] / in.Rd[i] / rho / cnt;
     }
     __shared__ double red[kSpongeThreads / 32][4];
     const int         lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -455,16 +456,16 @@ __global__ void __launch_bounds__(kSpongeThreads) sponge_means_kernel(Geometry g
 // (interpolated between the two nearest bin centres; the polar halves of the outermost bins take
 // their bin's mean), with the rate Rv_fac R sin^2(pi/2 (z/ztop - ns) / (1 - ns)) above ns; then
 // Wh at the interior interfaces from the new W; with the thermal sponge, p from the relaxed T.
-__device__ void sponge_column(const Geometry& g, const Phys& P, const Sponge& sp, const State& s,
-                              int c) {
-    const int     Np = g.Np, nv = g.nv, nlat = sp.nlat;
-    const double* Alt  = g.Altitude;
-    const double* Alth = g.Altitudeh;
-    const double  ztop = Alth[nv];
-    const double  dt   = P.timestep;
-    const double  rv   = sp.step->rv_fac;
-    const double  slon = sp.trig[c], clon = sp.trig[Np + c];
-    const double  slat = sp.trig[2 * Np + c], clat = sp.trig[3 * Np + c];
+struct SpongeLat { // the means at a column's latitude: bin b's, or wa x bin ba + wb x bin bb
+    bool   interp;
+    int    b, ba, bb;
+    double wa, wb;
+    __device__ double mean(const double* tab, int nv, int lev) const {
+        return interp ? tab[ba * nv + lev] * wa + tab[bb * nv + lev] * wb : tab[b * nv + lev];
+    }
+};
+__device__ SpongeLat sponge_lat(const Geometry& g, const Sponge& sp, int c) {
+    const int     nlat    = sp.nlat;
     const int     b       = sp.bin[c];
     const double  des_lat = M_PI / nlat;
     const double  lat1    = -M_PI / 2 + 0.5 * des_lat + des_lat * (b - 1);
@@ -493,9 +494,21 @@ __device__ void sponge_column(const Geometry& g, const Phys& P, const Sponge& sp
         wa = (lat - lat3) / (lat2 - lat3);
         wb = (lat - lat2) / (lat3 - lat2);
     }
-    auto mean = [&](const double* tab, int lev) {
-        return interp ? tab[ba * nv + lev] * wa + tab[bb * nv + lev] * wb : tab[b * nv + lev];
-    };
+    return SpongeLat{interp, b, ba, bb, wa, wb};
+}
+
+__device__ void sponge_column(const Geometry& g, const Phys& P, const Sponge& sp, const State& s,
+                              int c) {
+    const int       Np = g.Np, nv = g.nv, nlat = sp.nlat;
+    const double*   Alt  = g.Altitude;
+    const double*   Alth = g.Altitudeh;
+    const double    ztop = Alth[nv];
+    const double    dt   = P.timestep;
+    const double    rv   = sp.step->rv_fac;
+    const double    slon = sp.trig[c], clon = sp.trig[Np + c];
+    const double    slat = sp.trig[2 * Np + c], clat = sp.trig[3 * Np + c];
+    const SpongeLat L    = sponge_lat(g, sp, c);
+    auto            mean = [&](const double* tab, int lev) { return L.mean(tab, nv, lev); };
     const double* ubar = sp.vbar;
     const double* vbar = sp.vbar + nlat * nv;
     const double* wbar = sp.vbar + 2 * nlat * nv;
@@ -543,6 +556,77 @@ __device__ void sponge_column(const Geometry& g, const Phys& P, const Sponge& sp
     for (int lev = 1; lev < nv; lev++) {
         const double intt = g.lt[kLtHIntt * nvi + lev], intl = g.lt[kLtHIntl * nvi + lev];
         s.Wh[lev * Np + c] = s.W[(lev - 1) * Np + c] * intt + s.W[lev * Np + c] * intl;
+    }
+}
+
+// The explicit sponge (sponge_layer with implicit = false, raysp_calc_mode exp1 / exp3,
+// src/ESP/thor_driver.cu:749-866) on the RK stage's fields: the damping rates become tendencies,
+// profx_dMh (horizontal momentum), profx_dWh (the vertical one, interpolated to the interior
+// interfaces; zero at the bottom and the top) and, with the thermal sponge, heating added to
+// profx_Qheat (which the reference does not reset between RK stages either). One thread per column.
+__global__ void __launch_bounds__(kColBlock) sponge_explicit_kernel(Geometry g, Phys P, Sponge sp,
+                                                                   State s) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= g.N)
+        return;
+    const int       Np = g.Np, nv = g.nv, nvi = g.nvi;
+    const double*   Alt  = g.Altitude;
+    const double    ztop = g.Altitudeh[nv];
+    const double    rv   = sp.step->rv_fac;
+    const double    slon = sp.trig[c], clon = sp.trig[Np + c];
+    const double    slat = sp.trig[2 * Np + c], clat = sp.trig[3 * Np + c];
+    const SpongeLat L    = sponge_lat(g, sp, c);
+    const double*   ubar = sp.vbar;
+    const double*   vbar = sp.vbar + sp.nlat * nv;
+    const double*   wbar = sp.vbar + 2 * sp.nlat * nv;
+    double          dw_prev = 0.0;
+    s.dWh[c]                = 0.0;
+    s.dWh[nv * Np + c]      = 0.0;
+    for (int lev = 0; lev < nv; lev++) {
+        const int    i   = lev * Np + c;
+        const double rho = s.Rhok[i];
+        const double mx = s.Mhk[i], my = s.Mhk[nv * Np + i], mz = s.Mhk[2 * nv * Np + i];
+        const double u = (mx * (-slon) + my * (clon) + mz * 0) / rho;
+        const double v = (mx * (-slat * clon) + my * (-slat * slon) + mz * (clat)) / rho;
+        const double w = s.Wk[i] / rho;
+        const double n = Alt[lev] / ztop;
+        double       kuv = 0.0, kw = 0.0, kvT = 0.0;
+        if (n >= sp.ns) {
+            const double sn = pow(sin(0.5 * M_PI * (n - sp.ns) * (1.0) / (1.0 - sp.ns)), 2.0);
+            kuv             = rv * sp.Ruv * sn;
+            kw              = rv * sp.Rw * sn;
+            kvT             = rv * sp.RT * sn;
+        }
+        double du, dv, dw;
+        if (sp.uv_mean) {
+            du = -kuv * (u - L.mean(ubar, nv, lev));
+            dv = -kuv * (v - L.mean(vbar, nv, lev));
+        }
+        else {
+            du = -kuv * u;
+            dv = -kuv * v;
+        }
+        const double vx = du * (-slon) + dv * (-slat * clon);
+        const double vy = du * (clon) + dv * (-slat * slon);
+        const double vz = dv * (clat);
+        s.dMh[i]              = vx * rho;
+        s.dMh[nv * Np + i]     = vy * rho;
+        s.dMh[2 * nv * Np + i] = vz * rho;
+        if (sp.w_mean)
+            dw = -kw * (w - L.mean(wbar, nv, lev));
+        else
+            dw = -kw * (w);
+        const double dW = dw * rho;
+        if (lev > 0) {
+            const double intt = g.lt[kLtHIntt * nvi + lev], intl = g.lt[kLtHIntl * nvi + lev];
+            s.dWh[lev * Np + c] = dw_prev * intt + dW * intl;
+        }
+        dw_prev = dW;
+        if (sp.temp) {
+            const double temperature = s.pk[i] / s.Rd[i] / s.Rhok[i];
+            const double dT          = -kvT * (temperature - L.mean(sp.Tbar, nv, lev));
+            s.Qheat[i] += s.Rd[i] * s.Rhok[i] * dT;
+        }
     }
 }
 
@@ -2424,9 +2508,13 @@ void launch_stencil_weights(const Geometry& g, double* lapw, float* dmw, cudaStr
 void launch_sponge_trig(const Geometry& g, double* trig, cudaStream_t st) {
     sponge_trig_kernel<<<(g.N + kColBlock - 1) / kColBlock, kColBlock, 0, st>>>(g, trig);
 }
-void launch_sponge_means(const Geometry& g, const Phys& P, const Sponge& sp, const State& s,
+void launch_sponge_means(const Geometry& g, const Phys& P, const Sponge& sp, const SpongeIn& in,
                          cudaStream_t st) {
-    sponge_means_kernel<<<dim3(sp.nlat, g.nv), kSpongeThreads, 0, st>>>(g, P, sp, s);
+    sponge_means_kernel<<<dim3(sp.nlat, g.nv), kSpongeThreads, 0, st>>>(g, P, sp, in);
+}
+void launch_sponge_explicit(const Geometry& g, const Phys& P, const Sponge& sp, const State& s,
+                            cudaStream_t st) {
+    sponge_explicit_kernel<<<(g.N + kColBlock - 1) / kColBlock, kColBlock, 0, st>>>(g, P, sp, s);
 }
 void launch_profx(const Geometry& g, const Phys& P, const Sponge& sp, const State& s, bool finish,
                   cudaStream_t st) {

@@ -362,7 +362,8 @@ int class_launches(const thorx_ctx* ctx, int k) {
         return ctx->rt_enabled || has_phy_loop(ctx) ? 2 : 1;
     case KRt: return ctx->rt_enabled ? 1 : 0;     // one bracket: orbit kernel + column kernel
     case KSurrogate: return (ctx->sur && ctx->sur_mode == THORX_SUR_USE) ? 1 : 0;
-    case KSponge: return ctx->sp.nlat ? 1 : 0;
+    case KSponge: // ProfX's means, or per RK stage the explicit sponge (and, exp3, its means)
+        return !ctx->sp.nlat ? 0 : ctx->sp.mode == 0 ? 1 : ctx->sp.mode == 1 ? 4 : 6;
     case KVertDiff: return (P.HyDiff && P.vhd_order) ? 3 : 0;
     case KAdvTemp: return 3;
     case KDiffFirst: return 3 * (passes - (passes > 0 ? 1 : 0));
@@ -379,18 +380,23 @@ int class_launches(const thorx_ctx* ctx, int k) {
 // ESP::ProfX
 int enqueue_profx(thorx_ctx* ctx) {
     CK(cudaMemsetAsync(ctx->s.Qheat, 0, sizeof(double) * ctx->g.nv * ctx->g.Np, ctx->stream));
-    if (ctx->sp.nlat > 0) {
+    Sponge sp = ctx->sp; // the implicit sponge runs in ProfX, the explicit ones in Thor
+    if (sp.mode != 0)
+        sp.nlat = 0;
+    if (sp.nlat > 0) {
         KScope k(ctx, KSponge);
-        launch_sponge_means(ctx->g, ctx->P, ctx->sp, ctx->s, ctx->stream);
+        const State& s = ctx->s;
+        launch_sponge_means(ctx->g, ctx->P, sp, SpongeIn{s.Mh, s.Rho, nullptr, s.Wh, s.p, s.Rd, true},
+                            ctx->stream);
     }
     if (!ctx->rt_enabled && !has_phy_loop(ctx)) {
         KScope k(ctx, KProfx);
-        launch_profx(ctx->g, ctx->P, ctx->sp, ctx->s, true, ctx->stream);
+        launch_profx(ctx->g, ctx->P, sp, ctx->s, true, ctx->stream);
     }
     else { // the physics modules run before Compute_pressure (profx_driver.cu:405-432)
         {
             KScope k(ctx, KProfx);
-            launch_profx(ctx->g, ctx->P, ctx->sp, ctx->s, false, ctx->stream);
+            launch_profx(ctx->g, ctx->P, sp, ctx->s, false, ctx->stream);
         }
         if (!ctx->rt_enabled) {
         }
@@ -466,6 +472,13 @@ int enqueue_thor(thorx_ctx* ctx) {
         if (P.DivDampP) {
             KScope k(ctx, KDivm0);
             launch_divm0(g, P, s, false, st);
+        }
+        if (ctx->sp.nlat > 0 && ctx->sp.mode != 0) { // thor_driver.cu:749-866
+            KScope k(ctx, KSponge);
+            if (rk == 0 || ctx->sp.mode == 2)
+                launch_sponge_means(g, P, ctx->sp,
+                                    SpongeIn{s.Mhk, s.Rhok, s.Wk, nullptr, s.pk, s.Rd, rk == 0}, st);
+            launch_sponge_explicit(g, P, ctx->sp, s, st);
         }
         {
             KScope k(ctx, KSlow);
@@ -1318,6 +1331,8 @@ int thorx_sponge_enable(thorx_ctx* ctx, const thorx_sponge_params* p) {
             return fail(ctx, THORX_E_ARG, "thorx_sponge_enable: nlat_bins must be >= 1");
         if (!(p->ns_ray_sponge >= 0.0 && p->ns_ray_sponge < 1.0))
             return fail(ctx, THORX_E_ARG, "thorx_sponge_enable: ns_ray_sponge outside [0, 1)");
+        if (p->raysp_calc_mode < 0 || p->raysp_calc_mode > 2)
+            return fail(ctx, THORX_E_ARG, "thorx_sponge_enable: raysp_calc_mode not 0, 1 or 2");
         const int N = g.N, Np = g.Np, nv = g.nv, nlat = p->nlat_bins;
         // latitude bins as Icogrid::zonal_mean_tab_f (src/ESP/grid.cu:3203-3260): bin j holds
         // lat_array[j] <= lat < lat_array[j + 1], the edges accumulated from -pi/2 in steps of
@@ -1374,6 +1389,7 @@ int thorx_sponge_enable(thorx_ctx* ctx, const thorx_sponge_params* p) {
         sp.temp     = p->RayleighSpongeT != 0;
         sp.shrink   = p->shrink_sponge != 0;
         sp.t_shrink = p->t_shrink;
+        sp.mode     = p->raysp_calc_mode;
         sp.bin      = dbin;
         sp.start    = dstart;
         sp.members  = dmem;
@@ -1384,6 +1400,9 @@ int thorx_sponge_enable(thorx_ctx* ctx, const thorx_sponge_params* p) {
     }
     else
         ctx->sp.nlat = 0;
+    // an explicit sponge leaves its tendencies in profx_dMh / profx_dWh: start from zero
+    CK(cudaMemset(ctx->s.dMh, 0, sizeof(double) * 3 * g.nv * g.Np));
+    CK(cudaMemset(ctx->s.dWh, 0, sizeof(double) * g.nvi * g.Np));
     if (ctx->graph_exec) { // the captured step holds the previous set-up
         CK(cudaGraphExecDestroy(ctx->graph_exec));
         ctx->graph_exec = nullptr;

@@ -151,6 +151,7 @@ struct Sponge {
     bool          uv_mean, w_mean; // damp toward the zonal mean (else toward zero)
     bool          temp;            // thermal sponge (RayleighSpongeT)
     bool          shrink;          // shrink_sponge
+    int           mode;            // raysp_calc_mode: 0 imp (in ProfX), 1 exp1, 2 exp3 (in Thor)
     long long     t_shrink;        // steps after which the sponge shrinks
     const int*    bin;             // [Np] latitude bin of each column
     const int*    start;           // [nlat + 1] first entry of each bin in members
@@ -161,11 +162,21 @@ struct Sponge {
     SpongeStep*   step;
 };
 
+// What the sponge's zonal means read: the step's fields (ProfX: Mh, Rho, Wh interpolated to the
+// centres, p) or the RK stage's (explicit modes: Mhk, Rhok, Wk, pk); advance: this call starts a
+// step (the step counter and the shrink factor move on).
+struct SpongeIn {
+    const double *M, *Rho, *W, *Wh, *p, *Rd;
+    bool          advance;
+};
+
 // Kernel launchers (thor_b200/csrc/dyn_fp64.cu).
-// The sponge's zonal means and step factor, before launch_profx (sp.nlat > 0 only); and the
-// per-column trigonometric table it uses, once at set-up.
-void launch_sponge_means(const Geometry& g, const Phys& P, const Sponge& sp, const State& s,
+// The sponge's zonal means and step factor (sp.nlat > 0 only); the explicit sponge of an RK stage;
+// and the per-column trigonometric table they use, once at set-up.
+void launch_sponge_means(const Geometry& g, const Phys& P, const Sponge& sp, const SpongeIn& in,
                          cudaStream_t st);
+void launch_sponge_explicit(const Geometry& g, const Phys& P, const Sponge& sp, const State& s,
+                            cudaStream_t st);
 void launch_sponge_trig(const Geometry& g, double* trig, cudaStream_t st);
 // ProfX up to the physics modules; with finish, also the pressure update and NaN check, which
 // launch_profx_finish does separately when modules run in between. The sponge (sp.nlat > 0) runs

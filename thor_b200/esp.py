@@ -19,8 +19,8 @@ Differences, each stated where it applies:
     built here), the output files lack the per-cell global-diagnostic arrays (their global sums are
     written) and the RT's Qheat scaling; restart files may also be the .npz archives of earlier
     versions of this runner;
-  * keys for physics that this build does not implement (the diffusive sponge, the explicit
-    Rayleigh-sponge modes exp1 and exp3, the RayPH convective adjustment, chemistry, boundary layer, ultra-hot thermodynamics, refined vertical grids,
+  * keys for physics that this build does not implement (the diffusive sponge, the RayPH
+    convective adjustment, chemistry, boundary layer, ultra-hot thermodynamics, refined vertical grids,
     picket-fence or two-stream RT, the Parmentier and constant-N initial profiles) are accepted at
     their default values
     and rejected with an error naming the key otherwise;
@@ -267,9 +267,6 @@ def check_config(c, out=sys.stdout):
     if c["RayleighSponge"]:  # src/esp.cu:757-780: the mode is read only with the sponge on
         need(c["raysp_calc_mode"] in ("imp", "exp1", "exp3"),
              "raysp_calc_mode config item not recognised: [%s]" % c["raysp_calc_mode"])
-        need(c["raysp_calc_mode"] not in ("exp1", "exp3"),
-             "raysp_calc_mode = %s: not implemented in this build (allowed: imp)"
-             % c["raysp_calc_mode"])
         need(c["nlat_bins"] >= 1, "nlat_bins must be >= 1")
         need(0.0 <= c["ns_ray_sponge"] < 1.0, "ns_ray_sponge must be in [0, 1)")
     for k, (kind, default, role) in KEYS.items():
@@ -292,7 +289,8 @@ def sponge_config(c, first_step):
                 RT_sponge=c["RT_sponge"], ns_ray_sponge=c["ns_ray_sponge"],
                 damp_uv_to_mean=int(c["damp_uv_to_mean"]), damp_w_to_mean=int(c["damp_w_to_mean"]),
                 RayleighSpongeT=int(c["RayleighSpongeT"]), shrink_sponge=int(c["shrink_sponge"]),
-                t_shrink=c["t_shrink"], first_step=first_step)
+                t_shrink=c["t_shrink"], first_step=first_step,
+                raysp_calc_mode={"imp": 0, "exp1": 1, "exp3": 2}[c["raysp_calc_mode"]])
 
 
 def thorx_params(c):
