@@ -21,6 +21,8 @@
 // Stencils are templated on the ring size (6, or 5 at pentagons and poles) so that every index
 // is static and the ring values stay in registers.
 
+#include <type_traits>
+
 #include "thorx.h"
 #include "thorx_internal.h"
 
@@ -136,13 +138,25 @@ struct SGeo {
     __device__ double OA(int q) const { return oa[q * kTile + x]; }
     // 1 / areasTr rounded to nearest
     __device__ double RAT(int q) const { return rat[q * kTile + x]; }
-    // mixed form: the column's operator weights (Geometry::lapw, Geometry::dmw), [entry][32]
+    // the column's operator weights (Geometry::lapw, Geometry::dmw, dmw64), [entry][32]
     const double* lw;
     const float * lwf, *dm;
+    const double* dm64;
 };
 
 // The mixed form (compute type float) applies the operators through per-column weights.
 template<class R> constexpr bool kOperatorWeights = sizeof(R) < sizeof(double);
+// The FP64 form's hyperdiffusion and divergence damping through FP64 operator weights (the same
+// linear operators as the reference's triangle sequences, summed in another order); 0 restores
+// the reference's operation order.
+#ifndef THORX_FP64_DIFF_WEIGHTS
+#define THORX_FP64_DIFF_WEIGHTS 1
+#endif
+#ifndef THORX_FP64_DIVM_WEIGHTS
+#define THORX_FP64_DIVM_WEIGHTS 1
+#endif
+constexpr bool kDiffWeightsF64 = THORX_FP64_DIFF_WEIGHTS != 0;
+constexpr bool kDivmWeightsF64 = THORX_FP64_DIVM_WEIGHTS != 0;
 
 // areas 18, areasTr 6, nvecti 18, nvecte 18, nvecoa 18, 1/areasTr 6
 constexpr int kRingGeoRows = 84;
@@ -189,11 +203,23 @@ __device__ __forceinline__ SGeo stage_divm_weights(double* sm, const Geometry& g
     G.dm = smf;
     return G;
 }
-// What a kernel with divergence damping stages: ring geometry (FP64 form) or weights (mixed).
+// FP64 form: the divergence-damping weights in double, [84][32] (the size of the ring geometry).
+__device__ __forceinline__ SGeo stage_divm_weights64(double* sm, const Geometry& g, int col) {
+    for (int q = threadIdx.y; q < 84; q += blockDim.y)
+        sm[q * kTile + threadIdx.x] = col >= 0 ? __ldg(g.dmw64 + (size_t)q * g.Np + col) : 0.0;
+    SGeo G{};
+    G.x    = threadIdx.x;
+    G.dm64 = sm;
+    return G;
+}
+// What a kernel with divergence damping stages: float weights (mixed form), double weights or the
+// ring geometry (FP64 form).
 template<class R>
 __device__ __forceinline__ SGeo stage_divm_geo(double* sm, const Geometry& g, int col) {
     if constexpr (kOperatorWeights<R>)
         return stage_divm_weights(sm, g, col);
+    else if constexpr (kDivmWeightsF64)
+        return stage_divm_weights64(sm, g, col);
     else
         return stage_ring_geo(sm, g, col);
 }
@@ -1198,11 +1224,11 @@ __device__ __forceinline__ void diffusion_point(const Geometry& g, const Phys& P
     }
 }
 
-// Mixed form: the six Laplacians of one (column, level) in one pass over the stencil points. With
-// the operator weights each Laplacian is a running sum, so the values of all six variables at a
-// point are loaded together; each sum keeps laplacian_w's order (centre weight, then the ring in
-// order), v and w in float, rho and T in double.
-template<int n>
+// The six Laplacians of one (column, level) in one pass over the stencil points. With the operator
+// weights each Laplacian is a running sum, so the values of all six variables at a point are
+// loaded together; each sum keeps laplacian_w's order (centre weight, then the ring in order).
+// kF32 (mixed form): v and w in float, rho and T in double; otherwise all six in double.
+template<int n, bool kF32>
 __device__ __forceinline__ void diffusion_point_w(const Geometry& g, const Phys& P, const State& s,
                                                   const SGeo& G, const double* fr, const int* ring,
                                                   const double* __restrict__ diff_in,
@@ -1242,30 +1268,50 @@ __device__ __forceinline__ void diffusion_point_w(const Geometry& g, const Phys&
     };
     double a0[6];
     point(c, a0);
-    double accd0 = G.lw[x] * a0[0], accd5 = G.lw[x] * a0[5];
-    float  accf[4];
-#pragma unroll
-    for (int k = 0; k < 4; k++)
-        accf[k] = G.lwf[x] * (float)a0[1 + k];
-#pragma unroll 2
-    for (int j = 1; j <= n; j++) {
-        double v[6];
-        point(__ldg(g.ring + (j - 1) * Np + c), v);
-        const double w  = G.lw[j * kTile + x];
-        const float  wf = G.lwf[j * kTile + x];
-        accd0           = fma(w, v[0] - a0[0], accd0);
-        accd5           = fma(w, v[5] - a0[5], accd5);
-#pragma unroll
-        for (int k = 0; k < 4; k++)
-            accf[k] = fmaf(wf, (float)(v[1 + k] - a0[1 + k]), accf[k]);
-    }
     const double sc = rscale * rscale;
     double       lap[6];
-    lap[0] = accd0 * sc;
-    lap[5] = accd5 * sc;
+    if constexpr (kF32) {
+        double accd0 = G.lw[x] * a0[0], accd5 = G.lw[x] * a0[5];
+        float  accf[4];
 #pragma unroll
-    for (int k = 0; k < 4; k++)
-        lap[1 + k] = (double)(accf[k] * (float)sc);
+        for (int k = 0; k < 4; k++)
+            accf[k] = G.lwf[x] * (float)a0[1 + k];
+#pragma unroll 2
+        for (int j = 1; j <= n; j++) {
+            double v[6];
+            point(__ldg(g.ring + (j - 1) * Np + c), v);
+            const double w  = G.lw[j * kTile + x];
+            const float  wf = G.lwf[j * kTile + x];
+            accd0           = fma(w, v[0] - a0[0], accd0);
+            accd5           = fma(w, v[5] - a0[5], accd5);
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                accf[k] = fmaf(wf, (float)(v[1 + k] - a0[1 + k]), accf[k]);
+        }
+        lap[0] = accd0 * sc;
+        lap[5] = accd5 * sc;
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            lap[1 + k] = (double)(accf[k] * (float)sc);
+    }
+    else {
+        double acc[6];
+#pragma unroll
+        for (int var = 0; var < 6; var++)
+            acc[var] = G.lw[x] * a0[var];
+#pragma unroll 2
+        for (int j = 1; j <= n; j++) {
+            double v[6];
+            point(__ldg(g.ring + (j - 1) * Np + c), v);
+            const double w = G.lw[j * kTile + x];
+#pragma unroll
+            for (int var = 0; var < 6; var++)
+                acc[var] = fma(w, v[var] - a0[var], acc[var]);
+        }
+#pragma unroll
+        for (int var = 0; var < 6; var++)
+            lap[var] = acc[var] * sc;
+    }
     if (!last) {
 #pragma unroll
         for (int var = 0; var < 6; var++)
@@ -1302,7 +1348,11 @@ __device__ __forceinline__ void diffusion_body(const Geometry& g, const Phys& P,
     const double sign4 = pow(-1.0, P.HyDiffOrder / 2); // (-1)^(order/2) of the last pass
     for (int lev = threadIdx.y; lev < g.nv; lev += kLevGroups)
         if constexpr (kOperatorWeights<R>)
-            diffusion_point_w<n>(g, P, s, G, fr, ring, diff_in, diff_out, stepnum, last, c, lev, sign4);
+            diffusion_point_w<n, true>(g, P, s, G, fr, ring, diff_in, diff_out, stepnum, last, c,
+                                       lev, sign4);
+        else if constexpr (kDiffWeightsF64)
+            diffusion_point_w<n, false>(g, P, s, G, fr, ring, diff_in, diff_out, stepnum, last, c,
+                                        lev, sign4);
         else
             diffusion_point<n, R>(g, P, s, G, fr, ring, diff_in, diff_out, stepnum, last, c, lev, sign4);
 }
@@ -1315,7 +1365,7 @@ __global__ void THORX_KATTR_DIFF
     __shared__ double sgeo[kRingGeoRows * kTile];
     const int         c = lane_column(g);
     SGeo              G;
-    if constexpr (kOperatorWeights<R>)
+    if constexpr (kOperatorWeights<R> || kDiffWeightsF64)
         G = stage_lap_weights(sgeo, g, c);
     else
         G = stage_ring_geo(sgeo, g, c);
@@ -1408,7 +1458,8 @@ __device__ __forceinline__ void divm_core(const SGeo& G, const R* a0, const R (*
 // One thread per column; a column with a five-entry ring gets zero sixth weights.
 // ---------------------------------------------------------------------------------------------
 template<int n>
-__device__ void stencil_weights_of(const SGeo& G, int c2, int c, int Np, double* lapw, float* dmw) {
+__device__ void stencil_weights_of(const SGeo& G, int c2, int c, int Np, double* lapw, float* dmw,
+                                   double* dmw64) {
     // Laplacian
     double w[7] = {0, 0, 0, 0, 0, 0, 0}, wsum = 0.0;
     for (int k = 0; k <= n; k++) {
@@ -1441,9 +1492,12 @@ __device__ void stencil_weights_of(const SGeo& G, int c2, int c, int Np, double*
             double sum = 0.0;
             for (int k = 0; k <= n; k++)
                 sum += wm[o][k][comp];
-            dmw[(size_t)(o * 28 + comp) * Np + c] = (float)sum;
-            for (int k = 1; k < 7; k++)
-                dmw[(size_t)(o * 28 + k * 3 + comp) * Np + c] = (float)wm[o][k][comp];
+            dmw[(size_t)(o * 28 + comp) * Np + c]   = (float)sum;
+            dmw64[(size_t)(o * 28 + comp) * Np + c] = sum;
+            for (int k = 1; k < 7; k++) {
+                dmw[(size_t)(o * 28 + k * 3 + comp) * Np + c]   = (float)wm[o][k][comp];
+                dmw64[(size_t)(o * 28 + k * 3 + comp) * Np + c] = wm[o][k][comp];
+            }
         }
     // divergence damping, w part: response to a unit (Wh below - Wh above) at point k
     for (int k = 0; k < 7; k++) {
@@ -1458,12 +1512,15 @@ __device__ void stencil_weights_of(const SGeo& G, int c2, int c, int Np, double*
             divm_core<n, double>(G, a0, ar, true, k == 0 ? 1.0 : 0.0, 0.0, wl, wt, 1.0, 1.0, c2,
                                  out);
         }
-        for (int o = 0; o < 3; o++)
-            dmw[(size_t)(o * 28 + 21 + k) * Np + c] = (float)out[o];
+        for (int o = 0; o < 3; o++) {
+            dmw[(size_t)(o * 28 + 21 + k) * Np + c]   = (float)out[o];
+            dmw64[(size_t)(o * 28 + 21 + k) * Np + c] = out[o];
+        }
     }
 }
 
-__global__ void __launch_bounds__(kTile) stencil_weights_kernel(Geometry g, double* lapw, float* dmw) {
+__global__ void __launch_bounds__(kTile) stencil_weights_kernel(Geometry g, double* lapw, float* dmw,
+                                                                double* dmw64) {
     __shared__ double sgeo[kRingGeoRows * kTile];
     const int         c   = blockIdx.x * kTile + threadIdx.x;
     const int         col = c < g.N ? c : -1;
@@ -1473,46 +1530,53 @@ __global__ void __launch_bounds__(kTile) stencil_weights_kernel(Geometry g, doub
         return;
     const int c2 = (g.cflag[c] & kPole) ? 1 : 2;
     if (g.cflag[c] & kRing5)
-        stencil_weights_of<5>(G, c2, c, g.Np, lapw, dmw);
+        stencil_weights_of<5>(G, c2, c, g.Np, lapw, dmw, dmw64);
     else
-        stencil_weights_of<6>(G, c2, c, g.Np, lapw, dmw);
+        stencil_weights_of<6>(G, c2, c, g.Np, lapw, dmw, dmw64);
 }
 
 // Divergence damping from the weights, in float: a0 [3] and ar [n][3] the Mh (or divg) vectors
 // at the centre and the ring; dw [n + 1] the (below - above) Wh differences when with_w.
-template<int n>
+// T: float (mixed form, Geometry::dmw) or double (FP64 form, Geometry::dmw64).
+__device__ __forceinline__ float fma_t(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double fma_t(double a, double b, double c) { return fma(a, b, c); }
+template<int n, class T>
 __device__ __forceinline__ void divm_w(const SGeo& G, const double* a0, const double (*ar)[3],
                                        bool with_w, const double* dw, double rscale, double dz,
-                                       float* out) {
+                                       T* out) {
     const int x = G.x;
-    float     d[n][3], c0[3];
+    T         d[n][3], c0[3];
 #pragma unroll
     for (int comp = 0; comp < 3; comp++) {
-        c0[comp] = (float)a0[comp];
+        c0[comp] = (T)a0[comp];
 #pragma unroll
         for (int j = 0; j < n; j++)
-            d[j][comp] = (float)(ar[j][comp] - a0[comp]);
+            d[j][comp] = (T)(ar[j][comp] - a0[comp]);
     }
-    const float sv = (float)(rscale * rscale), sw = (float)(rscale * dz);
+    const T sv = (T)(rscale * rscale), sw = (T)(rscale * dz);
 #pragma unroll
     for (int o = 0; o < 3; o++) {
-        const float* W   = G.dm + o * 28 * kTile + x;
-        float        acc = 0.0f;
+        const T* W;
+        if constexpr (sizeof(T) < sizeof(double))
+            W = G.dm + o * 28 * kTile + x;
+        else
+            W = G.dm64 + o * 28 * kTile + x;
+        T acc = (T)0;
 #pragma unroll
         for (int comp = 0; comp < 3; comp++)
-            acc = fmaf(W[comp * kTile], c0[comp], acc);
+            acc = fma_t(W[comp * kTile], c0[comp], acc);
 #pragma unroll
         for (int j = 0; j < n; j++)
 #pragma unroll
             for (int comp = 0; comp < 3; comp++)
-                acc = fmaf(W[((j + 1) * 3 + comp) * kTile], d[j][comp], acc);
+                acc = fma_t(W[((j + 1) * 3 + comp) * kTile], d[j][comp], acc);
         acc *= sv;
         if (with_w) {
-            float accw = 0.0f;
+            T accw = (T)0;
 #pragma unroll
             for (int k = 0; k <= n; k++)
-                accw = fmaf(W[(21 + k) * kTile], (float)dw[k], accw);
-            acc = fmaf(accw, sw, acc);
+                accw = fma_t(W[(21 + k) * kTile], (T)dw[k], accw);
+            acc = fma_t(accw, sw, acc);
         }
         out[o] = acc;
     }
@@ -1526,7 +1590,8 @@ __device__ __forceinline__ void divm0_point(const Geometry& g, const Phys& P, co
     const int    Np = g.Np, nv = g.nv;
     const double rscale = rscale_of(P, g, lev);
     const double dz     = 1.0 / (g.Altitudeh[lev] - g.Altitudeh[lev + 1]);
-    if constexpr (kOperatorWeights<R>) {
+    if constexpr (kOperatorWeights<R> || kDivmWeightsF64) {
+        using T = std::conditional_t<kOperatorWeights<R>, float, double>;
         double a0[3], ar[n][3], dw[n + 1];
 #pragma unroll
         for (int k = 0; k < 3; k++)
@@ -1539,8 +1604,8 @@ __device__ __forceinline__ void divm0_point(const Geometry& g, const Phys& P, co
                 ar[j][k] = gz(Mh + (k * nv + lev) * Np, ring[j]);
             dw[j + 1] = gz(Wh + lev * Np, ring[j]) - gz(Wh + (lev + 1) * Np, ring[j]);
         }
-        float out[3];
-        divm_w<n>(G, a0, ar, true, dw, rscale, dz, out);
+        T out[3];
+        divm_w<n, T>(G, a0, ar, true, dw, rscale, dz, out);
 #pragma unroll
         for (int k = 0; k < 3; k++)
             divg[(k * nv + lev) * Np + c] = (double)out[k];
@@ -1605,7 +1670,7 @@ __device__ __forceinline__ void divm_final(const Geometry& g, const Phys& P, con
                                            int lev, const double* fr, R* DivM) {
     const int Np = g.Np, nv = g.nv;
     R         lap[3];
-    if constexpr (kOperatorWeights<R>) {
+    if constexpr (kOperatorWeights<R> || kDivmWeightsF64) {
         double a0[3], ar[n][3];
 #pragma unroll
         for (int k = 0; k < 3; k++)
@@ -1615,7 +1680,7 @@ __device__ __forceinline__ void divm_final(const Geometry& g, const Phys& P, con
 #pragma unroll
             for (int k = 0; k < 3; k++)
                 ar[j][k] = gz(divg + (k * nv + lev) * Np, ring[j]);
-        divm_w<n>(G, a0, ar, false, nullptr, rscale_of(P, g, lev), 0.0, lap);
+        divm_w<n, R>(G, a0, ar, false, nullptr, rscale_of(P, g, lev), 0.0, lap);
     }
     else {
         R a0[3], ar[n][3];
@@ -2501,8 +2566,9 @@ int max_levels() { return kRk2Groups * kMaxLevelsPerThread; }
 void launch_level_tables(const Geometry& g, const Phys& P, double* lt, cudaStream_t st) {
     level_tables_kernel<<<(g.nvi + 127) / 128, 128, 0, st>>>(g, P, lt);
 }
-void launch_stencil_weights(const Geometry& g, double* lapw, float* dmw, cudaStream_t st) {
-    stencil_weights_kernel<<<(g.N + kTile - 1) / kTile, kTile, 0, st>>>(g, lapw, dmw);
+void launch_stencil_weights(const Geometry& g, double* lapw, float* dmw, double* dmw64,
+                            cudaStream_t st) {
+    stencil_weights_kernel<<<(g.N + kTile - 1) / kTile, kTile, 0, st>>>(g, lapw, dmw, dmw64);
 }
 
 void launch_sponge_trig(const Geometry& g, double* trig, cudaStream_t st) {

@@ -727,11 +727,14 @@ int thorx_create(const thorx_grid* gr, const thorx_params* pr, void* stream, tho
         // operator weights of the mixed form, from the geometry just uploaded
         double* lapw;
         float*  dmw;
-        if (dev_alloc(ctx, &lapw, (size_t)7 * Np) || dev_alloc(ctx, &dmw, (size_t)84 * Np))
+        double* dmw64;
+        if (dev_alloc(ctx, &lapw, (size_t)7 * Np) || dev_alloc(ctx, &dmw, (size_t)84 * Np)
+            || dev_alloc(ctx, &dmw64, (size_t)84 * Np))
             return THORX_E_CUDA;
         g.lapw = lapw;
-        g.dmw  = dmw;
-        launch_stencil_weights(g, lapw, dmw, ctx->stream);
+        g.dmw   = dmw;
+        g.dmw64 = dmw64;
+        launch_stencil_weights(g, lapw, dmw, dmw64, ctx->stream);
         CK(cudaGetLastError());
     }
 

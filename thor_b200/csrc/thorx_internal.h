@@ -65,6 +65,7 @@ struct Geometry {
     //   ring), then 7 entries for (Wh below - Wh above) at points 0..6 at rscale = dz = 1.
     const double*  lapw;
     const float*   dmw;
+    const double*  dmw64; // dmw in double, for the FP64 form
 };
 
 // Per-level quantities that every column shares, tabulated once on the device at context
@@ -135,7 +136,8 @@ size_t vertical_smem_bytes(const Geometry& g);
 
 // Fills the per-level tables lt[kLtCount * (nv+1)] (thor_b200/csrc/dyn_fp64.cu).
 void launch_level_tables(const Geometry& g, const Phys& P, double* lt, cudaStream_t st);
-void launch_stencil_weights(const Geometry& g, double* lapw, float* dmw, cudaStream_t st);
+void launch_stencil_weights(const Geometry& g, double* lapw, float* dmw, double* dmw64,
+                            cudaStream_t st);
 
 // Rayleigh sponge layer at the top of the model (RayleighSponge with raysp_calc_mode = imp,
 // reference src/ESP/profx_sponge.cu, called at src/ESP/profx_driver.cu:96-194): winds (and with
