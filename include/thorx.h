@@ -217,6 +217,13 @@ int thorx_device_field(thorx_ctx* ctx, const char* name, double** dev, int* leve
  * with HyDiff on. order 0 switches it off. A step graph captured earlier is re-captured. */
 int thorx_vert_hydiff_enable(thorx_ctx* ctx, double Diffc_v, int order);
 
+/* The check of the vertical solve that the reference compiles in with
+ * DIAG_CHECK_THOR_VERTICAL_INT_THOMAS_RESULT (src/headers/dyn/thor_vertical_int.h:486-523): for
+ * the last small step's tridiagonal system, the largest residual relative to the right-hand side
+ * (absolute where it is 0) over the interior interfaces 2..nv-1 of all columns, and the number of
+ * interfaces above epsilon (the reference uses 1e-8). Synchronises the context's stream. */
+int thorx_check_thomas(thorx_ctx* ctx, double epsilon, double* max_rel, long long* n_bad);
+
 /* One physics step, ESP::ProfX (src/ESP/profx_driver.cu:70-474): W from Wh, T and potential
  * temperature from p and rho, Held-Suarez forcing when core_benchmark says so, p = rho Rd T,
  * and the NaN check (reported at the next synchronising call as THORX_E_NAN). */

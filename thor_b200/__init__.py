@@ -166,6 +166,9 @@ def lib():
         L.thorx_device_field.restype = ci
         L.thorx_vert_hydiff_enable.argtypes = [vp, ctypes.c_double, ci]
         L.thorx_vert_hydiff_enable.restype = ci
+        L.thorx_check_thomas.argtypes = [vp, ctypes.c_double, ctypes.POINTER(ctypes.c_double),
+                                         ctypes.POINTER(ctypes.c_longlong)]
+        L.thorx_check_thomas.restype = ci
         L.thorx_init_guillot_state.argtypes = [vp] + [ctypes.c_double] * 5 + [ctypes.c_ulonglong,
                                                                              ctypes.c_double]
         L.thorx_init_guillot_state.restype = ci
@@ -216,7 +219,8 @@ EXPORTED = ["thorx_create", "thorx_destroy", "thorx_last_error", "thorx_field_si
             "thorx_surrogate_forward_host", "thorx_surrogate_gradients_host",
             "thorx_check_division", "thorx_conv_adj_enable", "thorx_init_guillot_state",
             "thorx_sponge_enable", "thorx_sponge_means", "thorx_module_add",
-            "thorx_rk_register_array", "thorx_device_field", "thorx_vert_hydiff_enable"]
+            "thorx_rk_register_array", "thorx_device_field", "thorx_vert_hydiff_enable",
+            "thorx_check_thomas"]
 
 def device_sum(ptr, n, stream=0):
     """Compensated sum of n doubles at device address `ptr` (thorx_device_sum)."""
@@ -438,6 +442,12 @@ class Thorx:
             return
         self._sponge = sponge_params(d)
         self._check(lib().thorx_sponge_enable(self.h, ctypes.byref(self._sponge)))
+
+    def check_thomas(self, epsilon=1e-8):
+        """(largest relative residual, interfaces above epsilon) of the last vertical solve."""
+        m, n = ctypes.c_double(), ctypes.c_longlong()
+        self._check(lib().thorx_check_thomas(self.h, epsilon, ctypes.byref(m), ctypes.byref(n)))
+        return m.value, n.value
 
     def vert_hydiff(self, Diffc_v, order=6):
         """Vertical hyperdiffusion (VertHyDiff) in every following step; order 0: off."""

@@ -2649,6 +2649,41 @@ void launch_vertical(const Geometry& g, const Phys& P, const State& s, double dt
         launch_vertical_part<0>(g, P, s, dt, st);
 }
 
+// The check of the Thomas solution that the reference compiles in with
+// DIAG_CHECK_THOR_VERTICAL_INT_THOMAS_RESULT (src/headers/dyn/thor_vertical_int.h:486-523): at the
+// interior interfaces 2..nv-1, the residual of a w(l-1) + b w(l) + c w(l+1) = d for the rows and
+// the solution of the last vertical solve, relative to |d| (absolute where d == 0). Per column the
+// largest residual and the number of interfaces above epsilon (1e-8 in the reference).
+__global__ void thomas_residual_kernel(Geometry g, State s, double eps, double* colmax,
+                                       unsigned int* nbad) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= g.N)
+        return;
+    const int     Np = g.Np, nv = g.nv, nvi = g.nvi;
+    const double* ra = s.vrows;
+    const double* rb = ra + (size_t)nvi * Np;
+    const double* rc = rb + (size_t)nvi * Np;
+    const double* rd = rc + (size_t)nvi * Np;
+    double        worst = 0.0;
+    unsigned int  bad   = 0;
+    for (int lev = 2; lev < nv; lev++) {
+        const double dd  = rd[lev * Np + c];
+        const double out = ra[lev * Np + c] * s.Whs[(lev - 1) * Np + c]
+                           + rb[lev * Np + c] * s.Whs[lev * Np + c]
+                           + rc[lev * Np + c] * s.Whs[(lev + 1) * Np + c];
+        const double r = dd == 0.0 ? fabs(out - dd) : fabs((out - dd) / dd);
+        worst          = fmax(worst, r);
+        bad += r > eps ? 1u : 0u;
+    }
+    colmax[c] = worst;
+    if (bad)
+        atomicAdd(nbad, bad);
+}
+void launch_thomas_residual(const Geometry& g, const State& s, double eps, double* colmax,
+                            unsigned int* nbad, cudaStream_t st) {
+    thomas_residual_kernel<<<(g.N + 127) / 128, 128, 0, st>>>(g, s, eps, colmax, nbad);
+}
+
 // Registered module arrays (device_RK_array_manager, src/ESP/phy_modules_device.cu:47-77): the
 // deviation reset of UpdateRK, array = arrayi - arrayk (src/headers/dyn/thor_auxiliary.h:376-387),
 // and the accumulation of UpdateRK2, arrayk += array (:483-494), elementwise.

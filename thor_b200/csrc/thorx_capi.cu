@@ -1896,4 +1896,42 @@ int thorx_vert_hydiff_enable(thorx_ctx* ctx, double Diffc_v, int order) {
     return drop_graph(ctx);
 }
 
+int thorx_check_thomas(thorx_ctx* ctx, double epsilon, double* max_rel, long long* n_bad) {
+    if (!ctx)
+        return THORX_E_ARG;
+    if (!max_rel || !n_bad)
+        return fail(ctx, THORX_E_ARG, "thorx_check_thomas: null output");
+    const int     N = ctx->g.N;
+    double*       colmax = nullptr;
+    unsigned int* nbad   = nullptr;
+    CK(cudaMalloc(&colmax, (size_t)N * sizeof(double)));
+    cudaError_t e = cudaMalloc(&nbad, sizeof(unsigned int));
+    if (e == cudaSuccess)
+        e = cudaMemsetAsync(nbad, 0, sizeof(unsigned int), ctx->stream);
+    if (e == cudaSuccess) {
+        launch_thomas_residual(ctx->g, ctx->s, epsilon, colmax, nbad, ctx->stream);
+        e = cudaGetLastError();
+    }
+    std::vector<double> h(N);
+    unsigned int        hb = 0;
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(h.data(), colmax, (size_t)N * sizeof(double), cudaMemcpyDeviceToHost,
+                            ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(&hb, nbad, sizeof(unsigned int), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(colmax);
+    if (nbad)
+        cudaFree(nbad);
+    if (e != cudaSuccess)
+        return fail(ctx, THORX_E_CUDA, std::string("thorx_check_thomas: ") + cudaGetErrorString(e));
+    double m = 0.0;
+    for (double v : h)
+        m = v > m ? v : m;
+    *max_rel = m;
+    *n_bad   = hb;
+    return 0;
+}
+
 } // extern "C"

@@ -211,6 +211,10 @@ struct RkArrays {
     double*   arrayi[kMaxRkArrays];
     long long count[kMaxRkArrays];
 };
+// Residual of the last vertical solve's tridiagonal system per column (colmax [N]) and the count
+// of interfaces above eps (nbad, added to).
+void launch_thomas_residual(const Geometry& g, const State& s, double eps, double* colmax,
+                            unsigned int* nbad, cudaStream_t st);
 // mode 0: UpdateRK's deviation reset (array = arrayi - arrayk); 1: UpdateRK2 (arrayk += array).
 void launch_rk_arrays(const RkArrays& t, int mode, cudaStream_t st);
 void launch_update_rk2(const Geometry& g, const Phys& P, const State& s, cudaStream_t st);
