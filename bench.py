@@ -37,7 +37,9 @@ EARTH = dict(A=6.371e6, Omega=7.292e-5, Gravit=9.8, Rd=287.0, Cp=1005.0, P_Ref=1
              NonHydro=1, GravHeightVar=0, HyDiff=1, DivDampP=1, thermo_equation=0,
              core_benchmark=1)
 TMEAN, SEED, NOISE = 300.0, 20260101, 0.1
-STATE = ["Rho", "pressure", "Mh", "Wh", "W"]
+# the prognostic state a step reads and writes: the fields of the reference's restart files
+# (src/ESP/esp_initial.cu:1215-1260); W is diagnostic (ProfX recomputes it from Wh first)
+STATE = ["Rho", "pressure", "Mh", "Wh"]
 FALLBACK_HBM_GBS = 6650.0
 
 
