@@ -31,3 +31,17 @@ def test_null_arguments_are_rejected_without_a_gpu():
     assert L.thorx_field_size(None, b"Rho") == -1
     assert L.thorx_step(None, 1) == -1
     L.thorx_destroy(h.value)
+
+
+def test_unsupported_sizes_and_options_are_rejected_before_device_work():
+    """thorx_create checks its arguments before any CUDA call, so this runs without a GPU."""
+    import pytest
+    from thorx_testlib import EARTH, thorx_params
+    for nv, over, code in ((129, {}, -4), (8, dict(HyDiffOrder=3), -4),
+                           (8, dict(precision=5), -1), (8, dict(core_benchmark=9), -4)):
+        g = thor_b200.Icogrid(4, nv)
+        p = thorx_params(dict(EARTH), 600.0)
+        p.update(over)
+        with pytest.raises(thor_b200.ThorxError) as e:
+            thor_b200.Thorx(g.as_dict(), 4, p)
+        assert e.value.code == code, (nv, over, e.value)

@@ -30,6 +30,11 @@ CASES = [
     (4, 16, 1200.0, dict(GravHeightVar=1, energy_equation=1)),
     (5, 16, 600.0, dict(DivDampP=0)),
     (4, 12, 1200.0, dict(HyDiffOrder=2, held_suarez=0)),
+    # the extremes of the column: three levels (the least a context takes) and 95 levels, the
+    # most the reference's Vertical_Eq launches with its default shared-memory limit
+    # (2 x 32 x (nv + 1) doubles <= 48 KB)
+    (4, 3, 1200.0, {}),
+    (4, 95, 1200.0, {}),
 ]
 
 

@@ -99,6 +99,7 @@ def test_bad_lines_fail_the_file(line):
     ("core_benchmark = JetSteady", "core_benchmark"),
     ("HyDiffOrder = 5", "HyDiffOrder"),
     ("glevel = 9", "glevel"),
+    ("glevel = 3", "glevel"),
     ("n_out = 0", "n_out"),
     ("precision = fp16", "precision"),
 ])

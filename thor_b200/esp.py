@@ -254,6 +254,7 @@ def check_config(c, out=sys.stdout):
     need(c["P_ref"] > 0, "P_Ref must be > 0")
     need(c["Top_altitude"] > 0, "Top_altitude must be > 0")
     need(3 <= c["glevel"] <= 8, "glevel must be in [3, 8]")
+    need(4 <= c["glevel"] <= 7, "glevel = %d: this build's grid takes 4 to 7" % c["glevel"])
     need(c["vlevel"] > 0, "vlevel must be > 0")
     need(c["GPU_ID_N"] > -1, "GPU_ID_N must be > -1")
     need(c["n_out"] > 0, "n_out must be > 0")
