@@ -656,29 +656,43 @@ __global__ void __launch_bounds__(kColBlock) sponge_explicit_kernel(Geometry g, 
     }
 }
 
-__global__ void __launch_bounds__(kColBlock) profx_kernel(Geometry g, Phys P, Sponge sp, State s,
-                                                          bool finish) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= g.N)
-        return;
+// 32 columns x kProfxGroups level groups per block: the level-local parts run level-parallel
+// (group y: levels y, y + kProfxGroups, ...); the column-serial ones (sponge, convective
+// adjustment) run on group 0 between barriers.
+constexpr int kProfxCols = 32, kProfxGroups = 8;
+__global__ void __launch_bounds__(kProfxCols* kProfxGroups) profx_kernel(Geometry g, Phys P,
+                                                                        Sponge sp, State s,
+                                                                        bool finish) {
+    const int  c     = blockIdx.x * kProfxCols + threadIdx.x;
+    const bool valid = c < g.N;
+    const int  y0 = threadIdx.y, dy = kProfxGroups;
     const int     Np = g.Np, nv = g.nv;
     const double* Alt  = g.Altitude;
     const double* Alth = g.Altitudeh;
-    for (int lev = 0; lev < nv; lev++) {
+    for (int lev = y0; valid && lev < nv; lev += dy) {
         double whl = s.Wh[lev * Np + c], wht = s.Wh[(lev + 1) * Np + c];
         double xi = Alt[lev], xim = Alth[lev], xip = Alth[lev + 1];
         double intt = (xi - xip) / (xim - xip);
         double intl = (xi - xim) / (xip - xim);
         s.W[lev * Np + c] = whl * intt + wht * intl;
     }
-    if (sp.nlat > 0) // after Recompute_W, before the temperature (profx_driver.cu:96-194)
-        sponge_column(g, P, sp, s, c);
-    for (int lev = 0; lev < nv; lev++) {
+    if (sp.nlat > 0) { // after Recompute_W, before the temperature (profx_driver.cu:96-194)
+        __syncthreads();
+        if (valid && y0 == 0)
+            sponge_column(g, P, sp, s, c);
+        __syncthreads();
+    }
+    for (int lev = y0; valid && lev < nv; lev += dy) {
         int i  = lev * Np + c;
         s.T[i] = s.p[i] / (s.Rd[i] * s.Rho[i]);
     }
-    if (P.conv_adj_iter > 0) // after the temperature, before the forcing (profx_driver.cu:239-290)
-        conv_adj_column(g, P, s, c);
+    if (P.conv_adj_iter > 0) { // after the temperature, before the forcing (profx_driver.cu:239-290)
+        __syncthreads();
+        if (valid && y0 == 0)
+            conv_adj_column(g, P, s, c);
+        __syncthreads();
+    }
+
     if (P.held_suarez) {
         const double sigmab = 0.7, ka = (1.0 / 40.0) * (1.0 / 86400.0), kf = 1.0 / 86400.0;
         const double ks = (1.0 / 4.0) * (1.0 / 86400.0), kappa = P.Rd / P.Cp, dTy = 60.0,
@@ -686,7 +700,7 @@ __global__ void __launch_bounds__(kColBlock) profx_kernel(Geometry g, Phys P, Sp
         const double lat  = g.lat[c];
         const double psm1 = s.p[Np + c] - s.Rho[c] * P.Gravit * (-Alt[0] - Alt[1]);
         const double ps   = 0.5 * (s.p[c] + psm1);
-        for (int lev = 0; lev < nv; lev++) {
+        for (int lev = y0; valid && lev < nv; lev += dy) {
             int    i      = lev * Np + c;
             double pre    = s.p[i];
             double sigma  = (pre / ps);
@@ -715,7 +729,7 @@ __global__ void __launch_bounds__(kColBlock) profx_kernel(Geometry g, Phys P, Sp
         const double lat  = g.lat[c], lon = g.lon[c];
         const double psm1 = s.p[Np + c] - s.Rho[c] * P.Gravit * (-Alt[0] - Alt[1]);
         const double ps   = 0.5 * (s.p[c] + psm1);
-        for (int lev = 0; lev < nv; lev++) {
+        for (int lev = y0; valid && lev < nv; lev += dy) {
             int    i      = lev * Np + c;
             double pre    = s.p[i];
             double sigma  = (pre / ps);
@@ -742,7 +756,7 @@ __global__ void __launch_bounds__(kColBlock) profx_kernel(Geometry g, Phys P, Sp
         const double lat  = g.lat[c], lon = g.lon[c];
         const double psm1 = s.p[Np + c] - s.Rho[c] * P.Gravit * (-Alt[0] - Alt[1]);
         const double ps   = 0.5 * (s.p[c] + psm1);
-        for (int lev = 0; lev < nv; lev++) {
+        for (int lev = y0; valid && lev < nv; lev += dy) {
             int    i     = lev * Np + c;
             double sigma = (s.p[i] / ps);
             double beta_trop, T_vert;
@@ -768,8 +782,9 @@ __global__ void __launch_bounds__(kColBlock) profx_kernel(Geometry g, Phys P, Sp
     }
     if (!finish) // physics modules run before the pressure update (profx_driver.cu:405-416)
         return;
+    __syncthreads(); // the forcings read p at levels 0 and 1 of the column before this writes p
     bool bad = false;
-    for (int lev = 0; lev < nv; lev++) {
+    for (int lev = y0; valid && lev < nv; lev += dy) {
         int i  = lev * Np + c;
         s.p[i] = s.T[i] * s.Rd[i] * s.Rho[i];
         bad |= isnan(s.T[i]);
@@ -2584,7 +2599,8 @@ void launch_sponge_explicit(const Geometry& g, const Phys& P, const Sponge& sp, 
 }
 void launch_profx(const Geometry& g, const Phys& P, const Sponge& sp, const State& s, bool finish,
                   cudaStream_t st) {
-    profx_kernel<<<(g.N + kColBlock - 1) / kColBlock, kColBlock, 0, st>>>(g, P, sp, s, finish);
+    profx_kernel<<<(g.N + kProfxCols - 1) / kProfxCols, dim3(kProfxCols, kProfxGroups), 0, st>>>(
+        g, P, sp, s, finish);
 }
 void launch_profx_finish(const Geometry& g, const State& s, cudaStream_t st) {
     profx_finish_kernel<<<(g.N + kColBlock - 1) / kColBlock, kColBlock, 0, st>>>(g, s);
