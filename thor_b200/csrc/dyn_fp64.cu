@@ -2643,16 +2643,29 @@ void launch_momentum(const Geometry& g, const Phys& P, const State& s, double dt
         momentum_kernel<double><<<tile_grid_tail(g), tile_block(), 0, st>>>(g, P, s, dt);
 }
 size_t vertical_smem_bytes(const Geometry& g) { return sizeof(double) * kTile * (21 + 4 * g.nv); }
+
+// The largest dynamic shared memory a kernel has been opened to, per device (the attribute is a
+// per-device setting; a process may hold contexts on several devices).
+constexpr int kMaxDevices = 64;
+struct SmemOptIn {
+    size_t bytes[kMaxDevices] = {};
+    bool   need(size_t smem) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (dev < 0 || dev >= kMaxDevices || smem <= bytes[dev])
+            return dev < 0 || dev >= kMaxDevices; // unknown device: set it every time
+        bytes[dev] = smem;
+        return true;
+    }
+};
 template<int kPart>
 void launch_vertical_part(const Geometry& g, const Phys& P, const State& s, double dt,
                           cudaStream_t st) {
-    const size_t  smem       = vertical_smem_bytes(g);
-    static size_t configured = 0;
-    if (smem > configured) {
+    const size_t     smem = vertical_smem_bytes(g);
+    static SmemOptIn opt;
+    if (opt.need(smem))
         cudaFuncSetAttribute(vertical_kernel<kPart>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem);
-        configured = smem;
-    }
     vertical_kernel<kPart><<<tile_grid(g), tile_block(), smem, st>>>(g, P, s, dt);
 }
 void launch_vertical(const Geometry& g, const Phys& P, const State& s, double dt, int part,
@@ -2723,12 +2736,10 @@ void launch_rk_arrays(const RkArrays& t, int mode, cudaStream_t st) {
 }
 void launch_vertical_diff(const Geometry& g, const Phys& P, const State& s, cudaStream_t st) {
     const size_t  smem       = sizeof(double) * kVdCols * (2 * g.nv + 2);
-    static size_t configured = 0;
-    if (smem > configured) {
+    static SmemOptIn opt;
+    if (opt.need(smem))
         cudaFuncSetAttribute(vertical_diff_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem);
-        configured = smem;
-    }
     vertical_diff_kernel<<<(g.N + kVdCols - 1) / kVdCols, kVdCols, smem, st>>>(g, P, s);
 }
 void launch_update_rk2(const Geometry& g, const Phys& P, const State& s, cudaStream_t st) {

@@ -418,11 +418,14 @@ inline bool make_kmajor_map(CUtensorMap* map, const void* ptr, int rows, int K, 
 template<int BN, int EPI>
 inline void gemm_tma(const __nv_bfloat16* A, const __nv_bfloat16* B, int M, int N, int K,
                      const EpiArgs& e, unsigned int* err, cudaStream_t st, int splits = 1) {
-    static bool configured = false;
-    if (!configured) {
+    static bool configured[64] = {}; // the attribute is per device
+    int         dev            = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64 || !configured[dev]) {
         cudaFuncSetAttribute(gemm_tma_kernel<BN, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)gemm_tma_smem_bytes(BN));
-        configured = true;
+        if (dev >= 0 && dev < 64)
+            configured[dev] = true;
     }
     CUtensorMap ma, mb;
     if (!make_kmajor_map(&ma, A, M, K, kM) || !make_kmajor_map(&mb, B, N, K, BN)) {
