@@ -263,3 +263,32 @@ def test_runner_with_the_sponge(tmp_path):
     assert int(final["nstep"][0][0]) == 4 and np.all(np.isfinite(final["Mh"][0]))
     planet = h5.read(str(tmp_path / "o" / "esp_output_planet_TestHS.h5"))
     assert planet["RayleighSponge"][0][0] == 1.0 and planet["nlat_bins"][0][0] == 20
+
+
+@pytest.mark.gpu
+def test_reconfiguring_the_sponge_replaces_it():
+    """A second thorx_sponge_enable (other bins, after steps with the first) gives the steps of a
+    context that had only the second one; the first set-up's tables are released."""
+    g = RefGrid(GLEVEL, NV)
+    p, c = make_params(GLEVEL, DT)
+    st = windy_state(g, c)
+    second = dict(nlat_bins=7, ns_ray_sponge=0.4, Ruv_sponge=5e-4)
+    outs = []
+    for reconfigure in (False, True):
+        x = thor_b200.Thorx(grid_dict(g), GLEVEL, thorx_params(c, DT))
+        if reconfigure:
+            x.sponge(dict(nlat_bins=NLAT))
+            for k, v in st.items():
+                x.set(k, v)
+            x.step(2)
+            x.sync()
+        x.sponge(second)
+        for k, v in st.items():
+            x.set(k, v)
+        x.step(2)
+        x.sync()
+        outs.append((x.get("Mh"), x.sponge_means()[0]))
+        x.close()
+    g.close()
+    assert np.array_equal(outs[0][0], outs[1][0])
+    assert np.array_equal(outs[0][1], outs[1][1])

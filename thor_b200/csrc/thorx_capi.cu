@@ -96,6 +96,17 @@ template<class T> int dev_alloc(thorx_ctx* ctx, T** p, size_t n) {
     *p = (T*)d;
     return 0;
 }
+// Frees one allocation of dev_alloc before the context's end (null: nothing).
+void dev_free(thorx_ctx* ctx, const void* p) {
+    if (!p)
+        return;
+    for (size_t i = 0; i < ctx->allocs.size(); i++)
+        if (ctx->allocs[i] == p) {
+            cudaFree(ctx->allocs[i]);
+            ctx->allocs.erase(ctx->allocs.begin() + (long)i);
+            return;
+        }
+}
 
 // ref layout [N][L][K] <-> device layout [K][L][Np], through 32x32 shared-memory tiles of the
 // matrix view ref = [N rows][L*K columns].
@@ -1336,6 +1347,26 @@ int thorx_sponge_enable(thorx_ctx* ctx, const thorx_sponge_params* p) {
             return fail(ctx, THORX_E_ARG, "thorx_sponge_enable: ns_ray_sponge outside [0, 1)");
         if (p->raysp_calc_mode < 0 || p->raysp_calc_mode > 2)
             return fail(ctx, THORX_E_ARG, "thorx_sponge_enable: raysp_calc_mode not 0, 1 or 2");
+    }
+    // the step graph holds the previous set-up: drop it, then release that set-up's tables
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (ctx->graph_exec) {
+        CK(cudaGraphExecDestroy(ctx->graph_exec));
+        ctx->graph_exec = nullptr;
+    }
+    if (ctx->graph) {
+        CK(cudaGraphDestroy(ctx->graph));
+        ctx->graph = nullptr;
+    }
+    {
+        Sponge& old = ctx->sp;
+        for (const void* q : {(const void*)old.bin, (const void*)old.start, (const void*)old.members,
+                              (const void*)old.trig, (const void*)old.vbar, (const void*)old.Tbar,
+                              (const void*)old.step})
+            dev_free(ctx, q);
+        old = Sponge{};
+    }
+    if (p) {
         const int N = g.N, Np = g.Np, nv = g.nv, nlat = p->nlat_bins;
         // latitude bins as Icogrid::zonal_mean_tab_f (src/ESP/grid.cu:3203-3260): bin j holds
         // lat_array[j] <= lat < lat_array[j + 1], the edges accumulated from -pi/2 in steps of
@@ -1406,14 +1437,6 @@ int thorx_sponge_enable(thorx_ctx* ctx, const thorx_sponge_params* p) {
     // an explicit sponge leaves its tendencies in profx_dMh / profx_dWh: start from zero
     CK(cudaMemset(ctx->s.dMh, 0, sizeof(double) * 3 * g.nv * g.Np));
     CK(cudaMemset(ctx->s.dWh, 0, sizeof(double) * g.nvi * g.Np));
-    if (ctx->graph_exec) { // the captured step holds the previous set-up
-        CK(cudaGraphExecDestroy(ctx->graph_exec));
-        ctx->graph_exec = nullptr;
-    }
-    if (ctx->graph) {
-        CK(cudaGraphDestroy(ctx->graph));
-        ctx->graph = nullptr;
-    }
     return 0;
 }
 
