@@ -2299,7 +2299,7 @@ __global__ void THORX_KATTR_VERT
             double* sc = sCp;
             double* sd = sDp;
             double  cprev = 0, dprev = 0;
-#pragma unroll 4
+#pragma unroll 2
             for (int lev = 1; lev < nv; lev++) {
                 const int    q  = lev * Np + c;
                 const double aa = ra[q], bb = rb[q];
