@@ -373,6 +373,11 @@ int thorx_surrogate_gradients_host(thorx_ctx* ctx, const float* x, const float* 
  * addition is fixed: the same state gives the same bits on every call. Synchronises the
  * context's stream. */
 int thorx_globdiag(thorx_ctx* ctx, double* out);
+/* thorx_globdiag plus the per-cell terms the sums are made of, as the reference keeps them for its
+ * output files (Etotal_d, Mass_d, AngMomx_d, AngMomy_d, AngMomz_d, Entropy_d of CalcTotEnergy /
+ * CalcMass / CalcAngMom / CalcEntropy, src/ESP/profx_globdiag.cu:45-252): fields[q] (host, [col][lev],
+ * q in the order of out; NULL entries are skipped). */
+int thorx_globdiag_fields(thorx_ctx* ctx, double* out, double* const fields[6]);
 
 /* Compensated sum of n doubles in device memory of the current device
  * (replaces gpu_sum_on_device<1024>, src/headers/reduction_add.h:96-128). x must point into one

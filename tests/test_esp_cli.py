@@ -188,6 +188,8 @@ def test_run_outputs_logs_and_bitwise_continuation(tmp_path):
     assert final["Mh"][0].size == 3 * final["Rho"][0].size
     assert final["Rho"][1] == {"Variable": "Density", "units": "kg/m^3"}
     assert float(final["GlobalMass"][0][0]) == m1  # the file's global sums are the log's
+    assert final["Mass"][1] == {"Variable": "Mass", "units": "kg"}
+    assert abs(final["Mass"][0].sum() - m1) <= 1e-12 * m1  # the per-cell terms of that sum
     planet = h5.read(str(a / "esp_output_planet_TestHS.h5"))
     assert int(planet["glevel"][0][0]) == 4 and float(planet["A"][0][0]) == 6371000.0
     # run 2 steps, then continue from that output for the remaining 2

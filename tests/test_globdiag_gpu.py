@@ -42,8 +42,17 @@ def test_globdiag_matches_oracle_and_reference(glevel, nv, over):
         s.set(k, v)
     mine = np.array(x.globdiag())
     again = np.array(x.globdiag())
+    sums, cells = x.globdiag_fields()
     ref = s.globdiag()
+    # the per-cell terms against the reference's own arrays (CalcTotEnergy, CalcMass, CalcAngMom,
+    # CalcEntropy store them per cell for the output files)
+    names = ["Etotal", "Mass", "AngMomx", "AngMomy", "AngMomz", "Entropy"]
+    for q, n in enumerate(names):
+        r = s.get(n)
+        scale = np.abs(r).max()
+        assert np.abs(cells[q] - r).max() <= 1e-13 * scale, n
     x.close(), s.close(), o.close(), g.close()
+    assert np.array_equal(sums, mine)  # the same sums with the per-cell terms kept
     assert np.array_equal(mine, again), "globdiag is not deterministic"
     err = np.abs(mine - want) / mag
     err_ref = np.abs(ref - want) / mag

@@ -169,6 +169,9 @@ def lib():
         L.thorx_check_thomas.argtypes = [vp, ctypes.c_double, ctypes.POINTER(ctypes.c_double),
                                          ctypes.POINTER(ctypes.c_longlong)]
         L.thorx_check_thomas.restype = ci
+        L.thorx_globdiag_fields.argtypes = [vp, ctypes.POINTER(ctypes.c_double),
+                                            ctypes.POINTER(ctypes.c_void_p)]
+        L.thorx_globdiag_fields.restype = ci
         L.thorx_init_guillot_state.argtypes = [vp] + [ctypes.c_double] * 5 + [ctypes.c_ulonglong,
                                                                              ctypes.c_double]
         L.thorx_init_guillot_state.restype = ci
@@ -220,7 +223,7 @@ EXPORTED = ["thorx_create", "thorx_destroy", "thorx_last_error", "thorx_field_si
             "thorx_check_division", "thorx_conv_adj_enable", "thorx_init_guillot_state",
             "thorx_sponge_enable", "thorx_sponge_means", "thorx_module_add",
             "thorx_rk_register_array", "thorx_device_field", "thorx_vert_hydiff_enable",
-            "thorx_check_thomas"]
+            "thorx_check_thomas", "thorx_globdiag_fields"]
 
 def device_sum(ptr, n, stream=0):
     """Compensated sum of n doubles at device address `ptr` (thorx_device_sum)."""
@@ -442,6 +445,15 @@ class Thorx:
             return
         self._sponge = sponge_params(d)
         self._check(lib().thorx_sponge_enable(self.h, ctypes.byref(self._sponge)))
+
+    def globdiag_fields(self):
+        """(the six global sums, the six per-cell term arrays [col][lev]) of thorx_globdiag_fields."""
+        out = (ctypes.c_double * 6)()
+        n = self.size("Rho")
+        arrs = [np.zeros(n) for _ in range(6)]
+        ptrs = (ctypes.c_void_p * 6)(*[a.ctypes.data for a in arrs])
+        self._check(lib().thorx_globdiag_fields(self.h, out, ptrs))
+        return np.array(list(out)), arrs
 
     def check_thomas(self, epsilon=1e-8):
         """(largest relative residual, interfaces above epsilon) of the last vertical solve."""

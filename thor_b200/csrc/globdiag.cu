@@ -102,7 +102,8 @@ __global__ void __launch_bounds__(kSumThreads)
     globdiag_kernel(Geometry g, Phys P, const double* __restrict__ Rho,
                     const double* __restrict__ Mh, const double* __restrict__ W,
                     const double* __restrict__ T, const double* __restrict__ p,
-                    const double* __restrict__ Cp, const double* __restrict__ Rd, double2* part) {
+                    const double* __restrict__ Cp, const double* __restrict__ Rd, double2* part,
+                    double* __restrict__ cells) {
     __shared__ double2 sh[kSumThreads];
     const int          col = blockIdx.x * kSumThreads + threadIdx.x, lev = blockIdx.y;
     const int          Np = g.Np, nv = g.nv;
@@ -151,6 +152,10 @@ __global__ void __launch_bounds__(kSumThreads)
             term[5]      = Sdens * Vol;
         }
     }
+    if (cells && col < g.N) // the per-cell terms (the reference's Etotal_d, Mass_d, ... arrays)
+#pragma unroll
+        for (int q = 0; q < 6; q++)
+            cells[((size_t)q * nv + lev) * Np + col] = term[q];
     const int nblk = gridDim.x * gridDim.y, b = lev * gridDim.x + blockIdx.x;
 #pragma unroll
     for (int q = 0; q < 6; q++) {
@@ -165,10 +170,10 @@ __global__ void __launch_bounds__(kSumThreads)
 int globdiag_partials(const Geometry& g) { return ((g.N + kSumThreads - 1) / kSumThreads) * g.nv; }
 
 void launch_globdiag(const Geometry& g, const Phys& P, const State& s, double2* part, double* out6,
-                     cudaStream_t st) {
+                     cudaStream_t st, double* cells) {
     dim3 grid((g.N + kSumThreads - 1) / kSumThreads, g.nv);
     globdiag_kernel<<<grid, kSumThreads, 0, st>>>(g, P, s.Rho, s.Mh, s.W, s.T, s.p, s.Cp, s.Rd,
-                                                  part);
+                                                  part, cells);
     const int nblk = (int)(grid.x * grid.y);
     sum_final_kernel<<<6, kFinalThreads, 0, st>>>(part, nblk, nblk, out6);
 }

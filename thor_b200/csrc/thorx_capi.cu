@@ -1749,6 +1749,35 @@ int thorx_globdiag(thorx_ctx* ctx, double* out) {
     return 0;
 }
 
+int thorx_globdiag_fields(thorx_ctx* ctx, double* out, double* const fields[6]) {
+    if (!ctx)
+        return THORX_E_ARG;
+    if (!out || !fields)
+        return fail(ctx, THORX_E_ARG, "thorx_globdiag_fields: null argument");
+    if (!ctx->state_set)
+        return fail(ctx, THORX_E_STATE, "thorx_globdiag_fields: the state has not been set");
+    // the hyperdiffusion scratch (12 cell planes, idle between steps) holds the six planes
+    double* cells = ctx->s.diff;
+    launch_globdiag(ctx->g, ctx->P, ctx->s, ctx->gd_part, ctx->gd_out, ctx->stream, cells);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, ctx->gd_out, 6 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    const int    N = ctx->g.N, Np = ctx->g.Np, nv = ctx->g.nv;
+    const size_t plane = (size_t)nv * Np;
+    dim3         grid((N + 31) / 32, (nv + 31) / 32), block(32, 8);
+    for (int q = 0; q < 6; q++) {
+        if (!fields[q])
+            continue;
+        dev_to_ref_kernel<<<grid, block, 0, ctx->stream>>>(cells + q * plane, ctx->staging, N, Np,
+                                                          nv, 1);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(fields[q], ctx->staging, (size_t)N * nv * sizeof(double),
+                           cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream)); // the staging buffer is reused by the next plane
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
 int thorx_device_sum(const double* x, long long n, void* stream, double* out) {
     int rc = check_sum_args("thorx_device_sum", x, n, out);
     if (rc || n == 0)

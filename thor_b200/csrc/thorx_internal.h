@@ -256,8 +256,10 @@ void launch_rt(const Geometry& g, const Phys& P, const RtConst& c, const RtField
 int  globdiag_partials(const Geometry& g);
 // Energy, mass, AMx, AMy, AMz, entropy of the current state into out6 (device), using
 // 6 * globdiag_partials(g) double2 of scratch at part.
+// cells (optional): the six per-cell terms, six cell planes (energy, mass, AMx, AMy, AMz,
+// entropy).
 void launch_globdiag(const Geometry& g, const Phys& P, const State& s, double2* part, double* out6,
-                     cudaStream_t st);
+                     cudaStream_t st, double* cells = nullptr);
 // Partials a compensated sum of n doubles writes.
 long long device_sum_partials(long long n);
 // Compensated sum of x[0..n-1] (device) into *out (device), device_sum_partials(n) double2 of

@@ -16,9 +16,8 @@ Differences, each stated where it applies:
   * output files are HDF5 with the reference's file names, dataset names, units and descriptions
     and memory layout ([column][level][component]) (src/ESP/esp_output.cu:136-487), written and read
     by thor_b200/h5.py (there is no HDF5 library here); the grid file lacks the curl operator (not
-    built here), the output files lack the per-cell global-diagnostic arrays (their global sums are
-    written) and the RT's Qheat scaling; restart files may also be the .npz archives of earlier
-    versions of this runner;
+    built here) and the output files the RT's Qheat scaling; restart files may also be the .npz
+    archives of earlier versions of this runner;
   * keys for physics that this build does not implement (the diffusive sponge, the RayPH
     convective adjustment, chemistry, boundary layer, ultra-hot thermodynamics, refined vertical grids,
     picket-fence or two-stream RT, the Parmentier and constant-N initial profiles) are accepted at
@@ -343,7 +342,7 @@ def _atomic_h5(path):
     return h5.H5Writer(path + ".tmp")
 
 
-def write_state(path, x, nstep, sim_time, c, glob=None, rt=None):
+def write_state(path, x, nstep, sim_time, c, glob=None, rt=None, cells=None):
     """ESP::output's state file (src/ESP/esp_output.cu:306-470) and the RT module's and the
     insolation's store() (radiative_transfer.cu:1286-1336, insolation.cu:484-493)."""
     w = _atomic_h5(path)
@@ -353,6 +352,13 @@ def write_state(path, x, nstep, sim_time, c, glob=None, rt=None):
     w.table("/Pressure", x.get("pressure"), "Pa", "Pressure")
     w.table("/Mh", x.get("Mh"), "kg m^-2 s^-1", "Horizontal Momentum")
     w.table("/Wh", x.get("Wh"), "kg m^-2 s^-1", "Vertical Momentum")
+    if cells is not None:  # the per-cell terms of the global sums (esp_output.cu:410-428)
+        w.table("/Etotal", cells[0], "kg m^2/s^2", "Total Energy")
+        w.table("/Entropy", cells[5], "kg m^2/s^2 K^-1", "Entropy")
+        w.table("/Mass", cells[1], "kg", "Mass")
+        w.table("/AngMomx", cells[2], "kg m^2/s", "AngMom in X")
+        w.table("/AngMomy", cells[3], "kg m^2/s", "AngMom in Y")
+        w.table("/AngMomz", cells[4], "kg m^2/s", "AngMom in Z")
     if glob is not None:
         E, M, AMx, AMy, AMz, Ent = glob
         w.value("/GlobalE", E, "kg m^2/s^2", "Global Total Energy")
@@ -760,8 +766,8 @@ def run(argv=None, out=sys.stdout):
         rt_tot = (lambda: x.rt_totals()) if c["radiative_transfer"] else (lambda: None)
         if not continuing:
             name = output_name(sim_id, 0)
-            write_state(os.path.join(out_dir, name), x, 0, sim_time0, c,
-                        x.globdiag() if c["globdiag"] else None, rt_tot())
+            g0, cells0 = x.globdiag_fields() if c["globdiag"] else (None, None)
+            write_state(os.path.join(out_dir, name), x, 0, sim_time0, c, g0, rt_tot(), cells0)
             logs.output(0, 0, name)
             first_idx = 1
         del _caught[:]
@@ -786,12 +792,16 @@ def run(argv=None, out=sys.stdout):
             x.sync()
             nstep = nxt
             sim_time = sim_time0 + (nstep - step_idx + 1) * dt
-            glob = x.globdiag() if c["globdiag"] else None
+            writing = nstep % n_out == 0 or bool(_caught)
+            glob, cells = None, None
+            if c["globdiag"]:
+                glob, cells = x.globdiag_fields() if writing else (x.globdiag(), None)
             if c["globdiag"] and nstep % g_out == 0:
                 logs.globdiag(nstep, sim_time, glob)
-            if nstep % n_out == 0 or _caught:
+            if writing:
                 name = output_name(sim_id, idx)
-                write_state(os.path.join(out_dir, name), x, nstep, sim_time, c, glob, rt_tot())
+                write_state(os.path.join(out_dir, name), x, nstep, sim_time, c, glob, rt_tot(),
+                            cells)
                 logs.output(nstep, idx, name)
                 idx += 1
             elapsed = time.time() - t0
