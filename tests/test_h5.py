@@ -162,3 +162,23 @@ def test_planet_file_of_a_configuration(tmp_path):
     # the names the reference's planet file has are all there
     ref = h5.read(golden("planet_earth_g5L20.h5"))
     assert set(ref) <= set(d), set(ref) - set(d)
+
+
+def test_reader_rejects_what_it_does_not_read(tmp_path):
+    """Files that are not HDF5, or of a layout outside the one the reference writes, fail with
+    H5FormatError instead of returning wrong data."""
+    bad = tmp_path / "x.h5"
+    bad.write_bytes(b"not an hdf5 file at all" * 8)
+    with pytest.raises(h5.H5FormatError):
+        h5.read(str(bad))
+    data = bytearray(open(golden("planet_earth_hs_g4L32.h5"), "rb").read())
+    v2 = bytearray(data)
+    v2[8] = 2                                  # a version-2 superblock
+    (tmp_path / "v2.h5").write_bytes(bytes(v2))
+    with pytest.raises(h5.H5FormatError):
+        h5.read(str(tmp_path / "v2.h5"))
+    sizes = bytearray(data)
+    sizes[13] = 4                              # 4-byte offsets
+    (tmp_path / "s4.h5").write_bytes(bytes(sizes))
+    with pytest.raises(h5.H5FormatError):
+        h5.read(str(tmp_path / "s4.h5"))
