@@ -170,7 +170,7 @@ def ncu_traffic(kernel):
                                          / ((2 + 10 * 4 ** d["glevel"]) * d["nv"]))
 
 
-def cpu_baseline(grid, nsteps):
+def cpu_baseline(grid, nsteps, warmup=1):
     """The CPU restatement of the same step (oracle/) on all host cores, bounded sample."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from thorx_testlib import Oracle, make_params, oracle_lib
@@ -181,15 +181,25 @@ def cpu_baseline(grid, nsteps):
     st = initial_state_host(grid)
     for k, v in st.items():
         o.set(k, v)
-    o.step(1)  # warm-up
+    if warmup:
+        o.step(warmup)
     t0 = time.perf_counter()
     o.step(nsteps)
     sec = time.perf_counter() - t0
     o.close()
     return dict(value=sim_days_per_hour(nsteps, sec), unit="sim-days/wall-hour", cores=threads,
                 kind="port", seconds=sec,
-                sample="%d large steps of the g%d/L%d Held-Suarez step (after 1 warm-up), "
-                       "oracle/thor_oracle.cpp, OpenMP over columns" % (nsteps, GLEVEL, NV))
+                sample="%d large steps of the g%d/L%d Held-Suarez step (after %d warm-up), "
+                       "oracle/thor_oracle.cpp, OpenMP over columns" % (nsteps, GLEVEL, NV, warmup))
+
+
+def bench_config(form, world):
+    """The config dict of both arms' JSON lines (the same workload, the same keys)."""
+    n = 2 + 10 * 4 ** GLEVEL
+    return {"workload": workload_name(), "glevel": GLEVEL, "nv": NV, "dt": DT, "form": form,
+            "parallelism": "replicas%d" % world,
+            "l2": "state resident in HBM (%.3f GB per level-field x ~40 fields), far above the "
+                  "126 MB L2: no flush needed" % (n * NV * 8 / 1e9)}
 
 
 def initial_state_host(grid):
@@ -201,22 +211,30 @@ def initial_state_host(grid):
     return initial_state(grid.arrays, grid.point_num, grid.nv, c, seed=SEED, amp=NOISE)
 
 
+def reference_grid():
+    """The reference's own grid builder (Icogrid, src/ESP/grid.cu, compiled into oracle/_ref),
+    so that the reference arm maps none of the product's code."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from thorx_testlib import RefGrid
+    return RefGrid(GLEVEL, NV, A=EARTH["A"], top=EARTH["Top_altitude"])
+
+
 def run_reference(args):
-    world, rank, local = dist_setup()
-    if rank != 0:
-        return 0
-    grid = grid_for_bench()
-    base = cpu_baseline(grid, max(1, min(args.steps, 3)))
-    # each reference step is a bounded sample: steps x (time of one step)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0  # rank 0 alone runs the reference arm
+    grid = reference_grid()
+    # all K steps are timed (after W warm-up steps): each is one whole large step on the CPU
+    base = cpu_baseline(grid, args.steps, warmup=args.warmup)
     value = base["value"]
     ref_cuda = reference_cuda(grid, args)
+    grid.close()
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "sim-days/wall-hour",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": base["seconds"] * 1000.0 / max(1, min(args.steps, 3)),
+            "ms_per_step": base["seconds"] * 1000.0 / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded rest state)",
-            "config": {"workload": workload_name(),
-                       "glevel": GLEVEL, "nv": NV, "dt": DT, "form": "fp64"},
+            "data": "synthetic (seeded isothermal rest state, Held-Suarez forcing)",
+            "config": bench_config("fp64", world),
             "cpu_baseline": {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": value, "unit": "sim-days/wall-hour", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
@@ -456,11 +474,7 @@ def run_ours(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if args.form == "fp64" else "f32+f64",
             "data": "synthetic (seeded isothermal rest state, Held-Suarez forcing)",
-            "config": {"workload": workload_name(),
-                       "glevel": GLEVEL, "nv": NV, "dt": DT, "form": args.form,
-                       "parallelism": "replicas%d" % world,
-                       "l2": "state resident in HBM (%.2f GB per level-field x ~40 fields), "
-                             "far above the 126 MB L2: no flush needed" % (x.size("Rho") * 8 / 1e9)},
+            "config": bench_config(args.form, world),
             "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": ncu_traffic(name),

@@ -2,6 +2,7 @@
 this directory as golden fixtures for thor_b200/h5.py, and records their SHA-256 in MANIFEST.
 
     python tests/golden/h5/make_fixtures.py /path/to/reference
+    THOR_REFERENCE_DIR=/path/to/reference python tests/golden/h5/make_fixtures.py
 
 The files are data, written by the reference's bin/esp for three configurations (an Earth
 Held-Suarez run at glevel 4 / 32 levels, a deep hot-Jupiter set-up and an Earth set-up at
@@ -32,4 +33,7 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("THOR_REFERENCE_DIR")
+    if not ref:
+        sys.exit("usage: make_fixtures.py REFERENCE_DIR (or set THOR_REFERENCE_DIR)")
+    main(ref)

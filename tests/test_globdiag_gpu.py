@@ -134,3 +134,30 @@ def test_device_sum_rejects_bad_arguments_before_any_launch():
         assert e.value.code == thor_b200.E_ARG, (what, str(e.value))
     # the context is still healthy
     assert thor_b200.device_sum(xd.data_ptr(), 1000) == 1000.0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [thor_b200.FP64, thor_b200.MIXED])
+def test_globdiag_fields_leaves_the_next_steps_unchanged(precision):
+    """thorx_globdiag_fields computes its per-cell planes in the hyperdiffusion work buffer; the
+    steps after it must give the same bits as steps that never saw the call."""
+    glevel, nv, dt = 4, 16, 1200.0
+    g = RefGrid(glevel, nv)
+    p, c = make_params(glevel, dt)
+    ic = initial_state(g.arrays, g.point_num, nv, c)
+    out = []
+    for call in (False, True):
+        x = thor_b200.Thorx(grid_dict(g), glevel, thorx_params(c, dt, precision=precision))
+        for k, v in ic.items():
+            x.set(k, v)
+        x.step(2)
+        if call:
+            sums, cells = x.globdiag_fields()
+            assert np.all(np.isfinite(sums)) and all(np.all(np.isfinite(v)) for v in cells)
+        x.step(3)
+        x.sync()
+        out.append({f: x.get(f) for f in ["Rho", "pressure", "Mh", "Wh", "W"]})
+        x.close()
+    g.close()
+    for f in out[0]:
+        assert np.array_equal(out[0][f], out[1][f]), f

@@ -10,7 +10,9 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libthorx.so")
+# THORX_LIB selects another build of the same ABI (e.g. libthorx_reforder.so, the FP64 form with
+# the reference's operation order in the hyperdiffusion and divergence damping)
+LIB_PATH = os.environ.get("THORX_LIB") or os.path.join(HERE, "libthorx.so")
 
 FP64, MIXED = 0, 1
 ENTROPY, ENERGY = 0, 1
@@ -106,7 +108,7 @@ def lib():
     global _lib
     if _lib is None:
         if not os.path.exists(LIB_PATH):
-            raise RuntimeError("thor_b200/libthorx.so is missing: run `python -m thor_b200.build`")
+            raise RuntimeError("%s is missing: run `python -m thor_b200.build`" % LIB_PATH)
         L = ctypes.CDLL(LIB_PATH)
         vp, cp, ci = ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int
         L.thorx_create.argtypes = [ctypes.POINTER(GridC), ctypes.POINTER(ParamsC), vp,

@@ -21,6 +21,7 @@
 // Stencils are templated on the ring size (6, or 5 at pentagons and poles) so that every index
 // is static and the ring values stay in registers.
 
+#include <mutex>
 #include <type_traits>
 
 #include "thorx.h"
@@ -2645,17 +2646,27 @@ void launch_momentum(const Geometry& g, const Phys& P, const State& s, double dt
 size_t vertical_smem_bytes(const Geometry& g) { return sizeof(double) * kTile * (21 + 4 * g.nv); }
 
 // The largest dynamic shared memory a kernel has been opened to, per device (the attribute is a
-// per-device setting; a process may hold contexts on several devices).
+// per-device setting; a process may hold contexts on several devices, and host threads may launch
+// concurrently). A size is recorded only once the driver has accepted it; a refusal is returned
+// (and stays the runtime's last error, which the caller's error check reports), and the next
+// launch asks again.
 constexpr int kMaxDevices = 64;
 struct SmemOptIn {
-    size_t bytes[kMaxDevices] = {};
-    bool   need(size_t smem) {
+    std::mutex mu;
+    size_t     bytes[kMaxDevices] = {};
+    template<class Kernel>
+    cudaError_t ensure(Kernel* kernel, size_t smem) {
         int dev = 0;
-        cudaGetDevice(&dev);
-        if (dev < 0 || dev >= kMaxDevices || smem <= bytes[dev])
-            return dev < 0 || dev >= kMaxDevices; // unknown device: set it every time
-        bytes[dev] = smem;
-        return true;
+        if (cudaGetDevice(&dev) != cudaSuccess)
+            dev = -1;
+        std::lock_guard<std::mutex> lock(mu);
+        if (dev >= 0 && dev < kMaxDevices && smem <= bytes[dev])
+            return cudaSuccess;
+        const cudaError_t e =
+            cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e == cudaSuccess && dev >= 0 && dev < kMaxDevices)
+            bytes[dev] = smem;
+        return e;
     }
 };
 template<int kPart>
@@ -2663,9 +2674,8 @@ void launch_vertical_part(const Geometry& g, const Phys& P, const State& s, doub
                           cudaStream_t st) {
     const size_t     smem = vertical_smem_bytes(g);
     static SmemOptIn opt;
-    if (opt.need(smem))
-        cudaFuncSetAttribute(vertical_kernel<kPart>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem);
+    if (opt.ensure(vertical_kernel<kPart>, smem) != cudaSuccess)
+        return;
     vertical_kernel<kPart><<<tile_grid(g), tile_block(), smem, st>>>(g, P, s, dt);
 }
 void launch_vertical(const Geometry& g, const Phys& P, const State& s, double dt, int part,
@@ -2737,9 +2747,8 @@ void launch_rk_arrays(const RkArrays& t, int mode, cudaStream_t st) {
 void launch_vertical_diff(const Geometry& g, const Phys& P, const State& s, cudaStream_t st) {
     const size_t  smem       = sizeof(double) * kVdCols * (2 * g.nv + 2);
     static SmemOptIn opt;
-    if (opt.need(smem))
-        cudaFuncSetAttribute(vertical_diff_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem);
+    if (opt.ensure(vertical_diff_kernel, smem) != cudaSuccess)
+        return;
     vertical_diff_kernel<<<(g.N + kVdCols - 1) / kVdCols, kVdCols, smem, st>>>(g, P, s);
 }
 void launch_update_rk2(const Geometry& g, const Phys& P, const State& s, cudaStream_t st) {

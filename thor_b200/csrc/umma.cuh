@@ -12,6 +12,7 @@
 #pragma once
 
 #include <cstdint>
+#include <mutex>
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -418,14 +419,26 @@ inline bool make_kmajor_map(CUtensorMap* map, const void* ptr, int rows, int K, 
 template<int BN, int EPI>
 inline void gemm_tma(const __nv_bfloat16* A, const __nv_bfloat16* B, int M, int N, int K,
                      const EpiArgs& e, unsigned int* err, cudaStream_t st, int splits = 1) {
-    static bool configured[64] = {}; // the attribute is per device
-    int         dev            = 0;
-    cudaGetDevice(&dev);
-    if (dev < 0 || dev >= 64 || !configured[dev]) {
-        cudaFuncSetAttribute(gemm_tma_kernel<BN, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)gemm_tma_smem_bytes(BN));
-        if (dev >= 0 && dev < 64)
-            configured[dev] = true;
+    // the attribute is per device; recorded only once the driver accepted it, under a lock (host
+    // threads may launch concurrently); a refusal sets *err and launches nothing
+    static std::mutex mu;
+    static bool       configured[64] = {};
+    {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess)
+            dev = -1;
+        std::lock_guard<std::mutex> lock(mu);
+        if (dev < 0 || dev >= 64 || !configured[dev]) {
+            if (cudaFuncSetAttribute(gemm_tma_kernel<BN, EPI>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)gemm_tma_smem_bytes(BN))
+                != cudaSuccess) {
+                cudaMemsetAsync(err, 0xFF, sizeof(unsigned int), st);
+                return;
+            }
+            if (dev >= 0 && dev < 64)
+                configured[dev] = true;
+        }
     }
     CUtensorMap ma, mb;
     if (!make_kmajor_map(&ma, A, M, K, kM) || !make_kmajor_map(&mb, B, N, K, BN)) {
