@@ -24,7 +24,7 @@ CASES = [(4, 16, 1200.0, {}), (5, 16, 600.0, dict(DivDampP=0)),
 
 
 def child():
-    sys.path.insert(0, HERE)
+    sys.path[:0] = [ROOT, HERE]
     from test_dycore_parity_gpu import run_case
     out = [run_case(*c) for c in CASES]
     print("RESULT " + json.dumps(out))
@@ -34,7 +34,8 @@ def child():
 def test_reference_operation_order_build_matches_reference():
     from thorx_testlib import field_tolerance
     assert os.path.exists(VARIANT), "build thor_b200 first (python -m thor_b200.build)"
-    env = dict(os.environ, THORX_LIB=VARIANT)
+    env = dict(os.environ, THORX_LIB=VARIANT,
+               PYTHONPATH=os.pathsep.join([ROOT, HERE, os.environ.get("PYTHONPATH", "")]))
     r = subprocess.run([sys.executable, os.path.abspath(__file__), "--child"], env=env,
                        capture_output=True, text=True, timeout=900, cwd=ROOT)
     assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
