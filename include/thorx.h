@@ -202,6 +202,17 @@ int thorx_module_add(thorx_ctx* ctx, const thorx_module* m);
  * dimensions * nv * plane doubles (plane from thorx_device_field). At most 10 arrays. */
 int thorx_rk_register_array(thorx_ctx* ctx, double* array, double* arrayk, double* arrayi,
                             int dimensions);
+/* The same registry for arrays of any layout: the RK stages update `count` doubles of each array
+ * elementwise (for a module that keeps its arrays in the reference layout, [col][lev][dim] of
+ * point_num * nv * dimensions doubles; the register_array of the thorx_phy shim,
+ * thor_b200/phy/). At most 10 arrays in all. */
+int thorx_rk_register_array_n(thorx_ctx* ctx, double* array, double* arrayk, double* arrayi,
+                              long long count);
+/* use_graph = 0: thorx_step enqueues every step's kernels and calls every module hook each step,
+ * instead of capturing the step once as a CUDA graph and replaying it; for modules whose hooks do
+ * host work or launch on the legacy default stream (the reference's phy_modules_* managers through
+ * the thorx_phy shim). 1 (the default) restores graph replay. */
+int thorx_set_graph_mode(thorx_ctx* ctx, int use_graph);
 /* The context's device array of a field, for module kernels: *dev, its levels (nv or nv+1), its
  * components (1 or 3) and the plane stride (doubles): element (lev, col, comp) is at
  * dev[(comp * levels + lev) * plane + col]. Names: the thorx_get_field names and the dycore's

@@ -21,6 +21,7 @@
 // Stencils are templated on the ring size (6, or 5 at pentagons and poles) so that every index
 // is static and the ring values stay in registers.
 
+#include <algorithm>
 #include <mutex>
 #include <type_traits>
 
@@ -266,6 +267,9 @@ __global__ void level_tables_kernel(Geometry g, Phys P, double* lt) {
         lt[kLtGhv * nvi + i]    = pow(A / (A + Alt[i]), 2);
         lt[kLtCIntt * nvi + i]  = (Alt[i] - Alth[i + 1]) / (Alth[i] - Alth[i + 1]);
         lt[kLtCIntl * nvi + i]  = (Alt[i] - Alth[i]) / (Alth[i + 1] - Alth[i]);
+        lt[kLtRDz * nvi + i]    = 1.0 / (Alth[i + 1] - Alth[i]);
+        lt[kLtRDr2dz * nvi + i] = 1.0 / lt[kLtDr2dz * nvi + i];
+        lt[kLtRDzR2m * nvi + i] = 1.0 / ((Alth[i + 1] - Alth[i]) * lt[kLtR2cD * nvi + i]);
     }
 }
 
@@ -2123,17 +2127,328 @@ __global__ void __launch_bounds__(kVdCols) vertical_diff_kernel(Geometry g, Phys
 // update, reading the Whs a part-1 launch wrote). Parts 1 and 2 bracket a physics module's
 // fast-mode hook, which the reference calls between Vertical_Eq and Density_Pressure_Eqs
 // (src/ESP/thor_driver.cu:1222-1304); they compute what the fused kernel computes, value for value.
+//
+// Shared memory, [quantity][32 columns]: the div stencil (21 rows), then four nv-row arrays.
+// kVertMerge (the default): one gather pass per level computes Prepare_Implicit_Vertical's Sp and
+// Sd and Density_Pressure_Eqs' horizontal flux divergences Fr and Fpt together (Mhs is gathered
+// once for both; Sd's flux term is exactly -Fr: the same products summed in the same order,
+// negated); the arrays are Sp, Sd, Fr, Fpt, and the Thomas sweep writes its eliminated
+// coefficients over Sp and Sd, which the rows no longer need. Without kVertMerge the flux
+// divergences are gathered by warps 1-7 while warp 0 solves, into the Sp/Sd arrays, and the
+// eliminated coefficients have arrays of their own.
+#ifndef THORX_VERT_MERGE
+#define THORX_VERT_MERGE 1
+#endif
+#ifndef THORX_VERT_PF
+#define THORX_VERT_PF 4
+#endif
+#ifndef THORX_VERT_SMEM
+#define THORX_VERT_SMEM 2
+#endif
+constexpr bool kVertMerge = THORX_VERT_MERGE != 0;
+// Where the per-level work arrays live: 2 all in shared memory; 1 Sp and Sd in shared memory, Fr,
+// Fpt and the eliminated coefficients in global scratch planes; 0 all in global scratch (shared
+// memory holds the div stencil only, and the rest of the SM's 256 KB serves as L1 for the gathers).
+constexpr int kVertSmem = THORX_VERT_SMEM;
+
+// One per-level array of a tile: element lev of column lane x at p[lev * ld + ci] (shared memory:
+// ld 32, ci the lane; a global scratch plane set: ld Np, ci the column).
+struct LevArr {
+    double* p;
+    int     ld, ci;
+    __device__ double& operator[](int lev) const { return p[(size_t)lev * ld + ci]; }
+};
+constexpr int  kThomasPf  = THORX_VERT_PF; // rows loaded ahead of the elimination (0: none)
+constexpr int  kVertPre   = 8;             // levels whose pressure factor warps 1-7 precompute
+
+// The 7-point gathers of one level (rows of sdiv: point j, component k at (j * 3 + k)).
+// kSpSd: Sp and Sd of Prepare_Implicit_Vertical (thor_vertical_int.h:566-771);
+// kFlux: rscale div(Mhs) and rscale div((Mhs + Mhk) pt) (or the energy form's h + ep + ek) of
+// Density_Pressure_Eqs (thor_fastmodes.h:255-847). Each sum runs over the points in the
+// reference's order.
+template<bool kSpSd, bool kFlux>
+__device__ __forceinline__ void vert_gathers(const Geometry& g, const Phys& P, const State& s,
+                                             const double* sdiv, const int* nb, int c, int lev,
+                                             double& Sp, double& Sd, double& Fr, double& Fpt) {
+    const int     Np = g.Np, nv = g.nv, x = threadIdx.x;
+    const bool    eeq    = P.energy;
+    const double  rscale = g.lt[kLtRscale * g.nvi + lev]; // 1 in the shallow model
+    double        sdv[3], spv[3], st[3];
+    const double* h   = s.h + lev * Np;
+#pragma unroll
+    for (int j = 0; j < 7; j++) {
+        const int id = nb[j];
+        double    hv = 0.0, ms[3] = {0.0, 0.0, 0.0}, v1[3] = {0.0, 0.0, 0.0}, ptv = 0.0;
+        if (id >= 0) {
+            const int q = lev * Np + id;
+            if (kSpSd || (kFlux && eeq))
+                hv = h[id];
+#pragma unroll
+            for (int k = 0; k < 3; k++)
+                ms[k] = s.Mhs[(k * nv + lev) * Np + id];
+            if (kFlux) {
+#pragma unroll
+                for (int k = 0; k < 3; k++)
+                    v1[k] = ms[k] + s.Mhk[(k * nv + lev) * Np + id];
+                ptv = eeq ? (hv + s.ep[q] + s.ek[q]) : s.pt[q];
+            }
+        }
+        // explicit roundings: the fused and the split launches (and every instantiation) give the
+        // same bits whatever the compiler would contract
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const double d  = sdiv[(j * 3 + k) * kTile + x];
+            const double dm = __dmul_rn(d, ms[k]);
+            if (j == 0) {
+                sdv[k] = dm;
+                if (kSpSd)
+                    spv[k] = __dmul_rn(dm, hv);
+                if (kFlux)
+                    st[k] = __dmul_rn(__dmul_rn(d, v1[k]), ptv);
+            }
+            else {
+                sdv[k] = __dadd_rn(sdv[k], dm);
+                if (kSpSd)
+                    spv[k] = __fma_rn(dm, hv, spv[k]);
+                if (kFlux)
+                    st[k] = __fma_rn(__dmul_rn(d, v1[k]), ptv, st[k]);
+            }
+        }
+    }
+    double fr = 0.0, fpt = 0.0;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        fr = __fma_rn(rscale, sdv[k], fr);
+        if (kFlux)
+            fpt = __fma_rn(rscale, st[k], fpt);
+    }
+    Fr  = fr;
+    Fpt = fpt;
+    if (kSpSd) {
+        const int    i   = lev * Np + c;
+        const double RoC = s.Rd[i] / (s.Cp[i] - s.Rd[i]);
+        double       nflxp = 0.0;
+#pragma unroll
+        for (int k = 0; k < 3; k++)
+            nflxp = __fma_rn(-__dmul_rn(RoC, rscale), spv[k], nflxp);
+        Sp = nflxp + s.Slowp[i];
+        Sd = __dadd_rn(-fr, s.SlowRho[i]);
+    }
+}
+
+// x^y of the entropy form's pressure update. THORX_VPOW_EXPLOG=1 evaluates it as exp(y log x)
+// with CUDA's exp and log (inlined, within a few ulp of pow) instead of pow.
+#ifndef THORX_VPOW_EXPLOG
+#define THORX_VPOW_EXPLOG 0
+#endif
+__device__ __forceinline__ double vpow(double x, double y) {
+#if THORX_VPOW_EXPLOG
+    return exp(y * log(x));
+#else
+    return pow(x, y);
+#endif
+}
+
+// The entropy form's potential-temperature factor of Density_Pressure_Eqs at (c, lev): ptc =
+// (P_Ref / (Rd r)) (p / P_Ref)^(Cv / Cp) with the state before the update. It does not depend on
+// the vertical solve, so warps 1-7 evaluate it while warp 0 runs the Thomas sweep.
+__device__ __forceinline__ double vert_ptc(const Phys& P, const State& s, int i) {
+    const double Cv = s.Cp[i] - s.Rd[i];
+    const double r  = s.Rhok[i] + s.Rhos[i];
+    return (P.P_Ref / (s.Rd[i] * r)) * vpow(div_rcp(s.ps[i] + s.pk[i], P.P_Ref, P.rP_Ref), Cv / s.Cp[i]);
+}
+
+// Density_Pressure_Eqs at (c, lev): the vertical flux terms from the solved Whs, the update of
+// Rhos and ps (thor_fastmodes.h:255-847). Divisions by level constants go through div_rcp with
+// tabulated reciprocals (the IEEE quotients). ptc_pre: vert_ptc's value if precomputed.
+__device__ __forceinline__ void vert_update(const Geometry& g, const Phys& P, const State& s,
+                                            double deltat, int c, int lev, bool pole,
+                                            double nflxr, double nflxpt, const double* ptc_pre) {
+    const int     Np = g.Np, nvi = g.nvi, nv = g.nv;
+    const double* lt   = g.lt;
+    const double* Alt  = g.Altitude;
+    const double* Alth = g.Altitudeh;
+    const bool    deep = P.DeepModel, eeq = P.energy, ghv = P.GravHeightVar;
+    const int     i    = lev * Np + c;
+    const double  Cv   = s.Cp[i] - s.Rd[i];
+    const double  dz   = Alth[lev + 1] - Alth[lev];
+    double        r2p, r2m, r2l, dr2dz, rdr2dz, rdzr2m;
+    if (deep) {
+        r2p    = lt[kLtR2hD * nvi + lev + 1];
+        r2m    = lt[kLtR2cD * nvi + lev];
+        r2l    = lt[kLtR2hD * nvi + lev];
+        dr2dz  = lt[kLtDr2dz * nvi + lev];
+        rdr2dz = lt[kLtRDr2dz * nvi + lev];
+        rdzr2m = lt[kLtRDzR2m * nvi + lev];
+    }
+    else {
+        r2p = r2m = r2l = 1.0;
+        dr2dz           = r2m * dz;
+        rdr2dz = rdzr2m = lt[kLtRDz * nvi + lev]; // dz r2m = dz exactly
+    }
+    auto phv = [&](int l) -> double {
+        const int q = l * Np + c;
+        return eeq ? (s.hh[q] + s.eph[q] + s.ekh[q]) : s.pth[q];
+    };
+    double whl, wht, whl2, wht2, phl, pht;
+    if (lev == 0) {
+        whl  = 0.0;
+        wht  = s.Whs[(lev + 1) * Np + c];
+        whl2 = 0.0;
+        wht2 = wht + s.Whk[(lev + 1) * Np + c];
+        phl  = 0.0;
+        pht  = phv(lev + 1);
+    }
+    else {
+        whl  = s.Whs[lev * Np + c];
+        wht  = s.Whs[(lev + 1) * Np + c];
+        whl2 = whl + s.Whk[lev * Np + c];
+        wht2 = wht + s.Whk[(lev + 1) * Np + c];
+        phl  = phv(lev);
+        pht  = phv(lev + 1);
+    }
+    const double dwdz   = pole ? div_rcp(wht * r2p - whl * r2l, dz * r2m, rdzr2m)
+                               : div_rcp(wht * r2p - whl * r2l, dr2dz, rdr2dz);
+    const double dwptdz = div_rcp(wht2 * pht * r2p - whl2 * phl * r2l, dz * r2m, rdzr2m);
+    double       aux    = -(nflxpt + dwptdz) * deltat;
+    const double rk_    = s.Rhok[i];
+    const double rs     = s.Rhos[i];
+    const double r      = rk_ + rs;
+    // the entropy form's factor from the state before the update (Rhos is overwritten next)
+    const double ptc = eeq ? 0.0 : (ptc_pre ? *ptc_pre : vert_ptc(P, s, i));
+    nflxr += dwdz;
+    const double rhos_new = rs + (s.SlowRho[i] - nflxr) * deltat;
+    s.Rhos[i]             = rhos_new;
+    if (eeq) {
+        const double Gravit = P.Gravit;
+        aux += s.Etotal[i] + (s.diffpr[i]) * deltat + s.Qheat[i] * deltat;
+        s.Etotal[i] = aux;
+        const double m0 = s.Mhs[(0 * nv + lev) * Np + c] + s.Mhk[(0 * nv + lev) * Np + c];
+        const double m1 = s.Mhs[(1 * nv + lev) * Np + c] + s.Mhk[(1 * nv + lev) * Np + c];
+        const double m2 = s.Mhs[(2 * nv + lev) * Np + c] + s.Mhk[(2 * nv + lev) * Np + c];
+        const double w  = div_rcp(whl2 * (Alth[lev + 1] - Alt[lev]) + wht2 * (Alt[lev] - Alth[lev]),
+                                  Alth[lev + 1] - Alth[lev], lt[kLtRDz * nvi + lev]);
+        double Epot_kin;
+        if (ghv)
+            Epot_kin = (rhos_new + rk_) * Gravit * lt[kLtGhv * nvi + lev] * Alt[lev]
+                       + 0.5 * (pow(m0, 2) + pow(m1, 2) + pow(m2, 2) + pow(w, 2)) / (rhos_new + rk_);
+        else
+            Epot_kin = (rhos_new + rk_) * Gravit * Alt[lev]
+                       + 0.5 * (pow(m0, 2) + pow(m1, 2) + pow(m2, 2) + pow(w, 2)) / (rhos_new + rk_);
+        s.ps[i] = s.Rd[i] / Cv * (aux - Epot_kin) - s.pk[i];
+    }
+    else {
+        aux += ptc * r;
+        const double pn = P.P_Ref * vpow(div_rcp(s.Rd[i] * aux, P.P_Ref, P.rP_Ref), s.Cp[i] / Cv);
+        s.ps[i]         = pn - s.pk[i] + (s.diffpr[i]) * deltat + s.Rd[i] / Cv * s.Qheat[i] * deltat;
+    }
+}
+
+// The Thomas elimination and back substitution of one column (Vertical_Eq,
+// thor_vertical_int.h:463-484, same operations) from the row planes, the eliminated coefficients in
+// shared memory sc/sd [nv][32]; rows are loaded kThomasPf interfaces ahead of their use, so the
+// chain of dependent divisions does not wait on memory.
+__device__ __forceinline__ void thomas_column(const Geometry& g, const State& s, LevArr sc,
+                                              LevArr sd, int c) {
+    const int     nv = g.nv, Np = g.Np, nvi = g.nvi;
+    const double* ra = s.vrows;
+    const double* rb = ra + (size_t)nvi * Np;
+    const double* rc = rb + (size_t)nvi * Np;
+    const double* rd = rc + (size_t)nvi * Np;
+    double        cprev = 0, dprev = 0;
+    if constexpr (kThomasPf > 0) {
+        constexpr int kQ = kThomasPf > 0 ? kThomasPf : 1;
+        double        qa[kQ], qb[kQ], qc[kQ], qd[kQ];
+#pragma unroll
+        for (int k = 0; k < kThomasPf; k++) {
+            const int l = 1 + k;
+            if (l < nv) {
+                const int q = l * Np + c;
+                qa[k] = ra[q], qb[k] = rb[q], qc[k] = rc[q], qd[k] = rd[q];
+            }
+        }
+        for (int base = 1; base < nv; base += kThomasPf) {
+#pragma unroll
+            for (int k = 0; k < kThomasPf; k++) {
+                const int lev = base + k;
+                if (lev < nv) {
+                    const double aa = qa[k], bb = qb[k];
+                    double       ccv = qc[k], ddv = qd[k];
+                    const int    ln  = lev + kThomasPf;
+                    if (ln < nv) {
+                        const int q = ln * Np + c;
+                        qa[k] = ra[q], qb[k] = rb[q], qc[k] = rc[q], qd[k] = rd[q];
+                    }
+                    if (lev == 1) {
+                        ccv = ccv / bb;
+                        ddv = ddv / bb;
+                    }
+                    else {
+                        const double t = 1.0 / (bb - cprev * aa);
+                        ccv *= t;
+                        ddv = (ddv - dprev * aa) * t;
+                    }
+                    sc[lev] = ccv;
+                    sd[lev] = ddv;
+                    cprev = ccv;
+                    dprev = ddv;
+                }
+            }
+        }
+    }
+    else {
+#pragma unroll 2
+        for (int lev = 1; lev < nv; lev++) {
+            const int    q  = lev * Np + c;
+            const double aa = ra[q], bb = rb[q];
+            double       ccv = rc[q], ddv = rd[q];
+            if (lev == 1) {
+                ccv = ccv / bb;
+                ddv = ddv / bb;
+            }
+            else {
+                const double t = 1.0 / (bb - cprev * aa);
+                ccv *= t;
+                ddv = (ddv - dprev * aa) * t;
+            }
+            sc[lev] = ccv;
+            sd[lev] = ddv;
+            cprev = ccv;
+            dprev = ddv;
+        }
+    }
+    double w           = 0.0;
+    s.Whs[nv * Np + c] = 0.0;
+    for (int lev = nv - 1; lev > 0; lev--) {
+        const double cc = sc[lev], dd = sd[lev];
+        w               = (lev == nv - 1) ? dd : (-cc * w + dd);
+        s.Whs[lev * Np + c] = w;
+    }
+    s.Whs[c] = 0.0;
+}
+
 template<int kPart>
 __global__ void THORX_KATTR_VERT
     vertical_kernel(Geometry g, Phys P, State s, double deltat) {
     extern __shared__ double smem[];
     const int nv = g.nv, nvi = g.nvi, Np = g.Np;
-    double*   sdiv = smem;
-    double*   sSp  = sdiv + 21 * kTile;
-    double*   sSd  = sSp + nv * kTile;
-    double*   sCp  = sSd + nv * kTile; // eliminated Thomas coefficients c', d' [nv][32]
-    double*   sDp  = sCp + nv * kTile;
     const int c0 = blockIdx.x * kTile, x = threadIdx.x, c = c0 + x;
+    double*   sdiv = smem;
+    // the four per-level arrays: in shared memory after sdiv, or global scratch planes after the
+    // four row planes of s.vrows (kVertSmem)
+    double*   gscr = s.vrows + (size_t)4 * nvi * Np;
+    auto      arr  = [&](int k) -> LevArr {
+        const bool in_smem = kVertSmem == 2 || (kVertSmem == 1 && k < 2);
+        return in_smem ? LevArr{sdiv + 21 * kTile + (size_t)k * nv * kTile, kTile, x}
+                            : LevArr{gscr + (size_t)k * nv * Np, Np, c};
+    };
+    const LevArr sSp = arr(0), sSd = arr(1), sX = arr(2), sY = arr(3);
+    // merged: Fr, Fpt in X, Y, eliminated c', d' over Sp, Sd; otherwise c', d' in X, Y and Fr,
+    // Fpt over Sp, Sd (global scratch keeps them apart: planes 4 and 5 for c', d')
+    const LevArr sFr  = kVertMerge ? sX : sSp;
+    const LevArr sFpt = kVertMerge ? sY : sSd;
+    const LevArr sCp  = kVertSmem < 2 ? arr(4) : (kVertMerge ? sSp : sX);
+    const LevArr sDp  = kVertSmem < 2 ? arr(5) : (kVertMerge ? sSd : sY);
     stage(sdiv, g.div, 21, Np, c0);
     __syncthreads();
     const bool    active = c < g.N;
@@ -2155,38 +2470,19 @@ __global__ void THORX_KATTR_VERT
         pole = (g.cflag[c] & kPole) != 0;
     }
 
-    // ---- phase 1: Sp, Sd (Prepare_Implicit_Vertical) ----
+    // ---- phase 1: Sp, Sd (Prepare_Implicit_Vertical), merged: also Fr, Fpt ----
     if (kPart != 2 && active)
         for (int lev = threadIdx.y; lev < nv; lev += kLevGroups) {
-            const int    i      = lev * Np + c;
-            const double RoC    = s.Rd[i] / (s.Cp[i] - s.Rd[i]);
-            const double rscale = lt[kLtRscale * nvi + lev];
-            double       sdv[3], spv[3];
-#pragma unroll
-            for (int j = 0; j < 7; j++) {
-                const double hv = gz(s.h + lev * Np, nb[j]);
-#pragma unroll
-                for (int k = 0; k < 3; k++) {
-                    const double Mv = gz(s.Mhs + (k * nv + lev) * Np, nb[j]);
-                    const double d  = sdiv[(j * 3 + k) * kTile + x];
-                    if (j == 0) {
-                        sdv[k] = d * Mv;
-                        spv[k] = d * Mv * hv;
-                    }
-                    else {
-                        sdv[k] = sdv[k] + d * Mv;
-                        spv[k] = spv[k] + d * Mv * hv;
-                    }
-                }
+            double Sp, Sd, Fr, Fpt;
+            if (kVertMerge && kPart == 0) {
+                vert_gathers<true, true>(g, P, s, sdiv, nb, c, lev, Sp, Sd, Fr, Fpt);
+                sFr[lev]  = Fr;
+                sFpt[lev] = Fpt;
             }
-            double nflxr = 0.0, nflxp = 0.0;
-#pragma unroll
-            for (int k = 0; k < 3; k++) {
-                nflxr -= rscale * sdv[k];
-                nflxp -= (RoC)*rscale * spv[k];
-            }
-            sSp[lev * kTile + x] = nflxp + s.Slowp[i];
-            sSd[lev * kTile + x] = nflxr + s.SlowRho[i];
+            else
+                vert_gathers<true, false>(g, P, s, sdiv, nb, c, lev, Sp, Sd, Fr, Fpt);
+            sSp[lev] = Sp;
+            sSd[lev] = Sd;
         }
     if (kPart != 2)
         __syncthreads();
@@ -2201,8 +2497,8 @@ __global__ void THORX_KATTR_VERT
             const double gp = s.gtilh[(lev + 1) * Np + c], gg = s.gtilh[lev * Np + c], gm = s.gtilh[(lev - 1) * Np + c];
             const int    iu = lev * Np + c, il = (lev - 1) * Np + c;
             const double p = s.ps[iu], pl = s.ps[il], r = s.Rhos[iu], rl = s.Rhos[il];
-            const double Sp = sSp[lev * kTile + x], Spl = sSp[(lev - 1) * kTile + x];
-            const double Sd = sSd[lev * kTile + x], Sdl = sSd[(lev - 1) * kTile + x];
+            const double Sp = sSp[lev], Spl = sSp[lev - 1];
+            const double Sd = sSd[lev], Sdl = sSd[lev - 1];
             const double CRddl = (s.Cp[il] - s.Rd[il]) / (s.Rd[il] * deltat * deltat);
             const double CRddu = (s.Cp[iu] - s.Rd[iu]) / (s.Rd[iu] * deltat * deltat);
             double       GCoRl, GCoRu;
@@ -2215,15 +2511,15 @@ __global__ void THORX_KATTR_VERT
                 GCoRu = Gravit * (s.Cp[iu] - s.Rd[iu]) / s.Rd[iu];
             }
             const double dzp   = lt[kLtDzp * nvi + lev];
-            const double dzh   = lt[kLtDzh * nvi + lev];
+            const double dzh   = lt[kLtDzh * nvi + lev]; // RN(1 / (alt - altl))
             const double dzm   = lt[kLtDzm * nvi + lev];
             const double dzph  = dzp * dzh;
             const double dzmh  = dzm * dzh;
             const double intl  = lt[kLtIntl * nvi + lev];
             const double inttm = lt[kLtInttm * nvi + lev];
             double       aa, bb, ccv;
-            const double CRdd = (CRddl * (alt - alth) + CRddu * (alth - altl)) / (alt - altl);
-            const double GCoR = (GCoRl * (alt - alth) + GCoRu * (alth - altl)) / (alt - altl);
+            const double CRdd = div_rcp(CRddl * (alt - alth) + CRddu * (alth - altl), alt - altl, dzh);
+            const double GCoR = div_rcp(GCoRl * (alt - alth) + GCoRu * (alth - altl), alt - altl, dzh);
             if (deep) {
                 hp                = hp * lt[kLtR2hI * nvi + lev + 1];
                 h                 = h * lt[kLtR2hI * nvi + lev];
@@ -2287,89 +2583,33 @@ __global__ void THORX_KATTR_VERT
     if (kPart != 2)
         __syncthreads();
 
-    // ---- phase 3: the Thomas elimination and back substitution (warp 0), while the other warps
-    // compute the horizontal flux divergences of Density_Pressure_Eqs, which do not depend on
-    // the solve, into the shared memory Sp and Sd no longer need ----
-    double*    sFr  = sSp; // rscale * div(Mhs) per level
-    double*    sFpt = sSd; // rscale * div((Mhs + Mhk) pt) (or the energy form's) per level
-    const bool eeq  = P.energy;
+    // ---- phase 3: the Thomas sweep (warp 0); meanwhile the other warps compute what the update
+    // needs and the solve does not change: merged, the pressure factor of their update levels;
+    // otherwise the horizontal flux divergences (all warps in part 2) ----
+    const bool eeq = P.energy;
+    double     pre[kVertPre];
     if (kPart != 2 && threadIdx.y == 0) {
-        if (active) {
-            // the eliminated coefficients go to shared memory: no store to global memory inside
-            // the sweep, so the row loads of later interfaces are free to be issued early
-            double* sc = sCp;
-            double* sd = sDp;
-            double  cprev = 0, dprev = 0;
-#pragma unroll 2
-            for (int lev = 1; lev < nv; lev++) {
-                const int    q  = lev * Np + c;
-                const double aa = ra[q], bb = rb[q];
-                double       ccv = rc[q], ddv = rd[q];
-                if (lev == 1) {
-                    ccv = ccv / bb;
-                    ddv = ddv / bb;
-                }
-                else {
-                    const double t = 1.0 / (bb - cprev * aa);
-                    ccv *= t;
-                    ddv = (ddv - dprev * aa) * t;
-                }
-                sc[lev * kTile + x] = ccv;
-                sd[lev * kTile + x] = ddv;
-                cprev = ccv;
-                dprev = ddv;
+        if (active)
+            thomas_column(g, s, sCp, sDp, c);
+    }
+    else if (kPart == 0 && kVertMerge) {
+        if (active && !eeq) {
+#pragma unroll
+            for (int k = 0; k < kVertPre; k++) {
+                const int lev = (int)threadIdx.y - 1 + k * (kLevGroups - 1);
+                if (lev < nv)
+                    pre[k] = vert_ptc(P, s, lev * Np + c);
             }
-            double w           = 0.0;
-            s.Whs[nv * Np + c] = 0.0;
-            for (int lev = nv - 1; lev > 0; lev--) {
-                const double cc = sc[lev * kTile + x], dd = sd[lev * kTile + x];
-                w               = (lev == nv - 1) ? dd : (-cc * w + dd);
-                s.Whs[lev * Np + c] = w;
-            }
-            s.Whs[c] = 0.0;
         }
     }
     else if (kPart != 1 && active) {
-        // the fused kernel's warp 0 is solving meanwhile; part 2 has every warp here
         const int first = kPart == 2 ? (int)threadIdx.y : (int)threadIdx.y - 1;
         const int step  = kPart == 2 ? kLevGroups : kLevGroups - 1;
         for (int lev = first; lev < nv; lev += step) {
-            const double rscale = deep ? lt[kLtRscale * nvi + lev] : 1.0;
-            double       sr[3], st[3];
-#pragma unroll
-            for (int j = 0; j < 7; j++) {
-                const int id = nb[j];
-                double    vs[3] = {0.0, 0.0, 0.0}, v1[3] = {0.0, 0.0, 0.0}, ptv = 0.0;
-                if (id >= 0) {
-#pragma unroll
-                    for (int k = 0; k < 3; k++) {
-                        vs[k] = s.Mhs[(k * nv + lev) * Np + id];
-                        v1[k] = vs[k] + s.Mhk[(k * nv + lev) * Np + id];
-                    }
-                    const int q = lev * Np + id;
-                    ptv         = eeq ? (s.h[q] + s.ep[q] + s.ek[q]) : s.pt[q];
-                }
-#pragma unroll
-                for (int k = 0; k < 3; k++) {
-                    const double d = sdiv[(j * 3 + k) * kTile + x];
-                    if (j == 0) {
-                        sr[k] = d * vs[k];
-                        st[k] = d * v1[k] * ptv;
-                    }
-                    else {
-                        sr[k] = sr[k] + d * vs[k];
-                        st[k] = st[k] + d * v1[k] * ptv;
-                    }
-                }
-            }
-            double nflxr = 0.0, nflxpt = 0.0;
-#pragma unroll
-            for (int k = 0; k < 3; k++) {
-                nflxr += rscale * sr[k];
-                nflxpt += rscale * st[k];
-            }
-            sFr[lev * kTile + x]  = nflxr;
-            sFpt[lev * kTile + x] = nflxpt;
+            double Sp, Sd, Fr, Fpt;
+            vert_gathers<false, true>(g, P, s, sdiv, nb, c, lev, Sp, Sd, Fr, Fpt);
+            sFr[lev]  = Fr;
+            sFpt[lev] = Fpt;
         }
     }
     __syncthreads();
@@ -2377,127 +2617,72 @@ __global__ void THORX_KATTR_VERT
         return;
 
     // ---- phase 4: Density_Pressure_Eqs, vertical terms and the update ----
-    const double P_Ref = P.P_Ref;
-    for (int lev = threadIdx.y; lev < nv; lev += kLevGroups) {
-        const int    i     = lev * Np + c;
-        const double Cv    = s.Cp[i] - s.Rd[i];
-        const double dz    = Alth[lev + 1] - Alth[lev];
-        double       r2p, r2m, r2l, dr2dz;
-        if (deep) {
-            r2p    = lt[kLtR2hD * nvi + lev + 1];
-            r2m    = lt[kLtR2cD * nvi + lev];
-            r2l    = lt[kLtR2hD * nvi + lev];
-            dr2dz  = lt[kLtDr2dz * nvi + lev];
+    if (kPart == 0 && kVertMerge) {
+        // warps 1-7, the levels whose pressure factor they computed during the sweep
+        if (threadIdx.y == 0)
+            return;
+#pragma unroll
+        for (int k = 0; k < kVertPre; k++) {
+            const int lev = (int)threadIdx.y - 1 + k * (kLevGroups - 1);
+            if (lev < nv)
+                vert_update(g, P, s, deltat, c, lev, pole, sFr[lev], sFpt[lev],
+                            eeq ? nullptr : &pre[k]);
         }
-        else {
-            r2p = r2m = r2l = 1.0;
-            dr2dz           = r2m * dz;
-        }
-        double       nflxr  = sFr[lev * kTile + x];
-        const double nflxpt = sFpt[lev * kTile + x];
-        auto phv = [&](int l) -> double {
-            const int q = l * Np + c;
-            return eeq ? (s.hh[q] + s.eph[q] + s.ekh[q]) : s.pth[q];
-        };
-        double whl, wht, whl2, wht2, phl, pht;
-        if (lev == 0) {
-            whl  = 0.0;
-            wht  = s.Whs[(lev + 1) * Np + c];
-            whl2 = 0.0;
-            wht2 = wht + s.Whk[(lev + 1) * Np + c];
-            phl  = 0.0;
-            pht  = phv(lev + 1);
-        }
-        else {
-            whl  = s.Whs[lev * Np + c];
-            wht  = s.Whs[(lev + 1) * Np + c];
-            whl2 = whl + s.Whk[lev * Np + c];
-            wht2 = wht + s.Whk[(lev + 1) * Np + c];
-            phl  = phv(lev);
-            pht  = phv(lev + 1);
-        }
-        const double dwdz   = pole ? (wht * r2p - whl * r2l) / (dz * r2m) : (wht * r2p - whl * r2l) / (dr2dz);
-        const double dwptdz = (wht2 * pht * r2p - whl2 * phl * r2l) / (dz * r2m);
-        double       aux    = -(nflxpt + dwptdz) * deltat;
-        const double rk_    = s.Rhok[i];
-        const double rs     = s.Rhos[i];
-        const double r      = rk_ + rs;
-        nflxr += dwdz;
-        const double rhos_new = rs + (s.SlowRho[i] - nflxr) * deltat;
-        s.Rhos[i]             = rhos_new;
-        if (eeq) {
-            aux += s.Etotal[i] + (s.diffpr[i]) * deltat + s.Qheat[i] * deltat;
-            s.Etotal[i] = aux;
-            const double m0 = s.Mhs[(0 * nv + lev) * Np + c] + s.Mhk[(0 * nv + lev) * Np + c];
-            const double m1 = s.Mhs[(1 * nv + lev) * Np + c] + s.Mhk[(1 * nv + lev) * Np + c];
-            const double m2 = s.Mhs[(2 * nv + lev) * Np + c] + s.Mhk[(2 * nv + lev) * Np + c];
-            const double w  = (whl2 * (Alth[lev + 1] - Alt[lev]) + wht2 * (Alt[lev] - Alth[lev]))
-                             / (Alth[lev + 1] - Alth[lev]);
-            double Epot_kin;
-            if (ghv)
-                Epot_kin = (rhos_new + rk_) * Gravit * lt[kLtGhv * nvi + lev] * Alt[lev]
-                           + 0.5 * (pow(m0, 2) + pow(m1, 2) + pow(m2, 2) + pow(w, 2))
-                                 / (rhos_new + rk_);
-            else
-                Epot_kin = (rhos_new + rk_) * Gravit * Alt[lev]
-                           + 0.5 * (pow(m0, 2) + pow(m1, 2) + pow(m2, 2) + pow(w, 2))
-                                 / (rhos_new + rk_);
-            s.ps[i] = s.Rd[i] / Cv * (aux - Epot_kin) - s.pk[i];
-        }
-        else {
-            const double ptc = (P_Ref / (s.Rd[i] * r)) * pow((s.ps[i] + s.pk[i]) / P_Ref, Cv / s.Cp[i]);
-            aux += ptc * r;
-            const double pn = P_Ref * pow(s.Rd[i] * aux / P_Ref, s.Cp[i] / Cv);
-            s.ps[i]         = pn - s.pk[i] + (s.diffpr[i]) * deltat + s.Rd[i] / Cv * s.Qheat[i] * deltat;
-        }
+        for (int lev = (int)threadIdx.y - 1 + kVertPre * (kLevGroups - 1); lev < nv;
+             lev += kLevGroups - 1)
+            vert_update(g, P, s, deltat, c, lev, pole, sFr[lev], sFpt[lev], nullptr);
     }
+    else
+        for (int lev = threadIdx.y; lev < nv; lev += kLevGroups)
+            vert_update(g, P, s, deltat, c, lev, pole, sFr[lev], sFpt[lev], nullptr);
 }
 
 // ---------------------------------------------------------------------------------------------
 // End of an RK stage: UpdateRK2 (src/headers/dyn/thor_auxiliary.h:420-529, no module arrays).
-// Every level first reads the two interfaces it interpolates between; the writes follow a
-// barrier, so no level sees another's update.
 // ---------------------------------------------------------------------------------------------
-constexpr int kRk2Groups          = 8;
-constexpr int kMaxLevelsPerThread = 16; // nv <= kRk2Groups * 16
+// A CTA is one 32-column tile; warp y owns the contiguous levels [y chunk, (y + 1) chunk). Before a
+// barrier each warp reads the interface just above its chunk (the next warp writes it); then it
+// walks its chunk upward, so every other interface it reads is one it has not written yet. Few
+// registers, so 128-thread CTAs fit 16 to an SM: all of a g6 grid's 1281 tiles are resident at once.
+// The interpolation weights are the level tables' values of the same expressions (level 0, whose
+// lower interface the reference takes as 0, evaluates them here).
+constexpr int kRk2Groups = 4;
 
 __global__ void __launch_bounds__(kTile* kRk2Groups) update_rk2_kernel(Geometry g, Phys P, State s) {
     const int  c  = blockIdx.x * kTile + threadIdx.x;
-    const int  Np = g.Np, nv = g.nv;
+    const int  Np = g.Np, nv = g.nv, nvi = g.nvi;
     const bool active = c < g.N;
-    double     fr[3]  = {0, 0, 0};
-    if (active)
-        for (int k = 0; k < 3; k++)
-            fr[k] = g.func_r[k * Np + c];
-    double wk[kMaxLevelsPerThread], whk_new[kMaxLevelsPerThread];
-    auto   whk_after = [&](int i) -> double { // interface value after the update
+    const int  chunk  = (nv + kRk2Groups - 1) / kRk2Groups;
+    const int  l0 = threadIdx.y * chunk, l1 = min(nv, l0 + chunk);
+    auto       whk_after = [&](int i) -> double { // interface value after the update
         return (i == 0 || i == nv) ? 0.0 : s.Whk[i * Np + c] + s.Whs[i * Np + c];
     };
-    if (active) {
-        int cnt = 0;
-#pragma unroll
-        for (int t = 0; t < kMaxLevelsPerThread; t++) {
-            const int lev = threadIdx.y + t * kRk2Groups;
-            if (lev < nv) {
-                const double althl = (lev == 0) ? 0.0 : g.Altitudeh[lev];
-                const double altht = g.Altitudeh[lev + 1];
-                const double xi = g.Altitude[lev], xim = althl, xip = altht;
-                const double intt = (xi - xip) / (xim - xip), intl = (xi - xim) / (xip - xim);
-                const double whl = (lev == 0) ? 0.0 : whk_after(lev);
-                wk[t]            = whl * intt + whk_after(lev + 1) * intl;
-                whk_new[t]       = whk_after(lev);
-                cnt++;
-            }
-        }
+    double top = 0.0, whl = 0.0;
+    if (active && l0 < l1) {
+        top = whk_after(l1);
+        whl = whk_after(l0);
     }
     __syncthreads();
-    if (!active)
+    if (!active || l0 >= l1)
         return;
-#pragma unroll
-    for (int t = 0; t < kMaxLevelsPerThread; t++) {
-        const int lev = threadIdx.y + t * kRk2Groups;
-        if (lev >= nv)
-            break;
+    double fr[3];
+    for (int k = 0; k < 3; k++)
+        fr[k] = g.func_r[k * Np + c];
+    const double* lt = g.lt;
+#pragma unroll 2
+    for (int lev = l0; lev < l1; lev++) {
+        const double wht = (lev + 1 == l1) ? top : whk_after(lev + 1);
+        double       intt, intl;
+        if (lev == 0) {
+            const double xi = g.Altitude[0], xim = 0.0, xip = g.Altitudeh[1];
+            intt = (xi - xip) / (xim - xip);
+            intl = (xi - xim) / (xip - xim);
+        }
+        else {
+            intt = lt[kLtCIntt * nvi + lev];
+            intl = lt[kLtCIntl * nvi + lev];
+        }
+        const int    i   = lev * Np + c;
         const double Mx  = s.Mhs[(0 * nv + lev) * Np + c] + s.Mhk[(0 * nv + lev) * Np + c];
         const double My  = s.Mhs[(1 * nv + lev) * Np + c] + s.Mhk[(1 * nv + lev) * Np + c];
         const double Mz  = s.Mhs[(2 * nv + lev) * Np + c] + s.Mhk[(2 * nv + lev) * Np + c];
@@ -2505,14 +2690,14 @@ __global__ void __launch_bounds__(kTile* kRk2Groups) update_rk2_kernel(Geometry 
         s.Mhk[(0 * nv + lev) * Np + c] = Mx - aux * fr[0];
         s.Mhk[(1 * nv + lev) * Np + c] = My - aux * fr[1];
         s.Mhk[(2 * nv + lev) * Np + c] = Mz - aux * fr[2];
-        const int i = lev * Np + c;
         s.Rhok[i] += s.Rhos[i];
         s.pk[i] += s.ps[i];
-        s.Whk[lev * Np + c] = whk_new[t];
-        s.Wk[i]             = wk[t];
-        if (lev == nv - 1)
-            s.Whk[nv * Np + c] = 0.0;
+        s.Wk[i]  = whl * intt + wht * intl;
+        s.Whk[i] = whl; // whk_after(lev)
+        whl      = wht;
     }
+    if (l1 == nv)
+        s.Whk[nv * Np + c] = 0.0;
 }
 
 inline dim3 tile_grid(const Geometry& g) { return dim3(g.Np / kTile); }
@@ -2577,7 +2762,7 @@ __global__ void div_check_kernel(long long n, unsigned long long seed, unsigned 
 
 } // namespace
 
-int max_levels() { return kRk2Groups * kMaxLevelsPerThread; }
+int max_levels() { return 128; }
 
 void launch_level_tables(const Geometry& g, const Phys& P, double* lt, cudaStream_t st) {
     level_tables_kernel<<<(g.nvi + 127) / 128, 128, 0, st>>>(g, P, lt);
@@ -2643,7 +2828,9 @@ void launch_momentum(const Geometry& g, const Phys& P, const State& s, double dt
     else
         momentum_kernel<double><<<tile_grid_tail(g), tile_block(), 0, st>>>(g, P, s, dt);
 }
-size_t vertical_smem_bytes(const Geometry& g) { return sizeof(double) * kTile * (21 + 4 * g.nv); }
+size_t vertical_smem_bytes(const Geometry& g) {
+    return sizeof(double) * kTile * (21 + (kVertSmem == 2 ? 4 : kVertSmem == 1 ? 2 : 0) * g.nv);
+}
 
 // The largest dynamic shared memory a kernel has been opened to, per device (the attribute is a
 // per-device setting; a process may hold contexts on several devices, and host threads may launch
@@ -2676,6 +2863,15 @@ void launch_vertical_part(const Geometry& g, const Phys& P, const State& s, doub
     static SmemOptIn opt;
     if (opt.ensure(vertical_kernel<kPart>, smem) != cudaSuccess)
         return;
+    // the carveout: shared memory for the 3 CTAs an SM holds (register-limited), the rest is L1
+    // for the neighbour gathers (a hint; 228 KB is the most shared memory an SM has)
+    static bool carve = false;
+    if (!carve) {
+        const int pct = (int)std::min<size_t>(100, (3 * (smem + 1024) * 100 + 233471) / 233472);
+        cudaFuncSetAttribute(vertical_kernel<kPart>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             pct);
+        carve = true;
+    }
     vertical_kernel<kPart><<<tile_grid(g), tile_block(), smem, st>>>(g, P, s, dt);
 }
 void launch_vertical(const Geometry& g, const Phys& P, const State& s, double dt, int part,

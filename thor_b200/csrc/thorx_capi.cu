@@ -54,6 +54,7 @@ struct thorx_ctx {
     bool                             rt_enabled  = false;   // double-gray RT in ProfX
     Sponge                           sp{};                   // Rayleigh sponge (nlat 0: off)
     std::vector<thorx_module>        modules;                // physics modules, in call order
+    bool                             eager = false;          // thorx_step without a graph
     RkArrays                         rk_arrays{};            // their RK-updated arrays
     Surrogate*                       sur         = nullptr; // RT surrogate (thorx_surrogate_create)
     int                              sur_mode    = THORX_SUR_OFF;
@@ -657,6 +658,7 @@ int thorx_create(const thorx_grid* gr, const thorx_params* pr, void* stream, tho
     P.Rd              = pr->Rd;
     P.Cp              = pr->Cp;
     P.P_Ref           = pr->P_Ref;
+    P.rP_Ref          = 1.0 / pr->P_Ref;
     P.timestep        = pr->timestep;
     P.HyDiffOrder     = pr->HyDiffOrder;
     P.DeepModel       = pr->DeepModel != 0;
@@ -762,7 +764,7 @@ int thorx_create(const thorx_grid* gr, const thorx_params* pr, void* stream, tho
               {&s.Cp, cell},        {&s.h, cell},        {&s.hh, iface},       {&s.pt, cell},
               {&s.pth, iface},      {&s.gtil, cell},     {&s.gtilh, iface},    {&s.Adv, 3 * cell},
               {&s.diff, 12 * cell}, {&s.diffmh, 3 * cell}, {&s.diffw, cell},   {&s.diffrh, cell},
-              {&s.diffpr, cell},    {&s.divg, 3 * cell}, {&s.vrows, 4 * iface}, {&s.SlowMh, 3 * cell},
+              {&s.diffpr, cell},    {&s.divg, 3 * cell}, {&s.vrows, 4 * iface + 6 * cell}, {&s.SlowMh, 3 * cell},
               {&s.SlowWh, iface},
               {&s.SlowRho, cell},   {&s.Slowp, cell},    {&s.Qheat, cell},     {&s.dMh, 3 * cell},
               {&s.dWh, iface}};
@@ -1090,6 +1092,16 @@ int thorx_thor(thorx_ctx* ctx) {
 int thorx_step(thorx_ctx* ctx, int nsteps) {
     if (!ctx || nsteps < 0)
         return THORX_E_ARG;
+    if (ctx->eager) { // thorx_set_graph_mode(ctx, 0): every step enqueued, every hook called
+        for (int i = 0; i < nsteps; i++) {
+            int rc = enqueue_profx(ctx);
+            if (!rc)
+                rc = enqueue_thor(ctx);
+            if (rc)
+                return rc;
+        }
+        return 0;
+    }
     if (!ctx->graph_exec) {
         CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
         int rc = enqueue_profx(ctx);
@@ -1883,6 +1895,30 @@ int thorx_rk_register_array(thorx_ctx* ctx, double* array, double* arrayk, doubl
     t.arrayi[t.n] = arrayi;
     t.count[t.n]  = (long long)dimensions * ctx->g.nv * ctx->g.Np;
     t.n++;
+    return drop_graph(ctx);
+}
+
+int thorx_rk_register_array_n(thorx_ctx* ctx, double* array, double* arrayk, double* arrayi,
+                              long long count) {
+    if (!ctx)
+        return THORX_E_ARG;
+    RkArrays& t = ctx->rk_arrays;
+    if (!array || !arrayk || !arrayi || count < 1)
+        return fail(ctx, THORX_E_ARG, "thorx_rk_register_array_n: null array or count < 1");
+    if (t.n >= kMaxRkArrays)
+        return fail(ctx, THORX_E_ARG, "thorx_rk_register_array_n: at most 10 arrays");
+    t.array[t.n]  = array;
+    t.arrayk[t.n] = arrayk;
+    t.arrayi[t.n] = arrayi;
+    t.count[t.n]  = count;
+    t.n++;
+    return drop_graph(ctx);
+}
+
+int thorx_set_graph_mode(thorx_ctx* ctx, int use_graph) {
+    if (!ctx)
+        return THORX_E_ARG;
+    ctx->eager = !use_graph;
     return drop_graph(ctx);
 }
 

@@ -90,11 +90,16 @@ enum LevelTable : int {
     kLtInttm,  // interior interface: -(Alt[i-1] - Alth[i]) * dzm * dzh
     kLtHIntt,  // interior interface from centres: (Alth[i] - Alt[i]) / (Alt[i-1] - Alt[i])
     kLtHIntl,  // interior interface from centres: (Alth[i] - Alt[i-1]) / (Alt[i] - Alt[i-1])
+    // reciprocals of level-constant divisors, RN(1 / divisor), for div_rcp (the IEEE quotient)
+    kLtRDz,    // centre: 1 / (Alth[l+1] - Alth[l])
+    kLtRDr2dz, // centre: 1 / kLtDr2dz
+    kLtRDzR2m, // centre: 1 / ((Alth[l+1] - Alth[l]) * kLtR2cD)
     kLtCount
 };
 
 struct Phys {
     double A, Omega, Gravit, Rd, Cp, P_Ref, timestep;
+    double rP_Ref; // RN(1 / P_Ref), for div_rcp
     int    HyDiffOrder;
     bool   DeepModel, NonHydro, GravHeightVar, HyDiff, DivDampP, energy, held_suarez;
     int    benchmark; // THORX_NO_BENCHMARK .. THORX_SHALLOW_HOT_JUPITER (forcing in ProfX)
@@ -119,7 +124,8 @@ struct State {
     double *diff;                 // 6 planes (intermediate hyperdiffusion passes)
     double *diffmh, *diffw, *diffrh, *diffpr;
     double *divg;                 // 3 planes
-    double *vrows;                // 4 x (nv+1) planes: tridiagonal rows of the vertical solve
+    double *vrows;                // 4 x (nv+1) planes: tridiagonal rows of the vertical solve,
+                                  // then 6 x nv scratch planes of the vertical kernel
     double *SlowMh, *SlowWh, *SlowRho, *Slowp;
     double *Qheat, *dMh, *dWh;    // physics-module coupling (profx_Qheat_d, profx_dMh_d, ...)
     unsigned int* flags;          // device status word (kFlagNaN, kFlagConvAdj)
