@@ -81,6 +81,23 @@ __device__ __forceinline__ double rscale_of(const Phys&, const Geometry& g, int 
     return g.lt[kLtRscale * g.nvi + lev];
 }
 
+// Gas constant and heat capacity of a cell. kUni (Phys::uniform_thermo: every cell's Rd and Cp
+// are Phys::Rd and Phys::Cp, which the context checks whenever the fields are set): the scalars, so
+// the compiler folds the expressions built from them (Rd / (Cp - Rd) and the like) into per-thread
+// constants; they are the same values, so the results are the same bits as the per-cell loads.
+template<bool kUni> __device__ __forceinline__ double rd_at(const Phys& P, const State& s, int i) {
+    if constexpr (kUni)
+        return P.Rd;
+    else
+        return s.Rd[i];
+}
+template<bool kUni> __device__ __forceinline__ double cp_at(const Phys& P, const State& s, int i) {
+    if constexpr (kUni)
+        return P.Cp;
+    else
+        return s.Cp[i];
+}
+
 // Copies rows 0..Q-1 of a [q][Np] grid array for the tile's 32 columns into smem [q][32].
 __device__ __forceinline__ void stage(double* sm, const double* __restrict__ src, int Q, int Np,
                                       int c0) {
@@ -824,9 +841,10 @@ struct ColLevel { // thermodynamic quantities of one column at one level
     double p, rho, Rd, Cp;
 };
 
-__device__ __forceinline__ ColLevel col_level(const State& s, int Np, int lev, int c) {
+template<bool kUni>
+__device__ __forceinline__ ColLevel col_level(const Phys& P, const State& s, int Np, int lev, int c) {
     const int i = lev * Np + c;
-    return ColLevel{s.pk[i], s.Rhok[i], s.Rd[i], s.Cp[i]};
+    return ColLevel{s.pk[i], s.Rhok[i], rd_at<kUni>(P, s, i), cp_at<kUni>(P, s, i)};
 }
 // enthalpy h = Cv T + p / rho (thor_auxiliary.h:111,130,140)
 __device__ __forceinline__ double enthalpy(const ColLevel& q) {
@@ -841,6 +859,7 @@ __device__ __forceinline__ double pot_temp(const ColLevel& q, double P_Ref) {
     return (P_Ref / (q.Rd * q.rho)) * pow(q.p / P_Ref, CvoCp);
 }
 
+template<bool kUni>
 __global__ void THORX_KATTR_ADV adv_temp_kernel(Geometry g, Phys P, State s) {
     __shared__ double sdiv[21 * kTile];
     __shared__ double sfr[21 * kTile]; // func_r of the 7 stencil points, [point * 3 + k][32]
@@ -894,7 +913,7 @@ __global__ void THORX_KATTR_ADV adv_temp_kernel(Geometry g, Phys P, State s) {
     auto gtil_w = [&](int i) -> double {
         if (i <= 0 || i >= nv)
             return 0.0;
-        const ColLevel lo = col_level(s, Np, i - 1, c), hi = col_level(s, Np, i, c);
+        const ColLevel lo = col_level<kUni>(P, s, Np, i - 1, c), hi = col_level<kUni>(P, s, Np, i, c);
         const double   dz    = Alt[i] - Alt[i - 1];
         const double   dp_dz = (hi.p - lo.p) / dz;
         const double   intt = lt[kLtHIntt * nvi + i], intl = lt[kLtHIntl * nvi + i];
@@ -979,7 +998,7 @@ __global__ void THORX_KATTR_ADV adv_temp_kernel(Geometry g, Phys P, State s) {
         }
 
         // ---- Compute_Temperature_H_Pt_Geff at this level (and its interface below) ----
-        const ColLevel q  = col_level(s, Np, lev, c);
+        const ColLevel q  = col_level<kUni>(P, s, Np, lev, c);
         const double   Cv = q.Cp - q.Rd;
         const double   T  = q.p / (q.rho * q.Rd);
         const double   h  = Cv * T + q.p / q.rho;
@@ -998,7 +1017,7 @@ __global__ void THORX_KATTR_ADV adv_temp_kernel(Geometry g, Phys P, State s) {
             s.pt[i] = pt;
         }
         if (lev > 0) { // interior interface `lev`
-            const ColLevel lo    = col_level(s, Np, lev - 1, c);
+            const ColLevel lo    = col_level<kUni>(P, s, Np, lev - 1, c);
             const double   dzl   = alt - Alt[lev - 1];
             const double   dp_dz = (q.p - lo.p) / dzl;
             const double   intt = lt[kLtHIntt * nvi + lev], intl = lt[kLtHIntl * nvi + lev];
@@ -1013,7 +1032,7 @@ __global__ void THORX_KATTR_ADV adv_temp_kernel(Geometry g, Phys P, State s) {
             s.gtilh[i]        = -(1.0 / rhoh) * dp_dz;
         }
         else { // bottom boundary, extrapolated (thor_auxiliary.h:167-187)
-            const ColLevel up   = col_level(s, Np, 1, c);
+            const ColLevel up   = col_level<kUni>(P, s, Np, 1, c);
             const double   extr = (-alt - Alt[1]) / (Alt[1] - alt);
             s.hh[c]             = h;
             double pl;
@@ -1037,7 +1056,7 @@ __global__ void THORX_KATTR_ADV adv_temp_kernel(Geometry g, Phys P, State s) {
             s.gtil[i]         = gw0 * intt + gw1 * intl;
         }
         if (lev == nv - 1) { // top boundary and the bottom extrapolations (thor_auxiliary.h:188-258)
-            const ColLevel lo2  = col_level(s, Np, nv - 2, c);
+            const ColLevel lo2  = col_level<kUni>(P, s, Np, nv - 2, c);
             const ColLevel top  = q;
             const double   extr = (2 * Alth[nv] - alt - Alt[nv - 2]) / (Alt[nv - 1] - Alt[nv - 2]);
             s.hh[nv * Np + c]   = h;
@@ -1065,8 +1084,8 @@ __global__ void THORX_KATTR_ADV adv_temp_kernel(Geometry g, Phys P, State s) {
             }
             else {
                 const double pt2 = pot_temp(lo2, P_Ref);
-                const double pt0 = pot_temp(col_level(s, Np, 0, c), P_Ref);
-                const double pt1 = pot_temp(col_level(s, Np, 1, c), P_Ref);
+                const double pt0 = pot_temp(col_level<kUni>(P, s, Np, 0, c), P_Ref);
+                const double pt1 = pot_temp(col_level<kUni>(P, s, Np, 1, c), P_Ref);
                 s.pth[nv * Np + c] = pt2 + (pt - pt2) * extr;
                 s.pth[c]           = pt1 + (pt1 - pt0) * (Alth[0] - Alt[1]) / (Alt[1] - Alt[0]);
             }
@@ -1167,7 +1186,7 @@ __device__ __forceinline__ double laplacian_w(const SGeo& G, const double* a, do
 //   final pass (last)     : argument = diff (rho-weighted for v, w, T), scaled by -Kdh4 (-1)^(o/2)
 //                            -> diffrh, diffmh(3), diffw, diffpr
 // ---------------------------------------------------------------------------------------------
-template<int n, class R>
+template<int n, class R, bool kUni>
 __device__ __forceinline__ void diffusion_point(const Geometry& g, const Phys& P, const State& s,
                                                 const SGeo& G, const double* fr, const int* ring,
                                                 const double* __restrict__ diff_in,
@@ -1205,7 +1224,7 @@ __device__ __forceinline__ void diffusion_point(const Geometry& g, const Phys& P
                     else if (var == 4)
                         v = s.Wk[q];
                     else
-                        v = eeq ? (s.Cp[q] - s.Rd[q]) * s.T[q] : s.Rd[q] * s.T[q];
+                        v = eeq ? (cp_at<kUni>(P, s, q) - rd_at<kUni>(P, s, q)) * s.T[q] : rd_at<kUni>(P, s, q) * s.T[q];
                     if (var >= 1 && var <= 4)
                         v = v / rho[j];
                 }
@@ -1248,7 +1267,7 @@ __device__ __forceinline__ void diffusion_point(const Geometry& g, const Phys& P
 // weights each Laplacian is a running sum, so the values of all six variables at a point are
 // loaded together; each sum keeps laplacian_w's order (centre weight, then the ring in order).
 // kF32 (mixed form): v and w in float, rho and T in double; otherwise all six in double.
-template<int n, bool kF32>
+template<int n, bool kF32, bool kUni>
 __device__ __forceinline__ void diffusion_point_w(const Geometry& g, const Phys& P, const State& s,
                                                   const SGeo& G, const double* fr, const int* ring,
                                                   const double* __restrict__ diff_in,
@@ -1272,7 +1291,7 @@ __device__ __forceinline__ void diffusion_point_w(const Geometry& g, const Phys&
             for (int k = 0; k < 3; k++)
                 v[1 + k] = div_rcp(s.Mhk[(k * nv + lev) * Np + id], rho, yr);
             v[4] = div_rcp(s.Wk[q], rho, yr);
-            v[5] = eeq ? (s.Cp[q] - s.Rd[q]) * s.T[q] : s.Rd[q] * s.T[q];
+            v[5] = eeq ? (cp_at<kUni>(P, s, q) - rd_at<kUni>(P, s, q)) * s.T[q] : rd_at<kUni>(P, s, q) * s.T[q];
         }
         else {
 #pragma unroll
@@ -1353,7 +1372,7 @@ __device__ __forceinline__ void diffusion_point_w(const Geometry& g, const Phys&
     s.diffpr[i]                       = lap[5];
 }
 
-template<int n, class R>
+template<int n, class R, bool kUni>
 __device__ __forceinline__ void diffusion_body(const Geometry& g, const Phys& P, const State& s,
                                                const SGeo& G, const double* __restrict__ diff_in,
                                                double* __restrict__ diff_out, int stepnum,
@@ -1368,17 +1387,17 @@ __device__ __forceinline__ void diffusion_body(const Geometry& g, const Phys& P,
     const double sign4 = pow(-1.0, P.HyDiffOrder / 2); // (-1)^(order/2) of the last pass
     for (int lev = threadIdx.y; lev < g.nv; lev += kLevGroups)
         if constexpr (kOperatorWeights<R>)
-            diffusion_point_w<n, true>(g, P, s, G, fr, ring, diff_in, diff_out, stepnum, last, c,
+            diffusion_point_w<n, true, kUni>(g, P, s, G, fr, ring, diff_in, diff_out, stepnum, last, c,
                                        lev, sign4);
         else if constexpr (kDiffWeightsF64)
-            diffusion_point_w<n, false>(g, P, s, G, fr, ring, diff_in, diff_out, stepnum, last, c,
+            diffusion_point_w<n, false, kUni>(g, P, s, G, fr, ring, diff_in, diff_out, stepnum, last, c,
                                         lev, sign4);
         else
-            diffusion_point<n, R>(g, P, s, G, fr, ring, diff_in, diff_out, stepnum, last, c, lev, sign4);
+            diffusion_point<n, R, kUni>(g, P, s, G, fr, ring, diff_in, diff_out, stepnum, last, c, lev, sign4);
 }
 
 // R: compute type of the momentum and w Laplacians (double; float in the mixed form).
-template<class R>
+template<class R, bool kUni>
 __global__ void THORX_KATTR_DIFF
     diffusion_kernel(Geometry g, Phys P, State s, const double* __restrict__ diff_in,
                      double* __restrict__ diff_out, int stepnum, bool last) {
@@ -1393,9 +1412,9 @@ __global__ void THORX_KATTR_DIFF
     if (c < 0)
         return;
     if (tail_cta())
-        diffusion_body<5, R>(g, P, s, G, diff_in, diff_out, stepnum, last, c);
+        diffusion_body<5, R, kUni>(g, P, s, G, diff_in, diff_out, stepnum, last, c);
     else
-        diffusion_body<6, R>(g, P, s, G, diff_in, diff_out, stepnum, last, c);
+        diffusion_body<6, R, kUni>(g, P, s, G, diff_in, diff_out, stepnum, last, c);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1730,7 +1749,7 @@ __device__ __forceinline__ void divm_final(const Geometry& g, const Phys& P, con
 // (src/headers/dyn/thor_auxiliary.h:311-418, without module arrays and without the never-read
 // Ws). DivM is consumed where it is produced and not stored.
 // ---------------------------------------------------------------------------------------------
-template<int n, class R>
+template<int n, class R, bool kUni>
 __device__ __forceinline__ void slow_modes_body(const Geometry& g, const Phys& P, const State& s,
                                                 const SGeo& G, const double* sdiv,
                                                 const double* sgrad, bool update_rk, int c) {
@@ -1754,7 +1773,7 @@ __device__ __forceinline__ void slow_modes_body(const Geometry& g, const Phys& P
         R         DivM[3] = {0, 0, 0};
         if (P.DivDampP)
             divm_final<n, R>(g, P, G, ring, s.divg, c, lev, fr, DivM);
-        const double Cv = s.Cp[i] - s.Rd[i];
+        const double Cv = cp_at<kUni>(P, s, i) - rd_at<kUni>(P, s, i);
         double       adv[3];
         for (int k = 0; k < 3; k++)
             adv[k] = s.Adv[(k * nv + lev) * Np + c];
@@ -1879,9 +1898,9 @@ __device__ __forceinline__ void slow_modes_body(const Geometry& g, const Phys& P
         const double r_  = 1.0 / rho;
         const double vgp = (nflxv[0] - dpr * fr[0]) * M0[0] * r_ + (nflxv[1] - dpr * fr[1]) * M0[1] * r_
                            + (nflxv[2] - dpr * fr[2]) * M0[2] * r_;
-        double sp = (s.Rd[i] / Cv) * (-nflxp - s.gtil[i] - dwhdz + vgp + s.Qheat[i]);
+        double sp = (rd_at<kUni>(P, s, i) / Cv) * (-nflxp - s.gtil[i] - dwhdz + vgp + s.Qheat[i]);
         if (P.energy)
-            sp += s.Rd[i] / Cv * (s.diffpr[i]);
+            sp += rd_at<kUni>(P, s, i) / Cv * (s.diffpr[i]);
         else
             sp += s.diffpr[i];
         s.Slowp[i] = sp;
@@ -1904,7 +1923,7 @@ __device__ __forceinline__ void slow_modes_body(const Geometry& g, const Phys& P
     }
 }
 
-template<class R>
+template<class R, bool kUni>
 __global__ void THORX_KATTR_SLOW
     slow_modes_kernel(Geometry g, Phys P, State s, bool update_rk) {
     __shared__ double sgeo[kRingGeoRows * kTile];
@@ -1920,9 +1939,9 @@ __global__ void THORX_KATTR_SLOW
     if (c < 0)
         return;
     if (tail_cta())
-        slow_modes_body<5, R>(g, P, s, G, sdiv, sgrad, update_rk, c);
+        slow_modes_body<5, R, kUni>(g, P, s, G, sdiv, sgrad, update_rk, c);
     else
-        slow_modes_body<6, R>(g, P, s, G, sdiv, sgrad, update_rk, c);
+        slow_modes_body<6, R, kUni>(g, P, s, G, sdiv, sgrad, update_rk, c);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -2166,7 +2185,7 @@ constexpr int  kVertPre   = 8;             // levels whose pressure factor warps
 // kFlux: rscale div(Mhs) and rscale div((Mhs + Mhk) pt) (or the energy form's h + ep + ek) of
 // Density_Pressure_Eqs (thor_fastmodes.h:255-847). Each sum runs over the points in the
 // reference's order.
-template<bool kSpSd, bool kFlux>
+template<bool kSpSd, bool kFlux, bool kUni>
 __device__ __forceinline__ void vert_gathers(const Geometry& g, const Phys& P, const State& s,
                                              const double* sdiv, const int* nb, int c, int lev,
                                              double& Sp, double& Sd, double& Fr, double& Fpt) {
@@ -2226,7 +2245,7 @@ __device__ __forceinline__ void vert_gathers(const Geometry& g, const Phys& P, c
     Fpt = fpt;
     if (kSpSd) {
         const int    i   = lev * Np + c;
-        const double RoC = s.Rd[i] / (s.Cp[i] - s.Rd[i]);
+        const double RoC = rd_at<kUni>(P, s, i) / (cp_at<kUni>(P, s, i) - rd_at<kUni>(P, s, i));
         double       nflxp = 0.0;
 #pragma unroll
         for (int k = 0; k < 3; k++)
@@ -2252,15 +2271,17 @@ __device__ __forceinline__ double vpow(double x, double y) {
 // The entropy form's potential-temperature factor of Density_Pressure_Eqs at (c, lev): ptc =
 // (P_Ref / (Rd r)) (p / P_Ref)^(Cv / Cp) with the state before the update. It does not depend on
 // the vertical solve, so warps 1-7 evaluate it while warp 0 runs the Thomas sweep.
+template<bool kUni>
 __device__ __forceinline__ double vert_ptc(const Phys& P, const State& s, int i) {
-    const double Cv = s.Cp[i] - s.Rd[i];
+    const double Cv = cp_at<kUni>(P, s, i) - rd_at<kUni>(P, s, i);
     const double r  = s.Rhok[i] + s.Rhos[i];
-    return (P.P_Ref / (s.Rd[i] * r)) * vpow(div_rcp(s.ps[i] + s.pk[i], P.P_Ref, P.rP_Ref), Cv / s.Cp[i]);
+    return (P.P_Ref / (rd_at<kUni>(P, s, i) * r)) * vpow(div_rcp(s.ps[i] + s.pk[i], P.P_Ref, P.rP_Ref), Cv / cp_at<kUni>(P, s, i));
 }
 
 // Density_Pressure_Eqs at (c, lev): the vertical flux terms from the solved Whs, the update of
 // Rhos and ps (thor_fastmodes.h:255-847). Divisions by level constants go through div_rcp with
 // tabulated reciprocals (the IEEE quotients). ptc_pre: vert_ptc's value if precomputed.
+template<bool kUni>
 __device__ __forceinline__ void vert_update(const Geometry& g, const Phys& P, const State& s,
                                             double deltat, int c, int lev, bool pole,
                                             double nflxr, double nflxpt, const double* ptc_pre) {
@@ -2270,7 +2291,7 @@ __device__ __forceinline__ void vert_update(const Geometry& g, const Phys& P, co
     const double* Alth = g.Altitudeh;
     const bool    deep = P.DeepModel, eeq = P.energy, ghv = P.GravHeightVar;
     const int     i    = lev * Np + c;
-    const double  Cv   = s.Cp[i] - s.Rd[i];
+    const double  Cv   = cp_at<kUni>(P, s, i) - rd_at<kUni>(P, s, i);
     const double  dz   = Alth[lev + 1] - Alth[lev];
     double        r2p, r2m, r2l, dr2dz, rdr2dz, rdzr2m;
     if (deep) {
@@ -2315,7 +2336,7 @@ __device__ __forceinline__ void vert_update(const Geometry& g, const Phys& P, co
     const double rs     = s.Rhos[i];
     const double r      = rk_ + rs;
     // the entropy form's factor from the state before the update (Rhos is overwritten next)
-    const double ptc = eeq ? 0.0 : (ptc_pre ? *ptc_pre : vert_ptc(P, s, i));
+    const double ptc = eeq ? 0.0 : (ptc_pre ? *ptc_pre : vert_ptc<kUni>(P, s, i));
     nflxr += dwdz;
     const double rhos_new = rs + (s.SlowRho[i] - nflxr) * deltat;
     s.Rhos[i]             = rhos_new;
@@ -2335,12 +2356,12 @@ __device__ __forceinline__ void vert_update(const Geometry& g, const Phys& P, co
         else
             Epot_kin = (rhos_new + rk_) * Gravit * Alt[lev]
                        + 0.5 * (pow(m0, 2) + pow(m1, 2) + pow(m2, 2) + pow(w, 2)) / (rhos_new + rk_);
-        s.ps[i] = s.Rd[i] / Cv * (aux - Epot_kin) - s.pk[i];
+        s.ps[i] = rd_at<kUni>(P, s, i) / Cv * (aux - Epot_kin) - s.pk[i];
     }
     else {
         aux += ptc * r;
-        const double pn = P.P_Ref * vpow(div_rcp(s.Rd[i] * aux, P.P_Ref, P.rP_Ref), s.Cp[i] / Cv);
-        s.ps[i]         = pn - s.pk[i] + (s.diffpr[i]) * deltat + s.Rd[i] / Cv * s.Qheat[i] * deltat;
+        const double pn = P.P_Ref * vpow(div_rcp(rd_at<kUni>(P, s, i) * aux, P.P_Ref, P.rP_Ref), cp_at<kUni>(P, s, i) / Cv);
+        s.ps[i]         = pn - s.pk[i] + (s.diffpr[i]) * deltat + rd_at<kUni>(P, s, i) / Cv * s.Qheat[i] * deltat;
     }
 }
 
@@ -2427,7 +2448,7 @@ __device__ __forceinline__ void thomas_column(const Geometry& g, const State& s,
     s.Whs[c] = 0.0;
 }
 
-template<int kPart>
+template<int kPart, bool kUni>
 __global__ void THORX_KATTR_VERT
     vertical_kernel(Geometry g, Phys P, State s, double deltat) {
     extern __shared__ double smem[];
@@ -2475,12 +2496,12 @@ __global__ void THORX_KATTR_VERT
         for (int lev = threadIdx.y; lev < nv; lev += kLevGroups) {
             double Sp, Sd, Fr, Fpt;
             if (kVertMerge && kPart == 0) {
-                vert_gathers<true, true>(g, P, s, sdiv, nb, c, lev, Sp, Sd, Fr, Fpt);
+                vert_gathers<true, true, kUni>(g, P, s, sdiv, nb, c, lev, Sp, Sd, Fr, Fpt);
                 sFr[lev]  = Fr;
                 sFpt[lev] = Fpt;
             }
             else
-                vert_gathers<true, false>(g, P, s, sdiv, nb, c, lev, Sp, Sd, Fr, Fpt);
+                vert_gathers<true, false, kUni>(g, P, s, sdiv, nb, c, lev, Sp, Sd, Fr, Fpt);
             sSp[lev] = Sp;
             sSd[lev] = Sd;
         }
@@ -2499,16 +2520,16 @@ __global__ void THORX_KATTR_VERT
             const double p = s.ps[iu], pl = s.ps[il], r = s.Rhos[iu], rl = s.Rhos[il];
             const double Sp = sSp[lev], Spl = sSp[lev - 1];
             const double Sd = sSd[lev], Sdl = sSd[lev - 1];
-            const double CRddl = (s.Cp[il] - s.Rd[il]) / (s.Rd[il] * deltat * deltat);
-            const double CRddu = (s.Cp[iu] - s.Rd[iu]) / (s.Rd[iu] * deltat * deltat);
+            const double CRddl = (cp_at<kUni>(P, s, il) - rd_at<kUni>(P, s, il)) / (rd_at<kUni>(P, s, il) * deltat * deltat);
+            const double CRddu = (cp_at<kUni>(P, s, iu) - rd_at<kUni>(P, s, iu)) / (rd_at<kUni>(P, s, iu) * deltat * deltat);
             double       GCoRl, GCoRu;
             if (ghv) {
-                GCoRl = Gravit * lt[kLtGhv * nvi + lev - 1] * (s.Cp[il] - s.Rd[il]) / s.Rd[il];
-                GCoRu = Gravit * lt[kLtGhv * nvi + lev] * (s.Cp[iu] - s.Rd[iu]) / s.Rd[iu];
+                GCoRl = Gravit * lt[kLtGhv * nvi + lev - 1] * (cp_at<kUni>(P, s, il) - rd_at<kUni>(P, s, il)) / rd_at<kUni>(P, s, il);
+                GCoRu = Gravit * lt[kLtGhv * nvi + lev] * (cp_at<kUni>(P, s, iu) - rd_at<kUni>(P, s, iu)) / rd_at<kUni>(P, s, iu);
             }
             else {
-                GCoRl = Gravit * (s.Cp[il] - s.Rd[il]) / s.Rd[il];
-                GCoRu = Gravit * (s.Cp[iu] - s.Rd[iu]) / s.Rd[iu];
+                GCoRl = Gravit * (cp_at<kUni>(P, s, il) - rd_at<kUni>(P, s, il)) / rd_at<kUni>(P, s, il);
+                GCoRu = Gravit * (cp_at<kUni>(P, s, iu) - rd_at<kUni>(P, s, iu)) / rd_at<kUni>(P, s, iu);
             }
             const double dzp   = lt[kLtDzp * nvi + lev];
             const double dzh   = lt[kLtDzh * nvi + lev]; // RN(1 / (alt - altl))
@@ -2598,7 +2619,7 @@ __global__ void THORX_KATTR_VERT
             for (int k = 0; k < kVertPre; k++) {
                 const int lev = (int)threadIdx.y - 1 + k * (kLevGroups - 1);
                 if (lev < nv)
-                    pre[k] = vert_ptc(P, s, lev * Np + c);
+                    pre[k] = vert_ptc<kUni>(P, s, lev * Np + c);
             }
         }
     }
@@ -2607,7 +2628,7 @@ __global__ void THORX_KATTR_VERT
         const int step  = kPart == 2 ? kLevGroups : kLevGroups - 1;
         for (int lev = first; lev < nv; lev += step) {
             double Sp, Sd, Fr, Fpt;
-            vert_gathers<false, true>(g, P, s, sdiv, nb, c, lev, Sp, Sd, Fr, Fpt);
+            vert_gathers<false, true, kUni>(g, P, s, sdiv, nb, c, lev, Sp, Sd, Fr, Fpt);
             sFr[lev]  = Fr;
             sFpt[lev] = Fpt;
         }
@@ -2625,16 +2646,16 @@ __global__ void THORX_KATTR_VERT
         for (int k = 0; k < kVertPre; k++) {
             const int lev = (int)threadIdx.y - 1 + k * (kLevGroups - 1);
             if (lev < nv)
-                vert_update(g, P, s, deltat, c, lev, pole, sFr[lev], sFpt[lev],
+                vert_update<kUni>(g, P, s, deltat, c, lev, pole, sFr[lev], sFpt[lev],
                             eeq ? nullptr : &pre[k]);
         }
         for (int lev = (int)threadIdx.y - 1 + kVertPre * (kLevGroups - 1); lev < nv;
              lev += kLevGroups - 1)
-            vert_update(g, P, s, deltat, c, lev, pole, sFr[lev], sFpt[lev], nullptr);
+            vert_update<kUni>(g, P, s, deltat, c, lev, pole, sFr[lev], sFpt[lev], nullptr);
     }
     else
         for (int lev = threadIdx.y; lev < nv; lev += kLevGroups)
-            vert_update(g, P, s, deltat, c, lev, pole, sFr[lev], sFpt[lev], nullptr);
+            vert_update<kUni>(g, P, s, deltat, c, lev, pole, sFr[lev], sFpt[lev], nullptr);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -2792,7 +2813,10 @@ void launch_profx_finish(const Geometry& g, const State& s, cudaStream_t st) {
     profx_finish_kernel<<<(g.N + kColBlock - 1) / kColBlock, kColBlock, 0, st>>>(g, s);
 }
 void launch_adv_temp(const Geometry& g, const Phys& P, const State& s, cudaStream_t st) {
-    adv_temp_kernel<<<tile_grid(g), tile_block(), 0, st>>>(g, P, s);
+    if (P.uniform_thermo)
+        adv_temp_kernel<true><<<tile_grid(g), tile_block(), 0, st>>>(g, P, s);
+    else
+        adv_temp_kernel<false><<<tile_grid(g), tile_block(), 0, st>>>(g, P, s);
 }
 void launch_diffusion(const Geometry& g, const Phys& P, const State& s, int stepnum, bool last,
                       cudaStream_t st) {
@@ -2800,10 +2824,13 @@ void launch_diffusion(const Geometry& g, const Phys& P, const State& s, int step
     const size_t  plane6 = (size_t)6 * g.nv * g.Np;
     const double* in     = s.diff + ((stepnum + 1) % 2) * plane6;
     double*       out    = s.diff + (stepnum % 2) * plane6;
+    const dim3 gr = tile_grid_tail(g), bl = tile_block();
     if (P.mixed)
-        diffusion_kernel<float><<<tile_grid_tail(g), tile_block(), 0, st>>>(g, P, s, in, out, stepnum, last);
+        P.uniform_thermo ? diffusion_kernel<float, true><<<gr, bl, 0, st>>>(g, P, s, in, out, stepnum, last)
+                         : diffusion_kernel<float, false><<<gr, bl, 0, st>>>(g, P, s, in, out, stepnum, last);
     else
-        diffusion_kernel<double><<<tile_grid_tail(g), tile_block(), 0, st>>>(g, P, s, in, out, stepnum, last);
+        P.uniform_thermo ? diffusion_kernel<double, true><<<gr, bl, 0, st>>>(g, P, s, in, out, stepnum, last)
+                         : diffusion_kernel<double, false><<<gr, bl, 0, st>>>(g, P, s, in, out, stepnum, last);
 }
 void launch_divm0(const Geometry& g, const Phys& P, const State& s, bool small_step,
                   cudaStream_t st) {
@@ -2816,10 +2843,13 @@ void launch_divm0(const Geometry& g, const Phys& P, const State& s, bool small_s
 }
 void launch_slow_modes(const Geometry& g, const Phys& P, const State& s, bool update_rk,
                        cudaStream_t st) {
+    const dim3 gr = tile_grid_tail(g), bl = tile_block();
     if (P.mixed)
-        slow_modes_kernel<float><<<tile_grid_tail(g), tile_block(), 0, st>>>(g, P, s, update_rk);
+        P.uniform_thermo ? slow_modes_kernel<float, true><<<gr, bl, 0, st>>>(g, P, s, update_rk)
+                         : slow_modes_kernel<float, false><<<gr, bl, 0, st>>>(g, P, s, update_rk);
     else
-        slow_modes_kernel<double><<<tile_grid_tail(g), tile_block(), 0, st>>>(g, P, s, update_rk);
+        P.uniform_thermo ? slow_modes_kernel<double, true><<<gr, bl, 0, st>>>(g, P, s, update_rk)
+                         : slow_modes_kernel<double, false><<<gr, bl, 0, st>>>(g, P, s, update_rk);
 }
 void launch_momentum(const Geometry& g, const Phys& P, const State& s, double dt,
                      cudaStream_t st) {
@@ -2856,23 +2886,31 @@ struct SmemOptIn {
         return e;
     }
 };
-template<int kPart>
-void launch_vertical_part(const Geometry& g, const Phys& P, const State& s, double dt,
+template<int kPart, bool kUni>
+void launch_vertical_part_t(const Geometry& g, const Phys& P, const State& s, double dt,
                           cudaStream_t st) {
     const size_t     smem = vertical_smem_bytes(g);
     static SmemOptIn opt;
-    if (opt.ensure(vertical_kernel<kPart>, smem) != cudaSuccess)
+    if (opt.ensure(vertical_kernel<kPart, kUni>, smem) != cudaSuccess)
         return;
     // the carveout: shared memory for the 3 CTAs an SM holds (register-limited), the rest is L1
     // for the neighbour gathers (a hint; 228 KB is the most shared memory an SM has)
     static bool carve = false;
     if (!carve) {
         const int pct = (int)std::min<size_t>(100, (3 * (smem + 1024) * 100 + 233471) / 233472);
-        cudaFuncSetAttribute(vertical_kernel<kPart>, cudaFuncAttributePreferredSharedMemoryCarveout,
+        cudaFuncSetAttribute(vertical_kernel<kPart, kUni>, cudaFuncAttributePreferredSharedMemoryCarveout,
                              pct);
         carve = true;
     }
-    vertical_kernel<kPart><<<tile_grid(g), tile_block(), smem, st>>>(g, P, s, dt);
+    vertical_kernel<kPart, kUni><<<tile_grid(g), tile_block(), smem, st>>>(g, P, s, dt);
+}
+template<int kPart>
+void launch_vertical_part(const Geometry& g, const Phys& P, const State& s, double dt,
+                          cudaStream_t st) {
+    if (P.uniform_thermo)
+        launch_vertical_part_t<kPart, true>(g, P, s, dt, st);
+    else
+        launch_vertical_part_t<kPart, false>(g, P, s, dt, st);
 }
 void launch_vertical(const Geometry& g, const Phys& P, const State& s, double dt, int part,
                      cudaStream_t st) {

@@ -55,6 +55,9 @@ struct thorx_ctx {
     Sponge                           sp{};                   // Rayleigh sponge (nlat 0: off)
     std::vector<thorx_module>        modules;                // physics modules, in call order
     bool                             eager = false;          // thorx_step without a graph
+    // uniform thermodynamics (Phys::uniform_thermo): the last host arrays set for Rd and Cp were
+    // uniform at the scalar values; thermo_escaped: a module holds their device pointers
+    bool                             rd_uniform = false, cp_uniform = false, thermo_escaped = false;
     RkArrays                         rk_arrays{};            // their RK-updated arrays
     Surrogate*                       sur         = nullptr; // RT surrogate (thorx_surrogate_create)
     int                              sur_mode    = THORX_SUR_OFF;
@@ -321,15 +324,17 @@ double class_bytes(const thorx_ctx* ctx, int k) {
     const double S = 8.0 * N * nv, Si = 8.0 * N * nvi, G = 8.0 * N, I = 4.0 * N;
     const Phys&  P = ctx->P;
     const double ring_geo = 78 * G + 6 * I + N; // areas, areasTr, nvecoa/ti/te, ring, flag
+    // the Rd and Cp fields, which the dynamical core reads only without uniform thermodynamics
+    const double RdCp = P.uniform_thermo ? 0.0 : 2 * S;
     switch (k) {
     case KProfx: // Wh, p, Rd, Rho, Mh | W, T, p, Mh (+ with the sponge: Mh, sponge tables | Wh)
         return Si + 3 * S + (P.benchmark || ctx->sp.nlat ? 3 * S : 0) + G + 3 * S
                + (P.benchmark || ctx->sp.nlat ? 3 * S : 0) + (ctx->sp.nlat ? 5 * G + I + Si : 0);
     case KAdvTemp: // Mhk, Rhok, Wk, Whk, pk, Rd, Cp | Adv, T, h, hh, pt, pth, gtil, gtilh
-        return 7 * S + Si + 21 * G + 3 * G + 6 * I + 7 * S + 3 * Si
+        return 5 * S + RdCp + Si + 21 * G + 3 * G + 6 * I + 7 * S + 3 * Si
                + (P.energy ? 3 * S + 2 * Si - 2 * S - Si : 0);
     case KDiffFirst: // Rhok, Mhk, Wk, T, Rd (Cp) | diff (6)
-        return (6 + (P.energy ? 1 : 0)) * S + ring_geo + 6 * S;
+        return (5 + (P.energy ? 1 : 0)) * S + RdCp / 2 + ring_geo + 6 * S;
     case KDiffLast: // diff (6), Rhok | diffrh, diffmh, diffw, diffpr
         return 7 * S + ring_geo + 3 * G + 6 * S;
     case KDivm0: // Mh, Wh | divg
@@ -337,13 +342,13 @@ double class_bytes(const thorx_ctx* ctx, int k) {
     case KSlow: // divg, Cp, Rd, Adv, Rhok, pk, Mhk, h, Whk, hh, diffmh, dMh, diffw, dWh, diffrh,
                 // gtil, Qheat, diffpr (+ Mh, Rho, p, Wh) | SlowMh, SlowWh, SlowRho, Slowp (+ Mhs,
                 // Rhos, ps, Whs)
-        return (P.DivDampP ? 3 * S + ring_geo : 0) + 21 * S + 3 * Si + 45 * G + 6 * I
+        return (P.DivDampP ? 3 * S + ring_geo : 0) + 19 * S + RdCp + 3 * Si + 45 * G + 6 * I
                + 5 * S + Si;
     case KMomentum: // divg, ps, SlowMh, Mhs | Mhs
         return (P.DivDampP ? 3 * S + ring_geo : 0) + 7 * S + 24 * G + 6 * I + 3 * S;
     case KVertical: // Mhs, h, Slowp, SlowRho, hh, gtilh, ps, Rhos, SlowWh, Whs, Cp, Rd, Mhk, pt,
                     // pth, Rhok, pk, Whk, Qheat, diffpr | Whs, Rhos, ps
-        return 19 * S + 6 * Si + 21 * G + 6 * I + N + Si + 2 * S;
+        return 17 * S + RdCp + 6 * Si + 21 * G + 6 * I + N + Si + 2 * S;
     case KUpdateRk2: // Mhs, Mhk, Rhok, Rhos, pk, ps, Whk, Whs | Mhk, Rhok, pk, Whk, Wk
         return 10 * S + 2 * Si + 3 * G + 6 * S + Si;
     case KRt: // p, Rho, T, Rd, Cp, Qheat, lat, lon, areasT, insol_ann | phtemp, thtemp, fsw/flw
@@ -539,6 +544,18 @@ int enqueue_thor(thorx_ctx* ctx) {
     return 0;
 }
 
+// drops the captured step graph: the next thorx_step captures the step again
+int drop_graph(thorx_ctx* ctx) {
+    if (ctx->graph_exec) {
+        CK(cudaGraphExecDestroy(ctx->graph_exec));
+        ctx->graph_exec = nullptr;
+    }
+    if (ctx->graph) {
+        CK(cudaGraphDestroy(ctx->graph));
+        ctx->graph = nullptr;
+    }
+    return 0;
+}
 } // namespace
 
 namespace {
@@ -853,6 +870,25 @@ long thorx_field_size(const thorx_ctx* ctx, const char* name) {
     return (long)ctx->g.N * it->second.L * it->second.K;
 }
 
+namespace {
+// Phys::uniform_thermo from the context's record; a change re-captures the step graph (its kernels
+// were instantiated for the other form)
+int update_thermo(thorx_ctx* ctx) {
+    const bool u = ctx->rd_uniform && ctx->cp_uniform && !ctx->thermo_escaped;
+    if (u == ctx->P.uniform_thermo)
+        return 0;
+    ctx->P.uniform_thermo = u;
+    return drop_graph(ctx);
+}
+
+bool all_bits_equal(const double* a, size_t n, double v) {
+    for (size_t i = 0; i < n; i++)
+        if (std::memcmp(a + i, &v, sizeof v) != 0)
+            return false;
+    return true;
+}
+} // namespace
+
 int thorx_set_field(thorx_ctx* ctx, const char* name, const double* host) {
     if (!ctx)
         return THORX_E_ARG;
@@ -870,6 +906,11 @@ int thorx_set_field(thorx_ctx* ctx, const char* name, const double* host) {
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->state_set = true;
+    if (!std::strcmp(name, "Rd") || !std::strcmp(name, "Cp")) {
+        const bool rd = !std::strcmp(name, "Rd");
+        (rd ? ctx->rd_uniform : ctx->cp_uniform) = all_bits_equal(host, n, rd ? ctx->P.Rd : ctx->P.Cp);
+        return update_thermo(ctx);
+    }
     return 0;
 }
 
@@ -1475,17 +1516,6 @@ int thorx_sponge_means(thorx_ctx* ctx, double* vbar, double* Tbar) {
 
 // ---- RT surrogate ------------------------------------------------------------------------------
 namespace {
-int drop_graph(thorx_ctx* ctx) {
-    if (ctx->graph_exec) {
-        CK(cudaGraphExecDestroy(ctx->graph_exec));
-        ctx->graph_exec = nullptr;
-    }
-    if (ctx->graph) {
-        CK(cudaGraphDestroy(ctx->graph));
-        ctx->graph = nullptr;
-    }
-    return 0;
-}
 int sur_check(thorx_ctx* ctx, const char* fn) {
     if (!ctx->sur)
         return fail(ctx, THORX_E_STATE, std::string(fn) + ": no surrogate (thorx_surrogate_create)");
@@ -1937,6 +1967,11 @@ int thorx_device_field(thorx_ctx* ctx, const char* name, double** dev, int* leve
         {"Wk", {&s.Wk, nv, 1}},           {"pressurek", {&s.pk, nv, 1}},
         {"pressures", {&s.ps, nv, 1}},    {"profx_dMh", {&s.dMh, nv, 3}},
         {"profx_dWh", {&s.dWh, nv + 1, 1}}};
+    if (!std::strcmp(name, "Rd") || !std::strcmp(name, "Cp")) { // a module may write them
+        ctx->thermo_escaped = true;
+        if (int rc = update_thermo(ctx))
+            return rc;
+    }
     const FieldDesc* f  = nullptr;
     auto             it = ctx->fields.find(name);
     if (it != ctx->fields.end())

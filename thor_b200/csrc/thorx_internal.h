@@ -107,6 +107,10 @@ struct Phys {
     int    conv_adj_iter; // dry convective adjustment: iterations per step (0: off)
     int    vhd_order;     // vertical hyperdiffusion order (VertHyDiffOrder; 0: off)
     bool   conv_soft;     // its soft form (heating into profx_Qheat instead of T and p)
+    // every cell's Rd and Cp fields hold exactly Rd and Cp above (kept by the context: set from the
+    // host arrays given to thorx_set_field, off for good once a module holds the fields' device
+    // pointers); the dynamical-core kernels then use the scalars (rd_at, cp_at)
+    bool   uniform_thermo;
 };
 
 // Prognostic state (start of large step "x", RK stage "xk", small-step deviation "xs"),
