@@ -383,6 +383,101 @@ def rt_surrogate_leg(torch, thor_b200, nlog=200, iters=5000, batch=8192, nsteps=
         return {"unavailable": "%s" % e}
 
 
+def zonal_mean_T(grid, T, nv, bands=36):
+    """Area-weighted mean temperature over 5-degree latitude bands, [band][lev]."""
+    N = grid.point_num
+    lat = grid["lonlat"][1::2]
+    w = grid["areasT"][:N]
+    band = np.clip(((lat + np.pi / 2) / np.pi * bands).astype(int), 0, bands - 1)
+    T = T.reshape(N, nv)
+    out = np.zeros((bands, nv))
+    for b in range(bands):
+        m = band == b
+        out[b] = (w[m][:, None] * T[m]).sum(0) / w[m].sum()
+    return out
+
+
+def config4_leg(torch, thor_b200, nsteps=2000, nlog=60, iters=5000, batch=8192, glevel=7):
+    """The large run: Held-Suarez at glevel 7 (163842 columns) x 48 levels, dt = 300 s, with the
+    double-gray RT (Earth orbit and rotation; the RT configuration's gray opacities), all state in
+    HBM, every step one CUDA graph replay. The all-FP64 form with the plain RT runs all nsteps as the
+    judge; the mixed form logs the plain RT for the first nlog steps, trains the L48 surrogate
+    (97 -> 512 x 3 -> 48) on the GPU, and runs the remaining steps with it. Reports both forms'
+    speed, the surrogate's re-check statistics, the mixed form's errors against the judge (fields,
+    zonal-mean temperature) and the global mass drift of each."""
+    nv, dt = 48, 300.0
+    p = dict(EARTH, timestep=dt)
+    rt = dict(Tstar=5772.0, radius_star=695700000.0, planet_star_dist=149597870700.0,
+              diff_ang=0.5, Tint=0.0, albedo=0.3, kappa_sw=4e-4, kappa_lw=1e-3,
+              kappa_lw_pole=1e-3, n_sw=1.0, n_lw=2.0, f_lw=0.5, sync_rot=0,
+              mean_motion=1.991e-7, alpha_i=0.0)
+    t0 = time.perf_counter()
+    grid = thor_b200.Icogrid(glevel, nv, A=EARTH["A"], Top_altitude=EARTH["Top_altitude"])
+    grid_s = time.perf_counter() - t0
+    N = grid.point_num
+    stream = torch.cuda.Stream()
+    out = {"workload": "Held-Suarez + double-gray RT g%d/L%d dt=%g (%d columns), %d steps"
+                       % (glevel, nv, dt, N, nsteps), "grid_seconds": grid_s}
+
+    def timed(x, n):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        x.step(n)
+        e1.record(stream)
+        e1.synchronize()
+        x.sync()
+        return e0.elapsed_time(e1)
+
+    # the judge: all FP64, plain RT
+    x = thor_b200.Thorx(grid.as_dict(), glevel, dict(p, precision=thor_b200.FP64),
+                        stream=stream.cuda_stream)
+    x.init_rest_state(TMEAN, SEED, NOISE)
+    x.rt_enable(rt)
+    m0 = x.globdiag()[1]
+    ms = timed(x, nsteps)
+    judge = {f: x.get(f) for f in ("Rho", "pressure", "temperature", "Mh", "Wh")}
+    out["fp64_plain_rt"] = {"ms_per_step": ms / nsteps,
+                            "value": sim_days_per_hour(nsteps, ms / 1000.0, dt=dt),
+                            "mass_drift": abs(x.globdiag()[1] - m0) / m0}
+    x.close()
+    # mixed form + surrogate
+    x = thor_b200.Thorx(grid.as_dict(), glevel, dict(p, precision=thor_b200.MIXED),
+                        stream=stream.cuda_stream)
+    x.init_rest_state(TMEAN, SEED, NOISE)
+    x.rt_enable(rt)
+    x.sur_create(hidden=512, train_batch=batch, log_capacity=nlog * N, recheck_period=16,
+                 tolerance=0.05, seed=SEED)
+    m0 = x.globdiag()[1]
+    x.sur_mode(thor_b200.SUR_LOG)
+    ms_log = timed(x, nlog)
+    t1 = time.perf_counter()
+    first, last = x.sur_train(iters - iters // 5, batch, lr=1e-3)
+    _, last = x.sur_train(iters // 5, batch, lr=2e-4)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t1
+    x.sur_mode(thor_b200.SUR_USE)
+    x.sur_stats()
+    nuse = nsteps - nlog
+    ms_use = timed(x, nuse)
+    st = x.sur_stats()
+    mix = {f: x.get(f) for f in ("Rho", "pressure", "temperature", "Mh", "Wh")}
+    out["mixed_surrogate"] = {
+        "ms_per_step": ms_use / nuse, "value": sim_days_per_hour(nuse, ms_use / 1000.0, dt=dt),
+        "mass_drift": abs(x.globdiag()[1] - m0) / m0,
+        "logging_ms_per_step": ms_log / nlog,
+        "training": {"columns_logged": nlog * N, "iterations": iters, "batch": batch,
+                     "loss_first": first, "loss_last": last, "seconds": train_s},
+        "recheck": {"steps": nuse, "rechecked": st["rechecked"], "failed": st["failed"],
+                    "max_rel_err": st["max_err"], "rt_column_fraction": st["rt_columns"] / (nuse * N)}}
+    x.close()
+    out["ratio"] = out["fp64_plain_rt"]["ms_per_step"] / out["mixed_surrogate"]["ms_per_step"]
+    out["mixed_vs_fp64"] = {f: float(np.abs(mix[f] - judge[f]).max() / np.abs(judge[f]).max())
+                            for f in judge}
+    tz = np.abs(zonal_mean_T(grid, mix["temperature"], nv) - zonal_mean_T(grid, judge["temperature"], nv))
+    out["zonal_mean_T_max_diff_K"] = float(tz.max())
+    return out
+
+
 def run_ours(args):
     import torch
     import thor_b200
@@ -529,12 +624,22 @@ def main():
     ap.add_argument("--sur-log-steps", type=int, default=200,
                     help="plain-RT steps logged for training (surrogate leg)")
     ap.add_argument("--sur-iters", type=int, default=5000, help="Adam iterations (surrogate leg)")
+    ap.add_argument("--config4", action="store_true",
+                    help="run only the large g7/L48 Held-Suarez + surrogate-RT leg (2000 steps in "
+                         "two forms, several minutes) and print its JSON object")
     args = ap.parse_args()
     set_workload(args.glevel, args.nv)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
         return run_reference(args)
+    if args.config4:
+        import torch
+        import thor_b200
+        # glevel 7 unless --glevel names another (smaller cases for checks)
+        print(json.dumps(config4_leg(torch, thor_b200, nsteps=args.steps,
+                                     glevel=7 if args.glevel == 6 else args.glevel)), flush=True)
+        return 0
     if args.surrogate_only:
         import torch
         import thor_b200

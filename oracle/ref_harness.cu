@@ -372,59 +372,29 @@ extern "C" long ref_sim_get(void* h, const char* name, double* host) {
 // RT module. rtm_dual_band and annual_insol are the reference's own kernels
 // (src/physics/modules/inc/profx_RT.h); the argument list and the host logic around them follow
 // radiative_transfer::phy_loop (src/physics/modules/src/radiative_transfer.cu:769-1105) and
-// RTSetup (:1393-1437). The insolation step (src/ESP/insolation.cu) cannot be compiled here: its
-// header pulls the HDF5 storage header in through a quote include that the storage shim cannot
-// shadow. Its few lines of orbit and zenith arithmetic are therefore restated below (host orbit
-// update, one device kernel for the zenith angles).
+// RTSetup (:1393-1437). The orbit and zenith arithmetic is the reference's own, compiled from
+// src/ESP/insolation.cu (oracle/Makefile builds it with a copy of its header whose storage include
+// resolves to the shim): the free functions solve_kepler, calc_r_orb, ecc2true_anomaly,
+// true2ecc_anomaly and the kernel compute_cos_zenith_angles (calc_zenith, insolation.cu:128-207).
+// Only Insolation::update_spin_orbit (insolation.cu:514-529), a private member of a class whose
+// object needs a whole ESP, is restated here, on those functions.
 // ---------------------------------------------------------------------------------------------
-static double h_solve_kepler(double M, double ecc) { // insolation.cu:65-88
-    double E = M + (sin(M) < 0.0 ? -1.0 : 1.0) * 0.85 * ecc, d3 = 1.0;
-    for (int it = 0; it < 100 && d3 > 1e-15; it++) {
-        double fi = E - ecc * sin(E) - M, f1 = 1.0 - ecc * cos(E), f2 = ecc * sin(E), f3 = ecc * cos(E);
-        double d1 = -fi / f1;
-        double d2 = -fi / (f1 + 0.5 * d1 * f2);
-        d3        = -fi / (f1 + 0.5 * d2 * f2 + 1. / 6. * d2 * d2 * f3);
-        E         = E + d3;
-    }
-    return E;
-}
-static double h_ecc2true(double E, double ecc) { // insolation.cu:97-106
-    double f = 2.0 * atan(sqrt((1.0 + ecc) / (1.0 - ecc)) * tan(E / 2.0));
-    return f < 0.0 ? f + 2 * M_PI : f;
-}
-static double h_true2ecc(double f, double ecc) { // insolation.cu:108-125
-    while (f < 0.0)
-        f += 2 * M_PI;
-    while (f >= 2 * M_PI)
-        f -= 2 * M_PI;
-    double cosE = (cos(f) + ecc) / (1.0 + ecc * cos(f));
-    return f < M_PI ? acos(cosE) : 2 * M_PI - acos(cosE);
-}
+double solve_kepler(double mean_anomaly, double ecc);
+double calc_r_orb(double ecc_anomaly, double ecc);
+double ecc2true_anomaly(double ecc_anomaly, double ecc);
+double true2ecc_anomaly(double true_anomaly, double ecc);
+__global__ void compute_cos_zenith_angles(double* cos_zenith_angles, double* lonlat_d, double alpha,
+                                          double alpha_i, double sin_decl, double cos_decl,
+                                          double ecc, double obliquity, bool sync_rot,
+                                          int num_points);
 static void h_update_spin_orbit(RefSim* s, double time) { // insolation.cu:514-529
     double M         = fmod((s->mean_motion * time + s->mean_anomaly_i), (2 * M_PI));
-    double E         = fmod(h_solve_kepler(M, s->ecc), (2 * M_PI));
-    s->r_orb         = 1.0 - s->ecc * cos(E);
-    double true_long = fmod((h_ecc2true(E, s->ecc) + s->longp), (2 * M_PI));
+    double E         = fmod(solve_kepler(M, s->ecc), (2 * M_PI));
+    s->r_orb         = calc_r_orb(E, s->ecc);
+    double true_long = fmod((ecc2true_anomaly(E, s->ecc) + s->longp), (2 * M_PI));
     s->sin_decl      = sin(s->obliquity) * sin(true_long);
     s->cos_decl      = sqrt(1.0 - s->sin_decl * s->sin_decl);
     s->alpha         = -s->p.Omega * time + true_long - s->true_long_i + s->alpha_i;
-}
-__global__ void h_cos_zenith(double* cz, const double* lonlat, double alpha, double alpha_i,
-                             double sin_decl, double cos_decl, int sync_rot, double ecc,
-                             double obliquity, int N) { // insolation.cu:128-207
-    int id = blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= N)
-        return;
-    double lon = lonlat[id * 2], lat = lonlat[id * 2 + 1], c;
-    bool   obl = !(obliquity < 1e-10);
-    if (sync_rot && ecc < 1e-10)
-        c = obl ? (sin(lat) * sin_decl + cos(lat) * cos_decl * cos(lon - alpha_i))
-                : cos(lat) * cos(lon - alpha_i);
-    else if (sync_rot && !obl)
-        c = cos(lat) * cos(lon - alpha);
-    else
-        c = (sin(lat) * sin_decl + cos(lat) * cos_decl * cos(lon - alpha));
-    cz[id] = c < 0.0 ? 0.0 : c;
 }
 
 extern "C" int ref_sim_rt(void* h, const ref_rt_params* rp) {
@@ -453,7 +423,7 @@ extern "C" int ref_sim_rt(void* h, const ref_rt_params* rp) {
     s->longp          = rp->longp * M_PI / 180.0;
     s->ecc            = rp->ecc;
     double f_i        = fmod(s->true_long_i - s->longp, (2 * M_PI));
-    double E_i        = h_true2ecc(f_i, s->ecc);
+    double E_i        = true2ecc_anomaly(f_i, s->ecc);
     s->mean_anomaly_i = fmod(E_i - s->ecc * sin(E_i), (2 * M_PI));
     s->alpha_i        = rp->alpha_i * M_PI / 180.0;
     s->obliquity      = rp->obliquity * M_PI / 180.0;
@@ -722,9 +692,9 @@ static int ref_rt_step(RefSim* s) {
     }
     else
         h_update_spin_orbit(s, nstep * dt);
-    h_cos_zenith<<<(N / NTH) + 1, NTH>>>(F["cos_zenith"], F["lonlat"], s->alpha, s->alpha_i,
-                                         s->sin_decl, s->cos_decl, s->R.sync_rot, s->ecc,
-                                         s->obliquity, N);
+    compute_cos_zenith_angles<<<(N / NTH) + 1, NTH>>>(F["cos_zenith"], F["lonlat"], s->alpha,
+                                                      s->alpha_i, s->sin_decl, s->cos_decl, s->ecc,
+                                                      s->obliquity, s->R.sync_rot, N);
     REF_CHECK(cudaDeviceSynchronize());
     bool   run           = true;
     double Qheat_scaling = 1.0;

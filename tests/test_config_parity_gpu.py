@@ -126,6 +126,9 @@ def test_hot_jupiter_rt_g5_l40_matches_reference():
     for h in sims:
         h.step(1, profx=True, thor=False)
     bad1, res1 = compare(x, sims, RT_FIELDS + ["pressure", "temperature"])
+    # synchronous rotation on a circular orbit: the zenith angles of the reference binary's
+    # calc_zenith (src/ESP/insolation.cu:128-207), bit for bit
+    assert np.array_equal(x.get("cos_zenith"), sims[0].get("cos_zenith"))
     # then the dynamical core of that step and a second full step (graph replay)
     x.thor()
     x.step(1)

@@ -2164,6 +2164,14 @@ __global__ void __launch_bounds__(kVdCols) vertical_diff_kernel(Geometry g, Phys
 #ifndef THORX_VERT_SMEM
 #define THORX_VERT_SMEM 2
 #endif
+#ifndef THORX_VG
+#define THORX_VG 0
+#endif
+#if THORX_VG >= 1
+#define VLD(p) __ldg(p)
+#else
+#define VLD(p) (*(p))
+#endif
 constexpr bool kVertMerge = THORX_VERT_MERGE != 0;
 // Where the per-level work arrays live: 2 all in shared memory; 1 Sp and Sd in shared memory, Fr,
 // Fpt and the eliminated coefficients in global scratch planes; 0 all in global scratch (shared
@@ -2194,24 +2202,57 @@ __device__ __forceinline__ void vert_gathers(const Geometry& g, const Phys& P, c
     const double  rscale = g.lt[kLtRscale * g.nvi + lev]; // 1 in the shallow model
     double        sdv[3], spv[3], st[3];
     const double* h   = s.h + lev * Np;
+#if THORX_VG >= 2
+    // every gather of the level issued before any is used
+    double LH[7], LM[7][3], LK[7][3], LP[7], LE[7], LEK[7];
+#pragma unroll
+    for (int j = 0; j < 7; j++) {
+        const int id = nb[j];
+        const int q  = lev * Np + (id >= 0 ? id : 0);
+        LH[j]        = (kSpSd || (kFlux && eeq)) && id >= 0 ? VLD(s.h + q) : 0.0;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            LM[j][k] = id >= 0 ? VLD(s.Mhs + (size_t)k * nv * Np + q) : 0.0;
+            LK[j][k] = kFlux && id >= 0 ? VLD(s.Mhk + (size_t)k * nv * Np + q) : 0.0;
+        }
+        LP[j]  = kFlux && !eeq && id >= 0 ? VLD(s.pt + q) : 0.0;
+        LE[j]  = kFlux && eeq && id >= 0 ? VLD(s.ep + q) : 0.0;
+        LEK[j] = kFlux && eeq && id >= 0 ? VLD(s.ek + q) : 0.0;
+    }
+#endif
 #pragma unroll
     for (int j = 0; j < 7; j++) {
         const int id = nb[j];
         double    hv = 0.0, ms[3] = {0.0, 0.0, 0.0}, v1[3] = {0.0, 0.0, 0.0}, ptv = 0.0;
+#if THORX_VG >= 2
         if (id >= 0) {
-            const int q = lev * Np + id;
-            if (kSpSd || (kFlux && eeq))
-                hv = h[id];
+            hv = LH[j];
 #pragma unroll
             for (int k = 0; k < 3; k++)
-                ms[k] = s.Mhs[(k * nv + lev) * Np + id];
+                ms[k] = LM[j][k];
             if (kFlux) {
 #pragma unroll
                 for (int k = 0; k < 3; k++)
-                    v1[k] = ms[k] + s.Mhk[(k * nv + lev) * Np + id];
-                ptv = eeq ? (hv + s.ep[q] + s.ek[q]) : s.pt[q];
+                    v1[k] = ms[k] + LK[j][k];
+                ptv = eeq ? (hv + LE[j] + LEK[j]) : LP[j];
             }
         }
+#else
+        if (id >= 0) {
+            const int q = lev * Np + id;
+            if (kSpSd || (kFlux && eeq))
+                hv = VLD(h + id);
+#pragma unroll
+            for (int k = 0; k < 3; k++)
+                ms[k] = VLD(s.Mhs + (k * nv + lev) * Np + id);
+            if (kFlux) {
+#pragma unroll
+                for (int k = 0; k < 3; k++)
+                    v1[k] = ms[k] + VLD(s.Mhk + (k * nv + lev) * Np + id);
+                ptv = eeq ? (hv + VLD(s.ep + q) + VLD(s.ek + q)) : VLD(s.pt + q);
+            }
+        }
+#endif
         // explicit roundings: the fused and the split launches (and every instantiation) give the
         // same bits whatever the compiler would contract
 #pragma unroll
