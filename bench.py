@@ -330,7 +330,7 @@ def rt_params_planet():
 
 
 def rt_surrogate_leg(torch, thor_b200, nlog=200, iters=5000, batch=8192, nsteps=20,
-                     catch=True):
+                     catch=True, online_chunks=5, online_every=20, online_iters=300):
     """Plain FP64 + RT against mixed + trained surrogate RT on the RT configuration (g5/L40):
     time the plain form, log the plain RT, train the surrogate on the GPU, time the other form."""
     try:
@@ -354,6 +354,24 @@ def rt_surrogate_leg(torch, thor_b200, nlog=200, iters=5000, batch=8192, nsteps=
             _, last = x.sur_train(n_fine, batch, lr=2e-4)
         torch.cuda.synchronize()
         train_s = time.perf_counter() - t0
+        # online learning: the surrogate runs, the columns the plain RT re-checks or falls back to
+        # are logged, and the network trains between chunks of steps
+        x.sur_mode(thor_b200.SUR_USE_LOG)
+        x.sur_stats()
+        t1, online = time.perf_counter(), {"steps": 0, "rt_columns": 0, "rechecked": 0, "failed": 0}
+        for _ in range(online_chunks):
+            x.step(online_every)
+            x.sync()
+            so = x.sur_stats()
+            for k in ("rt_columns", "rechecked", "failed"):
+                online[k] += so[k]
+            online["steps"] += online_every
+            x.sur_train(online_iters, batch, lr=2e-4)
+        torch.cuda.synchronize()
+        online["seconds"] = time.perf_counter() - t1
+        online["rt_column_fraction"] = online["rt_columns"] / max(1, online["steps"] * grid.point_num)
+        online["what"] = ("%d chunks of %d steps, %d Adam steps (lr 2e-4) after each"
+                          % (online_chunks, online_every, online_iters))
         x.sur_mode(thor_b200.SUR_USE)
         x.sur_stats()
         ms_sur = time_steps(x, stream, thor_b200.MIXED, nsteps)
@@ -374,6 +392,7 @@ def rt_surrogate_leg(torch, thor_b200, nlog=200, iters=5000, batch=8192, nsteps=
                 "training": {"columns_logged": nlog * N, "iterations": iters, "batch": batch,
                              "lr": "1e-3, last fifth 2e-4", "loss_first": first,
                              "loss_last": last, "seconds": train_s},
+                "online_learning": online,
                 "recheck": {"steps": nsteps + 3, "rechecked": st["rechecked"],
                             "failed": st["failed"], "max_rel_err": st["max_err"],
                             "rt_column_fraction": st["rt_columns"] / ((nsteps + 3) * N)}}
@@ -397,14 +416,17 @@ def zonal_mean_T(grid, T, nv, bands=36):
     return out
 
 
-def config4_leg(torch, thor_b200, nsteps=2000, nlog=60, iters=5000, batch=8192, glevel=7):
+def config4_leg(torch, thor_b200, nsteps=2000, nlog=60, iters=5000, batch=8192, glevel=7,
+                chunk=100, online_iters=300):
     """The large run: Held-Suarez at glevel 7 (163842 columns) x 48 levels, dt = 300 s, with the
     double-gray RT (Earth orbit and rotation; the RT configuration's gray opacities), all state in
     HBM, every step one CUDA graph replay. The all-FP64 form with the plain RT runs all nsteps as the
     judge; the mixed form logs the plain RT for the first nlog steps, trains the L48 surrogate
-    (97 -> 512 x 3 -> 48) on the GPU, and runs the remaining steps with it. Reports both forms'
-    speed, the surrogate's re-check statistics, the mixed form's errors against the judge (fields,
-    zonal-mean temperature) and the global mass drift of each."""
+    (97 -> 512 x 3 -> 48) on the GPU, and runs the remaining steps with it, learning online
+    (the columns the plain RT re-checks or falls back to are logged; online_iters Adam steps
+    after every chunk of steps). Reports both forms' speed, the surrogate's re-check statistics,
+    the mixed form's errors against the judge (fields, zonal-mean temperature) and the global mass
+    drift of each."""
     nv, dt = 48, 300.0
     p = dict(EARTH, timestep=dt)
     rt = dict(Tstar=5772.0, radius_star=695700000.0, planet_star_dist=149597870700.0,
@@ -455,16 +477,33 @@ def config4_leg(torch, thor_b200, nsteps=2000, nlog=60, iters=5000, batch=8192, 
     _, last = x.sur_train(iters // 5, batch, lr=2e-4)
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t1
-    x.sur_mode(thor_b200.SUR_USE)
+    # the remaining steps in chunks with online learning: the columns the plain RT ran on are
+    # logged, and the network trains between chunks (graph replays timed, training apart)
+    x.sur_mode(thor_b200.SUR_USE_LOG)
     x.sur_stats()
-    nuse = nsteps - nlog
-    ms_use = timed(x, nuse)
-    st = x.sur_stats()
+    nuse, ms_use, st = nsteps - nlog, 0.0, {"rechecked": 0, "failed": 0, "rt_columns": 0, "max_err": 0.0}
+    online_s, left = 0.0, nsteps - nlog
+    while left > 0:
+        n = min(chunk, left)
+        ms_use += timed(x, n)
+        so = x.sur_stats()
+        for k in ("rechecked", "failed", "rt_columns"):
+            st[k] += so[k]
+        st["max_err"] = max(st["max_err"], so["max_err"])
+        left -= n
+        if left > 0:
+            t2 = time.perf_counter()
+            x.sur_train(online_iters, batch, lr=2e-4)
+            torch.cuda.synchronize()
+            online_s += time.perf_counter() - t2
     mix = {f: x.get(f) for f in ("Rho", "pressure", "temperature", "Mh", "Wh")}
     out["mixed_surrogate"] = {
         "ms_per_step": ms_use / nuse, "value": sim_days_per_hour(nuse, ms_use / 1000.0, dt=dt),
         "mass_drift": abs(x.globdiag()[1] - m0) / m0,
         "logging_ms_per_step": ms_log / nlog,
+        "online_learning": {"chunk_steps": chunk, "adam_steps_per_chunk": online_iters,
+                            "seconds": online_s,
+                            "amortised_ms_per_step": online_s * 1000.0 / nuse},
         "training": {"columns_logged": nlog * N, "iterations": iters, "batch": batch,
                      "loss_first": first, "loss_last": last, "seconds": train_s},
         "recheck": {"steps": nuse, "rechecked": st["rechecked"], "failed": st["failed"],

@@ -339,10 +339,14 @@ int thorx_check_division(long long n, unsigned long long seed, long long mismatc
  *                  plain RT's heating. The cooling limiter and profx_Qheat coupling of the plain
  *                  RT apply to the chosen heating. ASR/OLR are current only on the columns the
  *                  plain RT ran on.
+ *   THORX_SUR_USE_LOG as THORX_SUR_USE, and every column the plain RT ran on (re-checked or
+ *                  fallen back) is appended to the log ring, so that training between steps
+ *                  follows the states the run reaches (online learning; needs log_capacity > 0).
  * Requires thorx_rt_enable first. */
 #define THORX_SUR_OFF 0
 #define THORX_SUR_LOG 1
 #define THORX_SUR_USE 2
+#define THORX_SUR_USE_LOG 3
 typedef struct {
     int                hidden;         /* hidden width, a multiple of 256 (512)               */
     int                train_batch;    /* largest training batch, a multiple of 128 (8192)     */

@@ -135,3 +135,69 @@ def test_training_on_logged_columns_and_in_step_use():
     # two re-checks is caught at the next one
     assert change_err < 0.2, change_err
     assert rt_fraction < 0.5, (st, rt_fraction)
+
+
+@pytest.mark.gpu
+def test_surrogate_from_a_state_it_was_not_trained_on():
+    """Train on 48 logged plain-RT steps, run 32 more plain steps to a state S1 that was never
+    logged, then run 32 steps from S1 three ways: the plain RT (the judge), the surrogate as
+    trained, and the surrogate with online learning (THORX_SUR_USE_LOG: the columns the plain RT
+    re-checks or falls back to go into the log, and the network trains 200 Adam steps every 8
+    physics steps). States the fraction of column-steps the plain RT still ran on and the error of
+    the temperature change against the judge's, for both."""
+    nlog, nfree, nuse = 48, 32, 32
+    x, g = make_ctx(train_batch=2048, log_capacity=nlog * 2562, recheck_period=16,
+                    tolerance=0.05, seed=7)
+    N = g.point_num
+    fields = ["Rho", "pressure", "Mh", "Wh", "W", "temperature"]
+    x.step(4)
+    x.sur_mode(thor_b200.SUR_LOG)
+    x.step(nlog)
+    x.sync()
+    first, last = x.sur_train(2000, 2048, lr=1e-3)
+    x.sur_mode(thor_b200.SUR_OFF)
+    x.step(nfree)
+    x.sync()
+    s1 = {f: x.get(f) for f in fields}
+    W0 = [x.sur_layer(l) for l in range(4)]
+
+    def run(mode, online=False):
+        for f, v in s1.items():
+            x.set(f, v)
+        for l, (W, b) in enumerate(W0):  # every run starts from the same trained network
+            x.sur_set_layer(l, W, b)
+        x.sur_mode(mode)
+        x.sur_stats()
+        rt_cols, re, fa = 0, 0, 0
+        for _ in range(nuse // 8):
+            x.step(8)
+            x.sync()
+            st = x.sur_stats()
+            rt_cols, re, fa = rt_cols + st["rt_columns"], re + st["rechecked"], fa + st["failed"]
+            if online:
+                x.sur_train(200, 2048, lr=2e-4)
+        return {f: x.get(f) for f in fields}, rt_cols / (nuse * N), (re, fa)
+
+    plain, _, _ = run(thor_b200.SUR_OFF)
+    used, frac_used, st_used = run(thor_b200.SUR_USE)
+    online, frac_online, st_online = run(thor_b200.SUR_USE_LOG, online=True)
+    x.close(), g.close()
+    dT_plain = plain["temperature"] - s1["temperature"]
+
+    def change_err(r):
+        return np.max(np.abs((r["temperature"] - s1["temperature"]) - dT_plain)) / np.max(np.abs(dT_plain))
+
+    e_used, e_online = change_err(used), change_err(online)
+    print("surrogate from an unlogged state: loss %.3g -> %.3g; as trained: RT fraction %.3f, "
+          "re-checks %s, dT error %.3g; online: RT fraction %.3f, re-checks %s, dT error %.3g"
+          % (first, last, frac_used, st_used, e_used, frac_online, st_online, e_online))
+    for r in (used, online):
+        for f in fields:
+            assert np.all(np.isfinite(r[f])), f
+    assert st_used[0] == 2 * N and st_online[0] == 2 * N  # every column re-checked twice
+    # measured on a B200: as trained, every re-check from S1 fails (the network does not
+    # generalise beyond the logged states); the plain RT runs on 0.77 of the column-steps and the
+    # temperature change is off by 0.25 of itself before the fallbacks catch up. With online
+    # learning nearly every column falls back (0.99) and the error stays at 0.06.
+    assert e_used < 0.5 and e_online < 0.2, (e_used, e_online)
+    assert frac_used < 1.0 and frac_online <= 1.0

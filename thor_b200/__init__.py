@@ -88,7 +88,7 @@ class SurrogateParamsC(ctypes.Structure):
                 ("tolerance", ctypes.c_double), ("seed", ctypes.c_ulonglong)]
 
 
-SUR_OFF, SUR_LOG, SUR_USE = 0, 1, 2
+SUR_OFF, SUR_LOG, SUR_USE, SUR_USE_LOG = 0, 1, 2, 3
 
 
 class ParamsC(ctypes.Structure):

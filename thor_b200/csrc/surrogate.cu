@@ -348,6 +348,29 @@ __global__ void log_write_kernel(SurLog lg, SurNet net, Geometry g, State s, RtF
     x[2 * net.nv] = (float)f.cos_zenith[id];
 }
 
+// Online logging in surrogate mode: each column the plain RT ran on this step (fallen back, or
+// re-checked: the predicate of rt_column_kernel) takes the next row of the ring, with its raw
+// heating rate (before the combine's limiter, as the RT computed it).
+__global__ void log_used_kernel(SurLog lg, SurNet net, Geometry g, State s, RtFields f) {
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= g.N)
+        return;
+    const RtStep st = *f.step;
+    if (!st.run || !(f.fallback[id] || id % f.period == (int)(st.cur % f.period)))
+        return;
+    const long long n   = (long long)atomicAdd((unsigned long long*)lg.count, 1ull);
+    const long long row = n % lg.cap;
+    float*          x   = lg.X + (size_t)row * net.n_in;
+    float*          y   = lg.Y + (size_t)row * net.nv;
+    for (int lev = 0; lev < net.nv; lev++) {
+        const size_t i  = (size_t)lev * g.Np + id;
+        x[lev]          = (float)s.T[i];
+        x[net.nv + lev] = (float)log(s.p[i]);
+        y[lev]          = (float)(f.dtemp[i] / (s.Rho[i] * (s.Cp[i] - s.Rd[i]))); // K/s
+    }
+    x[2 * net.nv] = (float)f.cos_zenith[id];
+}
+
 // Mean and standard deviation of column j of a [rows][ld] f32 table (one block per column).
 __global__ void stats_kernel(const float* X, long long rows, int ld, float* mean, float* stdv) {
     __shared__ double s1[256], s2[256];
@@ -611,6 +634,10 @@ void Surrogate::step_combine(const Geometry& g, const Phys& P, const State& s, c
                              cudaStream_t st) {
     combine_kernel<<<(g.N + 31) / 32, 32 * kCombGroups, 0, st>>>(net, g, P, s, f, Yt, Bcap, fallback,
                                                                  period, tol, stats);
+}
+
+void Surrogate::log_used(const Geometry& g, const State& s, const RtFields& f, cudaStream_t st) {
+    log_used_kernel<<<nblk(g.N, 128), 128, 0, st>>>(log, net, g, s, f);
 }
 
 void Surrogate::log_step(const Geometry& g, const State& s, const RtFields& f, cudaStream_t st) {

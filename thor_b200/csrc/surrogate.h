@@ -70,6 +70,8 @@ struct Surrogate {
     void step_combine(const Geometry& g, const Phys& P, const State& s, const RtFields& f,
                       cudaStream_t st);
     void log_step(const Geometry& g, const State& s, const RtFields& f, cudaStream_t st);
+    // the columns the plain RT ran on in surrogate mode (f.fallback, f.period), into the log
+    void log_used(const Geometry& g, const State& s, const RtFields& f, cudaStream_t st);
     void gemm_n(const __nv_bfloat16* A, const __nv_bfloat16* B, int M, int N, int K,
                 const umma::EpiArgs& e, cudaStream_t st);
     void gemm_wgrad(const __nv_bfloat16* A, const __nv_bfloat16* B, int M, int N, int K,

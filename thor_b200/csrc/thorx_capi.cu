@@ -78,6 +78,10 @@ struct thorx_ctx {
 };
 
 namespace {
+// the surrogate heats the columns this step (THORX_SUR_USE, or with online logging)
+bool sur_using(const thorx_ctx* ctx) {
+    return ctx->sur_mode == THORX_SUR_USE || ctx->sur_mode == THORX_SUR_USE_LOG;
+}
 
 int fail(thorx_ctx* c, int code, const std::string& msg) {
     if (c)
@@ -356,7 +360,7 @@ double class_bytes(const thorx_ctx* ctx, int k) {
         return ctx->rt_enabled ? 6 * S + 4 * G + 6 * Si + 6 * S + 6 * G : 0;
     case KSurrogate: // T, p, coszen | features; weights; dtemp (RT columns), Y | dtemp, DG_Qheat,
                      // Qheat (bf16 activations between the layers stay in L2)
-        return (ctx->sur && ctx->sur_mode == THORX_SUR_USE)
+        return (ctx->sur && sur_using(ctx))
                    ? 2 * S + G + 2.0 * ctx->sur->net.Kin * N + 4.0 * ctx->sur->net.Nout * N
                          + 2.0 * (ctx->sur->net.Kin + 2.0 * ctx->sur->net.H + ctx->sur->net.Nout)
                                * ctx->sur->net.H
@@ -378,7 +382,7 @@ int class_launches(const thorx_ctx* ctx, int k) {
     case KProfx: // ProfX, then its pressure update after RT or the modules' phy_loop
         return ctx->rt_enabled || has_phy_loop(ctx) ? 2 : 1;
     case KRt: return ctx->rt_enabled ? 1 : 0;     // one bracket: orbit kernel + column kernel
-    case KSurrogate: return (ctx->sur && ctx->sur_mode == THORX_SUR_USE) ? 1 : 0;
+    case KSurrogate: return (ctx->sur && sur_using(ctx)) ? 1 : 0;
     case KSponge: // ProfX's means, or per RK stage the explicit sponge (and, exp3, its means)
         return !ctx->sp.nlat ? 0 : ctx->sp.mode == 0 ? 1 : ctx->sp.mode == 1 ? 4 : 6;
     case KVertDiff: return (P.HyDiff && P.vhd_order) ? 3 : 0;
@@ -417,7 +421,7 @@ int enqueue_profx(thorx_ctx* ctx) {
         }
         if (!ctx->rt_enabled) {
         }
-        else if (ctx->sur && ctx->sur_mode == THORX_SUR_USE) {
+        else if (ctx->sur && sur_using(ctx)) {
             RtFields fm = ctx->rt_f; // plain RT only on re-checked and fallen-back columns
             fm.fallback = ctx->sur->fallback;
             fm.period   = ctx->sur->period;
@@ -427,6 +431,8 @@ int enqueue_profx(thorx_ctx* ctx) {
             }
             {
                 KScope k(ctx, KSurrogate);
+                if (ctx->sur_mode == THORX_SUR_USE_LOG) // before the combine limits dtemp
+                    ctx->sur->log_used(ctx->g, ctx->s, fm, ctx->stream);
                 ctx->sur->step_features(ctx->g, ctx->s, fm, ctx->stream);
                 ctx->sur->step_combine(ctx->g, ctx->P, ctx->s, fm, ctx->stream);
             }
@@ -1180,7 +1186,7 @@ int thorx_kernels_per_step(const thorx_ctx* ctx) {
     n += ctx->rt_enabled ? 1 : 0; // the RT bracket holds two kernels
     if (ctx->rk_arrays.n > 0)
         n += 5; // UpdateRK's reset in stages 2 and 3, UpdateRK2's accumulation in all three
-    if (ctx->sur && ctx->sur_mode == THORX_SUR_USE)
+    if (ctx->sur && sur_using(ctx))
         n += 5; // features, four GEMMs and the combine in one bracket
     if (ctx->sur && ctx->sur_mode == THORX_SUR_LOG)
         n += 2; // log slot reservation and write
@@ -1569,15 +1575,18 @@ int thorx_surrogate_set_mode(thorx_ctx* ctx, int mode) {
     int rc;
     if ((rc = sur_check(ctx, "thorx_surrogate_set_mode")))
         return rc;
-    if (mode != THORX_SUR_OFF && mode != THORX_SUR_LOG && mode != THORX_SUR_USE)
+    if (mode != THORX_SUR_OFF && mode != THORX_SUR_LOG && mode != THORX_SUR_USE
+        && mode != THORX_SUR_USE_LOG)
         return fail(ctx, THORX_E_ARG, "thorx_surrogate_set_mode: unknown mode");
     if (mode != THORX_SUR_OFF && !ctx->rt_enabled)
         return fail(ctx, THORX_E_STATE, "thorx_surrogate_set_mode: RT is not enabled");
-    if (mode == THORX_SUR_LOG && ctx->sur->log.cap == 0)
+    if ((mode == THORX_SUR_LOG || mode == THORX_SUR_USE_LOG) && ctx->sur->log.cap == 0)
         return fail(ctx, THORX_E_ARG, "thorx_surrogate_set_mode: log_capacity is 0");
-    if (mode == THORX_SUR_USE && !ctx->sur->norm_fitted)
+    const bool using_now = sur_using(ctx);
+    const bool use       = mode == THORX_SUR_USE || mode == THORX_SUR_USE_LOG;
+    if (use && !ctx->sur->norm_fitted)
         return fail(ctx, THORX_E_STATE, "thorx_surrogate_set_mode: the surrogate is not trained");
-    if (mode == THORX_SUR_USE && mode != ctx->sur_mode)
+    if (use && !using_now) // entering the surrogate mode: no column has fallen back yet
         CK(cudaMemsetAsync(ctx->sur->fallback, 0, ctx->g.N, ctx->stream));
     if (mode != ctx->sur_mode && (rc = drop_graph(ctx)))
         return rc;
