@@ -213,6 +213,42 @@ int thorx_rk_register_array_n(thorx_ctx* ctx, double* array, double* arrayk, dou
  * host work or launch on the legacy default stream (the reference's phy_modules_* managers through
  * the thorx_phy shim). 1 (the default) restores graph replay. */
 int thorx_set_graph_mode(thorx_ctx* ctx, int use_graph);
+/* ---- Partitioned step: the grid's columns divided among several contexts (one per GPU, or several
+ * on one GPU), each computing its own columns and taking its halo (the neighbours of its columns
+ * that others compute) from the others after every kernel. The decomposition the reference sketches
+ * for multi-GPU runs (rhombi per rank, a one-cell halo exchanged before every horizontal stencil);
+ * the reference itself runs on one GPU. Every context holds whole-grid arrays; only its own columns
+ * (and, after an exchange, its halo) are current. The state after a step is bit for bit the
+ * unpartitioned one. Not with the Rayleigh sponge, the surrogate, physics modules or
+ * thorx_globdiag (whole-grid sums). ---- */
+/* Restricts ctx to columns [col_begin, col_end): col_begin a multiple of 32, col_end a multiple of
+ * 32 or point_num (whole rhombi qualify: 256 columns each at glevel >= 4; the two poles are the last
+ * columns). A step graph captured earlier is re-captured. */
+int thorx_set_partition(thorx_ctx* ctx, int col_begin, int col_end);
+/* Called after every kernel of a step with the names (as for thorx_device_field) of the fields the
+ * kernel wrote; the callee brings the halo columns of those fields up to date (thorx_copy_columns
+ * between contexts of one process, or thorx_pack_columns / thorx_unpack_columns around a transfer
+ * between processes), stream-ordered on `stream`, and returns 0 (else the step stops with that
+ * code). Setting it makes thorx_step enqueue every step eagerly (thorx_set_graph_mode(ctx, 0)).
+ * NULL removes it. */
+typedef int (*thorx_exchange_fn)(void* user, thorx_ctx* ctx, void* stream,
+                                 const char* const* fields, int nfields);
+int thorx_set_exchange(thorx_ctx* ctx, thorx_exchange_fn fn, void* user);
+/* Host only (no GPU needed): the halo of the columns [col_begin, col_end) of a grid, the columns
+ * outside the range whose values the step's stencils read at those columns, ascending. Writes at
+ * most cap of them to cols (which may be NULL) and returns how many there are, or a negative
+ * status. */
+int thorx_halo_columns(const thorx_grid* grid, int col_begin, int col_end, int* cols, int cap);
+/* All levels and components of the n columns dev_cols (a device array) of a field: copied from src
+ * to dst (contexts of the same grid whose devices can reach each other's memory), or packed to /
+ * unpacked from dev_buf [n][levels * components] (device). Enqueued on dst's / ctx's stream; the
+ * source's last write must be complete (the caller synchronises src). */
+int thorx_copy_columns(thorx_ctx* dst, thorx_ctx* src, const char* field, const int* dev_cols,
+                       int n);
+int thorx_pack_columns(thorx_ctx* ctx, const char* field, const int* dev_cols, int n,
+                       double* dev_buf);
+int thorx_unpack_columns(thorx_ctx* ctx, const char* field, const int* dev_cols, int n,
+                         const double* dev_buf);
 /* The context's device array of a field, for module kernels: *dev, its levels (nv or nv+1), its
  * components (1 or 3) and the plane stride (doubles): element (lev, col, comp) is at
  * dev[(comp * levels + lev) * plane + col]. Names: the thorx_get_field names and the dycore's

@@ -207,8 +207,50 @@ def lib():
         L.thorx_rt_totals.argtypes = [vp, ctypes.POINTER(ctypes.c_double),
                                       ctypes.POINTER(ctypes.c_double)]
         L.thorx_rt_totals.restype = ci
+        L.thorx_set_partition.argtypes = [vp, ci, ci]
+        L.thorx_set_partition.restype = ci
+        L.thorx_set_exchange.argtypes = [vp, EXCHANGE_FN, vp]
+        L.thorx_set_exchange.restype = ci
+        L.thorx_halo_columns.argtypes = [ctypes.POINTER(GridC), ci, ci, vp, ci]
+        L.thorx_halo_columns.restype = ci
+        L.thorx_copy_columns.argtypes = [vp, vp, cp, vp, ci]
+        L.thorx_copy_columns.restype = ci
+        for f in ("thorx_pack_columns", "thorx_unpack_columns"):
+            getattr(L, f).argtypes = [vp, cp, vp, ci, vp]
+            getattr(L, f).restype = ci
+        L.thorx_set_graph_mode.argtypes = [vp, ci]
+        L.thorx_set_graph_mode.restype = ci
         _lib = L
     return _lib
+
+
+# thorx_exchange_fn: (user, ctx, stream, fields, nfields) -> status
+EXCHANGE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                               ctypes.POINTER(ctypes.c_char_p), ctypes.c_int)
+
+
+def grid_struct(grid, glevel):
+    """(thorx_grid, the arrays it points to) from a mapping of reference-layout arrays."""
+    g = GridC(int(grid["point_num"]), int(grid["nv"]), int(grid["nl_region"]), int(grid["nr"]),
+              int(glevel))
+    keep = {}
+    for k in GRID_KEYS:
+        a = np.ascontiguousarray(grid[k], dtype=np.int32 if k in ("maps", "point_local")
+                                 else np.float64)
+        keep[k] = a
+        setattr(g, k, a.ctypes.data)
+    return g, keep
+
+
+def halo_columns(grid, glevel, col_begin, col_end):
+    """The halo of the columns [col_begin, col_end) of a grid (thorx_halo_columns; host only)."""
+    g, keep = grid_struct(grid, glevel)
+    n = lib().thorx_halo_columns(ctypes.byref(g), col_begin, col_end, None, 0)
+    if n < 0:
+        raise ThorxError(n, "thorx_halo_columns")
+    out = np.zeros(max(n, 1), dtype=np.int32)
+    lib().thorx_halo_columns(ctypes.byref(g), col_begin, col_end, out.ctypes.data, n)
+    return out[:n]
 
 
 EXPORTED = ["thorx_create", "thorx_destroy", "thorx_last_error", "thorx_field_size",
@@ -225,7 +267,9 @@ EXPORTED = ["thorx_create", "thorx_destroy", "thorx_last_error", "thorx_field_si
             "thorx_check_division", "thorx_conv_adj_enable", "thorx_init_guillot_state",
             "thorx_sponge_enable", "thorx_sponge_means", "thorx_module_add",
             "thorx_rk_register_array", "thorx_device_field", "thorx_vert_hydiff_enable",
-            "thorx_check_thomas", "thorx_globdiag_fields"]
+            "thorx_check_thomas", "thorx_globdiag_fields", "thorx_set_partition",
+            "thorx_set_exchange", "thorx_halo_columns", "thorx_copy_columns",
+            "thorx_pack_columns", "thorx_unpack_columns", "thorx_set_graph_mode"]
 
 def device_sum(ptr, n, stream=0):
     """Compensated sum of n doubles at device address `ptr` (thorx_device_sum)."""
@@ -474,6 +518,30 @@ class Thorx:
         self._check(lib().thorx_device_field(self.h, name.encode(), ctypes.byref(d),
                                              ctypes.byref(lv), ctypes.byref(k), ctypes.byref(pl)))
         return d.value, lv.value, k.value, pl.value
+
+    def set_partition(self, col_begin, col_end):
+        """Compute only the columns [col_begin, col_end) (thorx_set_partition)."""
+        self._check(lib().thorx_set_partition(self.h, col_begin, col_end))
+
+    def set_exchange(self, fn):
+        """fn(stream, [field names]) -> 0 after every kernel (thorx_set_exchange); None removes."""
+        if fn is None:
+            self._xfn = None
+            self._check(lib().thorx_set_exchange(self.h, EXCHANGE_FN(), None))
+            return
+
+        def cb(user, ctx, stream, fields, n):
+            try:
+                return int(fn(stream, [fields[i].decode() for i in range(n)]))
+            except Exception:  # an exception ends the step with an error, not the process
+                return -100
+        self._xfn = EXCHANGE_FN(cb)  # kept alive as long as the context uses it
+        self._check(lib().thorx_set_exchange(self.h, self._xfn, None))
+
+    def copy_columns(self, src, field, dev_cols, n):
+        """All levels of the n columns at device address dev_cols of `field`, from context src
+        (thorx_copy_columns, on this context's stream)."""
+        self._check(lib().thorx_copy_columns(self.h, src.h, field.encode(), dev_cols, n))
 
     def sponge_means(self):
         """(vbar [bin][lev][3], Tbar [bin][lev]) of the last sponge step."""

@@ -114,7 +114,7 @@ __device__ __forceinline__ int lane_column(const Geometry& g) {
     const int x = threadIdx.x;
     if (tail_cta())
         return x < g.nspecial ? g.special[x] : -1;
-    const int c = blockIdx.x * kTile + x;
+    const int c = (g.tile0 + blockIdx.x) * kTile + x;
     return (c < g.N && !(g.cflag[c] & kRing5)) ? c : -1;
 }
 // Copies rows 0..Q-1 of a [q][Np] grid array for the lanes' columns into smem [q][32].
@@ -685,7 +685,7 @@ constexpr int kProfxCols = 32, kProfxGroups = 8;
 __global__ void __launch_bounds__(kProfxCols* kProfxGroups) profx_kernel(Geometry g, Phys P,
                                                                         Sponge sp, State s,
                                                                         bool finish) {
-    const int  c     = blockIdx.x * kProfxCols + threadIdx.x;
+    const int  c     = (g.tile0 + blockIdx.x) * kProfxCols + threadIdx.x;
     const bool valid = c < g.N;
     const int  y0 = threadIdx.y, dy = kProfxGroups;
     const int     Np = g.Np, nv = g.nv;
@@ -817,8 +817,8 @@ __global__ void __launch_bounds__(kProfxCols* kProfxGroups) profx_kernel(Geometr
 
 // Compute_pressure (profx_auxiliary.h:94-107) and the NaN check, after the physics modules.
 __global__ void __launch_bounds__(kColBlock) profx_finish_kernel(Geometry g, State s) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= g.N)
+    const int c = g.tile0 * kTile + blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= g.col_end)
         return;
     bool bad = false;
     for (int lev = 0; lev < g.nv; lev++) {
@@ -863,7 +863,7 @@ template<bool kUni>
 __global__ void THORX_KATTR_ADV adv_temp_kernel(Geometry g, Phys P, State s) {
     __shared__ double sdiv[21 * kTile];
     __shared__ double sfr[21 * kTile]; // func_r of the 7 stencil points, [point * 3 + k][32]
-    const int         c0 = blockIdx.x * kTile, x = threadIdx.x, c = c0 + x;
+    const int         c0 = (g.tile0 + blockIdx.x) * kTile, x = threadIdx.x, c = c0 + x;
     const int         Np = g.Np, nv = g.nv;
     stage(sdiv, g.div, 21, Np, c0);
     for (int q = threadIdx.y; q < 21; q += blockDim.y) {
@@ -2043,7 +2043,7 @@ constexpr int kVdCols = 32;
 __global__ void __launch_bounds__(kVdCols) vertical_diff_kernel(Geometry g, Phys P, State s) {
     extern __shared__ double vsm[];
     const int nv = g.nv, Np = g.Np, x = threadIdx.x;
-    const int c  = blockIdx.x * kVdCols + x;
+    const int c  = (g.tile0 + blockIdx.x) * kVdCols + x;
     double*   b2 = vsm;                       // [nv + 2][kVdCols]
     double*   d  = vsm + (nv + 2) * kVdCols;  // [nv][kVdCols]
     if (c >= g.N)
@@ -2494,7 +2494,7 @@ __global__ void THORX_KATTR_VERT
     vertical_kernel(Geometry g, Phys P, State s, double deltat) {
     extern __shared__ double smem[];
     const int nv = g.nv, nvi = g.nvi, Np = g.Np;
-    const int c0 = blockIdx.x * kTile, x = threadIdx.x, c = c0 + x;
+    const int c0 = (g.tile0 + blockIdx.x) * kTile, x = threadIdx.x, c = c0 + x;
     double*   sdiv = smem;
     // the four per-level arrays: in shared memory after sdiv, or global scratch planes after the
     // four row planes of s.vrows (kVertSmem)
@@ -2711,7 +2711,7 @@ __global__ void THORX_KATTR_VERT
 constexpr int kRk2Groups = 4;
 
 __global__ void __launch_bounds__(kTile* kRk2Groups) update_rk2_kernel(Geometry g, Phys P, State s) {
-    const int  c  = blockIdx.x * kTile + threadIdx.x;
+    const int  c  = (g.tile0 + blockIdx.x) * kTile + threadIdx.x;
     const int  Np = g.Np, nv = g.nv, nvi = g.nvi;
     const bool active = c < g.N;
     const int  chunk  = (nv + kRk2Groups - 1) / kRk2Groups;
@@ -2762,8 +2762,9 @@ __global__ void __launch_bounds__(kTile* kRk2Groups) update_rk2_kernel(Geometry 
         s.Whk[nv * Np + c] = 0.0;
 }
 
-inline dim3 tile_grid(const Geometry& g) { return dim3(g.Np / kTile); }
-inline dim3 tile_grid_tail(const Geometry& g) { return dim3(g.Np / kTile + 1); }
+// the context's tiles (all of them without a partition), and the same plus the five-neighbour tail
+inline dim3 tile_grid(const Geometry& g) { return dim3(g.ntile); }
+inline dim3 tile_grid_tail(const Geometry& g) { return dim3(g.ntile + 1); }
 inline dim3 tile_block() { return dim3(kTile, kLevGroups); }
 
 // ---------------------------------------------------------------------------------------------
@@ -2847,11 +2848,12 @@ void launch_sponge_explicit(const Geometry& g, const Phys& P, const Sponge& sp, 
 }
 void launch_profx(const Geometry& g, const Phys& P, const Sponge& sp, const State& s, bool finish,
                   cudaStream_t st) {
-    profx_kernel<<<(g.N + kProfxCols - 1) / kProfxCols, dim3(kProfxCols, kProfxGroups), 0, st>>>(
+    static_assert(kProfxCols == kTile, "ProfX blocks are tiles");
+    profx_kernel<<<g.ntile, dim3(kProfxCols, kProfxGroups), 0, st>>>(
         g, P, sp, s, finish);
 }
 void launch_profx_finish(const Geometry& g, const State& s, cudaStream_t st) {
-    profx_finish_kernel<<<(g.N + kColBlock - 1) / kColBlock, kColBlock, 0, st>>>(g, s);
+    profx_finish_kernel<<<(g.ntile * kTile + kColBlock - 1) / kColBlock, kColBlock, 0, st>>>(g, s);
 }
 void launch_adv_temp(const Geometry& g, const Phys& P, const State& s, cudaStream_t st) {
     if (P.uniform_thermo)
@@ -3024,7 +3026,8 @@ void launch_vertical_diff(const Geometry& g, const Phys& P, const State& s, cuda
     static SmemOptIn opt;
     if (opt.ensure(vertical_diff_kernel, smem) != cudaSuccess)
         return;
-    vertical_diff_kernel<<<(g.N + kVdCols - 1) / kVdCols, kVdCols, smem, st>>>(g, P, s);
+    static_assert(kVdCols == kTile, "vertical hyperdiffusion blocks are tiles");
+    vertical_diff_kernel<<<g.ntile, kVdCols, smem, st>>>(g, P, s);
 }
 void launch_update_rk2(const Geometry& g, const Phys& P, const State& s, cudaStream_t st) {
     update_rk2_kernel<<<tile_grid(g), dim3(kTile, kRk2Groups), 0, st>>>(g, P, s);

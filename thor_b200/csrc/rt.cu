@@ -113,8 +113,8 @@ __device__ double source_func_lin(double bb, double bl, double bt, double tau, d
 // the RT; both depend on the zenith angle only, so computing them first changes no value.
 __global__ void __launch_bounds__(128) rt_column_kernel(Geometry g, Phys P, RtConst c, RtFields f,
                                                        State s) {
-    const int id = blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= g.N)
+    const int id = g.tile0 * 32 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= g.col_end)
         return;
     const RtStep  st = *f.step;
     const int     nv = g.nv, Np = g.Np;
@@ -262,7 +262,7 @@ __global__ void __launch_bounds__(128) rt_column_kernel(Geometry g, Phys P, RtCo
 void launch_rt(const Geometry& g, const Phys& P, const RtConst& c, const RtFields& f,
                const State& s, cudaStream_t st) {
     rt_orbit_kernel<<<1, 1, 0, st>>>(c, P, f.step);
-    rt_column_kernel<<<(g.N + 127) / 128, 128, 0, st>>>(g, P, c, f, s);
+    rt_column_kernel<<<(g.ntile * 32 + 127) / 128, 128, 0, st>>>(g, P, c, f, s);
 }
 
 } // namespace thorx

@@ -55,6 +55,12 @@ struct thorx_ctx {
     Sponge                           sp{};                   // Rayleigh sponge (nlat 0: off)
     std::vector<thorx_module>        modules;                // physics modules, in call order
     bool                             eager = false;          // thorx_step without a graph
+    // a partition (thorx_set_partition): the five-neighbour columns of the whole grid, and the
+    // halo exchange called after every kernel (thorx_set_exchange)
+    std::vector<int>                 special_all;
+    bool                             partitioned = false;
+    thorx_exchange_fn                xfn         = nullptr;
+    void*                            xuser       = nullptr;
     // uniform thermodynamics (Phys::uniform_thermo): the last host arrays set for Rd and Cp were
     // uniform at the scalar values; thermo_escaped: a module holds their device pointers
     bool                             rd_uniform = false, cp_uniform = false, thermo_escaped = false;
@@ -173,20 +179,22 @@ int upload_geo(thorx_ctx* ctx, const double* host, int J, const double** out) {
 }
 
 // Neighbour tables from the rhombus maps (halo tile of src/headers/kernel_halo_helpers.h:47-128)
-// and, for the two poles, point_local (the *_Poles kernels' neighbour lists).
-int build_neighbours(thorx_ctx* ctx, const thorx_grid* gr) {
-    const int N = gr->point_num, Np = ctx->g.Np, nl = gr->nl_region, nhl = nl + 2,
-              nhl2 = nhl * nhl;
-    std::vector<int>     nb((size_t)6 * Np, -1), ring((size_t)6 * Np, -1);
-    std::vector<uint8_t> flag(Np, 0);
-    std::vector<char>    seen(N, 0);
+// and, for the two poles, point_local (the *_Poles kernels' neighbour lists), on the host:
+// nb, ring [6][Np], flag [Np]. An empty string on success, else what is wrong with the grid.
+std::string neighbour_tables(const thorx_grid* gr, int Np, std::vector<int>& nb,
+                             std::vector<int>& ring, std::vector<uint8_t>& flag) {
+    const int N = gr->point_num, nl = gr->nl_region, nhl = nl + 2, nhl2 = nhl * nhl;
+    nb.assign((size_t)6 * Np, -1);
+    ring.assign((size_t)6 * Np, -1);
+    flag.assign(Np, 0);
+    std::vector<char> seen(N, 0);
     for (int r = 0; r < gr->nr; r++) {
         const int* m = gr->maps + (size_t)r * nhl2;
         for (int y = 0; y < nl; y++)
             for (int x = 0; x < nl; x++) {
                 const int id = m[(y + 1) * nhl + x + 1];
                 if (id < 0 || id >= N - 2 || seen[id])
-                    return fail(ctx, THORX_E_ARG, "maps: bad or repeated interior index");
+                    return "maps: bad or repeated interior index";
                 seen[id]      = 1;
                 const bool pe = (x == 0 && y == 0 && m[0] == -1);
                 const int  N0 = m[(y + 2) * nhl + x + 1], N1 = m[(y + 2) * nhl + x + 2],
@@ -195,7 +203,7 @@ int build_neighbours(thorx_ctx* ctx, const thorx_grid* gr) {
                 const int p[6] = {N0, N1, N2, N3, pe ? N5 : N4, N5};
                 for (int j = 0; j < 6; j++) {
                     if (p[j] >= N)
-                        return fail(ctx, THORX_E_ARG, "maps: neighbour index out of range");
+                        return "maps: neighbour index out of range";
                     nb[(size_t)j * Np + id] = p[j];
                 }
                 const int rg[6] = {N0, N1, N2, N3, pe ? N5 : N4, pe ? -1 : N5};
@@ -208,7 +216,7 @@ int build_neighbours(thorx_ctx* ctx, const thorx_grid* gr) {
         for (int i = 0; i < 5; i++) {
             int v = gr->point_local[(size_t)id * 6 + i];
             if (v < 0 || v >= N)
-                return fail(ctx, THORX_E_ARG, "point_local: bad pole neighbour");
+                return "point_local: bad pole neighbour";
             nb[(size_t)i * Np + id]   = v;
             ring[(size_t)i * Np + id] = v;
         }
@@ -218,7 +226,17 @@ int build_neighbours(thorx_ctx* ctx, const thorx_grid* gr) {
     }
     for (int id = 0; id < N; id++)
         if (!seen[id])
-            return fail(ctx, THORX_E_ARG, "maps do not cover every column");
+            return "maps do not cover every column";
+    return "";
+}
+
+int build_neighbours(thorx_ctx* ctx, const thorx_grid* gr) {
+    const int            N = gr->point_num, Np = ctx->g.Np;
+    std::vector<int>     nb, ring;
+    std::vector<uint8_t> flag;
+    const std::string    err = neighbour_tables(gr, Np, nb, ring, flag);
+    if (!err.empty())
+        return fail(ctx, THORX_E_ARG, err);
     std::vector<int> special;
     for (int id = 0; id < N; id++)
         if (flag[id] & kRing5)
@@ -233,8 +251,9 @@ int build_neighbours(thorx_ctx* ctx, const thorx_grid* gr) {
         || dev_alloc(ctx, &d_flag, flag.size()) || dev_alloc(ctx, &d_special, 32))
         return THORX_E_CUDA;
     CK(cudaMemcpy(d_special, special.data(), special.size() * sizeof(int), cudaMemcpyHostToDevice));
-    ctx->g.special  = d_special;
-    ctx->g.nspecial = (int)special.size();
+    ctx->g.special   = d_special;
+    ctx->g.nspecial  = (int)special.size();
+    ctx->special_all = special;
     CK(cudaMemcpy(d_nb, nb.data(), nb.size() * sizeof(int), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(d_ring, ring.data(), ring.size() * sizeof(int), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(d_flag, flag.data(), flag.size(), cudaMemcpyHostToDevice));
@@ -398,8 +417,37 @@ int class_launches(const thorx_ctx* ctx, int k) {
     return 0;
 }
 
+// After a kernel of a partitioned step: the caller's exchange brings the halo columns of the fields
+// the kernel wrote up to date (thorx_set_exchange); the energy form's extra fields are added where
+// eq is set.
+int exchange(thorx_ctx* ctx, std::initializer_list<const char*> f, bool eq = false) {
+    if (!ctx->xfn)
+        return 0;
+    std::vector<const char*> v(f);
+    if (eq && ctx->P.energy)
+        for (const char* e : {"ep", "eph", "ek", "ekh", "Etotal"})
+            v.push_back(e);
+    const int rc = ctx->xfn(ctx->xuser, ctx, (void*)ctx->stream, v.data(), (int)v.size());
+    return rc ? fail(ctx, rc, "halo exchange returned " + std::to_string(rc)) : 0;
+}
+#define THORX_XCHG(...)                                                                            \
+    do {                                                                                          \
+        if (const int rc_ = exchange(ctx, __VA_ARGS__))                                           \
+            return rc_;                                                                           \
+    } while (0)
+
+// what a partitioned context cannot run: whole-grid sums and module hooks on whole-grid arrays
+int partition_check(thorx_ctx* ctx) {
+    if (ctx->partitioned && (ctx->sp.nlat > 0 || ctx->sur || !ctx->modules.empty()))
+        return fail(ctx, THORX_E_UNSUPPORTED,
+                    "a partitioned context runs without the sponge, the surrogate and modules");
+    return 0;
+}
+
 // ESP::ProfX
 int enqueue_profx(thorx_ctx* ctx) {
+    if (int rc = partition_check(ctx))
+        return rc;
     CK(cudaMemsetAsync(ctx->s.Qheat, 0, sizeof(double) * ctx->g.nv * ctx->g.Np, ctx->stream));
     Sponge sp = ctx->sp; // the implicit sponge runs in ProfX, the explicit ones in Thor
     if (sp.mode != 0)
@@ -411,14 +459,18 @@ int enqueue_profx(thorx_ctx* ctx) {
                             ctx->stream);
     }
     if (!ctx->rt_enabled && !has_phy_loop(ctx)) {
-        KScope k(ctx, KProfx);
-        launch_profx(ctx->g, ctx->P, sp, ctx->s, true, ctx->stream);
+        {
+            KScope k(ctx, KProfx);
+            launch_profx(ctx->g, ctx->P, sp, ctx->s, true, ctx->stream);
+        }
+        THORX_XCHG({"W", "temperature", "pressure", "Mh", "pt"}, true);
     }
     else { // the physics modules run before Compute_pressure (profx_driver.cu:405-432)
         {
             KScope k(ctx, KProfx);
             launch_profx(ctx->g, ctx->P, sp, ctx->s, false, ctx->stream);
         }
+        THORX_XCHG({"W", "temperature", "Mh", "pt"}, true);
         if (!ctx->rt_enabled) {
         }
         else if (ctx->sur && sur_using(ctx)) {
@@ -450,6 +502,7 @@ int enqueue_profx(thorx_ctx* ctx) {
             KScope k(ctx, KProfx);
             launch_profx_finish(ctx->g, ctx->s, ctx->stream);
         }
+        THORX_XCHG({"pressure", "profx_Qheat"});
     }
     CK(cudaGetLastError());
     return 0;
@@ -462,6 +515,8 @@ int enqueue_thor(thorx_ctx* ctx) {
     State&          s  = ctx->s;
     cudaStream_t    st = ctx->stream;
     const size_t    cell = (size_t)g.nv * g.Np * sizeof(double), iface = (size_t)g.nvi * g.Np * sizeof(double);
+    if (int rc = partition_check(ctx))
+        return rc;
     CK(cudaMemcpyAsync(s.Mhk, s.Mh, 3 * cell, cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync(s.Whk, s.Wh, iface, cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync(s.Wk, s.W, cell, cudaMemcpyDeviceToDevice, st));
@@ -480,21 +535,34 @@ int enqueue_thor(thorx_ctx* ctx) {
             KScope k(ctx, KAdvTemp);
             launch_adv_temp(g, P, s, st);
         }
+        THORX_XCHG({"Adv", "temperature", "h", "hh", "pt", "pth", "gtil", "gtilh"}, true);
         if (P.HyDiff) {
             int passes = P.HyDiffOrder / 2;
             for (int i = 0; i < passes; i++) {
-                KScope k(ctx, i == passes - 1 ? KDiffLast : KDiffFirst);
-                launch_diffusion(g, P, s, i, i == passes - 1, st);
+                {
+                    KScope k(ctx, i == passes - 1 ? KDiffLast : KDiffFirst);
+                    launch_diffusion(g, P, s, i, i == passes - 1, st);
+                }
+                if (i == passes - 1)
+                    THORX_XCHG({"diffrh", "diffmh", "diffw", "diffpr"});
+                else
+                    THORX_XCHG({"diff"});
             }
             if (P.vhd_order) { // thor_driver.cu:590-612, inside the hyperdiffusion block
-                KScope k(ctx, KVertDiff);
-                launch_vertical_diff(g, P, s, st);
+                {
+                    KScope k(ctx, KVertDiff);
+                    launch_vertical_diff(g, P, s, st);
+                }
+                THORX_XCHG({"diffmh", "diffw", "diffpr"});
             }
         }
         THORX_HOOK(dyn_core_loop_slow_modes, rk, times);
         if (P.DivDampP) {
-            KScope k(ctx, KDivm0);
-            launch_divm0(g, P, s, false, st);
+            {
+                KScope k(ctx, KDivm0);
+                launch_divm0(g, P, s, false, st);
+            }
+            THORX_XCHG({"divg"});
         }
         if (ctx->sp.nlat > 0 && ctx->sp.mode != 0) { // thor_driver.cu:749-866
             KScope k(ctx, KSponge);
@@ -508,19 +576,31 @@ int enqueue_thor(thorx_ctx* ctx) {
             launch_slow_modes(g, P, s, rk > 0, st);
         }
         if (rk > 0)
+            THORX_XCHG({"SlowMh", "SlowWh", "SlowRho", "Slowpressure", "Mhs", "Rhos", "pressures",
+                        "Whs"});
+        else
+            THORX_XCHG({"SlowMh", "SlowWh", "SlowRho", "Slowpressure"});
+        if (rk > 0)
             launch_rk_arrays(ctx->rk_arrays, 0, st);
         for (int ns = 0; ns < ns_it; ns++) {
             if (P.DivDampP) {
-                KScope k(ctx, KDivm0);
-                launch_divm0(g, P, s, true, st);
+                {
+                    KScope k(ctx, KDivm0);
+                    launch_divm0(g, P, s, true, st);
+                }
+                THORX_XCHG({"divg"});
             }
             {
                 KScope k(ctx, KMomentum);
                 launch_momentum(g, P, s, times, st);
             }
+            THORX_XCHG({"Mhs"});
             if (!split) {
-                KScope k(ctx, KVertical);
-                launch_vertical(g, P, s, times, 0, st);
+                {
+                    KScope k(ctx, KVertical);
+                    launch_vertical(g, P, s, times, 0, st);
+                }
+                THORX_XCHG({"Whs", "Rhos", "pressures"}, true);
             }
             else { // the modules' fast-mode hooks between Vertical_Eq and Density_Pressure_Eqs
                 {
@@ -538,6 +618,7 @@ int enqueue_thor(thorx_ctx* ctx) {
             KScope k(ctx, KUpdateRk2);
             launch_update_rk2(g, P, s, st);
         }
+        THORX_XCHG({"Mhk", "Rhok", "pressurek", "Whk", "Wk"});
         launch_rk_arrays(ctx->rk_arrays, 1, st);
     }
     CK(cudaMemcpyAsync(s.Mh, s.Mhk, 3 * cell, cudaMemcpyDeviceToDevice, st));
@@ -671,6 +752,9 @@ int thorx_create(const thorx_grid* gr, const thorx_params* pr, void* stream, tho
     Geometry& g       = ctx->g;
     g.N               = N;
     g.Np              = (N + kColAlign - 1) / kColAlign * kColAlign;
+    g.tile0           = 0; // every tile: no partition
+    g.ntile           = g.Np / kColAlign;
+    g.col_end         = N;
     g.nv              = nv;
     g.nvi             = nv + 1;
     const int Np      = g.Np;
@@ -1789,6 +1873,8 @@ int thorx_surrogate_gradients_host(thorx_ctx* ctx, const float* x, const float* 
 int thorx_globdiag(thorx_ctx* ctx, double* out) {
     if (!ctx)
         return THORX_E_ARG;
+    if (ctx->partitioned)
+        return fail(ctx, THORX_E_UNSUPPORTED, "global sums need the whole state, not a partition");
     if (!out)
         return fail(ctx, THORX_E_ARG, "thorx_globdiag: null argument");
     if (!ctx->state_set)
@@ -1803,6 +1889,8 @@ int thorx_globdiag(thorx_ctx* ctx, double* out) {
 int thorx_globdiag_fields(thorx_ctx* ctx, double* out, double* const fields[6]) {
     if (!ctx)
         return THORX_E_ARG;
+    if (ctx->partitioned)
+        return fail(ctx, THORX_E_UNSUPPORTED, "global sums need the whole state, not a partition");
     if (!out || !fields)
         return fail(ctx, THORX_E_ARG, "thorx_globdiag_fields: null argument");
     if (!ctx->state_set)
@@ -1961,44 +2049,195 @@ int thorx_set_graph_mode(thorx_ctx* ctx, int use_graph) {
     return drop_graph(ctx);
 }
 
-int thorx_device_field(thorx_ctx* ctx, const char* name, double** dev, int* levels,
-                       int* components, long* plane) {
-    if (!ctx)
-        return THORX_E_ARG;
-    if (!name || !dev)
-        return fail(ctx, THORX_E_ARG, "thorx_device_field: null argument");
+namespace {
+// A field by name: the thorx_get_field fields, the dynamical core's stage, deviation and work
+// arrays, and the module tendencies; false when unknown (or not allocated in this form).
+bool find_field(thorx_ctx* ctx, const char* name, FieldDesc* out) {
     State&    s  = ctx->s;
     const int nv = ctx->g.nv;
+    auto      it = ctx->fields.find(name);
+    if (it != ctx->fields.end()) {
+        *out = it->second;
+        return *out->dev != nullptr;
+    }
     const std::map<std::string, FieldDesc> stage = {
         {"Rhok", {&s.Rhok, nv, 1}},       {"Rhos", {&s.Rhos, nv, 1}},
         {"Mhk", {&s.Mhk, nv, 3}},         {"Mhs", {&s.Mhs, nv, 3}},
         {"Whk", {&s.Whk, nv + 1, 1}},     {"Whs", {&s.Whs, nv + 1, 1}},
         {"Wk", {&s.Wk, nv, 1}},           {"pressurek", {&s.pk, nv, 1}},
         {"pressures", {&s.ps, nv, 1}},    {"profx_dMh", {&s.dMh, nv, 3}},
-        {"profx_dWh", {&s.dWh, nv + 1, 1}}};
+        {"profx_dWh", {&s.dWh, nv + 1, 1}}, {"divg", {&s.divg, nv, 3}},
+        {"diff", {&s.diff, nv, 12}},      {"Etotal", {&s.Etotal, nv, 1}},
+        {"ep", {&s.ep, nv, 1}},           {"ek", {&s.ek, nv, 1}},
+        {"eph", {&s.eph, nv + 1, 1}},     {"ekh", {&s.ekh, nv + 1, 1}}};
+    auto jt = stage.find(name);
+    if (jt == stage.end())
+        return false;
+    *out = jt->second;
+    return *out->dev != nullptr;
+}
+
+__global__ void copy_columns_kernel(double* __restrict__ dst, const double* __restrict__ src,
+                                    const int* __restrict__ cols, int n, int Q, int Np) {
+    const long long total = (long long)n * Q;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int    q = (int)(t / n), i = (int)(t % n);
+        const size_t k = (size_t)q * Np + cols[i];
+        dst[k]         = src[k];
+    }
+}
+// pack (dir 0): buf[i][q] = field[q][cols[i]]; unpack (dir 1): the reverse
+__global__ void pack_columns_kernel(double* __restrict__ field, double* __restrict__ buf,
+                                    const int* __restrict__ cols, int n, int Q, int Np, int dir) {
+    const long long total = (long long)n * Q;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int    q = (int)(t / n), i = (int)(t % n);
+        const size_t k = (size_t)q * Np + cols[i];
+        if (dir == 0)
+            buf[(size_t)i * Q + q] = field[k];
+        else
+            field[k] = buf[(size_t)i * Q + q];
+    }
+}
+unsigned column_blocks(long long total) {
+    return (unsigned)std::max<long long>(1, std::min<long long>((total + 255) / 256, 148LL * 16));
+}
+} // namespace
+
+int thorx_device_field(thorx_ctx* ctx, const char* name, double** dev, int* levels,
+                       int* components, long* plane) {
+    if (!ctx)
+        return THORX_E_ARG;
+    if (!name || !dev)
+        return fail(ctx, THORX_E_ARG, "thorx_device_field: null argument");
     if (!std::strcmp(name, "Rd") || !std::strcmp(name, "Cp")) { // a module may write them
         ctx->thermo_escaped = true;
         if (int rc = update_thermo(ctx))
             return rc;
     }
-    const FieldDesc* f  = nullptr;
-    auto             it = ctx->fields.find(name);
-    if (it != ctx->fields.end())
-        f = &it->second;
-    else {
-        auto jt = stage.find(name);
-        if (jt == stage.end())
-            return fail(ctx, THORX_E_ARG, std::string("thorx_device_field: unknown field ") + name);
-        f = &jt->second;
-    }
-    *dev = *f->dev;
+    FieldDesc f;
+    if (!find_field(ctx, name, &f))
+        return fail(ctx, THORX_E_ARG, std::string("thorx_device_field: unknown field ") + name);
+    *dev = *f.dev;
     if (levels)
-        *levels = f->L;
+        *levels = f.L;
     if (components)
-        *components = f->K;
+        *components = f.K;
     if (plane)
         *plane = ctx->g.Np;
     return 0;
+}
+
+int thorx_set_partition(thorx_ctx* ctx, int col_begin, int col_end) {
+    if (!ctx)
+        return THORX_E_ARG;
+    const int N = ctx->g.N;
+    if (col_begin < 0 || col_end > N || col_begin >= col_end || col_begin % kColAlign
+        || (col_end % kColAlign && col_end != N))
+        return fail(ctx, THORX_E_ARG, "thorx_set_partition: the range must be whole 32-column "
+                                      "tiles of the grid (the end may be point_num)");
+    if (ctx->sp.nlat > 0 || ctx->sur || !ctx->modules.empty())
+        return fail(ctx, THORX_E_UNSUPPORTED,
+                    "thorx_set_partition: not with the sponge, the surrogate or modules");
+    std::vector<int> sp;
+    for (int c : ctx->special_all)
+        if (c >= col_begin && c < col_end)
+            sp.push_back(c);
+    int* d_special;
+    if (dev_alloc(ctx, &d_special, 32))
+        return THORX_E_CUDA;
+    if (!sp.empty())
+        CK(cudaMemcpy(d_special, sp.data(), sp.size() * sizeof(int), cudaMemcpyHostToDevice));
+    ctx->g.special     = d_special;
+    ctx->g.nspecial    = (int)sp.size();
+    ctx->g.tile0       = col_begin / kColAlign;
+    ctx->g.ntile       = (col_end + kColAlign - 1) / kColAlign - ctx->g.tile0;
+    ctx->g.col_end     = col_end;
+    ctx->partitioned   = col_begin > 0 || col_end < N;
+    return drop_graph(ctx);
+}
+
+int thorx_set_exchange(thorx_ctx* ctx, thorx_exchange_fn fn, void* user) {
+    if (!ctx)
+        return THORX_E_ARG;
+    ctx->xfn   = fn;
+    ctx->xuser = user;
+    if (fn)
+        ctx->eager = true;
+    return drop_graph(ctx);
+}
+
+int thorx_halo_columns(const thorx_grid* gr, int col_begin, int col_end, int* cols, int cap) {
+    if (!gr || !gr->maps || !gr->point_local || gr->point_num < 3 || cap < 0
+        || col_begin < 0 || col_end > gr->point_num || col_begin >= col_end)
+        return free_fail(THORX_E_ARG, "thorx_halo_columns: bad grid or range");
+    const int            N = gr->point_num, Np = (N + kColAlign - 1) / kColAlign * kColAlign;
+    std::vector<int>     nb, ring;
+    std::vector<uint8_t> flag;
+    const std::string    err = neighbour_tables(gr, Np, nb, ring, flag);
+    if (!err.empty())
+        return free_fail(THORX_E_ARG, "thorx_halo_columns: " + err);
+    std::vector<char> need(N, 0);
+    for (int c = col_begin; c < col_end; c++)
+        for (int j = 0; j < 6; j++)
+            for (const std::vector<int>* t : {&nb, &ring}) {
+                const int v = (*t)[(size_t)j * Np + c];
+                if (v >= 0 && (v < col_begin || v >= col_end))
+                    need[v] = 1;
+            }
+    int n = 0;
+    for (int c = 0; c < N; c++)
+        if (need[c]) {
+            if (cols && n < cap)
+                cols[n] = c;
+            n++;
+        }
+    return n;
+}
+
+int thorx_copy_columns(thorx_ctx* dst, thorx_ctx* src, const char* field, const int* dev_cols,
+                       int n) {
+    if (!dst || !src)
+        return THORX_E_ARG;
+    FieldDesc fd, fs;
+    if (!field || n < 0 || (n > 0 && !dev_cols) || !find_field(dst, field, &fd)
+        || !find_field(src, field, &fs) || dst->g.Np != src->g.Np || dst->g.nv != src->g.nv)
+        return fail(dst, THORX_E_ARG, "thorx_copy_columns: bad arguments or field");
+    if (n == 0)
+        return 0;
+    const int Q = fd.L * fd.K;
+    copy_columns_kernel<<<column_blocks((long long)n * Q), 256, 0, dst->stream>>>(
+        *fd.dev, *fs.dev, dev_cols, n, Q, dst->g.Np);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? 0
+                            : fail(dst, THORX_E_CUDA,
+                                   std::string("thorx_copy_columns: ") + cudaGetErrorString(e));
+}
+
+static int pack_unpack(thorx_ctx* ctx, const char* field, const int* dev_cols, int n,
+                       double* dev_buf, int dir) {
+    if (!ctx)
+        return THORX_E_ARG;
+    FieldDesc f;
+    if (!field || n < 0 || (n > 0 && (!dev_cols || !dev_buf)) || !find_field(ctx, field, &f))
+        return fail(ctx, THORX_E_ARG, "thorx_pack_columns: bad arguments or field");
+    if (n == 0)
+        return 0;
+    const int Q = f.L * f.K;
+    pack_columns_kernel<<<column_blocks((long long)n * Q), 256, 0, ctx->stream>>>(
+        *f.dev, dev_buf, dev_cols, n, Q, ctx->g.Np, dir);
+    CK(cudaGetLastError());
+    return 0;
+}
+int thorx_pack_columns(thorx_ctx* ctx, const char* field, const int* dev_cols, int n,
+                       double* dev_buf) {
+    return pack_unpack(ctx, field, dev_cols, n, dev_buf, 0);
+}
+int thorx_unpack_columns(thorx_ctx* ctx, const char* field, const int* dev_cols, int n,
+                         const double* dev_buf) {
+    return pack_unpack(ctx, field, dev_cols, n, const_cast<double*>(dev_buf), 1);
 }
 
 int thorx_vert_hydiff_enable(thorx_ctx* ctx, double Diffc_v, int order) {

@@ -35,6 +35,10 @@ enum : uint8_t { kPole = 1, kRing5 = 2 };
 
 struct Geometry {
     int            N, Np, nv, nvi;
+    // The columns this context computes (a partition of the grid among several contexts or GPUs,
+    // thorx_set_partition): 32-column tiles tile0 .. tile0 + ntile - 1, and the columns below
+    // col_end; all tiles and N without a partition. The arrays stay whole-grid.
+    int            tile0, ntile, col_end;
     const int*     nb;
     const int*     ring;
     const uint8_t* cflag;
