@@ -25,6 +25,9 @@
 #include <mutex>
 #include <type_traits>
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include "thorx.h"
 #include "thorx_internal.h"
 
@@ -34,7 +37,7 @@ namespace {
 #ifndef THORX_LEVGROUPS
 #define THORX_LEVGROUPS 8
 #endif
-constexpr int kTile      = 32;              // columns per tile (lanes)
+constexpr int kTile      = kTileCols;       // columns per tile (lanes)
 constexpr int kLevGroups = THORX_LEVGROUPS; // warps per tile, each taking every kLevGroups-th level
 constexpr int kColBlock  = 128;
 
@@ -1702,6 +1705,19 @@ __global__ void THORX_KATTR_DIVM
         divm0_body<6, R>(g, P, G, Mh, Wh, divg, c);
 }
 
+// The end of pass 1: the radial component removed, scaled by -Kdhz.
+template<class R>
+__device__ __forceinline__ void divm_finish(const Geometry& g, int lev, const double* fr,
+                                            const R* lap, R* DivM) {
+    const R sdiff = (R)g.Kdhz[lev];
+    const R lapr  = (R)fr[0] * lap[0] + (R)fr[1] * lap[1] + (R)fr[2] * lap[2];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const R l = lap[k] - (R)fr[k] * lapr;
+        DivM[k]   = -l * sdiff;
+    }
+}
+
 // Pass 1 of the divergence damping at (column, level): DivM from divg.
 template<int n, class R>
 __device__ __forceinline__ void divm_final(const Geometry& g, const Phys& P, const SGeo& G,
@@ -1734,13 +1750,17 @@ __device__ __forceinline__ void divm_final(const Geometry& g, const Phys& P, con
         divm_core<n, R>(G, a0, ar, false, (R)0, (R)0, nullptr, nullptr, (R)0,
                         (R)rscale_of(P, g, lev), 2, lap);
     }
-    const R sdiff = (R)g.Kdhz[lev];
-    const R lapr  = (R)fr[0] * lap[0] + (R)fr[1] * lap[1] + (R)fr[2] * lap[2];
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-        const R l = lap[k] - (R)fr[k] * lapr;
-        DivM[k]   = -l * sdiff;
-    }
+    divm_finish<R>(g, lev, fr, lap, DivM);
+}
+
+// Pass 1 from values already gathered (a0: divg at the column; ar: at its ring), operator weights.
+template<int n, class R>
+__device__ __forceinline__ void divm_final_vals(const Geometry& g, const Phys& P, const SGeo& G,
+                                                const double* a0, const double (*ar)[3], int lev,
+                                                const double* fr, R* DivM) {
+    R lap[3];
+    divm_w<n, R>(G, a0, ar, false, nullptr, rscale_of(P, g, lev), 0.0, lap);
+    divm_finish<R>(g, lev, fr, lap, DivM);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1948,11 +1968,34 @@ __global__ void THORX_KATTR_SLOW
 // Small step, horizontal momentum: divergence-damping pass 1 on the deviations (Mhs, Whs) +
 // Momentum_Eq / _Poles (src/headers/dyn/thor_fastmodes.h:54-253).
 // ---------------------------------------------------------------------------------------------
+// The update of Mhs at (c, lev) from ps at the 7 stencil points (pv) and the damping term DivM.
+template<class R>
+__device__ __forceinline__ void momentum_apply(const Geometry& g, const Phys& P, const State& s,
+                                               const double* sgrad, double dt, int c, int lev,
+                                               const double* fr, const double* pv, const R* DivM) {
+    const int    x = threadIdx.x, Np = g.Np, nv = g.nv;
+    const double rscale = rscale_of(P, g, lev);
+    double       Mv[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        double sg = sgrad[k * kTile + x] * pv[0];
+#pragma unroll
+        for (int j = 1; j < 7; j++)
+            sg = sg + sgrad[(j * 3 + k) * kTile + x] * pv[j];
+        const double nflxv = rscale * sg;
+        Mv[k]              = (-nflxv + s.SlowMh[(k * nv + lev) * Np + c] + (double)DivM[k]) * dt;
+    }
+    const double vr = Mv[0] * fr[0] + Mv[1] * fr[1] + Mv[2] * fr[2];
+    for (int k = 0; k < 3; k++) {
+        Mv[k] += -vr * fr[k];
+        s.Mhs[(k * nv + lev) * Np + c] += Mv[k];
+    }
+}
+
 template<int n, class R>
 __device__ __forceinline__ void momentum_body(const Geometry& g, const Phys& P, const State& s,
                                               const SGeo& G, const double* sgrad, double dt,
                                               int c) {
-    const int x = threadIdx.x;
     const int Np = g.Np, nv = g.nv;
     int       nb[7], ring[6];
     nb[0] = c;
@@ -1967,26 +2010,11 @@ __device__ __forceinline__ void momentum_body(const Geometry& g, const Phys& P, 
         R DivM[3] = {0, 0, 0};
         if (P.DivDampP)
             divm_final<n, R>(g, P, G, ring, s.divg, c, lev, fr, DivM);
-        const double rscale = rscale_of(P, g, lev);
-        double       pv[7];
+        double pv[7];
 #pragma unroll
         for (int j = 0; j < 7; j++)
             pv[j] = gz(s.ps + lev * Np, nb[j]);
-        double Mv[3];
-#pragma unroll
-        for (int k = 0; k < 3; k++) {
-            double sg = sgrad[k * kTile + x] * pv[0];
-#pragma unroll
-            for (int j = 1; j < 7; j++)
-                sg = sg + sgrad[(j * 3 + k) * kTile + x] * pv[j];
-            const double nflxv = rscale * sg;
-            Mv[k]              = (-nflxv + s.SlowMh[(k * nv + lev) * Np + c] + (double)DivM[k]) * dt;
-        }
-        const double vr = Mv[0] * fr[0] + Mv[1] * fr[1] + Mv[2] * fr[2];
-        for (int k = 0; k < 3; k++) {
-            Mv[k] += -vr * fr[k];
-            s.Mhs[(k * nv + lev) * Np + c] += Mv[k];
-        }
+        momentum_apply<R>(g, P, s, sgrad, dt, c, lev, fr, pv, DivM);
     }
 }
 
@@ -2007,6 +2035,193 @@ __global__ void THORX_KATTR_MOM
         momentum_body<5, R>(g, P, s, G, sgrad, dt, c);
     else
         momentum_body<6, R>(g, P, s, G, sgrad, dt, c);
+}
+
+// The same update with the neighbour values staged in shared memory by the tensor-memory
+// accelerator: per round of 8 levels (one per warp), one thread copies, for each of the tile's
+// window spans (Geometry::wspan), a box of kWinW columns x 8 levels of ps and of the 3 divg
+// components (boxes of this GPU's own planes, no multicast), completing on an mbarrier; the warps
+// then read their stencil points from the window, and the few outside it (rhombus edges) from
+// global memory. kMomBuf windows: with 2, the copy of the next round overlaps this one's compute.
+// The values and the arithmetic are those of momentum_body. The five-neighbour tile reads
+// directly. A wait that runs past its bound sets kFlagWait and the CTA ends its work.
+// Off by default (THORX_MOM_TMA=1 builds it): on the glevel-6, 48-level step the staged kernel
+// took 1.58 ms per step with one window (2.09 ms with two: 2 CTAs per SM instead of 3) against
+// 1.18 ms for the direct gathers, the same bits. A CTA waits for a whole round's boxes before any
+// warp computes and meets at two barriers per round, where the gathering warps each run ahead on
+// their own loads; the neighbour reads hit L1 already.
+#ifndef THORX_MOM_TMA
+#define THORX_MOM_TMA 0
+#endif
+#ifndef THORX_MOM_TMA_BUF
+#define THORX_MOM_TMA_BUF 1
+#endif
+constexpr int      kMomBuf     = THORX_MOM_TMA_BUF;
+constexpr int      kWinFields  = 4; // ps, divg x, y, z
+constexpr int      kWinField   = kWinSpans * kLevGroups * kWinW; // doubles of one field's window
+constexpr int      kWinDoubles = kWinFields * kWinField;
+constexpr uint32_t kWinPolls   = 1u << 22;
+// the staged kernel serves the operator-weight forms (the default FP64 form and the mixed form)
+template<class R>
+constexpr bool kMomTma = THORX_MOM_TMA && (kOperatorWeights<R> || kDivmWeightsF64);
+size_t momentum_smem_bytes() { return sizeof(double) * kMomBuf * kWinDoubles + 128; }
+static_assert(kWinW * kLevGroups * sizeof(double) % 128 == 0, "window boxes keep 128-byte alignment");
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void win_bar_init(uint64_t* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void win_expect(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+// phase `parity` of the mbarrier completed within `limit` polls
+__device__ __forceinline__ bool win_wait(uint64_t* bar, uint32_t parity, uint32_t limit) {
+    for (uint32_t i = 0; i < limit; i++) {
+        uint32_t done;
+        asm volatile("{\n\t.reg .pred p;\n\t"
+                     "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.b32 %0, 1, 0, p;\n\t}"
+                     : "=r"(done)
+                     : "r"(smem_addr(bar)), "r"(parity)
+                     : "memory");
+        if (done)
+            return true;
+    }
+    return false;
+}
+// one box {kWinW columns, 8 levels, 1 plane} at (x, y, z) of a 3-D map into shared memory
+__device__ __forceinline__ void win_copy(double* dst, const CUtensorMap* map, int x, int y, int z,
+                                         uint64_t* bar) {
+    asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes "
+                 "[%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_addr(dst)),
+                 "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+template<class R>
+__global__ void THORX_KATTR_MOM
+    momentum_tma_kernel(Geometry g, Phys P, State s, double dt,
+                        const __grid_constant__ CUtensorMap map_ps,
+                        const __grid_constant__ CUtensorMap map_divg) {
+    __shared__ double              sgeo[kRingGeoRows * kTile];
+    __shared__ double              sgrad[21 * kTile];
+    __shared__ uint64_t            bar[kMomBuf];
+    extern __shared__ double       win_raw[];
+    // [kMomBuf][kWinFields][kWinSpans][8][kWinW], from the first 128-byte boundary (a box's
+    // destination must be 128-byte aligned; every box is 2304 bytes)
+    double* const win = win_raw + ((128u - (smem_addr(win_raw) & 127u)) & 127u) / sizeof(double);
+    const int     c   = lane_column(g);
+    SGeo                           G{};
+    if (P.DivDampP)
+        G = stage_divm_geo<R>(sgeo, g, c);
+    stage_cols(sgrad, g.grad, 21, g.Np, c);
+    if (tail_cta()) {
+        __syncthreads();
+        if (c >= 0)
+            momentum_body<5, R>(g, P, s, G, sgrad, dt, c);
+        return;
+    }
+    const int  Np = g.Np, nv = g.nv, tile = g.tile0 + blockIdx.x;
+    const int  nst    = (nv + kLevGroups - 1) / kLevGroups;
+    const bool leader = threadIdx.x == 0 && threadIdx.y == 0;
+    int        xs[kWinSpans], nsp = 0;
+#pragma unroll
+    for (int sp = 0; sp < kWinSpans; sp++) {
+        xs[sp] = g.wspan[tile * kWinSpans + sp];
+        nsp += xs[sp] >= 0;
+    }
+    const uint32_t bytes = nsp * kWinFields * kLevGroups * kWinW * sizeof(double);
+    auto           issue = [&](int st) {
+        double*   w = win + (st % kMomBuf) * kWinDoubles;
+        uint64_t* b = &bar[st % kMomBuf];
+        win_expect(b, bytes);
+#pragma unroll
+        for (int sp = 0; sp < kWinSpans; sp++) {
+            if (xs[sp] < 0)
+                continue;
+            double* d = w + sp * kLevGroups * kWinW;
+            win_copy(d, &map_ps, xs[sp], st * kLevGroups, 0, b);
+#pragma unroll
+            for (int k = 0; k < 3; k++)
+                win_copy(d + (1 + k) * kWinField, &map_divg, xs[sp], st * kLevGroups, k, b);
+        }
+    };
+    if (leader) {
+        for (int b = 0; b < kMomBuf; b++)
+            win_bar_init(&bar[b]);
+    }
+    __syncthreads();
+    int issued = 0;
+    if (leader)
+        for (; issued < kMomBuf && issued < nst; issued++)
+            issue(issued);
+    // window offset (span * 8 * kWinW + column - span start) of each point, -1 outside the window
+    auto woff = [&](int id) {
+        int o = -1;
+#pragma unroll
+        for (int sp = kWinSpans - 1; sp >= 0; sp--)
+            if (xs[sp] >= 0 && id >= xs[sp] && id < xs[sp] + kWinW)
+                o = sp * kLevGroups * kWinW + id - xs[sp];
+        return o;
+    };
+    int    onb[7], org[6];
+    double fr[3];
+    if (c >= 0) {
+        onb[0] = woff(c);
+#pragma unroll
+        for (int j = 0; j < 6; j++) {
+            onb[j + 1] = woff(g.nb[j * Np + c]);
+            org[j]     = woff(g.ring[j * Np + c]);
+        }
+#pragma unroll
+        for (int k = 0; k < 3; k++)
+            fr[k] = g.func_r[k * Np + c];
+    }
+    for (int st = 0; st < nst; st++) {
+        const int b  = st % kMomBuf;
+        const bool ok =
+            __syncthreads_and(win_wait(&bar[b], (uint32_t)((st / kMomBuf) & 1), kWinPolls));
+        if (!ok) {
+            if (leader) {
+                atomicOr(s.flags, kFlagWait);
+                for (int q = st; q < issued; q++) // the copies still in flight
+                    win_wait(&bar[q % kMomBuf], (uint32_t)((q / kMomBuf) & 1), kWinPolls);
+            }
+            return;
+        }
+        const int lev = st * kLevGroups + threadIdx.y;
+        if (c >= 0 && lev < nv) {
+            const double* w = win + b * kWinDoubles + threadIdx.y * kWinW;
+            double        pv[7];
+#pragma unroll
+            for (int j = 0; j < 7; j++)
+                pv[j] = onb[j] >= 0 ? w[onb[j]]
+                                    : gz(s.ps + lev * Np, j == 0 ? c : g.nb[(j - 1) * Np + c]);
+            R DivM[3] = {0, 0, 0};
+            if (P.DivDampP) {
+                double a0[3], ar[6][3];
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    const double* dg = s.divg + (k * nv + lev) * Np;
+                    a0[k] = onb[0] >= 0 ? w[(1 + k) * kWinField + onb[0]] : dg[c];
+#pragma unroll
+                    for (int j = 0; j < 6; j++)
+                        ar[j][k] = org[j] >= 0 ? w[(1 + k) * kWinField + org[j]]
+                                               : gz(dg, g.ring[j * Np + c]);
+                }
+                divm_final_vals<6, R>(g, P, G, a0, ar, lev, fr, DivM);
+            }
+            momentum_apply<R>(g, P, s, sgrad, dt, c, lev, fr, pv, DivM);
+        }
+        __syncthreads(); // the window of this round is read; the next copy may overwrite it
+        if (leader && issued < nst)
+            issue(issued++);
+    }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -2894,13 +3109,6 @@ void launch_slow_modes(const Geometry& g, const Phys& P, const State& s, bool up
         P.uniform_thermo ? slow_modes_kernel<double, true><<<gr, bl, 0, st>>>(g, P, s, update_rk)
                          : slow_modes_kernel<double, false><<<gr, bl, 0, st>>>(g, P, s, update_rk);
 }
-void launch_momentum(const Geometry& g, const Phys& P, const State& s, double dt,
-                     cudaStream_t st) {
-    if (P.mixed)
-        momentum_kernel<float><<<tile_grid_tail(g), tile_block(), 0, st>>>(g, P, s, dt);
-    else
-        momentum_kernel<double><<<tile_grid_tail(g), tile_block(), 0, st>>>(g, P, s, dt);
-}
 size_t vertical_smem_bytes(const Geometry& g) {
     return sizeof(double) * kTile * (21 + (kVertSmem == 2 ? 4 : kVertSmem == 1 ? 2 : 0) * g.nv);
 }
@@ -2929,6 +3137,59 @@ struct SmemOptIn {
         return e;
     }
 };
+// A 3-D tensor map over planes [planes][nv][Np] of doubles, boxes {kWinW, 8, 1}; false if the
+// driver's entry point is missing or the map is rejected (alignment, sizes).
+bool window_map(CUtensorMap* map, const double* base, int Np, int nv, int planes) {
+    static PFN_cuTensorMapEncodeTiled encode = nullptr;
+    static std::mutex                 mu;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (!encode) {
+            void*                           fn = nullptr;
+            cudaDriverEntryPointQueryResult q;
+            if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q)
+                    != cudaSuccess
+                || q != cudaDriverEntryPointSuccess || !fn)
+                return false;
+            encode = (PFN_cuTensorMapEncodeTiled)fn;
+        }
+    }
+    const cuuint64_t dims[3]    = {(cuuint64_t)Np, (cuuint64_t)nv, (cuuint64_t)planes};
+    const cuuint64_t strides[2] = {(cuuint64_t)Np * sizeof(double),
+                                   (cuuint64_t)Np * nv * sizeof(double)};
+    const cuuint32_t box[3]     = {(cuuint32_t)kWinW, (cuuint32_t)kLevGroups, 1};
+    const cuuint32_t estr[3]    = {1, 1, 1};
+    return encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double*>(base), dims,
+                  strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE)
+           == CUDA_SUCCESS;
+}
+
+template<class R>
+void launch_momentum_t(const Geometry& g, const Phys& P, const State& s, double dt,
+                       cudaStream_t st) {
+    if constexpr (kMomTma<R>) {
+        CUtensorMap mps, mdivg;
+        if (g.Np >= kWinW && window_map(&mps, s.ps, g.Np, g.nv, 1)
+            && window_map(&mdivg, s.divg, g.Np, g.nv, 3)) {
+            const size_t     smem = momentum_smem_bytes();
+            static SmemOptIn opt;
+            if (opt.ensure(momentum_tma_kernel<R>, smem) != cudaSuccess)
+                return;
+            momentum_tma_kernel<R>
+                <<<tile_grid_tail(g), tile_block(), smem, st>>>(g, P, s, dt, mps, mdivg);
+            return;
+        }
+    }
+    momentum_kernel<R><<<tile_grid_tail(g), tile_block(), 0, st>>>(g, P, s, dt);
+}
+void launch_momentum(const Geometry& g, const Phys& P, const State& s, double dt,
+                     cudaStream_t st) {
+    if (P.mixed)
+        launch_momentum_t<float>(g, P, s, dt, st);
+    else
+        launch_momentum_t<double>(g, P, s, dt, st);
+}
 template<int kPart, bool kUni>
 void launch_vertical_part_t(const Geometry& g, const Phys& P, const State& s, double dt,
                           cudaStream_t st) {

@@ -230,6 +230,52 @@ std::string neighbour_tables(const thorx_grid* gr, int Np, std::vector<int>& nb,
     return "";
 }
 
+// The momentum kernel's shared-memory windows (Geometry::wspan) from the neighbour tables: for
+// each tile, every reference its computed columns make (the column itself, its 6 stencil points,
+// its 6 ring points) is sorted by column, swept into spans of kWinW columns (a span starts at the
+// first uncovered reference, rounded down to even and kept inside the grid), and the kWinSpans
+// spans with the most references are kept. References outside them are read from global memory.
+std::vector<int> window_spans(int N, int Np, const std::vector<int>& nb,
+                              const std::vector<int>& ring, const std::vector<uint8_t>& flag) {
+    const int        tiles = (N + kTileCols - 1) / kTileCols;
+    std::vector<int> span((size_t)tiles * kWinSpans, -1);
+    if (Np < kWinW)
+        return span;
+    std::vector<int>                 refs;
+    std::vector<std::pair<int, int>> found; // (references, first column)
+    for (int t = 0; t < tiles; t++) {
+        refs.clear();
+        for (int c = t * kTileCols; c < std::min(N, (t + 1) * kTileCols); c++) {
+            if (flag[c] & kRing5)
+                continue;
+            refs.push_back(c);
+            for (int j = 0; j < 6; j++) {
+                if (nb[(size_t)j * Np + c] >= 0)
+                    refs.push_back(nb[(size_t)j * Np + c]);
+                if (ring[(size_t)j * Np + c] >= 0)
+                    refs.push_back(ring[(size_t)j * Np + c]);
+            }
+        }
+        std::sort(refs.begin(), refs.end());
+        found.clear();
+        for (size_t i = 0; i < refs.size();) {
+            const int x0 = std::min(refs[i] & ~1, Np - kWinW);
+            size_t    k  = i;
+            while (k < refs.size() && refs[k] < x0 + kWinW)
+                k++;
+            found.push_back({(int)(k - i), x0});
+            i = k;
+        }
+        std::stable_sort(found.begin(), found.end(),
+                         [](const std::pair<int, int>& a, const std::pair<int, int>& b) {
+                             return a.first > b.first;
+                         });
+        for (int s = 0; s < kWinSpans && s < (int)found.size(); s++)
+            span[(size_t)t * kWinSpans + s] = found[s].second;
+    }
+    return span;
+}
+
 int build_neighbours(thorx_ctx* ctx, const thorx_grid* gr) {
     const int            N = gr->point_num, Np = ctx->g.Np;
     std::vector<int>     nb, ring;
@@ -260,6 +306,12 @@ int build_neighbours(thorx_ctx* ctx, const thorx_grid* gr) {
     ctx->g.nb    = d_nb;
     ctx->g.ring  = d_ring;
     ctx->g.cflag = d_flag;
+    const std::vector<int> wspan = window_spans(N, Np, nb, ring, flag);
+    int*                   d_wspan;
+    if (dev_alloc(ctx, &d_wspan, wspan.size()))
+        return THORX_E_CUDA;
+    CK(cudaMemcpy(d_wspan, wspan.data(), wspan.size() * sizeof(int), cudaMemcpyHostToDevice));
+    ctx->g.wspan = d_wspan;
     return 0;
 }
 
@@ -275,6 +327,8 @@ int check_flags(thorx_ctx* ctx) {
     if (f & kFlagConvAdj)
         return fail(ctx, THORX_E_CONVERGENCE,
                     "convective adjustment: a column exceeded the pass bound");
+    if (f & kFlagWait)
+        return fail(ctx, THORX_E_CUDA, "a copy into shared memory did not complete in time");
     return 0;
 }
 

@@ -70,7 +70,14 @@ struct Geometry {
     const double*  lapw;
     const float*   dmw;
     const double*  dmw64; // dmw in double, for the FP64 form
+    // Shared-memory windows of the momentum kernel, per 32-column tile (whole grid): the first
+    // column of each of kWinSpans spans of kWinW columns that hold the tile's stencil points, or
+    // -1 for an unused span ([tiles][kWinSpans]).
+    const int*     wspan;
 };
+// Columns of a tile (the lanes of a warp); width (columns, even: every box row starts on a
+// 16-byte boundary) and number of the window spans.
+constexpr int kTileCols = 32, kWinW = 36, kWinSpans = 3;
 
 // Per-level quantities that every column shares, tabulated once on the device at context
 // creation with the same expressions the kernels would evaluate per cell (so the values are
@@ -140,8 +147,9 @@ struct State {
 };
 
 // device-side error flags (State::flags), read by thorx_sync: a NaN in the temperature after
-// the physics step; a column whose convective adjustment exceeded its pass bound
-enum : unsigned int { kFlagNaN = 1u, kFlagConvAdj = 2u };
+// the physics step; a column whose convective adjustment exceeded its pass bound; a copy into
+// shared memory that did not complete within its wait bound
+enum : unsigned int { kFlagNaN = 1u, kFlagConvAdj = 2u, kFlagWait = 4u };
 
 // Largest nv the kernels take (levels per thread are unrolled into registers).
 int max_levels();
