@@ -1674,6 +1674,113 @@ __device__ __forceinline__ void divm0_point(const Geometry& g, const Phys& P, co
     }
 }
 
+// Pass 0 through the operator weights at kL consecutive levels lev .. lev + kL - 1 of column c
+// (levels at or above nv are computed on the top level and not stored). The stencil points are
+// streamed: at each point the Mh vector of every level and the Wh values of the kL + 1 interfaces
+// are loaded once, and each weight read from shared memory serves all kL levels. For each output
+// the multiply-adds run in divm_w's order (the centre's components, then the ring point by point,
+// the Wh differences in their own sum), so every value is divm0_point's bit for bit.
+// Levels per thread: 3 in the FP64 form (glevel 6, 48 levels: divm0 1.245 -> 1.16 ms per step
+// against one level; 2: 1.19, 4: 1.36), 1 in the mixed form (1.13 ms; 2: 1.20, 3: 1.18).
+#ifndef THORX_DIVM_LEVELS
+#define THORX_DIVM_LEVELS 3
+#endif
+#ifndef THORX_DIVM_LEVELS_MIXED
+#define THORX_DIVM_LEVELS_MIXED 1
+#endif
+template<class R>
+constexpr int kDivmLevels = sizeof(R) < sizeof(double) ? THORX_DIVM_LEVELS_MIXED : THORX_DIVM_LEVELS;
+template<int n, class T, int kL>
+__device__ __forceinline__ void divm0_levels(const Geometry& g, const Phys& P, const SGeo& G,
+                                             const int* ring, const double* __restrict__ Mh,
+                                             const double* __restrict__ Wh,
+                                             double* __restrict__ divg, int c, int lev) {
+    const int Np = g.Np, nv = g.nv;
+    const T*  W;
+    if constexpr (sizeof(T) < sizeof(double))
+        W = G.dm + G.x;
+    else
+        W = G.dm64 + G.x;
+    auto w = [&](int o, int e) { return W[(o * 28 + e) * kTile]; };
+    int  lv[kL], li[kL + 1]; // the levels and interfaces read, clamped to the column
+#pragma unroll
+    for (int l = 0; l < kL; l++)
+        lv[l] = min(lev + l, nv - 1);
+#pragma unroll
+    for (int l = 0; l <= kL; l++)
+        li[l] = min(lev + l, nv);
+    double a0[kL][3], wv[kL + 1];
+    T      acc[kL][3], accw[kL][3];
+#pragma unroll
+    for (int l = 0; l < kL; l++)
+#pragma unroll
+        for (int k = 0; k < 3; k++)
+            a0[l][k] = Mh[(k * nv + lv[l]) * Np + c];
+#pragma unroll
+    for (int l = 0; l <= kL; l++)
+        wv[l] = Wh[li[l] * Np + c];
+#pragma unroll
+    for (int o = 0; o < 3; o++) {
+#pragma unroll
+        for (int l = 0; l < kL; l++) {
+            acc[l][o]  = (T)0;
+            accw[l][o] = (T)0;
+        }
+#pragma unroll
+        for (int comp = 0; comp < 3; comp++) {
+            const T wc = w(o, comp);
+#pragma unroll
+            for (int l = 0; l < kL; l++)
+                acc[l][o] = fma_t(wc, (T)a0[l][comp], acc[l][o]);
+        }
+        const T ww = w(o, 21);
+#pragma unroll
+        for (int l = 0; l < kL; l++)
+            accw[l][o] = fma_t(ww, (T)(wv[l] - wv[l + 1]), accw[l][o]);
+    }
+#pragma unroll
+    for (int j = 0; j < n; j++) {
+        double m[kL][3], wr[kL + 1];
+#pragma unroll
+        for (int l = 0; l < kL; l++)
+#pragma unroll
+            for (int k = 0; k < 3; k++)
+                m[l][k] = gz(Mh + (k * nv + lv[l]) * Np, ring[j]);
+#pragma unroll
+        for (int l = 0; l <= kL; l++)
+            wr[l] = gz(Wh + li[l] * Np, ring[j]);
+#pragma unroll
+        for (int o = 0; o < 3; o++) {
+#pragma unroll
+            for (int comp = 0; comp < 3; comp++) {
+                const T wc = w(o, (j + 1) * 3 + comp);
+#pragma unroll
+                for (int l = 0; l < kL; l++)
+                    acc[l][o] = fma_t(wc, (T)(m[l][comp] - a0[l][comp]), acc[l][o]);
+            }
+            const T ww = w(o, 22 + j);
+#pragma unroll
+            for (int l = 0; l < kL; l++)
+                accw[l][o] = fma_t(ww, (T)(wr[l] - wr[l + 1]), accw[l][o]);
+        }
+    }
+#pragma unroll
+    for (int l = 0; l < kL; l++) {
+        if (lev + l >= nv)
+            break;
+        const double rscale = rscale_of(P, g, lev + l);
+        const double dz     = 1.0 / (g.Altitudeh[lev + l] - g.Altitudeh[lev + l + 1]);
+        const T      sv = (T)(rscale * rscale), sw = (T)(rscale * dz);
+#pragma unroll
+        for (int o = 0; o < 3; o++) {
+            T a = acc[l][o];
+            a *= sv;
+            a = fma_t(accw[l][o], sw, a);
+            divg[(o * nv + lev + l) * Np + c] = (double)a;
+        }
+    }
+}
+
 // Pass 0 of the divergence damping on (Mh, Wh) -> divg.
 template<int n, class R>
 __device__ __forceinline__ void divm0_body(const Geometry& g, const Phys& P, const SGeo& G,
@@ -1684,9 +1791,17 @@ __device__ __forceinline__ void divm0_body(const Geometry& g, const Phys& P, con
     int       ring[6];
     for (int j = 0; j < 6; j++)
         ring[j] = g.ring[j * Np + c];
-    const int c2 = (g.cflag[c] & kPole) ? 1 : 2;
-    for (int lev = threadIdx.y; lev < g.nv; lev += kLevGroups)
-        divm0_point<n, R>(g, P, G, ring, c2, Mh, Wh, divg, c, lev);
+    if constexpr ((kOperatorWeights<R> || kDivmWeightsF64) && kDivmLevels<R> > 1) {
+        using T        = std::conditional_t<kOperatorWeights<R>, float, double>;
+        constexpr int L = kDivmLevels<R>;
+        for (int lev = threadIdx.y * L; lev < g.nv; lev += kLevGroups * L)
+            divm0_levels<n, T, L>(g, P, G, ring, Mh, Wh, divg, c, lev);
+    }
+    else {
+        const int c2 = (g.cflag[c] & kPole) ? 1 : 2;
+        for (int lev = threadIdx.y; lev < g.nv; lev += kLevGroups)
+            divm0_point<n, R>(g, P, G, ring, c2, Mh, Wh, divg, c, lev);
+    }
 }
 
 template<class R>
@@ -2919,11 +3034,15 @@ __global__ void THORX_KATTR_VERT
 // ---------------------------------------------------------------------------------------------
 // A CTA is one 32-column tile; warp y owns the contiguous levels [y chunk, (y + 1) chunk). Before a
 // barrier each warp reads the interface just above its chunk (the next warp writes it); then it
-// walks its chunk upward, so every other interface it reads is one it has not written yet. Few
-// registers, so 128-thread CTAs fit 16 to an SM: all of a g6 grid's 1281 tiles are resident at once.
+// walks its chunk upward, so every other interface it reads is one it has not written yet. Eight
+// warps of 6 levels at 48 levels (glevel 6: 0.204 ms per step; 4 warps of 12 levels: 0.235, 6:
+// 0.239, 12: 0.223, 16: 0.278; the same bits): more warps keep more loads in flight per SM.
 // The interpolation weights are the level tables' values of the same expressions (level 0, whose
 // lower interface the reference takes as 0, evaluates them here).
-constexpr int kRk2Groups = 4;
+#ifndef THORX_RK2_GROUPS
+#define THORX_RK2_GROUPS 8
+#endif
+constexpr int kRk2Groups = THORX_RK2_GROUPS;
 
 __global__ void __launch_bounds__(kTile* kRk2Groups) update_rk2_kernel(Geometry g, Phys P, State s) {
     const int  c  = (g.tile0 + blockIdx.x) * kTile + threadIdx.x;
