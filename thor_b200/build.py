@@ -7,6 +7,9 @@ libthorx_reforder.so, links the same objects except the dynamical-core kernels, 
 compiled with the reference's own operation order in the FP64 hyperdiffusion and divergence
 damping (THORX_FP64_DIFF_WEIGHTS=0, THORX_FP64_DIVM_WEIGHTS=0) instead of the operator weights;
 it exists for the parity test that keeps the two orders within rounding of each other.
+
+Then thor_b200/bin/esp, the C++ program that runs a simulation from a .thr file (thor_b200/esp/),
+is compiled with the host compiler against libthorx.so's C ABI (found through its run path).
 """
 import os
 import subprocess
@@ -19,6 +22,9 @@ CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libthorx.so")
 LIB_REFORDER = os.path.join(HERE, "libthorx_reforder.so")
+ESP_DIR = os.path.join(HERE, "esp")
+ESP_BIN = os.path.join(HERE, "bin", "esp")
+ESP_SOURCES = ["esp.cpp", "h5file.cpp"]
 
 SOURCES = ["thorx_capi.cu", "dyn_fp64.cu", "rt.cu", "globdiag.cu", "surrogate.cu", "icogrid.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -42,11 +48,33 @@ def deps():
     return d
 
 
+def esp_deps():
+    return [os.path.join(ESP_DIR, f) for f in os.listdir(ESP_DIR)
+            if f.endswith((".cpp", ".h"))] + [os.path.join(ROOT, "include", "thorx.h"), LIB]
+
+
 def needs_build():
     if not (os.path.exists(LIB) and os.path.exists(LIB_REFORDER)):
         return True
     t = min(os.path.getmtime(LIB), os.path.getmtime(LIB_REFORDER))
     return any(os.path.getmtime(d) > t for d in deps())
+
+
+def esp_needs_build():
+    if not os.path.exists(ESP_BIN):
+        return True
+    t = os.path.getmtime(ESP_BIN)
+    return any(os.path.getmtime(d) > t for d in esp_deps())
+
+
+def build_esp(verbose=True):
+    """thor_b200/bin/esp over libthorx.so (run path $ORIGIN/..)."""
+    os.makedirs(os.path.dirname(ESP_BIN), exist_ok=True)
+    cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else os.environ.get("CXX", "g++")
+    _run([cxx, "-O2", "-std=c++17", "-Wall", "-I" + os.path.join(ROOT, "include"), "-o", ESP_BIN]
+         + [os.path.join(ESP_DIR, s) for s in ESP_SOURCES]
+         + ["-L" + HERE, "-l:libthorx.so", "-Wl,-rpath,$ORIGIN/.."], verbose)
+    return ESP_BIN
 
 
 def _run(cmd, verbose):
@@ -61,6 +89,8 @@ def _run(cmd, verbose):
 
 def build(force=False, verbose=True):
     if not force and not needs_build():
+        if esp_needs_build():
+            build_esp(verbose)
         return LIB
     nvcc = os.environ.get("NVCC", "nvcc")
     os.makedirs(OBJ, exist_ok=True)
@@ -77,6 +107,7 @@ def build(force=False, verbose=True):
                 for (s, o, _) in jobs[:len(SOURCES)]]
     _run([nvcc] + LDFLAGS + HOST + ["-o", LIB] + objs, verbose)
     _run([nvcc] + LDFLAGS + HOST + ["-o", LIB_REFORDER] + ref_objs, verbose)
+    build_esp(verbose)
     return LIB
 
 
