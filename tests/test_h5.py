@@ -73,6 +73,63 @@ def test_writer_matches_the_reference_layout(tmp_path, name):
         assert sa[k][1] == sb[k][1], k
 
 
+def _group(d):
+    """(B-tree address, heap address, heap header, {name: SNOD entry bytes}, SNOD headers) of the
+    root group of file bytes d (superblock v0, root symbol-table entry cache)."""
+    import struct
+    bt, hp = struct.unpack_from("<QQ", d, 80)
+    heap_data = struct.unpack_from("<Q", d, hp + 24)[0]
+    used = struct.unpack_from("<H", d, bt + 6)[0]
+    entries, snods = {}, []
+    for i in range(used):
+        child = struct.unpack_from("<Q", d, bt + 24 + 16 * i + 8)[0]
+        snods.append(d[child:child + 6])
+        for s in range(struct.unpack_from("<H", d, child + 6)[0]):
+            e = d[child + 8 + 40 * s:child + 48 + 40 * s]
+            name_off = struct.unpack_from("<Q", e)[0]
+            name = d[heap_data + name_off:d.index(b"\0", heap_data + name_off)].decode()
+            entries[name] = (name_off, e[16:40])
+    return bt, hp, d[hp:hp + 8], entries, snods, d[bt:bt + 6]
+
+
+@pytest.mark.parametrize("name", sorted(PINNED))
+def test_writer_bytes_pinned_to_the_reference_files(tmp_path, name):
+    """Byte-level pins against the files the library wrote: the superblock (signature, versions,
+    sizes of offsets and lengths, group K values, base address, no free-space or driver block,
+    the root symbol-table entry with its cached B-tree and heap addresses), the end-of-file address
+    equal to the file length, the root object header, the group B-tree node header (type 0, leaf),
+    the symbol-table node headers and entry format (cache type 0, empty scratch), and the local
+    heap's packing of the names (the empty name, then each name null-terminated and 8-byte
+    aligned, so the free block starts where the reference's does). Not pinned: the order of the
+    names in the heap (the library's is creation order, the writer's sorted), how the library
+    splits symbol-table nodes (4 to 8 entries each, where the writer fills them) and where it puts
+    the heap's data and the objects after growing them."""
+    import struct
+    src, dst = golden(name), str(tmp_path / "out.h5")
+    rewrite(src, dst)
+    ref, out = open(src, "rb").read(), open(dst, "rb").read()
+    assert out[:40] == ref[:40] and out[48:96] == ref[48:96]
+    for d in (ref, out):
+        assert struct.unpack_from("<Q", d, 40)[0] == len(d)
+    root = struct.unpack_from("<Q", ref, 64)[0]
+    assert out[root:root + 40] == ref[root:root + 40]
+    gr, go = _group(ref), _group(out)
+    assert (gr[0], gr[1]) == (go[0], go[1])                      # B-tree and heap addresses
+    assert go[2] == gr[2] == b"HEAP\0\0\0\0"
+    assert go[5][:4] == gr[5][:4] == b"TREE" and go[5][4:6] == gr[5][4:6] == b"\0\0"
+    assert all(s[:6] == b"SNOD\x01\x00" for s in gr[4] + go[4])
+    assert set(gr[3]) == set(go[3])
+    packed = 8 + sum(-(-(len(n) + 1) // 8) * 8 for n in gr[3])    # the empty name, then each name
+    for g in (gr, go):
+        for n, (off, cache) in g[3].items():
+            assert off % 8 == 0 and cache == b"\0" * 24, n       # aligned; cache type 0, no scratch
+        slots = sorted(off for off, _ in g[3].values())
+        assert slots[0] == 8 and len(set(slots)) == len(slots)
+    free_ref = struct.unpack_from("<Q", ref, gr[1] + 16)[0]
+    free_out = struct.unpack_from("<Q", out, go[1] + 16)[0]
+    assert free_out == free_ref == packed
+
+
 def test_writer_round_trip_many_and_large(tmp_path):
     """More datasets than one symbol-table node holds, long arrays, int32, awkward names and
     an empty unit string."""
