@@ -242,7 +242,9 @@ int thorx_halo_columns(const thorx_grid* grid, int col_begin, int col_end, int* 
 /* All levels and components of the n columns dev_cols (a device array) of a field: copied from src
  * to dst (contexts of the same grid whose devices can reach each other's memory), or packed to /
  * unpacked from dev_buf [n][levels * components] (device). Enqueued on dst's / ctx's stream; the
- * source's last write must be complete (the caller synchronises src). */
+ * source's last write must be complete (the caller synchronises src). In the mixed form the
+ * intermediate "divg" holds FP32 values (the buffer of dev_buf stays doubles, exact both ways);
+ * both contexts of a copy must use the same form. */
 int thorx_copy_columns(thorx_ctx* dst, thorx_ctx* src, const char* field, const int* dev_cols,
                        int n);
 int thorx_pack_columns(thorx_ctx* ctx, const char* field, const int* dev_cols, int n,
@@ -253,7 +255,8 @@ int thorx_unpack_columns(thorx_ctx* ctx, const char* field, const int* dev_cols,
  * components (1 or 3) and the plane stride (doubles): element (lev, col, comp) is at
  * dev[(comp * levels + lev) * plane + col]. Names: the thorx_get_field names and the dycore's
  * stage and deviation arrays "Rhok", "Rhos", "Mhk", "Mhs", "Whk", "Whs", "Wk", "pressurek",
- * "pressures", and "profx_dMh", "profx_dWh" (module tendencies of the slow modes). */
+ * "pressures", and "profx_dMh", "profx_dWh" (module tendencies of the slow modes). A field held
+ * in FP32 (divg in the mixed form) returns THORX_E_UNSUPPORTED. */
 int thorx_device_field(thorx_ctx* ctx, const char* name, double** dev, int* levels,
                        int* components, long* plane);
 

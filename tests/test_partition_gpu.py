@@ -159,3 +159,31 @@ def test_partition_arguments_and_whole_grid_calls_are_rejected():
     x.set_partition(0, g.point_num)  # the whole grid again: no longer partitioned
     x.globdiag()
     x.close(), g.close()
+
+
+@pytest.mark.gpu
+def test_fp32_divg_of_the_mixed_form():
+    """The mixed form keeps divg in FP32 (its values are FP32 results, so the state is the same
+    bits as with FP64 storage): modules are refused its device array, which the FP64 form hands
+    out; switching forms between steps leaves a usable state (divg is recomputed before every
+    use)."""
+    glevel, nv, dt = 4, 8, 1200.0
+    p, c = make_params(glevel, dt)
+    g = RefGrid(glevel, nv)
+    ic = initial_state(g.arrays, g.point_num, nv, c, amp=2.0)
+    x = thor_b200.Thorx(grid_dict(g), glevel, thorx_params(c, dt, precision=1))
+    for k, v in ic.items():
+        x.set(k, v)
+    with pytest.raises(thor_b200.ThorxError) as e:
+        x.device_field("divg")
+    assert e.value.code == thor_b200.E_UNSUPPORTED
+    x.step(1)
+    x.set_precision(0)
+    assert x.device_field("divg")[1:3] == (nv, 3)
+    x.step(1)
+    x.set_precision(1)
+    x.step(1)
+    x.sync()
+    for f in FIELDS:
+        assert np.all(np.isfinite(x.get(f))), f
+    x.close(), g.close()

@@ -78,6 +78,9 @@ constexpr int kColBlock  = 128;
 __device__ __forceinline__ double gz(const double* __restrict__ plane, int id) {
     return id >= 0 ? __ldg(plane + id) : 0.0;
 }
+__device__ __forceinline__ double gz(const float* __restrict__ plane, int id) {
+    return id >= 0 ? (double)__ldg(plane + id) : 0.0;
+}
 
 // DeepModel ? A / (Altitude + A) : 1, from the level table that holds that expression's value
 __device__ __forceinline__ double rscale_of(const Phys&, const Geometry& g, int lev) {
@@ -168,6 +171,10 @@ struct SGeo {
 
 // The mixed form (compute type float) applies the operators through per-column weights.
 template<class R> constexpr bool kOperatorWeights = sizeof(R) < sizeof(double);
+// Storage type of divg (kDivgF32): FP32 in the mixed form (glevel 6, 48 levels: momentum 1.03
+// -> 0.97, divm0 1.13 -> 1.11, slow_modes 0.89 -> 0.87 ms per step, the same bits).
+template<class R>
+using DivgT = std::conditional_t<(kDivgF32 && sizeof(R) < sizeof(double)), float, double>;
 // The FP64 form's hyperdiffusion and divergence damping through FP64 operator weights (the same
 // linear operators as the reference's triangle sequences, summed in another order); 0 restores
 // the reference's operation order.
@@ -1628,7 +1635,7 @@ template<int n, class R>
 __device__ __forceinline__ void divm0_point(const Geometry& g, const Phys& P, const SGeo& G,
                                             const int* ring, int c2, const double* __restrict__ Mh,
                                             const double* __restrict__ Wh,
-                                            double* __restrict__ divg, int c, int lev) {
+                                            DivgT<R>* __restrict__ divg, int c, int lev) {
     const int    Np = g.Np, nv = g.nv;
     const double rscale = rscale_of(P, g, lev);
     const double dz     = 1.0 / (g.Altitudeh[lev] - g.Altitudeh[lev + 1]);
@@ -1650,7 +1657,7 @@ __device__ __forceinline__ void divm0_point(const Geometry& g, const Phys& P, co
         divm_w<n, T>(G, a0, ar, true, dw, rscale, dz, out);
 #pragma unroll
         for (int k = 0; k < 3; k++)
-            divg[(k * nv + lev) * Np + c] = (double)out[k];
+            divg[(k * nv + lev) * Np + c] = (DivgT<R>)out[k];
     }
     else {
         R            a0[3], ar[n][3], wl[n], wt[n];
@@ -1670,7 +1677,7 @@ __device__ __forceinline__ void divm0_point(const Geometry& g, const Phys& P, co
                         (R)rscale, c2, out);
 #pragma unroll
         for (int k = 0; k < 3; k++)
-            divg[(k * nv + lev) * Np + c] = (double)out[k];
+            divg[(k * nv + lev) * Np + c] = (DivgT<R>)out[k];
     }
 }
 
@@ -1786,7 +1793,7 @@ template<int n, class R>
 __device__ __forceinline__ void divm0_body(const Geometry& g, const Phys& P, const SGeo& G,
                                            const double* __restrict__ Mh,
                                            const double* __restrict__ Wh,
-                                           double* __restrict__ divg, int c) {
+                                           DivgT<R>* __restrict__ divg, int c) {
     const int Np = g.Np;
     int       ring[6];
     for (int j = 0; j < 6; j++)
@@ -1815,9 +1822,9 @@ __global__ void THORX_KATTR_DIVM
     if (c < 0)
         return;
     if (tail_cta())
-        divm0_body<5, R>(g, P, G, Mh, Wh, divg, c);
+        divm0_body<5, R>(g, P, G, Mh, Wh, reinterpret_cast<DivgT<R>*>(divg), c);
     else
-        divm0_body<6, R>(g, P, G, Mh, Wh, divg, c);
+        divm0_body<6, R>(g, P, G, Mh, Wh, reinterpret_cast<DivgT<R>*>(divg), c);
 }
 
 // The end of pass 1: the radial component removed, scaled by -Kdhz.
@@ -1836,7 +1843,7 @@ __device__ __forceinline__ void divm_finish(const Geometry& g, int lev, const do
 // Pass 1 of the divergence damping at (column, level): DivM from divg.
 template<int n, class R>
 __device__ __forceinline__ void divm_final(const Geometry& g, const Phys& P, const SGeo& G,
-                                           const int* ring, const double* __restrict__ divg, int c,
+                                           const int* ring, const DivgT<R>* __restrict__ divg, int c,
                                            int lev, const double* fr, R* DivM) {
     const int Np = g.Np, nv = g.nv;
     R         lap[3];
@@ -1907,7 +1914,8 @@ __device__ __forceinline__ void slow_modes_body(const Geometry& g, const Phys& P
         const int i       = lev * Np + c;
         R         DivM[3] = {0, 0, 0};
         if (P.DivDampP)
-            divm_final<n, R>(g, P, G, ring, s.divg, c, lev, fr, DivM);
+            divm_final<n, R>(g, P, G, ring, reinterpret_cast<const DivgT<R>*>(s.divg), c, lev, fr,
+                              DivM);
         const double Cv = cp_at<kUni>(P, s, i) - rd_at<kUni>(P, s, i);
         double       adv[3];
         for (int k = 0; k < 3; k++)
@@ -2124,7 +2132,8 @@ __device__ __forceinline__ void momentum_body(const Geometry& g, const Phys& P, 
     for (int lev = threadIdx.y; lev < nv; lev += kLevGroups) {
         R DivM[3] = {0, 0, 0};
         if (P.DivDampP)
-            divm_final<n, R>(g, P, G, ring, s.divg, c, lev, fr, DivM);
+            divm_final<n, R>(g, P, G, ring, reinterpret_cast<const DivgT<R>*>(s.divg), c, lev, fr,
+                              DivM);
         double pv[7];
 #pragma unroll
         for (int j = 0; j < 7; j++)
@@ -2171,6 +2180,7 @@ __global__ void THORX_KATTR_MOM
 #ifndef THORX_MOM_TMA_BUF
 #define THORX_MOM_TMA_BUF 1
 #endif
+#if THORX_MOM_TMA
 constexpr int      kMomBuf     = THORX_MOM_TMA_BUF;
 constexpr int      kWinFields  = 4; // ps, divg x, y, z
 constexpr int      kWinField   = kWinSpans * kLevGroups * kWinW; // doubles of one field's window
@@ -2178,7 +2188,8 @@ constexpr int      kWinDoubles = kWinFields * kWinField;
 constexpr uint32_t kWinPolls   = 1u << 22;
 // the staged kernel serves the operator-weight forms (the default FP64 form and the mixed form)
 template<class R>
-constexpr bool kMomTma = THORX_MOM_TMA && (kOperatorWeights<R> || kDivmWeightsF64);
+constexpr bool kMomTma = THORX_MOM_TMA && (kOperatorWeights<R> || kDivmWeightsF64)
+                         && std::is_same_v<DivgT<R>, double>;
 size_t momentum_smem_bytes() { return sizeof(double) * kMomBuf * kWinDoubles + 128; }
 static_assert(kWinW * kLevGroups * sizeof(double) % 128 == 0, "window boxes keep 128-byte alignment");
 
@@ -2338,6 +2349,7 @@ __global__ void THORX_KATTR_MOM
             issue(issued++);
     }
 }
+#endif // THORX_MOM_TMA
 
 // ---------------------------------------------------------------------------------------------
 // Small step, vertically implicit part:
@@ -3256,6 +3268,7 @@ struct SmemOptIn {
         return e;
     }
 };
+#if THORX_MOM_TMA
 // A 3-D tensor map over planes [planes][nv][Np] of doubles, boxes {kWinW, 8, 1}; false if the
 // driver's entry point is missing or the map is rejected (alignment, sizes).
 bool window_map(CUtensorMap* map, const double* base, int Np, int nv, int planes) {
@@ -3283,10 +3296,12 @@ bool window_map(CUtensorMap* map, const double* base, int Np, int nv, int planes
                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE)
            == CUDA_SUCCESS;
 }
+#endif
 
 template<class R>
 void launch_momentum_t(const Geometry& g, const Phys& P, const State& s, double dt,
                        cudaStream_t st) {
+#if THORX_MOM_TMA
     if constexpr (kMomTma<R>) {
         CUtensorMap mps, mdivg;
         if (g.Np >= kWinW && window_map(&mps, s.ps, g.Np, g.nv, 1)
@@ -3300,6 +3315,7 @@ void launch_momentum_t(const Geometry& g, const Phys& P, const State& s, double 
             return;
         }
     }
+#endif
     momentum_kernel<R><<<tile_grid_tail(g), tile_block(), 0, st>>>(g, P, s, dt);
 }
 void launch_momentum(const Geometry& g, const Phys& P, const State& s, double dt,

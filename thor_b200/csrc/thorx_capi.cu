@@ -32,9 +32,10 @@
 using namespace thorx;
 
 struct FieldDesc {
-    double** dev; // address of the device pointer in State
-    int      L;   // levels (nv or nv+1)
-    int      K;   // components (1 or 3)
+    double** dev;       // address of the device pointer in State
+    int      L;         // levels (nv or nv+1)
+    int      K;         // components (1 or 3)
+    int      esize = 8; // bytes per element: 4 for divg in the mixed form (kDivgF32)
 };
 
 struct thorx_ctx {
@@ -2128,10 +2129,14 @@ bool find_field(thorx_ctx* ctx, const char* name, FieldDesc* out) {
     if (jt == stage.end())
         return false;
     *out = jt->second;
+    if (jt->first == "divg" && kDivgF32 && ctx->P.mixed)
+        out->esize = 4;
     return *out->dev != nullptr;
 }
 
-__global__ void copy_columns_kernel(double* __restrict__ dst, const double* __restrict__ src,
+extern "C++" { // templates: C++ linkage inside the C ABI block
+template<class T>
+__global__ void copy_columns_kernel(T* __restrict__ dst, const T* __restrict__ src,
                                     const int* __restrict__ cols, int n, int Q, int Np) {
     const long long total = (long long)n * Q;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
@@ -2141,8 +2146,10 @@ __global__ void copy_columns_kernel(double* __restrict__ dst, const double* __re
         dst[k]         = src[k];
     }
 }
-// pack (dir 0): buf[i][q] = field[q][cols[i]]; unpack (dir 1): the reverse
-__global__ void pack_columns_kernel(double* __restrict__ field, double* __restrict__ buf,
+// pack (dir 0): buf[i][q] = field[q][cols[i]]; unpack (dir 1): the reverse (the buffer holds
+// doubles; an FP32 field's values convert exactly both ways)
+template<class T>
+__global__ void pack_columns_kernel(T* __restrict__ field, double* __restrict__ buf,
                                     const int* __restrict__ cols, int n, int Q, int Np, int dir) {
     const long long total = (long long)n * Q;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
@@ -2152,9 +2159,10 @@ __global__ void pack_columns_kernel(double* __restrict__ field, double* __restri
         if (dir == 0)
             buf[(size_t)i * Q + q] = field[k];
         else
-            field[k] = buf[(size_t)i * Q + q];
+            field[k] = (T)buf[(size_t)i * Q + q];
     }
 }
+} // extern "C++"
 unsigned column_blocks(long long total) {
     return (unsigned)std::max<long long>(1, std::min<long long>((total + 255) / 256, 148LL * 16));
 }
@@ -2174,6 +2182,9 @@ int thorx_device_field(thorx_ctx* ctx, const char* name, double** dev, int* leve
     FieldDesc f;
     if (!find_field(ctx, name, &f))
         return fail(ctx, THORX_E_ARG, std::string("thorx_device_field: unknown field ") + name);
+    if (f.esize != 8)
+        return fail(ctx, THORX_E_UNSUPPORTED,
+                    std::string("thorx_device_field: ") + name + " holds FP32 values in the mixed form");
     *dev = *f.dev;
     if (levels)
         *levels = f.L;
@@ -2257,13 +2268,20 @@ int thorx_copy_columns(thorx_ctx* dst, thorx_ctx* src, const char* field, const 
         return THORX_E_ARG;
     FieldDesc fd, fs;
     if (!field || n < 0 || (n > 0 && !dev_cols) || !find_field(dst, field, &fd)
-        || !find_field(src, field, &fs) || dst->g.Np != src->g.Np || dst->g.nv != src->g.nv)
+        || !find_field(src, field, &fs) || dst->g.Np != src->g.Np || dst->g.nv != src->g.nv
+        || fd.esize != fs.esize)
         return fail(dst, THORX_E_ARG, "thorx_copy_columns: bad arguments or field");
     if (n == 0)
         return 0;
-    const int Q = fd.L * fd.K;
-    copy_columns_kernel<<<column_blocks((long long)n * Q), 256, 0, dst->stream>>>(
-        *fd.dev, *fs.dev, dev_cols, n, Q, dst->g.Np);
+    const int      Q  = fd.L * fd.K;
+    const unsigned nb = column_blocks((long long)n * Q);
+    if (fd.esize == 4)
+        copy_columns_kernel<<<nb, 256, 0, dst->stream>>>(
+            reinterpret_cast<float*>(*fd.dev), reinterpret_cast<const float*>(*fs.dev), dev_cols, n,
+            Q, dst->g.Np);
+    else
+        copy_columns_kernel<<<nb, 256, 0, dst->stream>>>(*fd.dev, *fs.dev, dev_cols, n, Q,
+                                                         dst->g.Np);
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? 0
                             : fail(dst, THORX_E_CUDA,
@@ -2279,9 +2297,14 @@ static int pack_unpack(thorx_ctx* ctx, const char* field, const int* dev_cols, i
         return fail(ctx, THORX_E_ARG, "thorx_pack_columns: bad arguments or field");
     if (n == 0)
         return 0;
-    const int Q = f.L * f.K;
-    pack_columns_kernel<<<column_blocks((long long)n * Q), 256, 0, ctx->stream>>>(
-        *f.dev, dev_buf, dev_cols, n, Q, ctx->g.Np, dir);
+    const int      Q  = f.L * f.K;
+    const unsigned nb = column_blocks((long long)n * Q);
+    if (f.esize == 4)
+        pack_columns_kernel<<<nb, 256, 0, ctx->stream>>>(reinterpret_cast<float*>(*f.dev), dev_buf,
+                                                         dev_cols, n, Q, ctx->g.Np, dir);
+    else
+        pack_columns_kernel<<<nb, 256, 0, ctx->stream>>>(*f.dev, dev_buf, dev_cols, n, Q,
+                                                         ctx->g.Np, dir);
     CK(cudaGetLastError());
     return 0;
 }

@@ -75,6 +75,14 @@ struct Geometry {
     // -1 for an unused span ([tiles][kWinSpans]).
     const int*     wspan;
 };
+// The mixed form stores the divergence-damping intermediate divg in FP32 (its values are FP32
+// results, so the state is the same bits either way); the planes keep their [3][nv][Np]
+// indexing within the FP64-sized allocation. THORX_DIVG_F32=0 keeps FP64 storage.
+#ifndef THORX_DIVG_F32
+#define THORX_DIVG_F32 1
+#endif
+constexpr bool kDivgF32 = THORX_DIVG_F32 != 0;
+
 // Columns of a tile (the lanes of a warp); width (columns, even: every box row starts on a
 // 16-byte boundary) and number of the window spans.
 constexpr int kTileCols = 32, kWinW = 36, kWinSpans = 3;
