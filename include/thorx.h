@@ -370,8 +370,10 @@ int thorx_check_division(long long n, unsigned long long seed, long long mismatc
  *   THORX_SUR_LOG  every physics step runs the plain RT and appends each column's inputs and
  *                  heating rates to a ring of log_capacity columns (the training set);
  *   THORX_SUR_USE  every physics step runs the surrogate on all columns and the plain RT only on
- *                  the columns it re-checks this step (column % recheck_period == step %
- *                  recheck_period) and on those that have fallen back: a re-checked column whose
+ *                  the columns it re-checks this step (the blocks of 32 columns with
+ *                  (column / 32) % recheck_period == step % recheck_period, so a warp of the RT
+ *                  kernel re-checks all its columns or none) and on those that have fallen back:
+ *                  a re-checked column whose
  *                  relative error max|q_sur - q_rt| / max|q_rt| (q in K/s, maxima over the
  *                  column's levels) exceeds `tolerance` falls back
  *                  to the plain RT until a later re-check passes; re-checked columns use the

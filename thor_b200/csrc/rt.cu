@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(128) rt_column_kernel(Geometry g, Phys P, RtCo
     const long long nstep = st.cur;
     if (nstep * timestep < (2 * M_PI / c.mean_motion))
         f.insol_ann[id] = f.insol_ann[id] * (nstep - 1) / nstep + f.insol[id] / nstep;
-    if (f.fallback && !(f.fallback[id] || id % f.period == (int)(nstep % f.period)))
+    if (f.fallback && !(f.fallback[id] || recheck_column(id, f.period, nstep)))
         return;
     auto P_ = [&](int lev) { return s.p[lev * Np + id]; };
     auto R_ = [&](int lev) { return s.Rho[lev * Np + id]; };

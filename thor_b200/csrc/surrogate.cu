@@ -253,7 +253,7 @@ __global__ void __launch_bounds__(32 * kCombGroups)
         return;
     const bool valid   = id < g.N;
     const int  nv = g.nv, Np = g.Np;
-    const bool recheck = valid && id % period == (int)(st.cur % period);
+    const bool recheck = valid && recheck_column(id, period, st.cur);
     // heating rates compared as temperature tendencies (K/s): the thin upper layers, whose
     // W/m^3 are small, weigh as much as their temperature change does
     auto rho_cv = [&](int lev) {
@@ -356,7 +356,7 @@ __global__ void log_used_kernel(SurLog lg, SurNet net, Geometry g, State s, RtFi
     if (id >= g.N)
         return;
     const RtStep st = *f.step;
-    if (!st.run || !(f.fallback[id] || id % f.period == (int)(st.cur % f.period)))
+    if (!st.run || !(f.fallback[id] || recheck_column(id, f.period, st.cur)))
         return;
     const long long n   = (long long)atomicAdd((unsigned long long*)lg.count, 1ull);
     const long long row = n % lg.cap;

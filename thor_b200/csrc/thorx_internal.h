@@ -266,6 +266,12 @@ struct RtStep { // per-step scalars, device-resident so that a captured step gra
     double    Qheat_scaling;
     int       run;
 };
+// The surrogate's plain-RT re-check: the columns of every period-th block of 32 (one warp's
+// columns in the RT kernels), rotating with the step, so that every column is re-checked once in
+// `period` steps and the warps of the other blocks have no re-check to run.
+__host__ __device__ inline bool recheck_column(int id, int period, long long step) {
+    return (id >> 5) % period == (int)(step % period);
+}
 struct RtFields { // column-fastest device arrays (interfaces nv+1 planes, tau 2 x nv planes)
     double *phtemp, *thtemp, *ttemp, *dtemp, *qheat, *tau, *fsw_up, *fsw_dn, *flw_up, *flw_dn;
     double *insol, *insol_ann, *ASR, *OLR, *cos_zenith;
