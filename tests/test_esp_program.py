@@ -7,8 +7,10 @@ Without a GPU: the two read every configuration of the CLI tests to the same val
 same messages and exit codes for every rejected configuration and argument set; the program's HDF5
 reader reads the reference-written files as thor_b200/h5.py does, and its writer lays out a file
 byte for byte as h5.py does (apart from the modification times). On the GPU: a Held-Suarez run
-gives output files whose every dataset equals the Python runner's bit for bit, the same logs, a
-bitwise continuation, batch mode and the planet-file check.
+and a hot-Jupiter run (double-gray RT from the Guillot profile, Rayleigh sponge, convective
+adjustment, mixed form) give output files whose every dataset equals the Python runner's bit for
+bit and the same logs; the Held-Suarez run also a bitwise continuation, batch mode and the
+planet-file check.
 """
 import io
 import os
@@ -172,6 +174,62 @@ def test_writer_lays_out_files_as_h5py(program, tmp_path, name):
 
 def datasets(path):
     return {k: (a.dtype.str, a.tobytes(), attrs) for k, (a, attrs) in h5.read(path).items()}
+
+
+# a hot Jupiter with the double-gray RT from the Guillot profile, an implicit Rayleigh sponge,
+# dry convective adjustment and the mixed form: the RT's and the sponge's keys and output fields
+RT_THR = """\
+num_steps = 3
+timestep = 300
+n_out = 3
+globdiag = true
+simulation_ID = HotJ
+radius = 94400000.0
+rotation_rate = 2.06e-5
+gravitation = 9.42
+Rd = 3714.0
+Cp = 13000.0
+Tmean = 1400.0
+P_ref = 10000000.0
+Top_altitude = 4000000.0
+glevel = 4
+vlevel = 20
+core_benchmark = NoBenchmark
+init_PT_profile = guillot
+radiative_transfer = true
+Tstar = 4300.0
+planet_star_dist = 0.015
+radius_star = 0.667
+Tint = 100.0
+kappa_sw = 0.00125
+kappa_lw = 0.0025
+kappa_lw_pole = 0.0025
+RayleighSponge = true
+ns_ray_sponge = 0.7
+conv_adj = true
+precision = mixed
+"""
+
+
+@pytest.mark.gpu
+def test_rt_sponge_mixed_run_matches_the_python_runner(program, tmp_path):
+    cfg = tmp_path / "hj.thr"
+    cfg.write_text(RT_THR)
+    a, b = tmp_path / "cxx", tmp_path / "py"
+    rc, out, err = run_program(program, [cfg, "-o", a], tmp_path)
+    assert rc == 0, out + err
+    prc, pout = run_python([cfg, "-o", b])
+    assert prc == 0, pout
+    assert sorted(os.listdir(a)) == sorted(os.listdir(b))
+    final = h5.read(str(a / "esp_output_HotJ_1.h5"))
+    for k in ("insol", "flw_up", "DGQheat", "ASR", "OLR", "cos_zenith_angles", "GlobalMass"):
+        assert k in final, k
+    assert np.all(np.isfinite(final["Rho"][0]))
+    for n in sorted(os.listdir(a)):
+        if n.endswith(".h5"):
+            assert datasets(str(a / n)) == datasets(str(b / n)), n
+    for n in ("esp_write_log_HotJ.txt", "esp_global_HotJ.txt"):
+        assert (a / n).read_text() == (b / n).read_text(), n
 
 
 @pytest.mark.gpu
