@@ -2748,19 +2748,87 @@ __device__ __forceinline__ void vert_update(const Geometry& g, const Phys& P, co
     }
 }
 
+// Rows of the elimination staged through shared memory by cp.async, kThomasRing interfaces
+// ahead (0: the register prefetch of kThomasPf interfaces instead). The copies hold no registers
+// while in flight, so the ring runs further ahead of the chain than registers allow. glevel 6,
+// 48 levels: vertical 2.84 ms per step with the register prefetch, 2.57 with a ring of 8 (the
+// sweep 14.2 -> 10.0 us per CTA; the register prefetch's spills gone), 2.59 with 4, 2.95 with 16
+// (70.5 KB of shared memory per CTA leave the gathers less L1); the same bits.
+#ifndef THORX_THOMAS_RING
+#define THORX_THOMAS_RING 8
+#endif
+constexpr int kThomasRing = THORX_THOMAS_RING;
+static_assert(kThomasRing == 0 || (kThomasRing & (kThomasRing - 1)) == 0, "a power of two");
+// doubles of the vertical kernel's dynamic shared memory before the ring: sdiv [21][32] and the
+// per-level arrays of the columns ([4][nv][32] with THORX_VERT_SMEM=2)
+__host__ __device__ inline size_t vertical_ring_offset(int nv) {
+    return (size_t)kTile * (21 + (kVertSmem == 2 ? 4 : kVertSmem == 1 ? 2 : 0) * nv);
+}
+__device__ __forceinline__ void cp_async8(double* dst, const double* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(
+                     (unsigned)__cvta_generic_to_shared(dst)),
+                 "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template<int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // The Thomas elimination and back substitution of one column (Vertical_Eq,
 // thor_vertical_int.h:463-484, same operations) from the row planes, the eliminated coefficients in
-// shared memory sc/sd [nv][32]; rows are loaded kThomasPf interfaces ahead of their use, so the
-// chain of dependent divisions does not wait on memory.
+// shared memory sc/sd [nv][32]; rows are loaded ahead of their use (kThomasRing interfaces through
+// the shared-memory ring `ring` [kThomasRing][4][32], else kThomasPf into registers), so the chain
+// of dependent divisions does not wait on memory.
 __device__ __forceinline__ void thomas_column(const Geometry& g, const State& s, LevArr sc,
-                                              LevArr sd, int c) {
+                                              LevArr sd, int c, double* ring) {
     const int     nv = g.nv, Np = g.Np, nvi = g.nvi;
     const double* ra = s.vrows;
     const double* rb = ra + (size_t)nvi * Np;
     const double* rc = rb + (size_t)nvi * Np;
     const double* rd = rc + (size_t)nvi * Np;
     double        cprev = 0, dprev = 0;
-    if constexpr (kThomasPf > 0) {
+    if constexpr (kThomasRing > 0) {
+        const int x     = threadIdx.x;
+        auto      fetch = [&](int lev) { // interface lev into slot (lev - 1) % kThomasRing
+            if (lev < nv) {
+                double*   r = ring + ((lev - 1) & (kThomasRing - 1)) * 4 * kTile + x;
+                const int q = lev * Np + c;
+                cp_async8(r, ra + q);
+                cp_async8(r + kTile, rb + q);
+                cp_async8(r + 2 * kTile, rc + q);
+                cp_async8(r + 3 * kTile, rd + q);
+            }
+            cp_async_commit(); // one group per interface, empty past the top
+        };
+        for (int k = 0; k < kThomasRing; k++)
+            fetch(1 + k);
+        for (int lev = 1; lev < nv; lev++) {
+            cp_async_wait<kThomasRing - 1>(); // the group of interface lev is complete
+            const double* r  = ring + ((lev - 1) & (kThomasRing - 1)) * 4 * kTile + x;
+            const double  aa = r[0], bb = r[kTile];
+            double        ccv = r[2 * kTile], ddv = r[3 * kTile];
+            if (lev == 1) {
+                ccv = ccv / bb;
+                ddv = ddv / bb;
+            }
+            else {
+                const double t = 1.0 / (bb - cprev * aa);
+                ccv *= t;
+                ddv = (ddv - dprev * aa) * t;
+            }
+            sc[lev] = ccv;
+            sd[lev] = ddv;
+            cprev = ccv;
+            dprev = ddv;
+            fetch(lev + kThomasRing); // the slot's values are used: refill it
+        }
+        cp_async_wait<0>();
+    }
+    else if constexpr (kThomasPf > 0) {
         constexpr int kQ = kThomasPf > 0 ? kThomasPf : 1;
         double        qa[kQ], qb[kQ], qc[kQ], qd[kQ];
 #pragma unroll
@@ -2831,6 +2899,23 @@ __device__ __forceinline__ void thomas_column(const Geometry& g, const State& s,
     s.Whs[c] = 0.0;
 }
 
+#ifndef THORX_VERT_CLOCK
+#define THORX_VERT_CLOCK 0
+#endif
+#if THORX_VERT_CLOCK
+// phase timestamps of each CTA of the last launch: [cta][8] = smid, globaltimer at the start,
+// clock64 at the start and after phases 1, 2, 3, the latest warp end, the end of the sweep
+// (warp 0), the latest end of the other warps' phase-3 work
+__device__ unsigned long long g_vclock[16384 * 8];
+__device__ __forceinline__ unsigned long long vclk() { return clock64(); }
+#define VCLOCK(slot)                                                                              \
+    do {                                                                                           \
+        if (threadIdx.x == 0 && threadIdx.y == 0 && blockIdx.x < 16384)                           \
+            g_vclock[blockIdx.x * 8 + (slot)] = vclk();                                            \
+    } while (0)
+#else
+#define VCLOCK(slot) do {} while (0)
+#endif
 template<int kPart, bool kUni>
 __global__ void THORX_KATTR_VERT
     vertical_kernel(Geometry g, Phys P, State s, double deltat) {
@@ -2855,6 +2940,20 @@ __global__ void THORX_KATTR_VERT
     const LevArr sDp  = kVertSmem < 2 ? arr(5) : (kVertMerge ? sSd : sY);
     stage(sdiv, g.div, 21, Np, c0);
     __syncthreads();
+#if THORX_VERT_CLOCK
+    if (threadIdx.x == 0 && threadIdx.y == 0 && blockIdx.x < 16384) {
+        unsigned smid, gt_lo, gt_hi;
+        asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+        unsigned long long gt;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(gt));
+        (void)gt_lo, (void)gt_hi;
+        g_vclock[blockIdx.x * 8 + 0] = smid;
+        g_vclock[blockIdx.x * 8 + 1] = gt;
+        g_vclock[blockIdx.x * 8 + 6] = 0;
+        g_vclock[blockIdx.x * 8 + 7] = 0;
+    }
+#endif
+    VCLOCK(2);
     const bool    active = c < g.N;
     const double  Gravit = P.Gravit;
     const bool    deep = P.DeepModel, nonh = P.NonHydro, ghv = P.GravHeightVar;
@@ -2890,6 +2989,7 @@ __global__ void THORX_KATTR_VERT
         }
     if (kPart != 2)
         __syncthreads();
+    VCLOCK(3);
 
     // ---- phase 2: tridiagonal rows at the interior interfaces ----
     if (kPart != 2 && active) {
@@ -2986,6 +3086,7 @@ __global__ void THORX_KATTR_VERT
     }
     if (kPart != 2)
         __syncthreads();
+    VCLOCK(4);
 
     // ---- phase 3: the Thomas sweep (warp 0); meanwhile the other warps compute what the update
     // needs and the solve does not change: merged, the pressure factor of their update levels;
@@ -2994,7 +3095,8 @@ __global__ void THORX_KATTR_VERT
     double     pre[kVertPre];
     if (kPart != 2 && threadIdx.y == 0) {
         if (active)
-            thomas_column(g, s, sCp, sDp, c);
+            thomas_column(g, s, sCp, sDp, c, smem + vertical_ring_offset(nv));
+        VCLOCK(5);
     }
     else if (kPart == 0 && kVertMerge) {
         if (active && !eeq) {
@@ -3016,7 +3118,19 @@ __global__ void THORX_KATTR_VERT
             sFpt[lev] = Fpt;
         }
     }
+#if THORX_VERT_CLOCK
+    if (threadIdx.y != 0 && threadIdx.x == 0 && blockIdx.x < 16384)
+        atomicMax(&g_vclock[blockIdx.x * 8 + 7], vclk());
+#endif
     __syncthreads();
+#if THORX_VERT_CLOCK
+    struct EndMark {
+        __device__ ~EndMark() {
+            if (threadIdx.x == 0 && blockIdx.x < 16384)
+                atomicMax(&g_vclock[blockIdx.x * 8 + 6], vclk());
+        }
+    } end_mark;
+#endif
     if (kPart == 1 || !active)
         return;
 
@@ -3241,7 +3355,7 @@ void launch_slow_modes(const Geometry& g, const Phys& P, const State& s, bool up
                          : slow_modes_kernel<double, false><<<gr, bl, 0, st>>>(g, P, s, update_rk);
 }
 size_t vertical_smem_bytes(const Geometry& g) {
-    return sizeof(double) * kTile * (21 + (kVertSmem == 2 ? 4 : kVertSmem == 1 ? 2 : 0) * g.nv);
+    return sizeof(double) * (vertical_ring_offset(g.nv) + (size_t)kThomasRing * 4 * kTile);
 }
 
 // The largest dynamic shared memory a kernel has been opened to, per device (the attribute is a
@@ -3434,3 +3548,9 @@ void launch_div_check(long long n, unsigned long long seed, unsigned long long* 
 }
 
 } // namespace thorx
+
+#if THORX_VERT_CLOCK
+extern "C" int thorx_debug_vclock(unsigned long long* host, int n) {
+    return (int)cudaMemcpyFromSymbol(host, thorx::g_vclock, sizeof(unsigned long long) * n);
+}
+#endif
